@@ -1,0 +1,425 @@
+"""Seeded solid-mesh decks in FAST's neutral-file (.dat) format.
+
+A :class:`Deck` holds what FAST's reader builds for the solid hot path, as
+flat arrays: node coordinates, 0-based element incidence in FAST's local node
+order, per-element isotropic material, Gauss order, supports and uniform face
+tractions.  It can be written as a ``.dat`` deck that the reference program
+reads unchanged, and read back from one.
+
+Reference conventions restated here (FAST, paths inside its tree):
+
+* keyword blocks ``%NODE.COORD``, ``%NODE.SUPPORT``, ``%MATERIAL.ISOTROPIC``,
+  ``%SECTION.HOMOGENEOUS.ISOTROPIC.3D``, ``%INTEGRATION.ORDER``,
+  ``%ELEMENT.BRICK8/BRICK20(TL)``, ``%LOAD.CASE.AREA.UNIFORM`` and
+  ``%HEADER.ANALYSIS.*`` (main/input.cpp:76-330; readers node/node.cpp:78-102,
+  289-320, mat/material.cpp:95-119,824-830, sec/section.cpp:96-120,794-806,
+  elc/element.cpp:194-228,1985-2101, elc/elmparam.cpp:221-245,
+  load/load.cpp:229-248,1440-1480);
+* hex8 local order: nodes 1-4 on t=+1, 5-8 on t=-1, counter-clockwise in
+  (r, s) (shp/shpsolid.cpp:173-184); hex20 order shp/shpsolid.cpp:301-325;
+* equation numbers: node order, translational DOFs x, y, z, 1-based, 0 for a
+  fixed or unused DOF (ctrl/ctrl.cpp:2004-2104, cControl::InitDofs/CompEqs);
+* face loads name three corner nodes of the loaded face; the face is the
+  first face of the element whose corner set contains all three
+  (shp/shape.cpp:461-488).
+"""
+from __future__ import annotations
+
+import dataclasses
+import os
+from typing import Optional
+
+import numpy as np
+
+# Natural coordinates of the local nodes, in FAST's order.
+HEX8_NAT = np.array([
+    [-1, -1, 1], [1, -1, 1], [1, 1, 1], [-1, 1, 1],
+    [-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1]], dtype=np.int64)
+HEX20_NAT = np.array([
+    [-1, -1, 1], [0, -1, 1], [1, -1, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1], [-1, 1, 1], [-1, 0, 1],
+    [-1, -1, 0], [1, -1, 0], [1, 1, 0], [-1, 1, 0],
+    [-1, -1, -1], [0, -1, -1], [1, -1, -1], [1, 0, -1], [1, 1, -1], [0, 1, -1], [-1, 1, -1],
+    [-1, 0, -1]], dtype=np.int64)
+
+# Faces: (corner local nodes, face-shape local nodes) (shp/shpsolid.cpp:264-276, 459-471).
+HEX8_FACES = [
+    ((0, 1, 2, 3), (0, 1, 2, 3)), ((3, 2, 6, 7), (3, 2, 6, 7)), ((1, 5, 6, 2), (1, 5, 6, 2)),
+    ((0, 4, 5, 1), (0, 4, 5, 1)), ((0, 3, 7, 4), (0, 3, 7, 4)), ((4, 7, 6, 5), (4, 7, 6, 5))]
+HEX20_FACES = [
+    ((0, 2, 4, 6), (0, 1, 2, 3, 4, 5, 6, 7)),
+    ((2, 0, 12, 14), (2, 1, 0, 8, 12, 13, 14, 9)),
+    ((4, 2, 14, 16), (4, 3, 2, 9, 14, 15, 16, 10)),
+    ((6, 4, 16, 18), (6, 5, 4, 10, 16, 17, 18, 11)),
+    ((12, 18, 16, 14), (12, 19, 18, 17, 16, 15, 14, 13)),
+    ((18, 6, 0, 12), (18, 11, 6, 7, 0, 8, 12, 19))]
+
+KINDS = {"hex8": (8, HEX8_NAT, HEX8_FACES), "hex20": (20, HEX20_NAT, HEX20_FACES)}
+
+
+@dataclasses.dataclass
+class Deck:
+    kind: str                       # "hex8" | "hex20"
+    coords: np.ndarray              # [nnode, 3] float64
+    conn: np.ndarray                # [ne, nn] int32, 0-based node index
+    E: np.ndarray                   # [ne] float64
+    nu: np.ndarray                  # [ne] float64
+    ngp: tuple = (2, 2, 2)          # Gauss order per direction
+    fixed: Optional[np.ndarray] = None   # [nnode, 3] bool, support flags
+    face_elem: Optional[np.ndarray] = None   # [nf] int32 element index
+    face_corners: Optional[np.ndarray] = None  # [nf, 3] int32 node index
+    face_q: Optional[np.ndarray] = None      # [nf, 3] float64 traction
+    face_local: Optional[np.ndarray] = None  # [nf] int32 Local flag
+    rho: Optional[np.ndarray] = None         # [ne] float64 density
+    total_lagrangian: bool = False
+    algorithm: str = "linear"
+    matrix_type: str = "skyline"
+    tol: float = 1e-5
+    maxit: int = 0
+    maxstep: int = 1
+    step_factor: float = 1.0
+    node_labels: Optional[np.ndarray] = None  # [nnode] labels used in a .dat
+    title: str = "deck"
+
+    @property
+    def nn(self) -> int:
+        return KINDS[self.kind][0]
+
+    @property
+    def num_nodes(self) -> int:
+        return int(self.coords.shape[0])
+
+    @property
+    def num_elems(self) -> int:
+        return int(self.conn.shape[0])
+
+    def labels(self) -> np.ndarray:
+        if self.node_labels is None:
+            return np.arange(1, self.num_nodes + 1, dtype=np.int64)
+        return self.node_labels
+
+    def node_eq(self) -> np.ndarray:
+        """1-based equation number per (node, direction); 0 = fixed or unused.
+
+        Follows cControl::InitDofs/CompEqs (ctrl/ctrl.cpp:2004-2104): DOFs
+        are activated by the elements that use the node, supports remove
+        them, and numbering runs over nodes in label order, x, y, z.
+        """
+        active = np.zeros((self.num_nodes, 3), dtype=bool)
+        active[np.unique(self.conn.ravel())] = True
+        if self.fixed is not None:
+            active &= ~self.fixed
+        order = np.argsort(self.labels(), kind="stable")
+        eq = np.zeros((self.num_nodes, 3), dtype=np.int32)
+        flat = active[order].ravel()
+        nums = np.cumsum(flat, dtype=np.int64)
+        eq_sorted = np.where(flat, nums, 0).reshape(-1, 3)
+        eq[order] = eq_sorted
+        return eq
+
+    def num_eq(self) -> int:
+        return int(self.node_eq().max(initial=0))
+
+    def face_nodes(self) -> np.ndarray:
+        """[nf, nface] node indices of each loaded face in face-shape order."""
+        nn, _, faces = KINDS[self.kind]
+        out = []
+        for e, cs in zip(self.face_elem, self.face_corners):
+            en = self.conn[e]
+            for corner, fnodes in faces:
+                cn = set(int(en[c]) for c in corner)
+                if all(int(c) in cn for c in cs):
+                    out.append([int(en[k]) for k in fnodes])
+                    break
+            else:
+                raise ValueError(f"face load on element {e}: corners {cs} match no face")
+        return np.asarray(out, dtype=np.int32)
+
+
+# --------------------------------------------------------------------------
+# structured boxes
+
+def _grid_index(shape, order):
+    """Map grid coordinates to node numbers with the given fastest-first axis order."""
+    idx = -np.ones(shape, dtype=np.int64)
+    return idx
+
+
+def box_mesh(kind: str, n, L, origin=(0.0, 0.0, 0.0), fastest=None) -> tuple:
+    """Structured box of hex8 or hex20 elements.
+
+    Returns ``(coords, conn, grid)``; ``grid`` maps node index -> integer grid
+    coordinate (on the doubled grid for hex20).  Nodes are numbered with the
+    axis of fewest elements varying fastest (a banded numbering), elements in
+    the same axis order.
+    """
+    nx, ny, nz = (int(v) for v in n)
+    Lx, Ly, Lz = (float(v) for v in L)
+    if fastest is None:
+        fastest = tuple(int(a) for a in np.argsort([nx, ny, nz], kind="stable"))
+    m = 1 if kind == "hex8" else 2
+    G = (m * nx + 1, m * ny + 1, m * nz + 1)
+    ii = np.indices(G).reshape(3, -1).T  # all grid points
+    if kind == "hex20":
+        keep = (ii % 2).sum(axis=1) <= 1
+        ii = ii[keep]
+    # sort nodes: key = slowest..fastest axis
+    a0, a1, a2 = fastest
+    okey = np.lexsort((ii[:, a0], ii[:, a1], ii[:, a2]))
+    ii = ii[okey]
+    lut = -np.ones(G, dtype=np.int64)
+    lut[ii[:, 0], ii[:, 1], ii[:, 2]] = np.arange(len(ii))
+    h = np.array([Lx / (m * nx), Ly / (m * ny), Lz / (m * nz)])
+    coords = np.asarray(origin, dtype=np.float64)[None, :] + ii * h[None, :]
+
+    nat = KINDS[kind][1]
+    e = np.indices((nx, ny, nz)).reshape(3, -1).T
+    ekey = np.lexsort((e[:, a0], e[:, a1], e[:, a2]))
+    e = e[ekey]
+    base = m * e  # lower corner on the (doubled) grid
+    off = (nat + 1) * m // 2 if kind == "hex20" else (nat + 1) // 2
+    pts = base[:, None, :] + off[None, :, :]
+    conn = lut[pts[..., 0], pts[..., 1], pts[..., 2]]
+    assert (conn >= 0).all()
+    return coords, conn.astype(np.int32), ii
+
+
+def boundary_faces(kind: str, coords, conn, axis: int, value: float, tol=1e-9):
+    """(element, three corner nodes) for every element face lying on x[axis]==value."""
+    nn, nat, faces = KINDS[kind]
+    elems, corners = [], []
+    for e in range(conn.shape[0]):
+        en = conn[e]
+        for corner, _ in faces:
+            xs = coords[en[list(corner)], axis]
+            if np.all(np.abs(xs - value) < tol):
+                elems.append(e)
+                corners.append([en[corner[0]], en[corner[1]], en[corner[2]]])
+    return np.asarray(elems, np.int32), np.asarray(corners, np.int32)
+
+
+def _boundary_faces_fast(kind, coords, conn, axis, value, tol=1e-9):
+    nn, nat, faces = KINDS[kind]
+    out_e, out_c = [], []
+    for corner, _ in faces:
+        cidx = list(corner)
+        xs = coords[conn[:, cidx], axis]
+        hit = np.all(np.abs(xs - value) < tol, axis=1)
+        es = np.nonzero(hit)[0]
+        out_e.append(es)
+        out_c.append(conn[es][:, cidx[:3]])
+    e = np.concatenate(out_e)
+    c = np.concatenate(out_c)
+    o = np.argsort(e, kind="stable")
+    return e[o].astype(np.int32), c[o].astype(np.int32)
+
+
+def lognormal_E(ne: int, median=1000.0, sigma=0.5, seed=0) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return median * np.exp(sigma * rng.standard_normal(ne))
+
+
+def cantilever_hex8(nx=20, ny=4, nz=4, L=(10.0, 1.0, 1.0), E=1000.0, nu=0.3, q=(0.0, 0.0, -1.0)) -> Deck:
+    """hex8 cantilever: x=0 face clamped, uniform traction on the x=L face.
+
+    Default sizes are the 20x4x4 box on 10x1x1 with 2x2x2 Gauss points,
+    E=1000, nu=0.3 and a traction of -1 in z (1575 DOFs).
+    """
+    coords, conn, _ = box_mesh("hex8", (nx, ny, nz), L)
+    ne = conn.shape[0]
+    fixed = np.zeros((coords.shape[0], 3), bool)
+    fixed[np.abs(coords[:, 0]) < 1e-12] = True
+    fe, fc = _boundary_faces_fast("hex8", coords, conn, 0, L[0])
+    return Deck("hex8", coords, conn, np.full(ne, E), np.full(ne, nu), (2, 2, 2), fixed,
+                fe, fc, np.tile(np.asarray(q, float), (len(fe), 1)), np.zeros(len(fe), np.int32),
+                title=f"hex8 cantilever {nx}x{ny}x{nz}")
+
+
+def box_hex20_lognormal(nx=64, ny=64, nz=32, L=(4.0, 4.0, 2.0), median=1000.0, sigma=0.5, seed=0,
+                        nu=0.3, ngp=3, pressure=1.0) -> Deck:
+    """hex20 box with a lognormal Young's modulus per element.
+
+    z=0 face clamped, unit pressure (traction -p in z) on the top face.  The
+    default 64x64x32 box on 4x4x2 with 3x3x3 Gauss points has 131,072
+    elements and 1,609,920 free equations.
+    """
+    coords, conn, _ = box_mesh("hex20", (nx, ny, nz), L)
+    ne = conn.shape[0]
+    fixed = np.zeros((coords.shape[0], 3), bool)
+    fixed[np.abs(coords[:, 2]) < 1e-12] = True
+    fe, fc = _boundary_faces_fast("hex20", coords, conn, 2, L[2])
+    E = lognormal_E(ne, median, sigma, seed)
+    return Deck("hex20", coords, conn, E, np.full(ne, nu), (ngp, ngp, ngp), fixed,
+                fe, fc, np.tile([0.0, 0.0, -pressure], (len(fe), 1)), np.zeros(len(fe), np.int32),
+                matrix_type="sparse", tol=1e-10, maxit=100000,
+                title=f"hex20 lognormal box {nx}x{ny}x{nz} seed {seed}")
+
+
+# --------------------------------------------------------------------------
+# .dat writer / reader
+
+def _fmt(x: float) -> str:
+    return repr(float(x))
+
+
+def write_dat(deck: Deck, base: str) -> str:
+    """Write ``base + '.dat'`` readable by FAST; returns the path."""
+    path = base + ".dat"
+    lab = deck.labels()
+    nn = deck.nn
+    ne = deck.num_elems
+    lines = ["%HEADER", deck.title, ""]
+    lines += ["%HEADER.ANALYSIS.ALGORITHM", f"'{deck.algorithm}'", ""]
+    lines += ["%HEADER.ANALYSIS.MATRIX.TYPE", f"'{deck.matrix_type}'", ""]
+    lines += ["%HEADER.ANALYSIS.TOLERANCE", _fmt(deck.tol), ""]
+    if deck.maxit:
+        lines += ["%HEADER.ANALYSIS.MAXIMUM.ITERATIONS", str(int(deck.maxit)), ""]
+    if deck.maxstep != 1:
+        lines += ["%HEADER.ANALYSIS.MAXIMUM.STEPS", str(int(deck.maxstep)), ""]
+    if deck.step_factor != 1.0:
+        lines += ["%HEADER.ANALYSIS.STEP.FACTOR", _fmt(deck.step_factor), ""]
+    lines += ["%HEADER.OUTPUT.PRECISION", "15", ""]
+    lines += ["%NODE", str(deck.num_nodes), "", "%NODE.COORD", str(deck.num_nodes)]
+    lines += [f"{int(l)} {_fmt(x)} {_fmt(y)} {_fmt(z)}" for l, (x, y, z) in zip(lab, deck.coords)]
+    lines.append("")
+    if deck.fixed is not None and deck.fixed.any():
+        sup = np.nonzero(deck.fixed.any(axis=1))[0]
+        lines += ["%NODE.SUPPORT", str(len(sup))]
+        lines += [f"{int(lab[i])} {int(deck.fixed[i,0])} {int(deck.fixed[i,1])} {int(deck.fixed[i,2])} 0 0 0" for i in sup]
+        lines.append("")
+    # one material per distinct (E, nu) pair, one section per material
+    pairs = np.stack([deck.E, deck.nu], axis=1)
+    uniq, inv = np.unique(pairs, axis=0, return_inverse=True)
+    inv = inv.ravel()
+    nm = len(uniq)
+    lines += ["%MATERIAL", str(nm), "", "%MATERIAL.ISOTROPIC", str(nm)]
+    lines += [f"{i+1} {_fmt(E)} {_fmt(nu)}" for i, (E, nu) in enumerate(uniq)]
+    lines.append("")
+    if deck.rho is not None:
+        # density is per material; one density per distinct material is required
+        dens = np.zeros(nm)
+        dens[inv] = deck.rho
+        lines += ["%MATERIAL.DENSITY", str(nm)] + [f"{i+1} {_fmt(d)}" for i, d in enumerate(dens)] + [""]
+    lines += ["%SECTION", str(nm), "", "%SECTION.HOMOGENEOUS.ISOTROPIC.3D", str(nm)]
+    lines += [f"{i+1} {i+1}" for i in range(nm)]
+    lines.append("")
+    g = deck.ngp
+    lines += ["%INTEGRATION.ORDER", "1", f"1 {g[0]} {g[1]} {g[2]} {g[0]} {g[1]} {g[2]}", ""]
+    key = {"hex8": "BRICK8", "hex20": "BRICK20"}[deck.kind] + ("TL" if deck.total_lagrangian else "")
+    lines += ["%ELEMENT", str(ne), "", f"%ELEMENT.{key}", str(ne)]
+    cl = lab[deck.conn]
+    lines += [f"{e+1} {inv[e]+1} 1 " + " ".join(str(int(v)) for v in cl[e]) for e in range(ne)]
+    lines.append("")
+    if deck.face_elem is not None and len(deck.face_elem):
+        nf = len(deck.face_elem)
+        lines += ["%LOAD", "1", "1 'Load_Case_1'", "%LOAD.CASE", "1", "%LOAD.CASE.AREA.UNIFORM", str(nf)]
+        for k in range(nf):
+            c = lab[deck.face_corners[k]]
+            q = deck.face_q[k]
+            lines.append(f"{int(deck.face_elem[k])+1} {int(c[0])} {int(c[1])} {int(c[2])} "
+                         f"{int(deck.face_local[k])} {_fmt(q[0])} {_fmt(q[1])} {_fmt(q[2])}")
+        lines.append("")
+    lines += ["%END", ""]
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    with open(path, "w") as fp:
+        fp.write("\n".join(lines))
+    return path
+
+
+def _tokens_by_label(text: str) -> dict:
+    blocks, cur, buf = {}, None, []
+    for raw in text.splitlines():
+        s = raw.strip()
+        if s.startswith("%"):
+            if cur is not None:
+                blocks[cur] = buf
+            cur, buf = s[1:].split()[0], []
+        elif cur is not None:
+            buf.extend(s.split())
+    if cur is not None:
+        blocks[cur] = buf
+    return blocks
+
+
+def read_dat(path: str) -> Deck:
+    """Read the solid hot-path subset of a FAST ``.dat`` deck."""
+    with open(path) as fp:
+        blk = _tokens_by_label(fp.read())
+    t = blk["NODE.COORD"]
+    n = int(t[0])
+    arr = np.array(t[1:1 + 4 * n], dtype=np.float64).reshape(n, 4)
+    labels = arr[:, 0].astype(np.int64)
+    order = np.argsort(labels)
+    labels = labels[order]
+    coords = arr[order, 1:4].copy()
+    l2i = {int(l): i for i, l in enumerate(labels)}
+    fixed = np.zeros((n, 3), bool)
+    if "NODE.SUPPORT" in blk:
+        t = blk["NODE.SUPPORT"]
+        ns = int(t[0])
+        a = np.array(t[1:1 + 7 * ns], dtype=np.int64).reshape(ns, 7)
+        for row in a:
+            fixed[l2i[int(row[0])]] |= row[1:4].astype(bool)
+    mats = {}
+    t = blk.get("MATERIAL.ISOTROPIC", ["0"])
+    for k in range(int(t[0])):
+        mid, E, nu = t[1 + 3 * k: 4 + 3 * k]
+        mats[int(mid)] = (float(E), float(nu))
+    dens = {}
+    if "MATERIAL.DENSITY" in blk:
+        t = blk["MATERIAL.DENSITY"]
+        for k in range(int(t[0])):
+            dens[int(t[1 + 2 * k])] = float(t[2 + 2 * k])
+    secs = {}
+    t = blk.get("SECTION.HOMOGENEOUS.ISOTROPIC.3D", ["0"])
+    for k in range(int(t[0])):
+        secs[int(t[1 + 2 * k])] = int(t[2 + 2 * k])
+    t = blk["INTEGRATION.ORDER"]
+    ords = {}
+    for k in range(int(t[0])):
+        row = [int(v) for v in t[1 + 7 * k: 8 + 7 * k]]
+        ords[row[0]] = tuple(row[1:4])
+    kind, tl, key = None, False, None
+    for k, (kd, t_) in {"ELEMENT.BRICK8": ("hex8", False), "ELEMENT.BRICK20": ("hex20", False),
+                        "ELEMENT.BRICK8TL": ("hex8", True), "ELEMENT.BRICK20TL": ("hex20", True)}.items():
+        if k in blk:
+            if kind is not None:
+                raise ValueError("decks with more than one solid element type are not read here")
+            kind, tl, key = kd, t_, k
+    nn = KINDS[kind][0]
+    t = blk[key]
+    ne = int(t[0])
+    a = np.array(t[1:1 + (3 + nn) * ne], dtype=np.int64).reshape(ne, 3 + nn)
+    a = a[np.argsort(a[:, 0])]
+    elem_labels = a[:, 0]
+    conn = np.vectorize(lambda l: l2i[int(l)])(a[:, 3:]).astype(np.int32)
+    E = np.array([mats[secs[int(s)]][0] for s in a[:, 1]])
+    nu = np.array([mats[secs[int(s)]][1] for s in a[:, 1]])
+    rho = np.array([dens.get(secs[int(s)], 0.0) for s in a[:, 1]]) if dens else None
+    ordset = {ords[int(o)] for o in a[:, 2]}
+    if len(ordset) != 1:
+        raise ValueError("one integration order per deck is read here")
+    ngp = ordset.pop()
+    e2i = {int(l): i for i, l in enumerate(elem_labels)}
+    fe = fc = fq = fl = None
+    if "LOAD.CASE.AREA.UNIFORM" in blk:
+        t = blk["LOAD.CASE.AREA.UNIFORM"]
+        nf = int(t[0])
+        rows = [t[1 + 8 * k: 9 + 8 * k] for k in range(nf)]
+        fe = np.array([e2i[int(r[0])] for r in rows], np.int32)
+        fc = np.array([[l2i[int(v)] for v in r[1:4]] for r in rows], np.int32)
+        fl = np.array([int(r[4]) for r in rows], np.int32)
+        fq = np.array([[float(v) for v in r[5:8]] for r in rows])
+
+    def s1(label, default, cast):
+        if label in blk and blk[label]:
+            return cast(blk[label][0].strip("'"))
+        return default
+
+    return Deck(kind, coords, conn, E, nu, ngp, fixed, fe, fc, fq, fl, rho, tl,
+                algorithm=s1("HEADER.ANALYSIS.ALGORITHM", "linear", str),
+                matrix_type=s1("HEADER.ANALYSIS.MATRIX.TYPE", "skyline", str),
+                tol=s1("HEADER.ANALYSIS.TOLERANCE", 1e-5, float),
+                maxit=s1("HEADER.ANALYSIS.MAXIMUM.ITERATIONS", 0, int),
+                maxstep=s1("HEADER.ANALYSIS.MAXIMUM.STEPS", 1, int),
+                step_factor=s1("HEADER.ANALYSIS.STEP.FACTOR", 1.0, float),
+                node_labels=labels, title=os.path.basename(path))

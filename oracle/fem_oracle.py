@@ -1,0 +1,161 @@
+"""Python side of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Loads ``oracle/_build/libfem_oracle.so`` (the C restatement in
+``fem_oracle.c``) and offers whole-deck helpers built from it: element
+matrices, the assembled equation-space matrix, the external load vector and
+FAST's Jacobi PCG.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` import this module, and only as a checker.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libfem_oracle.so")
+
+_lib = None
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        L.fo_elem_stiff.argtypes = [ctypes.c_int, _ip, _dp, ctypes.c_double, ctypes.c_double, _dp]
+        L.fo_elems_stiff.argtypes = [ctypes.c_int, _ip, ctypes.c_int64, ctypes.POINTER(ctypes.c_int32), _dp, _dp, _dp, _dp]
+        L.fo_elem_intforce.argtypes = [ctypes.c_int, _ip, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp]
+        L.fo_elem_mass.argtypes = [ctypes.c_int, _ip, _dp, ctypes.c_double, _dp]
+        L.fo_elem_tl.argtypes = [ctypes.c_int, _ip, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp]
+        L.fo_face_load.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp]
+        L.fo_pcg.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32), _dp,
+                             _dp, _dp, ctypes.c_int, ctypes.c_double, _ip, _dp]
+        L.fo_spmv.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32), _dp, _dp, _dp]
+        _lib = L
+    return _lib
+
+
+def _p(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+def _ngp(ngp):
+    return (ctypes.c_int * 3)(*[int(v) for v in ngp])
+
+
+def elem_stiff(nn, ngp, X, E, nu):
+    K = np.zeros((3 * nn, 3 * nn))
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    rc = lib().fo_elem_stiff(nn, _ngp(ngp), _p(X), float(E), float(nu), _p(K))
+    return K, rc
+
+
+def elems_stiff(deck, elems=None):
+    nn = deck.nn
+    conn = deck.conn if elems is None else deck.conn[elems]
+    E = deck.E if elems is None else deck.E[elems]
+    nu = deck.nu if elems is None else deck.nu[elems]
+    conn = np.ascontiguousarray(conn, dtype=np.int32)
+    X = np.ascontiguousarray(deck.coords, dtype=np.float64)
+    E = np.ascontiguousarray(E, dtype=np.float64)
+    nu = np.ascontiguousarray(nu, dtype=np.float64)
+    Ke = np.zeros((conn.shape[0], 3 * nn, 3 * nn))
+    rc = lib().fo_elems_stiff(nn, _ngp(deck.ngp), conn.shape[0], _p(conn, ctypes.POINTER(ctypes.c_int32)),
+                              _p(X), _p(E), _p(nu), _p(Ke))
+    return Ke, rc
+
+
+def elem_intforce(nn, ngp, X, E, nu, ue):
+    g = np.zeros(3 * nn)
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    ue = np.ascontiguousarray(ue, dtype=np.float64)
+    rc = lib().fo_elem_intforce(nn, _ngp(ngp), _p(X), float(E), float(nu), _p(ue), _p(g))
+    return g, rc
+
+
+def elem_mass(nn, ngp, X, rho):
+    M = np.zeros((3 * nn, 3 * nn))
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    rc = lib().fo_elem_mass(nn, _ngp(ngp), _p(X), float(rho), _p(M))
+    return M, rc
+
+
+def elem_tl(nn, ngp, X, E, nu, ue):
+    K = np.zeros((3 * nn, 3 * nn))
+    g = np.zeros(3 * nn)
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    ue = np.ascontiguousarray(ue, dtype=np.float64)
+    rc = lib().fo_elem_tl(nn, _ngp(ngp), _p(X), float(E), float(nu), _p(ue), _p(K), _p(g))
+    return K, g, rc
+
+
+def elem_dofs(deck):
+    """[ne][3nn] 1-based equations (cElement::GetElmDofs order: node-major, x y z)."""
+    eq = deck.node_eq()
+    return eq[deck.conn].reshape(deck.num_elems, -1)
+
+
+def assemble(deck, Ke=None):
+    """Equation-space K (scipy CSR, full symmetric) from element matrices."""
+    import scipy.sparse as sp
+    if Ke is None:
+        Ke, _ = elems_stiff(deck)
+    dofs = elem_dofs(deck)
+    neq = deck.num_eq()
+    nd = dofs.shape[1]
+    I = np.repeat(dofs, nd, axis=1).ravel()
+    J = np.tile(dofs, (1, nd)).ravel()
+    V = Ke.reshape(len(dofs), -1).ravel()
+    m = (I > 0) & (J > 0)
+    K = sp.csr_matrix((V[m], (I[m] - 1, J[m] - 1)), shape=(neq, neq))
+    K.sum_duplicates()
+    K.sort_indices()
+    return K
+
+
+def face_loads(deck):
+    """External load vector (cControl::ExtLoadVector, ctrl/ctrl.cpp:668-715)."""
+    neq = deck.num_eq()
+    f = np.zeros(neq)
+    if deck.face_elem is None or not len(deck.face_elem):
+        return f
+    eq = deck.node_eq()
+    fn = deck.face_nodes()
+    nf = fn.shape[1]
+    ngp1d = max(deck.ngp)
+    for k in range(len(fn)):
+        Xf = np.ascontiguousarray(deck.coords[fn[k]])
+        fe = np.zeros(3 * nf)
+        q = np.ascontiguousarray(deck.face_q[k], dtype=np.float64)
+        lib().fo_face_load(nf, ngp1d, _p(Xf), _p(q), int(deck.face_local[k]), _p(fe))
+        dofs = eq[fn[k]].ravel()
+        for i in range(3 * nf):
+            if dofs[i]:
+                f[dofs[i] - 1] += fe[i]
+    return f
+
+
+def pcg(K, f, tol, maxit):
+    """FAST's Jacobi PCG on a scipy CSR matrix; returns (u, converged, iters, err)."""
+    n = K.shape[0]
+    rp = np.ascontiguousarray(K.indptr, dtype=np.int64)
+    ci = np.ascontiguousarray(K.indices, dtype=np.int32)
+    v = np.ascontiguousarray(K.data, dtype=np.float64)
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    u = np.zeros(n)
+    it = ctypes.c_int(0)
+    err = ctypes.c_double(0)
+    ok = lib().fo_pcg(n, _p(rp, ctypes.POINTER(ctypes.c_int64)), _p(ci, ctypes.POINTER(ctypes.c_int32)), _p(v),
+                      _p(f), _p(u), int(maxit), float(tol), ctypes.byref(it), ctypes.byref(err))
+    return u, bool(ok), it.value, err.value

@@ -1,0 +1,142 @@
+"""Regenerate the golden fixtures in this directory from the reference FAST
+program itself.
+
+Run in a container that has the reference tree (default /root/reference,
+override with FAST_REF):
+
+    python tests/golden/make_golden.py
+
+It builds ``oracle/_ref/fastref`` (the reference's own sources compiled by
+``oracle/Makefile``, plus a dump harness), writes each deck with
+``fast_b200.decks.write_dat`` (or copies a deck shipped with the reference),
+runs the harness on it and stores the reference's element matrices, recorded
+global-matrix Add calls, load vector and displacements as ``.npz``.  Nothing
+here is hand-written data: every number comes out of the reference run.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
+sys.path.insert(0, ROOT)
+
+from fast_b200 import decks  # noqa: E402
+from oracle import refdump  # noqa: E402
+
+FAST_REF = os.environ.get("FAST_REF", "/root/reference")
+
+
+def deck_arrays(d: decks.Deck) -> dict:
+    out = dict(kind=np.array(d.kind), coords=d.coords, conn=d.conn, E=d.E, nu=d.nu,
+               ngp=np.array(d.ngp, np.int32), fixed=d.fixed, tl=np.array(int(d.total_lagrangian)))
+    if d.face_elem is not None:
+        out.update(face_elem=d.face_elem, face_corners=d.face_corners, face_q=d.face_q,
+                   face_local=d.face_local)
+    if d.rho is not None:
+        out["rho"] = d.rho
+    if d.node_labels is not None:
+        out["node_labels"] = d.node_labels
+    return out
+
+
+def lower_csr(ref: dict):
+    n = int(ref["neq"][0])
+    K = refdump.lower_csr_from_triplets(n, ref["K_i"], ref["K_j"], ref["K_v"])
+    return dict(K_indptr=K.indptr.astype(np.int64), K_indices=K.indices.astype(np.int32), K_data=K.data)
+
+
+def run_case(name, deck, tmp, keep_elems=None, triplets=True, extra=(), uvec=None, mass=False):
+    base = os.path.join(tmp, name)
+    decks.write_dat(deck, base)
+    opts = list(extra)
+    if not triplets:
+        opts.append("--no-triplets")
+    if mass:
+        opts.append("--mass")
+    if uvec is not None:
+        upath = base + ".u.f8"
+        np.asarray(uvec, "<f8").tofile(upath)
+        opts += ["--u", upath]
+    ref = refdump.run_dump(base, base + ".bin", *opts)
+    out = deck_arrays(deck)
+    out["ref_neq"] = ref["neq"]
+    out["ref_node_eq"] = ref["node_eq"]
+    sel = slice(None) if keep_elems is None else np.asarray(keep_elems)
+    out["ref_elems"] = np.arange(deck.num_elems)[sel]
+    out["ref_elm_K"] = ref["elm_K"][sel]
+    out["ref_elm_g"] = ref["elm_g"][sel]
+    out["ref_elm_dofs"] = ref["elm_dofs"]
+    if "elm_M" in ref:
+        out["ref_elm_M"] = ref["elm_M"][sel]
+    out["ref_f"] = ref["f"]
+    if triplets:
+        out.update({"ref_" + k: v for k, v in lower_csr(ref).items()})
+    if "u" in ref:
+        out["ref_u"] = ref["u"]
+        out["ref_g_of_u"] = ref["g_of_u"]
+    if uvec is not None:
+        out["u_state"] = np.asarray(uvec)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(f"{name}: neq={int(ref['neq'][0])} ne={deck.num_elems} "
+          f"-> {os.path.getsize(os.path.join(HERE, name + '.npz')) / 1e6:.2f} MB")
+
+
+def main():
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"FAST_REF={FAST_REF}", "ref"], check=True)
+    tmp = tempfile.mkdtemp(prefix="golden_")
+    try:
+        # known-answer decks shipped with the reference
+        for nm, rel in [("ref_testb8", "dat/continuum/TestB8.dat"), ("ref_beamb20", "dat/continuum/BeamB20.dat")]:
+            src = os.path.join(FAST_REF, rel)
+            d = decks.read_dat(src)
+            base = os.path.join(tmp, nm)
+            shutil.copy(src, base + ".dat")
+            os.chmod(base + ".dat", 0o644)
+            ref = refdump.run_dump(base, base + ".bin")
+            out = deck_arrays(d)
+            keep = np.arange(min(4, d.num_elems))
+            out.update(ref_neq=ref["neq"], ref_node_eq=ref["node_eq"], ref_elems=keep,
+                       ref_elm_K=ref["elm_K"][keep], ref_elm_dofs=ref["elm_dofs"], ref_f=ref["f"],
+                       ref_u=ref["u"], ref_g_of_u=ref["g_of_u"])
+            if d.num_elems <= 8:
+                out.update({"ref_" + k: v for k, v in lower_csr(ref).items()})
+            np.savez_compressed(os.path.join(HERE, nm + ".npz"), **out)
+            print(nm, "written")
+
+        # hex8 cantilever 20x4x4 (1500 equations), skyline + Crout
+        run_case("cfg_hex8_cantilever", decks.cantilever_hex8(), tmp)
+
+        # hex20 lognormal boxes (sparse Jacobi-PCG in the reference), small enough for full dumps
+        d = decks.box_hex20_lognormal(4, 4, 2, seed=7)
+        d.tol = 1e-13
+        run_case("cfg_hex20_lognormal_4x4x2", d, tmp)
+        d = decks.box_hex20_lognormal(8, 8, 4, seed=11)
+        d.tol = 1e-12
+        run_case("cfg_hex20_lognormal_8x8x4", d, tmp, keep_elems=np.arange(0, 256, 17), triplets=False)
+
+        # hex8 with density: consistent mass matrices
+        d = decks.cantilever_hex8(4, 2, 2)
+        d.rho = np.full(d.num_elems, 1e-3)
+        run_case("cfg_hex8_mass", d, tmp, mass=True)
+
+        # total-Lagrangian hex8 plate evaluated at a seeded displacement state
+        d = decks.cantilever_hex8(4, 4, 2, L=(4.0, 4.0, 0.4))
+        d.total_lagrangian = True
+        d.algorithm = "lcm"
+        rng = np.random.default_rng(3)
+        neq = d.num_eq()
+        u = 0.05 * rng.standard_normal(neq)
+        run_case("cfg_hex8_tl_state", d, tmp, uvec=u, triplets=False)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+if __name__ == "__main__":
+    main()

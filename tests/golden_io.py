@@ -1,0 +1,37 @@
+"""Load the golden fixtures (made by tests/golden/make_golden.py from the
+reference FAST program) as a Deck plus the reference outputs."""
+import os
+
+import numpy as np
+
+from fast_b200 import decks
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def names():
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+
+
+def load(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    g = {k: z[k] for k in z.files}
+    fq = g.get("face_q")
+    d = decks.Deck(str(g["kind"]), g["coords"], g["conn"].astype(np.int32), g["E"], g["nu"],
+                   tuple(int(v) for v in g["ngp"]), g["fixed"].astype(bool),
+                   g.get("face_elem"), g.get("face_corners"), fq, g.get("face_local"),
+                   g.get("rho"), bool(int(g["tl"])), node_labels=g.get("node_labels"), title=name)
+    return d, g
+
+
+def lower_K(g):
+    import scipy.sparse as sp
+    n = int(g["ref_neq"][0])
+    return sp.csr_matrix((g["ref_K_data"], g["ref_K_indices"], g["ref_K_indptr"]), shape=(n, n))
+
+
+def rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    den = np.abs(b).max()
+    return float(np.abs(a - b).max() / (den if den > 0 else 1.0))
