@@ -1,0 +1,375 @@
+#!/usr/bin/env python
+"""Linear-static benchmark of the element-integration -> assembly -> K.u solve
+path on a hex20 box (64x64x32 elements on 4x4x2, 3x3x3 Gauss points,
+lognormal Young's modulus per element, z=0 clamped, unit pressure on top:
+131,072 elements, 1,609,920 equations).
+
+One step = assemble K from the element integrals (FP64, colour-scheduled
+scatter) and solve K u = f to |r|/|f| <= 1e-8.  The headline value is
+equations solved per second (DOF/s = num_eq / step time).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision mixed|fp64] [--precond jacobi|block]
+
+--impl reference runs the reference FAST program's own CPU code (built from
+its sources into oracle/_ref by oracle/Makefile) on the same workload: it
+assembles the full matrix once with cControl::StiffnessMatrix into its sparse
+matrix, then times samples of PCGSolver iterations; its solve time is the
+assembly time plus the per-iteration time times the FP64 Jacobi-PCG iteration
+count of this workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX, NY, NZ = 64, 64, 32
+TOL = 1e-8
+SEED = 0
+METRIC = "linear static hex20 box 64x64x32 (assemble K + solve to |r|/|f|<=1e-8): equations solved per second"
+UNIT = "DOF/s"
+# Jacobi-PCG iterations from u = 0 to |r|/|f| < 1e-8 on this workload: the
+# iteration count of the reference's PCGSolver algorithm, taken from the FP64
+# Jacobi solve this script runs on the device (the same iteration, FP64).
+FP64_JACOBI_ITERS = None
+FALLBACK_HBM_GBS = 6650.0
+
+
+def workload_config(args, deck_neq=None):
+    return {"workload": f"hex20 box {NX}x{NY}x{NZ} on 4x4x2, 3x3x3 Gauss, lognormal E (median 1000, sigma 0.5, "
+                        f"seed {SEED}), nu 0.3, z=0 clamped, unit pressure on z=2; assemble K then solve to "
+                        f"|r|/|f|<={TOL:g}",
+            "elements": NX * NY * NZ, "equations": deck_neq, "precision": args.precision,
+            "precond": args.precond, "l2": "inputs larger than L2 (block matrix 2.2 GB FP64)",
+            "parallelism": "replicas" if args.gpus > 1 else "single"}
+
+
+def measured_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fp:
+            return float(json.load(fp)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(neq_full, nnz_lower_full, ne_full, iters_fp64):
+    """Reference FAST CPU path on a bounded sample (1 host thread)."""
+    from fast_b200 import decks
+    from oracle import refdump
+    if not refdump.available():
+        return None
+    n = 16
+    d = decks.box_hex20_lognormal(n, n, n // 2, seed=SEED)
+    with tempfile.TemporaryDirectory() as tmp:
+        base = os.path.join(tmp, "sample")
+        decks.write_dat(d, base)
+        r = refdump.run_bench(base, 20, 1)
+    t_elem = r["assembly_s"] / r["ne"]
+    t_nnz_iter = r["pcg_s"] / (r["pcg_iters"] * r["nnz_lower"])
+    T = ne_full * t_elem + iters_fp64 * nnz_lower_full * t_nnz_iter
+    return {"value": neq_full / T, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": (f"reference FAST (oracle/_ref) on the same box at {n}x{n}x{n//2} ({r['ne']} elements, "
+                       f"{r['neq']} eq): StiffnessMatrix into cSymSprsMatrix ({r['assembly_s']:.2f} s) + "
+                       f"{r['pcg_iters']} PCGSolver iterations ({r['pcg_s']:.2f} s); per-element and "
+                       f"per-nonzero-iteration costs scaled to {ne_full} elements, {nnz_lower_full} stored "
+                       f"nonzeros and {iters_fp64} iterations"),
+            "seconds_per_solve": T}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from fast_b200 import decks
+    from oracle import refdump
+    if not refdump.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/fastref was not built "
+                          "(the reference sources are needed to build it)"}))
+        return 0
+    if FP64_JACOBI_ITERS is None:
+        print(json.dumps({"impl": "reference", "unavailable": "FP64 Jacobi-PCG iteration count of this workload "
+                          "not recorded yet"}))
+        return 0
+    d = decks.box_hex20_lognormal(NX, NY, NZ, seed=SEED)
+    d.tol = TOL
+    reps = max(1, min(args.warmup + args.steps, 40))
+    t0 = time.time()
+    with tempfile.TemporaryDirectory() as tmp:
+        base = os.path.join(tmp, "box")
+        decks.write_dat(d, base)
+        r = refdump.run_bench(base, 1, reps)
+    wall = time.time() - t0
+    per_iter = r["pcg_rep_s"][min(args.warmup, reps - 1):]
+    t_iter = statistics.mean(per_iter)
+    T = r["assembly_s"] + FP64_JACOBI_ITERS * t_iter
+    value = r["neq"] / T
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": len(per_iter),
+            "warmup": min(args.warmup, reps - 1), "ms_per_step": T * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(args, r["neq"]), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                             "sample": (f"reference FAST (oracle/_ref), 1 thread, full {NX}x{NY}x{NZ} deck: "
+                                        f"StiffnessMatrix into cSymSprsMatrix once ({r['assembly_s']:.1f} s), then "
+                                        f"{len(per_iter)} timed single PCGSolver iterations "
+                                        f"({t_iter:.3f} s each, {r['nnz_lower']} stored nonzeros); solve time = "
+                                        f"assembly + {FP64_JACOBI_ITERS} iterations")},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_detail": {"assembly_s": r["assembly_s"], "integration_s": r["integration_s"],
+                                 "read_s": r["read_s"], "pcg_iter_s": t_iter, "wall_s": wall}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from fast_b200 import decks, gpu
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    prec = gpu.PREC_MIXED if args.precision == "mixed" else gpu.PREC_FP64
+    pc = gpu.PRECOND_BLOCK_JACOBI if args.precond == "block" else gpu.PRECOND_JACOBI
+
+    deck = decks.box_hex20_lognormal(NX, NY, NZ, seed=SEED)
+    f = gpu.face_load_vector(deck)
+    neq = deck.num_eq()
+    S = gpu.GpuSystem(local)
+    t0 = time.time()
+    S.upload(deck)
+    setup_s = time.time() - t0
+    pinfo = S.pattern_info()
+    # the library runs on an explicit (non-NULL) torch stream so that the CUDA
+    # events recorded below bracket its kernels
+    stream = torch.cuda.Stream(dev)
+    d_f = torch.from_numpy(f).to(dev)
+    d_u = torch.zeros(neq, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize(dev)
+    S.set_stream(stream.cuda_stream)
+
+    def step(precision=prec, precond=pc):
+        S.assemble()
+        return S.solve_device(d_f.data_ptr(), d_u.data_ptr(), tol=TOL, precision=precision, precond=precond)
+
+    for _ in range(args.warmup):
+        rep = step()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- timed region: device-resident inputs
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    n0 = S.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    reps = []
+    for _ in range(args.steps):
+        reps.append(step())
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    n1 = S.launch_count()
+    clk = clocks.stop()
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    ms = max_over_ranks(ms)
+    value = world * neq / (ms / 1e3)
+    u_main = d_u.cpu().numpy().copy()
+    last = reps[-1]
+
+    # ---- plain FP64 GPU path (the reference's Jacobi PCG) for comparison, timed once
+    ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ea.record(stream)
+    rep64 = step(gpu.PREC_FP64, gpu.PRECOND_JACOBI)
+    eb.record(stream)
+    torch.cuda.synchronize(dev)
+    ms64 = ea.elapsed_time(eb)
+    u64 = d_u.cpu().numpy().copy()
+    rel_u = float(np.abs(u_main - u64).max() / np.abs(u64).max())
+
+    # ---- dominant kernel and assembly, timed with CUDA events on the library's stream
+    hbm, hbm_kind = measured_hbm()
+    spmv_which = gpu.KERNEL_SPMV_FP32 if prec == gpu.PREC_MIXED else gpu.KERNEL_SPMV_FP64
+    k_ms, k_bytes = S.time_kernel(spmv_which, 20)
+    a_ms, a_bytes = S.time_kernel(gpu.KERNEL_ASSEMBLE, 3)
+    S.assemble()
+    achieved = k_bytes / (k_ms / 1e3) / 1e9
+    a_gbs = a_bytes / (a_ms / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "spmv_bsr_fp32_hex20_64x64x32.txt" if spmv_which == gpu.KERNEL_SPMV_FP32
+                      else "spmv_bsr_fp64_hex20_64x64x32.txt")
+    if os.path.exists(tp):
+        for ln in open(tp):
+            if ln.startswith("dram_bytes_per_launch:"):
+                traffic = float(ln.split(":")[1])
+
+    # ---- end to end through the public API with host buffers (pinned)
+    e2e = None
+    if not args.no_e2e:
+        coords_h = torch.from_numpy(np.ascontiguousarray(deck.coords)).pin_memory().numpy()
+        E_h = torch.from_numpy(np.ascontiguousarray(deck.E)).pin_memory().numpy()
+        f_h = torch.from_numpy(f).pin_memory().numpy()
+        S.update_coords(coords_h)
+        S.update_material(E=E_h)
+        S.assemble()
+        S.solve(f_h, tol=TOL, precision=prec, precond=pc)
+        barrier()
+        torch.cuda.synchronize(dev)
+        ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        w0 = time.perf_counter()
+        ee0.record(stream)
+        for _ in range(args.steps):
+            S.update_coords(coords_h)
+            S.update_material(E=E_h)
+            S.assemble()
+            u_h, _ = S.solve(f_h, tol=TOL, precision=prec, precond=pc)
+        ee1.record(stream)
+        torch.cuda.synchronize(dev)
+        wall = (time.perf_counter() - w0) / args.steps
+        e_ms = max(ee0.elapsed_time(ee1) / args.steps, wall * 1e3)
+        e_ms = max_over_ranks(e_ms)
+        e2e = {"value": world * neq / (e_ms / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": int(coords_h.nbytes + E_h.nbytes + f_h.nbytes),
+               "d2h_bytes_per_step": int(u_h.nbytes), "ms_per_step": e_ms}
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            base = cpu_baseline(neq, pinfo["nnz_lower_eq"], deck.num_elems, rep64["iterations"])
+        except Exception as ex:  # reported, not fatal
+            base = {"value": None, "error": str(ex)[:200]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64+f32" if prec == gpu.PREC_MIXED else "f64", "data": "synthetic",
+            "config": workload_config(args, neq),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": traffic,
+                         "kernel": "spmv_kernel<float> (inner FP32 PCG K.p)" if spmv_which == gpu.KERNEL_SPMV_FP32
+                         else "spmv_kernel<double> (FP64 PCG K.p)",
+                         "bytes_per_launch": k_bytes, "ms_per_launch": k_ms, "peak_kind": hbm_kind},
+            "cpu_baseline": base,
+            "e2e": e2e,
+            "gpu_launches": int(n1 - n0),
+            "clocks": clk,
+            "solve": {"iterations": last["iterations"], "outer": last["outer"],
+                      "rel_residual": last["rel_residual"], "true_rel_residual": last["true_rel_residual"],
+                      "u_rel_diff_vs_fp64_jacobi": rel_u},
+            "plain_fp64_gpu": {"ms_per_step": ms64, "iterations": rep64["iterations"],
+                               "true_rel_residual": rep64["true_rel_residual"], "speedup_of_value_path": ms64 / ms},
+            "assembly": {"ms": a_ms, "elements_per_s": deck.num_elems / (a_ms / 1e3), "algorithmic_bytes": a_bytes,
+                         "GB_per_s": a_gbs, "frac": a_gbs / hbm},
+            "pattern": {**pinfo, "setup_s": setup_s},
+        }
+        print(json.dumps(line))
+    S.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--precond", default="jacobi", choices=["jacobi", "block"])
+    ap.add_argument("--size", type=int, default=64, help="elements along x and y (z = size/2)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    global NX, NY, NZ
+    NX = NY = args.size
+    NZ = args.size // 2
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

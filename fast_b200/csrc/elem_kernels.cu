@@ -1,0 +1,371 @@
+// elem_kernels.cu - element integration and colour-scheduled scatter (sm_100a).
+//
+// Computes what cElmParam::StiffMat (elc/elmparam.cpp:539-597) computes for an
+// isotropic solid element,
+//     K_e = sum_g w_g detJ_g B_g^T C B_g ,
+// and adds it into the node-block CSR matrix the way cElement::AddGlobMat
+// (elc/element.cpp:2975-3002) adds it into a cSysMatrix.
+//
+// Arithmetic.  With per-element E and nu, B^T C B factors through the
+// Gauss-point contraction
+//     H[(i,a),(j,b)] = sum_g c_g dN_a/dx_i(g) dN_b/dx_j(g),   c_g = w_g detJ_g,
+// a (3nn x 3nn) symmetric product over the ngp Gauss points, after which the
+// (a,b) 3x3 block of K_e is
+//     i == j : C00 H_ii(a,b) + G (S(a,b) - H_ii(a,b)),  S = H_xx + H_yy + H_zz
+//     i != j : C01 H_ij(a,b) + G H_ji(a,b)
+// with C00 = E(1-nu)/d, C01 = E nu/d, G = E/(2(1+nu)), d = (1+nu)(1-2nu)
+// (cSolid::QMatrix, elc/anmodel.cpp:1286-1298; Voigt order and engineering
+// shear as cSolid::BMatrix, elc/anmodel.cpp:1418-1447).  This is the same
+// sum as the reference's zero-skipping MatTripBtCB (mlib/matvec.cpp:372-388)
+// in a different association order; FP64 results agree to rounding.
+//
+// Work per element (hex20, 3x3x3): H is 1830 unique entries x 27 FMAs, about
+// 0.1 MFLOP, an order of magnitude below the dense B^T(CB) count, so the
+// FP64 kernel is bound by the K read-modify-write, not by arithmetic.
+//
+// Scatter.  A launch covers one colour of one bucket; elements of a colour
+// share no node, hence write disjoint 3x3 blocks: no atomics, and the order
+// in which contributions reach an entry is the fixed colour order, so K is
+// bit-identical from run to run.
+#include <cstdint>
+
+#include "internal.h"
+
+namespace fastgpu {
+
+struct ElemArgs {
+  int64_t ne;                 // elements in this launch
+  const int32_t *index;       // optional: colour-sorted positions to process (else 0..ne-1 + offset)
+  int64_t offset;             // first colour-sorted element of this launch
+  const int32_t *conn;        // [*][NN]
+  const double *E, *nu, *rho;
+  const int32_t *slot;        // [*][NN][NN]
+  const double *X;            // [nnode][3]
+  const uint8_t *fix;         // [nnode]
+  const double *dN;           // [NG][NN][3]
+  const double *N;            // [NG][NN]
+  const double *w;            // [NG]
+  double *K;                  // block values [nnzb][3][3] or null
+  double *Ke_out;             // [ne][3NN][3NN] or null (unmasked element matrices)
+  int32_t *status;            // bit 0: non-positive Jacobian determinant
+};
+
+template <int NN, int NG>
+struct ElemSmem {
+  static constexpr int ND = 3 * NN;
+  static constexpr int LDH = ND + 1;
+  static constexpr int kDN = NG * NN * 3;
+  static constexpr int kW = NG;
+  static constexpr int kN = NG * NN;
+  static constexpr int kX = NN * 3;
+  static constexpr int kJ = NG * 9;
+  static constexpr int kC = NG;
+  static constexpr int kD = NG * ND;
+  static constexpr int kH = ND * LDH;
+  // doubles; J is aliased into H (J is dead before H is written)
+  static constexpr int total = kDN + kW + kN + kX + kC + kD + (kH > kJ ? kH : kJ);
+  static constexpr size_t bytes = total * sizeof(double) + 2 * 256 + 64;
+};
+
+// (a, b) pair index -> a <= b, row-major over the upper triangle
+__device__ __forceinline__ void pair_of(int p, int n, int &a, int &b) {
+  int r = 0;
+  while (p >= n - r) { p -= n - r; r++; }
+  a = r;
+  b = r + p;
+}
+
+template <int NN, int NG, int NT, bool MASS>
+__global__ void __launch_bounds__(NT) elem_kernel(ElemArgs A) {
+  using S = ElemSmem<NN, NG>;
+  constexpr int ND = S::ND, LDH = S::LDH;
+  extern __shared__ __align__(16) double sm[];
+  double *sdN = sm;
+  double *sw = sdN + S::kDN;
+  double *sN = sw + S::kW;
+  double *sX = sN + S::kN;
+  double *sc = sX + S::kX;
+  double *sD = sc + S::kC;
+  double *sH = sD + S::kD;
+  double *sJ = sH;  // aliased
+  uint8_t *sfix = reinterpret_cast<uint8_t *>(sH + (S::kH > S::kJ ? S::kH : S::kJ));
+  uint8_t *spa = sfix + 64;
+  uint8_t *spb = spa + 256;
+  constexpr int NP = NN * (NN + 1) / 2;
+
+  const int tid = threadIdx.x;
+  for (int i = tid; i < S::kDN; i += NT) sdN[i] = A.dN[i];
+  for (int i = tid; i < NG; i += NT) sw[i] = A.w[i];
+  if (MASS)
+    for (int i = tid; i < S::kN; i += NT) sN[i] = A.N[i];
+  for (int p = tid; p < NP; p += NT) {
+    int a, b;
+    pair_of(p, NN, a, b);
+    spa[p] = (uint8_t)a;
+    spb[p] = (uint8_t)b;
+  }
+
+  for (int64_t it = blockIdx.x; it < A.ne; it += gridDim.x) {
+    const int64_t e = A.index ? (int64_t)A.index[it] : A.offset + it;
+    __syncthreads();
+    const int32_t *en = A.conn + e * NN;
+    for (int i = tid; i < NN * 3; i += NT) {
+      const int32_t n = en[i / 3];
+      sX[i] = A.X[3 * (int64_t)n + (i % 3)];
+    }
+    for (int i = tid; i < NN; i += NT) sfix[i] = A.fix[en[i]];
+    __syncthreads();
+
+    // Jacobians J[g][p][q] = sum_a dN_a/dxi_p X_a,q (cShapeSolid::DrvShpXYZ, shp/shpsolid.cpp:58-126)
+    for (int t = tid; t < NG * 9; t += NT) {
+      const int g = t / 9, pq = t - 9 * g, p = pq / 3, q = pq - 3 * p;
+      const double *d = sdN + g * NN * 3 + p;
+      double s = 0.0;
+#pragma unroll 4
+      for (int a = 0; a < NN; a++) s += d[3 * a] * sX[3 * a + q];
+      sJ[t] = s;
+    }
+    __syncthreads();
+    // determinant and inverse by cofactors (cShape::ShpMatInv, shp/shape.cpp:360-393)
+    for (int g = tid; g < NG; g += NT) {
+      double *J = sJ + 9 * g;
+      const double j00 = J[0], j01 = J[1], j02 = J[2], j10 = J[3], j11 = J[4], j12 = J[5], j20 = J[6],
+                   j21 = J[7], j22 = J[8];
+      const double det = j00 * (j11 * j22 - j12 * j21) - j01 * (j10 * j22 - j12 * j20) + j02 * (j10 * j21 - j11 * j20);
+      if (!(det > 0.0)) atomicOr(A.status, 1);
+      const double id = (det != 0.0) ? det : 1.0;
+      J[0] = (j11 * j22 - j12 * j21) / id;
+      J[1] = -(j01 * j22 - j02 * j21) / id;
+      J[2] = (j01 * j12 - j02 * j11) / id;
+      J[3] = -(j10 * j22 - j12 * j20) / id;
+      J[4] = (j00 * j22 - j02 * j20) / id;
+      J[5] = -(j00 * j12 - j02 * j10) / id;
+      J[6] = (j10 * j21 - j11 * j20) / id;
+      J[7] = -(j00 * j21 - j01 * j20) / id;
+      J[8] = (j00 * j11 - j01 * j10) / id;
+      sc[g] = sw[g] * det;
+    }
+    __syncthreads();
+
+    if (MASS) {
+      // M_ab = rho * sum_g c_g N_a N_b * I3  (cElmParam::MassMat, elc/elmparam.cpp:672-739)
+      const double rho = A.rho ? A.rho[e] : 0.0;
+      for (int p = tid; p < NP; p += NT) {
+        const int a = spa[p], b = spb[p];
+        double s = 0.0;
+        for (int g = 0; g < NG; g++) s += sc[g] * sN[g * NN + a] * sN[g * NN + b];
+        s *= rho;
+        for (int i = 0; i < 3; i++) {
+          if (A.Ke_out) {
+            double *Ko = A.Ke_out + it * ND * ND;
+            Ko[(3 * a + i) * ND + 3 * b + i] = s;
+            Ko[(3 * b + i) * ND + 3 * a + i] = s;
+          }
+          if (A.K && !((sfix[a] >> i) & 1) && !((sfix[b] >> i) & 1)) {
+            const int32_t sab = A.slot[(e * NN + a) * NN + b];
+            A.K[(int64_t)sab * 9 + 4 * i] += s;
+            if (a != b) {
+              const int32_t sba = A.slot[(e * NN + b) * NN + a];
+              A.K[(int64_t)sba * 9 + 4 * i] += s;
+            }
+          }
+        }
+      }
+      continue;
+    }
+
+    // D[g][i*NN + a] = dN_a/dx_i at Gauss point g
+    for (int t = tid; t < NG * NN; t += NT) {
+      const int g = t / NN, a = t - NN * g;
+      const double *J = sJ + 9 * g;
+      const double d0 = sdN[(g * NN + a) * 3], d1 = sdN[(g * NN + a) * 3 + 1], d2 = sdN[(g * NN + a) * 3 + 2];
+      double *D = sD + g * ND;
+      D[a] = J[0] * d0 + J[1] * d1 + J[2] * d2;
+      D[NN + a] = J[3] * d0 + J[4] * d1 + J[5] * d2;
+      D[2 * NN + a] = J[6] * d0 + J[7] * d1 + J[8] * d2;
+    }
+    __syncthreads();
+
+    // H = sum_g c_g D_g D_g^T, 4x4 register tiles over the upper triangle
+    constexpr int T = ND / 4;
+    constexpr int NTILE = T * (T + 1) / 2;
+    for (int tile = tid; tile < NTILE; tile += NT) {
+      int ti, tj;
+      pair_of(tile, T, ti, tj);
+      double acc[4][4];
+#pragma unroll
+      for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) acc[r][q] = 0.0;
+      for (int g = 0; g < NG; g++) {
+        const double cg = sc[g];
+        const double *D = sD + g * ND;
+        double ra[4], cb[4];
+#pragma unroll
+        for (int r = 0; r < 4; r++) ra[r] = cg * D[4 * ti + r];
+#pragma unroll
+        for (int q = 0; q < 4; q++) cb[q] = D[4 * tj + q];
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+          for (int q = 0; q < 4; q++) acc[r][q] = fma(ra[r], cb[q], acc[r][q]);
+      }
+#pragma unroll
+      for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          sH[(4 * ti + r) * LDH + 4 * tj + q] = acc[r][q];
+          sH[(4 * tj + q) * LDH + 4 * ti + r] = acc[r][q];
+        }
+    }
+    __syncthreads();
+
+    // element matrix blocks and scatter
+    const double E = A.E[e], nu = A.nu[e];
+    const double dd = (1.0 + nu) * (1.0 - 2.0 * nu);
+    const double C00 = E * (1.0 - nu) / dd, C01 = E * nu / dd, G = 0.5 * E / (1.0 + nu);
+    double *__restrict__ Kg = A.K;
+    for (int t = tid; t < NP * 9; t += NT) {
+      const int p = t / 9, ij = t - 9 * p, i = ij / 3, j = ij - 3 * i;
+      const int a = spa[p], b = spb[p];
+      double v;
+      if (i == j) {
+        const double hs = sH[a * LDH + b] + sH[(NN + a) * LDH + NN + b] + sH[(2 * NN + a) * LDH + 2 * NN + b];
+        const double hii = sH[(i * NN + a) * LDH + i * NN + b];
+        v = C00 * hii + G * (hs - hii);
+      } else {
+        v = C01 * sH[(i * NN + a) * LDH + j * NN + b] + G * sH[(j * NN + a) * LDH + i * NN + b];
+      }
+      if (A.Ke_out) {
+        double *Ko = A.Ke_out + it * ND * ND;
+        Ko[(3 * a + i) * ND + 3 * b + j] = v;
+        Ko[(3 * b + j) * ND + 3 * a + i] = v;
+      }
+      if (Kg && !((sfix[a] >> i) & 1) && !((sfix[b] >> j) & 1)) {
+        const int32_t sab = A.slot[(e * NN + a) * NN + b];
+        Kg[(int64_t)sab * 9 + 3 * i + j] += v;
+        if (a != b) {
+          const int32_t sba = A.slot[(e * NN + b) * NN + a];
+          Kg[(int64_t)sba * 9 + 3 * j + i] += v;
+        }
+      }
+    }
+  }
+}
+
+template <int NN, int NG, int NT, bool MASS>
+static cudaError_t run(Ctx &c, ElemArgs a, int64_t count) {
+  if (count <= 0) return cudaSuccess;
+  using S = ElemSmem<NN, NG>;
+  auto kern = elem_kernel<NN, NG, NT, MASS>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, S::bytes);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  int64_t grid = (int64_t)per_sm * c.sm_count;
+  if (grid > count) grid = count;
+  a.ne = count;
+  kern<<<(unsigned)grid, NT, S::bytes, c.stream>>>(a);
+  c.launches++;
+  return cudaGetLastError();
+}
+
+template <bool MASS>
+static cudaError_t dispatch(Ctx &c, const Bucket &B, ElemArgs a, int64_t count) {
+  const int ng = B.ng;
+  if (B.type == FAST_ELEM_HEX8) {
+    switch (ng) {
+      case 1: return run<8, 1, 64, MASS>(c, a, count);
+      case 8: return run<8, 8, 64, MASS>(c, a, count);
+      case 27: return run<8, 27, 64, MASS>(c, a, count);
+      default: break;
+    }
+  } else if (B.type == FAST_ELEM_HEX20) {
+    switch (ng) {
+      case 8: return run<20, 8, 128, MASS>(c, a, count);
+      case 27: return run<20, 27, 128, MASS>(c, a, count);
+      case 64: return run<20, 64, 128, MASS>(c, a, count);
+      default: break;
+    }
+  }
+  return cudaErrorInvalidValue;
+}
+
+static ElemArgs base_args(Ctx &c, const Bucket &B, double *K) {
+  ElemArgs a{};
+  a.conn = B.d_conn;
+  a.E = B.d_E;
+  a.nu = B.d_nu;
+  a.rho = B.d_rho;
+  a.slot = B.d_slot;
+  a.X = c.d_X;
+  a.fix = c.d_fix;
+  a.dN = B.d_dN;
+  a.N = B.d_N;
+  a.w = B.d_w;
+  a.K = K;
+  a.status = c.d_status;
+  return a;
+}
+
+__global__ void zero_fixed_identity(int64_t nnode, const uint8_t *fix, const int32_t *diag, double *K) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= nnode) return;
+  const uint8_t f = fix[n];
+  if (!f) return;
+  const int32_t d = diag[n];
+  if (d < 0) return;
+  for (int i = 0; i < 3; i++)
+    if ((f >> i) & 1) K[(int64_t)d * 9 + 4 * i] = 1.0;
+}
+
+cudaError_t launch_zero_matrix(Ctx &c, double *K, bool identity_on_fixed) {
+  cudaError_t e = cudaMemsetAsync(K, 0, sizeof(double) * 9 * (size_t)c.nnzb, c.stream);
+  if (e != cudaSuccess || !identity_on_fixed) return e;
+  const int bs = 256;
+  zero_fixed_identity<<<(unsigned)((c.nnode + bs - 1) / bs), bs, 0, c.stream>>>(c.nnode, c.d_fix, c.d_diag, K);
+  c.launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_assemble(Ctx &c, int what, double *target) {
+  for (size_t b = 0; b < c.buckets.size(); b++) {
+    const Bucket &B = c.buckets[b];
+    if (what == FAST_ASM_MASS && !B.has_rho) continue;
+    for (size_t k = 0; k + 1 < B.color_off.size(); k++) {
+      ElemArgs a = base_args(c, B, target);
+      a.offset = B.color_off[k];
+      const int64_t cnt = B.color_off[k + 1] - B.color_off[k];
+      cudaError_t e = (what == FAST_ASM_MASS) ? dispatch<true>(c, B, a, cnt) : dispatch<false>(c, B, a, cnt);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_element_matrices(Ctx &c, int what, int bucket, int64_t first_sorted_unused, int64_t count,
+                                    double *d_out_and_index) {
+  (void)first_sorted_unused;
+  // d_out_and_index: caller packs [count] int32 positions at the end of the buffer
+  const Bucket &B = c.buckets[bucket];
+  const int nd = 3 * B.nn;
+  ElemArgs a = base_args(c, B, nullptr);
+  a.Ke_out = d_out_and_index;
+  a.index = reinterpret_cast<const int32_t *>(d_out_and_index + (size_t)count * nd * nd);
+  return (what == FAST_ASM_MASS) ? dispatch<true>(c, B, a, count) : dispatch<false>(c, B, a, count);
+}
+
+__global__ void to_fp32_kernel(const double *__restrict__ s, float *__restrict__ d, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    d[i] = (float)s[i];
+}
+
+cudaError_t launch_to_fp32(Ctx &c, const double *src, float *dst, int64_t n) {
+  to_fp32_kernel<<<c.sm_count * 8, 256, 0, c.stream>>>(src, dst, n);
+  c.launches++;
+  return cudaGetLastError();
+}
+
+}  // namespace fastgpu

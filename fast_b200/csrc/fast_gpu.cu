@@ -1,0 +1,644 @@
+// fast_gpu.cu - the C ABI of libfastgpu.so (declared in include/fast_gpu.h).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+using namespace fastgpu;
+
+struct fast_gpu_ctx : public Ctx {};
+
+namespace {
+
+#define CK(call)                                                                      \
+  do {                                                                                \
+    cudaError_t _e = (call);                                                          \
+    if (_e != cudaSuccess) {                                                          \
+      c->err = std::string(#call) + ": " + cudaGetErrorString(_e);                    \
+      return FAST_GPU_ECUDA;                                                          \
+    }                                                                                 \
+  } while (0)
+
+template <typename T>
+cudaError_t dalloc(T **p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  return cudaMalloc((void **)p, sizeof(T) * count);
+}
+
+template <typename T>
+void dfree(T *&p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+void free_mesh(Ctx &c) {
+  for (Bucket &B : c.buckets) {
+    dfree(B.d_conn); dfree(B.d_E); dfree(B.d_nu); dfree(B.d_rho); dfree(B.d_slot);
+    dfree(B.d_dN); dfree(B.d_N); dfree(B.d_w);
+  }
+  c.buckets.clear();
+  dfree(c.d_X); dfree(c.d_fix); dfree(c.d_dof_of_eq);
+  dfree(c.d_rowptr); dfree(c.d_col); dfree(c.d_diag);
+  dfree(c.d_K); dfree(c.d_M); dfree(c.d_K32);
+  dfree(c.d_u); dfree(c.d_r); dfree(c.d_z); dfree(c.d_p); dfree(c.d_w); dfree(c.d_f); dfree(c.d_dinv);
+  dfree(c.s_u); dfree(c.s_r); dfree(c.s_z); dfree(c.s_p); dfree(c.s_w); dfree(c.s_dinv);
+  dfree(c.d_eq_tmp);
+  if (c.h_eq_tmp) cudaFreeHost(c.h_eq_tmp);
+  c.h_eq_tmp = nullptr;
+  c.K_ok = c.M_ok = c.K32_ok = false;
+  c.precond_built = -1;
+  c.nnode = 0;
+  c.neq = 0;
+  c.nnzb = 0;
+}
+
+int check_ctx(const fast_gpu_ctx *c) { return c ? FAST_GPU_OK : FAST_GPU_EINVAL; }
+
+double *target_of(Ctx &c, int what) {
+  if (what == FAST_ASM_STIFFNESS) return c.d_K;
+  if (what == FAST_ASM_MASS) return c.d_M;
+  return nullptr;
+}
+
+// (eq i, eq j) 0-based -> flat value index in the block matrix, or -1
+int64_t value_index(const Ctx &c, int32_t i, int32_t j) {
+  if (i < 0 || j < 0 || i >= c.neq || j >= c.neq) return -1;
+  const int32_t di = c.h_dof_of_eq[i], dj = c.h_dof_of_eq[j];
+  const int32_t ni = di / 3, pi = di % 3, nj = dj / 3, pj = dj % 3;
+  const int32_t *b0 = c.h_col.data() + c.h_rowptr[ni], *b1 = c.h_col.data() + c.h_rowptr[ni + 1];
+  const int32_t *p = std::lower_bound(b0, b1, nj);
+  if (p == b1 || *p != nj) return -1;
+  return (int64_t)(p - c.h_col.data()) * 9 + pi * 3 + pj;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fast_gpu_version(void) { return FAST_GPU_ABI_VERSION; }
+
+int fast_gpu_create(int device, fast_gpu_ctx **out) {
+  if (!out) return FAST_GPU_EINVAL;
+  *out = nullptr;
+  fast_gpu_ctx *c = new (std::nothrow) fast_gpu_ctx();
+  if (!c) return FAST_GPU_ENOMEM;
+  c->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_status, sizeof(int32_t) * 4);
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_status, sizeof(int32_t) * 4);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_state, sizeof(PcgState) * 2);
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_state, sizeof(PcgState) * 2);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_partials, sizeof(double) * 16384);
+  if (e != cudaSuccess) {
+    delete c;
+    return FAST_GPU_ECUDA;
+  }
+  c->stream = c->own_stream;
+  *out = c;
+  return FAST_GPU_OK;
+}
+
+int fast_gpu_destroy(fast_gpu_ctx *c) {
+  if (!c) return FAST_GPU_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_mesh(*c);
+  dfree(c->d_status);
+  if (c->h_status) cudaFreeHost(c->h_status);
+  dfree(c->d_state);
+  if (c->h_state) cudaFreeHost(c->h_state);
+  dfree(c->d_partials);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+  return FAST_GPU_OK;
+}
+
+const char *fast_gpu_last_error(const fast_gpu_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+int fast_gpu_set_stream(fast_gpu_ctx *c, void *s) {
+  if (check_ctx(c)) return FAST_GPU_EINVAL;
+  c->stream = s ? (cudaStream_t)s : c->own_stream;
+  return FAST_GPU_OK;
+}
+
+int fast_gpu_synchronize(fast_gpu_ctx *c) {
+  if (check_ctx(c)) return FAST_GPU_EINVAL;
+  CK(cudaStreamSynchronize(c->stream));
+  return FAST_GPU_OK;
+}
+
+int fast_gpu_upload_mesh(fast_gpu_ctx *c, const fast_gpu_mesh *m) {
+  if (check_ctx(c) || !m || m->num_nodes <= 0 || !m->coords || !m->node_eq || m->num_buckets <= 0 || !m->buckets) {
+    if (c) c->err = "upload_mesh: invalid mesh description";
+    return FAST_GPU_EINVAL;
+  }
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->stream));
+  free_mesh(*c);
+  const int64_t nnode = m->num_nodes;
+  c->nnode = nnode;
+  c->neq = m->num_eq;
+  c->h_eq.assign(m->node_eq, m->node_eq + 3 * nnode);
+  c->h_dof_of_eq.assign(std::max(0, m->num_eq), -1);
+  std::vector<uint8_t> fix(nnode, 0);
+  for (int64_t n = 0; n < nnode; n++)
+    for (int i = 0; i < 3; i++) {
+      const int32_t q = c->h_eq[3 * n + i];
+      if (q <= 0) {
+        fix[n] |= (uint8_t)(1 << i);
+      } else {
+        if (q > m->num_eq || c->h_dof_of_eq[q - 1] != -1) {
+          c->err = "upload_mesh: node_eq is not a numbering of 1..num_eq";
+          return FAST_GPU_EINVAL;
+        }
+        c->h_dof_of_eq[q - 1] = (int32_t)(3 * n + i);
+      }
+    }
+  for (int32_t k = 0; k < m->num_eq; k++)
+    if (c->h_dof_of_eq[k] < 0) {
+      c->err = "upload_mesh: equation without a DOF";
+      return FAST_GPU_EINVAL;
+    }
+  c->buckets.resize(m->num_buckets);
+  for (int b = 0; b < m->num_buckets; b++) {
+    const fast_gpu_bucket &bk = m->buckets[b];
+    Bucket &B = c->buckets[b];
+    B.type = bk.elem_type;
+    B.nn = nodes_of(bk.elem_type);
+    if (!B.nn) { c->err = "upload_mesh: unsupported element type"; return FAST_GPU_ENOTSUP; }
+    for (int k = 0; k < 3; k++) B.ngp[k] = bk.ngp[k];
+    B.ng = B.ngp[0] * B.ngp[1] * B.ngp[2];
+    const bool ok_rule = (B.ngp[0] == B.ngp[1] && B.ngp[1] == B.ngp[2]) &&
+                         ((B.type == FAST_ELEM_HEX8 && (B.ngp[0] == 1 || B.ngp[0] == 2 || B.ngp[0] == 3)) ||
+                          (B.type == FAST_ELEM_HEX20 && (B.ngp[0] >= 2 && B.ngp[0] <= 4)));
+    if (!ok_rule) { c->err = "upload_mesh: unsupported Gauss rule for this element type"; return FAST_GPU_ENOTSUP; }
+    B.ne = bk.num_elems;
+    if (B.ne <= 0 || !bk.conn || !bk.E || !bk.nu) { c->err = "upload_mesh: empty bucket"; return FAST_GPU_EINVAL; }
+    B.has_rho = bk.rho != nullptr;
+  }
+  if (!build_pattern(*c, *m)) return FAST_GPU_EINVAL;
+
+  CK(dalloc(&c->d_X, 3 * nnode));
+  CK(cudaMemcpy(c->d_X, m->coords, sizeof(double) * 3 * nnode, cudaMemcpyHostToDevice));
+  CK(dalloc(&c->d_fix, nnode));
+  CK(cudaMemcpy(c->d_fix, fix.data(), nnode, cudaMemcpyHostToDevice));
+  CK(dalloc(&c->d_dof_of_eq, c->neq));
+  if (c->neq) CK(cudaMemcpy(c->d_dof_of_eq, c->h_dof_of_eq.data(), sizeof(int32_t) * c->neq, cudaMemcpyHostToDevice));
+  CK(dalloc(&c->d_rowptr, nnode + 1));
+  CK(cudaMemcpy(c->d_rowptr, c->h_rowptr.data(), sizeof(int32_t) * (nnode + 1), cudaMemcpyHostToDevice));
+  CK(dalloc(&c->d_col, c->nnzb));
+  CK(cudaMemcpy(c->d_col, c->h_col.data(), sizeof(int32_t) * c->nnzb, cudaMemcpyHostToDevice));
+  CK(dalloc(&c->d_diag, nnode));
+  CK(cudaMemcpy(c->d_diag, c->h_diag.data(), sizeof(int32_t) * nnode, cudaMemcpyHostToDevice));
+  for (int b = 0; b < m->num_buckets; b++) {
+    const fast_gpu_bucket &bk = m->buckets[b];
+    Bucket &B = c->buckets[b];
+    const int64_t ne = B.ne;
+    std::vector<double> E(ne), nu(ne), rho;
+    for (int64_t s = 0; s < ne; s++) { E[s] = bk.E[B.perm[s]]; nu[s] = bk.nu[B.perm[s]]; }
+    CK(dalloc(&B.d_conn, ne * B.nn));
+    CK(cudaMemcpy(B.d_conn, B.h_conn.data(), sizeof(int32_t) * ne * B.nn, cudaMemcpyHostToDevice));
+    CK(dalloc(&B.d_slot, ne * B.nn * B.nn));
+    CK(cudaMemcpy(B.d_slot, B.h_slot.data(), sizeof(int32_t) * ne * B.nn * B.nn, cudaMemcpyHostToDevice));
+    std::vector<int32_t>().swap(B.h_slot);
+    CK(dalloc(&B.d_E, ne));
+    CK(cudaMemcpy(B.d_E, E.data(), sizeof(double) * ne, cudaMemcpyHostToDevice));
+    CK(dalloc(&B.d_nu, ne));
+    CK(cudaMemcpy(B.d_nu, nu.data(), sizeof(double) * ne, cudaMemcpyHostToDevice));
+    if (B.has_rho) {
+      rho.resize(ne);
+      for (int64_t s = 0; s < ne; s++) rho[s] = bk.rho[B.perm[s]];
+      CK(dalloc(&B.d_rho, ne));
+      CK(cudaMemcpy(B.d_rho, rho.data(), sizeof(double) * ne, cudaMemcpyHostToDevice));
+    }
+    std::vector<double> N, dN, w;
+    gauss_point_tables(B.type, B.ngp, N, dN, w);
+    CK(dalloc(&B.d_N, N.size()));
+    CK(cudaMemcpy(B.d_N, N.data(), sizeof(double) * N.size(), cudaMemcpyHostToDevice));
+    CK(dalloc(&B.d_dN, dN.size()));
+    CK(cudaMemcpy(B.d_dN, dN.data(), sizeof(double) * dN.size(), cudaMemcpyHostToDevice));
+    CK(dalloc(&B.d_w, w.size()));
+    CK(cudaMemcpy(B.d_w, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice));
+  }
+  const int64_t n3 = 3 * nnode;
+  CK(dalloc(&c->d_K, 9 * c->nnzb));
+  CK(dalloc(&c->d_u, n3)); CK(dalloc(&c->d_r, n3)); CK(dalloc(&c->d_z, n3)); CK(dalloc(&c->d_p, n3));
+  CK(dalloc(&c->d_w, n3)); CK(dalloc(&c->d_f, n3)); CK(dalloc(&c->d_dinv, 9 * nnode));
+  CK(dalloc(&c->s_u, n3)); CK(dalloc(&c->s_r, n3)); CK(dalloc(&c->s_z, n3)); CK(dalloc(&c->s_p, n3));
+  CK(dalloc(&c->s_w, n3)); CK(dalloc(&c->s_dinv, 9 * nnode));
+  CK(dalloc(&c->d_eq_tmp, std::max<int64_t>(2 * (int64_t)c->neq, 1)));
+  CK(cudaMallocHost((void **)&c->h_eq_tmp, sizeof(double) * std::max<int64_t>(2 * (int64_t)c->neq, 1)));
+  return FAST_GPU_OK;
+}
+
+int fast_gpu_pattern_info(fast_gpu_ctx *c, int64_t *nnzb, int64_t *nnz_lower, int32_t *ncol, double *secs) {
+  if (check_ctx(c)) return FAST_GPU_EINVAL;
+  if (nnzb) *nnzb = c->nnzb;
+  if (nnz_lower) *nnz_lower = c->nnz_lower_eq;
+  if (ncol) *ncol = c->ncolors;
+  if (secs) *secs = c->pattern_seconds;
+  return FAST_GPU_OK;
+}
+
+int fast_gpu_update_coords(fast_gpu_ctx *c, const double *coords) {
+  if (check_ctx(c) || !coords || !c->d_X) return FAST_GPU_EINVAL;
+  CK(cudaMemcpyAsync(c->d_X, coords, sizeof(double) * 3 * c->nnode, cudaMemcpyHostToDevice, c->stream));
+  c->K_ok = c->M_ok = c->K32_ok = false;
+  return FAST_GPU_OK;
+}
+
+int fast_gpu_update_material(fast_gpu_ctx *c, int32_t b, const double *E, const double *nu) {
+  if (check_ctx(c) || b < 0 || b >= (int)c->buckets.size()) return FAST_GPU_EINVAL;
+  Bucket &B = c->buckets[b];
+  if (!c->h_eq_tmp || B.ne > 2 * (int64_t)std::max(c->neq, 1)) {
+    // permute through a temporary host buffer
+    std::vector<double> t(B.ne);
+    if (E) {
+      for (int64_t s = 0; s < B.ne; s++) t[s] = E[B.perm[s]];
+      CK(cudaMemcpyAsync(B.d_E, t.data(), sizeof(double) * B.ne, cudaMemcpyHostToDevice, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+    }
+    if (nu) {
+      for (int64_t s = 0; s < B.ne; s++) t[s] = nu[B.perm[s]];
+      CK(cudaMemcpyAsync(B.d_nu, t.data(), sizeof(double) * B.ne, cudaMemcpyHostToDevice, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+    }
+  } else {
+    double *h = c->h_eq_tmp;
+    if (E) {
+      CK(cudaStreamSynchronize(c->stream));
+      for (int64_t s = 0; s < B.ne; s++) h[s] = E[B.perm[s]];
+      CK(cudaMemcpyAsync(B.d_E, h, sizeof(double) * B.ne, cudaMemcpyHostToDevice, c->stream));
+    }
+    if (nu) {
+      CK(cudaStreamSynchronize(c->stream));
+      for (int64_t s = 0; s < B.ne; s++) h[s] = nu[B.perm[s]];
+      CK(cudaMemcpyAsync(B.d_nu, h, sizeof(double) * B.ne, cudaMemcpyHostToDevice, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  c->K_ok = c->M_ok = c->K32_ok = false;
+  return FAST_GPU_OK;
+}
+
+int fast_gpu_zero(fast_gpu_ctx *c, int32_t what) {
+  if (check_ctx(c) || !c->d_K) return FAST_GPU_ESTATE;
+  if (what == FAST_ASM_MASS && !c->d_M) CK(dalloc(&c->d_M, 9 * c->nnzb));
+  double *T = target_of(*c, what);
+  if (!T) return FAST_GPU_EINVAL;
+  CK(launch_zero_matrix(*c, T, what == FAST_ASM_STIFFNESS));
+  if (what == FAST_ASM_STIFFNESS) { c->K_ok = true; c->K32_ok = false; c->precond_built = -1; }
+  else c->M_ok = true;
+  return FAST_GPU_OK;
+}
+
+int fast_gpu_assemble(fast_gpu_ctx *c, int32_t what) {
+  if (check_ctx(c) || !c->d_K) { if (c) c->err = "assemble: no mesh"; return FAST_GPU_ESTATE; }
+  if (what != FAST_ASM_STIFFNESS && what != FAST_ASM_MASS) return FAST_GPU_EINVAL;
+  if (what == FAST_ASM_MASS && !c->d_M) CK(dalloc(&c->d_M, 9 * c->nnzb));
+  double *T = target_of(*c, what);
+  CK(cudaMemsetAsync(c->d_status, 0, sizeof(int32_t), c->stream));
+  CK(launch_zero_matrix(*c, T, what == FAST_ASM_STIFFNESS));
+  CK(launch_assemble(*c, what, T));
+  CK(cudaMemcpyAsync(c->h_status, c->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (what == FAST_ASM_STIFFNESS) { c->K_ok = true; c->K32_ok = false; c->precond_built = -1; }
+  else c->M_ok = true;
+  if (c->h_status[0] & 1) {
+    c->err = "assemble: non-positive Jacobian determinant in at least one element";
+    return FAST_GPU_EDETJ;
+  }
+  return FAST_GPU_OK;
+}
+
+int fast_gpu_add(fast_gpu_ctx *c, int32_t what, int32_t i, int32_t j, double v) {
+  if (check_ctx(c)) return FAST_GPU_EINVAL;
+  double *T = target_of(*c, what);
+  if (!T) return FAST_GPU_ESTATE;
+  const int64_t k1 = value_index(*c, i, j);
+  if (k1 < 0) { c->err = "add: (i, j) outside the pattern"; return FAST_GPU_ENOTFOUND; }
+  const int64_t k2 = value_index(*c, j, i);
+  double a = 0, b = 0;
+  CK(cudaMemcpyAsync(&a, T + k1, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  a += v;
+  CK(cudaMemcpyAsync(T + k1, &a, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if (k2 != k1) {
+    CK(cudaMemcpyAsync(&b, T + k2, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    b += v;
+    CK(cudaMemcpyAsync(T + k2, &b, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  if (what == FAST_ASM_STIFFNESS) { c->K32_ok = false; c->precond_built = -1; }
+  return FAST_GPU_OK;
+}
+
+int fast_gpu_get(fast_gpu_ctx *c, int32_t what, int32_t i, int32_t j, double *v) {
+  if (check_ctx(c) || !v) return FAST_GPU_EINVAL;
+  double *T = target_of(*c, what);
+  if (!T) return FAST_GPU_ESTATE;
+  const int64_t k = value_index(*c, i, j);
+  if (k < 0) { *v = 0.0; return FAST_GPU_OK; }
+  CK(cudaMemcpyAsync(v, T + k, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return FAST_GPU_OK;
+}
+
+int fast_gpu_mult_vect(fast_gpu_ctx *c, int32_t what, const double *x, double *y) {
+  if (check_ctx(c) || !x || !y) return FAST_GPU_EINVAL;
+  double *T = target_of(*c, what);
+  if (!T || (what == FAST_ASM_STIFFNESS && !c->K_ok) || (what == FAST_ASM_MASS && !c->M_ok)) return FAST_GPU_ESTATE;
+  const size_t nb = sizeof(double) * c->neq;
+  CK(cudaStreamSynchronize(c->stream));
+  std::memcpy(c->h_eq_tmp, x, nb);
+  CK(cudaMemcpyAsync(c->d_eq_tmp, c->h_eq_tmp, nb, cudaMemcpyHostToDevice, c->stream));
+  CK(launch_eq_to_node(*c, c->d_eq_tmp, c->d_p));
+  CK(launch_spmv(*c, T, c->d_p, c->d_w));
+  CK(launch_node_to_eq(*c, c->d_w, c->d_eq_tmp));
+  CK(cudaMemcpyAsync(c->h_eq_tmp, c->d_eq_tmp, nb, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  std::memcpy(y, c->h_eq_tmp, nb);
+  return FAST_GPU_OK;
+}
+
+namespace {
+
+int solve_node_space(fast_gpu_ctx *c, const fast_gpu_solve_opts *o, bool warm, fast_gpu_solve_report *rep) {
+  // d_f holds the node-space load, d_u the initial / returned solution
+  fast_gpu_solve_opts opts{};
+  if (o) opts = *o;
+  const int maxit = opts.maxit > 0 ? opts.maxit : std::max(20 * c->neq, 100);
+  const double tol = opts.tol > 0 ? opts.tol : 1e-5;
+  const int precond = opts.precond;
+  if (precond != FAST_PRECOND_JACOBI && precond != FAST_PRECOND_BLOCK_JACOBI) return FAST_GPU_EINVAL;
+  if (c->precond_built != precond) CK(launch_build_precond(*c, c->d_K, precond));
+  fast_gpu_solve_report R{};
+  const int64_t n3 = 3 * c->nnode;
+  if (opts.precision == FAST_PREC_FP64) {
+    int it = 0, done = 0;
+    double err = 0;
+    CK(pcg_solve_device(*c, false, c->d_f, c->d_u, warm, tol, maxit, opts.check_every, precond, &it, &err, &done));
+    R.iterations = it;
+    R.outer = 1;
+    R.rel_residual = err;
+    R.converged = (done == 1);
+  } else if (opts.precision == FAST_PREC_MIXED) {
+    if (!c->d_K32) CK(dalloc(&c->d_K32, 9 * c->nnzb));
+    if (!c->K32_ok) {
+      CK(launch_to_fp32(*c, c->d_K, c->d_K32, 9 * c->nnzb));
+      c->K32_ok = true;
+    }
+    const double inner = opts.inner_tol > 0 ? opts.inner_tol : 1e-5;
+    const int max_outer = opts.max_outer > 0 ? opts.max_outer : 30;
+    double *d_rr = c->d_partials + 12288;
+    double *d_ff = c->d_partials + 12289;
+    CK(launch_norm2(*c, c->d_f, n3, d_ff));
+    double hff = 0;
+    CK(cudaMemcpyAsync(&hff, d_ff, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    double lenf = std::sqrt(hff);
+    if (lenf > 10e+10) lenf = 1.0;
+    if (!warm) CK(cudaMemsetAsync(c->d_u, 0, sizeof(double) * n3, c->stream));
+    int total = 0;
+    for (int k = 0; k < max_outer; k++) {
+      // FP64 residual r = f - K u
+      CK(launch_residual(*c, c->d_K, c->d_f, c->d_u, c->d_r, d_rr));
+      double hrr = 0;
+      CK(cudaMemcpyAsync(&hrr, d_rr, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      const double rn = std::sqrt(hrr);
+      R.rel_residual = (lenf > 0) ? rn / lenf : 0.0;
+      if (lenf < tol || R.rel_residual < tol) { R.converged = 1; break; }
+      if (!std::isfinite(rn) || total >= maxit) break;
+      R.outer = k + 1;
+      // FP32 inner solve K32 d = r / |r| (scaled so the FP32 right-hand side has unit norm)
+      double *d_rs = c->d_w;
+      double *d_d = c->d_z;
+      CK(cudaMemcpyAsync(d_rs, c->d_r, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->stream));
+      CK(scale_inplace(*c, d_rs, n3, 1.0 / rn));
+      int it = 0, done = 0;
+      double err = 0;
+      CK(pcg_solve_device(*c, true, d_rs, d_d, false, inner, std::max(1, maxit - total), opts.check_every,
+                          precond, &it, &err, &done));
+      total += it;
+      if (done == 3 || it == 0) break;
+      // FP64 refinement update u += |r| d
+      CK(axpy_inplace(*c, c->d_u, d_d, n3, rn));
+    }
+    R.iterations = total;
+  } else {
+    return FAST_GPU_EINVAL;
+  }
+  // true FP64 residual
+  {
+    double *d_rr = c->d_partials + 12290;
+    double *d_ff = c->d_partials + 12291;
+    CK(launch_residual(*c, c->d_K, c->d_f, c->d_u, c->d_r, d_rr));
+    CK(launch_norm2(*c, c->d_f, n3, d_ff));
+    double h[2] = {0, 0};
+    CK(cudaMemcpyAsync(h, d_rr, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    R.true_rel_residual = h[1] > 0 ? std::sqrt(h[0] / h[1]) : 0.0;
+  }
+  if (rep) *rep = R;
+  if (!R.converged) {
+    c->err = "solve: no convergence within the iteration cap";
+    return FAST_GPU_ENONCONV;
+  }
+  return FAST_GPU_OK;
+}
+
+}  // namespace
+
+int fast_gpu_solve_device(fast_gpu_ctx *c, const double *d_f, double *d_u, const fast_gpu_solve_opts *o,
+                          fast_gpu_solve_report *rep) {
+  if (check_ctx(c) || !d_f || !d_u) return FAST_GPU_EINVAL;
+  if (!c->K_ok) { c->err = "solve: matrix not assembled"; return FAST_GPU_ESTATE; }
+  const bool warm = o && o->warm_start;
+  CK(launch_eq_to_node(*c, d_f, c->d_f));
+  if (warm) CK(launch_eq_to_node(*c, d_u, c->d_u));
+  const int rc = solve_node_space(c, o, warm, rep);
+  if (rc == FAST_GPU_OK || rc == FAST_GPU_ENONCONV) CK(launch_node_to_eq(*c, c->d_u, d_u));
+  return rc;
+}
+
+int fast_gpu_solve(fast_gpu_ctx *c, const double *f, double *u, const fast_gpu_solve_opts *o,
+                   fast_gpu_solve_report *rep) {
+  if (check_ctx(c) || !f || !u) return FAST_GPU_EINVAL;
+  if (!c->K_ok) { c->err = "solve: matrix not assembled"; return FAST_GPU_ESTATE; }
+  const size_t nb = sizeof(double) * c->neq;
+  double *d_feq = c->d_eq_tmp, *d_ueq = c->d_eq_tmp + c->neq;
+  CK(cudaStreamSynchronize(c->stream));
+  std::memcpy(c->h_eq_tmp, f, nb);
+  if (o && o->warm_start) std::memcpy(c->h_eq_tmp + c->neq, u, nb);
+  CK(cudaMemcpyAsync(d_feq, c->h_eq_tmp, (o && o->warm_start) ? 2 * nb : nb, cudaMemcpyHostToDevice, c->stream));
+  const int rc = fast_gpu_solve_device(c, d_feq, d_ueq, o, rep);
+  if (rc == FAST_GPU_OK || rc == FAST_GPU_ENONCONV) {
+    CK(cudaMemcpyAsync(c->h_eq_tmp, d_ueq, nb, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::memcpy(u, c->h_eq_tmp, nb);
+  }
+  return rc;
+}
+
+int fast_gpu_get_lower_csr(fast_gpu_ctx *c, int32_t what, int64_t *nnz, int64_t *rowptr, int32_t *col, double *val) {
+  if (check_ctx(c) || !nnz) return FAST_GPU_EINVAL;
+  double *T = target_of(*c, what);
+  if (!T) return FAST_GPU_ESTATE;
+  // count per equation row
+  const int32_t neq = c->neq;
+  std::vector<int64_t> cnt(neq + 1, 0);
+  for (int32_t i = 0; i < neq; i++) {
+    const int32_t d = c->h_dof_of_eq[i], n = d / 3;
+    for (int32_t k = c->h_rowptr[n]; k < c->h_rowptr[n + 1]; k++)
+      for (int q = 0; q < 3; q++) {
+        const int32_t ej = c->h_eq[3 * (int64_t)c->h_col[k] + q];
+        if (ej && ej - 1 <= i) cnt[i + 1]++;
+      }
+  }
+  for (int32_t i = 0; i < neq; i++) cnt[i + 1] += cnt[i];
+  *nnz = cnt[neq];
+  if (!col || !val || !rowptr) return FAST_GPU_OK;
+  std::vector<double> hv((size_t)9 * c->nnzb);
+  CK(cudaMemcpyAsync(hv.data(), T, sizeof(double) * hv.size(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  std::memcpy(rowptr, cnt.data(), sizeof(int64_t) * (neq + 1));
+  std::vector<std::pair<int32_t, double>> row;
+  for (int32_t i = 0; i < neq; i++) {
+    const int32_t d = c->h_dof_of_eq[i], n = d / 3, p = d % 3;
+    row.clear();
+    for (int32_t k = c->h_rowptr[n]; k < c->h_rowptr[n + 1]; k++)
+      for (int q = 0; q < 3; q++) {
+        const int32_t ej = c->h_eq[3 * (int64_t)c->h_col[k] + q];
+        if (ej && ej - 1 <= i) row.emplace_back(ej - 1, hv[(size_t)k * 9 + p * 3 + q]);
+      }
+    std::sort(row.begin(), row.end(), [](const auto &a, const auto &b) { return a.first < b.first; });
+    int64_t o = cnt[i];
+    for (auto &pr : row) { col[o] = pr.first; val[o] = pr.second; o++; }
+  }
+  return FAST_GPU_OK;
+}
+
+int fast_gpu_element_matrices(fast_gpu_ctx *c, int32_t what, int32_t b, int64_t first, int64_t count, double *Ke) {
+  if (check_ctx(c) || !Ke || b < 0 || b >= (int)c->buckets.size()) return FAST_GPU_EINVAL;
+  const Bucket &B = c->buckets[b];
+  if (first < 0 || count <= 0 || first + count > B.ne) return FAST_GPU_EINVAL;
+  if (what == FAST_ASM_MASS && !B.has_rho) { c->err = "element_matrices: bucket has no density"; return FAST_GPU_ESTATE; }
+  const int nd = 3 * B.nn;
+  const size_t mat_bytes = sizeof(double) * (size_t)count * nd * nd;
+  double *buf = nullptr;
+  CK(cudaMalloc((void **)&buf, mat_bytes + sizeof(int32_t) * count + 16));
+  std::vector<int32_t> idx(count);
+  for (int64_t k = 0; k < count; k++) idx[k] = B.inv[first + k];
+  cudaError_t e = cudaMemcpyAsync((char *)buf + mat_bytes, idx.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(buf, 0, mat_bytes, c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_status, 0, sizeof(int32_t), c->stream);
+  if (e == cudaSuccess) e = launch_element_matrices(*c, what, b, 0, count, buf);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(Ke, buf, mat_bytes, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(buf);
+  if (e != cudaSuccess) { c->err = std::string("element_matrices: ") + cudaGetErrorString(e); return FAST_GPU_ECUDA; }
+  return FAST_GPU_OK;
+}
+
+int fast_gpu_inspect_pattern(const fast_gpu_mesh *m, int64_t *nnzb, int64_t *nnz_lower, int32_t *ncol,
+                             int32_t *rowptr, int32_t *col, int32_t *color) {
+  if (!m || m->num_nodes <= 0 || !m->node_eq || m->num_buckets <= 0 || !m->buckets) return FAST_GPU_EINVAL;
+  Ctx c;
+  c.nnode = m->num_nodes;
+  c.h_eq.assign(m->node_eq, m->node_eq + 3 * m->num_nodes);
+  c.buckets.resize(m->num_buckets);
+  for (int b = 0; b < m->num_buckets; b++) {
+    c.buckets[b].type = m->buckets[b].elem_type;
+    c.buckets[b].nn = nodes_of(m->buckets[b].elem_type);
+    c.buckets[b].ne = m->buckets[b].num_elems;
+    if (!c.buckets[b].nn || !m->buckets[b].conn) return FAST_GPU_ENOTSUP;
+  }
+  if (!build_pattern(c, *m)) return FAST_GPU_EINVAL;
+  if (nnzb) *nnzb = c.nnzb;
+  if (nnz_lower) *nnz_lower = c.nnz_lower_eq;
+  if (ncol) *ncol = c.ncolors;
+  if (rowptr) std::memcpy(rowptr, c.h_rowptr.data(), sizeof(int32_t) * (m->num_nodes + 1));
+  if (col) std::memcpy(col, c.h_col.data(), sizeof(int32_t) * c.nnzb);
+  if (color) {
+    const Bucket &B = c.buckets[0];
+    for (size_t k = 0; k + 1 < B.color_off.size(); k++)
+      for (int64_t s = B.color_off[k]; s < B.color_off[k + 1]; s++) color[B.perm[s]] = (int32_t)k;
+  }
+  // the slot map must cover every element node pair
+  for (const Bucket &B : c.buckets)
+    for (int32_t v : B.h_slot)
+      if (v < 0) return FAST_GPU_EINVAL;
+  return FAST_GPU_OK;
+}
+
+int fast_gpu_launch_count(fast_gpu_ctx *c, int64_t *n) {
+  if (check_ctx(c) || !n) return FAST_GPU_EINVAL;
+  *n = c->launches;
+  return FAST_GPU_OK;
+}
+
+int fast_gpu_time_kernel(fast_gpu_ctx *c, int32_t which, int32_t reps, double *avg_ms, double *bytes) {
+  if (check_ctx(c) || reps < 1 || !avg_ms) return FAST_GPU_EINVAL;
+  if (!c->K_ok) { c->err = "time_kernel: matrix not assembled"; return FAST_GPU_ESTATE; }
+  const int64_t n3 = 3 * c->nnode;
+  double algo = 0.0;
+  if (which == FAST_KERNEL_SPMV_FP32 && !c->K32_ok) {
+    if (!c->d_K32) CK(dalloc(&c->d_K32, 9 * c->nnzb));
+    CK(launch_to_fp32(*c, c->d_K, c->d_K32, 9 * c->nnzb));
+    c->K32_ok = true;
+  }
+  auto run = [&]() -> cudaError_t {
+    if (which == FAST_KERNEL_SPMV_FP64) return launch_spmv(*c, c->d_K, c->d_p, c->d_w);
+    if (which == FAST_KERNEL_SPMV_FP32) return launch_spmv32(*c, c->d_K32, c->s_p, c->s_w);
+    if (which == FAST_KERNEL_ASSEMBLE) {
+      cudaError_t e = launch_zero_matrix(*c, c->d_K, true);
+      return e == cudaSuccess ? launch_assemble(*c, FAST_ASM_STIFFNESS, c->d_K) : e;
+    }
+    return cudaErrorInvalidValue;
+  };
+  if (which == FAST_KERNEL_SPMV_FP64) {
+    algo = (double)c->nnzb * (9 * 8 + 4) + 4.0 * (c->nnode + 1) + 2.0 * 8 * n3;
+  } else if (which == FAST_KERNEL_SPMV_FP32) {
+    algo = (double)c->nnzb * (9 * 4 + 4) + 4.0 * (c->nnode + 1) + 2.0 * 4 * n3;
+  } else if (which == FAST_KERNEL_ASSEMBLE) {
+    // scatter model per element: incidence + coordinates + fixity + E, nu + slot map + 3x3 block RMW,
+    // plus the zero fill of the block values
+    for (const Bucket &B : c->buckets) {
+      const double nn = B.nn;
+      algo += (double)B.ne * (nn * (4 + 24 + 1) + 16 + nn * nn * (4 + 2 * 72));
+    }
+    algo += 72.0 * c->nnzb;
+  } else {
+    return FAST_GPU_EINVAL;
+  }
+  CK(cudaMemsetAsync(c->d_p, 0, sizeof(double) * n3, c->stream));
+  CK(cudaMemsetAsync(c->s_p, 0, sizeof(float) * n3, c->stream));
+  CK(run());
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, c->stream));
+  for (int r = 0; r < reps; r++) CK(run());
+  CK(cudaEventRecord(e1, c->stream));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *avg_ms = ms / reps;
+  if (bytes) *bytes = algo;
+  if (which == FAST_KERNEL_ASSEMBLE) { c->K32_ok = false; c->precond_built = -1; }
+  return FAST_GPU_OK;
+}
+
+}  // extern "C"

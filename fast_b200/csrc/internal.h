@@ -1,0 +1,137 @@
+// internal.h - private types of libfastgpu (not part of the C ABI).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "fast_gpu.h"
+
+namespace fastgpu {
+
+// Largest element supported by the integration kernels (hex20) and largest
+// Gauss rule (4x4x4).
+constexpr int kMaxNodes = 20;
+constexpr int kMaxGauss = 64;
+
+// Device-side solver scalars.  All scalars are FP64 even when the vectors
+// are FP32; reductions are fixed-order, so a solve is bit-reproducible.
+struct PcgState {
+  double dot0;    // z.r of the current iterate
+  double alpha;
+  double beta;
+  double lenf;    // |rhs| (the reference's normaliser, PCGSolver)
+  double rr;      // r.r after the last update
+  double err;     // sqrt(rr) / lenf
+  double tol;
+  double pw;      // p.w of the last iteration
+  int32_t iter;   // iterations completed
+  int32_t done;   // 0 running, 1 converged, 2 iteration cap, 3 breakdown
+  int32_t maxit;
+  int32_t pad;
+};
+
+struct Bucket {
+  int type = 0;            // FAST_ELEM_*
+  int nn = 0;              // nodes per element
+  int ngp[3] = {0, 0, 0};
+  int ng = 0;              // total Gauss points
+  int64_t ne = 0;
+  std::vector<int32_t> perm;       // colour-sorted position -> original element
+  std::vector<int32_t> inv;        // original element -> colour-sorted position
+  std::vector<int64_t> color_off;  // [ncolors+1] offsets in colour-sorted order
+  std::vector<int32_t> h_conn;     // colour-sorted incidence
+  std::vector<int32_t> h_slot;     // colour-sorted slot map (freed after upload)
+  bool has_rho = false;
+  int32_t *d_conn = nullptr;       // [ne][nn] colour-sorted
+  double *d_E = nullptr, *d_nu = nullptr, *d_rho = nullptr;
+  int32_t *d_slot = nullptr;       // [ne][nn][nn] block index of node pair (a, b)
+  double *d_dN = nullptr;          // [ng][nn][3] natural derivatives at the Gauss points
+  double *d_N = nullptr;           // [ng][nn] shape functions
+  double *d_w = nullptr;           // [ng] Gauss weights
+};
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int sm_count = 148;
+
+  // mesh
+  int64_t nnode = 0;
+  int32_t neq = 0;
+  std::vector<int32_t> h_eq;      // [nnode*3] 1-based, 0 fixed
+  std::vector<int32_t> h_dof_of_eq;  // [neq] node-DOF index 3*n+i of equation k+1
+  double *d_X = nullptr;          // [nnode][3]
+  uint8_t *d_fix = nullptr;       // [nnode] bit i set: DOF i has no equation
+  int32_t *d_dof_of_eq = nullptr; // [neq]
+  std::vector<Bucket> buckets;
+
+  // node-block (3x3) CSR pattern, full (both triangles)
+  int64_t nnzb = 0;
+  std::vector<int32_t> h_rowptr, h_col, h_diag;
+  int32_t *d_rowptr = nullptr, *d_col = nullptr, *d_diag = nullptr;
+  int32_t ncolors = 0;
+  double pattern_seconds = 0.0;
+  int64_t nnz_lower_eq = 0;
+
+  // assembled matrices: [nnzb][3][3]
+  double *d_K = nullptr, *d_M = nullptr;
+  float *d_K32 = nullptr;
+  bool K_ok = false, M_ok = false, K32_ok = false;
+  int32_t *d_status = nullptr;    // device error flags (detJ)
+  int32_t *h_status = nullptr;    // pinned
+
+  // solver workspace in node-DOF space (3*nnode)
+  double *d_u = nullptr, *d_r = nullptr, *d_z = nullptr, *d_p = nullptr, *d_w = nullptr, *d_f = nullptr;
+  double *d_dinv = nullptr;       // [nnode][9] inverse diagonal (Jacobi) or inverse 3x3 block
+  float *s_u = nullptr, *s_r = nullptr, *s_z = nullptr, *s_p = nullptr, *s_w = nullptr;
+  float *s_dinv = nullptr;        // [nnode][9]
+  int precond_built = -1;         // which preconditioner d_dinv holds
+  double *d_partials = nullptr;   // reduction partials [2][kRedBlocks]
+  PcgState *d_state = nullptr;
+  PcgState *h_state = nullptr;    // pinned
+  double *d_eq_tmp = nullptr;     // [neq] staging for host <-> device in equation space
+  double *h_eq_tmp = nullptr;     // pinned [neq]
+
+  int64_t launches = 0;          // kernels launched by this context (all entry points)
+
+  bool set_error(const std::string &m) { err = m; return false; }
+};
+
+// pattern.cpp
+bool build_pattern(Ctx &c, const fast_gpu_mesh &m);
+
+// shape tables (shape_tables.cpp)
+bool gauss_rule(int n, double *r, double *w);
+void gauss_point_tables(int type, const int ngp[3], std::vector<double> &N, std::vector<double> &dN,
+                        std::vector<double> &w);
+int nodes_of(int type);
+
+// kernels (elem_kernels.cu / solve_kernels.cu); all launched on c.stream
+cudaError_t launch_zero_matrix(Ctx &c, double *K, bool identity_on_fixed);
+cudaError_t launch_assemble(Ctx &c, int what, double *target);
+cudaError_t launch_element_matrices(Ctx &c, int what, int bucket, int64_t first_sorted, int64_t count,
+                                    double *d_out);
+cudaError_t launch_to_fp32(Ctx &c, const double *src, float *dst, int64_t n);
+
+constexpr int kRedBlocks = 592;   // fixed reduction grid: 4 x 148 SMs
+cudaError_t launch_build_precond(Ctx &c, const double *K, int precond);
+// FP64 / FP32 PCG building blocks (node-DOF space vectors)
+cudaError_t pcg_solve_device(Ctx &c, bool fp32, const double *d_rhs_node, double *d_x_node, bool warm,
+                             double tol, int maxit, int check_every, int precond, int *iters,
+                             double *err, int *done);
+cudaError_t launch_residual(Ctx &c, const double *K, const double *f, const double *u, double *r,
+                            double *rr_out_dev);
+cudaError_t launch_spmv(Ctx &c, const double *K, const double *x, double *y);
+cudaError_t launch_spmv32(Ctx &c, const float *K, const float *x, float *y);
+cudaError_t launch_eq_to_node(Ctx &c, const double *eqv, double *nodev);
+cudaError_t launch_node_to_eq(Ctx &c, const double *nodev, double *eqv);
+cudaError_t launch_norm2(Ctx &c, const double *x, int64_t n, double *out_dev);
+cudaError_t scale_inplace(Ctx &c, double *x, int64_t n, double a);
+cudaError_t axpy_inplace(Ctx &c, double *y, const double *x, int64_t n, double a);
+
+}  // namespace fastgpu

@@ -1,0 +1,316 @@
+"""ctypes binding of libfastgpu.so (the C ABI in include/fast_gpu.h).
+
+:class:`GpuSystem` mirrors the part of FAST's interface the C ABI replaces:
+
+* ``upload(deck)``           - cControl::Init's equation/profile set-up
+                               (ctrl/ctrl.cpp:2004-2157) for the device matrix;
+* ``assemble()``             - cControl::StiffnessMatrix (ctrl/ctrl.cpp:886-975);
+* ``assemble_mass()``        - cControl::MassMatrix (ctrl/ctrl.cpp:979-1027);
+* ``add/get/mult_vect``      - cSysMatrix::Add/Get/MultVect (mlib/sysmat.h:60-99);
+* ``solve(f)``               - cSysMatrix::Solve -> PCGSolver (mlib/sysmat.cpp:1061-1125);
+* ``ext_load(deck)``         - cControl::ExtLoadVector for face tractions.
+
+There is no CPU fallback: if the library is missing or no CUDA device is
+present, constructing a :class:`GpuSystem` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+from . import decks as _decks
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfastgpu.so")
+
+FAST_GPU_OK = 0
+ERRORS = {-1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ESTATE", -5: "ENONCONV", -6: "EDETJ", -7: "ENOTSUP",
+          -8: "ENOTFOUND"}
+ELEM = {"hex8": 1, "hex20": 2}
+ASM_K, ASM_M = 1, 2
+PREC_FP64, PREC_MIXED = 0, 1
+PRECOND_JACOBI, PRECOND_BLOCK_JACOBI = 0, 1
+
+# Every entry point the header declares; the CPU test checks the library exports all of them.
+EXPORTS = [
+    "fast_gpu_create", "fast_gpu_destroy", "fast_gpu_last_error", "fast_gpu_version", "fast_gpu_set_stream",
+    "fast_gpu_synchronize", "fast_gpu_upload_mesh", "fast_gpu_pattern_info", "fast_gpu_update_coords",
+    "fast_gpu_update_material", "fast_gpu_zero", "fast_gpu_assemble", "fast_gpu_add", "fast_gpu_get",
+    "fast_gpu_mult_vect", "fast_gpu_solve", "fast_gpu_solve_device", "fast_gpu_face_load_vector",
+    "fast_gpu_get_lower_csr", "fast_gpu_element_matrices", "fast_gpu_launch_count", "fast_gpu_time_kernel",
+    "fast_gpu_inspect_pattern",
+]
+KERNEL_SPMV_FP64, KERNEL_SPMV_FP32, KERNEL_ASSEMBLE = 0, 1, 2
+
+
+class FastGpuError(RuntimeError):
+    def __init__(self, rc, msg=""):
+        super().__init__(f"{ERRORS.get(rc, rc)}: {msg}")
+        self.rc = rc
+
+
+class Bucket(ctypes.Structure):
+    _fields_ = [("elem_type", ctypes.c_int32), ("ngp", ctypes.c_int32 * 3), ("num_elems", ctypes.c_int64),
+                ("conn", ctypes.POINTER(ctypes.c_int32)), ("E", ctypes.POINTER(ctypes.c_double)),
+                ("nu", ctypes.POINTER(ctypes.c_double)), ("rho", ctypes.POINTER(ctypes.c_double))]
+
+
+class Mesh(ctypes.Structure):
+    _fields_ = [("num_nodes", ctypes.c_int64), ("coords", ctypes.POINTER(ctypes.c_double)),
+                ("node_eq", ctypes.POINTER(ctypes.c_int32)), ("num_eq", ctypes.c_int32),
+                ("num_buckets", ctypes.c_int32), ("buckets", ctypes.POINTER(Bucket))]
+
+
+class SolveOpts(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int32), ("precond", ctypes.c_int32), ("maxit", ctypes.c_int32),
+                ("warm_start", ctypes.c_int32), ("tol", ctypes.c_double), ("inner_tol", ctypes.c_double),
+                ("max_outer", ctypes.c_int32), ("check_every", ctypes.c_int32)]
+
+
+class SolveReport(ctypes.Structure):
+    _fields_ = [("converged", ctypes.c_int32), ("iterations", ctypes.c_int32), ("outer", ctypes.c_int32),
+                ("reserved", ctypes.c_int32), ("rel_residual", ctypes.c_double),
+                ("true_rel_residual", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+_lib = None
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int32)
+_lp = ctypes.POINTER(ctypes.c_int64)
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libfastgpu.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FastGpuError(-4, f"{path} is missing: build it with `python -m fast_b200.build`")
+    L = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    L.fast_gpu_create.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
+    L.fast_gpu_destroy.argtypes = [vp]
+    L.fast_gpu_last_error.argtypes = [vp]
+    L.fast_gpu_last_error.restype = ctypes.c_char_p
+    L.fast_gpu_set_stream.argtypes = [vp, vp]
+    L.fast_gpu_synchronize.argtypes = [vp]
+    L.fast_gpu_upload_mesh.argtypes = [vp, ctypes.POINTER(Mesh)]
+    L.fast_gpu_pattern_info.argtypes = [vp, _lp, _lp, _ip, _dp]
+    L.fast_gpu_update_coords.argtypes = [vp, _dp]
+    L.fast_gpu_update_material.argtypes = [vp, ctypes.c_int32, _dp, _dp]
+    L.fast_gpu_zero.argtypes = [vp, ctypes.c_int32]
+    L.fast_gpu_assemble.argtypes = [vp, ctypes.c_int32]
+    L.fast_gpu_add.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_double]
+    L.fast_gpu_get.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _dp]
+    L.fast_gpu_mult_vect.argtypes = [vp, ctypes.c_int32, _dp, _dp]
+    L.fast_gpu_solve.argtypes = [vp, _dp, _dp, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveReport)]
+    L.fast_gpu_solve_device.argtypes = [vp, vp, vp, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveReport)]
+    L.fast_gpu_face_load_vector.argtypes = [ctypes.c_int64, _dp, _ip, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                            _ip, _dp, _ip, ctypes.c_int32, _dp]
+    L.fast_gpu_get_lower_csr.argtypes = [vp, ctypes.c_int32, _lp, _lp, _ip, _dp]
+    L.fast_gpu_element_matrices.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, _dp]
+    L.fast_gpu_launch_count.argtypes = [vp, _lp]
+    L.fast_gpu_inspect_pattern.argtypes = [ctypes.POINTER(Mesh), _lp, _lp, _ip, _ip, _ip, _ip]
+    L.fast_gpu_time_kernel.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, _dp, _dp]
+    _lib = L
+    return L
+
+
+def _p(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+def face_load_vector(deck: _decks.Deck) -> np.ndarray:
+    """External load vector of the deck's face tractions (library host routine)."""
+    L = load_library()
+    neq = deck.num_eq()
+    f = np.zeros(neq)
+    if deck.face_elem is None or not len(deck.face_elem):
+        return f
+    fn = np.ascontiguousarray(deck.face_nodes(), dtype=np.int32)
+    X = np.ascontiguousarray(deck.coords, dtype=np.float64)
+    eq = np.ascontiguousarray(deck.node_eq(), dtype=np.int32)
+    q = np.ascontiguousarray(deck.face_q, dtype=np.float64)
+    loc = np.ascontiguousarray(deck.face_local, dtype=np.int32)
+    rc = L.fast_gpu_face_load_vector(deck.num_nodes, _p(X), _p(eq, _ip), neq, fn.shape[0], fn.shape[1], _p(fn, _ip),
+                                     _p(q), _p(loc, _ip), int(max(deck.ngp)), _p(f))
+    if rc != FAST_GPU_OK:
+        raise FastGpuError(rc, "face_load_vector")
+    return f
+
+
+def _mesh_struct(deck: _decks.Deck):
+    coords = np.ascontiguousarray(deck.coords, dtype=np.float64)
+    eq = np.ascontiguousarray(deck.node_eq(), dtype=np.int32)
+    conn = np.ascontiguousarray(deck.conn, dtype=np.int32)
+    E = np.ascontiguousarray(deck.E, dtype=np.float64)
+    nu = np.ascontiguousarray(deck.nu, dtype=np.float64)
+    rho = None if deck.rho is None else np.ascontiguousarray(deck.rho, dtype=np.float64)
+    b = Bucket(ELEM[deck.kind], (ctypes.c_int32 * 3)(*deck.ngp), deck.num_elems, _p(conn, _ip), _p(E), _p(nu),
+               _p(rho) if rho is not None else ctypes.POINTER(ctypes.c_double)())
+    buckets = (Bucket * 1)(b)
+    m = Mesh(deck.num_nodes, _p(coords), _p(eq, _ip), int(eq.max(initial=0)), 1, buckets)
+    return m, (coords, eq, conn, E, nu, rho, buckets)
+
+
+def inspect_pattern(deck: _decks.Deck) -> dict:
+    """Host-only pattern and colouring of a deck (no device needed)."""
+    L = load_library()
+    m, keep = _mesh_struct(deck)
+    nnzb, nlow, ncol = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32()
+    rc = L.fast_gpu_inspect_pattern(ctypes.byref(m), ctypes.byref(nnzb), ctypes.byref(nlow), ctypes.byref(ncol),
+                                    _ip(), _ip(), _ip())
+    if rc != FAST_GPU_OK:
+        raise FastGpuError(rc, "inspect_pattern")
+    rp = np.zeros(deck.num_nodes + 1, np.int32)
+    col = np.zeros(nnzb.value, np.int32)
+    color = np.zeros(deck.num_elems, np.int32)
+    rc = L.fast_gpu_inspect_pattern(ctypes.byref(m), ctypes.byref(nnzb), ctypes.byref(nlow), ctypes.byref(ncol),
+                                    _p(rp, _ip), _p(col, _ip), _p(color, _ip))
+    if rc != FAST_GPU_OK:
+        raise FastGpuError(rc, "inspect_pattern")
+    return {"nnz_blocks": nnzb.value, "nnz_lower_eq": nlow.value, "num_colors": ncol.value, "rowptr": rp,
+            "col": col, "color": color}
+
+
+class GpuSystem:
+    """One device context holding one mesh, its matrices and solver state."""
+
+    def __init__(self, device: int = 0):
+        self.L = load_library()
+        self.ctx = ctypes.c_void_p()
+        rc = self.L.fast_gpu_create(device, ctypes.byref(self.ctx))
+        if rc != FAST_GPU_OK:
+            raise FastGpuError(rc, "fast_gpu_create (is a CUDA device present?)")
+        self.neq = 0
+        self._keep = []
+
+    # -- plumbing
+    def _ck(self, rc, what=""):
+        if rc != FAST_GPU_OK:
+            msg = self.L.fast_gpu_last_error(self.ctx).decode(errors="replace")
+            raise FastGpuError(rc, f"{what}: {msg}")
+
+    def close(self):
+        if self.ctx:
+            self.L.fast_gpu_destroy(self.ctx)
+            self.ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: Optional[int]):
+        self._ck(self.L.fast_gpu_set_stream(self.ctx, ctypes.c_void_p(stream_ptr or 0)), "set_stream")
+
+    def synchronize(self):
+        self._ck(self.L.fast_gpu_synchronize(self.ctx), "synchronize")
+
+    # -- mesh
+    def upload(self, deck: _decks.Deck):
+        self.deck = deck
+        m, keep = _mesh_struct(deck)
+        self.neq = int(m.num_eq)
+        self._ck(self.L.fast_gpu_upload_mesh(self.ctx, ctypes.byref(m)), "upload_mesh")
+        self.node_eq = keep[1]
+        return self
+
+    def pattern_info(self):
+        a, b, c, d = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32(), ctypes.c_double()
+        self._ck(self.L.fast_gpu_pattern_info(self.ctx, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c),
+                                              ctypes.byref(d)))
+        return {"nnz_blocks": a.value, "nnz_lower_eq": b.value, "num_colors": c.value, "pattern_seconds": d.value}
+
+    def update_coords(self, coords):
+        coords = np.ascontiguousarray(coords, dtype=np.float64)
+        self._ck(self.L.fast_gpu_update_coords(self.ctx, _p(coords)), "update_coords")
+
+    def update_material(self, E=None, nu=None, bucket=0):
+        Ep = _p(np.ascontiguousarray(E, dtype=np.float64)) if E is not None else _dp()
+        nup = _p(np.ascontiguousarray(nu, dtype=np.float64)) if nu is not None else _dp()
+        self._ck(self.L.fast_gpu_update_material(self.ctx, bucket, Ep, nup), "update_material")
+
+    # -- cSysMatrix
+    def zero(self, what=ASM_K):
+        self._ck(self.L.fast_gpu_zero(self.ctx, what), "zero")
+
+    def assemble(self, what=ASM_K):
+        self._ck(self.L.fast_gpu_assemble(self.ctx, what), "assemble")
+
+    def assemble_mass(self):
+        self.assemble(ASM_M)
+
+    def add(self, i, j, v, what=ASM_K):
+        self._ck(self.L.fast_gpu_add(self.ctx, what, int(i), int(j), float(v)), "add")
+
+    def get(self, i, j, what=ASM_K):
+        v = ctypes.c_double()
+        self._ck(self.L.fast_gpu_get(self.ctx, what, int(i), int(j), ctypes.byref(v)), "get")
+        return v.value
+
+    def mult_vect(self, x, what=ASM_K):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros(self.neq)
+        self._ck(self.L.fast_gpu_mult_vect(self.ctx, what, _p(x), _p(y)), "mult_vect")
+        return y
+
+    def solve(self, f, tol=1e-8, precision=PREC_FP64, precond=PRECOND_JACOBI, maxit=0, u0=None,
+              inner_tol=0.0, max_outer=0, check_every=0, raise_on_nonconv=True):
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        u = np.zeros(self.neq) if u0 is None else np.array(u0, dtype=np.float64)
+        o = SolveOpts(precision, precond, int(maxit), int(u0 is not None), float(tol), float(inner_tol),
+                      int(max_outer), int(check_every))
+        rep = SolveReport()
+        rc = self.L.fast_gpu_solve(self.ctx, _p(f), _p(u), ctypes.byref(o), ctypes.byref(rep))
+        if rc != FAST_GPU_OK and (raise_on_nonconv or rc != -5):
+            self._ck(rc, "solve")
+        return u, rep.as_dict()
+
+    def solve_device(self, d_f_ptr: int, d_u_ptr: int, tol=1e-8, precision=PREC_FP64, precond=PRECOND_JACOBI,
+                     maxit=0, warm=False, inner_tol=0.0, max_outer=0, check_every=0):
+        o = SolveOpts(precision, precond, int(maxit), int(warm), float(tol), float(inner_tol), int(max_outer),
+                      int(check_every))
+        rep = SolveReport()
+        self._ck(self.L.fast_gpu_solve_device(self.ctx, ctypes.c_void_p(d_f_ptr), ctypes.c_void_p(d_u_ptr),
+                                              ctypes.byref(o), ctypes.byref(rep)), "solve_device")
+        return rep.as_dict()
+
+    # -- measurement
+    def launch_count(self) -> int:
+        n = ctypes.c_int64()
+        self._ck(self.L.fast_gpu_launch_count(self.ctx, ctypes.byref(n)), "launch_count")
+        return n.value
+
+    def time_kernel(self, which: int, reps: int = 10):
+        ms, b = ctypes.c_double(), ctypes.c_double()
+        self._ck(self.L.fast_gpu_time_kernel(self.ctx, which, reps, ctypes.byref(ms), ctypes.byref(b)), "time_kernel")
+        return ms.value, b.value
+
+    # -- parity
+    def lower_csr(self, what=ASM_K):
+        import scipy.sparse as sp
+        nnz = ctypes.c_int64()
+        self._ck(self.L.fast_gpu_get_lower_csr(self.ctx, what, ctypes.byref(nnz), _lp(), _ip(), _dp()), "lower_csr")
+        rp = np.zeros(self.neq + 1, np.int64)
+        ci = np.zeros(nnz.value, np.int32)
+        v = np.zeros(nnz.value)
+        self._ck(self.L.fast_gpu_get_lower_csr(self.ctx, what, ctypes.byref(nnz), _p(rp, _lp), _p(ci, _ip), _p(v)),
+                 "lower_csr")
+        return sp.csr_matrix((v, ci, rp), shape=(self.neq, self.neq))
+
+    def element_matrices(self, first=0, count=None, what=ASM_K, bucket=0):
+        nn = _decks.KINDS[self.deck.kind][0]
+        if count is None:
+            count = self.deck.num_elems - first
+        out = np.zeros((count, 3 * nn, 3 * nn))
+        self._ck(self.L.fast_gpu_element_matrices(self.ctx, what, bucket, int(first), int(count), _p(out)),
+                 "element_matrices")
+        return out

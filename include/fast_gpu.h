@@ -1,0 +1,192 @@
+/* fast_gpu.h - C ABI of libfastgpu.so, the B200 (sm_100a) implementation of
+ * FAST's solid element-integration, assembly and K.u solve path.
+ *
+ * The library sits under FAST's own C++ interfaces.  Each entry point below
+ * names the reference interface it replaces (file:line inside the FAST
+ * tree).  INTEGRATION.md shows the C++ shim a FAST maintainer adds: a
+ * cSysMatrix subclass whose virtuals forward here, and a batched
+ * cControl::StiffnessMatrix that uploads the mesh once and assembles on the
+ * device.
+ *
+ * Conventions
+ *   - Every call returns an int status: FAST_GPU_OK (0) or a negative
+ *     FAST_GPU_E* code; fast_gpu_last_error() gives a message.  No C++
+ *     exception crosses this boundary.
+ *   - Vectors passed as host pointers have length num_eq and follow FAST's
+ *     equation numbering (cControl::CompEqs, ctrl/ctrl.cpp:2056-2104):
+ *     entry k belongs to equation k+1.  They are what cVector::Val() gives.
+ *   - Matrix indices (i, j) are 0-based equation indices, as in
+ *     cSysMatrix::Add/Get (mlib/sysmat.h:85-86).
+ *   - The context owns all device memory; one context serves one host thread.
+ *   - Calls are stream-ordered on the context's stream; calls that return
+ *     host data synchronise that stream.  Every device wait is bounded.
+ */
+#ifndef FAST_GPU_H
+#define FAST_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FAST_GPU_ABI_VERSION 1
+
+/* ---- status codes ---------------------------------------------------- */
+#define FAST_GPU_OK         0
+#define FAST_GPU_EINVAL    -1   /* bad argument                                  */
+#define FAST_GPU_ENOMEM    -2   /* device or host allocation failed              */
+#define FAST_GPU_ECUDA     -3   /* CUDA runtime error                            */
+#define FAST_GPU_ESTATE    -4   /* call out of order (e.g. solve before assemble) */
+#define FAST_GPU_ENONCONV  -5   /* solver reached maxit without convergence       */
+#define FAST_GPU_EDETJ     -6   /* non-positive Jacobian determinant in an element */
+#define FAST_GPU_ENOTSUP   -7   /* element type / option not supported           */
+#define FAST_GPU_ENOTFOUND -8   /* (i, j) outside the sparsity pattern           */
+
+/* ---- element types (FAST readers elc/element.cpp:1985-2101) ----------- */
+#define FAST_ELEM_HEX8      1   /* %ELEMENT.BRICK8   cElmParam,  SHAPE_BRICK8  */
+#define FAST_ELEM_HEX20     2   /* %ELEMENT.BRICK20  cElmParam,  SHAPE_BRICK20 */
+
+/* ---- what to assemble ------------------------------------------------- */
+#define FAST_ASM_STIFFNESS  1   /* cControl::StiffnessMatrix (ctrl/ctrl.cpp:886-975) */
+#define FAST_ASM_MASS       2   /* cControl::MassMatrix      (ctrl/ctrl.cpp:979-1027) */
+
+/* ---- solver precision ------------------------------------------------- */
+#define FAST_PREC_FP64      0   /* FP64 Jacobi PCG, as PCGSolver (mlib/sysmat.cpp:1061-1125) */
+#define FAST_PREC_MIXED     1   /* FP32 PCG inside FP64 iterative refinement     */
+
+/* ---- preconditioner --------------------------------------------------- */
+#define FAST_PRECOND_JACOBI        0  /* z = r / diag(K), as the reference      */
+#define FAST_PRECOND_BLOCK_JACOBI  1  /* z = inv(3x3 nodal block) r               */
+
+typedef struct fast_gpu_ctx fast_gpu_ctx;
+
+/* One bucket = one element type with one Gauss rule (a FAST element reader
+ * block with one %INTEGRATION.ORDER). */
+typedef struct {
+  int32_t        elem_type;     /* FAST_ELEM_*                                 */
+  int32_t        ngp[3];        /* Gauss points per direction (r, s, t)        */
+  int64_t        num_elems;
+  const int32_t *conn;          /* [num_elems][nn] 0-based node indices, FAST local order */
+  const double  *E;             /* [num_elems] Young's modulus                 */
+  const double  *nu;            /* [num_elems] Poisson's ratio                 */
+  const double  *rho;           /* [num_elems] density, or NULL                */
+} fast_gpu_bucket;
+
+typedef struct {
+  int64_t                num_nodes;
+  const double          *coords;    /* [num_nodes][3]                          */
+  const int32_t         *node_eq;   /* [num_nodes][3] 1-based equation, 0 = fixed/unused */
+  int32_t                num_eq;
+  int32_t                num_buckets;
+  const fast_gpu_bucket *buckets;
+} fast_gpu_mesh;
+
+typedef struct {
+  int32_t precision;      /* FAST_PREC_*                                        */
+  int32_t precond;        /* FAST_PRECOND_*                                     */
+  int32_t maxit;          /* iteration cap (total inner iterations); 0 = 20*num_eq */
+  int32_t warm_start;     /* 1: start from the u passed in (mixed path: as the first iterate) */
+  double  tol;            /* stop when |r|/|f| < tol (|f| > 1e11 replaced by 1, as the reference) */
+  double  inner_tol;      /* FAST_PREC_MIXED: relative reduction per FP32 inner solve; 0 = 1e-5 */
+  int32_t max_outer;      /* FAST_PREC_MIXED: refinement steps cap; 0 = 30       */
+  int32_t check_every;    /* convergence read-back period in iterations; 0 = 32 */
+} fast_gpu_solve_opts;
+
+typedef struct {
+  int32_t converged;
+  int32_t iterations;      /* PCG iterations (sum of inner iterations when mixed) */
+  int32_t outer;           /* refinement steps (1 for FP64)                        */
+  int32_t reserved;
+  double  rel_residual;    /* |r|/|f| of the final FP64 residual (mixed) or recurrence (FP64) */
+  double  true_rel_residual; /* |f - K u| / |f| recomputed in FP64 at exit           */
+} fast_gpu_solve_report;
+
+/* ---- lifetime ---------------------------------------------------------- */
+int         fast_gpu_create(int device, fast_gpu_ctx **ctx);
+int         fast_gpu_destroy(fast_gpu_ctx *ctx);
+const char *fast_gpu_last_error(const fast_gpu_ctx *ctx);
+int         fast_gpu_version(void);
+/* Use a caller's CUDA stream (a cudaStream_t passed as void*); NULL = context's own. */
+int         fast_gpu_set_stream(fast_gpu_ctx *ctx, void *cuda_stream);
+int         fast_gpu_synchronize(fast_gpu_ctx *ctx);
+
+/* ---- mesh and pattern ---------------------------------------------------
+ * Replaces cControl::Init's CompEqs/CompProf (ctrl/ctrl.cpp:2004-2157) for the
+ * device matrix: copies the mesh, builds the node-block (3x3) CSR pattern,
+ * the element-to-block slot map and a greedy element colouring. */
+int fast_gpu_upload_mesh(fast_gpu_ctx *ctx, const fast_gpu_mesh *mesh);
+int fast_gpu_pattern_info(fast_gpu_ctx *ctx, int64_t *nnz_blocks, int64_t *nnz_lower_eq,
+                          int32_t *num_colors, double *pattern_seconds);
+/* Same topology, new values (host buffers of the upload's sizes). */
+int fast_gpu_update_coords(fast_gpu_ctx *ctx, const double *coords);
+int fast_gpu_update_material(fast_gpu_ctx *ctx, int32_t bucket, const double *E, const double *nu);
+
+/* ---- cSysMatrix replacement (mlib/sysmat.h:60-99) ------------------------ */
+/* cSysMatrix::Zero */
+int fast_gpu_zero(fast_gpu_ctx *ctx, int32_t what);
+/* cControl::StiffnessMatrix / MassMatrix over every bucket: element
+ * integration (cElmParam::StiffMat elc/elmparam.cpp:539-597, MassMat :672-739)
+ * and colour-scheduled scatter (cElement::AddGlobMat elc/element.cpp:2975-3002).
+ * Zeroes the target first.  Deterministic: the result is bit-identical run to run. */
+int fast_gpu_assemble(fast_gpu_ctx *ctx, int32_t what);
+/* cSysMatrix::Add(i, j, v): adds v to K(i,j) and K(j,i) when i != j, like the
+ * reference's symmetric matrices; (i, j) must lie in the pattern. */
+int fast_gpu_add(fast_gpu_ctx *ctx, int32_t what, int32_t i, int32_t j, double v);
+/* cSysMatrix::Get(i, j) */
+int fast_gpu_get(fast_gpu_ctx *ctx, int32_t what, int32_t i, int32_t j, double *v);
+/* cSysMatrix::MultVect(in, out): out = K in, equation space, host buffers. */
+int fast_gpu_mult_vect(fast_gpu_ctx *ctx, int32_t what, const double *x, double *y);
+/* cSysMatrix::Solve(b, x) (mlib/sysmat.cpp:966-970 -> PCGSolver :1061-1125):
+ * host f and u of length num_eq. */
+int fast_gpu_solve(fast_gpu_ctx *ctx, const double *f, double *u,
+                   const fast_gpu_solve_opts *opts, fast_gpu_solve_report *rep);
+/* Same with device pointers (equation space, length num_eq). */
+int fast_gpu_solve_device(fast_gpu_ctx *ctx, const double *d_f, double *d_u,
+                          const fast_gpu_solve_opts *opts, fast_gpu_solve_report *rep);
+
+/* ---- external load (host) ---------------------------------------------
+ * cControl::ExtLoadVector (ctrl/ctrl.cpp:668-715) for uniform face tractions
+ * (%LOAD.CASE.AREA.UNIFORM; cElemLoad::ExtForce load/load.cpp:618-706):
+ * face_nodes [num_faces][nodes_per_face] in the Q4 (4) / Q8 (8) face-shape
+ * order of cShapeBrick8/20::GetFace (shp/shpsolid.cpp:264-276, 459-471);
+ * q [num_faces][3]; local [num_faces] (NULL = all global); f [num_eq] out.
+ * Needs no context and no device. */
+int fast_gpu_face_load_vector(int64_t num_nodes, const double *coords, const int32_t *node_eq, int32_t num_eq,
+                              int32_t num_faces, int32_t nodes_per_face, const int32_t *face_nodes,
+                              const double *q, const int32_t *local, int32_t ngp1d, double *f);
+
+/* ---- parity / inspection ---------------------------------------------- */
+/* Host-only: builds the node-block pattern and element colouring of a mesh
+ * without a device and reports them.  rowptr [num_nodes+1], col [nnz_blocks]
+ * and color [num_elems of bucket 0] may be NULL (call once with NULLs to get
+ * the sizes). */
+int fast_gpu_inspect_pattern(const fast_gpu_mesh *mesh, int64_t *nnz_blocks, int64_t *nnz_lower_eq,
+                             int32_t *num_colors, int32_t *rowptr, int32_t *col, int32_t *color);
+/* Equation-space lower triangle of the assembled matrix as CSR (what the
+ * reference's symmetric matrices store).  Call with col == NULL to get nnz. */
+int fast_gpu_get_lower_csr(fast_gpu_ctx *ctx, int32_t what, int64_t *nnz,
+                           int64_t *rowptr, int32_t *col, double *val);
+/* Element matrices of elements [first, first+count) of a bucket, computed by
+ * the same device kernels as the assembly: [count][3nn][3nn] row-major in
+ * FAST's element DOF order (cElement::GetElmDofs). */
+int fast_gpu_element_matrices(fast_gpu_ctx *ctx, int32_t what, int32_t bucket, int64_t first,
+                              int64_t count, double *Ke);
+
+/* ---- measurement ------------------------------------------------------ */
+#define FAST_KERNEL_SPMV_FP64  0   /* one K.p of the FP64 PCG (node-block CSR, FP64 values) */
+#define FAST_KERNEL_SPMV_FP32  1   /* one K32.p of the FP32 inner PCG                       */
+#define FAST_KERNEL_ASSEMBLE   2   /* one full stiffness assembly (zero fill + all colours)  */
+/* Kernels this context has launched so far (every entry point counts). */
+int fast_gpu_launch_count(fast_gpu_ctx *ctx, int64_t *count);
+/* Times `reps` back-to-back runs of one kernel with CUDA events on the
+ * context's stream (after one untimed run) and returns the mean duration and
+ * the algorithmic bytes one run moves (the roofline numerator). */
+int fast_gpu_time_kernel(fast_gpu_ctx *ctx, int32_t which, int32_t reps, double *avg_ms,
+                         double *bytes_per_run);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FAST_GPU_H */

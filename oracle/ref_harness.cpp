@@ -27,11 +27,11 @@
 //       With --u the element quantities are evaluated at the given nodal state
 //       (for total-Lagrangian elements).
 //
-//   fastref bench <deck> <pcg_iters>
+//   fastref bench <deck> <pcg_iters> [reps]
 //       Times the reference CPU path on one host thread: StiffnessMatrix into
-//       the deck's sparse matrix (cSymSprsMatrix, mlib/sysmat.cpp:889) and
-//       <pcg_iters> iterations of PCGSolver (mlib/sysmat.cpp:1061).  Prints
-//       one JSON line.
+//       the deck's sparse matrix (cSymSprsMatrix, mlib/sysmat.cpp:889) once,
+//       then [reps] (default 1) runs of <pcg_iters> iterations of PCGSolver
+//       (mlib/sysmat.cpp:1061), each timed.  Prints one JSON line.
 
 #include <chrono>
 #include <cmath>
@@ -252,6 +252,8 @@ static int mode_bench(int argc, char **argv)
 {
   string deck = argv[2];
   int iters = argc > 3 ? atoi(argv[3]) : 5;
+  int reps = argc > 4 ? atoi(argv[4]) : 1;
+  if (reps < 1) reps = 1;
   streambuf *coutbuf = cout.rdbuf( );
   ofstream devnull("/dev/null");
   cout.rdbuf(devnull.rdbuf( ));
@@ -278,13 +280,19 @@ static int mode_bench(int argc, char **argv)
   double t_int = now_s( ) - t2;
 
   cVector u(neq);
-  double t3 = now_s( );
-  PCGSolver(iters, 1e-300, K, f, u);
-  double t_pcg = now_s( ) - t3;
+  vector<double> t_pcg(reps);
+  for (int r = 0; r < reps; r++)
+  {
+    double t3 = now_s( );
+    PCGSolver(iters, 1e-300, K, f, u);
+    t_pcg[r] = now_s( ) - t3;
+  }
   cout.rdbuf(coutbuf);
   printf("{\"neq\": %d, \"ne\": %d, \"nnz_lower\": %lld, \"read_s\": %.6f, \"assembly_s\": %.6f, "
-         "\"integration_s\": %.6f, \"pcg_iters\": %d, \"pcg_s\": %.6f}\n",
-         neq, ne, nnz_lower, t_read, t_asm, t_int, iters, t_pcg);
+         "\"integration_s\": %.6f, \"pcg_iters\": %d, \"pcg_s\": %.6f, \"pcg_rep_s\": [",
+         neq, ne, nnz_lower, t_read, t_asm, t_int, iters, t_pcg[0]);
+  for (int r = 0; r < reps; r++) printf("%s%.6f", r ? ", " : "", t_pcg[r]);
+  printf("]}\n");
   return 0;
 }
 

@@ -1,0 +1,157 @@
+"""Device parity: the CUDA path (through the C ABI) against the reference's
+golden dumps and the CPU oracle.  Needs a B200."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from fast_b200 import decks, gpu
+from oracle import fem_oracle as fo
+from tests import golden_io as gio
+
+pytestmark = pytest.mark.gpu
+
+# FP64 element and assembly parity bound (relative to the largest entry)
+TOL_K = 1e-12
+# displacement parity bound for well-conditioned decks
+TOL_U = 1e-9
+
+LINEAR = [n for n in gio.names() if n not in ("cfg_hex8_tl_state",)]
+WITH_K = [n for n in LINEAR if "ref_K_data" in gio.load(n)[1]]
+SOLVABLE = ["cfg_hex8_cantilever", "cfg_hex20_lognormal_4x4x2", "cfg_hex20_lognormal_8x8x4"]
+
+
+def system(d):
+    s = gpu.GpuSystem(0)
+    s.upload(d)
+    return s
+
+
+@pytest.mark.parametrize("name", LINEAR)
+def test_element_stiffness_matches_reference(name):
+    d, g = gio.load(name)
+    s = system(d)
+    el = g["ref_elems"]
+    for k, e in enumerate(el):
+        Ke = s.element_matrices(int(e), 1)[0]
+        assert gio.rel(Ke, g["ref_elm_K"][k]) < TOL_K, (name, e)
+
+
+@pytest.mark.parametrize("name", WITH_K)
+def test_assembled_matrix_matches_reference(name):
+    d, g = gio.load(name)
+    s = system(d)
+    s.assemble()
+    K = s.lower_csr()
+    R = gio.lower_K(g)
+    assert K.nnz == R.nnz
+    assert (abs(K - R)).max() / abs(R).max() < TOL_K
+
+
+def test_assembly_is_bit_identical_run_to_run():
+    d = decks.box_hex20_lognormal(12, 12, 6, seed=3)
+    s = system(d)
+    s.assemble()
+    a = s.lower_csr().data.copy()
+    s.assemble()
+    b = s.lower_csr().data.copy()
+    assert a.tobytes() == b.tobytes()
+
+
+@pytest.mark.parametrize("name", SOLVABLE)
+@pytest.mark.parametrize("precision", [gpu.PREC_FP64, gpu.PREC_MIXED])
+def test_displacements_match_reference(name, precision):
+    d, g = gio.load(name)
+    s = system(d)
+    s.assemble()
+    u, rep = s.solve(g["ref_f"], tol=1e-13, precision=precision)
+    assert rep["converged"]
+    assert gio.rel(u, g["ref_u"]) < TOL_U, rep
+
+
+def test_fp64_iterations_match_oracle_pcg():
+    d, g = gio.load("cfg_hex20_lognormal_8x8x4")
+    s = system(d)
+    s.assemble()
+    K = fo.assemble(d)
+    f = g["ref_f"]
+    for tol in (1e-6, 1e-10):
+        u_o, ok, it_o, err_o = fo.pcg(K, f, tol, 100000)
+        u, rep = s.solve(f, tol=tol, precision=gpu.PREC_FP64, precond=gpu.PRECOND_JACOBI)
+        assert ok and rep["converged"]
+        assert abs(rep["iterations"] - it_o) <= 2, (rep, it_o)
+        assert gio.rel(u, u_o) < 1e-6
+
+
+def test_solve_is_bit_identical_run_to_run():
+    d = decks.box_hex20_lognormal(8, 8, 4, seed=1)
+    s = system(d)
+    s.assemble()
+    f = gpu.face_load_vector(d)
+    u1, _ = s.solve(f, tol=1e-10)
+    u2, _ = s.solve(f, tol=1e-10)
+    assert u1.tobytes() == u2.tobytes()
+
+
+def test_mult_vect_and_get_add():
+    d, g = gio.load("cfg_hex8_cantilever")
+    s = system(d)
+    s.assemble()
+    K = fo.assemble(d)
+    x = np.random.default_rng(0).standard_normal(d.num_eq())
+    assert gio.rel(s.mult_vect(x), K @ x) < 1e-12
+    assert abs(s.get(10, 10) - K[10, 10]) <= 1e-12 * abs(K[10, 10])
+    i, j = 10, int(K[10].indices[0])
+    before = s.get(i, j)
+    s.add(i, j, 2.5)
+    assert abs(s.get(i, j) - (before + 2.5)) < 1e-12 * max(1.0, abs(before))
+    assert abs(s.get(j, i) - (before + 2.5)) < 1e-12 * max(1.0, abs(before))
+
+
+def test_mass_matrices_match_reference():
+    d, g = gio.load("cfg_hex8_mass")
+    s = system(d)
+    for k, e in enumerate(g["ref_elems"]):
+        M = s.element_matrices(int(e), 1, what=gpu.ASM_M)[0]
+        assert gio.rel(M, g["ref_elm_M"][k]) < TOL_K
+    s.assemble_mass()
+    Ml = s.lower_csr(gpu.ASM_M)
+    Me = np.stack([fo.elem_mass(8, d.ngp, d.coords[d.conn[e]], d.rho[e])[0] for e in range(d.num_elems)])
+    R = sp.tril(fo.assemble(d, Me)).tocsr()
+    assert abs(Ml - R).max() / abs(R).max() < TOL_K
+
+
+@pytest.mark.parametrize("precond", [gpu.PRECOND_JACOBI, gpu.PRECOND_BLOCK_JACOBI])
+def test_medium_hex20_against_oracle(precond):
+    d = decks.box_hex20_lognormal(16, 16, 8, seed=2)
+    s = system(d)
+    s.assemble()
+    K = fo.assemble(d)
+    Kl = s.lower_csr()
+    R = sp.tril(K).tocsr()
+    assert abs(Kl - R).max() / abs(R).max() < TOL_K
+    f = gpu.face_load_vector(d)
+    u_o, ok, it, err = fo.pcg(K, f, 1e-12, 100000)
+    assert ok
+    for prec in (gpu.PREC_FP64, gpu.PREC_MIXED):
+        u, rep = s.solve(f, tol=1e-12, precision=prec, precond=precond)
+        assert rep["converged"] and rep["true_rel_residual"] < 1e-10
+        assert gio.rel(u, u_o) < TOL_U, (prec, rep)
+
+
+def test_nonpositive_jacobian_is_reported():
+    d = decks.cantilever_hex8(2, 1, 1)
+    d.conn = d.conn[:, [4, 5, 6, 7, 0, 1, 2, 3]].copy()   # mirrored element: detJ < 0
+    s = system(d)
+    with pytest.raises(gpu.FastGpuError) as ei:
+        s.assemble()
+    assert ei.value.rc == -6
+
+
+def test_nonconvergence_is_reported():
+    d = decks.box_hex20_lognormal(6, 6, 3, seed=4)
+    s = system(d)
+    s.assemble()
+    f = gpu.face_load_vector(d)
+    with pytest.raises(gpu.FastGpuError) as ei:
+        s.solve(f, tol=1e-12, maxit=5)
+    assert ei.value.rc == -5
