@@ -50,20 +50,19 @@ struct ElemArgs {
   int32_t *status;            // bit 0: non-positive Jacobian determinant
 };
 
-template <int NN, int NG>
+template <int NN, int NG, bool MASS>
 struct ElemSmem {
   static constexpr int ND = 3 * NN;
   static constexpr int LDH = ND + 1;
-  static constexpr int kDN = NG * NN * 3;
-  static constexpr int kW = NG;
-  static constexpr int kN = NG * NN;
+  static constexpr int kN = MASS ? NG * NN : 0;   // shape functions (mass only)
   static constexpr int kX = NN * 3;
   static constexpr int kJ = NG * 9;
   static constexpr int kC = NG;
-  static constexpr int kD = NG * ND;
-  static constexpr int kH = ND * LDH;
+  static constexpr int kD = MASS ? 0 : NG * ND;
+  static constexpr int kH = MASS ? 0 : ND * LDH;
   // doubles; J is aliased into H (J is dead before H is written)
-  static constexpr int total = kDN + kW + kN + kX + kC + kD + (kH > kJ ? kH : kJ);
+  static constexpr int kHJ = kH > kJ ? kH : kJ;
+  static constexpr int total = kN + kX + kC + kD + kHJ;
   static constexpr size_t bytes = total * sizeof(double) + 2 * 256 + 64;
 };
 
@@ -76,26 +75,25 @@ __device__ __forceinline__ void pair_of(int p, int n, int &a, int &b) {
 }
 
 template <int NN, int NG, int NT, bool MASS>
-__global__ void __launch_bounds__(NT) elem_kernel(ElemArgs A) {
-  using S = ElemSmem<NN, NG>;
+__global__ void __launch_bounds__(NT, (NT >= 256 ? 4 : 8)) elem_kernel(ElemArgs A) {
+  using S = ElemSmem<NN, NG, MASS>;
   constexpr int ND = S::ND, LDH = S::LDH;
   extern __shared__ __align__(16) double sm[];
-  double *sdN = sm;
-  double *sw = sdN + S::kDN;
-  double *sN = sw + S::kW;
+  double *sN = sm;
   double *sX = sN + S::kN;
   double *sc = sX + S::kX;
   double *sD = sc + S::kC;
   double *sH = sD + S::kD;
   double *sJ = sH;  // aliased
-  uint8_t *sfix = reinterpret_cast<uint8_t *>(sH + (S::kH > S::kJ ? S::kH : S::kJ));
+  uint8_t *sfix = reinterpret_cast<uint8_t *>(sH + S::kHJ);
   uint8_t *spa = sfix + 64;
   uint8_t *spb = spa + 256;
   constexpr int NP = NN * (NN + 1) / 2;
+  // Gauss-point tables are read through the L1 cache (read-only, shared by all blocks)
+  const double *__restrict__ sdN = A.dN;
+  const double *__restrict__ sw = A.w;
 
   const int tid = threadIdx.x;
-  for (int i = tid; i < S::kDN; i += NT) sdN[i] = A.dN[i];
-  for (int i = tid; i < NG; i += NT) sw[i] = A.w[i];
   if (MASS)
     for (int i = tid; i < S::kN; i += NT) sN[i] = A.N[i];
   for (int p = tid; p < NP; p += NT) {
@@ -186,12 +184,11 @@ __global__ void __launch_bounds__(NT) elem_kernel(ElemArgs A) {
     }
     __syncthreads();
 
-    // H = sum_g c_g D_g D_g^T, 4x4 register tiles over the upper triangle
+    // H = sum_g c_g D_g D_g^T in 4x4 register tiles (all T*T tiles: no
+    // triangular bookkeeping; the FP64 pipe has room for the symmetric half)
     constexpr int T = ND / 4;
-    constexpr int NTILE = T * (T + 1) / 2;
-    for (int tile = tid; tile < NTILE; tile += NT) {
-      int ti, tj;
-      pair_of(tile, T, ti, tj);
+    for (int tile = tid; tile < T * T; tile += NT) {
+      const int ti = tile / T, tj = tile - T * ti;
       double acc[4][4];
 #pragma unroll
       for (int r = 0; r < 4; r++)
@@ -213,40 +210,65 @@ __global__ void __launch_bounds__(NT) elem_kernel(ElemArgs A) {
 #pragma unroll
       for (int r = 0; r < 4; r++)
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-          sH[(4 * ti + r) * LDH + 4 * tj + q] = acc[r][q];
-          sH[(4 * tj + q) * LDH + 4 * ti + r] = acc[r][q];
-        }
+        for (int q = 0; q < 4; q++) sH[(4 * ti + r) * LDH + 4 * tj + q] = acc[r][q];
     }
     __syncthreads();
 
-    // element matrix blocks and scatter
+    // element matrix blocks and scatter: one thread per node pair (a <= b).
+    // The 9 values of block (a,b) and of its transpose (b,a) are loaded before
+    // any store, so a thread keeps 18 independent loads in flight.
     const double E = A.E[e], nu = A.nu[e];
     const double dd = (1.0 + nu) * (1.0 - 2.0 * nu);
     const double C00 = E * (1.0 - nu) / dd, C01 = E * nu / dd, G = 0.5 * E / (1.0 + nu);
-    double *__restrict__ Kg = A.K;
-    for (int t = tid; t < NP * 9; t += NT) {
-      const int p = t / 9, ij = t - 9 * p, i = ij / 3, j = ij - 3 * i;
+    for (int p = tid; p < NP; p += NT) {
       const int a = spa[p], b = spb[p];
-      double v;
-      if (i == j) {
-        const double hs = sH[a * LDH + b] + sH[(NN + a) * LDH + NN + b] + sH[(2 * NN + a) * LDH + 2 * NN + b];
-        const double hii = sH[(i * NN + a) * LDH + i * NN + b];
-        v = C00 * hii + G * (hs - hii);
-      } else {
-        v = C01 * sH[(i * NN + a) * LDH + j * NN + b] + G * sH[(j * NN + a) * LDH + i * NN + b];
-      }
+      double v[9];
+      const double hs = sH[a * LDH + b] + sH[(NN + a) * LDH + NN + b] + sH[(2 * NN + a) * LDH + 2 * NN + b];
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+          if (i == j) {
+            const double hii = sH[(i * NN + a) * LDH + i * NN + b];
+            v[3 * i + j] = C00 * hii + G * (hs - hii);
+          } else {
+            v[3 * i + j] = C01 * sH[(i * NN + a) * LDH + j * NN + b] + G * sH[(j * NN + a) * LDH + i * NN + b];
+          }
+        }
       if (A.Ke_out) {
         double *Ko = A.Ke_out + it * ND * ND;
-        Ko[(3 * a + i) * ND + 3 * b + j] = v;
-        Ko[(3 * b + j) * ND + 3 * a + i] = v;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+          for (int j = 0; j < 3; j++) {
+            Ko[(3 * a + i) * ND + 3 * b + j] = v[3 * i + j];
+            Ko[(3 * b + j) * ND + 3 * a + i] = v[3 * i + j];
+          }
       }
-      if (Kg && !((sfix[a] >> i) & 1) && !((sfix[b] >> j) & 1)) {
-        const int32_t sab = A.slot[(e * NN + a) * NN + b];
-        Kg[(int64_t)sab * 9 + 3 * i + j] += v;
+      if (A.K) {
+        const uint8_t fa = sfix[a], fb = sfix[b];
+        double *Kab = A.K + (int64_t)A.slot[(e * NN + a) * NN + b] * 9;
+        double oab[9], oba[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) oab[k] = Kab[k];
         if (a != b) {
-          const int32_t sba = A.slot[(e * NN + b) * NN + a];
-          Kg[(int64_t)sba * 9 + 3 * j + i] += v;
+          double *Kba = A.K + (int64_t)A.slot[(e * NN + b) * NN + a] * 9;
+#pragma unroll
+          for (int k = 0; k < 9; k++) oba[k] = Kba[k];
+#pragma unroll
+          for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++)
+              if (!((fa >> i) & 1) && !((fb >> j) & 1)) {
+                Kab[3 * i + j] = oab[3 * i + j] + v[3 * i + j];
+                Kba[3 * j + i] = oba[3 * j + i] + v[3 * i + j];
+              }
+        } else {
+#pragma unroll
+          for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++)
+              if (!((fa >> i) & 1) && !((fb >> j) & 1)) Kab[3 * i + j] = oab[3 * i + j] + v[3 * i + j];
         }
       }
     }
@@ -256,7 +278,7 @@ __global__ void __launch_bounds__(NT) elem_kernel(ElemArgs A) {
 template <int NN, int NG, int NT, bool MASS>
 static cudaError_t run(Ctx &c, ElemArgs a, int64_t count) {
   if (count <= 0) return cudaSuccess;
-  using S = ElemSmem<NN, NG>;
+  using S = ElemSmem<NN, NG, MASS>;
   auto kern = elem_kernel<NN, NG, NT, MASS>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
   if (e != cudaSuccess) return e;
@@ -284,9 +306,9 @@ static cudaError_t dispatch(Ctx &c, const Bucket &B, ElemArgs a, int64_t count) 
     }
   } else if (B.type == FAST_ELEM_HEX20) {
     switch (ng) {
-      case 8: return run<20, 8, 128, MASS>(c, a, count);
-      case 27: return run<20, 27, 128, MASS>(c, a, count);
-      case 64: return run<20, 64, 128, MASS>(c, a, count);
+      case 8: return run<20, 8, 256, MASS>(c, a, count);
+      case 27: return run<20, 27, 256, MASS>(c, a, count);
+      case 64: return run<20, 64, 256, MASS>(c, a, count);
       default: break;
     }
   }
@@ -355,17 +377,6 @@ cudaError_t launch_element_matrices(Ctx &c, int what, int bucket, int64_t first_
   a.Ke_out = d_out_and_index;
   a.index = reinterpret_cast<const int32_t *>(d_out_and_index + (size_t)count * nd * nd);
   return (what == FAST_ASM_MASS) ? dispatch<true>(c, B, a, count) : dispatch<false>(c, B, a, count);
-}
-
-__global__ void to_fp32_kernel(const double *__restrict__ s, float *__restrict__ d, int64_t n) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    d[i] = (float)s[i];
-}
-
-cudaError_t launch_to_fp32(Ctx &c, const double *src, float *dst, int64_t n) {
-  to_fp32_kernel<<<c.sm_count * 8, 256, 0, c.stream>>>(src, dst, n);
-  c.launches++;
-  return cudaGetLastError();
 }
 
 }  // namespace fastgpu

@@ -45,13 +45,13 @@ void free_mesh(Ctx &c) {
   c.buckets.clear();
   dfree(c.d_X); dfree(c.d_fix); dfree(c.d_dof_of_eq);
   dfree(c.d_rowptr); dfree(c.d_col); dfree(c.d_diag);
-  dfree(c.d_K); dfree(c.d_M); dfree(c.d_K32);
+  dfree(c.d_K); dfree(c.d_M); dfree(c.d_Ks); dfree(c.d_Ms); dfree(c.d_Ks32);
   dfree(c.d_u); dfree(c.d_r); dfree(c.d_z); dfree(c.d_p); dfree(c.d_w); dfree(c.d_f); dfree(c.d_dinv);
-  dfree(c.s_u); dfree(c.s_r); dfree(c.s_z); dfree(c.s_p); dfree(c.s_w); dfree(c.s_dinv);
+  dfree(c.s_x); dfree(c.s_r); dfree(c.s_z); dfree(c.s_p); dfree(c.s_w); dfree(c.s_dinv);
   dfree(c.d_eq_tmp);
   if (c.h_eq_tmp) cudaFreeHost(c.h_eq_tmp);
   c.h_eq_tmp = nullptr;
-  c.K_ok = c.M_ok = c.K32_ok = false;
+  c.K_ok = c.M_ok = c.Ks_ok = c.Ms_ok = false;
   c.precond_built = -1;
   c.nnode = 0;
   c.neq = 0;
@@ -64,6 +64,29 @@ double *target_of(Ctx &c, int what) {
   if (what == FAST_ASM_STIFFNESS) return c.d_K;
   if (what == FAST_ASM_MASS) return c.d_M;
   return nullptr;
+}
+
+void invalidate(Ctx &c, int what) {
+  if (what == FAST_ASM_STIFFNESS) { c.Ks_ok = false; c.precond_built = -1; }
+  else c.Ms_ok = false;
+}
+
+// row-local SoA copies for the solve (FP64, and FP32 when asked)
+cudaError_t ensure_soa(Ctx &c, int what, bool fp32) {
+  cudaError_t e = cudaSuccess;
+  if (what == FAST_ASM_MASS) {
+    if (!c.d_Ms && (e = cudaMalloc((void **)&c.d_Ms, sizeof(double) * 9 * c.nnzb)) != cudaSuccess) return e;
+    if (!c.Ms_ok) { e = launch_to_soa(c, c.d_M, c.d_Ms, nullptr); c.Ms_ok = (e == cudaSuccess); }
+    return e;
+  }
+  if (!c.d_Ks && (e = cudaMalloc((void **)&c.d_Ks, sizeof(double) * 9 * c.nnzb)) != cudaSuccess) return e;
+  if (fp32 && !c.d_Ks32 && (e = cudaMalloc((void **)&c.d_Ks32, sizeof(float) * 9 * c.nnzb)) != cudaSuccess) return e;
+  if (!c.Ks_ok) {
+    // the FP32 copy is always refreshed with the FP64 one once it exists
+    e = launch_to_soa(c, c.d_K, c.d_Ks, c.d_Ks32);
+    c.Ks_ok = (e == cudaSuccess);
+  }
+  return e;
 }
 
 // (eq i, eq j) 0-based -> flat value index in the block matrix, or -1
@@ -191,7 +214,11 @@ int fast_gpu_upload_mesh(fast_gpu_ctx *c, const fast_gpu_mesh *m) {
   CK(dalloc(&c->d_fix, nnode));
   CK(cudaMemcpy(c->d_fix, fix.data(), nnode, cudaMemcpyHostToDevice));
   CK(dalloc(&c->d_dof_of_eq, c->neq));
-  if (c->neq) CK(cudaMemcpy(c->d_dof_of_eq, c->h_dof_of_eq.data(), sizeof(int32_t) * c->neq, cudaMemcpyHostToDevice));
+  {
+    std::vector<int32_t> d4(c->neq);
+    for (int32_t k = 0; k < c->neq; k++) d4[k] = 4 * (c->h_dof_of_eq[k] / 3) + c->h_dof_of_eq[k] % 3;
+    if (c->neq) CK(cudaMemcpy(c->d_dof_of_eq, d4.data(), sizeof(int32_t) * c->neq, cudaMemcpyHostToDevice));
+  }
   CK(dalloc(&c->d_rowptr, nnode + 1));
   CK(cudaMemcpy(c->d_rowptr, c->h_rowptr.data(), sizeof(int32_t) * (nnode + 1), cudaMemcpyHostToDevice));
   CK(dalloc(&c->d_col, c->nnzb));
@@ -228,12 +255,14 @@ int fast_gpu_upload_mesh(fast_gpu_ctx *c, const fast_gpu_mesh *m) {
     CK(dalloc(&B.d_w, w.size()));
     CK(cudaMemcpy(B.d_w, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice));
   }
-  const int64_t n3 = 3 * nnode;
+  const int64_t n4 = 4 * nnode;
   CK(dalloc(&c->d_K, 9 * c->nnzb));
-  CK(dalloc(&c->d_u, n3)); CK(dalloc(&c->d_r, n3)); CK(dalloc(&c->d_z, n3)); CK(dalloc(&c->d_p, n3));
-  CK(dalloc(&c->d_w, n3)); CK(dalloc(&c->d_f, n3)); CK(dalloc(&c->d_dinv, 9 * nnode));
-  CK(dalloc(&c->s_u, n3)); CK(dalloc(&c->s_r, n3)); CK(dalloc(&c->s_z, n3)); CK(dalloc(&c->s_p, n3));
-  CK(dalloc(&c->s_w, n3)); CK(dalloc(&c->s_dinv, 9 * nnode));
+  CK(dalloc(&c->d_u, n4)); CK(dalloc(&c->d_r, n4)); CK(dalloc(&c->d_z, n4)); CK(dalloc(&c->d_p, n4));
+  CK(dalloc(&c->d_w, n4)); CK(dalloc(&c->d_f, n4)); CK(dalloc(&c->d_dinv, 12 * nnode));
+  CK(dalloc(&c->s_x, n4)); CK(dalloc(&c->s_r, n4)); CK(dalloc(&c->s_z, n4)); CK(dalloc(&c->s_p, n4));
+  CK(dalloc(&c->s_w, n4)); CK(dalloc(&c->s_dinv, 12 * nnode));
+  CK(cudaMemset(c->d_p, 0, sizeof(double) * n4));
+  CK(cudaMemset(c->s_p, 0, sizeof(float) * n4));
   CK(dalloc(&c->d_eq_tmp, std::max<int64_t>(2 * (int64_t)c->neq, 1)));
   CK(cudaMallocHost((void **)&c->h_eq_tmp, sizeof(double) * std::max<int64_t>(2 * (int64_t)c->neq, 1)));
   return FAST_GPU_OK;
@@ -251,7 +280,9 @@ int fast_gpu_pattern_info(fast_gpu_ctx *c, int64_t *nnzb, int64_t *nnz_lower, in
 int fast_gpu_update_coords(fast_gpu_ctx *c, const double *coords) {
   if (check_ctx(c) || !coords || !c->d_X) return FAST_GPU_EINVAL;
   CK(cudaMemcpyAsync(c->d_X, coords, sizeof(double) * 3 * c->nnode, cudaMemcpyHostToDevice, c->stream));
-  c->K_ok = c->M_ok = c->K32_ok = false;
+  c->K_ok = c->M_ok = false;
+  invalidate(*c, FAST_ASM_STIFFNESS);
+  invalidate(*c, FAST_ASM_MASS);
   return FAST_GPU_OK;
 }
 
@@ -285,7 +316,9 @@ int fast_gpu_update_material(fast_gpu_ctx *c, int32_t b, const double *E, const 
     }
     CK(cudaStreamSynchronize(c->stream));
   }
-  c->K_ok = c->M_ok = c->K32_ok = false;
+  c->K_ok = c->M_ok = false;
+  invalidate(*c, FAST_ASM_STIFFNESS);
+  invalidate(*c, FAST_ASM_MASS);
   return FAST_GPU_OK;
 }
 
@@ -295,8 +328,8 @@ int fast_gpu_zero(fast_gpu_ctx *c, int32_t what) {
   double *T = target_of(*c, what);
   if (!T) return FAST_GPU_EINVAL;
   CK(launch_zero_matrix(*c, T, what == FAST_ASM_STIFFNESS));
-  if (what == FAST_ASM_STIFFNESS) { c->K_ok = true; c->K32_ok = false; c->precond_built = -1; }
-  else c->M_ok = true;
+  if (what == FAST_ASM_STIFFNESS) c->K_ok = true; else c->M_ok = true;
+  invalidate(*c, what);
   return FAST_GPU_OK;
 }
 
@@ -306,12 +339,15 @@ int fast_gpu_assemble(fast_gpu_ctx *c, int32_t what) {
   if (what == FAST_ASM_MASS && !c->d_M) CK(dalloc(&c->d_M, 9 * c->nnzb));
   double *T = target_of(*c, what);
   CK(cudaMemsetAsync(c->d_status, 0, sizeof(int32_t), c->stream));
+  if (what == FAST_ASM_STIFFNESS) c->begin_span(2);
   CK(launch_zero_matrix(*c, T, what == FAST_ASM_STIFFNESS));
   CK(launch_assemble(*c, what, T));
+  if (what == FAST_ASM_STIFFNESS) c->end_span();
   CK(cudaMemcpyAsync(c->h_status, c->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  if (what == FAST_ASM_STIFFNESS) { c->K_ok = true; c->K32_ok = false; c->precond_built = -1; }
-  else c->M_ok = true;
+  c->harvest();
+  if (what == FAST_ASM_STIFFNESS) c->K_ok = true; else c->M_ok = true;
+  invalidate(*c, what);
   if (c->h_status[0] & 1) {
     c->err = "assemble: non-positive Jacobian determinant in at least one element";
     return FAST_GPU_EDETJ;
@@ -338,7 +374,7 @@ int fast_gpu_add(fast_gpu_ctx *c, int32_t what, int32_t i, int32_t j, double v) 
     CK(cudaMemcpyAsync(T + k2, &b, sizeof(double), cudaMemcpyHostToDevice, c->stream));
   }
   CK(cudaStreamSynchronize(c->stream));
-  if (what == FAST_ASM_STIFFNESS) { c->K32_ok = false; c->precond_built = -1; }
+  invalidate(*c, what);
   return FAST_GPU_OK;
 }
 
@@ -361,8 +397,9 @@ int fast_gpu_mult_vect(fast_gpu_ctx *c, int32_t what, const double *x, double *y
   CK(cudaStreamSynchronize(c->stream));
   std::memcpy(c->h_eq_tmp, x, nb);
   CK(cudaMemcpyAsync(c->d_eq_tmp, c->h_eq_tmp, nb, cudaMemcpyHostToDevice, c->stream));
-  CK(launch_eq_to_node(*c, c->d_eq_tmp, c->d_p));
-  CK(launch_spmv(*c, T, c->d_p, c->d_w));
+  CK(ensure_soa(*c, what, false));
+  CK(launch_eq_to_node(*c, c->d_eq_tmp, c->d_z));
+  CK(launch_spmv(*c, what == FAST_ASM_MASS ? c->d_Ms : c->d_Ks, c->d_z, c->d_w));
   CK(launch_node_to_eq(*c, c->d_w, c->d_eq_tmp));
   CK(cudaMemcpyAsync(c->h_eq_tmp, c->d_eq_tmp, nb, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -373,83 +410,58 @@ int fast_gpu_mult_vect(fast_gpu_ctx *c, int32_t what, const double *x, double *y
 namespace {
 
 int solve_node_space(fast_gpu_ctx *c, const fast_gpu_solve_opts *o, bool warm, fast_gpu_solve_report *rep) {
-  // d_f holds the node-space load, d_u the initial / returned solution
+  // c->d_f holds the padded load, c->d_u the initial / returned solution
   fast_gpu_solve_opts opts{};
   if (o) opts = *o;
   const int maxit = opts.maxit > 0 ? opts.maxit : std::max(20 * c->neq, 100);
   const double tol = opts.tol > 0 ? opts.tol : 1e-5;
   const int precond = opts.precond;
   if (precond != FAST_PRECOND_JACOBI && precond != FAST_PRECOND_BLOCK_JACOBI) return FAST_GPU_EINVAL;
+  const bool mixed = opts.precision == FAST_PREC_MIXED;
+  if (!mixed && opts.precision != FAST_PREC_FP64) return FAST_GPU_EINVAL;
   if (c->precond_built != precond) CK(launch_build_precond(*c, c->d_K, precond));
+  CK(ensure_soa(*c, FAST_ASM_STIFFNESS, mixed));
+  const int chunk = opts.check_every > 0 ? opts.check_every : (mixed ? 50 : 32);
   fast_gpu_solve_report R{};
-  const int64_t n3 = 3 * c->nnode;
-  if (opts.precision == FAST_PREC_FP64) {
-    int it = 0, done = 0;
-    double err = 0;
-    CK(pcg_solve_device(*c, false, c->d_f, c->d_u, warm, tol, maxit, opts.check_every, precond, &it, &err, &done));
-    R.iterations = it;
-    R.outer = 1;
-    R.rel_residual = err;
-    R.converged = (done == 1);
-  } else if (opts.precision == FAST_PREC_MIXED) {
-    if (!c->d_K32) CK(dalloc(&c->d_K32, 9 * c->nnzb));
-    if (!c->K32_ok) {
-      CK(launch_to_fp32(*c, c->d_K, c->d_K32, 9 * c->nnzb));
-      c->K32_ok = true;
+  if (mixed) {
+    CK(pcg_mixed(*c, warm, tol, maxit, chunk));
+    R.outer = c->h_state->updates;
+    const int done = c->h_state->done, it = c->h_state->iter;
+    if ((done == 3 || done == 4) && it < maxit) {
+      // FP32 iterates stopped making progress (ill-conditioned system): go on
+      // with the FP64 iteration from the current FP64 solution
+      R.escalated = 1;
+      CK(pcg_fp64(*c, true, tol, maxit, chunk, it));
     }
-    const double inner = opts.inner_tol > 0 ? opts.inner_tol : 1e-5;
-    const int max_outer = opts.max_outer > 0 ? opts.max_outer : 30;
-    double *d_rr = c->d_partials + 12288;
-    double *d_ff = c->d_partials + 12289;
-    CK(launch_norm2(*c, c->d_f, n3, d_ff));
-    double hff = 0;
-    CK(cudaMemcpyAsync(&hff, d_ff, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    double lenf = std::sqrt(hff);
-    if (lenf > 10e+10) lenf = 1.0;
-    if (!warm) CK(cudaMemsetAsync(c->d_u, 0, sizeof(double) * n3, c->stream));
-    int total = 0;
-    for (int k = 0; k < max_outer; k++) {
-      // FP64 residual r = f - K u
-      CK(launch_residual(*c, c->d_K, c->d_f, c->d_u, c->d_r, d_rr));
-      double hrr = 0;
-      CK(cudaMemcpyAsync(&hrr, d_rr, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-      CK(cudaStreamSynchronize(c->stream));
-      const double rn = std::sqrt(hrr);
-      R.rel_residual = (lenf > 0) ? rn / lenf : 0.0;
-      if (lenf < tol || R.rel_residual < tol) { R.converged = 1; break; }
-      if (!std::isfinite(rn) || total >= maxit) break;
-      R.outer = k + 1;
-      // FP32 inner solve K32 d = r / |r| (scaled so the FP32 right-hand side has unit norm)
-      double *d_rs = c->d_w;
-      double *d_d = c->d_z;
-      CK(cudaMemcpyAsync(d_rs, c->d_r, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->stream));
-      CK(scale_inplace(*c, d_rs, n3, 1.0 / rn));
-      int it = 0, done = 0;
-      double err = 0;
-      CK(pcg_solve_device(*c, true, d_rs, d_d, false, inner, std::max(1, maxit - total), opts.check_every,
-                          precond, &it, &err, &done));
-      total += it;
-      if (done == 3 || it == 0) break;
-      // FP64 refinement update u += |r| d
-      CK(axpy_inplace(*c, c->d_u, d_d, n3, rn));
-    }
-    R.iterations = total;
   } else {
-    return FAST_GPU_EINVAL;
+    CK(pcg_fp64(*c, warm, tol, maxit, chunk));
+    R.outer = 1;
   }
-  // true FP64 residual
+  c->harvest();
+  const PcgState &st = *c->h_state;
+  R.iterations = st.iter;
+  R.rel_residual = (mixed && !R.escalated) ? st.err_true : st.err;
+  R.converged = (st.done == 1);
+  // true FP64 residual |f - K u| / |f|
   {
     double *d_rr = c->d_partials + 12290;
     double *d_ff = c->d_partials + 12291;
-    CK(launch_residual(*c, c->d_K, c->d_f, c->d_u, c->d_r, d_rr));
-    CK(launch_norm2(*c, c->d_f, n3, d_ff));
+    CK(launch_residual(*c, c->d_Ks, c->d_f, c->d_u, c->d_r, d_rr));
+    CK(launch_norm2(*c, c->d_f, 4 * c->nnode, d_ff));
     double h[2] = {0, 0};
     CK(cudaMemcpyAsync(h, d_rr, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     R.true_rel_residual = h[1] > 0 ? std::sqrt(h[0] / h[1]) : 0.0;
   }
   if (rep) *rep = R;
+  if (st.done == 3) {
+    c->err = "solve: breakdown (non-positive or non-finite p.Kp or residual)";
+    return FAST_GPU_ENONCONV;
+  }
+  if (st.done == 4) {
+    c->err = "solve: FP64 residual stagnated above the tolerance (attainable accuracy reached)";
+    return FAST_GPU_ENONCONV;
+  }
   if (!R.converged) {
     c->err = "solve: no convergence within the iteration cap";
     return FAST_GPU_ENONCONV;
@@ -587,57 +599,38 @@ int fast_gpu_launch_count(fast_gpu_ctx *c, int64_t *n) {
   return FAST_GPU_OK;
 }
 
-int fast_gpu_time_kernel(fast_gpu_ctx *c, int32_t which, int32_t reps, double *avg_ms, double *bytes) {
-  if (check_ctx(c) || reps < 1 || !avg_ms) return FAST_GPU_EINVAL;
-  if (!c->K_ok) { c->err = "time_kernel: matrix not assembled"; return FAST_GPU_ESTATE; }
-  const int64_t n3 = 3 * c->nnode;
-  double algo = 0.0;
-  if (which == FAST_KERNEL_SPMV_FP32 && !c->K32_ok) {
-    if (!c->d_K32) CK(dalloc(&c->d_K32, 9 * c->nnzb));
-    CK(launch_to_fp32(*c, c->d_K, c->d_K32, 9 * c->nnzb));
-    c->K32_ok = true;
-  }
-  auto run = [&]() -> cudaError_t {
-    if (which == FAST_KERNEL_SPMV_FP64) return launch_spmv(*c, c->d_K, c->d_p, c->d_w);
-    if (which == FAST_KERNEL_SPMV_FP32) return launch_spmv32(*c, c->d_K32, c->s_p, c->s_w);
+int fast_gpu_kernel_timing(fast_gpu_ctx *c, int32_t enable) {
+  if (check_ctx(c)) return FAST_GPU_EINVAL;
+  CK(cudaStreamSynchronize(c->stream));
+  c->harvest();
+  c->timing = enable != 0;
+  for (int k = 0; k < 3; k++) { c->kt_ms[k] = 0; c->kt_n[k] = 0; }
+  return FAST_GPU_OK;
+}
+
+int fast_gpu_kernel_stats(fast_gpu_ctx *c, int32_t which, int64_t *launches, double *total_ms, double *bytes) {
+  if (check_ctx(c) || which < 0 || which > 2) return FAST_GPU_EINVAL;
+  CK(cudaStreamSynchronize(c->stream));
+  c->harvest();
+  if (launches) *launches = c->kt_n[which];
+  if (total_ms) *total_ms = c->kt_ms[which];
+  if (bytes) {
+    const double n4 = 4.0 * c->nnode;
+    double algo = 0.0;
+    // SpMV: block values + column indices + row pointers + x read once + y written once
+    if (which == FAST_KERNEL_SPMV_FP64) algo = (double)c->nnzb * (9 * 8 + 4) + 4.0 * (c->nnode + 1) + 2.0 * 8 * n4;
+    if (which == FAST_KERNEL_SPMV_FP32) algo = (double)c->nnzb * (9 * 4 + 4) + 4.0 * (c->nnode + 1) + 2.0 * 4 * n4;
     if (which == FAST_KERNEL_ASSEMBLE) {
-      cudaError_t e = launch_zero_matrix(*c, c->d_K, true);
-      return e == cudaSuccess ? launch_assemble(*c, FAST_ASM_STIFFNESS, c->d_K) : e;
+      // scatter model per element: incidence + coordinates + fixity + E, nu + slot map + 3x3 block
+      // read-modify-write, plus the zero fill of the block values
+      for (const Bucket &B : c->buckets) {
+        const double nn = B.nn;
+        algo += (double)B.ne * (nn * (4 + 24 + 1) + 16 + nn * nn * (4 + 2 * 72));
+      }
+      algo += 72.0 * c->nnzb;
     }
-    return cudaErrorInvalidValue;
-  };
-  if (which == FAST_KERNEL_SPMV_FP64) {
-    algo = (double)c->nnzb * (9 * 8 + 4) + 4.0 * (c->nnode + 1) + 2.0 * 8 * n3;
-  } else if (which == FAST_KERNEL_SPMV_FP32) {
-    algo = (double)c->nnzb * (9 * 4 + 4) + 4.0 * (c->nnode + 1) + 2.0 * 4 * n3;
-  } else if (which == FAST_KERNEL_ASSEMBLE) {
-    // scatter model per element: incidence + coordinates + fixity + E, nu + slot map + 3x3 block RMW,
-    // plus the zero fill of the block values
-    for (const Bucket &B : c->buckets) {
-      const double nn = B.nn;
-      algo += (double)B.ne * (nn * (4 + 24 + 1) + 16 + nn * nn * (4 + 2 * 72));
-    }
-    algo += 72.0 * c->nnzb;
-  } else {
-    return FAST_GPU_EINVAL;
+    *bytes = algo;
   }
-  CK(cudaMemsetAsync(c->d_p, 0, sizeof(double) * n3, c->stream));
-  CK(cudaMemsetAsync(c->s_p, 0, sizeof(float) * n3, c->stream));
-  CK(run());
-  cudaEvent_t e0, e1;
-  CK(cudaEventCreate(&e0));
-  CK(cudaEventCreate(&e1));
-  CK(cudaEventRecord(e0, c->stream));
-  for (int r = 0; r < reps; r++) CK(run());
-  CK(cudaEventRecord(e1, c->stream));
-  CK(cudaEventSynchronize(e1));
-  float ms = 0;
-  CK(cudaEventElapsedTime(&ms, e0, e1));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  *avg_ms = ms / reps;
-  if (bytes) *bytes = algo;
-  if (which == FAST_KERNEL_ASSEMBLE) { c->K32_ok = false; c->precond_built = -1; }
   return FAST_GPU_OK;
 }
 

@@ -27,9 +27,15 @@ struct PcgState {
   double err;     // sqrt(rr) / lenf
   double tol;
   double pw;      // p.w of the last iteration
+  double err_true;  // |f - K u| / |f| at the last FP64 residual (mixed path)
+  double best_err;  // smallest err_true so far (mixed path stagnation guard)
   int32_t iter;   // iterations completed
-  int32_t done;   // 0 running, 1 converged, 2 iteration cap, 3 breakdown
+  int32_t done;   // 0 running, 1 converged, 2 iteration cap, 3 breakdown, 4 stagnation
   int32_t maxit;
+  int32_t updates;  // FP64 residual replacements (mixed path)
+  int32_t null_rhs; // |f| < tol: the solution is u = 0 (PCGSolver returns at once)
+  int32_t stall;    // FP64 residual replacements without a 2x improvement
+  int32_t final;    // converged on the FP64 residual: later launches do nothing
   int32_t pad;
 };
 
@@ -64,10 +70,10 @@ struct Ctx {
   int64_t nnode = 0;
   int32_t neq = 0;
   std::vector<int32_t> h_eq;      // [nnode*3] 1-based, 0 fixed
-  std::vector<int32_t> h_dof_of_eq;  // [neq] node-DOF index 3*n+i of equation k+1
+  std::vector<int32_t> h_dof_of_eq;  // [neq] node-DOF index 3*n+i of equation k+1 (unpadded)
   double *d_X = nullptr;          // [nnode][3]
   uint8_t *d_fix = nullptr;       // [nnode] bit i set: DOF i has no equation
-  int32_t *d_dof_of_eq = nullptr; // [neq]
+  int32_t *d_dof_of_eq = nullptr; // [neq] padded vector index 4*n+i of equation k+1
   std::vector<Bucket> buckets;
 
   // node-block (3x3) CSR pattern, full (both triangles)
@@ -78,18 +84,20 @@ struct Ctx {
   double pattern_seconds = 0.0;
   int64_t nnz_lower_eq = 0;
 
-  // assembled matrices: [nnzb][3][3]
+  // assembled matrices: [nnzb][3][3] blocks (assembly target, AoS)
   double *d_K = nullptr, *d_M = nullptr;
-  float *d_K32 = nullptr;
-  bool K_ok = false, M_ok = false, K32_ok = false;
+  // solve copies in row-local SoA layout (FP64 and FP32), rebuilt after each assembly
+  double *d_Ks = nullptr, *d_Ms = nullptr;
+  float *d_Ks32 = nullptr;
+  bool K_ok = false, M_ok = false, Ks_ok = false, Ms_ok = false;
   int32_t *d_status = nullptr;    // device error flags (detJ)
   int32_t *h_status = nullptr;    // pinned
 
-  // solver workspace in node-DOF space (3*nnode)
+  // solver workspace: node vectors padded to 4 entries (x, y, z, 0) per node
   double *d_u = nullptr, *d_r = nullptr, *d_z = nullptr, *d_p = nullptr, *d_w = nullptr, *d_f = nullptr;
-  double *d_dinv = nullptr;       // [nnode][9] inverse diagonal (Jacobi) or inverse 3x3 block
-  float *s_u = nullptr, *s_r = nullptr, *s_z = nullptr, *s_p = nullptr, *s_w = nullptr;
-  float *s_dinv = nullptr;        // [nnode][9]
+  double *d_dinv = nullptr;       // [nnode][3][4] inverse diagonal (Jacobi) or inverse 3x3 block
+  float *s_x = nullptr, *s_r = nullptr, *s_z = nullptr, *s_p = nullptr, *s_w = nullptr;
+  float *s_dinv = nullptr;        // [nnode][3][4]
   int precond_built = -1;         // which preconditioner d_dinv holds
   double *d_partials = nullptr;   // reduction partials [2][kRedBlocks]
   PcgState *d_state = nullptr;
@@ -98,6 +106,19 @@ struct Ctx {
   double *h_eq_tmp = nullptr;     // pinned [neq]
 
   int64_t launches = 0;          // kernels launched by this context (all entry points)
+
+  // live kernel timing: CUDA events around SpMV launches and assemblies
+  // (kind 0 FP64 SpMV, 1 FP32 SpMV, 2 assembly), harvested at each host sync
+  bool timing = false;
+  std::vector<cudaEvent_t> ev_pool;
+  struct Span { int kind; cudaEvent_t a, b; };
+  std::vector<Span> spans;
+  double kt_ms[3] = {0, 0, 0};
+  int64_t kt_n[3] = {0, 0, 0};
+  cudaEvent_t take_event();
+  void begin_span(int kind);
+  void end_span();
+  void harvest();
 
   bool set_error(const std::string &m) { err = m; return false; }
 };
@@ -116,22 +137,20 @@ cudaError_t launch_zero_matrix(Ctx &c, double *K, bool identity_on_fixed);
 cudaError_t launch_assemble(Ctx &c, int what, double *target);
 cudaError_t launch_element_matrices(Ctx &c, int what, int bucket, int64_t first_sorted, int64_t count,
                                     double *d_out);
-cudaError_t launch_to_fp32(Ctx &c, const double *src, float *dst, int64_t n);
 
 constexpr int kRedBlocks = 592;   // fixed reduction grid: 4 x 148 SMs
 cudaError_t launch_build_precond(Ctx &c, const double *K, int precond);
-// FP64 / FP32 PCG building blocks (node-DOF space vectors)
-cudaError_t pcg_solve_device(Ctx &c, bool fp32, const double *d_rhs_node, double *d_x_node, bool warm,
-                             double tol, int maxit, int check_every, int precond, int *iters,
-                             double *err, int *done);
-cudaError_t launch_residual(Ctx &c, const double *K, const double *f, const double *u, double *r,
+// AoS blocks -> row-local SoA copies (either output may be null)
+cudaError_t launch_to_soa(Ctx &c, const double *K, double *Ks, float *Ks32);
+// PCG on the padded node vectors c.d_f -> c.d_u; state left in c.h_state
+cudaError_t pcg_fp64(Ctx &c, bool warm, double tol, int maxit, int chunk, int iter0 = 0);
+cudaError_t pcg_mixed(Ctx &c, bool warm, double tol, int maxit, int chunk);
+cudaError_t launch_residual(Ctx &c, const double *Ks, const double *f, const double *u, double *r,
                             double *rr_out_dev);
-cudaError_t launch_spmv(Ctx &c, const double *K, const double *x, double *y);
-cudaError_t launch_spmv32(Ctx &c, const float *K, const float *x, float *y);
+cudaError_t launch_spmv(Ctx &c, const double *Ks, const double *x, double *y);
+cudaError_t launch_spmv32(Ctx &c, const float *Ks, const float *x, float *y);
 cudaError_t launch_eq_to_node(Ctx &c, const double *eqv, double *nodev);
 cudaError_t launch_node_to_eq(Ctx &c, const double *nodev, double *eqv);
 cudaError_t launch_norm2(Ctx &c, const double *x, int64_t n, double *out_dev);
-cudaError_t scale_inplace(Ctx &c, double *x, int64_t n, double a);
-cudaError_t axpy_inplace(Ctx &c, double *y, const double *x, int64_t n, double a);
 
 }  // namespace fastgpu

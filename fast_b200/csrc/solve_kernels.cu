@@ -1,26 +1,33 @@
-// solve_kernels.cu - K.u solve on the node-block CSR matrix (sm_100a).
+// solve_kernels.cu - K.u solve on the node-block matrix (sm_100a).
 //
 // Replaces cSymSprsMatrix::MultVect (mlib/sysmat.cpp:942-963) and PCGSolver
-// (mlib/sysmat.cpp:1061-1125).  The iteration is the reference's Jacobi PCG:
+// (mlib/sysmat.cpp:1061-1125).  The FP64 path is the reference's Jacobi PCG:
 //
 //   r = f, z = D^-1 r, p = z, dot0 = z.r
 //   loop: w = K p; alpha = dot0 / p.w; u += alpha p; r -= alpha w; z = D^-1 r
 //         err = |r| / |f|  (|f| > 1e11 replaced by 1);  stop if err < tol
 //         dot1 = z.r; beta = dot1/dot0; dot0 = dot1; p = z + beta p
 //
-// Vectors live in node-DOF space (3 per node); DOFs without an equation
-// carry an identity row in K and a zero right-hand side, so they stay zero
-// and the iteration is the reference's on the free equations.
+// The mixed path runs the same iteration in FP32 (FP32 matrix, vectors and
+// products) and keeps FP64 only for the solution and the true residual: after
+// every chunk of iterations the FP32 correction is flushed into the FP64
+// solution, r = f - K u is recomputed with the FP64 matrix and replaces the
+// FP32 recurrence residual while the search direction is kept ("reliable
+// updates").  Convergence is decided on that FP64 residual.
+//
+// Layouts.  The assembly target is the node-block CSR with each 3x3 block
+// stored contiguously (AoS).  For the solve, each block-row is transposed
+// once per assembly into a row-local structure-of-arrays: entry k (0..8) of
+// block p of row n sits at 9*rowptr[n] + k*nb(n) + p.  One warp handles one
+// block-row, one lane one block, so each of the nine value loads is a
+// contiguous, fully coalesced warp access.  Vectors are padded to 4 entries
+// per node (x, y, z, 0) so a node's part of x is one 16-byte (FP32) or two
+// 16-byte (FP64) loads.
 //
 // Every scalar lives on the device (PcgState) and every reduction uses a
 // fixed grid and a fixed combination order, so the host never waits inside
 // an iteration and a solve is bit-reproducible.  Kernels check state->done
 // first, so iterations launched past convergence cost only their launch.
-//
-// SpMV: one warp per block-row; a row's 3x3 blocks are contiguous, so the
-// warp streams 9*nb values with consecutive lanes on consecutive addresses
-// (fully coalesced) and gathers x through L1/L2.  HBM-bound: bytes per call
-// = nnzb*(9*sizeof(VT) + 4) + 4*(nnode+1) + vector traffic.
 #include <cmath>
 #include <cstdint>
 
@@ -36,7 +43,7 @@ __device__ __forceinline__ double warp_sum(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
-__device__ __forceinline__ float warp_sumf(float v) {
+__device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
@@ -58,47 +65,95 @@ __device__ __forceinline__ double block_sum(double v, double *sbuf) {
   return t;
 }
 
-// y = K x  (MODE 0),  y = b - K x  (MODE 1).  Optional per-block partial of
-// x.y (MODE 0) or y.y (MODE 1).
-template <typename VT, typename XT, typename AT, int MODE>
+// padded node vectors
+template <typename T> struct V4;
+template <> struct V4<float> {
+  static __device__ __forceinline__ void load(const float *p, float &a, float &b, float &c) {
+    const float4 v = *reinterpret_cast<const float4 *>(p);
+    a = v.x; b = v.y; c = v.z;
+  }
+  static __device__ __forceinline__ void store(float *p, float a, float b, float c) {
+    *reinterpret_cast<float4 *>(p) = make_float4(a, b, c, 0.f);
+  }
+};
+template <> struct V4<double> {
+  static __device__ __forceinline__ void load(const double *p, double &a, double &b, double &c) {
+    const double2 v0 = *reinterpret_cast<const double2 *>(p);
+    a = v0.x; b = v0.y; c = p[2];
+  }
+  static __device__ __forceinline__ void store(double *p, double a, double b, double c) {
+    *reinterpret_cast<double2 *>(p) = make_double2(a, b);
+    *reinterpret_cast<double2 *>(p + 2) = make_double2(c, 0.0);
+  }
+};
+
+// AoS blocks -> row-local SoA, FP64 and FP32 copies
+__global__ void __launch_bounds__(256)
+aos_to_soa(int64_t nrows, const int32_t *__restrict__ rowptr, const double *__restrict__ K,
+           double *__restrict__ Ks, float *__restrict__ Ks32) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t row = warp; row < nrows; row += nwarps) {
+    const int32_t b0 = rowptr[row], nb = rowptr[row + 1] - b0;
+    const int64_t base = 9 * (int64_t)b0;
+    for (int p = lane; p < nb; p += 32) {
+      const double *src = K + base + 9 * p;
+#pragma unroll
+      for (int k = 0; k < 9; k++) {
+        const double v = src[k];
+        if (Ks) Ks[base + (int64_t)k * nb + p] = v;
+        if (Ks32) Ks32[base + (int64_t)k * nb + p] = (float)v;
+      }
+    }
+  }
+}
+
+// y = K x (MODE 0, partial x.y) or y = b - K x (MODE 1, partial y.y); SoA rows, padded vectors.
+template <typename VT, typename XT, int MODE>
 __global__ void __launch_bounds__(kSpmvThreads)
-spmv_kernel(int64_t nrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ col,
-            const VT *__restrict__ val, const XT *__restrict__ x, const XT *__restrict__ b,
-            XT *__restrict__ y, double *__restrict__ part, const PcgState *__restrict__ st) {
-  if (st && st->done) return;
+spmv_soa(int64_t nrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ col,
+         const VT *__restrict__ val, const XT *__restrict__ x, const XT *__restrict__ b, XT *__restrict__ y,
+         double *__restrict__ part, const int32_t *__restrict__ skip) {
+  if (skip && *skip) return;
   __shared__ double sbuf[32];
   const int lane = threadIdx.x & 31;
   const int64_t warp = (blockIdx.x * (int64_t)kSpmvThreads + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * kSpmvThreads) >> 5;
   double pacc = 0.0;
   for (int64_t row = warp; row < nrows; row += nwarps) {
-    const int32_t b0 = rowptr[row], b1 = rowptr[row + 1];
-    const VT *vrow = val + (int64_t)b0 * 9;
-    const int nv = (b1 - b0) * 9;
-    AT a0 = 0, a1 = 0, a2 = 0;
-    for (int v = lane; v < nv; v += 32) {
-      const int blk = v / 9, e = v - 9 * blk, i = e / 3, j = e - 3 * i;
-      const int32_t cidx = col[b0 + blk];
-      const AT prod = (AT)vrow[v] * (AT)x[3 * (int64_t)cidx + j];
-      a0 += (i == 0) ? prod : (AT)0;
-      a1 += (i == 1) ? prod : (AT)0;
-      a2 += (i == 2) ? prod : (AT)0;
+    const int32_t b0 = rowptr[row], nb = rowptr[row + 1] - b0;
+    const VT *__restrict__ vr = val + 9 * (int64_t)b0;
+    XT a0 = 0, a1 = 0, a2 = 0;
+    for (int p = lane; p < nb; p += 32) {
+      const int32_t c = col[b0 + p];
+      XT x0, x1, x2;
+      V4<XT>::load(x + 4 * (int64_t)c, x0, x1, x2);
+      VT v[9];
+#pragma unroll
+      for (int k = 0; k < 9; k++) v[k] = vr[k * nb + p];
+      a0 += (XT)v[0] * x0 + (XT)v[1] * x1 + (XT)v[2] * x2;
+      a1 += (XT)v[3] * x0 + (XT)v[4] * x1 + (XT)v[5] * x2;
+      a2 += (XT)v[6] * x0 + (XT)v[7] * x1 + (XT)v[8] * x2;
     }
-    if (sizeof(AT) == 8) {
-      a0 = (AT)warp_sum((double)a0); a1 = (AT)warp_sum((double)a1); a2 = (AT)warp_sum((double)a2);
-    } else {
-      a0 = (AT)warp_sumf((float)a0); a1 = (AT)warp_sumf((float)a1); a2 = (AT)warp_sumf((float)a2);
-    }
+    a0 = warp_sum(a0);
+    a1 = warp_sum(a1);
+    a2 = warp_sum(a2);
     if (lane == 0) {
-      XT y0, y1, y2;
       if (MODE == 0) {
-        y0 = (XT)a0; y1 = (XT)a1; y2 = (XT)a2;
-        if (part) pacc += (double)x[3 * row] * y0 + (double)x[3 * row + 1] * y1 + (double)x[3 * row + 2] * y2;
+        V4<XT>::store(y + 4 * row, a0, a1, a2);
+        if (part) {
+          XT x0, x1, x2;
+          V4<XT>::load(x + 4 * row, x0, x1, x2);
+          pacc += (double)x0 * a0 + (double)x1 * a1 + (double)x2 * a2;
+        }
       } else {
-        y0 = b[3 * row] - (XT)a0; y1 = b[3 * row + 1] - (XT)a1; y2 = b[3 * row + 2] - (XT)a2;
+        XT b0_, b1_, b2_;
+        V4<XT>::load(b + 4 * row, b0_, b1_, b2_);
+        const XT y0 = b0_ - a0, y1 = b1_ - a1, y2 = b2_ - a2;
+        V4<XT>::store(y + 4 * row, y0, y1, y2);
         if (part) pacc += (double)y0 * y0 + (double)y1 * y1 + (double)y2 * y2;
       }
-      y[3 * row] = y0; y[3 * row + 1] = y1; y[3 * row + 2] = y2;
     }
   }
   if (part) {
@@ -126,7 +181,15 @@ __global__ void __launch_bounds__(256) pcg_alpha(PcgState *st, const double *par
   }
 }
 
-// u += alpha p; r -= alpha w; z = Dinv r (3x3 per node); partials r.r, z.r
+// z = Dinv r with Dinv stored as 3 padded rows per node
+template <typename T>
+__device__ __forceinline__ void apply_dinv(const T *D, T r0, T r1, T r2, T &z0, T &z1, T &z2) {
+  z0 = D[0] * r0 + D[1] * r1 + D[2] * r2;
+  z1 = D[4] * r0 + D[5] * r1 + D[6] * r2;
+  z2 = D[8] * r0 + D[9] * r1 + D[10] * r2;
+}
+
+// u += alpha p; r -= alpha w; z = Dinv r; partials r.r, z.r
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads)
 pcg_update(int64_t nnode, T *__restrict__ u, T *__restrict__ r, T *__restrict__ z, const T *__restrict__ p,
@@ -137,22 +200,19 @@ pcg_update(int64_t nnode, T *__restrict__ u, T *__restrict__ r, T *__restrict__ 
   const T alpha = (T)st->alpha;
   double rr = 0.0, zr = 0.0;
   for (int64_t n = blockIdx.x * (int64_t)kVecThreads + threadIdx.x; n < nnode; n += (int64_t)gridDim.x * kVecThreads) {
-    T rv[3];
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-      const int64_t i = 3 * n + k;
-      u[i] = u[i] + alpha * p[i];
-      rv[k] = r[i] + (-alpha) * w[i];
-      r[i] = rv[k];
-    }
-    const T *D = dinv + 9 * n;
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-      const T zk = D[3 * k] * rv[0] + D[3 * k + 1] * rv[1] + D[3 * k + 2] * rv[2];
-      z[3 * n + k] = zk;
-      rr += (double)rv[k] * (double)rv[k];
-      zr += (double)zk * (double)rv[k];
-    }
+    T u0, u1, u2, p0, p1, p2, r0, r1, r2, w0, w1, w2, z0, z1, z2;
+    V4<T>::load(u + 4 * n, u0, u1, u2);
+    V4<T>::load(p + 4 * n, p0, p1, p2);
+    V4<T>::load(r + 4 * n, r0, r1, r2);
+    V4<T>::load(w + 4 * n, w0, w1, w2);
+    u0 = u0 + alpha * p0; u1 = u1 + alpha * p1; u2 = u2 + alpha * p2;
+    r0 = r0 + (-alpha) * w0; r1 = r1 + (-alpha) * w1; r2 = r2 + (-alpha) * w2;
+    apply_dinv(dinv + 12 * n, r0, r1, r2, z0, z1, z2);
+    V4<T>::store(u + 4 * n, u0, u1, u2);
+    V4<T>::store(r + 4 * n, r0, r1, r2);
+    V4<T>::store(z + 4 * n, z0, z1, z2);
+    rr += (double)r0 * r0 + (double)r1 * r1 + (double)r2 * r2;
+    zr += (double)z0 * r0 + (double)z1 * r1 + (double)z2 * r2;
   }
   const double t1 = block_sum<kVecThreads>(rr, sbuf);
   if (threadIdx.x == 0) part_rr[blockIdx.x] = t1;
@@ -180,101 +240,183 @@ __global__ void __launch_bounds__(256) pcg_beta(PcgState *st, const double *part
 
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads)
-pcg_pupdate(int64_t n3, T *__restrict__ p, const T *__restrict__ z, const PcgState *__restrict__ st) {
+pcg_pupdate(int64_t nnode, T *__restrict__ p, const T *__restrict__ z, const PcgState *__restrict__ st) {
   if (st->done) return;
   const T beta = (T)st->beta;
-  for (int64_t i = blockIdx.x * (int64_t)kVecThreads + threadIdx.x; i < n3; i += (int64_t)gridDim.x * kVecThreads)
-    p[i] = z[i] + beta * p[i];
+  for (int64_t n = blockIdx.x * (int64_t)kVecThreads + threadIdx.x; n < nnode; n += (int64_t)gridDim.x * kVecThreads) {
+    T p0, p1, p2, z0, z1, z2;
+    V4<T>::load(p + 4 * n, p0, p1, p2);
+    V4<T>::load(z + 4 * n, z0, z1, z2);
+    V4<T>::store(p + 4 * n, z0 + beta * p0, z1 + beta * p1, z2 + beta * p2);
+  }
 }
 
-// z = Dinv r, p = z; partials z.r and rhs.rhs
+// z = Dinv r, p = z (if init_p); partials z.r and f.f
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads)
-pcg_init_vec(int64_t nnode, const T *__restrict__ r, T *__restrict__ z, T *__restrict__ p,
-             const T *__restrict__ dinv, const T *__restrict__ rhs, double *part_zr, double *part_ff) {
+pcg_precond(int64_t nnode, const T *__restrict__ r, T *__restrict__ z, T *__restrict__ p, const T *__restrict__ dinv,
+            const T *__restrict__ f, double *part_zr, double *part_ff) {
   __shared__ double sbuf[32];
   double zr = 0.0, ff = 0.0;
   for (int64_t n = blockIdx.x * (int64_t)kVecThreads + threadIdx.x; n < nnode; n += (int64_t)gridDim.x * kVecThreads) {
-    const T r0 = r[3 * n], r1 = r[3 * n + 1], r2 = r[3 * n + 2];
-    const T *D = dinv + 9 * n;
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-      const T zk = D[3 * k] * r0 + D[3 * k + 1] * r1 + D[3 * k + 2] * r2;
-      z[3 * n + k] = zk;
-      p[3 * n + k] = zk;
-      const T rk = (k == 0) ? r0 : (k == 1) ? r1 : r2;
-      zr += (double)zk * (double)rk;
-      const double fk = (double)rhs[3 * n + k];
-      ff += fk * fk;
+    T r0, r1, r2, z0, z1, z2;
+    V4<T>::load(r + 4 * n, r0, r1, r2);
+    apply_dinv(dinv + 12 * n, r0, r1, r2, z0, z1, z2);
+    V4<T>::store(z + 4 * n, z0, z1, z2);
+    if (p) V4<T>::store(p + 4 * n, z0, z1, z2);
+    zr += (double)z0 * r0 + (double)z1 * r1 + (double)z2 * r2;
+    if (f) {
+      T f0, f1, f2;
+      V4<T>::load(f + 4 * n, f0, f1, f2);
+      ff += (double)f0 * f0 + (double)f1 * f1 + (double)f2 * f2;
     }
   }
   const double t1 = block_sum<kVecThreads>(zr, sbuf);
   if (threadIdx.x == 0) part_zr[blockIdx.x] = t1;
-  const double t2 = block_sum<kVecThreads>(ff, sbuf);
-  if (threadIdx.x == 0) part_ff[blockIdx.x] = t2;
+  if (part_ff) {
+    const double t2 = block_sum<kVecThreads>(ff, sbuf);
+    if (threadIdx.x == 0) part_ff[blockIdx.x] = t2;
+  }
 }
 
-__global__ void __launch_bounds__(256) pcg_init_scalar(PcgState *st, const double *part_zr, const double *part_ff,
-                                                       const double *part_rr0, int n, double tol, int maxit) {
+// FP64 start: state from z.r, f.f and the initial r.r (warm start) or f.f
+__global__ void __launch_bounds__(256) pcg_init_scalar(PcgState *st, const double *part_zr, int nz,
+                                                       const double *part_ff, int nf, const double *part_rr0,
+                                                       int nr, double tol, int maxit, int iter0) {
   __shared__ double sbuf[32];
-  const double zr = sum_partials(part_zr, n, sbuf);
-  const double ff = sum_partials(part_ff, n, sbuf);
+  const double zr = sum_partials(part_zr, nz, sbuf);
+  const double ff = sum_partials(part_ff, nf, sbuf);
   double rr0 = ff;
-  if (part_rr0) rr0 = sum_partials(part_rr0, n, sbuf);
+  if (part_rr0) rr0 = sum_partials(part_rr0, nr, sbuf);
   if (threadIdx.x == 0) {
     PcgState s{};
     s.dot0 = zr;
     double lenf = sqrt(ff);
     s.tol = tol;
     s.maxit = maxit;
-    s.iter = 0;
-    s.done = 0;
+    s.iter = iter0;
     if (lenf < tol) s.done = 1;        // PCGSolver returns at once for a null load
     if (lenf > 10e+10) lenf = 1.0;     // PCGSolver's large-load normaliser
     s.lenf = lenf;
     s.rr = rr0;
     s.err = sqrt(rr0) / lenf;
+    s.err_true = s.err;
     if (!s.done && s.err < tol) s.done = 1;
     *st = s;
   }
 }
 
-// x = 0 copy helpers
-template <typename S, typename D>
-__global__ void convert_scale(int64_t n, const S *__restrict__ s, D *__restrict__ d, double scale) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    d[i] = (D)((double)s[i] * scale);
+// mixed path: u64 += x32, x32 = 0  (flush the FP32 correction)
+__global__ void flush_correction(int64_t n4, double *__restrict__ u, float *__restrict__ x,
+                                 const PcgState *__restrict__ st) {
+  if (st->final) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
+    u[i] += (double)x[i];
+    x[i] = 0.f;
+  }
 }
 
-// Jacobi / block-Jacobi inverse per node from the diagonal block
+// mixed path: r32 = (float) r64; z32 = Dinv32 r32; p32 = z32 on the first update; partials z.r
+__global__ void __launch_bounds__(kVecThreads)
+replace_residual(int64_t nnode, const double *__restrict__ r64, float *__restrict__ r, float *__restrict__ z,
+                 float *__restrict__ p, const float *__restrict__ dinv, const PcgState *__restrict__ st,
+                 double *part_zr) {
+  if (st->final) return;
+  __shared__ double sbuf[32];
+  const bool first = st->iter == 0;
+  double zr = 0.0;
+  for (int64_t n = blockIdx.x * (int64_t)kVecThreads + threadIdx.x; n < nnode; n += (int64_t)gridDim.x * kVecThreads) {
+    double d0, d1, d2;
+    V4<double>::load(r64 + 4 * n, d0, d1, d2);
+    const float r0 = (float)d0, r1 = (float)d1, r2 = (float)d2;
+    float z0, z1, z2;
+    apply_dinv(dinv + 12 * n, r0, r1, r2, z0, z1, z2);
+    V4<float>::store(r + 4 * n, r0, r1, r2);
+    V4<float>::store(z + 4 * n, z0, z1, z2);
+    if (first) V4<float>::store(p + 4 * n, z0, z1, z2);
+    zr += (double)z0 * r0 + (double)z1 * r1 + (double)z2 * r2;
+  }
+  const double t = block_sum<kVecThreads>(zr, sbuf);
+  if (threadIdx.x == 0) part_zr[blockIdx.x] = t;
+}
+
+// mixed path: the FP64 residual decides convergence; the iteration resumes otherwise
+__global__ void __launch_bounds__(256) reliable_scalar(PcgState *st, const double *part_rr, int nr,
+                                                       const double *part_zr, int nz) {
+  __shared__ double sbuf[32];
+  const double rr = sum_partials(part_rr, nr, sbuf);
+  const double zr = sum_partials(part_zr, nz, sbuf);
+  if (threadIdx.x == 0) {
+    if (st->final || st->null_rhs || st->done >= 2) return;
+    st->err_true = sqrt(rr) / st->lenf;
+    st->rr = rr;
+    st->err = st->err_true;
+    st->updates += 1;
+    if (!isfinite(st->err_true)) { st->done = 3; return; }
+    if (st->err_true < st->tol) { st->done = 1; st->final = 1; return; }
+    // the FP64 residual must halve within 10 replacements (10 chunks of FP32
+    // iterations); otherwise FP32 iterates cannot make progress on this system
+    if (st->updates == 1 || st->err_true < 0.5 * st->best_err) {
+      st->best_err = st->err_true;
+      st->stall = 0;
+    } else if (++st->stall >= 10) {
+      st->done = 4;
+      return;
+    }
+    st->done = 0;
+    st->dot0 = zr;
+  }
+}
+
+// mixed path start: lenf = |f| (with the reference's normaliser)
+__global__ void __launch_bounds__(256) mixed_init_scalar(PcgState *st, const double *part_ff, int nf, double tol,
+                                                         int maxit) {
+  __shared__ double sbuf[32];
+  const double ff = sum_partials(part_ff, nf, sbuf);
+  if (threadIdx.x == 0) {
+    PcgState s{};
+    double lenf = sqrt(ff);
+    s.tol = tol;
+    s.maxit = maxit;
+    if (lenf < tol) { s.done = 1; s.null_rhs = 1; }   // PCGSolver returns at once for a null load
+    if (lenf > 10e+10) lenf = 1.0;
+    s.lenf = lenf > 0.0 ? lenf : 1.0;
+    *st = s;
+  }
+}
+
+// Jacobi / block-Jacobi inverse per node from the diagonal block; 3 padded rows
 template <typename T>
 __global__ void build_dinv(int64_t nnode, const int32_t *__restrict__ diag, const double *__restrict__ K,
                            T *__restrict__ dinv, int block) {
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n >= nnode) return;
-  T *D = dinv + 9 * n;
+  T *D = dinv + 12 * n;
   const int32_t d = diag[n];
   double a[9];
   for (int k = 0; k < 9; k++) a[k] = (d >= 0) ? K[(int64_t)d * 9 + k] : (k % 4 == 0 ? 1.0 : 0.0);
+  double inv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   if (!block) {
-    for (int k = 0; k < 9; k++) D[k] = (T)0;
-    D[0] = (T)(1.0 / a[0]);
-    D[4] = (T)(1.0 / a[4]);
-    D[8] = (T)(1.0 / a[8]);
-    return;
+    inv[0] = 1.0 / a[0];
+    inv[4] = 1.0 / a[4];
+    inv[8] = 1.0 / a[8];
+  } else {
+    const double c00 = a[4] * a[8] - a[5] * a[7], c01 = -(a[3] * a[8] - a[5] * a[6]), c02 = a[3] * a[7] - a[4] * a[6];
+    const double id = 1.0 / (a[0] * c00 + a[1] * c01 + a[2] * c02);
+    inv[0] = c00 * id;
+    inv[1] = -(a[1] * a[8] - a[2] * a[7]) * id;
+    inv[2] = (a[1] * a[5] - a[2] * a[4]) * id;
+    inv[3] = c01 * id;
+    inv[4] = (a[0] * a[8] - a[2] * a[6]) * id;
+    inv[5] = -(a[0] * a[5] - a[2] * a[3]) * id;
+    inv[6] = c02 * id;
+    inv[7] = -(a[0] * a[7] - a[1] * a[6]) * id;
+    inv[8] = (a[0] * a[4] - a[1] * a[3]) * id;
   }
-  const double c00 = a[4] * a[8] - a[5] * a[7], c01 = -(a[3] * a[8] - a[5] * a[6]), c02 = a[3] * a[7] - a[4] * a[6];
-  const double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
-  const double id = 1.0 / det;
-  D[0] = (T)(c00 * id);
-  D[1] = (T)(-(a[1] * a[8] - a[2] * a[7]) * id);
-  D[2] = (T)((a[1] * a[5] - a[2] * a[4]) * id);
-  D[3] = (T)(c01 * id);
-  D[4] = (T)((a[0] * a[8] - a[2] * a[6]) * id);
-  D[5] = (T)(-(a[0] * a[5] - a[2] * a[3]) * id);
-  D[6] = (T)(c02 * id);
-  D[7] = (T)(-(a[0] * a[7] - a[1] * a[6]) * id);
-  D[8] = (T)((a[0] * a[4] - a[1] * a[3]) * id);
+  for (int i = 0; i < 3; i++) {
+    for (int j = 0; j < 3; j++) D[4 * i + j] = (T)inv[3 * i + j];
+    D[4 * i + 3] = (T)0;
+  }
 }
 
 __global__ void scatter_eq_to_node(int32_t neq, const int32_t *__restrict__ dof, const double *__restrict__ v,
@@ -302,49 +444,76 @@ __global__ void __launch_bounds__(256) finish_sum(const double *part, int n, dou
   if (threadIdx.x == 0) *out = t;
 }
 
-__global__ void scale_kernel(int64_t n, double *__restrict__ x, double a) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    x[i] *= a;
-}
-__global__ void axpy_kernel(int64_t n, double *__restrict__ y, const double *__restrict__ x, double a) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    y[i] += a * x[i];
-}
-
 // ---------------------------------------------------------------------------
 // host side
 
-cudaError_t scale_inplace(Ctx &c, double *x, int64_t n, double a) {
-  scale_kernel<<<kRedBlocks, 256, 0, c.stream>>>(n, x, a);
-  c.launches++;
-  return cudaGetLastError();
+cudaEvent_t Ctx::take_event() {
+  if (ev_pool.empty()) {
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+  }
+  cudaEvent_t e = ev_pool.back();
+  ev_pool.pop_back();
+  return e;
 }
-cudaError_t axpy_inplace(Ctx &c, double *y, const double *x, int64_t n, double a) {
-  axpy_kernel<<<kRedBlocks, 256, 0, c.stream>>>(n, y, x, a);
-  c.launches++;
-  return cudaGetLastError();
+void Ctx::begin_span(int kind) {
+  if (!timing) return;
+  Span sp{kind, take_event(), take_event()};
+  cudaEventRecord(sp.a, stream);
+  spans.push_back(sp);
+}
+void Ctx::end_span() {
+  if (!timing || spans.empty()) return;
+  cudaEventRecord(spans.back().b, stream);
+}
+// call after the stream has been synchronised
+void Ctx::harvest() {
+  for (Span &sp : spans) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, sp.a, sp.b) == cudaSuccess) {
+      kt_ms[sp.kind] += ms;
+      kt_n[sp.kind] += 1;
+    }
+    ev_pool.push_back(sp.a);
+    ev_pool.push_back(sp.b);
+  }
+  spans.clear();
 }
 
 static int spmv_grid(const Ctx &c) { return c.sm_count * 8; }
 
-cudaError_t launch_spmv(Ctx &c, const double *K, const double *x, double *y) {
-  spmv_kernel<double, double, double, 0><<<spmv_grid(c), kSpmvThreads, 0, c.stream>>>(
-      c.nnode, c.d_rowptr, c.d_col, K, x, nullptr, y, nullptr, nullptr);
+// partial buffers inside c.d_partials (16384 doubles)
+static double *P_A(Ctx &c) { return c.d_partials; }           // [G]  p.w
+static double *P_B(Ctx &c) { return c.d_partials + 2048; }    // [R]  r.r
+static double *P_C(Ctx &c) { return c.d_partials + 4096; }    // [R]  z.r
+static double *P_D(Ctx &c) { return c.d_partials + 6144; }    // [R]  f.f
+static double *P_E(Ctx &c) { return c.d_partials + 8192; }    // [G]  true r.r
+
+cudaError_t launch_to_soa(Ctx &c, const double *K, double *Ks, float *Ks32) {
+  aos_to_soa<<<spmv_grid(c), 256, 0, c.stream>>>(c.nnode, c.d_rowptr, K, Ks, Ks32);
   c.launches++;
   return cudaGetLastError();
 }
 
-cudaError_t launch_spmv32(Ctx &c, const float *K, const float *x, float *y) {
-  spmv_kernel<float, float, float, 0><<<spmv_grid(c), kSpmvThreads, 0, c.stream>>>(
-      c.nnode, c.d_rowptr, c.d_col, K, x, nullptr, y, nullptr, nullptr);
+cudaError_t launch_spmv(Ctx &c, const double *Ks, const double *x, double *y) {
+  spmv_soa<double, double, 0><<<spmv_grid(c), kSpmvThreads, 0, c.stream>>>(
+      c.nnode, c.d_rowptr, c.d_col, Ks, x, nullptr, y, nullptr, nullptr);
   c.launches++;
   return cudaGetLastError();
 }
 
-cudaError_t launch_residual(Ctx &c, const double *K, const double *f, const double *u, double *r, double *rr_out) {
-  double *part = c.d_partials;
-  spmv_kernel<double, double, double, 1><<<spmv_grid(c), kSpmvThreads, 0, c.stream>>>(
-      c.nnode, c.d_rowptr, c.d_col, K, u, f, r, part, nullptr);
+cudaError_t launch_spmv32(Ctx &c, const float *Ks, const float *x, float *y) {
+  spmv_soa<float, float, 0><<<spmv_grid(c), kSpmvThreads, 0, c.stream>>>(
+      c.nnode, c.d_rowptr, c.d_col, Ks, x, nullptr, y, nullptr, nullptr);
+  c.launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_residual(Ctx &c, const double *Ks, const double *f, const double *u, double *r, double *rr_out) {
+  double *part = P_E(c);
+  spmv_soa<double, double, 1><<<spmv_grid(c), kSpmvThreads, 0, c.stream>>>(
+      c.nnode, c.d_rowptr, c.d_col, Ks, u, f, r, part, nullptr);
   c.launches++;
   finish_sum<<<1, 256, 0, c.stream>>>(part, spmv_grid(c), rr_out);
   c.launches++;
@@ -360,16 +529,20 @@ cudaError_t launch_norm2(Ctx &c, const double *x, int64_t n, double *out_dev) {
 }
 
 cudaError_t launch_eq_to_node(Ctx &c, const double *eqv, double *nodev) {
-  cudaError_t e = cudaMemsetAsync(nodev, 0, sizeof(double) * 3 * (size_t)c.nnode, c.stream);
+  cudaError_t e = cudaMemsetAsync(nodev, 0, sizeof(double) * 4 * (size_t)c.nnode, c.stream);
   if (e != cudaSuccess) return e;
-  if (c.neq > 0) scatter_eq_to_node<<<(c.neq + 255) / 256, 256, 0, c.stream>>>(c.neq, c.d_dof_of_eq, eqv, nodev);
-  c.launches++;
+  if (c.neq > 0) {
+    scatter_eq_to_node<<<(c.neq + 255) / 256, 256, 0, c.stream>>>(c.neq, c.d_dof_of_eq, eqv, nodev);
+    c.launches++;
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_node_to_eq(Ctx &c, const double *nodev, double *eqv) {
-  if (c.neq > 0) gather_node_to_eq<<<(c.neq + 255) / 256, 256, 0, c.stream>>>(c.neq, c.d_dof_of_eq, nodev, eqv);
-  c.launches++;
+  if (c.neq > 0) {
+    gather_node_to_eq<<<(c.neq + 255) / 256, 256, 0, c.stream>>>(c.neq, c.d_dof_of_eq, nodev, eqv);
+    c.launches++;
+  }
   return cudaGetLastError();
 }
 
@@ -384,109 +557,113 @@ cudaError_t launch_build_precond(Ctx &c, const double *K, int precond) {
   return cudaGetLastError();
 }
 
-// Runs PCG on K (FP64) or K32 (FP32).  rhs and x are FP64 node-DOF vectors;
-// in FP32 mode they are converted at entry/exit (x returned = FP32 solution).
-cudaError_t pcg_solve_device(Ctx &c, bool fp32, const double *d_rhs, double *d_x, bool warm, double tol,
-                             int maxit, int check_every, int precond, int *iters, double *err, int *done) {
-  (void)precond;
-  const int64_t nn = c.nnode, n3 = 3 * nn;
-  const int G = spmv_grid(c);
-  const int R = kRedBlocks;
-  double *pA = c.d_partials;            // [G]  p.w
-  double *pB = c.d_partials + 2048;     // [R]  r.r
-  double *pC = c.d_partials + 4096;     // [R]  z.r
-  double *pD = c.d_partials + 6144;     // [R]  rhs.rhs
-  double *pE = c.d_partials + 8192;     // [G]  initial r.r
-  PcgState *st = c.d_state;
+// Pipelined host loop: launch a chunk, then look at the state copied after the
+// previous chunk; returns when done or when maxit iterations were launched.
+template <typename LaunchChunk>
+static cudaError_t drive(Ctx &c, int maxit, int chunk, LaunchChunk launch_chunk) {
   cudaError_t e;
-  if (!fp32) {
-    if (warm) {
-      spmv_kernel<double, double, double, 1><<<G, kSpmvThreads, 0, c.stream>>>(
-          nn, c.d_rowptr, c.d_col, c.d_K, d_x, d_rhs, c.d_r, pE, nullptr);
-      c.launches++;
-    } else {
-      cudaMemsetAsync(d_x, 0, sizeof(double) * n3, c.stream);
-      cudaMemcpyAsync(c.d_r, d_rhs, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c.stream);
-    }
-    pcg_init_vec<double><<<R, kVecThreads, 0, c.stream>>>(nn, c.d_r, c.d_z, c.d_p, c.d_dinv, d_rhs, pC, pD);
-    c.launches++;
-    pcg_init_scalar<<<1, 256, 0, c.stream>>>(st, pC, pD, warm ? pE : nullptr, warm ? G : R, tol, maxit);
-    c.launches++;
-  } else {
-    // FP32: rhs converted, x starts at 0
-    convert_scale<double, float><<<R, 256, 0, c.stream>>>(n3, d_rhs, c.s_r, 1.0);
-    c.launches++;
-    cudaMemsetAsync(c.s_u, 0, sizeof(float) * n3, c.stream);
-    pcg_init_vec<float><<<R, kVecThreads, 0, c.stream>>>(nn, c.s_r, c.s_z, c.s_p, c.s_dinv, c.s_r, pC, pD);
-    c.launches++;
-    pcg_init_scalar<<<1, 256, 0, c.stream>>>(st, pC, pD, nullptr, R, tol, maxit);
-    c.launches++;
-  }
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-
-  if (check_every <= 0) check_every = 32;
   cudaEvent_t ev;
   if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return e;
   int launched = 0;
   bool pending = false;
   while (true) {
-    // launch one chunk
-    for (int k = 0; k < check_every && launched < maxit; k++, launched++) {
-      if (!fp32) {
-        spmv_kernel<double, double, double, 0><<<G, kSpmvThreads, 0, c.stream>>>(
-            nn, c.d_rowptr, c.d_col, c.d_K, c.d_p, nullptr, c.d_w, pA, st);
-        c.launches++;
-        pcg_alpha<<<1, 256, 0, c.stream>>>(st, pA, G);
-        c.launches++;
-        pcg_update<double><<<R, kVecThreads, 0, c.stream>>>(nn, d_x, c.d_r, c.d_z, c.d_p, c.d_w, c.d_dinv, st, pB, pC);
-        c.launches++;
-        pcg_beta<<<1, 256, 0, c.stream>>>(st, pB, pC, R);
-        c.launches++;
-        pcg_pupdate<double><<<R, kVecThreads, 0, c.stream>>>(n3, c.d_p, c.d_z, st);
-        c.launches++;
-      } else {
-        spmv_kernel<float, float, float, 0><<<G, kSpmvThreads, 0, c.stream>>>(
-            nn, c.d_rowptr, c.d_col, c.d_K32, c.s_p, nullptr, c.s_w, pA, st);
-        c.launches++;
-        pcg_alpha<<<1, 256, 0, c.stream>>>(st, pA, G);
-        c.launches++;
-        pcg_update<float><<<R, kVecThreads, 0, c.stream>>>(nn, c.s_u, c.s_r, c.s_z, c.s_p, c.s_w, c.s_dinv, st, pB, pC);
-        c.launches++;
-        pcg_beta<<<1, 256, 0, c.stream>>>(st, pB, pC, R);
-        c.launches++;
-        pcg_pupdate<float><<<R, kVecThreads, 0, c.stream>>>(n3, c.s_p, c.s_z, st);
-        c.launches++;
-      }
-    }
-    if ((e = cudaGetLastError()) != cudaSuccess) break;
-    // check the state of the previous chunk while this one runs
+    const int k = (maxit - launched < chunk) ? (maxit - launched) : chunk;
+    if ((e = launch_chunk(k)) != cudaSuccess) break;
+    launched += k;
     if (pending) {
       if ((e = cudaEventSynchronize(ev)) != cudaSuccess) break;
       if (c.h_state->done) break;
     }
-    if ((e = cudaMemcpyAsync(c.h_state, st, sizeof(PcgState), cudaMemcpyDeviceToHost, c.stream)) != cudaSuccess) break;
+    if ((e = cudaMemcpyAsync(c.h_state, c.d_state, sizeof(PcgState), cudaMemcpyDeviceToHost, c.stream)) != cudaSuccess)
+      break;
     if ((e = cudaEventRecord(ev, c.stream)) != cudaSuccess) break;
     pending = true;
     if (launched >= maxit) {
-      if ((e = cudaEventSynchronize(ev)) != cudaSuccess) break;
+      e = cudaEventSynchronize(ev);
       break;
     }
   }
   cudaEventDestroy(ev);
   if (e != cudaSuccess) return e;
-  // final state
-  if ((e = cudaMemcpyAsync(c.h_state, st, sizeof(PcgState), cudaMemcpyDeviceToHost, c.stream)) != cudaSuccess) return e;
-  if ((e = cudaStreamSynchronize(c.stream)) != cudaSuccess) return e;
-  *iters = c.h_state->iter;
-  *err = c.h_state->err;
-  *done = c.h_state->done;
-  if (fp32) {
-    // return the FP32 solution in d_x
-    convert_scale<float, double><<<R, 256, 0, c.stream>>>(n3, c.s_u, d_x, 1.0);
+  if ((e = cudaMemcpyAsync(c.h_state, c.d_state, sizeof(PcgState), cudaMemcpyDeviceToHost, c.stream)) != cudaSuccess)
+    return e;
+  return cudaStreamSynchronize(c.stream);
+}
+
+cudaError_t pcg_fp64(Ctx &c, bool warm, double tol, int maxit, int chunk, int iter0) {
+  const int64_t nn = c.nnode;
+  const int G = spmv_grid(c), R = kRedBlocks;
+  PcgState *st = c.d_state;
+  cudaError_t e;
+  if (warm) {
+    spmv_soa<double, double, 1><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_rowptr, c.d_col, c.d_Ks, c.d_u, c.d_f,
+                                                                   c.d_r, P_E(c), nullptr);
     c.launches++;
-    e = cudaGetLastError();
+  } else {
+    cudaMemsetAsync(c.d_u, 0, sizeof(double) * 4 * nn, c.stream);
+    cudaMemcpyAsync(c.d_r, c.d_f, sizeof(double) * 4 * nn, cudaMemcpyDeviceToDevice, c.stream);
   }
-  return e;
+  pcg_precond<double><<<R, kVecThreads, 0, c.stream>>>(nn, c.d_r, c.d_z, c.d_p, c.d_dinv, c.d_f, P_C(c), P_D(c));
+  c.launches++;
+  pcg_init_scalar<<<1, 256, 0, c.stream>>>(st, P_C(c), R, P_D(c), R, warm ? P_E(c) : nullptr, G, tol, maxit, iter0);
+  c.launches++;
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  return drive(c, maxit, chunk, [&](int k) -> cudaError_t {
+    for (int i = 0; i < k; i++) {
+      c.begin_span(0);
+      spmv_soa<double, double, 0><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_rowptr, c.d_col, c.d_Ks, c.d_p, nullptr,
+                                                                     c.d_w, P_A(c), &st->done);
+      c.end_span();
+      pcg_alpha<<<1, 256, 0, c.stream>>>(st, P_A(c), G);
+      pcg_update<double><<<R, kVecThreads, 0, c.stream>>>(nn, c.d_u, c.d_r, c.d_z, c.d_p, c.d_w, c.d_dinv, st,
+                                                           P_B(c), P_C(c));
+      pcg_beta<<<1, 256, 0, c.stream>>>(st, P_B(c), P_C(c), R);
+      pcg_pupdate<double><<<R, kVecThreads, 0, c.stream>>>(nn, c.d_p, c.d_z, st);
+      c.launches += 5;
+    }
+    return cudaGetLastError();
+  });
+}
+
+// FP32 PCG with FP64 reliable updates every `chunk` iterations.
+cudaError_t pcg_mixed(Ctx &c, bool warm, double tol, int maxit, int chunk) {
+  const int64_t nn = c.nnode;
+  const int G = spmv_grid(c), R = kRedBlocks;
+  PcgState *st = c.d_state;
+  cudaError_t e;
+  if (!warm) cudaMemsetAsync(c.d_u, 0, sizeof(double) * 4 * nn, c.stream);
+  cudaMemsetAsync(c.s_x, 0, sizeof(float) * 4 * nn, c.stream);
+  sumsq_kernel<<<R, 256, 0, c.stream>>>(4 * nn, c.d_f, P_D(c));
+  mixed_init_scalar<<<1, 256, 0, c.stream>>>(st, P_D(c), R, tol, maxit);
+  c.launches += 2;
+  auto reliable = [&]() {
+    flush_correction<<<R, 256, 0, c.stream>>>(4 * nn, c.d_u, c.s_x, st);
+    c.begin_span(0);
+    spmv_soa<double, double, 1><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_rowptr, c.d_col, c.d_Ks, c.d_u, c.d_f,
+                                                                   c.d_r, P_E(c), &st->final);
+    c.end_span();
+    replace_residual<<<R, kVecThreads, 0, c.stream>>>(nn, c.d_r, c.s_r, c.s_z, c.s_p, c.s_dinv, st, P_C(c));
+    reliable_scalar<<<1, 256, 0, c.stream>>>(st, P_E(c), G, P_C(c), R);
+    c.launches += 4;
+  };
+  reliable();
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  return drive(c, maxit, chunk, [&](int k) -> cudaError_t {
+    for (int i = 0; i < k; i++) {
+      c.begin_span(1);
+      spmv_soa<float, float, 0><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_rowptr, c.d_col, c.d_Ks32, c.s_p, nullptr,
+                                                                   c.s_w, P_A(c), &st->done);
+      c.end_span();
+      pcg_alpha<<<1, 256, 0, c.stream>>>(st, P_A(c), G);
+      pcg_update<float><<<R, kVecThreads, 0, c.stream>>>(nn, c.s_x, c.s_r, c.s_z, c.s_p, c.s_w, c.s_dinv, st,
+                                                          P_B(c), P_C(c));
+      pcg_beta<<<1, 256, 0, c.stream>>>(st, P_B(c), P_C(c), R);
+      pcg_pupdate<float><<<R, kVecThreads, 0, c.stream>>>(nn, c.s_p, c.s_z, st);
+      c.launches += 5;
+    }
+    reliable();
+    return cudaGetLastError();
+  });
 }
 
 }  // namespace fastgpu

@@ -40,7 +40,7 @@ EXPORTS = [
     "fast_gpu_synchronize", "fast_gpu_upload_mesh", "fast_gpu_pattern_info", "fast_gpu_update_coords",
     "fast_gpu_update_material", "fast_gpu_zero", "fast_gpu_assemble", "fast_gpu_add", "fast_gpu_get",
     "fast_gpu_mult_vect", "fast_gpu_solve", "fast_gpu_solve_device", "fast_gpu_face_load_vector",
-    "fast_gpu_get_lower_csr", "fast_gpu_element_matrices", "fast_gpu_launch_count", "fast_gpu_time_kernel",
+    "fast_gpu_get_lower_csr", "fast_gpu_element_matrices", "fast_gpu_launch_count", "fast_gpu_kernel_timing", "fast_gpu_kernel_stats",
     "fast_gpu_inspect_pattern",
 ]
 KERNEL_SPMV_FP64, KERNEL_SPMV_FP32, KERNEL_ASSEMBLE = 0, 1, 2
@@ -72,11 +72,11 @@ class SolveOpts(ctypes.Structure):
 
 class SolveReport(ctypes.Structure):
     _fields_ = [("converged", ctypes.c_int32), ("iterations", ctypes.c_int32), ("outer", ctypes.c_int32),
-                ("reserved", ctypes.c_int32), ("rel_residual", ctypes.c_double),
+                ("escalated", ctypes.c_int32), ("rel_residual", ctypes.c_double),
                 ("true_rel_residual", ctypes.c_double)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 _lib = None
@@ -117,7 +117,8 @@ def load_library(path: str = LIB_PATH):
     L.fast_gpu_element_matrices.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, _dp]
     L.fast_gpu_launch_count.argtypes = [vp, _lp]
     L.fast_gpu_inspect_pattern.argtypes = [ctypes.POINTER(Mesh), _lp, _lp, _ip, _ip, _ip, _ip]
-    L.fast_gpu_time_kernel.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, _dp, _dp]
+    L.fast_gpu_kernel_timing.argtypes = [vp, ctypes.c_int32]
+    L.fast_gpu_kernel_stats.argtypes = [vp, ctypes.c_int32, _lp, _dp, _dp]
     _lib = L
     return L
 
@@ -289,10 +290,18 @@ class GpuSystem:
         self._ck(self.L.fast_gpu_launch_count(self.ctx, ctypes.byref(n)), "launch_count")
         return n.value
 
-    def time_kernel(self, which: int, reps: int = 10):
-        ms, b = ctypes.c_double(), ctypes.c_double()
-        self._ck(self.L.fast_gpu_time_kernel(self.ctx, which, reps, ctypes.byref(ms), ctypes.byref(b)), "time_kernel")
-        return ms.value, b.value
+    def kernel_timing(self, enable: bool = True):
+        self._ck(self.L.fast_gpu_kernel_timing(self.ctx, int(enable)), "kernel_timing")
+
+    def kernel_stats(self, which: int):
+        """(timed launches, summed device ms, algorithmic bytes per launch) since timing was enabled.
+
+        Launches issued after convergence return at once and are counted here;
+        divide the summed time by the number of real launches for a mean."""
+        n, ms, b = ctypes.c_int64(), ctypes.c_double(), ctypes.c_double()
+        self._ck(self.L.fast_gpu_kernel_stats(self.ctx, which, ctypes.byref(n), ctypes.byref(ms), ctypes.byref(b)),
+                 "kernel_stats")
+        return n.value, ms.value, b.value
 
     # -- parity
     def lower_csr(self, what=ASM_K):

@@ -54,7 +54,9 @@ extern "C" {
 
 /* ---- solver precision ------------------------------------------------- */
 #define FAST_PREC_FP64      0   /* FP64 Jacobi PCG, as PCGSolver (mlib/sysmat.cpp:1061-1125) */
-#define FAST_PREC_MIXED     1   /* FP32 PCG inside FP64 iterative refinement     */
+#define FAST_PREC_MIXED     1   /* FP32 PCG, FP64 solution and residual replacement
+                                   ("reliable updates"); continues in FP64 if the FP32
+                                   iterates stall on an ill-conditioned system       */
 
 /* ---- preconditioner --------------------------------------------------- */
 #define FAST_PRECOND_JACOBI        0  /* z = r / diag(K), as the reference      */
@@ -89,16 +91,17 @@ typedef struct {
   int32_t maxit;          /* iteration cap (total inner iterations); 0 = 20*num_eq */
   int32_t warm_start;     /* 1: start from the u passed in (mixed path: as the first iterate) */
   double  tol;            /* stop when |r|/|f| < tol (|f| > 1e11 replaced by 1, as the reference) */
-  double  inner_tol;      /* FAST_PREC_MIXED: relative reduction per FP32 inner solve; 0 = 1e-5 */
-  int32_t max_outer;      /* FAST_PREC_MIXED: refinement steps cap; 0 = 30       */
-  int32_t check_every;    /* convergence read-back period in iterations; 0 = 32 */
+  double  inner_tol;      /* reserved, 0                                          */
+  int32_t max_outer;      /* reserved, 0                                          */
+  int32_t check_every;    /* iterations per chunk: convergence read-back period and,
+                             mixed, FP64 residual replacement period; 0 = 32 (FP64) / 50 (mixed) */
 } fast_gpu_solve_opts;
 
 typedef struct {
   int32_t converged;
-  int32_t iterations;      /* PCG iterations (sum of inner iterations when mixed) */
-  int32_t outer;           /* refinement steps (1 for FP64)                        */
-  int32_t reserved;
+  int32_t iterations;      /* PCG iterations (FP32 + FP64 iterations when mixed)  */
+  int32_t outer;           /* FP64 residual replacements (mixed), 1 for FP64        */
+  int32_t escalated;       /* mixed: FP32 iterates stalled, finished in FP64       */
   double  rel_residual;    /* |r|/|f| of the final FP64 residual (mixed) or recurrence (FP64) */
   double  true_rel_residual; /* |f - K u| / |f| recomputed in FP64 at exit           */
 } fast_gpu_solve_report;
@@ -175,16 +178,19 @@ int fast_gpu_element_matrices(fast_gpu_ctx *ctx, int32_t what, int32_t bucket, i
                               int64_t count, double *Ke);
 
 /* ---- measurement ------------------------------------------------------ */
-#define FAST_KERNEL_SPMV_FP64  0   /* one K.p of the FP64 PCG (node-block CSR, FP64 values) */
-#define FAST_KERNEL_SPMV_FP32  1   /* one K32.p of the FP32 inner PCG                       */
-#define FAST_KERNEL_ASSEMBLE   2   /* one full stiffness assembly (zero fill + all colours)  */
+#define FAST_KERNEL_SPMV_FP64  0   /* K.p with FP64 values (FP64 PCG, FP64 residuals)       */
+#define FAST_KERNEL_SPMV_FP32  1   /* K.p with FP32 values (mixed path)                     */
+#define FAST_KERNEL_ASSEMBLE   2   /* one stiffness assembly (zero fill + all colours)      */
 /* Kernels this context has launched so far (every entry point counts). */
 int fast_gpu_launch_count(fast_gpu_ctx *ctx, int64_t *count);
-/* Times `reps` back-to-back runs of one kernel with CUDA events on the
- * context's stream (after one untimed run) and returns the mean duration and
- * the algorithmic bytes one run moves (the roofline numerator). */
-int fast_gpu_time_kernel(fast_gpu_ctx *ctx, int32_t which, int32_t reps, double *avg_ms,
-                         double *bytes_per_run);
+/* Live timing: while enabled, every SpMV launched by a solve and every
+ * stiffness assembly is bracketed by CUDA events on the context's stream.
+ * Enabling resets the statistics. */
+int fast_gpu_kernel_timing(fast_gpu_ctx *ctx, int32_t enable);
+/* Launches, summed device time and algorithmic bytes per launch (the
+ * roofline numerator) of one timed kind since timing was enabled. */
+int fast_gpu_kernel_stats(fast_gpu_ctx *ctx, int32_t which, int64_t *launches, double *total_ms,
+                          double *bytes_per_launch);
 
 #ifdef __cplusplus
 }

@@ -18,6 +18,9 @@ TOL_U = 1e-9
 LINEAR = [n for n in gio.names() if n not in ("cfg_hex8_tl_state",)]
 WITH_K = [n for n in LINEAR if "ref_K_data" in gio.load(n)[1]]
 SOLVABLE = ["cfg_hex8_cantilever", "cfg_hex20_lognormal_4x4x2", "cfg_hex20_lognormal_8x8x4"]
+# solver tolerance per deck: the slender cantilever's attainable FP64 residual
+# is about 1e-11 (the reference's own skyline solution has 4.7e-11)
+SOLVE_TOL = {"cfg_hex8_cantilever": 1e-10}
 
 
 def system(d):
@@ -63,7 +66,7 @@ def test_displacements_match_reference(name, precision):
     d, g = gio.load(name)
     s = system(d)
     s.assemble()
-    u, rep = s.solve(g["ref_f"], tol=1e-13, precision=precision)
+    u, rep = s.solve(g["ref_f"], tol=SOLVE_TOL.get(name, 1e-12), precision=precision)
     assert rep["converged"]
     assert gio.rel(u, g["ref_u"]) < TOL_U, rep
 
@@ -145,6 +148,44 @@ def test_nonpositive_jacobian_is_reported():
     with pytest.raises(gpu.FastGpuError) as ei:
         s.assemble()
     assert ei.value.rc == -6
+
+
+def test_mixed_escalates_on_ill_conditioned_system():
+    # slender cantilever, cond(K) ~ 1e6: FP32 iterates stall, the solve goes on in FP64
+    d, g = gio.load("cfg_hex8_cantilever")
+    s = system(d)
+    s.assemble()
+    u, rep = s.solve(g["ref_f"], tol=1e-10, precision=gpu.PREC_MIXED)
+    assert rep["converged"] and rep["escalated"] == 1
+    assert gio.rel(u, g["ref_u"]) < TOL_U
+
+
+def test_mixed_does_not_escalate_on_lognormal_box():
+    d = decks.box_hex20_lognormal(12, 12, 6, seed=5)
+    s = system(d)
+    s.assemble()
+    f = gpu.face_load_vector(d)
+    u, rep = s.solve(f, tol=1e-10, precision=gpu.PREC_MIXED)
+    u64, rep64 = s.solve(f, tol=1e-10, precision=gpu.PREC_FP64)
+    assert rep["converged"] and rep["escalated"] == 0
+    assert rep["iterations"] <= 1.1 * rep64["iterations"] + 60
+    assert rep["true_rel_residual"] < 1e-10
+    assert gio.rel(u, u64) < 1e-8
+
+
+def test_live_kernel_timing_counts_launches():
+    d = decks.box_hex20_lognormal(8, 8, 4, seed=1)
+    s = system(d)
+    s.kernel_timing(True)
+    s.assemble()
+    f = gpu.face_load_vector(d)
+    u, rep = s.solve(f, tol=1e-8, precision=gpu.PREC_MIXED)
+    n32, ms32, b32 = s.kernel_stats(gpu.KERNEL_SPMV_FP32)
+    n64, ms64, b64 = s.kernel_stats(gpu.KERNEL_SPMV_FP64)
+    na, msa, ba = s.kernel_stats(gpu.KERNEL_ASSEMBLE)
+    assert na == 1 and msa > 0 and ba > 0
+    assert n32 >= rep["iterations"] and ms32 > 0 and b32 > 0
+    assert n64 >= rep["outer"] and ms64 > 0
 
 
 def test_nonconvergence_is_reported():
