@@ -53,16 +53,12 @@ struct ElemArgs {
 template <int NN, int NG, bool MASS>
 struct ElemSmem {
   static constexpr int ND = 3 * NN;
-  static constexpr int LDH = ND + 1;
   static constexpr int kN = MASS ? NG * NN : 0;   // shape functions (mass only)
   static constexpr int kX = NN * 3;
-  static constexpr int kJ = NG * 9;
+  static constexpr int kJ = NG * 9;               // Jacobian, then its inverse
   static constexpr int kC = NG;
-  static constexpr int kD = MASS ? 0 : NG * ND;
-  static constexpr int kH = MASS ? 0 : ND * LDH;
-  // doubles; J is aliased into H (J is dead before H is written)
-  static constexpr int kHJ = kH > kJ ? kH : kJ;
-  static constexpr int total = kN + kX + kC + kD + kHJ;
+  static constexpr int kD = MASS ? 0 : NG * ND;   // dN/dx at the Gauss points
+  static constexpr int total = kN + kX + kJ + kC + kD;
   static constexpr size_t bytes = total * sizeof(double) + 2 * 256 + 64;
 };
 
@@ -74,34 +70,39 @@ __device__ __forceinline__ void pair_of(int p, int n, int &a, int &b) {
   b = r + p;
 }
 
+// One CTA integrates one element at a time (grid-stride over the colour).
+// Thread p < NP owns node pair (a, b), a <= b: it loads the pair's two slot
+// indices and the current 3x3 blocks (a,b) and (b,a) at the start of the
+// element, so the global read latency overlaps the Jacobian and derivative
+// work, then forms
+//     M_ij = sum_g c_g dN_a/dx_i dN_b/dx_j
+// in registers, turns M into the 3x3 stiffness block and adds it.
 template <int NN, int NG, int NT, bool MASS>
-__global__ void __launch_bounds__(NT, (NT >= 256 ? 4 : 8)) elem_kernel(ElemArgs A) {
+__global__ void __launch_bounds__(NT, (NT >= 128 ? 3 : 8)) elem_kernel(ElemArgs A) {
   using S = ElemSmem<NN, NG, MASS>;
-  constexpr int ND = S::ND, LDH = S::LDH;
+  constexpr int ND = S::ND;
   extern __shared__ __align__(16) double sm[];
   double *sN = sm;
   double *sX = sN + S::kN;
-  double *sc = sX + S::kX;
+  double *sJ = sX + S::kX;
+  double *sc = sJ + S::kJ;
   double *sD = sc + S::kC;
-  double *sH = sD + S::kD;
-  double *sJ = sH;  // aliased
-  uint8_t *sfix = reinterpret_cast<uint8_t *>(sH + S::kHJ);
+  uint8_t *sfix = reinterpret_cast<uint8_t *>(sD + S::kD);
   uint8_t *spa = sfix + 64;
   uint8_t *spb = spa + 256;
   constexpr int NP = NN * (NN + 1) / 2;
+  static_assert(NP <= NT, "one thread per node pair");
   // Gauss-point tables are read through the L1 cache (read-only, shared by all blocks)
-  const double *__restrict__ sdN = A.dN;
-  const double *__restrict__ sw = A.w;
+  const double *__restrict__ gdN = A.dN;
+  const double *__restrict__ gw = A.w;
 
   const int tid = threadIdx.x;
   if (MASS)
     for (int i = tid; i < S::kN; i += NT) sN[i] = A.N[i];
-  for (int p = tid; p < NP; p += NT) {
-    int a, b;
-    pair_of(p, NN, a, b);
-    spa[p] = (uint8_t)a;
-    spb[p] = (uint8_t)b;
-  }
+  int pa = 0, pb = 0;
+  if (tid < NP) pair_of(tid, NN, pa, pb);
+  (void)spa;
+  (void)spb;
 
   for (int64_t it = blockIdx.x; it < A.ne; it += gridDim.x) {
     const int64_t e = A.index ? (int64_t)A.index[it] : A.offset + it;
@@ -112,12 +113,26 @@ __global__ void __launch_bounds__(NT, (NT >= 256 ? 4 : 8)) elem_kernel(ElemArgs 
       sX[i] = A.X[3 * (int64_t)n + (i % 3)];
     }
     for (int i = tid; i < NN; i += NT) sfix[i] = A.fix[en[i]];
+
+    // early scatter loads: slots, then the current block values
+    double *Kab = nullptr, *Kba = nullptr;
+    double oab[9], oba[9];
+    if (A.K && tid < NP) {
+      Kab = A.K + (int64_t)A.slot[(e * NN + pa) * NN + pb] * 9;
+      if (pa != pb) Kba = A.K + (int64_t)A.slot[(e * NN + pb) * NN + pa] * 9;
+#pragma unroll
+      for (int k = 0; k < 9; k++) oab[k] = Kab[k];
+      if (Kba) {
+#pragma unroll
+        for (int k = 0; k < 9; k++) oba[k] = Kba[k];
+      }
+    }
     __syncthreads();
 
     // Jacobians J[g][p][q] = sum_a dN_a/dxi_p X_a,q (cShapeSolid::DrvShpXYZ, shp/shpsolid.cpp:58-126)
     for (int t = tid; t < NG * 9; t += NT) {
       const int g = t / 9, pq = t - 9 * g, p = pq / 3, q = pq - 3 * p;
-      const double *d = sdN + g * NN * 3 + p;
+      const double *d = gdN + g * NN * 3 + p;
       double s = 0.0;
 #pragma unroll 4
       for (int a = 0; a < NN; a++) s += d[3 * a] * sX[3 * a + q];
@@ -141,135 +156,83 @@ __global__ void __launch_bounds__(NT, (NT >= 256 ? 4 : 8)) elem_kernel(ElemArgs 
       J[6] = (j10 * j21 - j11 * j20) / id;
       J[7] = -(j00 * j21 - j01 * j20) / id;
       J[8] = (j00 * j11 - j01 * j10) / id;
-      sc[g] = sw[g] * det;
+      sc[g] = gw[g] * det;
     }
     __syncthreads();
 
+    double v[9];
     if (MASS) {
       // M_ab = rho * sum_g c_g N_a N_b * I3  (cElmParam::MassMat, elc/elmparam.cpp:672-739)
-      const double rho = A.rho ? A.rho[e] : 0.0;
-      for (int p = tid; p < NP; p += NT) {
-        const int a = spa[p], b = spb[p];
+      if (tid < NP) {
+        const double rho = A.rho ? A.rho[e] : 0.0;
         double s = 0.0;
-        for (int g = 0; g < NG; g++) s += sc[g] * sN[g * NN + a] * sN[g * NN + b];
+        for (int g = 0; g < NG; g++) s += sc[g] * sN[g * NN + pa] * sN[g * NN + pb];
         s *= rho;
-        for (int i = 0; i < 3; i++) {
-          if (A.Ke_out) {
-            double *Ko = A.Ke_out + it * ND * ND;
-            Ko[(3 * a + i) * ND + 3 * b + i] = s;
-            Ko[(3 * b + i) * ND + 3 * a + i] = s;
-          }
-          if (A.K && !((sfix[a] >> i) & 1) && !((sfix[b] >> i) & 1)) {
-            const int32_t sab = A.slot[(e * NN + a) * NN + b];
-            A.K[(int64_t)sab * 9 + 4 * i] += s;
-            if (a != b) {
-              const int32_t sba = A.slot[(e * NN + b) * NN + a];
-              A.K[(int64_t)sba * 9 + 4 * i] += s;
-            }
-          }
-        }
+#pragma unroll
+        for (int k = 0; k < 9; k++) v[k] = (k % 4 == 0) ? s : 0.0;
       }
-      continue;
-    }
-
-    // D[g][i*NN + a] = dN_a/dx_i at Gauss point g
-    for (int t = tid; t < NG * NN; t += NT) {
-      const int g = t / NN, a = t - NN * g;
-      const double *J = sJ + 9 * g;
-      const double d0 = sdN[(g * NN + a) * 3], d1 = sdN[(g * NN + a) * 3 + 1], d2 = sdN[(g * NN + a) * 3 + 2];
-      double *D = sD + g * ND;
-      D[a] = J[0] * d0 + J[1] * d1 + J[2] * d2;
-      D[NN + a] = J[3] * d0 + J[4] * d1 + J[5] * d2;
-      D[2 * NN + a] = J[6] * d0 + J[7] * d1 + J[8] * d2;
-    }
-    __syncthreads();
-
-    // H = sum_g c_g D_g D_g^T in 4x4 register tiles (all T*T tiles: no
-    // triangular bookkeeping; the FP64 pipe has room for the symmetric half)
-    constexpr int T = ND / 4;
-    for (int tile = tid; tile < T * T; tile += NT) {
-      const int ti = tile / T, tj = tile - T * ti;
-      double acc[4][4];
-#pragma unroll
-      for (int r = 0; r < 4; r++)
-#pragma unroll
-        for (int q = 0; q < 4; q++) acc[r][q] = 0.0;
-      for (int g = 0; g < NG; g++) {
-        const double cg = sc[g];
-        const double *D = sD + g * ND;
-        double ra[4], cb[4];
-#pragma unroll
-        for (int r = 0; r < 4; r++) ra[r] = cg * D[4 * ti + r];
-#pragma unroll
-        for (int q = 0; q < 4; q++) cb[q] = D[4 * tj + q];
-#pragma unroll
-        for (int r = 0; r < 4; r++)
-#pragma unroll
-          for (int q = 0; q < 4; q++) acc[r][q] = fma(ra[r], cb[q], acc[r][q]);
+    } else {
+      // D[g][i*NN + a] = dN_a/dx_i at Gauss point g
+      for (int t = tid; t < NG * NN; t += NT) {
+        const int g = t / NN, a = t - NN * g;
+        const double *J = sJ + 9 * g;
+        const double *dn = gdN + (g * NN + a) * 3;
+        const double d0 = dn[0], d1 = dn[1], d2 = dn[2];
+        double *D = sD + g * ND;
+        D[a] = J[0] * d0 + J[1] * d1 + J[2] * d2;
+        D[NN + a] = J[3] * d0 + J[4] * d1 + J[5] * d2;
+        D[2 * NN + a] = J[6] * d0 + J[7] * d1 + J[8] * d2;
       }
+      __syncthreads();
+      if (tid < NP) {
+        // M_ij = sum_g c_g dNa/dx_i dNb/dx_j, then the isotropic block
+        //   i == j : C00 M_ii + G (tr M - M_ii);   i != j : C01 M_ij + G M_ji
+        // (cSolid::QMatrix elc/anmodel.cpp:1286-1298, BMatrix :1418-1447)
+        double M[9];
 #pragma unroll
-      for (int r = 0; r < 4; r++)
-#pragma unroll
-        for (int q = 0; q < 4; q++) sH[(4 * ti + r) * LDH + 4 * tj + q] = acc[r][q];
-    }
-    __syncthreads();
-
-    // element matrix blocks and scatter: one thread per node pair (a <= b).
-    // The 9 values of block (a,b) and of its transpose (b,a) are loaded before
-    // any store, so a thread keeps 18 independent loads in flight.
-    const double E = A.E[e], nu = A.nu[e];
-    const double dd = (1.0 + nu) * (1.0 - 2.0 * nu);
-    const double C00 = E * (1.0 - nu) / dd, C01 = E * nu / dd, G = 0.5 * E / (1.0 + nu);
-    for (int p = tid; p < NP; p += NT) {
-      const int a = spa[p], b = spb[p];
-      double v[9];
-      const double hs = sH[a * LDH + b] + sH[(NN + a) * LDH + NN + b] + sH[(2 * NN + a) * LDH + 2 * NN + b];
-#pragma unroll
-      for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-          if (i == j) {
-            const double hii = sH[(i * NN + a) * LDH + i * NN + b];
-            v[3 * i + j] = C00 * hii + G * (hs - hii);
-          } else {
-            v[3 * i + j] = C01 * sH[(i * NN + a) * LDH + j * NN + b] + G * sH[(j * NN + a) * LDH + i * NN + b];
-          }
+        for (int k = 0; k < 9; k++) M[k] = 0.0;
+        for (int g = 0; g < NG; g++) {
+          const double *D = sD + g * ND;
+          const double cg = sc[g];
+          const double a0 = cg * D[pa], a1 = cg * D[NN + pa], a2 = cg * D[2 * NN + pa];
+          const double b0 = D[pb], b1 = D[NN + pb], b2 = D[2 * NN + pb];
+          M[0] = fma(a0, b0, M[0]); M[1] = fma(a0, b1, M[1]); M[2] = fma(a0, b2, M[2]);
+          M[3] = fma(a1, b0, M[3]); M[4] = fma(a1, b1, M[4]); M[5] = fma(a1, b2, M[5]);
+          M[6] = fma(a2, b0, M[6]); M[7] = fma(a2, b1, M[7]); M[8] = fma(a2, b2, M[8]);
         }
+        const double E = A.E[e], nu = A.nu[e];
+        const double dd = (1.0 + nu) * (1.0 - 2.0 * nu);
+        const double C00 = E * (1.0 - nu) / dd, C01 = E * nu / dd, G = 0.5 * E / (1.0 + nu);
+        const double tr = M[0] + M[4] + M[8];
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+          for (int j = 0; j < 3; j++)
+            v[3 * i + j] = (i == j) ? C00 * M[4 * i] + G * (tr - M[4 * i]) : C01 * M[3 * i + j] + G * M[3 * j + i];
+      }
+    }
+
+    if (tid < NP) {
       if (A.Ke_out) {
         double *Ko = A.Ke_out + it * ND * ND;
 #pragma unroll
         for (int i = 0; i < 3; i++)
 #pragma unroll
           for (int j = 0; j < 3; j++) {
-            Ko[(3 * a + i) * ND + 3 * b + j] = v[3 * i + j];
-            Ko[(3 * b + j) * ND + 3 * a + i] = v[3 * i + j];
+            Ko[(3 * pa + i) * ND + 3 * pb + j] = v[3 * i + j];
+            Ko[(3 * pb + j) * ND + 3 * pa + i] = v[3 * i + j];
           }
       }
-      if (A.K) {
-        const uint8_t fa = sfix[a], fb = sfix[b];
-        double *Kab = A.K + (int64_t)A.slot[(e * NN + a) * NN + b] * 9;
-        double oab[9], oba[9];
+      if (Kab) {
+        const uint8_t fa = sfix[pa], fb = sfix[pb];
 #pragma unroll
-        for (int k = 0; k < 9; k++) oab[k] = Kab[k];
-        if (a != b) {
-          double *Kba = A.K + (int64_t)A.slot[(e * NN + b) * NN + a] * 9;
+        for (int i = 0; i < 3; i++)
 #pragma unroll
-          for (int k = 0; k < 9; k++) oba[k] = Kba[k];
-#pragma unroll
-          for (int i = 0; i < 3; i++)
-#pragma unroll
-            for (int j = 0; j < 3; j++)
-              if (!((fa >> i) & 1) && !((fb >> j) & 1)) {
-                Kab[3 * i + j] = oab[3 * i + j] + v[3 * i + j];
-                Kba[3 * j + i] = oba[3 * j + i] + v[3 * i + j];
-              }
-        } else {
-#pragma unroll
-          for (int i = 0; i < 3; i++)
-#pragma unroll
-            for (int j = 0; j < 3; j++)
-              if (!((fa >> i) & 1) && !((fb >> j) & 1)) Kab[3 * i + j] = oab[3 * i + j] + v[3 * i + j];
-        }
+          for (int j = 0; j < 3; j++)
+            if (!((fa >> i) & 1) && !((fb >> j) & 1)) {
+              Kab[3 * i + j] = oab[3 * i + j] + v[3 * i + j];
+              if (Kba) Kba[3 * j + i] = oba[3 * j + i] + v[3 * i + j];
+            }
       }
     }
   }
@@ -306,9 +269,9 @@ static cudaError_t dispatch(Ctx &c, const Bucket &B, ElemArgs a, int64_t count) 
     }
   } else if (B.type == FAST_ELEM_HEX20) {
     switch (ng) {
-      case 8: return run<20, 8, 256, MASS>(c, a, count);
-      case 27: return run<20, 27, 256, MASS>(c, a, count);
-      case 64: return run<20, 64, 256, MASS>(c, a, count);
+      case 8: return run<20, 8, 224, MASS>(c, a, count);
+      case 27: return run<20, 27, 224, MASS>(c, a, count);
+      case 64: return run<20, 64, 224, MASS>(c, a, count);
       default: break;
     }
   }

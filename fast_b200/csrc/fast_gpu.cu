@@ -44,7 +44,7 @@ void free_mesh(Ctx &c) {
   }
   c.buckets.clear();
   dfree(c.d_X); dfree(c.d_fix); dfree(c.d_dof_of_eq);
-  dfree(c.d_rowptr); dfree(c.d_col); dfree(c.d_diag);
+  dfree(c.d_rowptr); dfree(c.d_col); dfree(c.d_diag); dfree(c.d_srow); dfree(c.d_scol);
   dfree(c.d_K); dfree(c.d_M); dfree(c.d_Ks); dfree(c.d_Ms); dfree(c.d_Ks32);
   dfree(c.d_u); dfree(c.d_r); dfree(c.d_z); dfree(c.d_p); dfree(c.d_w); dfree(c.d_f); dfree(c.d_dinv);
   dfree(c.s_x); dfree(c.s_r); dfree(c.s_z); dfree(c.s_p); dfree(c.s_w); dfree(c.s_dinv);
@@ -74,13 +74,25 @@ void invalidate(Ctx &c, int what) {
 // row-local SoA copies for the solve (FP64, and FP32 when asked)
 cudaError_t ensure_soa(Ctx &c, int what, bool fp32) {
   cudaError_t e = cudaSuccess;
+  // padded rows: the padding values are zeroed once at allocation and never written
+  const size_t nv = (size_t)9 * c.nnzb_pad;
   if (what == FAST_ASM_MASS) {
-    if (!c.d_Ms && (e = cudaMalloc((void **)&c.d_Ms, sizeof(double) * 9 * c.nnzb)) != cudaSuccess) return e;
+    if (!c.d_Ms) {
+      if ((e = cudaMalloc((void **)&c.d_Ms, sizeof(double) * nv)) != cudaSuccess) return e;
+      if ((e = cudaMemsetAsync(c.d_Ms, 0, sizeof(double) * nv, c.stream)) != cudaSuccess) return e;
+    }
     if (!c.Ms_ok) { e = launch_to_soa(c, c.d_M, c.d_Ms, nullptr); c.Ms_ok = (e == cudaSuccess); }
     return e;
   }
-  if (!c.d_Ks && (e = cudaMalloc((void **)&c.d_Ks, sizeof(double) * 9 * c.nnzb)) != cudaSuccess) return e;
-  if (fp32 && !c.d_Ks32 && (e = cudaMalloc((void **)&c.d_Ks32, sizeof(float) * 9 * c.nnzb)) != cudaSuccess) return e;
+  if (!c.d_Ks) {
+    if ((e = cudaMalloc((void **)&c.d_Ks, sizeof(double) * nv)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(c.d_Ks, 0, sizeof(double) * nv, c.stream)) != cudaSuccess) return e;
+  }
+  if (fp32 && !c.d_Ks32) {
+    if ((e = cudaMalloc((void **)&c.d_Ks32, sizeof(float) * nv)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(c.d_Ks32, 0, sizeof(float) * nv, c.stream)) != cudaSuccess) return e;
+    c.Ks_ok = false;
+  }
   if (!c.Ks_ok) {
     // the FP32 copy is always refreshed with the FP64 one once it exists
     e = launch_to_soa(c, c.d_K, c.d_Ks, c.d_Ks32);
@@ -225,6 +237,10 @@ int fast_gpu_upload_mesh(fast_gpu_ctx *c, const fast_gpu_mesh *m) {
   CK(cudaMemcpy(c->d_col, c->h_col.data(), sizeof(int32_t) * c->nnzb, cudaMemcpyHostToDevice));
   CK(dalloc(&c->d_diag, nnode));
   CK(cudaMemcpy(c->d_diag, c->h_diag.data(), sizeof(int32_t) * nnode, cudaMemcpyHostToDevice));
+  CK(dalloc(&c->d_srow, nnode + 1));
+  CK(cudaMemcpy(c->d_srow, c->h_srow.data(), sizeof(int32_t) * (nnode + 1), cudaMemcpyHostToDevice));
+  CK(dalloc(&c->d_scol, c->nnzb_pad));
+  CK(cudaMemcpy(c->d_scol, c->h_scol.data(), sizeof(int32_t) * c->nnzb_pad, cudaMemcpyHostToDevice));
   for (int b = 0; b < m->num_buckets; b++) {
     const fast_gpu_bucket &bk = m->buckets[b];
     Bucket &B = c->buckets[b];
@@ -618,6 +634,7 @@ int fast_gpu_kernel_stats(fast_gpu_ctx *c, int32_t which, int64_t *launches, dou
     const double n4 = 4.0 * c->nnode;
     double algo = 0.0;
     // SpMV: block values + column indices + row pointers + x read once + y written once
+    // (the padding blocks of the solve layout are not counted: they are overhead)
     if (which == FAST_KERNEL_SPMV_FP64) algo = (double)c->nnzb * (9 * 8 + 4) + 4.0 * (c->nnode + 1) + 2.0 * 8 * n4;
     if (which == FAST_KERNEL_SPMV_FP32) algo = (double)c->nnzb * (9 * 4 + 4) + 4.0 * (c->nnode + 1) + 2.0 * 4 * n4;
     if (which == FAST_KERNEL_ASSEMBLE) {

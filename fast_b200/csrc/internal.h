@@ -80,6 +80,11 @@ struct Ctx {
   int64_t nnzb = 0;
   std::vector<int32_t> h_rowptr, h_col, h_diag;
   int32_t *d_rowptr = nullptr, *d_col = nullptr, *d_diag = nullptr;
+  // solve layout: each block-row padded to a multiple of 4 blocks, so its
+  // structure-of-arrays segments start on 16-byte boundaries (vector loads)
+  int64_t nnzb_pad = 0;
+  std::vector<int32_t> h_srow, h_scol;
+  int32_t *d_srow = nullptr, *d_scol = nullptr;
   int32_t ncolors = 0;
   double pattern_seconds = 0.0;
   int64_t nnz_lower_eq = 0;

@@ -121,6 +121,26 @@ bool build_pattern(Ctx &c, const fast_gpu_mesh &m) {
     if (p != b1 && *p == i) c.h_diag[i] = (int32_t)(p - c.h_col.data());
   }
 
+  // padded solve layout: rows rounded up to 4 blocks; padding columns point at
+  // the row itself and carry zero values
+  c.h_srow.assign(nnode + 1, 0);
+  {
+    int64_t acc = 0;
+    for (int64_t i = 0; i < nnode; i++) {
+      const int64_t nb = c.h_rowptr[i + 1] - c.h_rowptr[i];
+      acc += (nb + 3) & ~int64_t(3);
+      if (9 * acc > INT32_MAX) return c.set_error("padded pattern too large for 32-bit value indices");
+      c.h_srow[i + 1] = (int32_t)acc;
+    }
+    c.nnzb_pad = acc;
+    c.h_scol.assign(acc, 0);
+    for (int64_t i = 0; i < nnode; i++) {
+      const int32_t nb = c.h_rowptr[i + 1] - c.h_rowptr[i];
+      const int32_t nbp = c.h_srow[i + 1] - c.h_srow[i];
+      for (int32_t p = 0; p < nbp; p++) c.h_scol[c.h_srow[i] + p] = p < nb ? c.h_col[c.h_rowptr[i] + p] : (int32_t)i;
+    }
+  }
+
   // equation-space lower-triangle count (what the reference stores)
   {
     int64_t cnt = 0;

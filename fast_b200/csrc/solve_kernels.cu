@@ -17,12 +17,15 @@
 //
 // Layouts.  The assembly target is the node-block CSR with each 3x3 block
 // stored contiguously (AoS).  For the solve, each block-row is transposed
-// once per assembly into a row-local structure-of-arrays: entry k (0..8) of
-// block p of row n sits at 9*rowptr[n] + k*nb(n) + p.  One warp handles one
-// block-row, one lane one block, so each of the nine value loads is a
-// contiguous, fully coalesced warp access.  Vectors are padded to 4 entries
-// per node (x, y, z, 0) so a node's part of x is one 16-byte (FP32) or two
-// 16-byte (FP64) loads.
+// once per assembly into a row-local structure-of-arrays padded to a
+// multiple of 4 blocks: with s = srow[n] and nbp the padded row length,
+// entry k (0..8) of block p of row n sits at 9*s + k*nbp + p.  Every such
+// segment starts on a 16-byte boundary, so a lane loads 4 FP32 blocks
+// (float4 per entry) or 2 FP64 blocks (double2 per entry) at once and the
+// lanes of a row read consecutive 16-byte words.  Padding blocks hold zeros
+// and point at the row's own node.  Vectors are padded to 4 entries per node
+// (x, y, z, 0) so a node's part of x is one 16-byte (FP32) or two 16-byte
+// (FP64) loads.
 //
 // Every scalar lives on the device (PcgState) and every reduction uses a
 // fixed grid and a fixed combination order, so the host never waits inside
@@ -37,6 +40,8 @@ namespace fastgpu {
 
 constexpr int kSpmvThreads = 256;
 constexpr int kVecThreads = 256;
+constexpr int kLPR32 = 16;  // lanes per block-row, FP32 SpMV (4 blocks per lane trip)
+constexpr int kLPR64 = 16;  // lanes per block-row, FP64 SpMV (2 blocks per lane trip)
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -87,74 +92,147 @@ template <> struct V4<double> {
   }
 };
 
-// AoS blocks -> row-local SoA, FP64 and FP32 copies
+// AoS blocks -> padded row-local SoA, FP64 and FP32 copies
 __global__ void __launch_bounds__(256)
-aos_to_soa(int64_t nrows, const int32_t *__restrict__ rowptr, const double *__restrict__ K,
-           double *__restrict__ Ks, float *__restrict__ Ks32) {
+aos_to_soa(int64_t nrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ srow,
+           const double *__restrict__ K, double *__restrict__ Ks, float *__restrict__ Ks32) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t row = warp; row < nrows; row += nwarps) {
     const int32_t b0 = rowptr[row], nb = rowptr[row + 1] - b0;
-    const int64_t base = 9 * (int64_t)b0;
+    const int32_t s0 = srow[row], nbp = srow[row + 1] - s0;
+    const int64_t dst = 9 * (int64_t)s0;
     for (int p = lane; p < nb; p += 32) {
-      const double *src = K + base + 9 * p;
+      const double *src = K + 9 * ((int64_t)b0 + p);
 #pragma unroll
       for (int k = 0; k < 9; k++) {
         const double v = src[k];
-        if (Ks) Ks[base + (int64_t)k * nb + p] = v;
-        if (Ks32) Ks32[base + (int64_t)k * nb + p] = (float)v;
+        if (Ks) Ks[dst + (int64_t)k * nbp + p] = v;
+        if (Ks32) Ks32[dst + (int64_t)k * nbp + p] = (float)v;
       }
     }
   }
 }
 
-// y = K x (MODE 0, partial x.y) or y = b - K x (MODE 1, partial y.y); SoA rows, padded vectors.
-template <typename VT, typename XT, int MODE>
-__global__ void __launch_bounds__(kSpmvThreads)
-spmv_soa(int64_t nrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ col,
-         const VT *__restrict__ val, const XT *__restrict__ x, const XT *__restrict__ b, XT *__restrict__ y,
-         double *__restrict__ part, const int32_t *__restrict__ skip) {
+// Row epilogue shared by the SpMV kernels: y = K x (MODE 0, partial x.y) or
+// y = b - K x (MODE 1, partial y.y).
+template <typename XT, int MODE>
+__device__ __forceinline__ void spmv_row_out(int64_t row, XT a0, XT a1, XT a2, const XT *__restrict__ x,
+                                             const XT *__restrict__ b, XT *__restrict__ y, bool part,
+                                             double &pacc) {
+  if (MODE == 0) {
+    V4<XT>::store(y + 4 * row, a0, a1, a2);
+    if (part) {
+      XT x0, x1, x2;
+      V4<XT>::load(x + 4 * row, x0, x1, x2);
+      pacc += (double)x0 * a0 + (double)x1 * a1 + (double)x2 * a2;
+    }
+  } else {
+    XT b0, b1, b2;
+    V4<XT>::load(b + 4 * row, b0, b1, b2);
+    const XT y0 = b0 - a0, y1 = b1 - a1, y2 = b2 - a2;
+    V4<XT>::store(y + 4 * row, y0, y1, y2);
+    if (part) pacc += (double)y0 * y0 + (double)y1 * y1 + (double)y2 * y2;
+  }
+}
+
+// FP32 SpMV: LPR lanes per block-row; a lane takes 4 blocks per trip (one
+// int4 of columns, nine float4 of values, four float4 gathers of x): 14
+// independent 16-byte loads in flight per lane.
+template <int MODE, int LPR>
+__global__ void __launch_bounds__(kSpmvThreads, 4)
+spmv_f32(int64_t nrows, const int32_t *__restrict__ srow, const int32_t *__restrict__ scol,
+         const float *__restrict__ val, const float *__restrict__ x, const float *__restrict__ b,
+         float *__restrict__ y, double *__restrict__ part, const int32_t *__restrict__ skip) {
   if (skip && *skip) return;
   __shared__ double sbuf[32];
-  const int lane = threadIdx.x & 31;
+  constexpr int RPW = 32 / LPR;
+  const int lane = threadIdx.x & 31, q = lane % LPR;
+  const int64_t warp = (blockIdx.x * (int64_t)kSpmvThreads + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * kSpmvThreads) >> 5;
+  const float4 *__restrict__ x4 = reinterpret_cast<const float4 *>(x);
+  double pacc = 0.0;
+  for (int64_t row0 = warp * RPW; row0 < nrows; row0 += nwarps * RPW) {
+    const int64_t row = row0 + lane / LPR;
+    const bool live = row < nrows;
+    int32_t s0 = 0, nbp = 0;
+    if (live) {
+      s0 = srow[row];
+      nbp = srow[row + 1] - s0;
+    }
+    const float *__restrict__ vr = val + 9 * (int64_t)s0;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+    for (int j = 4 * q; j < nbp; j += 4 * LPR) {
+      const int4 c = *reinterpret_cast<const int4 *>(scol + s0 + j);
+      float4 v[9];
+#pragma unroll
+      for (int k = 0; k < 9; k++) v[k] = *reinterpret_cast<const float4 *>(vr + k * nbp + j);
+      const float4 xa = x4[c.x], xb = x4[c.y], xc = x4[c.z], xd = x4[c.w];
+      a0 += v[0].x * xa.x + v[1].x * xa.y + v[2].x * xa.z + v[0].y * xb.x + v[1].y * xb.y + v[2].y * xb.z +
+            v[0].z * xc.x + v[1].z * xc.y + v[2].z * xc.z + v[0].w * xd.x + v[1].w * xd.y + v[2].w * xd.z;
+      a1 += v[3].x * xa.x + v[4].x * xa.y + v[5].x * xa.z + v[3].y * xb.x + v[4].y * xb.y + v[5].y * xb.z +
+            v[3].z * xc.x + v[4].z * xc.y + v[5].z * xc.z + v[3].w * xd.x + v[4].w * xd.y + v[5].w * xd.z;
+      a2 += v[6].x * xa.x + v[7].x * xa.y + v[8].x * xa.z + v[6].y * xb.x + v[7].y * xb.y + v[8].y * xb.z +
+            v[6].z * xc.x + v[7].z * xc.y + v[8].z * xc.z + v[6].w * xd.x + v[7].w * xd.y + v[8].w * xd.z;
+    }
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) {
+      a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+      a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+      a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+    }
+    if (live && q == 0) spmv_row_out<float, MODE>(row, a0, a1, a2, x, b, y, part != nullptr, pacc);
+  }
+  if (part) {
+    const double t = block_sum<kSpmvThreads>(pacc, sbuf);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+  }
+}
+
+// FP64 SpMV: LPR lanes per block-row; a lane takes 2 blocks per trip (one
+// int2 of columns, nine double2 of values, two gathers of x).
+template <int MODE, int LPR>
+__global__ void __launch_bounds__(kSpmvThreads, 4)
+spmv_f64(int64_t nrows, const int32_t *__restrict__ srow, const int32_t *__restrict__ scol,
+         const double *__restrict__ val, const double *__restrict__ x, const double *__restrict__ b,
+         double *__restrict__ y, double *__restrict__ part, const int32_t *__restrict__ skip) {
+  if (skip && *skip) return;
+  __shared__ double sbuf[32];
+  constexpr int RPW = 32 / LPR;
+  const int lane = threadIdx.x & 31, q = lane % LPR;
   const int64_t warp = (blockIdx.x * (int64_t)kSpmvThreads + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * kSpmvThreads) >> 5;
   double pacc = 0.0;
-  for (int64_t row = warp; row < nrows; row += nwarps) {
-    const int32_t b0 = rowptr[row], nb = rowptr[row + 1] - b0;
-    const VT *__restrict__ vr = val + 9 * (int64_t)b0;
-    XT a0 = 0, a1 = 0, a2 = 0;
-    for (int p = lane; p < nb; p += 32) {
-      const int32_t c = col[b0 + p];
-      XT x0, x1, x2;
-      V4<XT>::load(x + 4 * (int64_t)c, x0, x1, x2);
-      VT v[9];
+  for (int64_t row0 = warp * RPW; row0 < nrows; row0 += nwarps * RPW) {
+    const int64_t row = row0 + lane / LPR;
+    const bool live = row < nrows;
+    int32_t s0 = 0, nbp = 0;
+    if (live) {
+      s0 = srow[row];
+      nbp = srow[row + 1] - s0;
+    }
+    const double *__restrict__ vr = val + 9 * (int64_t)s0;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int j = 2 * q; j < nbp; j += 2 * LPR) {
+      const int2 c = *reinterpret_cast<const int2 *>(scol + s0 + j);
+      double2 v[9];
 #pragma unroll
-      for (int k = 0; k < 9; k++) v[k] = vr[k * nb + p];
-      a0 += (XT)v[0] * x0 + (XT)v[1] * x1 + (XT)v[2] * x2;
-      a1 += (XT)v[3] * x0 + (XT)v[4] * x1 + (XT)v[5] * x2;
-      a2 += (XT)v[6] * x0 + (XT)v[7] * x1 + (XT)v[8] * x2;
+      for (int k = 0; k < 9; k++) v[k] = *reinterpret_cast<const double2 *>(vr + k * nbp + j);
+      double xa0, xa1, xa2, xb0, xb1, xb2;
+      V4<double>::load(x + 4 * (int64_t)c.x, xa0, xa1, xa2);
+      V4<double>::load(x + 4 * (int64_t)c.y, xb0, xb1, xb2);
+      a0 += v[0].x * xa0 + v[1].x * xa1 + v[2].x * xa2 + v[0].y * xb0 + v[1].y * xb1 + v[2].y * xb2;
+      a1 += v[3].x * xa0 + v[4].x * xa1 + v[5].x * xa2 + v[3].y * xb0 + v[4].y * xb1 + v[5].y * xb2;
+      a2 += v[6].x * xa0 + v[7].x * xa1 + v[8].x * xa2 + v[6].y * xb0 + v[7].y * xb1 + v[8].y * xb2;
     }
-    a0 = warp_sum(a0);
-    a1 = warp_sum(a1);
-    a2 = warp_sum(a2);
-    if (lane == 0) {
-      if (MODE == 0) {
-        V4<XT>::store(y + 4 * row, a0, a1, a2);
-        if (part) {
-          XT x0, x1, x2;
-          V4<XT>::load(x + 4 * row, x0, x1, x2);
-          pacc += (double)x0 * a0 + (double)x1 * a1 + (double)x2 * a2;
-        }
-      } else {
-        XT b0_, b1_, b2_;
-        V4<XT>::load(b + 4 * row, b0_, b1_, b2_);
-        const XT y0 = b0_ - a0, y1 = b1_ - a1, y2 = b2_ - a2;
-        V4<XT>::store(y + 4 * row, y0, y1, y2);
-        if (part) pacc += (double)y0 * y0 + (double)y1 * y1 + (double)y2 * y2;
-      }
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) {
+      a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+      a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+      a2 += __shfl_xor_sync(0xffffffffu, a2, o);
     }
+    if (live && q == 0) spmv_row_out<double, MODE>(row, a0, a1, a2, x, b, y, part != nullptr, pacc);
   }
   if (part) {
     const double t = block_sum<kSpmvThreads>(pacc, sbuf);
@@ -491,29 +569,29 @@ static double *P_D(Ctx &c) { return c.d_partials + 6144; }    // [R]  f.f
 static double *P_E(Ctx &c) { return c.d_partials + 8192; }    // [G]  true r.r
 
 cudaError_t launch_to_soa(Ctx &c, const double *K, double *Ks, float *Ks32) {
-  aos_to_soa<<<spmv_grid(c), 256, 0, c.stream>>>(c.nnode, c.d_rowptr, K, Ks, Ks32);
+  aos_to_soa<<<spmv_grid(c), 256, 0, c.stream>>>(c.nnode, c.d_rowptr, c.d_srow, K, Ks, Ks32);
   c.launches++;
   return cudaGetLastError();
 }
 
 cudaError_t launch_spmv(Ctx &c, const double *Ks, const double *x, double *y) {
-  spmv_soa<double, double, 0><<<spmv_grid(c), kSpmvThreads, 0, c.stream>>>(
-      c.nnode, c.d_rowptr, c.d_col, Ks, x, nullptr, y, nullptr, nullptr);
+  spmv_f64<0, kLPR64><<<spmv_grid(c), kSpmvThreads, 0, c.stream>>>(
+      c.nnode, c.d_srow, c.d_scol, Ks, x, nullptr, y, nullptr, nullptr);
   c.launches++;
   return cudaGetLastError();
 }
 
 cudaError_t launch_spmv32(Ctx &c, const float *Ks, const float *x, float *y) {
-  spmv_soa<float, float, 0><<<spmv_grid(c), kSpmvThreads, 0, c.stream>>>(
-      c.nnode, c.d_rowptr, c.d_col, Ks, x, nullptr, y, nullptr, nullptr);
+  spmv_f32<0, kLPR32><<<spmv_grid(c), kSpmvThreads, 0, c.stream>>>(
+      c.nnode, c.d_srow, c.d_scol, Ks, x, nullptr, y, nullptr, nullptr);
   c.launches++;
   return cudaGetLastError();
 }
 
 cudaError_t launch_residual(Ctx &c, const double *Ks, const double *f, const double *u, double *r, double *rr_out) {
   double *part = P_E(c);
-  spmv_soa<double, double, 1><<<spmv_grid(c), kSpmvThreads, 0, c.stream>>>(
-      c.nnode, c.d_rowptr, c.d_col, Ks, u, f, r, part, nullptr);
+  spmv_f64<1, kLPR64><<<spmv_grid(c), kSpmvThreads, 0, c.stream>>>(
+      c.nnode, c.d_srow, c.d_scol, Ks, u, f, r, part, nullptr);
   c.launches++;
   finish_sum<<<1, 256, 0, c.stream>>>(part, spmv_grid(c), rr_out);
   c.launches++;
@@ -596,7 +674,7 @@ cudaError_t pcg_fp64(Ctx &c, bool warm, double tol, int maxit, int chunk, int it
   PcgState *st = c.d_state;
   cudaError_t e;
   if (warm) {
-    spmv_soa<double, double, 1><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_rowptr, c.d_col, c.d_Ks, c.d_u, c.d_f,
+    spmv_f64<1, kLPR64><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, c.d_Ks, c.d_u, c.d_f,
                                                                    c.d_r, P_E(c), nullptr);
     c.launches++;
   } else {
@@ -611,7 +689,7 @@ cudaError_t pcg_fp64(Ctx &c, bool warm, double tol, int maxit, int chunk, int it
   return drive(c, maxit, chunk, [&](int k) -> cudaError_t {
     for (int i = 0; i < k; i++) {
       c.begin_span(0);
-      spmv_soa<double, double, 0><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_rowptr, c.d_col, c.d_Ks, c.d_p, nullptr,
+      spmv_f64<0, kLPR64><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, c.d_Ks, c.d_p, nullptr,
                                                                      c.d_w, P_A(c), &st->done);
       c.end_span();
       pcg_alpha<<<1, 256, 0, c.stream>>>(st, P_A(c), G);
@@ -639,7 +717,7 @@ cudaError_t pcg_mixed(Ctx &c, bool warm, double tol, int maxit, int chunk) {
   auto reliable = [&]() {
     flush_correction<<<R, 256, 0, c.stream>>>(4 * nn, c.d_u, c.s_x, st);
     c.begin_span(0);
-    spmv_soa<double, double, 1><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_rowptr, c.d_col, c.d_Ks, c.d_u, c.d_f,
+    spmv_f64<1, kLPR64><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, c.d_Ks, c.d_u, c.d_f,
                                                                    c.d_r, P_E(c), &st->final);
     c.end_span();
     replace_residual<<<R, kVecThreads, 0, c.stream>>>(nn, c.d_r, c.s_r, c.s_z, c.s_p, c.s_dinv, st, P_C(c));
@@ -651,7 +729,7 @@ cudaError_t pcg_mixed(Ctx &c, bool warm, double tol, int maxit, int chunk) {
   return drive(c, maxit, chunk, [&](int k) -> cudaError_t {
     for (int i = 0; i < k; i++) {
       c.begin_span(1);
-      spmv_soa<float, float, 0><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_rowptr, c.d_col, c.d_Ks32, c.s_p, nullptr,
+      spmv_f32<0, kLPR32><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, c.d_Ks32, c.s_p, nullptr,
                                                                    c.s_w, P_A(c), &st->done);
       c.end_span();
       pcg_alpha<<<1, 256, 0, c.stream>>>(st, P_A(c), G);
