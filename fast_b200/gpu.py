@@ -28,7 +28,7 @@ LIB_PATH = os.path.join(HERE, "libfastgpu.so")
 
 FAST_GPU_OK = 0
 ERRORS = {-1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ESTATE", -5: "ENONCONV", -6: "EDETJ", -7: "ENOTSUP",
-          -8: "ENOTFOUND"}
+          -8: "ENOTFOUND", -9: "ETOOBIG"}
 ELEM = {"hex8": 1, "hex20": 2}
 ASM_K, ASM_M = 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
@@ -41,7 +41,7 @@ EXPORTS = [
     "fast_gpu_update_material", "fast_gpu_zero", "fast_gpu_assemble", "fast_gpu_add", "fast_gpu_get",
     "fast_gpu_mult_vect", "fast_gpu_solve", "fast_gpu_solve_device", "fast_gpu_face_load_vector",
     "fast_gpu_get_lower_csr", "fast_gpu_element_matrices", "fast_gpu_launch_count", "fast_gpu_kernel_timing", "fast_gpu_kernel_stats",
-    "fast_gpu_inspect_pattern",
+    "fast_gpu_inspect_pattern", "fast_gpu_pcg_solve_noalloc",
 ]
 KERNEL_SPMV_FP64, KERNEL_SPMV_FP32, KERNEL_ASSEMBLE = 0, 1, 2
 
@@ -116,6 +116,8 @@ def load_library(path: str = LIB_PATH):
     L.fast_gpu_get_lower_csr.argtypes = [vp, ctypes.c_int32, _lp, _lp, _ip, _dp]
     L.fast_gpu_element_matrices.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, _dp]
     L.fast_gpu_launch_count.argtypes = [vp, _lp]
+    L.fast_gpu_pcg_solve_noalloc.argtypes = [ctypes.c_int32, vp, vp, vp, vp, vp, ctypes.c_double, ctypes.c_int32, vp,
+                                             ctypes.POINTER(SolveReport)]
     L.fast_gpu_inspect_pattern.argtypes = [ctypes.POINTER(Mesh), _lp, _lp, _ip, _ip, _ip, _ip]
     L.fast_gpu_kernel_timing.argtypes = [vp, ctypes.c_int32]
     L.fast_gpu_kernel_stats.argtypes = [vp, ctypes.c_int32, _lp, _dp, _dp]

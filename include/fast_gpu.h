@@ -43,6 +43,7 @@ extern "C" {
 #define FAST_GPU_EDETJ     -6   /* non-positive Jacobian determinant in an element */
 #define FAST_GPU_ENOTSUP   -7   /* element type / option not supported           */
 #define FAST_GPU_ENOTFOUND -8   /* (i, j) outside the sparsity pattern           */
+#define FAST_GPU_ETOOBIG   -9   /* system larger than an entry point's fixed limit */
 
 /* ---- element types (FAST readers elc/element.cpp:1985-2101) ----------- */
 #define FAST_ELEM_HEX8      1   /* %ELEMENT.BRICK8   cElmParam,  SHAPE_BRICK8  */
@@ -191,6 +192,28 @@ int fast_gpu_kernel_timing(fast_gpu_ctx *ctx, int32_t enable);
  * roofline numerator) of one timed kind since timing was enabled. */
 int fast_gpu_kernel_stats(fast_gpu_ctx *ctx, int32_t which, int64_t *launches, double *total_ms,
                           double *bytes_per_launch);
+
+/* ---- solve without device allocation ----------------------------------
+ * No counterpart in the reference.  For callers that cannot let a library
+ * allocate device memory (their own memory pool owns the device, or a
+ * cudaMalloc/cudaFree, which synchronises the device, would stall their other
+ * streams): FP64 Jacobi PCG, the same iteration and stopping test as
+ * fast_gpu_solve with FAST_PREC_FP64 / FAST_PRECOND_JACOBI, on a caller's
+ * equation-space CSR matrix (full symmetric storage: d_rowptr [num_eq+1],
+ * d_col / d_val [nnz]), load d_f and solution d_u [num_eq], all device
+ * memory.  Needs no context.  Work vectors live in a static device array of
+ * the library (20 MB on each device that loads it, held until exit), so
+ * num_eq is limited to 500000; a larger system is rejected with
+ * FAST_GPU_ETOOBIG before any CUDA call.  The first call on a device looks up
+ * that array's device address with the device current; make that first call
+ * before any stream capture.  Calls share the array and it keeps the last
+ * call's contents (each call re-initialises what it uses): calls that overlap
+ * on the GPU race.  Runs on cuda_stream (a cudaStream_t, NULL = legacy
+ * default stream) and synchronises it every 32 iterations; rep may be NULL
+ * (its true_rel_residual is not computed here and is set to -1). */
+int fast_gpu_pcg_solve_noalloc(int32_t num_eq, const int64_t *d_rowptr, const int32_t *d_col, const double *d_val,
+                               const double *d_f, double *d_u, double tol, int32_t maxit, void *cuda_stream,
+                               fast_gpu_solve_report *rep);
 
 #ifdef __cplusplus
 }
