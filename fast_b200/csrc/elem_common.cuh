@@ -1,0 +1,35 @@
+// elem_common.cuh - shared by the element kernels (private to libfastgpu).
+#pragma once
+
+#include <cstdint>
+
+namespace fastgpu {
+
+struct ElemArgs {
+  int64_t ne;                 // elements in this launch
+  const int32_t *index;       // optional: colour-sorted positions to process (else 0..ne-1 + offset)
+  int64_t offset;             // first colour-sorted element of this launch
+  const int32_t *conn;        // [*][NN]
+  const double *E, *nu, *rho;
+  const int32_t *slot;        // [*][NN][NN]
+  const double *X;            // [nnode][3]
+  const uint8_t *fix;         // [nnode]
+  const double *dN;           // [NG][NN][3]
+  const double *N;            // [NG][NN]
+  const double *w;            // [NG]
+  double *K;                  // block values [nnzb][3][3] or null
+  double *Ke_out;             // [ne][3NN][3NN] or null (unmasked element matrices)
+  int32_t *status;            // bit 0: non-positive Jacobian determinant
+  const double *U;            // [nnode][4] nodal displacements (total-Lagrangian / internal force)
+  double *G;                  // [nnode][4] internal force, added to (colour-safe) or null
+};
+
+// (a, b) pair index -> a <= b, row-major over the upper triangle
+__device__ __forceinline__ void pair_of(int p, int n, int &a, int &b) {
+  int r = 0;
+  while (p >= n - r) { p -= n - r; r++; }
+  a = r;
+  b = r + p;
+}
+
+}  // namespace fastgpu

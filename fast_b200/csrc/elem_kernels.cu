@@ -29,26 +29,10 @@
 // bit-identical from run to run.
 #include <cstdint>
 
+#include "elem_common.cuh"
 #include "internal.h"
 
 namespace fastgpu {
-
-struct ElemArgs {
-  int64_t ne;                 // elements in this launch
-  const int32_t *index;       // optional: colour-sorted positions to process (else 0..ne-1 + offset)
-  int64_t offset;             // first colour-sorted element of this launch
-  const int32_t *conn;        // [*][NN]
-  const double *E, *nu, *rho;
-  const int32_t *slot;        // [*][NN][NN]
-  const double *X;            // [nnode][3]
-  const uint8_t *fix;         // [nnode]
-  const double *dN;           // [NG][NN][3]
-  const double *N;            // [NG][NN]
-  const double *w;            // [NG]
-  double *K;                  // block values [nnzb][3][3] or null
-  double *Ke_out;             // [ne][3NN][3NN] or null (unmasked element matrices)
-  int32_t *status;            // bit 0: non-positive Jacobian determinant
-};
 
 template <int NN, int NG, bool MASS>
 struct ElemSmem {
@@ -61,14 +45,6 @@ struct ElemSmem {
   static constexpr int total = kN + kX + kJ + kC + kD;
   static constexpr size_t bytes = total * sizeof(double) + 2 * 256 + 64;
 };
-
-// (a, b) pair index -> a <= b, row-major over the upper triangle
-__device__ __forceinline__ void pair_of(int p, int n, int &a, int &b) {
-  int r = 0;
-  while (p >= n - r) { p -= n - r; r++; }
-  a = r;
-  b = r + p;
-}
 
 // One CTA integrates one element at a time (grid-stride over the colour).
 // Thread p < NP owns node pair (a, b), a <= b: it loads the pair's two slot
@@ -319,6 +295,7 @@ cudaError_t launch_assemble(Ctx &c, int what, double *target) {
   for (size_t b = 0; b < c.buckets.size(); b++) {
     const Bucket &B = c.buckets[b];
     if (what == FAST_ASM_MASS && !B.has_rho) continue;
+    if (what == FAST_ASM_STIFFNESS && B.tl) continue;  // tangent: launch_tl
     for (size_t k = 0; k + 1 < B.color_off.size(); k++) {
       ElemArgs a = base_args(c, B, target);
       a.offset = B.color_off[k];

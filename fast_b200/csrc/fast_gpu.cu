@@ -49,6 +49,7 @@ void free_mesh(Ctx &c) {
   dfree(c.d_u); dfree(c.d_r); dfree(c.d_z); dfree(c.d_p); dfree(c.d_w); dfree(c.d_f); dfree(c.d_dinv);
   dfree(c.s_x); dfree(c.s_r); dfree(c.s_z); dfree(c.s_p); dfree(c.s_w); dfree(c.s_dinv);
   dfree(c.d_eq_tmp);
+  dfree(c.d_disp); dfree(c.d_gint);
   if (c.h_eq_tmp) cudaFreeHost(c.h_eq_tmp);
   c.h_eq_tmp = nullptr;
   c.K_ok = c.M_ok = c.Ks_ok = c.Ms_ok = false;
@@ -218,6 +219,11 @@ int fast_gpu_upload_mesh(fast_gpu_ctx *c, const fast_gpu_mesh *m) {
     B.ne = bk.num_elems;
     if (B.ne <= 0 || !bk.conn || !bk.E || !bk.nu) { c->err = "upload_mesh: empty bucket"; return FAST_GPU_EINVAL; }
     B.has_rho = bk.rho != nullptr;
+    if (bk.formulation != FAST_FORM_SMALL_STRAIN && bk.formulation != FAST_FORM_TOTAL_LAGRANGIAN) {
+      c->err = "upload_mesh: unknown element formulation";
+      return FAST_GPU_ENOTSUP;
+    }
+    B.tl = bk.formulation == FAST_FORM_TOTAL_LAGRANGIAN;
   }
   if (!build_pattern(*c, *m)) return FAST_GPU_EINVAL;
 
@@ -279,6 +285,9 @@ int fast_gpu_upload_mesh(fast_gpu_ctx *c, const fast_gpu_mesh *m) {
   CK(dalloc(&c->s_w, n4)); CK(dalloc(&c->s_dinv, 12 * nnode));
   CK(cudaMemset(c->d_p, 0, sizeof(double) * n4));
   CK(cudaMemset(c->s_p, 0, sizeof(float) * n4));
+  CK(dalloc(&c->d_disp, n4));
+  CK(dalloc(&c->d_gint, n4));
+  CK(cudaMemset(c->d_disp, 0, sizeof(double) * n4));
   CK(dalloc(&c->d_eq_tmp, std::max<int64_t>(2 * (int64_t)c->neq, 1)));
   CK(cudaMallocHost((void **)&c->h_eq_tmp, sizeof(double) * std::max<int64_t>(2 * (int64_t)c->neq, 1)));
   return FAST_GPU_OK;
@@ -338,6 +347,47 @@ int fast_gpu_update_material(fast_gpu_ctx *c, int32_t b, const double *E, const 
   return FAST_GPU_OK;
 }
 
+int fast_gpu_set_displacement_device(fast_gpu_ctx *c, const double *d_u) {
+  if (check_ctx(c) || !d_u || !c->d_disp) return FAST_GPU_EINVAL;
+  CK(launch_eq_to_node(*c, d_u, c->d_disp));
+  return FAST_GPU_OK;
+}
+
+int fast_gpu_set_displacement(fast_gpu_ctx *c, const double *u) {
+  if (check_ctx(c) || !u || !c->d_disp) return FAST_GPU_EINVAL;
+  const size_t nb = sizeof(double) * c->neq;
+  CK(cudaStreamSynchronize(c->stream));
+  std::memcpy(c->h_eq_tmp, u, nb);
+  CK(cudaMemcpyAsync(c->d_eq_tmp, c->h_eq_tmp, nb, cudaMemcpyHostToDevice, c->stream));
+  CK(launch_eq_to_node(*c, c->d_eq_tmp, c->d_disp));
+  return FAST_GPU_OK;
+}
+
+int fast_gpu_internal_force_device(fast_gpu_ctx *c, double *d_g) {
+  if (check_ctx(c) || !d_g || !c->d_gint) return FAST_GPU_EINVAL;
+  CK(cudaMemsetAsync(c->d_status, 0, sizeof(int32_t), c->stream));
+  CK(cudaMemsetAsync(c->d_gint, 0, sizeof(double) * 4 * c->nnode, c->stream));
+  CK(launch_tl(*c, nullptr, c->d_gint, false, true));
+  CK(launch_node_to_eq(*c, c->d_gint, d_g));
+  return FAST_GPU_OK;
+}
+
+int fast_gpu_internal_force(fast_gpu_ctx *c, double *g) {
+  if (check_ctx(c) || !g) return FAST_GPU_EINVAL;
+  const int rc = fast_gpu_internal_force_device(c, c->d_eq_tmp);
+  if (rc != FAST_GPU_OK) return rc;
+  const size_t nb = sizeof(double) * c->neq;
+  CK(cudaMemcpyAsync(c->h_eq_tmp, c->d_eq_tmp, nb, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(c->h_status, c->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  std::memcpy(g, c->h_eq_tmp, nb);
+  if (c->h_status[0] & 1) {
+    c->err = "internal_force: non-positive Jacobian determinant in at least one element";
+    return FAST_GPU_EDETJ;
+  }
+  return FAST_GPU_OK;
+}
+
 int fast_gpu_zero(fast_gpu_ctx *c, int32_t what) {
   if (check_ctx(c) || !c->d_K) return FAST_GPU_ESTATE;
   if (what == FAST_ASM_MASS && !c->d_M) CK(dalloc(&c->d_M, 9 * c->nnzb));
@@ -358,6 +408,7 @@ int fast_gpu_assemble(fast_gpu_ctx *c, int32_t what) {
   if (what == FAST_ASM_STIFFNESS) c->begin_span(2);
   CK(launch_zero_matrix(*c, T, what == FAST_ASM_STIFFNESS));
   CK(launch_assemble(*c, what, T));
+  if (what == FAST_ASM_STIFFNESS) CK(launch_tl(*c, T, nullptr, true, false));
   if (what == FAST_ASM_STIFFNESS) c->end_span();
   CK(cudaMemcpyAsync(c->h_status, c->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -561,8 +612,9 @@ int fast_gpu_element_matrices(fast_gpu_ctx *c, int32_t what, int32_t b, int64_t 
   const Bucket &B = c->buckets[b];
   if (first < 0 || count <= 0 || first + count > B.ne) return FAST_GPU_EINVAL;
   if (what == FAST_ASM_MASS && !B.has_rho) { c->err = "element_matrices: bucket has no density"; return FAST_GPU_ESTATE; }
+  if (what != FAST_ASM_STIFFNESS && what != FAST_ASM_MASS && what != FAST_ASM_INTERNAL_FORCE) return FAST_GPU_EINVAL;
   const int nd = 3 * B.nn;
-  const size_t mat_bytes = sizeof(double) * (size_t)count * nd * nd;
+  const size_t mat_bytes = sizeof(double) * (size_t)count * (what == FAST_ASM_INTERNAL_FORCE ? nd : nd * nd);
   double *buf = nullptr;
   CK(cudaMalloc((void **)&buf, mat_bytes + sizeof(int32_t) * count + 16));
   std::vector<int32_t> idx(count);
@@ -570,7 +622,11 @@ int fast_gpu_element_matrices(fast_gpu_ctx *c, int32_t what, int32_t b, int64_t 
   cudaError_t e = cudaMemcpyAsync((char *)buf + mat_bytes, idx.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice, c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(buf, 0, mat_bytes, c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->d_status, 0, sizeof(int32_t), c->stream);
-  if (e == cudaSuccess) e = launch_element_matrices(*c, what, b, 0, count, buf);
+  if (e == cudaSuccess) {
+    if (what == FAST_ASM_INTERNAL_FORCE) e = launch_tl_element(*c, 1, b, count, buf);
+    else if (what == FAST_ASM_STIFFNESS && B.tl) e = launch_tl_element(*c, 0, b, count, buf);
+    else e = launch_element_matrices(*c, what, b, 0, count, buf);
+  }
   if (e == cudaSuccess) e = cudaMemcpyAsync(Ke, buf, mat_bytes, cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   cudaFree(buf);

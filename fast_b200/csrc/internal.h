@@ -51,6 +51,7 @@ struct Bucket {
   std::vector<int32_t> h_conn;     // colour-sorted incidence
   std::vector<int32_t> h_slot;     // colour-sorted slot map (freed after upload)
   bool has_rho = false;
+  int tl = 0;                      // 1: total-Lagrangian (St. Venant-Kirchhoff) formulation
   int32_t *d_conn = nullptr;       // [ne][nn] colour-sorted
   double *d_E = nullptr, *d_nu = nullptr, *d_rho = nullptr;
   int32_t *d_slot = nullptr;       // [ne][nn][nn] block index of node pair (a, b)
@@ -98,6 +99,9 @@ struct Ctx {
   int32_t *d_status = nullptr;    // device error flags (detJ)
   int32_t *h_status = nullptr;    // pinned
 
+  // nodal displacement state (TL tangent, internal force) and internal force
+  double *d_disp = nullptr;       // [nnode][4]
+  double *d_gint = nullptr;       // [nnode][4]
   // solver workspace: node vectors padded to 4 entries (x, y, z, 0) per node
   double *d_u = nullptr, *d_r = nullptr, *d_z = nullptr, *d_p = nullptr, *d_w = nullptr, *d_f = nullptr;
   double *d_dinv = nullptr;       // [nnode][3][4] inverse diagonal (Jacobi) or inverse 3x3 block
@@ -142,6 +146,10 @@ cudaError_t launch_zero_matrix(Ctx &c, double *K, bool identity_on_fixed);
 cudaError_t launch_assemble(Ctx &c, int what, double *target);
 cudaError_t launch_element_matrices(Ctx &c, int what, int bucket, int64_t first_sorted, int64_t count,
                                     double *d_out);
+
+// tl_kernels.cu
+cudaError_t launch_tl(Ctx &c, double *K, double *G, bool want_k, bool want_g);
+cudaError_t launch_tl_element(Ctx &c, int what, int bucket, int64_t count, double *d_out_and_index);
 
 constexpr int kRedBlocks = 592;   // fixed reduction grid: 4 x 148 SMs
 cudaError_t launch_build_precond(Ctx &c, const double *K, int precond);

@@ -1,0 +1,254 @@
+// nr.cu - load-control Newton-Raphson on the device.
+//
+// Mirrors cCtrlNR::Solver (ctrl/ctrlnr.cpp:47-270) with proportional loading:
+//
+//   q = external load, u = 0, g = IntForce(u), lambda = 0
+//   for each step: lambda += dlambda; f = lambda q; r = f - g
+//     for each iteration: K = tangent at u; solve K du = r; u += du;
+//                         g = IntForce(u); r = f - g
+//                         converged when |r| / max(1, |f|) < tol
+//                         (cControl::Convergence, ctrl/ctrl.cpp:1366-1413)
+//
+// Everything stays on the device; the host reads two norms per iteration.
+// The reference starts each step from the last converged u; a secant
+// predictor (u_k + (u_k - u_{k-1}) for equal steps) and a caller-supplied
+// predictor (e.g. a learned one) can start it elsewhere.  A predicted start is
+// only taken if its residual is smaller than the residual of the secant
+// start; Newton always iterates to the same tolerance.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "internal.h"
+
+namespace fastgpu {
+
+namespace {
+
+constexpr int kNrBlocks = 592;
+
+__global__ void nr_axpby(int32_t n, double a, const double *__restrict__ x, double b, const double *__restrict__ y,
+                         double *__restrict__ z) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    z[i] = a * x[i] + b * y[i];
+}
+
+__device__ __forceinline__ double nr_warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// fixed-order sums of squares of two vectors: part[0][blk], part[1][blk]
+__global__ void __launch_bounds__(256) nr_sumsq2(int32_t n, const double *__restrict__ x, const double *__restrict__ y,
+                                                double *__restrict__ part) {
+  __shared__ double s0[8], s1[8];
+  double a = 0.0, b = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    a += x[i] * x[i];
+    if (y) b += y[i] * y[i];
+  }
+  a = nr_warp_sum(a);
+  b = nr_warp_sum(b);
+  if ((threadIdx.x & 31) == 0) { s0[threadIdx.x >> 5] = a; s1[threadIdx.x >> 5] = b; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double ta = 0.0, tb = 0.0;
+    for (int w = 0; w < 8; w++) { ta += s0[w]; tb += s1[w]; }
+    part[blockIdx.x] = ta;
+    part[kNrBlocks + blockIdx.x] = tb;
+  }
+}
+
+__global__ void __launch_bounds__(256) nr_finish2(const double *__restrict__ part, double *__restrict__ out) {
+  __shared__ double s0[8], s1[8];
+  double a = 0.0, b = 0.0;
+  for (int i = threadIdx.x; i < kNrBlocks; i += blockDim.x) { a += part[i]; b += part[kNrBlocks + i]; }
+  a = nr_warp_sum(a);
+  b = nr_warp_sum(b);
+  if ((threadIdx.x & 31) == 0) { s0[threadIdx.x >> 5] = a; s1[threadIdx.x >> 5] = b; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double ta = 0.0, tb = 0.0;
+    for (int w = 0; w < 8; w++) { ta += s0[w]; tb += s1[w]; }
+    out[0] = ta;
+    out[1] = tb;
+  }
+}
+
+}  // namespace
+
+struct NrWork {
+  double *q = nullptr, *f = nullptr, *g = nullptr, *r = nullptr, *u = nullptr, *du = nullptr, *up = nullptr,
+         *ucand = nullptr, *part = nullptr, *sums = nullptr, *hsums = nullptr;
+};
+
+static cudaError_t axpby(Ctx &c, double a, const double *x, double b, const double *y, double *z) {
+  nr_axpby<<<kNrBlocks, 256, 0, c.stream>>>(c.neq, a, x, b, y, z);
+  c.launches++;
+  return cudaGetLastError();
+}
+
+// |x|^2 and |y|^2 read back to the host (y may be null)
+static cudaError_t norms2(Ctx &c, NrWork &w, const double *x, const double *y, double *nx, double *ny) {
+  nr_sumsq2<<<kNrBlocks, 256, 0, c.stream>>>(c.neq, x, y, w.part);
+  nr_finish2<<<1, 256, 0, c.stream>>>(w.part, w.sums);
+  c.launches += 2;
+  cudaError_t e = cudaMemcpyAsync(w.hsums, w.sums, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+  *nx = w.hsums[0];
+  if (ny) *ny = w.hsums[1];
+  return e;
+}
+
+}  // namespace fastgpu
+
+using namespace fastgpu;
+
+struct fast_gpu_ctx : public Ctx {};
+
+#define NRCK(call)                                                           \
+  do {                                                                       \
+    cudaError_t _e = (call);                                                 \
+    if (_e != cudaSuccess) {                                                 \
+      c->err = std::string("nr_solve: ") + cudaGetErrorString(_e);          \
+      rc = FAST_GPU_ECUDA;                                                   \
+      goto done;                                                             \
+    }                                                                        \
+  } while (0)
+#define NRRC(call)                   \
+  do {                               \
+    rc = (call);                     \
+    if (rc != FAST_GPU_OK) goto done; \
+  } while (0)
+
+extern "C" int fast_gpu_nr_solve(fast_gpu_ctx *c, const double *q_host, const fast_gpu_nr_opts *o,
+                                 fast_gpu_nr_predictor predictor, void *predictor_user, double *u_hist,
+                                 int32_t *iters, fast_gpu_nr_report *rep) {
+  if (!c || !q_host || !o || o->steps <= 0 || o->max_iter <= 0) return FAST_GPU_EINVAL;
+  if (!c->d_K) { c->err = "nr_solve: no mesh"; return FAST_GPU_ESTATE; }
+  const int32_t n = c->neq;
+  const size_t nb = sizeof(double) * n;
+  NrWork w;
+  int rc = FAST_GPU_OK;
+  fast_gpu_nr_report R{};
+  double lam = 0.0, flen2 = 0.0, rlen2 = 0.0, glen2 = 0.0, best = 0.0;
+  bool use_secant = true;
+  std::vector<double> hq;
+  const double tol = o->tol > 0 ? o->tol : 1e-5;
+  if (n <= 0) return FAST_GPU_EINVAL;
+  {
+    cudaError_t e = cudaSuccess;
+    double **bufs[] = {&w.q, &w.f, &w.g, &w.r, &w.u, &w.du, &w.up, &w.ucand};
+    for (double **b : bufs)
+      if (e == cudaSuccess) e = cudaMalloc((void **)b, nb);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&w.part, sizeof(double) * 2 * kNrBlocks);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&w.sums, sizeof(double) * 2);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&w.hsums, sizeof(double) * 2);
+    NRCK(e);
+  }
+  hq.assign(q_host, q_host + n);
+  NRCK(cudaMemcpyAsync(w.q, hq.data(), nb, cudaMemcpyHostToDevice, c->stream));
+  NRCK(cudaMemsetAsync(w.u, 0, nb, c->stream));
+  NRCK(cudaMemsetAsync(w.up, 0, nb, c->stream));
+  NRRC(fast_gpu_set_displacement_device(c, w.u));
+  NRRC(fast_gpu_internal_force_device(c, w.g));  // initial stresses (zero for these models)
+
+  for (int step = 1; step <= o->steps; step++) {
+    const double lam_prev = lam;
+    lam += o->step_factor;
+    NRCK(axpby(*c, lam, w.q, 0.0, w.q, w.f));  // f = lambda q
+
+    // start of the step: the last converged u (the reference), the secant
+    // extrapolation 2 u_k - u_{k-1} (equal load steps), or the caller's
+    // prediction when its residual is smaller than the secant start's
+    NRCK(cudaMemcpyAsync(w.ucand, w.u, nb, cudaMemcpyDeviceToDevice, c->stream));
+    if (step >= 2 && o->predictor != FAST_NR_PREDICT_NONE) {
+      NRCK(axpby(*c, 2.0, w.u, -1.0, w.up, w.ucand));
+      NRRC(fast_gpu_set_displacement_device(c, w.ucand));
+      NRRC(fast_gpu_internal_force_device(c, w.g));
+      NRCK(axpby(*c, 1.0, w.f, -1.0, w.g, w.r));
+      NRCK(norms2(*c, w, w.r, nullptr, &best, nullptr));
+      R.secant_starts++;
+      use_secant = true;
+      if (o->predictor == FAST_NR_PREDICT_CALLBACK && predictor) {
+        // the caller writes its prediction of u at this load level into du
+        const int prc = predictor(predictor_user, step, lam, w.u, w.up, w.du);
+        if (prc == 0) {
+          NRRC(fast_gpu_set_displacement_device(c, w.du));
+          NRRC(fast_gpu_internal_force_device(c, w.g));
+          NRCK(axpby(*c, 1.0, w.f, -1.0, w.g, w.r));
+          double rl = 0.0;
+          NRCK(norms2(*c, w, w.r, nullptr, &rl, nullptr));
+          R.predictions++;
+          if (rl < best) {
+            use_secant = false;
+            R.predictions_accepted++;
+            NRCK(cudaMemcpyAsync(w.ucand, w.du, nb, cudaMemcpyDeviceToDevice, c->stream));
+          }
+        }
+      }
+    }
+    NRCK(cudaMemcpyAsync(w.up, w.u, nb, cudaMemcpyDeviceToDevice, c->stream));  // last converged
+    NRCK(cudaMemcpyAsync(w.u, w.ucand, nb, cudaMemcpyDeviceToDevice, c->stream));
+    NRRC(fast_gpu_set_displacement_device(c, w.u));
+    NRRC(fast_gpu_internal_force_device(c, w.g));
+    NRCK(axpby(*c, 1.0, w.f, -1.0, w.g, w.r));  // r = f - g
+    NRCK(norms2(*c, w, w.r, w.f, &rlen2, &flen2));
+    (void)use_secant;
+
+    int conv = 0, it = 0;
+    for (it = 1; it <= o->max_iter; it++) {
+      NRRC(fast_gpu_assemble(c, FAST_ASM_STIFFNESS));  // tangent at u
+      fast_gpu_solve_opts lo = o->lin;
+      if (o->lin_tol_rel > 0) {
+        // inexact Newton: the linear tolerance follows the current residual
+        const double err = std::sqrt(rlen2) / std::max(1.0, std::sqrt(flen2));
+        lo.tol = std::min(o->lin_tol_max > 0 ? o->lin_tol_max : 1e-2, std::max(o->lin_tol_min > 0 ? o->lin_tol_min : 1e-12,
+                                                                                o->lin_tol_rel * err));
+      }
+      fast_gpu_solve_report lr{};
+      NRCK(cudaMemsetAsync(w.du, 0, nb, c->stream));
+      rc = fast_gpu_solve_device(c, w.r, w.du, &lo, &lr);
+      R.linear_iterations += lr.iterations;
+      if (rc != FAST_GPU_OK && rc != FAST_GPU_ENONCONV) goto done;
+      rc = FAST_GPU_OK;
+      NRCK(axpby(*c, 1.0, w.u, 1.0, w.du, w.u));  // u += du
+      NRRC(fast_gpu_set_displacement_device(c, w.u));
+      NRRC(fast_gpu_internal_force_device(c, w.g));
+      NRCK(axpby(*c, 1.0, w.f, -1.0, w.g, w.r));  // r = f - g
+      NRCK(norms2(*c, w, w.r, w.f, &rlen2, &flen2));
+      R.iterations++;
+      const double flen = std::sqrt(flen2), rlen = std::sqrt(rlen2);
+      double err;
+      if (flen > tol) {
+        err = rlen / std::max(1.0, flen);
+      } else {
+        NRCK(norms2(*c, w, w.g, nullptr, &glen2, nullptr));
+        err = rlen / std::max(1.0, std::sqrt(glen2));
+      }
+      R.last_err = err;
+      R.last_rel_residual = flen > 0 ? rlen / flen : rlen;
+      if (err < tol) { conv = 1; break; }
+      if (!std::isfinite(err)) break;
+    }
+    if (iters) iters[step - 1] = conv ? it : -1;
+    if (!conv) {
+      c->err = "nr_solve: Newton iterations did not converge (\"Convergence not achived\")";
+      R.failed_step = step;
+      rc = FAST_GPU_ENONCONV;
+      goto done;
+    }
+    R.converged_steps = step;
+    if (u_hist) {
+      NRCK(cudaMemcpyAsync(u_hist + (size_t)(step - 1) * n, w.u, nb, cudaMemcpyDeviceToHost, c->stream));
+      NRCK(cudaStreamSynchronize(c->stream));
+    }
+  }
+done:
+  if (rep) *rep = R;
+  if (w.hsums) cudaFreeHost(w.hsums);
+  for (double *p : {w.q, w.f, w.g, w.r, w.u, w.du, w.up, w.ucand, w.part, w.sums})
+    if (p) cudaFree(p);
+  return rc;
+}

@@ -138,12 +138,6 @@ class Deck:
 # --------------------------------------------------------------------------
 # structured boxes
 
-def _grid_index(shape, order):
-    """Map grid coordinates to node numbers with the given fastest-first axis order."""
-    idx = -np.ones(shape, dtype=np.int64)
-    return idx
-
-
 def box_mesh(kind: str, n, L, origin=(0.0, 0.0, 0.0), fastest=None) -> tuple:
     """Structured box of hex8 or hex20 elements.
 
@@ -252,6 +246,53 @@ def box_hex20_lognormal(nx=64, ny=64, nz=32, L=(4.0, 4.0, 2.0), median=1000.0, s
                 fe, fc, np.tile([0.0, 0.0, -pressure], (len(fe), 1)), np.zeros(len(fe), np.int32),
                 matrix_type="sparse", tol=1e-10, maxit=100000,
                 title=f"hex20 lognormal box {nx}x{ny}x{nz} seed {seed}")
+
+
+def plate_tl_hex8(nx=40, ny=40, nz=4, L=10.0, t=1.0, E=1000.0, nu=0.3, pressure=1.0, steps=40,
+                  tol=1e-8, maxit=30) -> Deck:
+    """Total-Lagrangian (St. Venant-Kirchhoff) hex8 plate under transverse pressure.
+
+    L x L x t plate of nx x ny x nz hex8 elements (%ELEMENT.BRICK8TL), 2x2x2
+    Gauss points; every node on the four side faces pinned (u = v = w = 0);
+    uniform pressure on the top face (traction -pressure in z).  Load-control
+    Newton-Raphson ('lcm', proportional loading) over `steps` equal steps to
+    the full pressure.
+    """
+    coords, conn, _ = box_mesh("hex8", (nx, ny, nz), (L, L, t))
+    ne = conn.shape[0]
+    fixed = np.zeros((coords.shape[0], 3), bool)
+    side = ((np.abs(coords[:, 0]) < 1e-12) | (np.abs(coords[:, 0] - L) < 1e-12) |
+            (np.abs(coords[:, 1]) < 1e-12) | (np.abs(coords[:, 1] - L) < 1e-12))
+    fixed[side] = True
+    fe, fc = _boundary_faces_fast("hex8", coords, conn, 2, t)
+    return Deck("hex8", coords, conn, np.full(ne, E), np.full(ne, nu), (2, 2, 2), fixed,
+                fe, fc, np.tile([0.0, 0.0, -pressure], (len(fe), 1)), np.zeros(len(fe), np.int32),
+                total_lagrangian=True, algorithm="lcm", matrix_type="skyline", tol=tol, maxit=maxit,
+                maxstep=steps, step_factor=1.0 / steps,
+                title=f"TL hex8 plate {nx}x{ny}x{nz}, pressure {pressure}, {steps} steps")
+
+
+def read_pos_displacements(path: str, labels=None) -> np.ndarray:
+    """Nodal displacements of every printed step of a FAST .pos file: [steps][nnode][3].
+
+    Reads the %RESULT.CASE.STEP.NODAL.DISPLACEMENT blocks (written by
+    cControl::PrintResult); rows are ordered by node label.
+    """
+    steps = []
+    with open(path) as fp:
+        lines = fp.read().splitlines()
+    i = 0
+    while i < len(lines):
+        if lines[i].strip() == "%RESULT.CASE.STEP.NODAL.DISPLACEMENT":
+            n = int(lines[i + 1].split()[0])
+            rows = [lines[i + 2 + k].split() for k in range(n)]
+            lab = np.array([int(r[0]) for r in rows])
+            u = np.array([[float(v) for v in r[1:4]] for r in rows])
+            steps.append(u[np.argsort(lab)])
+            i += 2 + n
+        else:
+            i += 1
+    return np.asarray(steps)
 
 
 # --------------------------------------------------------------------------

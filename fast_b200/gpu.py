@@ -30,7 +30,8 @@ FAST_GPU_OK = 0
 ERRORS = {-1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ESTATE", -5: "ENONCONV", -6: "EDETJ", -7: "ENOTSUP",
           -8: "ENOTFOUND", -9: "ETOOBIG"}
 ELEM = {"hex8": 1, "hex20": 2}
-ASM_K, ASM_M = 1, 2
+ASM_K, ASM_M, ASM_G = 1, 2, 3
+FORM_SMALL, FORM_TL = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 PRECOND_JACOBI, PRECOND_BLOCK_JACOBI = 0, 1
 
@@ -41,7 +42,9 @@ EXPORTS = [
     "fast_gpu_update_material", "fast_gpu_zero", "fast_gpu_assemble", "fast_gpu_add", "fast_gpu_get",
     "fast_gpu_mult_vect", "fast_gpu_solve", "fast_gpu_solve_device", "fast_gpu_face_load_vector",
     "fast_gpu_get_lower_csr", "fast_gpu_element_matrices", "fast_gpu_launch_count", "fast_gpu_kernel_timing", "fast_gpu_kernel_stats",
-    "fast_gpu_inspect_pattern", "fast_gpu_pcg_solve_noalloc",
+    "fast_gpu_inspect_pattern", "fast_gpu_pcg_solve_noalloc", "fast_gpu_set_displacement",
+    "fast_gpu_set_displacement_device", "fast_gpu_internal_force", "fast_gpu_internal_force_device",
+    "fast_gpu_nr_solve",
 ]
 KERNEL_SPMV_FP64, KERNEL_SPMV_FP32, KERNEL_ASSEMBLE = 0, 1, 2
 
@@ -55,7 +58,8 @@ class FastGpuError(RuntimeError):
 class Bucket(ctypes.Structure):
     _fields_ = [("elem_type", ctypes.c_int32), ("ngp", ctypes.c_int32 * 3), ("num_elems", ctypes.c_int64),
                 ("conn", ctypes.POINTER(ctypes.c_int32)), ("E", ctypes.POINTER(ctypes.c_double)),
-                ("nu", ctypes.POINTER(ctypes.c_double)), ("rho", ctypes.POINTER(ctypes.c_double))]
+                ("nu", ctypes.POINTER(ctypes.c_double)), ("rho", ctypes.POINTER(ctypes.c_double)),
+                ("formulation", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class Mesh(ctypes.Structure):
@@ -77,6 +81,30 @@ class SolveReport(ctypes.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class NrOpts(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_int32), ("max_iter", ctypes.c_int32), ("step_factor", ctypes.c_double),
+                ("tol", ctypes.c_double), ("predictor", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("lin", SolveOpts), ("lin_tol_rel", ctypes.c_double), ("lin_tol_min", ctypes.c_double),
+                ("lin_tol_max", ctypes.c_double)]
+
+
+class NrReport(ctypes.Structure):
+    _fields_ = [("converged_steps", ctypes.c_int32), ("failed_step", ctypes.c_int32),
+                ("iterations", ctypes.c_int32), ("linear_iterations", ctypes.c_int32),
+                ("secant_starts", ctypes.c_int32), ("predictions", ctypes.c_int32),
+                ("predictions_accepted", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("last_err", ctypes.c_double), ("last_rel_residual", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+# int (*)(void *user, int32 step, double lambda, const double *d_u_last, const double *d_u_prev, double *d_u_pred)
+NR_PREDICTOR = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int32, ctypes.c_double, ctypes.c_void_p,
+                                ctypes.c_void_p, ctypes.c_void_p)
+PREDICT_NONE, PREDICT_SECANT, PREDICT_CALLBACK = 0, 1, 2
 
 
 _lib = None
@@ -119,6 +147,12 @@ def load_library(path: str = LIB_PATH):
     L.fast_gpu_pcg_solve_noalloc.argtypes = [ctypes.c_int32, vp, vp, vp, vp, vp, ctypes.c_double, ctypes.c_int32, vp,
                                              ctypes.POINTER(SolveReport)]
     L.fast_gpu_inspect_pattern.argtypes = [ctypes.POINTER(Mesh), _lp, _lp, _ip, _ip, _ip, _ip]
+    L.fast_gpu_set_displacement.argtypes = [vp, _dp]
+    L.fast_gpu_set_displacement_device.argtypes = [vp, vp]
+    L.fast_gpu_internal_force.argtypes = [vp, _dp]
+    L.fast_gpu_internal_force_device.argtypes = [vp, vp]
+    L.fast_gpu_nr_solve.argtypes = [vp, _dp, ctypes.POINTER(NrOpts), NR_PREDICTOR, vp, _dp, _ip,
+                                    ctypes.POINTER(NrReport)]
     L.fast_gpu_kernel_timing.argtypes = [vp, ctypes.c_int32]
     L.fast_gpu_kernel_stats.argtypes = [vp, ctypes.c_int32, _lp, _dp, _dp]
     _lib = L
@@ -156,7 +190,8 @@ def _mesh_struct(deck: _decks.Deck):
     nu = np.ascontiguousarray(deck.nu, dtype=np.float64)
     rho = None if deck.rho is None else np.ascontiguousarray(deck.rho, dtype=np.float64)
     b = Bucket(ELEM[deck.kind], (ctypes.c_int32 * 3)(*deck.ngp), deck.num_elems, _p(conn, _ip), _p(E), _p(nu),
-               _p(rho) if rho is not None else ctypes.POINTER(ctypes.c_double)())
+               _p(rho) if rho is not None else ctypes.POINTER(ctypes.c_double)(),
+               FORM_TL if deck.total_lagrangian else FORM_SMALL, 0)
     buckets = (Bucket * 1)(b)
     m = Mesh(deck.num_nodes, _p(coords), _p(eq, _ip), int(eq.max(initial=0)), 1, buckets)
     return m, (coords, eq, conn, E, nu, rho, buckets)
@@ -241,6 +276,34 @@ class GpuSystem:
         nup = _p(np.ascontiguousarray(nu, dtype=np.float64)) if nu is not None else _dp()
         self._ck(self.L.fast_gpu_update_material(self.ctx, bucket, Ep, nup), "update_material")
 
+    # -- displacement state and internal force
+    def set_displacement(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        self._ck(self.L.fast_gpu_set_displacement(self.ctx, _p(u)), "set_displacement")
+
+    def internal_force(self):
+        g = np.zeros(self.neq)
+        self._ck(self.L.fast_gpu_internal_force(self.ctx, _p(g)), "internal_force")
+        return g
+
+    # -- load-control Newton-Raphson (cCtrlNR::Solver)
+    def nr_solve(self, q, steps, step_factor, tol=1e-8, max_iter=30, predictor=PREDICT_NONE, callback=None,
+                 precision=PREC_FP64, precond=PRECOND_JACOBI, lin_tol=1e-12, lin_tol_rel=0.0, lin_tol_min=1e-12,
+                 lin_tol_max=1e-2, keep_history=True, raise_on_fail=True):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        lin = SolveOpts(precision, precond, 0, 0, float(lin_tol), 0.0, 0, 0)
+        o = NrOpts(int(steps), int(max_iter), float(step_factor), float(tol), int(predictor), 0, lin,
+                   float(lin_tol_rel), float(lin_tol_min), float(lin_tol_max))
+        hist = np.zeros((steps, self.neq)) if keep_history else None
+        iters = np.zeros(steps, np.int32)
+        rep = NrReport()
+        cb = callback if callback is not None else NR_PREDICTOR()
+        rc = self.L.fast_gpu_nr_solve(self.ctx, _p(q), ctypes.byref(o), cb, None,
+                                      _p(hist) if hist is not None else _dp(), _p(iters, _ip), ctypes.byref(rep))
+        if rc != FAST_GPU_OK and raise_on_fail:
+            self._ck(rc, "nr_solve")
+        return hist, iters, rep.as_dict()
+
     # -- cSysMatrix
     def zero(self, what=ASM_K):
         self._ck(self.L.fast_gpu_zero(self.ctx, what), "zero")
@@ -321,7 +384,7 @@ class GpuSystem:
         nn = _decks.KINDS[self.deck.kind][0]
         if count is None:
             count = self.deck.num_elems - first
-        out = np.zeros((count, 3 * nn, 3 * nn))
+        out = np.zeros((count, 3 * nn) if what == ASM_G else (count, 3 * nn, 3 * nn))
         self._ck(self.L.fast_gpu_element_matrices(self.ctx, what, bucket, int(first), int(count), _p(out)),
                  "element_matrices")
         return out

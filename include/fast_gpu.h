@@ -49,9 +49,17 @@ extern "C" {
 #define FAST_ELEM_HEX8      1   /* %ELEMENT.BRICK8   cElmParam,  SHAPE_BRICK8  */
 #define FAST_ELEM_HEX20     2   /* %ELEMENT.BRICK20  cElmParam,  SHAPE_BRICK20 */
 
+/* ---- element formulation --------------------------------------------- */
+#define FAST_FORM_SMALL_STRAIN       0  /* cElmParam   (%ELEMENT.BRICK8 / BRICK20)     */
+#define FAST_FORM_TOTAL_LAGRANGIAN   1  /* cElmParamTL (%ELEMENT.BRICK8TL / BRICK20TL),
+                                           St. Venant-Kirchhoff, elc/elmparam.cpp:1615-1807 */
+
 /* ---- what to assemble ------------------------------------------------- */
-#define FAST_ASM_STIFFNESS  1   /* cControl::StiffnessMatrix (ctrl/ctrl.cpp:886-975) */
+#define FAST_ASM_STIFFNESS  1   /* cControl::StiffnessMatrix (ctrl/ctrl.cpp:886-975); total-
+                                   Lagrangian buckets give their tangent at the current
+                                   displacements */
 #define FAST_ASM_MASS       2   /* cControl::MassMatrix      (ctrl/ctrl.cpp:979-1027) */
+#define FAST_ASM_INTERNAL_FORCE 3  /* element internal forces (fast_gpu_element_matrices only) */
 
 /* ---- solver precision ------------------------------------------------- */
 #define FAST_PREC_FP64      0   /* FP64 Jacobi PCG, as PCGSolver (mlib/sysmat.cpp:1061-1125) */
@@ -75,6 +83,8 @@ typedef struct {
   const double  *E;             /* [num_elems] Young's modulus                 */
   const double  *nu;            /* [num_elems] Poisson's ratio                 */
   const double  *rho;           /* [num_elems] density, or NULL                */
+  int32_t        formulation;   /* FAST_FORM_*                                 */
+  int32_t        reserved;
 } fast_gpu_bucket;
 
 typedef struct {
@@ -127,6 +137,65 @@ int fast_gpu_pattern_info(fast_gpu_ctx *ctx, int64_t *nnz_blocks, int64_t *nnz_l
 int fast_gpu_update_coords(fast_gpu_ctx *ctx, const double *coords);
 int fast_gpu_update_material(fast_gpu_ctx *ctx, int32_t bucket, const double *E, const double *nu);
 
+/* ---- displacement state and internal force ----------------------------
+ * cControl::AssignDispl (ctrl/ctrl.cpp:1094-1113): the nodal displacements
+ * the total-Lagrangian tangent and the internal force are evaluated at
+ * (equation space, length num_eq; initially zero). */
+int fast_gpu_set_displacement(fast_gpu_ctx *ctx, const double *u);
+int fast_gpu_set_displacement_device(fast_gpu_ctx *ctx, const double *d_u);
+/* cControl::IntForceVector (ctrl/ctrl.cpp:719-813): g = sum of element
+ * internal forces at the current displacements (cElmParam::IntForce
+ * elc/elmparam.cpp:449-535, cElmParamTL::IntForce :1615-1707). */
+int fast_gpu_internal_force(fast_gpu_ctx *ctx, double *g);
+int fast_gpu_internal_force_device(fast_gpu_ctx *ctx, double *d_g);
+
+/* ---- load-control Newton-Raphson ----------------------------------------
+ * cCtrlNR::Solver (ctrl/ctrlnr.cpp:47-270) with proportional loading on the
+ * device: per step f = lambda q; per iteration tangent at u, K du = r,
+ * u += du, g = IntForce(u), r = f - g, converged when |r|/max(1,|f|) < tol
+ * (cControl::Convergence, ctrl/ctrl.cpp:1366-1413).  Each step starts from
+ * the last converged u (FAST_NR_PREDICT_NONE, the reference), from the secant
+ * extrapolation 2u_k - u_{k-1}, or from a caller's prediction, taken only when
+ * its residual is smaller than the secant start's. */
+#define FAST_NR_PREDICT_NONE      0
+#define FAST_NR_PREDICT_SECANT    1
+#define FAST_NR_PREDICT_CALLBACK  2
+
+typedef struct {
+  int32_t steps;              /* MAXIMUM.STEPS                                       */
+  int32_t max_iter;           /* MAXIMUM.ITERATIONS                                  */
+  double  step_factor;        /* STEP.FACTOR (load increment)                        */
+  double  tol;                /* TOLERANCE                                           */
+  int32_t predictor;          /* FAST_NR_PREDICT_*                                   */
+  int32_t reserved;
+  fast_gpu_solve_opts lin;    /* linear solves K du = r                             */
+  double  lin_tol_rel;        /* > 0: linear tol = clamp(lin_tol_rel * Newton error,
+                                 lin_tol_min, lin_tol_max); 0: lin.tol as given       */
+  double  lin_tol_min, lin_tol_max;
+} fast_gpu_nr_opts;
+
+typedef struct {
+  int32_t converged_steps;
+  int32_t failed_step;        /* 0, or the step that did not converge                */
+  int32_t iterations;         /* Newton iterations (tangent assemblies), all steps    */
+  int32_t linear_iterations;  /* PCG iterations, all steps                           */
+  int32_t secant_starts, predictions, predictions_accepted, reserved;
+  double  last_err;           /* |r|/max(1,|f|) at the last iteration                */
+  double  last_rel_residual;  /* |r|/|f| at the last iteration                       */
+} fast_gpu_nr_report;
+
+/* Caller predictor: write the predicted u at load factor lambda (step >= 2)
+ * into d_u_pred (device, equation space) and return 0, or return non-zero to
+ * skip.  d_u_last / d_u_prev are the last two converged solutions. */
+typedef int (*fast_gpu_nr_predictor)(void *user, int32_t step, double lambda, const double *d_u_last,
+                                     const double *d_u_prev, double *d_u_pred);
+
+/* q: reference load (host, num_eq).  u_hist (host, [steps][num_eq]) and iters
+ * ([steps], -1 for a failed step) may be NULL. */
+int fast_gpu_nr_solve(fast_gpu_ctx *ctx, const double *q, const fast_gpu_nr_opts *opts,
+                      fast_gpu_nr_predictor predictor, void *predictor_user, double *u_hist, int32_t *iters,
+                      fast_gpu_nr_report *rep);
+
 /* ---- cSysMatrix replacement (mlib/sysmat.h:60-99) ------------------------ */
 /* cSysMatrix::Zero */
 int fast_gpu_zero(fast_gpu_ctx *ctx, int32_t what);
@@ -174,7 +243,8 @@ int fast_gpu_get_lower_csr(fast_gpu_ctx *ctx, int32_t what, int64_t *nnz,
                            int64_t *rowptr, int32_t *col, double *val);
 /* Element matrices of elements [first, first+count) of a bucket, computed by
  * the same device kernels as the assembly: [count][3nn][3nn] row-major in
- * FAST's element DOF order (cElement::GetElmDofs). */
+ * FAST's element DOF order (cElement::GetElmDofs); with
+ * FAST_ASM_INTERNAL_FORCE the element internal forces, [count][3nn]. */
 int fast_gpu_element_matrices(fast_gpu_ctx *ctx, int32_t what, int32_t bucket, int64_t first,
                               int64_t count, double *Ke);
 

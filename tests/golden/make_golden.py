@@ -134,6 +134,21 @@ def main():
         neq = d.num_eq()
         u = 0.05 * rng.standard_normal(neq)
         run_case("cfg_hex8_tl_state", d, tmp, uvec=u, triplets=False)
+
+        # the reference's own load-control Newton-Raphson (cCtrlNR, unmodified
+        # `fast` binary) on a small TL plate: displacements of every step
+        d = decks.plate_tl_hex8(6, 6, 2, L=4.0, t=0.4, pressure=8.0, steps=4, tol=1e-10, maxit=30)
+        base = os.path.join(tmp, "nr_plate_tl")
+        decks.write_dat(d, base)
+        subprocess.run([refdump.FAST, base, "-silent"], check=True, stdout=subprocess.DEVNULL)
+        us = decks.read_pos_displacements(base + ".pos")
+        ref = refdump.run_dump(base, base + ".bin", "--no-solve", "--no-triplets")
+        out = deck_arrays(d)
+        out.update(ref_neq=ref["neq"], ref_node_eq=ref["node_eq"], ref_f=ref["f"], ref_u_steps=us,
+                   steps=np.array(d.maxstep), step_factor=np.array(d.step_factor), tol=np.array(d.tol),
+                   maxit=np.array(d.maxit))
+        np.savez_compressed(os.path.join(HERE, "nr_plate_tl.npz"), **out)
+        print("nr_plate_tl:", us.shape, "max |w|", np.abs(us[..., 2]).max())
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
 

@@ -1,0 +1,94 @@
+"""Device parity of the total-Lagrangian element, the internal force and the
+load-control Newton driver (through the C ABI) against the reference."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from fast_b200 import decks, gpu
+from oracle import fem_oracle as fo
+from tests import golden_io as gio
+
+pytestmark = pytest.mark.gpu
+
+TOL_K = 1e-12
+
+
+def system(d):
+    s = gpu.GpuSystem(0)
+    s.upload(d)
+    return s
+
+
+def _assemble_vec(d, elm_vals):
+    dofs = fo.elem_dofs(d)
+    g = np.zeros(d.num_eq())
+    for e in range(d.num_elems):
+        m = dofs[e] > 0
+        np.add.at(g, dofs[e][m] - 1, elm_vals[e][m])
+    return g
+
+
+def test_tl_element_tangent_and_force_match_reference():
+    d, g = gio.load("cfg_hex8_tl_state")
+    s = system(d)
+    s.set_displacement(g["u_state"])
+    Kt = s.element_matrices(0, d.num_elems, what=gpu.ASM_K)
+    ge = s.element_matrices(0, d.num_elems, what=gpu.ASM_G)
+    for k, e in enumerate(g["ref_elems"]):
+        assert gio.rel(Kt[e], g["ref_elm_K"][k]) < TOL_K, e
+        assert gio.rel(ge[e], g["ref_elm_g"][k]) < 1e-12, e
+    # assembled internal force and tangent
+    gg = s.internal_force()
+    assert gio.rel(gg, _assemble_vec(d, g["ref_elm_g"])) < 1e-12
+    s.assemble()
+    Kl = s.lower_csr()
+    R = sp.tril(fo.assemble(d, g["ref_elm_K"])).tocsr()
+    assert abs(Kl - R).max() / abs(R).max() < TOL_K
+
+
+def test_small_strain_internal_force_matches_reference():
+    d, g = gio.load("cfg_hex20_lognormal_4x4x2")
+    s = system(d)
+    s.set_displacement(g["ref_u"])
+    assert gio.rel(s.internal_force(), g["ref_g_of_u"]) < 1e-10
+
+
+@pytest.mark.parametrize("precision", [gpu.PREC_FP64, gpu.PREC_MIXED])
+@pytest.mark.parametrize("predictor", [gpu.PREDICT_NONE, gpu.PREDICT_SECANT])
+def test_newton_matches_reference_cctrlnr(precision, predictor):
+    """Every load step of the device Newton equals the displacements the
+    reference's own cCtrlNR printed (TL hex8 plate, 4 steps)."""
+    d, g = gio.load("nr_plate_tl")
+    s = system(d)
+    hist, iters, rep = s.nr_solve(g["ref_f"], int(g["steps"]), float(g["step_factor"]), tol=float(g["tol"]),
+                                  max_iter=int(g["maxit"]), predictor=predictor, precision=precision,
+                                  lin_tol=1e-12)
+    assert rep["converged_steps"] == int(g["steps"]) and (iters > 0).all()
+    eq = d.node_eq()
+    m = eq > 0
+    for k in range(hist.shape[0]):
+        unode = np.zeros((d.num_nodes, 3))
+        unode[m] = hist[k][eq[m] - 1]
+        assert gio.rel(unode, g["ref_u_steps"][k]) < 1e-8, (k, iters, rep)
+
+
+def test_secant_predictor_saves_newton_iterations():
+    d = decks.plate_tl_hex8(10, 10, 2, L=4.0, t=0.4, pressure=12.0, steps=8, tol=1e-8)
+    s = system(d)
+    q = gpu.face_load_vector(d)
+    h0, it0, r0 = s.nr_solve(q, 8, 1 / 8, tol=1e-8, predictor=gpu.PREDICT_NONE, precision=gpu.PREC_MIXED,
+                             lin_tol_rel=1e-3)
+    h1, it1, r1 = s.nr_solve(q, 8, 1 / 8, tol=1e-8, predictor=gpu.PREDICT_SECANT, precision=gpu.PREC_MIXED,
+                             lin_tol_rel=1e-3)
+    assert r0["converged_steps"] == 8 and r1["converged_steps"] == 8
+    assert r1["iterations"] < r0["iterations"], (it0, it1)
+    assert gio.rel(h1[-1], h0[-1]) < 1e-6
+
+
+def test_newton_reports_failure():
+    d = decks.plate_tl_hex8(4, 4, 2, L=4.0, t=0.4, pressure=8.0, steps=2, tol=1e-14)
+    s = system(d)
+    q = gpu.face_load_vector(d)
+    with pytest.raises(gpu.FastGpuError) as ei:
+        s.nr_solve(q, 2, 0.5, tol=1e-30, max_iter=3)
+    assert ei.value.rc == -5
