@@ -38,6 +38,7 @@ void dfree(T *&p) {
 }
 
 void free_mesh(Ctx &c) {
+  c.drop_graphs();
   for (Bucket &B : c.buckets) {
     dfree(B.d_conn); dfree(B.d_E); dfree(B.d_nu); dfree(B.d_rho); dfree(B.d_slot);
     dfree(B.d_dN); dfree(B.d_N); dfree(B.d_w);
@@ -47,6 +48,7 @@ void free_mesh(Ctx &c) {
   dfree(c.d_rowptr); dfree(c.d_col); dfree(c.d_diag); dfree(c.d_srow); dfree(c.d_scol);
   dfree(c.d_K); dfree(c.d_M); dfree(c.d_Ks); dfree(c.d_Ms); dfree(c.d_Ks32);
   dfree(c.d_u); dfree(c.d_r); dfree(c.d_z); dfree(c.d_p); dfree(c.d_w); dfree(c.d_f); dfree(c.d_dinv);
+  dfree(c.d_ubest);
   dfree(c.s_x); dfree(c.s_r); dfree(c.s_z); dfree(c.s_p); dfree(c.s_w); dfree(c.s_dinv);
   dfree(c.d_eq_tmp);
   dfree(c.d_disp); dfree(c.d_gint);
@@ -281,6 +283,7 @@ int fast_gpu_upload_mesh(fast_gpu_ctx *c, const fast_gpu_mesh *m) {
   CK(dalloc(&c->d_K, 9 * c->nnzb));
   CK(dalloc(&c->d_u, n4)); CK(dalloc(&c->d_r, n4)); CK(dalloc(&c->d_z, n4)); CK(dalloc(&c->d_p, n4));
   CK(dalloc(&c->d_w, n4)); CK(dalloc(&c->d_f, n4)); CK(dalloc(&c->d_dinv, 12 * nnode));
+  CK(dalloc(&c->d_ubest, n4));
   CK(dalloc(&c->s_x, n4)); CK(dalloc(&c->s_r, n4)); CK(dalloc(&c->s_z, n4)); CK(dalloc(&c->s_p, n4));
   CK(dalloc(&c->s_w, n4)); CK(dalloc(&c->s_dinv, 12 * nnode));
   CK(cudaMemset(c->d_p, 0, sizeof(double) * n4));
@@ -496,8 +499,9 @@ int solve_node_space(fast_gpu_ctx *c, const fast_gpu_solve_opts *o, bool warm, f
     const int done = c->h_state->done, it = c->h_state->iter;
     if ((done == 3 || done == 4) && it < maxit) {
       // FP32 iterates stopped making progress (ill-conditioned system): go on
-      // with the FP64 iteration from the current FP64 solution
+      // with the FP64 iteration from the best FP64 iterate seen
       R.escalated = 1;
+      CK(cudaMemcpyAsync(c->d_u, c->d_ubest, sizeof(double) * 4 * c->nnode, cudaMemcpyDeviceToDevice, c->stream));
       CK(pcg_fp64(*c, true, tol, maxit, chunk, it));
     }
   } else {

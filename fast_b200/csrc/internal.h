@@ -36,7 +36,7 @@ struct PcgState {
   int32_t null_rhs; // |f| < tol: the solution is u = 0 (PCGSolver returns at once)
   int32_t stall;    // FP64 residual replacements without a 2x improvement
   int32_t final;    // converged on the FP64 residual: later launches do nothing
-  int32_t pad;
+  int32_t best;     // the last FP64 residual was the smallest so far (mixed path)
 };
 
 struct Bucket {
@@ -105,6 +105,7 @@ struct Ctx {
   // solver workspace: node vectors padded to 4 entries (x, y, z, 0) per node
   double *d_u = nullptr, *d_r = nullptr, *d_z = nullptr, *d_p = nullptr, *d_w = nullptr, *d_f = nullptr;
   double *d_dinv = nullptr;       // [nnode][3][4] inverse diagonal (Jacobi) or inverse 3x3 block
+  double *d_ubest = nullptr;      // mixed path: FP64 iterate with the smallest true residual
   float *s_x = nullptr, *s_r = nullptr, *s_z = nullptr, *s_p = nullptr, *s_w = nullptr;
   float *s_dinv = nullptr;        // [nnode][3][4]
   int precond_built = -1;         // which preconditioner d_dinv holds
@@ -115,6 +116,16 @@ struct Ctx {
   double *h_eq_tmp = nullptr;     // pinned [neq]
 
   int64_t launches = 0;          // kernels launched by this context (all entry points)
+
+  // CUDA graphs of one chunk of PCG iterations (captured once, replayed)
+  cudaGraphExec_t graph_fp64 = nullptr, graph_mixed = nullptr;
+  int graph_fp64_chunk = 0, graph_mixed_chunk = 0;
+  int64_t graph_fp64_kernels = 0, graph_mixed_kernels = 0;
+  void drop_graphs() {
+    if (graph_fp64) cudaGraphExecDestroy(graph_fp64);
+    if (graph_mixed) cudaGraphExecDestroy(graph_mixed);
+    graph_fp64 = graph_mixed = nullptr;
+  }
 
   // live kernel timing: CUDA events around SpMV launches and assemblies
   // (kind 0 FP64 SpMV, 1 FP32 SpMV, 2 assembly), harvested at each host sync

@@ -430,10 +430,14 @@ __global__ void __launch_bounds__(256) reliable_scalar(PcgState *st, const doubl
     st->rr = rr;
     st->err = st->err_true;
     st->updates += 1;
+    st->best = 0;
     if (!isfinite(st->err_true)) { st->done = 3; return; }
-    if (st->err_true < st->tol) { st->done = 1; st->final = 1; return; }
-    // the FP64 residual must halve within 10 replacements (10 chunks of FP32
-    // iterations); otherwise FP32 iterates cannot make progress on this system
+    if (st->err_true < st->tol) { st->done = 1; st->final = 1; st->best = 1; return; }
+    // The FP64 residual must halve within 10 replacements (10 chunks of FP32
+    // iterations) and must not grow 100x above its best; otherwise FP32
+    // iterates cannot resolve this system (cond(K) * eps_fp32 near 1).
+    if (st->updates > 1 && st->err_true > 100.0 * st->best_err) { st->done = 4; return; }
+    if (st->updates == 1 || st->err_true < st->best_err) st->best = 1;
     if (st->updates == 1 || st->err_true < 0.5 * st->best_err) {
       st->best_err = st->err_true;
       st->stall = 0;
@@ -441,9 +445,18 @@ __global__ void __launch_bounds__(256) reliable_scalar(PcgState *st, const doubl
       st->done = 4;
       return;
     }
+    if (st->best) st->best_err = fmin(st->best_err, st->err_true);
     st->done = 0;
     st->dot0 = zr;
   }
+}
+
+// mixed path: remember the FP64 iterate with the smallest true residual
+__global__ void keep_best(int64_t n4, const double *__restrict__ u, double *__restrict__ ubest,
+                          const PcgState *__restrict__ st) {
+  if (!st->best) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x)
+    ubest[i] = u[i];
 }
 
 // mixed path start: lenf = |f| (with the reference's normaliser)
@@ -637,16 +650,42 @@ cudaError_t launch_build_precond(Ctx &c, const double *K, int precond) {
 
 // Pipelined host loop: launch a chunk, then look at the state copied after the
 // previous chunk; returns when done or when maxit iterations were launched.
+// Full chunks run as a CUDA graph captured on first use (the scalars live on
+// the device, so the same graph serves every chunk and every later solve of
+// this context); live kernel timing launches the kernels directly instead.
 template <typename LaunchChunk>
-static cudaError_t drive(Ctx &c, int maxit, int chunk, LaunchChunk launch_chunk) {
+static cudaError_t drive(Ctx &c, int maxit, int chunk, cudaGraphExec_t *graph, int *graph_chunk,
+                         int64_t *graph_kernels, LaunchChunk launch_chunk) {
   cudaError_t e;
   cudaEvent_t ev;
   if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return e;
+  const bool use_graph = graph != nullptr && !c.timing;
   int launched = 0;
   bool pending = false;
   while (true) {
     const int k = (maxit - launched < chunk) ? (maxit - launched) : chunk;
-    if ((e = launch_chunk(k)) != cudaSuccess) break;
+    if (use_graph && k == chunk) {
+      if (!*graph || *graph_chunk != chunk) {
+        if (*graph) cudaGraphExecDestroy(*graph);
+        *graph = nullptr;
+        cudaGraph_t g = nullptr;
+        const int64_t before = c.launches;
+        if ((e = cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) break;
+        cudaError_t el = launch_chunk(k);
+        e = cudaStreamEndCapture(c.stream, &g);
+        if (el != cudaSuccess) e = el;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(graph, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) { *graph = nullptr; break; }
+        *graph_chunk = chunk;
+        *graph_kernels = c.launches - before;
+        c.launches = before;
+      }
+      if ((e = cudaGraphLaunch(*graph, c.stream)) != cudaSuccess) break;
+      c.launches += *graph_kernels;
+    } else {
+      if ((e = launch_chunk(k)) != cudaSuccess) break;
+    }
     launched += k;
     if (pending) {
       if ((e = cudaEventSynchronize(ev)) != cudaSuccess) break;
@@ -686,7 +725,7 @@ cudaError_t pcg_fp64(Ctx &c, bool warm, double tol, int maxit, int chunk, int it
   pcg_init_scalar<<<1, 256, 0, c.stream>>>(st, P_C(c), R, P_D(c), R, warm ? P_E(c) : nullptr, G, tol, maxit, iter0);
   c.launches++;
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  return drive(c, maxit, chunk, [&](int k) -> cudaError_t {
+  return drive(c, maxit, chunk, &c.graph_fp64, &c.graph_fp64_chunk, &c.graph_fp64_kernels, [&](int k) -> cudaError_t {
     for (int i = 0; i < k; i++) {
       c.begin_span(0);
       spmv_f64<0, kLPR64><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, c.d_Ks, c.d_p, nullptr,
@@ -722,11 +761,13 @@ cudaError_t pcg_mixed(Ctx &c, bool warm, double tol, int maxit, int chunk) {
     c.end_span();
     replace_residual<<<R, kVecThreads, 0, c.stream>>>(nn, c.d_r, c.s_r, c.s_z, c.s_p, c.s_dinv, st, P_C(c));
     reliable_scalar<<<1, 256, 0, c.stream>>>(st, P_E(c), G, P_C(c), R);
-    c.launches += 4;
+    keep_best<<<R, 256, 0, c.stream>>>(4 * nn, c.d_u, c.d_ubest, st);
+    c.launches += 5;
   };
   reliable();
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  return drive(c, maxit, chunk, [&](int k) -> cudaError_t {
+  return drive(c, maxit, chunk, &c.graph_mixed, &c.graph_mixed_chunk, &c.graph_mixed_kernels,
+               [&](int k) -> cudaError_t {
     for (int i = 0; i < k; i++) {
       c.begin_span(1);
       spmv_f32<0, kLPR32><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, c.d_Ks32, c.s_p, nullptr,
