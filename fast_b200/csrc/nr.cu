@@ -198,7 +198,26 @@ extern "C" int fast_gpu_nr_solve(fast_gpu_ctx *c, const double *q_host, const fa
     (void)use_secant;
 
     int conv = 0, it = 0;
-    for (it = 1; it <= o->max_iter; it++) {
+    bool start_ok = false;
+    if (step >= 2 && o->predictor != FAST_NR_PREDICT_NONE) {
+      // a predicted start may already meet the tolerance (never the case for
+      // the reference's start, which carries the whole load increment)
+      const double flen = std::sqrt(flen2), rlen = std::sqrt(rlen2);
+      double err;
+      if (flen > tol) {
+        err = rlen / std::max(1.0, flen);
+      } else {
+        NRCK(norms2(*c, w, w.g, nullptr, &glen2, nullptr));
+        err = rlen / std::max(1.0, std::sqrt(glen2));
+      }
+      if (err < tol) {
+        conv = 1;
+        start_ok = true;
+        R.last_err = err;
+        R.last_rel_residual = flen > 0 ? rlen / flen : rlen;
+      }
+    }
+    for (it = 1; !conv && it <= o->max_iter; it++) {
       NRRC(fast_gpu_assemble(c, FAST_ASM_STIFFNESS));  // tangent at u
       fast_gpu_solve_opts lo = o->lin;
       if (o->lin_tol_rel > 0) {
@@ -232,7 +251,7 @@ extern "C" int fast_gpu_nr_solve(fast_gpu_ctx *c, const double *q_host, const fa
       if (err < tol) { conv = 1; break; }
       if (!std::isfinite(err)) break;
     }
-    if (iters) iters[step - 1] = conv ? it : -1;
+    if (iters) iters[step - 1] = conv ? (start_ok ? 0 : it) : -1;
     if (!conv) {
       c->err = "nr_solve: Newton iterations did not converge (\"Convergence not achived\")";
       R.failed_step = step;

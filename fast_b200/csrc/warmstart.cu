@@ -1,0 +1,614 @@
+// warmstart.cu - the learned load-step predictor (fast_gpu_ws_* and
+// fast_gpu_mlp_* in include/fast_gpu.h).  No counterpart in the reference:
+// cCtrlNR::Solver (ctrl/ctrlnr.cpp:47-270) starts every load step from the
+// last converged displacements.
+//
+// Training data are whole load-control trajectories (the converged u of every
+// step).  Their POD basis Phi comes from a randomized range finder over the
+// snapshot matrix in FP64 on the device; the POD coefficients a_s = Phi^T u_s
+// of every snapshot then give one training sample per step s >= 2:
+//   x = [lambda_s, a_{s-1}/sigma, da_{s-1}/delta, ..., da_{s-H+1}/delta]
+//   t = (da_s - rho da_{s-1}) / tau          da_j = a_j - a_{j-1},  a_j = 0 for j <= 0,
+//                                            rho = dlambda_s / dlambda_{s-1}
+// i.e. the last H coefficient sets, given as the latest set and its H-1
+// backward differences (each scaled by its own per-mode RMS, so that the BF16
+// inputs keep the increments' digits), and as target what the secant
+// increment misses inside the basis.  Prediction adds that correction to the
+// secant start; the Newton driver accepts it only when its residual is below
+// the secant start's.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+#include "learned.h"
+
+using namespace fastgpu;
+
+struct fast_gpu_ctx : public Ctx {};
+
+namespace {
+
+__global__ void ws_combine(int32_t n, double rho, const double *__restrict__ ul, const double *__restrict__ up,
+                           const double *__restrict__ corr, double *__restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = ul[i] + rho * (ul[i] - up[i]) + corr[i];
+}
+
+__global__ void ws_pack2(int32_t n, const double *__restrict__ a, const double *__restrict__ b,
+                         double *__restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    out[i] = a[i];
+    out[n + i] = b[i];
+  }
+}
+
+uint64_t mix64(uint64_t &x) {
+  uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+double gauss(uint64_t &st) {  // Box-Muller
+  const double u1 = ((mix64(st) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+  const double u2 = ((mix64(st) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+  return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+}
+
+}  // namespace
+
+struct fast_gpu_ws {
+  Ctx *c = nullptr;
+  fast_gpu_ws_opts o{};
+  int32_t n = 0;
+  // training trajectories (device snapshots, host load factors)
+  std::vector<double *> traj;
+  std::vector<std::vector<double>> lam;
+  // POD
+  int k = 0;
+  double *d_phi = nullptr;       // [n][k]
+  double energy = 0.0;
+  std::vector<double> sigma, delta, tau;   // per-mode scales of a, da and the target
+  // network
+  Mlp net;
+  bool trained = false;
+  int in_dim = 0;
+  std::vector<float> hx, ht;     // scaled samples
+  int samples = 0, epochs = 0;
+  float first_loss = 0.f, last_loss = 0.f;
+  double basis_ms = 0.0, train_ms = 0.0;
+  int64_t launches = 0;
+  // dgemm split workspace and prediction scratch
+  double *d_ws = nullptr;
+  size_t ws_cap = 0;
+  double *d_pair = nullptr;      // [2][n]
+  double *d_coef = nullptr;      // [2][k]
+  double *d_corr = nullptr;      // [n]
+  double *d_delta = nullptr;     // [k]
+  double *h_buf = nullptr;       // pinned [2k]
+  float *h_y = nullptr;          // pinned [k]
+  // coefficient history of the current solve (host), by step
+  std::map<int, std::vector<double>> hist;
+  int last_step = 0;
+
+  bool fail(const std::string &m) { c->err = "ws: " + m; return false; }
+  cudaError_t ensure_ws(int M, int N, int K) {
+    const int s = dgemm_splits(M, N, K);
+    const size_t need = s > 1 ? (size_t)s * M * N : 0;
+    if (need <= ws_cap) return cudaSuccess;
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return e;
+    if (d_ws) cudaFree(d_ws);
+    d_ws = nullptr;
+    ws_cap = 0;
+    e = cudaMalloc((void **)&d_ws, sizeof(double) * need);
+    if (e == cudaSuccess) ws_cap = need;
+    return e;
+  }
+  cudaError_t gemm(int M, int N, int K, const double *A, int lda, bool ta, const double *B, int ldb, bool tb,
+                   double *C, int ldc) {
+    cudaError_t e = ensure_ws(M, N, K);
+    if (e != cudaSuccess) return e;
+    launches += dgemm_splits(M, N, K) > 1 ? 2 : 1;
+    return dgemm(c->stream, M, N, K, A, lda, ta, B, ldb, tb, C, ldc, d_ws);
+  }
+  // Q = Y V_r Lambda_r^{-1/2} from the eigenpairs of Y^T Y (rank-revealing
+  // orthonormalisation of the rows x l matrix Y); returns the rank r
+  int orth(int rows, int l, double *Y, double *Q, cudaError_t &e);
+};
+
+int fast_gpu_ws::orth(int rows, int l, double *Y, double *Q, cudaError_t &e) {
+  double *d_g = nullptr, *d_t = nullptr;
+  std::vector<double> G((size_t)l * l), w, V;
+  int r = 0;
+  e = cudaMalloc((void **)&d_g, sizeof(double) * l * l);
+  if (e == cudaSuccess) e = gemm(l, l, rows, Y, l, true, Y, l, false, d_g, l);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(G.data(), d_g, sizeof(double) * l * l, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e == cudaSuccess) {
+    sym_eig(l, G, w, V);
+    const double wmax = w.empty() ? 0.0 : w[0];
+    while (r < l && w[r] > 1e-24 * wmax && w[r] > 0.0) r++;
+    std::vector<double> T((size_t)l * std::max(r, 1), 0.0);
+    for (int i = 0; i < l; i++)
+      for (int j = 0; j < r; j++) T[(size_t)i * r + j] = V[(size_t)i * l + j] / std::sqrt(w[j]);
+    if (r > 0) {
+      e = cudaMalloc((void **)&d_t, sizeof(double) * l * r);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_t, T.data(), sizeof(double) * l * r, cudaMemcpyHostToDevice, c->stream);
+      if (e == cudaSuccess) e = gemm(rows, r, l, Y, l, false, d_t, r, false, Q, r);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    }
+  }
+  if (d_g) cudaFree(d_g);
+  if (d_t) cudaFree(d_t);
+  return r;
+}
+
+#define WCK(call)                                                          \
+  do {                                                                     \
+    cudaError_t _e = (call);                                               \
+    if (_e != cudaSuccess) {                                               \
+      w->c->err = std::string("ws: ") + #call + ": " + cudaGetErrorString(_e); \
+      return FAST_GPU_ECUDA;                                               \
+    }                                                                      \
+  } while (0)
+
+extern "C" int fast_gpu_ws_create(fast_gpu_ctx *ctx, const fast_gpu_ws_opts *opts, fast_gpu_ws **out) {
+  if (!ctx || !opts || !out) return FAST_GPU_EINVAL;
+  *out = nullptr;
+  if (ctx->neq <= 0) { ctx->err = "ws_create: no mesh"; return FAST_GPU_ESTATE; }
+  if (opts->modes <= 0 || opts->modes > 64 || opts->history <= 0 || opts->history > 16 || opts->width <= 0 ||
+      opts->width > 1024 || opts->hidden <= 0 || opts->hidden > 8 || opts->oversample < 0 || opts->power_iters < 0) {
+    ctx->err = "ws_create: options out of range (modes 1..64, history 1..16, width 1..1024, hidden 1..8)";
+    return FAST_GPU_EINVAL;
+  }
+  fast_gpu_ws *w = new (std::nothrow) fast_gpu_ws;
+  if (!w) return FAST_GPU_ENOMEM;
+  w->c = ctx;
+  w->o = *opts;
+  w->n = ctx->neq;
+  w->in_dim = 1 + opts->history * opts->modes;
+  std::vector<int> dims{w->in_dim};
+  for (int i = 0; i < opts->hidden; i++) dims.push_back(opts->width);
+  dims.push_back(opts->modes);
+  cudaError_t e = w->net.init(dims, opts->seed);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_pair, sizeof(double) * 2 * (size_t)w->n);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_corr, sizeof(double) * (size_t)w->n);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_coef, sizeof(double) * 2 * 64);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_delta, sizeof(double) * 64);
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&w->h_buf, sizeof(double) * 2 * 64);
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&w->h_y, sizeof(float) * 64);
+  if (e != cudaSuccess) {
+    ctx->err = std::string("ws_create: ") + cudaGetErrorString(e);
+    fast_gpu_ws_destroy(w);
+    return FAST_GPU_ENOMEM;
+  }
+  *out = w;
+  return FAST_GPU_OK;
+}
+
+extern "C" void fast_gpu_ws_destroy(fast_gpu_ws *w) {
+  if (!w) return;
+  if (w->c) cudaStreamSynchronize(w->c->stream);
+  for (double *p : w->traj) cudaFree(p);
+  for (double *p : {w->d_phi, w->d_ws, w->d_pair, w->d_coef, w->d_corr, w->d_delta})
+    if (p) cudaFree(p);
+  if (w->h_buf) cudaFreeHost(w->h_buf);
+  if (w->h_y) cudaFreeHost(w->h_y);
+  w->net.release();
+  delete w;
+}
+
+extern "C" int fast_gpu_ws_add_trajectory(fast_gpu_ws *w, int32_t steps, const double *lambda,
+                                          const double *u_steps) {
+  if (!w || steps <= 0 || !lambda || !u_steps) return FAST_GPU_EINVAL;
+  double *d = nullptr;
+  const size_t bytes = sizeof(double) * (size_t)steps * w->n;
+  WCK(cudaMalloc((void **)&d, bytes));
+  cudaError_t e = cudaMemcpy(d, u_steps, bytes, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(d);
+    w->c->err = std::string("ws_add_trajectory: ") + cudaGetErrorString(e);
+    return FAST_GPU_ECUDA;
+  }
+  w->traj.push_back(d);
+  w->lam.emplace_back(lambda, lambda + steps);
+  w->trained = false;
+  return FAST_GPU_OK;
+}
+
+extern "C" int fast_gpu_ws_build_basis(fast_gpu_ws *w, double *captured_energy) {
+  if (!w) return FAST_GPU_EINVAL;
+  Ctx &c = *w->c;
+  int m = 0;
+  for (auto &l : w->lam) m += (int)l.size();
+  if (m < w->o.modes) { c.err = "ws_build_basis: fewer snapshots than modes"; return FAST_GPU_ESTATE; }
+  const auto t0 = std::chrono::steady_clock::now();
+  const int n = w->n;
+  const int l = std::min(m, w->o.modes + w->o.oversample);
+  // S: [m][n], the snapshots as rows
+  double *S = nullptr, *Om = nullptr, *Y = nullptr, *Q = nullptr, *Z = nullptr, *Zq = nullptr, *d_u = nullptr,
+         *d_fro = nullptr;
+  int rc = FAST_GPU_OK;
+  cudaError_t e = cudaMalloc((void **)&S, sizeof(double) * (size_t)m * n);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&Om, sizeof(double) * (size_t)m * l);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&Y, sizeof(double) * (size_t)n * l);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&Q, sizeof(double) * (size_t)n * l);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&Z, sizeof(double) * (size_t)m * l);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&Zq, sizeof(double) * (size_t)m * l);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&d_fro, sizeof(double));
+  size_t row = 0;
+  for (size_t t = 0; t < w->traj.size() && e == cudaSuccess; t++) {
+    const size_t cnt = w->lam[t].size();
+    e = cudaMemcpyAsync(S + row * n, w->traj[t], sizeof(double) * cnt * n, cudaMemcpyDeviceToDevice, c.stream);
+    row += cnt;
+  }
+  std::vector<double> hom((size_t)m * l);
+  uint64_t st = w->o.seed ^ 0x5DEECE66Dull;
+  for (double &x : hom) x = gauss(st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(Om, hom.data(), sizeof(double) * hom.size(), cudaMemcpyHostToDevice, c.stream);
+  int r = l;
+  // Y = S^T Omega ... in snapshot-as-row terms: Y[n][l] = S^T[n][m] Om[m][l]
+  if (e == cudaSuccess) e = w->gemm(n, l, m, S, n, true, Om, l, false, Y, l);
+  if (e == cudaSuccess) r = w->orth(n, l, Y, Q, e);
+  for (int it = 0; it < w->o.power_iters && e == cudaSuccess && r > 0; it++) {
+    e = w->gemm(m, r, n, S, n, false, Q, r, false, Z, r);            // Z = S Q       [m][r]
+    int r2 = r;
+    if (e == cudaSuccess) r2 = w->orth(m, r, Z, Zq, e);
+    if (e == cudaSuccess && r2 > 0) e = w->gemm(n, r2, m, S, n, true, Zq, r2, false, Y, r2);  // Y = S^T Zq
+    if (e == cudaSuccess && r2 > 0) r = w->orth(n, r2, Y, Q, e);
+  }
+  std::vector<double> B2, ev, U;
+  if (e == cudaSuccess && r > 0) e = w->gemm(m, r, n, S, n, false, Q, r, false, Z, r);  // Z = S Q = B^T
+  if (e == cudaSuccess && r > 0) {
+    double *d_b = nullptr;
+    e = cudaMalloc((void **)&d_b, sizeof(double) * r * r);
+    if (e == cudaSuccess) e = w->gemm(r, r, m, Z, r, true, Z, r, false, d_b, r);  // B B^T = Z^T Z
+    B2.resize((size_t)r * r);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(B2.data(), d_b, sizeof(double) * r * r, cudaMemcpyDeviceToHost, c.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+    if (d_b) cudaFree(d_b);
+  }
+  const int k = std::min(w->o.modes, r);
+  double kept = 0.0, fro = 0.0;
+  if (e == cudaSuccess && k > 0) {
+    sym_eig(r, B2, ev, U);
+    for (int j = 0; j < k; j++) kept += std::max(0.0, ev[j]);
+    std::vector<double> Uk((size_t)r * k);
+    for (int i = 0; i < r; i++)
+      for (int j = 0; j < k; j++) Uk[(size_t)i * k + j] = U[(size_t)i * r + j];
+    e = cudaMalloc((void **)&d_u, sizeof(double) * r * k);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_u, Uk.data(), sizeof(double) * r * k, cudaMemcpyHostToDevice, c.stream);
+    if (w->d_phi) { cudaFree(w->d_phi); w->d_phi = nullptr; }
+    if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_phi, sizeof(double) * (size_t)n * k);
+    if (e == cudaSuccess) e = w->gemm(n, k, r, Q, r, false, d_u, k, false, w->d_phi, k);  // Phi = Q U_k
+    if (e == cudaSuccess) e = launch_norm2(c, S, (int64_t)m * n, d_fro);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&fro, d_fro, sizeof(double), cudaMemcpyDeviceToHost, c.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+  }
+  if (e == cudaSuccess && k > 0) {
+    w->k = k;
+    w->energy = fro > 0 ? kept / fro : 0.0;
+    if (captured_energy) *captured_energy = w->energy;
+    w->trained = false;
+  } else if (e != cudaSuccess) {
+    c.err = std::string("ws_build_basis: ") + cudaGetErrorString(e);
+    rc = FAST_GPU_ECUDA;
+  } else {
+    c.err = "ws_build_basis: snapshots have rank 0";
+    rc = FAST_GPU_ESTATE;
+  }
+  for (double *p : {S, Om, Y, Q, Z, Zq, d_u, d_fro})
+    if (p) cudaFree(p);
+  w->basis_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return rc;
+}
+
+namespace {
+
+// scaled samples from the POD coefficients of every snapshot
+void build_samples(fast_gpu_ws *w, const std::vector<double> &A) {
+  const int k = w->k, H = w->o.history, in = w->in_dim;
+  const int kk = w->o.modes;  // network output width (modes beyond k stay zero)
+  size_t off = 0;
+  std::vector<size_t> toff;
+  for (size_t t = 0; t < w->lam.size(); t++) { toff.push_back(off); off += w->lam[t].size(); }
+  auto coef = [&](size_t t, long s, int j) -> double {  // a_s of trajectory t (s = 1..S), 0 for s <= 0
+    return s <= 0 ? 0.0 : A[(toff[t] + (size_t)(s - 1)) * k + j];
+  };
+  auto lamv = [&](size_t t, long s) -> double { return s <= 0 ? 0.0 : w->lam[t][(size_t)(s - 1)]; };
+  struct Sm { size_t t; long s; double rho; };
+  std::vector<Sm> list;
+  for (size_t t = 0; t < w->lam.size(); t++) {
+    const long S = (long)w->lam[t].size();
+    for (long s = 2; s <= S; s++) {
+      const double d1 = lamv(t, s - 1) - lamv(t, s - 2);
+      list.push_back({t, s, d1 != 0.0 ? (lamv(t, s) - lamv(t, s - 1)) / d1 : 1.0});
+    }
+  }
+  const size_t ns = list.size();
+  // per-mode RMS scales: a over all snapshots, da_{s-1} and the target over the samples
+  auto floor_scale = [](std::vector<double> &v, double rel) {
+    double mx = 0.0;
+    for (double x : v) mx = std::max(mx, x);
+    for (double &x : v) x = std::max(x, rel * mx + 1e-300);
+  };
+  w->sigma.assign(k, 0.0);
+  w->delta.assign(k, 0.0);
+  w->tau.assign(k, 0.0);
+  const size_t rows = A.size() / k;
+  for (size_t r = 0; r < rows; r++)
+    for (int j = 0; j < k; j++) w->sigma[j] += A[r * k + j] * A[r * k + j];
+  std::vector<double> raw(ns * k);
+  for (size_t i = 0; i < ns; i++) {
+    const Sm &m = list[i];
+    for (int j = 0; j < k; j++) {
+      const double d1 = coef(m.t, m.s - 1, j) - coef(m.t, m.s - 2, j);
+      w->delta[j] += d1 * d1;
+      raw[i * k + j] = coef(m.t, m.s, j) - coef(m.t, m.s - 1, j) - m.rho * d1;
+      w->tau[j] += raw[i * k + j] * raw[i * k + j];
+    }
+  }
+  for (int j = 0; j < k; j++) {
+    w->sigma[j] = std::sqrt(w->sigma[j] / std::max<size_t>(1, rows));
+    w->delta[j] = std::sqrt(w->delta[j] / std::max<size_t>(1, ns));
+    w->tau[j] = std::sqrt(w->tau[j] / std::max<size_t>(1, ns));
+  }
+  floor_scale(w->sigma, 1e-12);
+  floor_scale(w->delta, 1e-12);
+  floor_scale(w->tau, 1e-6);
+  w->hx.assign(ns * in, 0.f);
+  w->ht.assign(ns * kk, 0.f);
+  for (size_t i = 0; i < ns; i++) {
+    const Sm &m = list[i];
+    float *x = &w->hx[i * in];
+    x[0] = (float)lamv(m.t, m.s);
+    for (int j = 0; j < k; j++) x[1 + j] = (float)(coef(m.t, m.s - 1, j) / w->sigma[j]);
+    for (int h = 1; h < H; h++)
+      for (int j = 0; j < k; j++)
+        x[1 + h * kk + j] = (float)((coef(m.t, m.s - h, j) - coef(m.t, m.s - h - 1, j)) / w->delta[j]);
+    for (int j = 0; j < k; j++) w->ht[i * kk + j] = (float)(raw[i * k + j] / w->tau[j]);
+  }
+  w->samples = (int)ns;
+}
+
+}  // namespace
+
+extern "C" int fast_gpu_ws_train(fast_gpu_ws *w, int32_t epochs, float lr, float *loss_history) {
+  if (!w || epochs < 0 || !(lr > 0.f)) return FAST_GPU_EINVAL;
+  Ctx &c = *w->c;
+  if (!w->d_phi || w->k <= 0) { c.err = "ws_train: build the basis first"; return FAST_GPU_ESTATE; }
+  const auto t0 = std::chrono::steady_clock::now();
+  const int n = w->n, k = w->k;
+  int m = 0;
+  for (auto &l : w->lam) m += (int)l.size();
+  // POD coefficients of every snapshot: A[m][k] = S Phi
+  std::vector<double> A((size_t)m * k);
+  {
+    double *d_a = nullptr;
+    WCK(cudaMalloc((void **)&d_a, sizeof(double) * (size_t)m * k));
+    size_t row = 0;
+    cudaError_t e = cudaSuccess;
+    for (size_t t = 0; t < w->traj.size() && e == cudaSuccess; t++) {
+      const int cnt = (int)w->lam[t].size();
+      e = w->gemm(cnt, k, n, w->traj[t], n, false, w->d_phi, k, false, d_a + row * k, k);
+      row += cnt;
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(A.data(), d_a, sizeof(double) * A.size(), cudaMemcpyDeviceToHost, c.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+    cudaFree(d_a);
+    WCK(e);
+  }
+  build_samples(w, A);
+  const int ns = w->samples;
+  if (ns <= 0) { c.err = "ws_train: trajectories need at least 2 steps"; return FAST_GPU_ESTATE; }
+  Mlp &net = w->net;
+  WCK(net.reserve(ns));
+  WCK(cudaMemcpyAsync(net.d_h[0], w->hx.data(), sizeof(float) * w->hx.size(), cudaMemcpyHostToDevice, c.stream));
+  WCK(cudaMemcpyAsync(net.d_target, w->ht.data(), sizeof(float) * w->ht.size(), cudaMemcpyHostToDevice, c.stream));
+  WCK(cudaMemsetAsync(net.d_status, 0, sizeof(int32_t), c.stream));
+  float *d_hist = nullptr;
+  WCK(cudaMalloc((void **)&d_hist, sizeof(float) * std::max(1, epochs)));
+  cudaError_t e = cudaSuccess;
+  const int64_t l0 = net.launches;
+  for (int ep = 0; ep < epochs && e == cudaSuccess; ep++) {
+    const float lr_t = (float)(0.5 * lr * (1.0 + std::cos(3.141592653589793 * ep / std::max(1, epochs))));
+    e = net.forward(c.stream, ns);
+    if (e == cudaSuccess) e = net.backward(c.stream, ns);
+    if (e == cudaSuccess) e = net.adam(c.stream, lr_t, 0.9f, 0.999f, 1e-8f);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_hist + ep, net.d_loss, sizeof(float), cudaMemcpyDeviceToDevice, c.stream);
+  }
+  std::vector<float> hh(std::max(1, epochs));
+  int32_t status = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hh.data(), d_hist, sizeof(float) * hh.size(), cudaMemcpyDeviceToHost, c.stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&status, net.d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+  cudaFree(d_hist);
+  w->launches += net.launches - l0;
+  c.launches += net.launches - l0;
+  WCK(e);
+  if (status) { c.err = "ws_train: a tensor-core wait timed out"; return FAST_GPU_ECUDA; }
+  if (loss_history && epochs > 0) std::memcpy(loss_history, hh.data(), sizeof(float) * epochs);
+  w->epochs = epochs;
+  if (epochs > 0) { w->first_loss = hh[0]; w->last_loss = hh[epochs - 1]; }
+  w->trained = true;
+  w->hist.clear();
+  w->last_step = 0;
+  w->train_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return FAST_GPU_OK;
+}
+
+extern "C" int fast_gpu_ws_predict(void *user, int32_t step, double lambda, const double *d_u_last,
+                                   const double *d_u_prev, double *d_u_pred) {
+  fast_gpu_ws *w = static_cast<fast_gpu_ws *>(user);
+  if (!w || !d_u_last || !d_u_prev || !d_u_pred || step < 2) return FAST_GPU_EINVAL;
+  if (!w->trained) return FAST_GPU_ESTATE;
+  Ctx &c = *w->c;
+  const int n = w->n, k = w->k, kk = w->o.modes, H = w->o.history;
+  if (step <= w->last_step) w->hist.clear();  // a new solve
+  w->last_step = step;
+  // a_last, a_prev = Phi^T u  (one GEMM over both vectors)
+  ws_pack2<<<148, 256, 0, c.stream>>>(n, d_u_last, d_u_prev, w->d_pair);
+  w->launches++;
+  WCK(w->gemm(2, k, n, w->d_pair, n, false, w->d_phi, k, false, w->d_coef, k));
+  WCK(cudaMemcpyAsync(w->h_buf, w->d_coef, sizeof(double) * 2 * k, cudaMemcpyDeviceToHost, c.stream));
+  WCK(cudaStreamSynchronize(c.stream));
+  w->hist[step - 1].assign(w->h_buf, w->h_buf + k);
+  w->hist[step - 2].assign(w->h_buf + k, w->h_buf + 2 * k);
+  // load factors of the two previous steps: proportional loading with equal steps
+  const double lam1 = lambda * (step - 1) / step, lam2 = lambda * (step - 2) / step;
+  const double rho = (lam1 - lam2) != 0.0 ? (lambda - lam1) / (lam1 - lam2) : 1.0;
+  // a_s of this solve: zero before the first step; a missing (skipped) step
+  // repeats the closest earlier one that is known
+  auto a_of = [&](int s, int j) -> double {
+    for (; s > 0; s--) {
+      auto it = w->hist.find(s);
+      if (it != w->hist.end()) return it->second[j];
+    }
+    return 0.0;
+  };
+  std::vector<float> x(w->in_dim, 0.f);
+  x[0] = (float)lambda;
+  for (int j = 0; j < k; j++) x[1 + j] = (float)(a_of(step - 1, j) / w->sigma[j]);
+  for (int h = 1; h < H; h++)
+    for (int j = 0; j < k; j++)
+      x[1 + h * kk + j] = (float)((a_of(step - h, j) - a_of(step - h - 1, j)) / w->delta[j]);
+  Mlp &net = w->net;
+  WCK(net.reserve(1));
+  WCK(cudaMemcpyAsync(net.d_h[0], x.data(), sizeof(float) * w->in_dim, cudaMemcpyHostToDevice, c.stream));
+  const int64_t l0 = net.launches;
+  WCK(net.forward(c.stream, 1));
+  WCK(cudaMemcpyAsync(w->h_y, net.d_h[net.layers()], sizeof(float) * kk, cudaMemcpyDeviceToHost, c.stream));
+  WCK(cudaStreamSynchronize(c.stream));
+  w->launches += net.launches - l0;
+  std::vector<double> delta(k);
+  for (int j = 0; j < k; j++) delta[j] = w->tau[j] * (double)w->h_y[j];
+  WCK(cudaMemcpyAsync(w->d_delta, delta.data(), sizeof(double) * k, cudaMemcpyHostToDevice, c.stream));
+  WCK(w->gemm(n, 1, k, w->d_phi, k, false, w->d_delta, 1, false, w->d_corr, 1));  // Phi delta
+  ws_combine<<<148, 256, 0, c.stream>>>(n, rho, d_u_last, d_u_prev, w->d_corr, d_u_pred);
+  w->launches++;
+  c.launches += 2 + (net.launches - l0) + 2;
+  WCK(cudaGetLastError());
+  return FAST_GPU_OK;
+}
+
+extern "C" int fast_gpu_ws_report(fast_gpu_ws *w, fast_gpu_ws_stats *r) {
+  if (!w || !r) return FAST_GPU_EINVAL;
+  fast_gpu_ws_stats R{};
+  R.trajectories = (int32_t)w->traj.size();
+  for (auto &l : w->lam) R.snapshots += (int32_t)l.size();
+  R.samples = w->samples;
+  R.modes = w->k;
+  R.input_dim = w->in_dim;
+  R.output_dim = w->o.modes;
+  R.epochs = w->epochs;
+  R.params = w->net.nparams;
+  R.captured_energy = w->energy;
+  R.basis_ms = w->basis_ms;
+  R.train_ms = w->train_ms;
+  R.first_loss = w->first_loss;
+  R.last_loss = w->last_loss;
+  R.launches = w->launches;
+  *r = R;
+  return FAST_GPU_OK;
+}
+
+extern "C" int fast_gpu_ws_get_basis(fast_gpu_ws *w, double *phi) {
+  if (!w || !phi) return FAST_GPU_EINVAL;
+  if (!w->d_phi) { w->c->err = "ws_get_basis: no basis"; return FAST_GPU_ESTATE; }
+  WCK(cudaMemcpyAsync(phi, w->d_phi, sizeof(double) * (size_t)w->n * w->k, cudaMemcpyDeviceToHost, w->c->stream));
+  WCK(cudaStreamSynchronize(w->c->stream));
+  return FAST_GPU_OK;
+}
+
+extern "C" int fast_gpu_ws_get_samples(fast_gpu_ws *w, float *x, float *t) {
+  if (!w) return FAST_GPU_EINVAL;
+  if (w->samples <= 0) { w->c->err = "ws_get_samples: not trained"; return FAST_GPU_ESTATE; }
+  if (x) std::memcpy(x, w->hx.data(), sizeof(float) * w->hx.size());
+  if (t) std::memcpy(t, w->ht.data(), sizeof(float) * w->ht.size());
+  return FAST_GPU_OK;
+}
+
+extern "C" int fast_gpu_mlp_params(fast_gpu_ws *w, float *get, const float *set, int64_t *count) {
+  if (!w) return FAST_GPU_EINVAL;
+  if (count) *count = w->net.nparams;
+  if (set) WCK(cudaMemcpy(w->net.d_params, set, sizeof(float) * w->net.nparams, cudaMemcpyHostToDevice));
+  if (get) WCK(cudaMemcpy(get, w->net.d_params, sizeof(float) * w->net.nparams, cudaMemcpyDeviceToHost));
+  return FAST_GPU_OK;
+}
+
+extern "C" int fast_gpu_mlp_forward(fast_gpu_ws *w, int32_t batch, const float *x, float *y) {
+  if (!w || batch <= 0 || !x || !y) return FAST_GPU_EINVAL;
+  Ctx &c = *w->c;
+  Mlp &net = w->net;
+  WCK(net.reserve(batch));
+  WCK(cudaMemcpyAsync(net.d_h[0], x, sizeof(float) * (size_t)batch * net.dims[0], cudaMemcpyHostToDevice, c.stream));
+  WCK(cudaMemsetAsync(net.d_status, 0, sizeof(int32_t), c.stream));
+  const int64_t l0 = net.launches;
+  WCK(net.forward(c.stream, batch));
+  int32_t status = 0;
+  WCK(cudaMemcpyAsync(y, net.d_h[net.layers()], sizeof(float) * (size_t)batch * net.dims.back(),
+                      cudaMemcpyDeviceToHost, c.stream));
+  WCK(cudaMemcpyAsync(&status, net.d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
+  WCK(cudaStreamSynchronize(c.stream));
+  w->launches += net.launches - l0;
+  c.launches += net.launches - l0;
+  if (status) { c.err = "mlp_forward: a tensor-core wait timed out"; return FAST_GPU_ECUDA; }
+  return FAST_GPU_OK;
+}
+
+extern "C" int fast_gpu_mlp_loss_grad(fast_gpu_ws *w, int32_t batch, const float *x, const float *t, float *loss,
+                                      float *grad) {
+  if (!w || batch <= 0 || !x || !t) return FAST_GPU_EINVAL;
+  Ctx &c = *w->c;
+  Mlp &net = w->net;
+  WCK(net.reserve(batch));
+  WCK(cudaMemcpyAsync(net.d_h[0], x, sizeof(float) * (size_t)batch * net.dims[0], cudaMemcpyHostToDevice, c.stream));
+  WCK(cudaMemcpyAsync(net.d_target, t, sizeof(float) * (size_t)batch * net.dims.back(), cudaMemcpyHostToDevice,
+                      c.stream));
+  WCK(cudaMemsetAsync(net.d_status, 0, sizeof(int32_t), c.stream));
+  const int64_t l0 = net.launches;
+  WCK(net.forward(c.stream, batch));
+  WCK(net.backward(c.stream, batch));
+  int32_t status = 0;
+  if (loss) WCK(cudaMemcpyAsync(loss, net.d_loss, sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+  if (grad) WCK(cudaMemcpyAsync(grad, net.d_grads, sizeof(float) * net.nparams, cudaMemcpyDeviceToHost, c.stream));
+  WCK(cudaMemcpyAsync(&status, net.d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
+  WCK(cudaStreamSynchronize(c.stream));
+  w->launches += net.launches - l0;
+  c.launches += net.launches - l0;
+  if (status) { c.err = "mlp_loss_grad: a tensor-core wait timed out"; return FAST_GPU_ECUDA; }
+  return FAST_GPU_OK;
+}
+
+extern "C" int fast_gpu_mlp_gemm(fast_gpu_ctx *c, int32_t M, int32_t N, int32_t K, const float *A, int32_t ta,
+                                 const float *B, int32_t tb, float *C) {
+  if (!c || M <= 0 || N <= 0 || K <= 0 || !A || !B || !C) return FAST_GPU_EINVAL;
+  float *dA = nullptr, *dB = nullptr, *dC = nullptr;
+  int32_t *dst = nullptr, status = 0;
+  cudaError_t e = cudaMalloc((void **)&dA, sizeof(float) * (size_t)M * K);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&dB, sizeof(float) * (size_t)N * K);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&dC, sizeof(float) * (size_t)M * N);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&dst, sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMemsetAsync(dst, 0, sizeof(int32_t), c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dA, A, sizeof(float) * (size_t)M * K, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dB, B, sizeof(float) * (size_t)N * K, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess)
+    e = gemm_bf16(c->stream, M, N, K, dA, ta ? M : K, ta != 0, dB, tb ? N : K, tb != 0, dC, N, kEpiStore, nullptr,
+                  nullptr, 0, dst);
+  c->launches++;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(C, dC, sizeof(float) * (size_t)M * N, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&status, dst, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  for (void *p : {(void *)dA, (void *)dB, (void *)dC, (void *)dst})
+    if (p) cudaFree(p);
+  if (e != cudaSuccess) { c->err = std::string("mlp_gemm: ") + cudaGetErrorString(e); return FAST_GPU_ECUDA; }
+  if (status) { c->err = "mlp_gemm: a tensor-core wait timed out"; return FAST_GPU_ECUDA; }
+  return FAST_GPU_OK;
+}

@@ -272,6 +272,18 @@ def plate_tl_hex8(nx=40, ny=40, nz=4, L=10.0, t=1.0, E=1000.0, nu=0.3, pressure=
                 title=f"TL hex8 plate {nx}x{ny}x{nz}, pressure {pressure}, {steps} steps")
 
 
+def plate_variant_params(seed: int, num_elems: int, E: float = 1000.0, p_range=(0.75, 1.25), e_range=(0.8, 1.25),
+                         e_sigma: float = 0.1):
+    """One seeded pressure/stiffness variant of a plate: (pressure scale,
+    Young's modulus per element).  The pressure scale is U[p_range]; the
+    modulus is E times a plate-wide factor U[e_range] times an element-wise
+    lognormal factor exp(e_sigma N(0, 1))."""
+    rng = np.random.default_rng(seed)
+    ps = float(rng.uniform(*p_range))
+    es = float(rng.uniform(*e_range))
+    return ps, E * es * np.exp(e_sigma * rng.standard_normal(num_elems))
+
+
 def read_pos_displacements(path: str, labels=None) -> np.ndarray:
     """Nodal displacements of every printed step of a FAST .pos file: [steps][nnode][3].
 

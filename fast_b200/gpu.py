@@ -44,7 +44,10 @@ EXPORTS = [
     "fast_gpu_get_lower_csr", "fast_gpu_element_matrices", "fast_gpu_launch_count", "fast_gpu_kernel_timing", "fast_gpu_kernel_stats",
     "fast_gpu_inspect_pattern", "fast_gpu_pcg_solve_noalloc", "fast_gpu_set_displacement",
     "fast_gpu_set_displacement_device", "fast_gpu_internal_force", "fast_gpu_internal_force_device",
-    "fast_gpu_nr_solve",
+    "fast_gpu_nr_solve", "fast_gpu_ws_create", "fast_gpu_ws_destroy", "fast_gpu_ws_add_trajectory",
+    "fast_gpu_ws_build_basis", "fast_gpu_ws_train", "fast_gpu_ws_predict", "fast_gpu_ws_report",
+    "fast_gpu_ws_get_basis", "fast_gpu_ws_get_samples", "fast_gpu_mlp_params", "fast_gpu_mlp_forward",
+    "fast_gpu_mlp_loss_grad", "fast_gpu_mlp_gemm",
 ]
 KERNEL_SPMV_FP64, KERNEL_SPMV_FP32, KERNEL_ASSEMBLE = 0, 1, 2
 
@@ -107,6 +110,23 @@ NR_PREDICTOR = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int32, c
 PREDICT_NONE, PREDICT_SECANT, PREDICT_CALLBACK = 0, 1, 2
 
 
+class WsOpts(ctypes.Structure):
+    _fields_ = [("modes", ctypes.c_int32), ("history", ctypes.c_int32), ("width", ctypes.c_int32),
+                ("hidden", ctypes.c_int32), ("oversample", ctypes.c_int32), ("power_iters", ctypes.c_int32),
+                ("seed", ctypes.c_uint64)]
+
+
+class WsStats(ctypes.Structure):
+    _fields_ = [("trajectories", ctypes.c_int32), ("snapshots", ctypes.c_int32), ("samples", ctypes.c_int32),
+                ("modes", ctypes.c_int32), ("input_dim", ctypes.c_int32), ("output_dim", ctypes.c_int32),
+                ("epochs", ctypes.c_int32), ("reserved", ctypes.c_int32), ("params", ctypes.c_int64),
+                ("captured_energy", ctypes.c_double), ("basis_ms", ctypes.c_double), ("train_ms", ctypes.c_double),
+                ("first_loss", ctypes.c_float), ("last_loss", ctypes.c_float), ("launches", ctypes.c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 _lib = None
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int32)
@@ -153,6 +173,22 @@ def load_library(path: str = LIB_PATH):
     L.fast_gpu_internal_force_device.argtypes = [vp, vp]
     L.fast_gpu_nr_solve.argtypes = [vp, _dp, ctypes.POINTER(NrOpts), NR_PREDICTOR, vp, _dp, _ip,
                                     ctypes.POINTER(NrReport)]
+    _fp = ctypes.POINTER(ctypes.c_float)
+    L.fast_gpu_ws_create.argtypes = [vp, ctypes.POINTER(WsOpts), ctypes.POINTER(vp)]
+    L.fast_gpu_ws_destroy.argtypes = [vp]
+    L.fast_gpu_ws_destroy.restype = None
+    L.fast_gpu_ws_add_trajectory.argtypes = [vp, ctypes.c_int32, _dp, _dp]
+    L.fast_gpu_ws_build_basis.argtypes = [vp, _dp]
+    L.fast_gpu_ws_train.argtypes = [vp, ctypes.c_int32, ctypes.c_float, _fp]
+    L.fast_gpu_ws_predict.argtypes = [vp, ctypes.c_int32, ctypes.c_double, vp, vp, vp]
+    L.fast_gpu_ws_report.argtypes = [vp, ctypes.POINTER(WsStats)]
+    L.fast_gpu_ws_get_basis.argtypes = [vp, _dp]
+    L.fast_gpu_ws_get_samples.argtypes = [vp, _fp, _fp]
+    L.fast_gpu_mlp_params.argtypes = [vp, _fp, _fp, _lp]
+    L.fast_gpu_mlp_forward.argtypes = [vp, ctypes.c_int32, _fp, _fp]
+    L.fast_gpu_mlp_loss_grad.argtypes = [vp, ctypes.c_int32, _fp, _fp, _fp, _fp]
+    L.fast_gpu_mlp_gemm.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _fp, ctypes.c_int32, _fp,
+                                    ctypes.c_int32, _fp]
     L.fast_gpu_kernel_timing.argtypes = [vp, ctypes.c_int32]
     L.fast_gpu_kernel_stats.argtypes = [vp, ctypes.c_int32, _lp, _dp, _dp]
     _lib = L
@@ -246,6 +282,21 @@ class GpuSystem:
         except Exception:
             pass
 
+    def mlp_gemm(self, A, B, ta=False, tb=False):
+        """The tensor-core GEMM alone: C = opA(A) opB(B)^T with opA = A^T when ta
+        (A given as [K][M]) and opB = B^T when tb (B given as [K][N])."""
+        A = np.ascontiguousarray(A, dtype=np.float32)
+        B = np.ascontiguousarray(B, dtype=np.float32)
+        M = A.shape[1] if ta else A.shape[0]
+        K = A.shape[0] if ta else A.shape[1]
+        N = B.shape[1] if tb else B.shape[0]
+        assert (B.shape[0] if tb else B.shape[1]) == K
+        C = np.zeros((M, N), np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        self._ck(self.L.fast_gpu_mlp_gemm(self.ctx, M, N, K, _p(A, fp), int(ta), _p(B, fp), int(tb), _p(C, fp)),
+                 "mlp_gemm")
+        return C
+
     def set_stream(self, stream_ptr: Optional[int]):
         self._ck(self.L.fast_gpu_set_stream(self.ctx, ctypes.c_void_p(stream_ptr or 0)), "set_stream")
 
@@ -289,7 +340,10 @@ class GpuSystem:
     # -- load-control Newton-Raphson (cCtrlNR::Solver)
     def nr_solve(self, q, steps, step_factor, tol=1e-8, max_iter=30, predictor=PREDICT_NONE, callback=None,
                  precision=PREC_FP64, precond=PRECOND_JACOBI, lin_tol=1e-12, lin_tol_rel=0.0, lin_tol_min=1e-12,
-                 lin_tol_max=1e-2, keep_history=True, raise_on_fail=True):
+                 lin_tol_max=1e-2, keep_history=True, raise_on_fail=True, learned=None):
+        """Load-control Newton-Raphson.  ``learned``: a trained
+        :class:`LearnedPredictor` used as the caller predictor (implies
+        ``predictor=PREDICT_CALLBACK``)."""
         q = np.ascontiguousarray(q, dtype=np.float64)
         lin = SolveOpts(precision, precond, 0, 0, float(lin_tol), 0.0, 0, 0)
         o = NrOpts(int(steps), int(max_iter), float(step_factor), float(tol), int(predictor), 0, lin,
@@ -297,8 +351,13 @@ class GpuSystem:
         hist = np.zeros((steps, self.neq)) if keep_history else None
         iters = np.zeros(steps, np.int32)
         rep = NrReport()
+        user = None
+        if learned is not None:
+            o.predictor = PREDICT_CALLBACK
+            callback = NR_PREDICTOR(("fast_gpu_ws_predict", self.L))
+            user = learned.handle
         cb = callback if callback is not None else NR_PREDICTOR()
-        rc = self.L.fast_gpu_nr_solve(self.ctx, _p(q), ctypes.byref(o), cb, None,
+        rc = self.L.fast_gpu_nr_solve(self.ctx, _p(q), ctypes.byref(o), cb, user,
                                       _p(hist) if hist is not None else _dp(), _p(iters, _ip), ctypes.byref(rep))
         if rc != FAST_GPU_OK and raise_on_fail:
             self._ck(rc, "nr_solve")
@@ -388,3 +447,97 @@ class GpuSystem:
         self._ck(self.L.fast_gpu_element_matrices(self.ctx, what, bucket, int(first), int(count), _p(out)),
                  "element_matrices")
         return out
+
+
+_fp = ctypes.POINTER(ctypes.c_float)
+
+
+class LearnedPredictor:
+    """The learned load-step predictor (fast_gpu_ws_*): POD basis of converged
+    displacements plus a tanh MLP trained on the device with BF16 tensor-core
+    GEMMs.  Pass it as ``GpuSystem.nr_solve(..., learned=p)``."""
+
+    def __init__(self, system: "GpuSystem", modes=32, history=4, width=256, hidden=2, oversample=16,
+                 power_iters=2, seed=0):
+        self.sys = system
+        self.L = system.L
+        o = WsOpts(int(modes), int(history), int(width), int(hidden), int(oversample), int(power_iters), int(seed))
+        h = ctypes.c_void_p()
+        system._ck(self.L.fast_gpu_ws_create(system.ctx, ctypes.byref(o), ctypes.byref(h)), "ws_create")
+        self.handle = h
+        self.modes, self.history, self.width, self.hidden = modes, history, width, hidden
+
+    def close(self):
+        if self.handle:
+            self.L.fast_gpu_ws_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_trajectory(self, lambdas, u_steps):
+        lam = np.ascontiguousarray(lambdas, dtype=np.float64)
+        u = np.ascontiguousarray(u_steps, dtype=np.float64)
+        assert u.shape == (len(lam), self.sys.neq)
+        self.sys._ck(self.L.fast_gpu_ws_add_trajectory(self.handle, len(lam), _p(lam), _p(u)), "ws_add_trajectory")
+
+    def build_basis(self):
+        e = ctypes.c_double()
+        self.sys._ck(self.L.fast_gpu_ws_build_basis(self.handle, ctypes.byref(e)), "ws_build_basis")
+        return e.value
+
+    def train(self, epochs=2000, lr=2e-3):
+        h = np.zeros(max(1, epochs), np.float32)
+        self.sys._ck(self.L.fast_gpu_ws_train(self.handle, int(epochs), float(lr), _p(h, _fp)), "ws_train")
+        return h[:epochs]
+
+    def report(self):
+        r = WsStats()
+        self.sys._ck(self.L.fast_gpu_ws_report(self.handle, ctypes.byref(r)), "ws_report")
+        return r.as_dict()
+
+    def basis(self):
+        k = self.report()["modes"]
+        phi = np.zeros((self.sys.neq, k))
+        self.sys._ck(self.L.fast_gpu_ws_get_basis(self.handle, _p(phi)), "ws_get_basis")
+        return phi
+
+    def samples(self):
+        r = self.report()
+        x = np.zeros((r["samples"], r["input_dim"]), np.float32)
+        t = np.zeros((r["samples"], r["output_dim"]), np.float32)
+        self.sys._ck(self.L.fast_gpu_ws_get_samples(self.handle, _p(x, _fp), _p(t, _fp)), "ws_get_samples")
+        return x, t
+
+    # -- the network alone
+    def params(self, set_to=None):
+        n = ctypes.c_int64()
+        self.sys._ck(self.L.fast_gpu_mlp_params(self.handle, None, None, ctypes.byref(n)), "mlp_params")
+        if set_to is not None:
+            p = np.ascontiguousarray(set_to, dtype=np.float32)
+            assert p.size == n.value
+            self.sys._ck(self.L.fast_gpu_mlp_params(self.handle, None, _p(p, _fp), None), "mlp_params")
+        out = np.zeros(n.value, np.float32)
+        self.sys._ck(self.L.fast_gpu_mlp_params(self.handle, _p(out, _fp), None, None), "mlp_params")
+        return out
+
+    def dims(self):
+        return [1 + self.history * self.modes] + [self.width] * self.hidden + [self.modes]
+
+    def forward(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.zeros((x.shape[0], self.modes), np.float32)
+        self.sys._ck(self.L.fast_gpu_mlp_forward(self.handle, x.shape[0], _p(x, _fp), _p(y, _fp)), "mlp_forward")
+        return y
+
+    def loss_grad(self, x, t):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        loss = np.zeros(1, np.float32)
+        g = np.zeros(self.params().size, np.float32)
+        self.sys._ck(self.L.fast_gpu_mlp_loss_grad(self.handle, x.shape[0], _p(x, _fp), _p(t, _fp), _p(loss, _fp),
+                                                   _p(g, _fp)), "mlp_loss_grad")
+        return float(loss[0]), g

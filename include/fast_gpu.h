@@ -196,6 +196,77 @@ int fast_gpu_nr_solve(fast_gpu_ctx *ctx, const double *q, const fast_gpu_nr_opts
                       fast_gpu_nr_predictor predictor, void *predictor_user, double *u_hist, int32_t *iters,
                       fast_gpu_nr_report *rep);
 
+/* ---- learned load-step predictor ------------------------------------------
+ * No counterpart in the reference (cCtrlNR starts every step from the last
+ * converged u).  A POD basis Phi (num_eq x modes) of converged displacements
+ * and a tanh MLP that maps the load factor lambda_s and the last `history`
+ * coefficient sets (a = Phi^T u), given as a_{s-1} and its history-1 backward
+ * differences, each scaled per mode, to the in-basis correction of the secant
+ * increment:
+ *   u_pred = u_{s-1} + rho (u_{s-1} - u_{s-2}) + Phi (tau * mlp(x)),
+ * rho = dlambda_s / dlambda_{s-1}.  The network trains and runs on the
+ * device with BF16 tensor-core GEMMs accumulating in FP32; the POD is FP64.
+ * fast_gpu_ws_predict has the fast_gpu_nr_predictor signature: pass it with
+ * the predictor object as user to fast_gpu_nr_solve (FAST_NR_PREDICT_CALLBACK);
+ * fast_gpu_nr_solve takes the prediction only when its residual is below the
+ * secant start's, and Newton iterates to the same tolerance either way. */
+typedef struct fast_gpu_ws fast_gpu_ws;
+
+typedef struct {
+  int32_t modes;        /* POD modes k (e.g. 32)                                 */
+  int32_t history;      /* coefficient sets in the network input (e.g. 4)       */
+  int32_t width;        /* hidden layer width (e.g. 256)                         */
+  int32_t hidden;       /* hidden layers (e.g. 2: in -> 256 -> 256 -> k)         */
+  int32_t oversample;   /* range-finder columns beyond k (e.g. 16)               */
+  int32_t power_iters;  /* range-finder power iterations (e.g. 2)                */
+  uint64_t seed;        /* initial weights and range-finder test matrix          */
+} fast_gpu_ws_opts;
+
+typedef struct {
+  int32_t trajectories, snapshots, samples, modes;
+  int32_t input_dim, output_dim, epochs, reserved;
+  int64_t params;
+  double captured_energy;   /* sum of the kept squared singular values / |S|_F^2 */
+  double basis_ms, train_ms;
+  float  first_loss, last_loss;
+  int64_t launches;         /* kernels launched by the predictor object           */
+} fast_gpu_ws_stats;
+
+/* The predictor lives on ctx's device and stream; ctx must hold a mesh. */
+int fast_gpu_ws_create(fast_gpu_ctx *ctx, const fast_gpu_ws_opts *opts, fast_gpu_ws **out);
+void fast_gpu_ws_destroy(fast_gpu_ws *ws);
+/* One training trajectory: the converged u of every load step (host,
+ * [steps][num_eq], e.g. fast_gpu_nr_solve's u_hist) and its load factors. */
+int fast_gpu_ws_add_trajectory(fast_gpu_ws *ws, int32_t steps, const double *lambda, const double *u_steps);
+/* POD basis of all snapshots added so far (randomized range finder, FP64). */
+int fast_gpu_ws_build_basis(fast_gpu_ws *ws, double *captured_energy);
+/* Full-batch Adam with a cosine learning-rate decay from lr; loss_history
+ * [epochs] (mean squared error in scaled units) may be NULL. */
+int fast_gpu_ws_train(fast_gpu_ws *ws, int32_t epochs, float lr, float *loss_history);
+/* fast_gpu_nr_predictor: user = the fast_gpu_ws.  Returns 0 with d_u_pred
+ * written, or non-zero (no prediction) before training. */
+int fast_gpu_ws_predict(void *ws, int32_t step, double lambda, const double *d_u_last, const double *d_u_prev,
+                        double *d_u_pred);
+int fast_gpu_ws_report(fast_gpu_ws *ws, fast_gpu_ws_stats *rep);
+/* Phi, host [num_eq][modes] row-major. */
+int fast_gpu_ws_get_basis(fast_gpu_ws *ws, double *phi);
+/* Training inputs [samples][input_dim] and targets [samples][modes] (scaled),
+ * as built by fast_gpu_ws_train; either may be NULL. */
+int fast_gpu_ws_get_samples(fast_gpu_ws *ws, float *x, float *t);
+
+/* The network alone (gradient checks against a CPU oracle).  Parameters are
+ * FP32, per layer W [out][in] row-major then b [out]. */
+int fast_gpu_mlp_params(fast_gpu_ws *ws, float *get, const float *set, int64_t *count);
+int fast_gpu_mlp_forward(fast_gpu_ws *ws, int32_t batch, const float *x, float *y);
+/* Mean squared error against t and its gradient with respect to every parameter. */
+int fast_gpu_mlp_loss_grad(fast_gpu_ws *ws, int32_t batch, const float *x, const float *t, float *loss,
+                           float *grad);
+/* The tensor-core GEMM by itself (host buffers): C[M][N] = sum_k opA(m,k) opB(n,k),
+ * opA(m,k) = ta ? A[k*M+m] : A[m*K+k], opB(n,k) = tb ? B[k*N+n] : B[n*K+k];
+ * FP32 in and out, BF16 products, FP32 accumulation. */
+int fast_gpu_mlp_gemm(fast_gpu_ctx *ctx, int32_t M, int32_t N, int32_t K, const float *A, int32_t ta,
+                      const float *B, int32_t tb, float *C);
+
 /* ---- cSysMatrix replacement (mlib/sysmat.h:60-99) ------------------------ */
 /* cSysMatrix::Zero */
 int fast_gpu_zero(fast_gpu_ctx *ctx, int32_t what);
