@@ -368,10 +368,12 @@ int fast_gpu_set_displacement(fast_gpu_ctx *c, const double *u) {
 
 int fast_gpu_internal_force_device(fast_gpu_ctx *c, double *d_g) {
   if (check_ctx(c) || !d_g || !c->d_gint) return FAST_GPU_EINVAL;
+  const int64_t sp = c->begin_span(FAST_KERNEL_INTERNAL_FORCE);
   CK(cudaMemsetAsync(c->d_status, 0, sizeof(int32_t), c->stream));
   CK(cudaMemsetAsync(c->d_gint, 0, sizeof(double) * 4 * c->nnode, c->stream));
   CK(launch_tl(*c, nullptr, c->d_gint, false, true));
   CK(launch_node_to_eq(*c, c->d_gint, d_g));
+  c->end_span(sp);
   return FAST_GPU_OK;
 }
 
@@ -547,10 +549,12 @@ int fast_gpu_solve_device(fast_gpu_ctx *c, const double *d_f, double *d_u, const
   if (check_ctx(c) || !d_f || !d_u) return FAST_GPU_EINVAL;
   if (!c->K_ok) { c->err = "solve: matrix not assembled"; return FAST_GPU_ESTATE; }
   const bool warm = o && o->warm_start;
+  const int64_t sp = c->begin_span(FAST_KERNEL_LINEAR_SOLVE);
   CK(launch_eq_to_node(*c, d_f, c->d_f));
   if (warm) CK(launch_eq_to_node(*c, d_u, c->d_u));
   const int rc = solve_node_space(c, o, warm, rep);
   if (rc == FAST_GPU_OK || rc == FAST_GPU_ENONCONV) CK(launch_node_to_eq(*c, c->d_u, d_u));
+  c->end_span(sp);
   return rc;
 }
 
@@ -680,12 +684,12 @@ int fast_gpu_kernel_timing(fast_gpu_ctx *c, int32_t enable) {
   CK(cudaStreamSynchronize(c->stream));
   c->harvest();
   c->timing = enable != 0;
-  for (int k = 0; k < 3; k++) { c->kt_ms[k] = 0; c->kt_n[k] = 0; }
+  for (int k = 0; k < Ctx::kSpanKinds; k++) { c->kt_ms[k] = 0; c->kt_n[k] = 0; }
   return FAST_GPU_OK;
 }
 
 int fast_gpu_kernel_stats(fast_gpu_ctx *c, int32_t which, int64_t *launches, double *total_ms, double *bytes) {
-  if (check_ctx(c) || which < 0 || which > 2) return FAST_GPU_EINVAL;
+  if (check_ctx(c) || which < 0 || which >= Ctx::kSpanKinds) return FAST_GPU_EINVAL;
   CK(cudaStreamSynchronize(c->stream));
   c->harvest();
   if (launches) *launches = c->kt_n[which];

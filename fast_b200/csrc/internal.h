@@ -127,18 +127,21 @@ struct Ctx {
     graph_fp64 = graph_mixed = nullptr;
   }
 
-  // live kernel timing: CUDA events around SpMV launches and assemblies
-  // (kind 0 FP64 SpMV, 1 FP32 SpMV, 2 assembly), harvested at each host sync
+  // live kernel timing: CUDA events around SpMV launches, assemblies, the
+  // learned predictor, internal forces and linear solves (the FAST_KERNEL_*
+  // kinds), harvested at each host sync; spans may nest
+  static constexpr int kSpanKinds = 7;
   bool timing = false;
   std::vector<cudaEvent_t> ev_pool;
-  struct Span { int kind; cudaEvent_t a, b; };
+  struct Span { int kind; int64_t id; bool closed; cudaEvent_t a, b; };
   std::vector<Span> spans;
-  double kt_ms[3] = {0, 0, 0};
-  int64_t kt_n[3] = {0, 0, 0};
+  int64_t span_ids = 0;
+  double kt_ms[kSpanKinds] = {};
+  int64_t kt_n[kSpanKinds] = {};
   cudaEvent_t take_event();
-  void begin_span(int kind);
-  void end_span();
-  void harvest();
+  int64_t begin_span(int kind);   // span id, -1 when timing is off
+  void end_span(int64_t id = -1); // -1: the most recent open span
+  void harvest();                 // closed spans only (call after a stream sync)
 
   bool set_error(const std::string &m) { err = m; return false; }
 };

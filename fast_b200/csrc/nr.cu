@@ -173,7 +173,7 @@ extern "C" int fast_gpu_nr_solve(fast_gpu_ctx *c, const double *q_host, const fa
       use_secant = true;
       if (o->predictor == FAST_NR_PREDICT_CALLBACK && predictor) {
         // the caller writes its prediction of u at this load level into du
-        const int prc = predictor(predictor_user, step, lam, w.u, w.up, w.du);
+        const int prc = predictor(predictor_user, step, lam, w.u, w.up, w.f, w.du);
         if (prc == 0) {
           NRRC(fast_gpu_set_displacement_device(c, w.du));
           NRRC(fast_gpu_internal_force_device(c, w.g));
@@ -221,18 +221,30 @@ extern "C" int fast_gpu_nr_solve(fast_gpu_ctx *c, const double *q_host, const fa
       NRRC(fast_gpu_assemble(c, FAST_ASM_STIFFNESS));  // tangent at u
       fast_gpu_solve_opts lo = o->lin;
       if (o->lin_tol_rel > 0) {
-        // inexact Newton: the linear tolerance follows the current residual
+        // inexact Newton: the forcing term follows the current residual, but
+        // never asks for more than what takes this iteration to the Newton
+        // tolerance (eta >= tol / (2 |r|), the safeguard of Kelley, Solving
+        // Nonlinear Equations with Newton's Method, SIAM 2003, sec. 3.2.3)
         const double err = std::sqrt(rlen2) / std::max(1.0, std::sqrt(flen2));
-        lo.tol = std::min(o->lin_tol_max > 0 ? o->lin_tol_max : 1e-2, std::max(o->lin_tol_min > 0 ? o->lin_tol_min : 1e-12,
-                                                                                o->lin_tol_rel * err));
+        const double eta = std::max(o->lin_tol_rel * err, err > 0 ? 0.5 * tol / err : 1.0);
+        lo.tol = std::min(o->lin_tol_max > 0 ? o->lin_tol_max : 1e-2,
+                          std::max(o->lin_tol_min > 0 ? o->lin_tol_min : 1e-12, eta));
       }
       fast_gpu_solve_report lr{};
       NRCK(cudaMemsetAsync(w.du, 0, nb, c->stream));
-      rc = fast_gpu_solve_device(c, w.r, w.du, &lo, &lr);
-      R.linear_iterations += lr.iterations;
-      if (rc != FAST_GPU_OK && rc != FAST_GPU_ENONCONV) goto done;
-      rc = FAST_GPU_OK;
-      NRCK(axpby(*c, 1.0, w.u, 1.0, w.du, w.u));  // u += du
+      {
+        // K du = r solved for the unit right-hand side r / |r|: PCGSolver's
+        // early exit on an absolute |rhs| < tol would otherwise return du = 0
+        // once the Newton residual falls below a loose relative tolerance
+        const double rn = std::sqrt(rlen2);
+        const double sc = rn > 0 ? 1.0 / rn : 1.0;
+        NRCK(axpby(*c, sc, w.r, 0.0, w.r, w.ucand));
+        rc = fast_gpu_solve_device(c, w.ucand, w.du, &lo, &lr);
+        R.linear_iterations += lr.iterations;
+        if (rc != FAST_GPU_OK && rc != FAST_GPU_ENONCONV) goto done;
+        rc = FAST_GPU_OK;
+        NRCK(axpby(*c, 1.0, w.u, rn > 0 ? rn : 1.0, w.du, w.u));  // u += |r| du
+      }
       NRRC(fast_gpu_set_displacement_device(c, w.u));
       NRRC(fast_gpu_internal_force_device(c, w.g));
       NRCK(axpby(*c, 1.0, w.f, -1.0, w.g, w.r));  // r = f - g

@@ -548,19 +548,31 @@ cudaEvent_t Ctx::take_event() {
   ev_pool.pop_back();
   return e;
 }
-void Ctx::begin_span(int kind) {
-  if (!timing) return;
-  Span sp{kind, take_event(), take_event()};
+int64_t Ctx::begin_span(int kind) {
+  if (!timing) return -1;
+  Span sp{kind, span_ids++, false, take_event(), take_event()};
   cudaEventRecord(sp.a, stream);
   spans.push_back(sp);
+  return sp.id;
 }
-void Ctx::end_span() {
-  if (!timing || spans.empty()) return;
-  cudaEventRecord(spans.back().b, stream);
+void Ctx::end_span(int64_t id) {
+  if (!timing) return;
+  for (int i = (int)spans.size() - 1; i >= 0; i--) {
+    Span &sp = spans[i];
+    if (sp.closed || (id >= 0 && sp.id != id)) continue;
+    cudaEventRecord(sp.b, stream);
+    sp.closed = true;
+    return;
+  }
 }
-// call after the stream has been synchronised
+// call after the stream has been synchronised; open spans stay
 void Ctx::harvest() {
+  std::vector<Span> open;
   for (Span &sp : spans) {
+    if (!sp.closed) {
+      open.push_back(sp);
+      continue;
+    }
     float ms = 0;
     if (cudaEventElapsedTime(&ms, sp.a, sp.b) == cudaSuccess) {
       kt_ms[sp.kind] += ms;
@@ -569,7 +581,7 @@ void Ctx::harvest() {
     ev_pool.push_back(sp.a);
     ev_pool.push_back(sp.b);
   }
-  spans.clear();
+  spans.swap(open);
 }
 
 static int spmv_grid(const Ctx &c) { return c.sm_count * 8; }

@@ -20,7 +20,6 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
-#include <map>
 #include <string>
 #include <vector>
 
@@ -33,17 +32,166 @@ struct fast_gpu_ctx : public Ctx {};
 
 namespace {
 
-__global__ void ws_combine(int32_t n, double rho, const double *__restrict__ ul, const double *__restrict__ up,
-                           const double *__restrict__ corr, double *__restrict__ out) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    out[i] = ul[i] + rho * (ul[i] - up[i]) + corr[i];
+// Phi_node[4 n + i][m] = Phi[eq][m] for the equation eq of DOF i of node n
+__global__ void ws_phi_to_node(int32_t neq, int k, const int32_t *__restrict__ dof, const double *__restrict__ phi,
+                               double *__restrict__ phin) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= (int64_t)neq * k) return;
+  const int64_t e = t / k;
+  const int m = (int)(t % k);
+  phin[(int64_t)dof[e] * k + m] = phi[t];
 }
 
-__global__ void ws_pack2(int32_t n, const double *__restrict__ a, const double *__restrict__ b,
-                         double *__restrict__ out) {
+// Y = K Phi_node with the assembled node-block matrix (AoS row-major 3x3
+// blocks, full pattern): one thread per (node row, mode); rows node-padded
+__global__ void ws_block_spmm(int64_t nnode, int k, const int32_t *__restrict__ rowptr,
+                              const int32_t *__restrict__ col, const double *__restrict__ K,
+                              const double *__restrict__ phin, double *__restrict__ Y) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= nnode * k) return;
+  const int64_t i = t / k;
+  const int m = (int)(t % k);
+  double y0 = 0.0, y1 = 0.0, y2 = 0.0;
+  for (int32_t b = rowptr[i]; b < rowptr[i + 1]; b++) {
+    const double *v = K + 9 * (int64_t)b;
+    const int64_t j = col[b];
+    const double x0 = phin[(4 * j + 0) * k + m], x1 = phin[(4 * j + 1) * k + m], x2 = phin[(4 * j + 2) * k + m];
+    y0 += v[0] * x0 + v[1] * x1 + v[2] * x2;
+    y1 += v[3] * x0 + v[4] * x1 + v[5] * x2;
+    y2 += v[6] * x0 + v[7] * x1 + v[8] * x2;
+  }
+  Y[(4 * i + 0) * k + m] = y0;
+  Y[(4 * i + 1) * k + m] = y1;
+  Y[(4 * i + 2) * k + m] = y2;
+  Y[(4 * i + 3) * k + m] = 0.0;
+}
+
+// u += Phi da
+__global__ void ws_add_phi(int32_t n, int k, const double *__restrict__ phi, const double *__restrict__ da,
+                           double *__restrict__ u) {
+  __shared__ double s[64];
+  if (threadIdx.x < k) s[threadIdx.x] = da[threadIdx.x];
+  __syncthreads();
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    out[i] = a[i];
-    out[n + i] = b[i];
+    double t = 0.0;
+    for (int m = 0; m < k; m++) t += phi[i * k + m] * s[m];
+    u[i] += t;
+  }
+}
+
+__global__ void ws_sub(int32_t n, const double *__restrict__ a, const double *__restrict__ b, double *__restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = a[i] - b[i];
+}
+
+// network input from the coefficient ring: slot[j] holds a_{s-j} (-1: zero)
+struct FeatArgs {
+  int k, kk, H;
+  double lambda;
+  int slot[18];
+};
+
+__global__ void ws_features(FeatArgs a, const double *__restrict__ ring, const double *__restrict__ sigma,
+                            const double *__restrict__ delta, float *__restrict__ x) {
+  const int nin = 1 + a.H * a.kk;
+  for (int t = threadIdx.x; t < nin; t += blockDim.x) {
+    float v = 0.f;
+    if (t == 0) {
+      v = (float)a.lambda;
+    } else {
+      const int h = (t - 1) / a.kk, j = (t - 1) % a.kk;
+      if (j < a.k) {
+        // block 0: a_{s-1} / sigma;  block h >= 1: (a_{s-h} - a_{s-h-1}) / delta
+        const int sp = a.slot[h == 0 ? 1 : h], sq = a.slot[h + 1];
+        const double p = sp < 0 ? 0.0 : ring[sp * 64 + j];
+        if (h == 0) {
+          v = (float)(p / sigma[j]);
+        } else {
+          const double q = sq < 0 ? 0.0 : ring[sq * 64 + j];
+          v = (float)((p - q) / delta[j]);
+        }
+      }
+    }
+    x[t] = v;
+  }
+}
+
+// start = u_last + rho (u_last - u_prev) + Phi (tau * y)   (y: network output, or none)
+__global__ void ws_start(int32_t n, int k, double rho, const double *__restrict__ ul, const double *__restrict__ up,
+                         const double *__restrict__ phi, const double *__restrict__ tau, const float *__restrict__ y,
+                         double *__restrict__ out) {
+  __shared__ double cf[64];
+  if (threadIdx.x < k) cf[threadIdx.x] = y ? tau[threadIdx.x] * (double)y[threadIdx.x] : 0.0;
+  __syncthreads();
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double t = ul[i] + rho * (ul[i] - up[i]);
+    if (y)
+      for (int m = 0; m < k; m++) t += phi[i * k + m] * cf[m];
+    out[i] = t;
+  }
+}
+
+// Cholesky factor of the (symmetrised) reduced tangent, one block; ok = 0
+// when a pivot is not positive
+__global__ void ws_chol(int k, const double *__restrict__ E, double *__restrict__ L, int32_t *__restrict__ ok) {
+  __shared__ double A[64][65];
+  __shared__ int bad;
+  __shared__ double dmax;
+  for (int t = threadIdx.x; t < k * k; t += blockDim.x) {
+    const int i = t / k, j = t % k;
+    A[i][j] = 0.5 * (E[i * k + j] + E[j * k + i]);
+  }
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int i = 0; i < k; i++) m = fmax(m, fabs(A[i][i]));
+    dmax = m;
+  }
+  __syncthreads();
+  for (int j = 0; j < k; j++) {
+    if (threadIdx.x == 0) {
+      double d = A[j][j];
+      for (int p = 0; p < j; p++) d -= A[j][p] * A[j][p];
+      if (!(d > 1e-14 * dmax)) { bad = 1; d = 1.0; }
+      A[j][j] = sqrt(d);
+    }
+    __syncthreads();
+    for (int i = j + 1 + threadIdx.x; i < k; i += blockDim.x) {
+      double v = A[i][j];
+      for (int p = 0; p < j; p++) v -= A[i][p] * A[j][p];
+      A[i][j] = v / A[j][j];
+    }
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < k * k; t += blockDim.x) {
+    const int i = t / k, j = t % k;
+    L[t] = j <= i ? A[i][j] : 0.0;
+  }
+  if (threadIdx.x == 0) *ok = bad ? 0 : 1;
+}
+
+// da = (L L^T)^-1 t, or 0 when the factor failed or |t| <= tol |tf|
+__global__ void ws_reduced_solve(int k, const double *__restrict__ L, const int32_t *__restrict__ ok,
+                                 const double *__restrict__ t, const double *__restrict__ tf, double tol,
+                                 double *__restrict__ da) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double tn = 0.0, fn = 0.0;
+  for (int j = 0; j < k; j++) { tn += t[j] * t[j]; fn += tf[j] * tf[j]; }
+  if (!*ok || !(sqrt(tn) > tol * sqrt(fn))) {
+    for (int j = 0; j < k; j++) da[j] = 0.0;
+    return;
+  }
+  double y[64];
+  for (int i = 0; i < k; i++) {
+    double v = t[i];
+    for (int p = 0; p < i; p++) v -= L[i * k + p] * y[p];
+    y[i] = v / L[i * k + i];
+  }
+  for (int i = k - 1; i >= 0; i--) {
+    double v = y[i];
+    for (int p = i + 1; p < k; p++) v -= L[p * k + i] * da[p];
+    da[i] = v / L[i * k + i];
   }
 }
 
@@ -86,15 +234,25 @@ struct fast_gpu_ws {
   // dgemm split workspace and prediction scratch
   double *d_ws = nullptr;
   size_t ws_cap = 0;
-  double *d_pair = nullptr;      // [2][n]
-  double *d_coef = nullptr;      // [2][k]
-  double *d_corr = nullptr;      // [n]
-  double *d_delta = nullptr;     // [k]
-  double *h_buf = nullptr;       // pinned [2k]
-  float *h_y = nullptr;          // pinned [k]
-  // coefficient history of the current solve (host), by step
-  std::map<int, std::vector<double>> hist;
-  int last_step = 0;
+  double *d_coef = nullptr;      // [2][64]: Phi^T r, Phi^T f
+  double *d_delta = nullptr;     // [64] reduced correction
+  int last_step = 0;             // step of the last prediction (a smaller one starts a new solve)
+  // POD coefficients of recent converged steps (device ring), by step
+  static constexpr int kRing = 18;
+  double *d_ring = nullptr;      // [kRing][64]
+  int ring_step[kRing];
+  double *d_scales = nullptr;    // [3][64] sigma, delta, tau
+  // Galerkin refinement of the start in the basis
+  int use_network = 1, gal_iters = 0;
+  double gal_tol = 1e-3;
+  double *d_phin = nullptr;      // [nnode*4][k] basis in the node-padded layout
+  double *d_Y = nullptr;         // [nnode*4][k] K Phi
+  double *d_Er = nullptr;        // [64*64] Phi^T K Phi
+  double *d_L = nullptr;         // [64*64] its Cholesky factor
+  int32_t *d_ok = nullptr;
+  double *d_g = nullptr, *d_r = nullptr;  // [n]
+  int64_t n_pred = 0, n_gal = 0;
+  double pred_ms = 0.0;
 
   bool fail(const std::string &m) { c->err = "ws: " + m; return false; }
   cudaError_t ensure_ws(int M, int N, int K) {
@@ -178,12 +336,16 @@ extern "C" int fast_gpu_ws_create(fast_gpu_ctx *ctx, const fast_gpu_ws_opts *opt
   for (int i = 0; i < opts->hidden; i++) dims.push_back(opts->width);
   dims.push_back(opts->modes);
   cudaError_t e = w->net.init(dims, opts->seed);
-  if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_pair, sizeof(double) * 2 * (size_t)w->n);
-  if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_corr, sizeof(double) * (size_t)w->n);
   if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_coef, sizeof(double) * 2 * 64);
   if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_delta, sizeof(double) * 64);
-  if (e == cudaSuccess) e = cudaMallocHost((void **)&w->h_buf, sizeof(double) * 2 * 64);
-  if (e == cudaSuccess) e = cudaMallocHost((void **)&w->h_y, sizeof(float) * 64);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_ring, sizeof(double) * fast_gpu_ws::kRing * 64);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_scales, sizeof(double) * 3 * 64);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_Er, sizeof(double) * 64 * 64);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_L, sizeof(double) * 64 * 64);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_ok, sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_g, sizeof(double) * (size_t)w->n);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_r, sizeof(double) * (size_t)w->n);
+  for (int i = 0; i < fast_gpu_ws::kRing; i++) w->ring_step[i] = -1;
   if (e != cudaSuccess) {
     ctx->err = std::string("ws_create: ") + cudaGetErrorString(e);
     fast_gpu_ws_destroy(w);
@@ -197,10 +359,10 @@ extern "C" void fast_gpu_ws_destroy(fast_gpu_ws *w) {
   if (!w) return;
   if (w->c) cudaStreamSynchronize(w->c->stream);
   for (double *p : w->traj) cudaFree(p);
-  for (double *p : {w->d_phi, w->d_ws, w->d_pair, w->d_coef, w->d_corr, w->d_delta})
+  for (double *p : {w->d_phi, w->d_ws, w->d_coef, w->d_delta, w->d_ring, w->d_scales, w->d_phin, w->d_Y, w->d_Er,
+                    w->d_L, w->d_g, w->d_r})
     if (p) cudaFree(p);
-  if (w->h_buf) cudaFreeHost(w->h_buf);
-  if (w->h_y) cudaFreeHost(w->h_y);
+  if (w->d_ok) cudaFree(w->d_ok);
   w->net.release();
   delete w;
 }
@@ -288,6 +450,18 @@ extern "C" int fast_gpu_ws_build_basis(fast_gpu_ws *w, double *captured_energy) 
     if (w->d_phi) { cudaFree(w->d_phi); w->d_phi = nullptr; }
     if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_phi, sizeof(double) * (size_t)n * k);
     if (e == cudaSuccess) e = w->gemm(n, k, r, Q, r, false, d_u, k, false, w->d_phi, k);  // Phi = Q U_k
+    for (double **p : {&w->d_phin, &w->d_Y})
+      if (*p) { cudaFree(*p); *p = nullptr; }
+    const size_t nrow = 4 * (size_t)c.nnode;
+    if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_phin, sizeof(double) * nrow * k);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_Y, sizeof(double) * nrow * k);
+    if (e == cudaSuccess) e = cudaMemsetAsync(w->d_phin, 0, sizeof(double) * nrow * k, c.stream);
+    if (e == cudaSuccess) {
+      const int64_t tot = (int64_t)n * k;
+      ws_phi_to_node<<<(unsigned)((tot + 255) / 256), 256, 0, c.stream>>>(n, k, c.d_dof_of_eq, w->d_phi, w->d_phin);
+      w->launches++;
+      e = cudaGetLastError();
+    }
     if (e == cudaSuccess) e = launch_norm2(c, S, (int64_t)m * n, d_fro);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&fro, d_fro, sizeof(double), cudaMemcpyDeviceToHost, c.stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
@@ -437,64 +611,128 @@ extern "C" int fast_gpu_ws_train(fast_gpu_ws *w, int32_t epochs, float lr, float
   if (loss_history && epochs > 0) std::memcpy(loss_history, hh.data(), sizeof(float) * epochs);
   w->epochs = epochs;
   if (epochs > 0) { w->first_loss = hh[0]; w->last_loss = hh[epochs - 1]; }
+  {
+    std::vector<double> sc(3 * 64, 1.0);
+    for (int j = 0; j < w->k; j++) {
+      sc[j] = w->sigma[j];
+      sc[64 + j] = w->delta[j];
+      sc[128 + j] = w->tau[j];
+    }
+    WCK(cudaMemcpy(w->d_scales, sc.data(), sizeof(double) * sc.size(), cudaMemcpyHostToDevice));
+  }
   w->trained = true;
-  w->hist.clear();
   w->last_step = 0;
+  for (int i = 0; i < fast_gpu_ws::kRing; i++) w->ring_step[i] = -1;
   w->train_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   return FAST_GPU_OK;
 }
 
 extern "C" int fast_gpu_ws_predict(void *user, int32_t step, double lambda, const double *d_u_last,
-                                   const double *d_u_prev, double *d_u_pred) {
+                                   const double *d_u_prev, const double *d_f, double *d_u_pred) {
+  // Everything below is stream-ordered device work: no host synchronisation.
   fast_gpu_ws *w = static_cast<fast_gpu_ws *>(user);
   if (!w || !d_u_last || !d_u_prev || !d_u_pred || step < 2) return FAST_GPU_EINVAL;
   if (!w->trained) return FAST_GPU_ESTATE;
+  if (w->gal_iters > 0 && !d_f) return FAST_GPU_EINVAL;
+  const auto t0 = std::chrono::steady_clock::now();
   Ctx &c = *w->c;
   const int n = w->n, k = w->k, kk = w->o.modes, H = w->o.history;
-  if (step <= w->last_step) w->hist.clear();  // a new solve
+  constexpr int R = fast_gpu_ws::kRing;
+  const int64_t l_start = w->launches;
+  if (step <= w->last_step)  // a new solve
+    for (int i = 0; i < R; i++) w->ring_step[i] = -1;
   w->last_step = step;
-  // a_last, a_prev = Phi^T u  (one GEMM over both vectors)
-  ws_pack2<<<148, 256, 0, c.stream>>>(n, d_u_last, d_u_prev, w->d_pair);
-  w->launches++;
-  WCK(w->gemm(2, k, n, w->d_pair, n, false, w->d_phi, k, false, w->d_coef, k));
-  WCK(cudaMemcpyAsync(w->h_buf, w->d_coef, sizeof(double) * 2 * k, cudaMemcpyDeviceToHost, c.stream));
-  WCK(cudaStreamSynchronize(c.stream));
-  w->hist[step - 1].assign(w->h_buf, w->h_buf + k);
-  w->hist[step - 2].assign(w->h_buf + k, w->h_buf + 2 * k);
   // load factors of the two previous steps: proportional loading with equal steps
   const double lam1 = lambda * (step - 1) / step, lam2 = lambda * (step - 2) / step;
   const double rho = (lam1 - lam2) != 0.0 ? (lambda - lam1) / (lam1 - lam2) : 1.0;
-  // a_s of this solve: zero before the first step; a missing (skipped) step
-  // repeats the closest earlier one that is known
-  auto a_of = [&](int s, int j) -> double {
-    for (; s > 0; s--) {
-      auto it = w->hist.find(s);
-      if (it != w->hist.end()) return it->second[j];
+  const double *tau = w->d_scales + 128;
+  const float *y = nullptr;
+  const int64_t span_net = c.begin_span(FAST_KERNEL_PREDICT_NET);
+  if (w->use_network) {
+    // a_{s-1} = Phi^T u_last, a_{s-2} = Phi^T u_prev into the ring
+    const int s1 = (step - 1) % R, s2 = (step - 2) % R;
+    WCK(w->gemm(1, k, n, d_u_last, n, false, w->d_phi, k, false, w->d_ring + s1 * 64, k));
+    w->ring_step[s1] = step - 1;
+    if (step - 2 >= 1) {
+      WCK(w->gemm(1, k, n, d_u_prev, n, false, w->d_phi, k, false, w->d_ring + s2 * 64, k));
+      w->ring_step[s2] = step - 2;
     }
-    return 0.0;
-  };
-  std::vector<float> x(w->in_dim, 0.f);
-  x[0] = (float)lambda;
-  for (int j = 0; j < k; j++) x[1 + j] = (float)(a_of(step - 1, j) / w->sigma[j]);
-  for (int h = 1; h < H; h++)
-    for (int j = 0; j < k; j++)
-      x[1 + h * kk + j] = (float)((a_of(step - h, j) - a_of(step - h - 1, j)) / w->delta[j]);
-  Mlp &net = w->net;
-  WCK(net.reserve(1));
-  WCK(cudaMemcpyAsync(net.d_h[0], x.data(), sizeof(float) * w->in_dim, cudaMemcpyHostToDevice, c.stream));
-  const int64_t l0 = net.launches;
-  WCK(net.forward(c.stream, 1));
-  WCK(cudaMemcpyAsync(w->h_y, net.d_h[net.layers()], sizeof(float) * kk, cudaMemcpyDeviceToHost, c.stream));
-  WCK(cudaStreamSynchronize(c.stream));
-  w->launches += net.launches - l0;
-  std::vector<double> delta(k);
-  for (int j = 0; j < k; j++) delta[j] = w->tau[j] * (double)w->h_y[j];
-  WCK(cudaMemcpyAsync(w->d_delta, delta.data(), sizeof(double) * k, cudaMemcpyHostToDevice, c.stream));
-  WCK(w->gemm(n, 1, k, w->d_phi, k, false, w->d_delta, 1, false, w->d_corr, 1));  // Phi delta
-  ws_combine<<<148, 256, 0, c.stream>>>(n, rho, d_u_last, d_u_prev, w->d_corr, d_u_pred);
+    FeatArgs fa{};
+    fa.k = k;
+    fa.kk = kk;
+    fa.H = H;
+    fa.lambda = lambda;
+    for (int j = 0; j < 18; j++) fa.slot[j] = -1;
+    for (int j = 1; j <= H + 1 && j < 18; j++) {
+      // a_{s-j}: zero before the first step; a step missing from the ring
+      // repeats the closest earlier one that is there
+      for (int st = step - j; st >= 1; st--)
+        if (w->ring_step[st % R] == st) { fa.slot[j] = st % R; break; }
+    }
+    Mlp &net = w->net;
+    WCK(net.reserve(1));
+    ws_features<<<1, 256, 0, c.stream>>>(fa, w->d_ring, w->d_scales, w->d_scales + 64, net.d_h[0]);
+    w->launches++;
+    const int64_t l0 = net.launches;
+    WCK(net.forward(c.stream, 1));
+    w->launches += net.launches - l0;
+    y = net.d_h[net.layers()];
+  }
+  ws_start<<<148, 256, 0, c.stream>>>(n, k, rho, d_u_last, d_u_prev, w->d_phi, tau, y, d_u_pred);
   w->launches++;
-  c.launches += 2 + (net.launches - l0) + 2;
   WCK(cudaGetLastError());
+  c.end_span(span_net);
+
+  if (w->gal_iters > 0 && c.d_K && c.K_ok) {
+    const int64_t span_gal = c.begin_span(FAST_KERNEL_PREDICT_GALERKIN);
+    // reduced tangent Phi^T K Phi from the last assembled tangent, its
+    // Cholesky factor, and Phi^T f
+    const int64_t nrow = 4 * c.nnode;
+    const int64_t tot = c.nnode * k;
+    ws_block_spmm<<<(unsigned)((tot + 127) / 128), 128, 0, c.stream>>>(c.nnode, k, c.d_rowptr, c.d_col, c.d_K,
+                                                                         w->d_phin, w->d_Y);
+    w->launches++;
+    WCK(w->gemm(k, k, (int)nrow, w->d_phin, k, true, w->d_Y, k, false, w->d_Er, k));
+    ws_chol<<<1, 64, 0, c.stream>>>(k, w->d_Er, w->d_L, w->d_ok);
+    w->launches++;
+    WCK(w->gemm(1, k, n, d_f, n, false, w->d_phi, k, false, w->d_coef + 64, k));
+    fast_gpu_ctx *fc = static_cast<fast_gpu_ctx *>(w->c);
+    for (int it = 0; it < w->gal_iters; it++) {
+      int rc = fast_gpu_set_displacement_device(fc, d_u_pred);
+      if (rc == FAST_GPU_OK) rc = fast_gpu_internal_force_device(fc, w->d_g);
+      if (rc != FAST_GPU_OK) return rc;
+      ws_sub<<<148, 256, 0, c.stream>>>(n, d_f, w->d_g, w->d_r);
+      w->launches++;
+      WCK(w->gemm(1, k, n, w->d_r, n, false, w->d_phi, k, false, w->d_coef, k));  // Phi^T r
+      ws_reduced_solve<<<1, 32, 0, c.stream>>>(k, w->d_L, w->d_ok, w->d_coef, w->d_coef + 64, w->gal_tol,
+                                                w->d_delta);
+      ws_add_phi<<<148, 256, 0, c.stream>>>(n, k, w->d_phi, w->d_delta, d_u_pred);
+      w->launches += 2;
+      w->n_gal++;
+    }
+    WCK(cudaGetLastError());
+    c.end_span(span_gal);
+  }
+  w->n_pred++;
+  c.launches += w->launches - l_start;
+  w->pred_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return FAST_GPU_OK;
+}
+
+extern "C" int fast_gpu_ws_configure(fast_gpu_ws *w, int32_t use_network, int32_t galerkin_iters,
+                                     double galerkin_tol) {
+  if (!w || galerkin_iters < 0 || !(galerkin_tol >= 0.0)) return FAST_GPU_EINVAL;
+  w->use_network = use_network ? 1 : 0;
+  w->gal_iters = galerkin_iters;
+  w->gal_tol = galerkin_tol;
+  return FAST_GPU_OK;
+}
+
+extern "C" int fast_gpu_ws_last_input(fast_gpu_ws *w, float *x) {
+  if (!w || !x) return FAST_GPU_EINVAL;
+  if (w->n_pred == 0 || !w->use_network) { w->c->err = "ws_last_input: no network prediction yet"; return FAST_GPU_ESTATE; }
+  WCK(cudaMemcpyAsync(x, w->net.d_h[0], sizeof(float) * w->in_dim, cudaMemcpyDeviceToHost, w->c->stream));
+  WCK(cudaStreamSynchronize(w->c->stream));
   return FAST_GPU_OK;
 }
 
@@ -515,6 +753,9 @@ extern "C" int fast_gpu_ws_report(fast_gpu_ws *w, fast_gpu_ws_stats *r) {
   R.first_loss = w->first_loss;
   R.last_loss = w->last_loss;
   R.launches = w->launches;
+  R.predictions = w->n_pred;
+  R.galerkin_iterations = w->n_gal;
+  R.predict_ms = w->pred_ms;
   *r = R;
   return FAST_GPU_OK;
 }

@@ -47,9 +47,10 @@ EXPORTS = [
     "fast_gpu_nr_solve", "fast_gpu_ws_create", "fast_gpu_ws_destroy", "fast_gpu_ws_add_trajectory",
     "fast_gpu_ws_build_basis", "fast_gpu_ws_train", "fast_gpu_ws_predict", "fast_gpu_ws_report",
     "fast_gpu_ws_get_basis", "fast_gpu_ws_get_samples", "fast_gpu_mlp_params", "fast_gpu_mlp_forward",
-    "fast_gpu_mlp_loss_grad", "fast_gpu_mlp_gemm",
+    "fast_gpu_mlp_loss_grad", "fast_gpu_mlp_gemm", "fast_gpu_ws_configure", "fast_gpu_ws_last_input",
 ]
 KERNEL_SPMV_FP64, KERNEL_SPMV_FP32, KERNEL_ASSEMBLE = 0, 1, 2
+KERNEL_PREDICT_NET, KERNEL_PREDICT_GALERKIN, KERNEL_INTERNAL_FORCE, KERNEL_LINEAR_SOLVE = 3, 4, 5, 6
 
 
 class FastGpuError(RuntimeError):
@@ -104,9 +105,10 @@ class NrReport(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
-# int (*)(void *user, int32 step, double lambda, const double *d_u_last, const double *d_u_prev, double *d_u_pred)
+# int (*)(void *user, int32 step, double lambda, const double *d_u_last, const double *d_u_prev, const double *d_f,
+#         double *d_u_pred)
 NR_PREDICTOR = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int32, ctypes.c_double, ctypes.c_void_p,
-                                ctypes.c_void_p, ctypes.c_void_p)
+                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p)
 PREDICT_NONE, PREDICT_SECANT, PREDICT_CALLBACK = 0, 1, 2
 
 
@@ -121,7 +123,9 @@ class WsStats(ctypes.Structure):
                 ("modes", ctypes.c_int32), ("input_dim", ctypes.c_int32), ("output_dim", ctypes.c_int32),
                 ("epochs", ctypes.c_int32), ("reserved", ctypes.c_int32), ("params", ctypes.c_int64),
                 ("captured_energy", ctypes.c_double), ("basis_ms", ctypes.c_double), ("train_ms", ctypes.c_double),
-                ("first_loss", ctypes.c_float), ("last_loss", ctypes.c_float), ("launches", ctypes.c_int64)]
+                ("first_loss", ctypes.c_float), ("last_loss", ctypes.c_float), ("launches", ctypes.c_int64),
+                ("predictions", ctypes.c_int64), ("galerkin_iterations", ctypes.c_int64),
+                ("predict_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -180,7 +184,9 @@ def load_library(path: str = LIB_PATH):
     L.fast_gpu_ws_add_trajectory.argtypes = [vp, ctypes.c_int32, _dp, _dp]
     L.fast_gpu_ws_build_basis.argtypes = [vp, _dp]
     L.fast_gpu_ws_train.argtypes = [vp, ctypes.c_int32, ctypes.c_float, _fp]
-    L.fast_gpu_ws_predict.argtypes = [vp, ctypes.c_int32, ctypes.c_double, vp, vp, vp]
+    L.fast_gpu_ws_predict.argtypes = [vp, ctypes.c_int32, ctypes.c_double, vp, vp, vp, vp]
+    L.fast_gpu_ws_configure.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double]
+    L.fast_gpu_ws_last_input.argtypes = [vp, _fp]
     L.fast_gpu_ws_report.argtypes = [vp, ctypes.POINTER(WsStats)]
     L.fast_gpu_ws_get_basis.argtypes = [vp, _dp]
     L.fast_gpu_ws_get_samples.argtypes = [vp, _fp, _fp]
@@ -477,6 +483,18 @@ class LearnedPredictor:
             self.close()
         except Exception:
             pass
+
+    def configure(self, use_network=True, galerkin_iters=0, galerkin_tol=1e-3):
+        """Start from the network's prediction (or the secant start) and refine
+        it with `galerkin_iters` reduced Newton corrections in the basis."""
+        self.sys._ck(self.L.fast_gpu_ws_configure(self.handle, int(bool(use_network)), int(galerkin_iters),
+                                                  float(galerkin_tol)), "ws_configure")
+
+    def last_input(self):
+        """Network input of the last prediction (scaled features)."""
+        x = np.zeros(self.dims()[0], np.float32)
+        self.sys._ck(self.L.fast_gpu_ws_last_input(self.handle, _p(x, _fp)), "ws_last_input")
+        return x
 
     def add_trajectory(self, lambdas, u_steps):
         lam = np.ascontiguousarray(lambdas, dtype=np.float64)

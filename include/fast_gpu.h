@@ -169,8 +169,9 @@ typedef struct {
   int32_t predictor;          /* FAST_NR_PREDICT_*                                   */
   int32_t reserved;
   fast_gpu_solve_opts lin;    /* linear solves K du = r                             */
-  double  lin_tol_rel;        /* > 0: linear tol = clamp(lin_tol_rel * Newton error,
-                                 lin_tol_min, lin_tol_max); 0: lin.tol as given       */
+  double  lin_tol_rel;        /* > 0: inexact Newton, linear tol = clamp(max(lin_tol_rel *
+                                 err, tol / (2 err)), lin_tol_min, lin_tol_max) with err
+                                 the current Newton error; 0: lin.tol as given        */
   double  lin_tol_min, lin_tol_max;
 } fast_gpu_nr_opts;
 
@@ -186,9 +187,11 @@ typedef struct {
 
 /* Caller predictor: write the predicted u at load factor lambda (step >= 2)
  * into d_u_pred (device, equation space) and return 0, or return non-zero to
- * skip.  d_u_last / d_u_prev are the last two converged solutions. */
+ * skip.  d_u_last / d_u_prev are the last two converged solutions, d_f the
+ * external load of this step (lambda q).  The context's displacement state
+ * may be changed by the predictor. */
 typedef int (*fast_gpu_nr_predictor)(void *user, int32_t step, double lambda, const double *d_u_last,
-                                     const double *d_u_prev, double *d_u_pred);
+                                     const double *d_u_prev, const double *d_f, double *d_u_pred);
 
 /* q: reference load (host, num_eq).  u_hist (host, [steps][num_eq]) and iters
  * ([steps], -1 for a failed step) may be NULL. */
@@ -230,6 +233,8 @@ typedef struct {
   double basis_ms, train_ms;
   float  first_loss, last_loss;
   int64_t launches;         /* kernels launched by the predictor object           */
+  int64_t predictions, galerkin_iterations;
+  double predict_ms;        /* host time inside fast_gpu_ws_predict               */
 } fast_gpu_ws_stats;
 
 /* The predictor lives on ctx's device and stream; ctx must hold a mesh. */
@@ -244,15 +249,26 @@ int fast_gpu_ws_build_basis(fast_gpu_ws *ws, double *captured_energy);
  * [epochs] (mean squared error in scaled units) may be NULL. */
 int fast_gpu_ws_train(fast_gpu_ws *ws, int32_t epochs, float lr, float *loss_history);
 /* fast_gpu_nr_predictor: user = the fast_gpu_ws.  Returns 0 with d_u_pred
- * written, or non-zero (no prediction) before training. */
+ * written, or non-zero (no prediction) before training.  Stream-ordered
+ * device work only (no host synchronisation).  The network's start (or, with
+ * use_network = 0, the secant start) is refined by galerkin_iters reduced
+ * Newton corrections in the POD basis,
+ *   a += (Phi^T K Phi)^-1 Phi^T (f - g(u)),  u = u_start + Phi a,
+ * with K the context's last assembled tangent; a correction is skipped when
+ * |Phi^T r| <= galerkin_tol |Phi^T f| or Phi^T K Phi is not positive definite
+ * (POD-Galerkin projection of the step's equilibrium). */
 int fast_gpu_ws_predict(void *ws, int32_t step, double lambda, const double *d_u_last, const double *d_u_prev,
-                        double *d_u_pred);
+                        const double *d_f, double *d_u_pred);
+/* Defaults: use_network 1, galerkin_iters 0, galerkin_tol 1e-3. */
+int fast_gpu_ws_configure(fast_gpu_ws *ws, int32_t use_network, int32_t galerkin_iters, double galerkin_tol);
 int fast_gpu_ws_report(fast_gpu_ws *ws, fast_gpu_ws_stats *rep);
 /* Phi, host [num_eq][modes] row-major. */
 int fast_gpu_ws_get_basis(fast_gpu_ws *ws, double *phi);
 /* Training inputs [samples][input_dim] and targets [samples][modes] (scaled),
  * as built by fast_gpu_ws_train; either may be NULL. */
 int fast_gpu_ws_get_samples(fast_gpu_ws *ws, float *x, float *t);
+/* The network input [input_dim] of the last fast_gpu_ws_predict. */
+int fast_gpu_ws_last_input(fast_gpu_ws *ws, float *x);
 
 /* The network alone (gradient checks against a CPU oracle).  Parameters are
  * FP32, per layer W [out][in] row-major then b [out]. */
@@ -323,14 +339,20 @@ int fast_gpu_element_matrices(fast_gpu_ctx *ctx, int32_t what, int32_t bucket, i
 #define FAST_KERNEL_SPMV_FP64  0   /* K.p with FP64 values (FP64 PCG, FP64 residuals)       */
 #define FAST_KERNEL_SPMV_FP32  1   /* K.p with FP32 values (mixed path)                     */
 #define FAST_KERNEL_ASSEMBLE   2   /* one stiffness assembly (zero fill + all colours)      */
+#define FAST_KERNEL_PREDICT_NET       3  /* learned predictor: projections, network, start */
+#define FAST_KERNEL_PREDICT_GALERKIN  4  /* learned predictor: reduced Newton corrections  */
+#define FAST_KERNEL_INTERNAL_FORCE    5  /* one internal-force evaluation                  */
+#define FAST_KERNEL_LINEAR_SOLVE      6  /* one fast_gpu_solve_device call                 */
 /* Kernels this context has launched so far (every entry point counts). */
 int fast_gpu_launch_count(fast_gpu_ctx *ctx, int64_t *count);
-/* Live timing: while enabled, every SpMV launched by a solve and every
- * stiffness assembly is bracketed by CUDA events on the context's stream.
- * Enabling resets the statistics. */
+/* Live timing: while enabled, every SpMV launched by a solve, every
+ * stiffness assembly and each FAST_KERNEL_* span above is bracketed by CUDA
+ * events on the context's stream (spans nest).  Enabling resets the
+ * statistics. */
 int fast_gpu_kernel_timing(fast_gpu_ctx *ctx, int32_t enable);
 /* Launches, summed device time and algorithmic bytes per launch (the
- * roofline numerator) of one timed kind since timing was enabled. */
+ * roofline numerator; 0 for the spans 3-6) of one timed kind since timing
+ * was enabled. */
 int fast_gpu_kernel_stats(fast_gpu_ctx *ctx, int32_t which, int64_t *launches, double *total_ms,
                           double *bytes_per_launch);
 

@@ -137,24 +137,84 @@ def test_training_reduces_loss(predictor):
     assert info["last_loss"] < 0.05 * info["first_loss"], info
 
 
+def _solve_variant(system, d, q, seed, **kw):
+    ps, E = decks.plate_variant_params(seed, d.num_elems)
+    system.update_material(E=E)
+    try:
+        return system.nr_solve(ps * q, 16, 1 / 16, tol=1e-8, max_iter=30, precision=gpu.PREC_FP64, lin_tol=1e-12,
+                               **kw)
+    finally:
+        system.update_material(E=d.E)
+
+
+def test_device_features_match_training_samples(system, small_plate, predictor):
+    """The features the predictor builds on the device from its coefficient
+    ring equal the training sample of the same trajectory and step."""
+    d, q = small_plate
+    p, _ = predictor
+    p.configure(use_network=True, galerkin_iters=0)
+    _, _, r = _solve_variant(system, d, q, 3 * 100003 + 0, learned=p)
+    assert r["converged_steps"] == 16
+    xs, _ = p.samples()
+    np.testing.assert_allclose(p.last_input(), xs[14], rtol=1e-3, atol=1e-4)
+
+
 def test_learned_start_beats_secant_on_unseen_variant(system, small_plate, predictor):
-    """What the network gains: on a held-out variant the learned start is
+    """What the network gains: on a held-out variant the network's start is
     accepted over the secant start at most steps, and Newton needs fewer
     iterations than with the secant start alone; both reach the same
     tolerance and the same displacements."""
     d, q = small_plate
     p, _ = predictor
-    ps, E = decks.plate_variant_params(999, d.num_elems)
-    system.update_material(E=E)
-    try:
-        kw = dict(tol=1e-8, max_iter=30, precision=gpu.PREC_FP64, lin_tol=1e-12)
-        h0, _, r0 = system.nr_solve(ps * q, 16, 1 / 16, predictor=gpu.PREDICT_SECANT, **kw)
-        h1, _, r1 = system.nr_solve(ps * q, 16, 1 / 16, learned=p, **kw)
-        h2, _, r2 = system.nr_solve(ps * q, 16, 1 / 16, predictor=gpu.PREDICT_NONE, **kw)
-    finally:
-        system.update_material(E=d.E)
+    p.configure(use_network=True, galerkin_iters=0)
+    h0, _, r0 = _solve_variant(system, d, q, 999, predictor=gpu.PREDICT_SECANT)
+    h1, _, r1 = _solve_variant(system, d, q, 999, learned=p)
+    h2, _, r2 = _solve_variant(system, d, q, 999, predictor=gpu.PREDICT_NONE)
     assert r0["converged_steps"] == r1["converged_steps"] == r2["converged_steps"] == 16
     assert r1["predictions"] == 15
     assert r1["predictions_accepted"] >= 12, r1
     assert r1["iterations"] < r0["iterations"] <= r2["iterations"], (r1, r0, r2)
     assert rel(h1[-1], h2[-1]) < 1e-6 and rel(h0[-1], h2[-1]) < 1e-6
+
+
+def test_galerkin_refined_start(system, small_plate, predictor):
+    """One reduced (POD-Galerkin) Newton correction of the network's start:
+    accepted at every step, fewer Newton iterations than the unrefined
+    network start and than the refined secant start (the network's gain)."""
+    d, q = small_plate
+    p, _ = predictor
+    try:
+        p.configure(use_network=True, galerkin_iters=0)
+        _, _, r_net = _solve_variant(system, d, q, 999, learned=p)
+        p.configure(use_network=False, galerkin_iters=1)
+        _, _, r_sec = _solve_variant(system, d, q, 999, learned=p)
+        p.configure(use_network=True, galerkin_iters=1)
+        h, _, r_both = _solve_variant(system, d, q, 999, learned=p)
+        h_ref, _, r_none = _solve_variant(system, d, q, 999, predictor=gpu.PREDICT_NONE)
+    finally:
+        p.configure(use_network=True, galerkin_iters=0)
+    assert r_both["converged_steps"] == 16 and r_both["predictions_accepted"] == 15, r_both
+    assert r_both["iterations"] < r_net["iterations"], (r_both, r_net)
+    assert r_both["iterations"] <= r_sec["iterations"], (r_both, r_sec)
+    assert r_both["iterations"] < r_none["iterations"]
+    assert rel(h[-1], h_ref[-1]) < 1e-6
+
+
+def test_predictor_spans_are_timed(system, small_plate, predictor):
+    """Live timing covers the predictor's two phases, the internal forces and
+    the linear solves of a Newton run."""
+    d, q = small_plate
+    p, _ = predictor
+    try:
+        p.configure(use_network=True, galerkin_iters=1)
+        system.kernel_timing(True)
+        _, _, r = _solve_variant(system, d, q, 999, learned=p)
+        st = {k: system.kernel_stats(k) for k in (gpu.KERNEL_PREDICT_NET, gpu.KERNEL_PREDICT_GALERKIN,
+                                                  gpu.KERNEL_INTERNAL_FORCE, gpu.KERNEL_LINEAR_SOLVE)}
+    finally:
+        system.kernel_timing(False)
+        p.configure(use_network=True, galerkin_iters=0)
+    assert st[gpu.KERNEL_PREDICT_NET][0] == 15 and st[gpu.KERNEL_PREDICT_GALERKIN][0] == 15
+    assert st[gpu.KERNEL_LINEAR_SOLVE][0] == r["iterations"]
+    assert st[gpu.KERNEL_INTERNAL_FORCE][0] >= r["iterations"] + 15
+    assert all(v[1] > 0 for v in st.values())
