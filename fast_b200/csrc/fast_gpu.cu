@@ -48,6 +48,7 @@ void free_mesh(Ctx &c) {
   dfree(c.d_rowptr); dfree(c.d_col); dfree(c.d_diag); dfree(c.d_srow); dfree(c.d_scol);
   dfree(c.d_K); dfree(c.d_M); dfree(c.d_Ks); dfree(c.d_Ms); dfree(c.d_Ks32);
   dfree(c.d_u); dfree(c.d_r); dfree(c.d_z); dfree(c.d_p); dfree(c.d_w); dfree(c.d_f); dfree(c.d_dinv);
+  dfree(c.d_p2); dfree(c.s_p2);
   dfree(c.d_ubest);
   dfree(c.s_x); dfree(c.s_r); dfree(c.s_z); dfree(c.s_p); dfree(c.s_w); dfree(c.s_dinv);
   dfree(c.d_eq_tmp);
@@ -135,6 +136,13 @@ int fast_gpu_create(int device, fast_gpu_ctx **out) {
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_state, sizeof(PcgState) * 2);
   if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_state, sizeof(PcgState) * 2);
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_partials, sizeof(double) * 16384);
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_bar, Ctx::kBarrierBytes);
+  if (e == cudaSuccess) e = cudaMemset(c->d_bar, 0, Ctx::kBarrierBytes);
+  if (e == cudaSuccess) {
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+    if (!coop) c->persist_max_nodes = 0;
+  }
   if (e != cudaSuccess) {
     delete c;
     return FAST_GPU_ECUDA;
@@ -142,6 +150,18 @@ int fast_gpu_create(int device, fast_gpu_ctx **out) {
   c->stream = c->own_stream;
   *out = c;
   return FAST_GPU_OK;
+}
+
+int fast_gpu_set_option(fast_gpu_ctx *c, int32_t option, int64_t value) {
+  if (!c) return FAST_GPU_EINVAL;
+  if (option == FAST_OPT_PERSISTENT_MAX_NODES) {
+    if (value < 0) return FAST_GPU_EINVAL;
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device);
+    c->persist_max_nodes = coop ? value : 0;
+    return FAST_GPU_OK;
+  }
+  return FAST_GPU_EINVAL;
 }
 
 int fast_gpu_destroy(fast_gpu_ctx *c) {
@@ -154,6 +174,7 @@ int fast_gpu_destroy(fast_gpu_ctx *c) {
   dfree(c->d_state);
   if (c->h_state) cudaFreeHost(c->h_state);
   dfree(c->d_partials);
+  if (c->d_bar) cudaFree(c->d_bar);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
   return FAST_GPU_OK;
@@ -282,6 +303,7 @@ int fast_gpu_upload_mesh(fast_gpu_ctx *c, const fast_gpu_mesh *m) {
   const int64_t n4 = 4 * nnode;
   CK(dalloc(&c->d_K, 9 * c->nnzb));
   CK(dalloc(&c->d_u, n4)); CK(dalloc(&c->d_r, n4)); CK(dalloc(&c->d_z, n4)); CK(dalloc(&c->d_p, n4));
+  CK(dalloc(&c->d_p2, n4)); CK(dalloc(&c->s_p2, n4));
   CK(dalloc(&c->d_w, n4)); CK(dalloc(&c->d_f, n4)); CK(dalloc(&c->d_dinv, 12 * nnode));
   CK(dalloc(&c->d_ubest, n4));
   CK(dalloc(&c->s_x, n4)); CK(dalloc(&c->s_r, n4)); CK(dalloc(&c->s_z, n4)); CK(dalloc(&c->s_p, n4));
@@ -527,6 +549,10 @@ int solve_node_space(fast_gpu_ctx *c, const fast_gpu_solve_opts *o, bool warm, f
     R.true_rel_residual = h[1] > 0 ? std::sqrt(h[0] / h[1]) : 0.0;
   }
   if (rep) *rep = R;
+  if (st.done == kDoneBarrierTimeout) {
+    c->err = "solve: a grid-barrier wait of the persistent PCG kernel timed out";
+    return FAST_GPU_ECUDA;
+  }
   if (st.done == 3) {
     c->err = "solve: breakdown (non-positive or non-finite p.Kp or residual)";
     return FAST_GPU_ENONCONV;

@@ -30,7 +30,8 @@ struct PcgState {
   double err_true;  // |f - K u| / |f| at the last FP64 residual (mixed path)
   double best_err;  // smallest err_true so far (mixed path stagnation guard)
   int32_t iter;   // iterations completed
-  int32_t done;   // 0 running, 1 converged, 2 iteration cap, 3 breakdown, 4 stagnation
+  int32_t done;   // 0 running, 1 converged, 2 iteration cap, 3 breakdown, 4 stagnation,
+                  // 6 grid-barrier timeout (persistent kernel)
   int32_t maxit;
   int32_t updates;  // FP64 residual replacements (mixed path)
   int32_t null_rhs; // |f| < tol: the solution is u = 0 (PCGSolver returns at once)
@@ -104,9 +105,11 @@ struct Ctx {
   double *d_gint = nullptr;       // [nnode][4]
   // solver workspace: node vectors padded to 4 entries (x, y, z, 0) per node
   double *d_u = nullptr, *d_r = nullptr, *d_z = nullptr, *d_p = nullptr, *d_w = nullptr, *d_f = nullptr;
+  double *d_p2 = nullptr;         // second search-direction buffer (persistent PCG)
   double *d_dinv = nullptr;       // [nnode][3][4] inverse diagonal (Jacobi) or inverse 3x3 block
   double *d_ubest = nullptr;      // mixed path: FP64 iterate with the smallest true residual
   float *s_x = nullptr, *s_r = nullptr, *s_z = nullptr, *s_p = nullptr, *s_w = nullptr;
+  float *s_p2 = nullptr;
   float *s_dinv = nullptr;        // [nnode][3][4]
   int precond_built = -1;         // which preconditioner d_dinv holds
   double *d_partials = nullptr;   // reduction partials [2][kRedBlocks]
@@ -116,6 +119,13 @@ struct Ctx {
   double *h_eq_tmp = nullptr;     // pinned [neq]
 
   int64_t launches = 0;          // kernels launched by this context (all entry points)
+
+  // persistent PCG: systems with at most persist_max_nodes nodes run each
+  // chunk of iterations as one cooperative kernel (grid barriers in d_bar)
+  int64_t persist_max_nodes = 65536;
+  int persist_grid = 0;           // blocks of that kernel (0: not yet sized)
+  void *d_bar = nullptr;          // grid barrier words (kBarrierBytes)
+  static constexpr size_t kBarrierBytes = 8192;
 
   // CUDA graphs of one chunk of PCG iterations (captured once, replayed)
   cudaGraphExec_t graph_fp64 = nullptr, graph_mixed = nullptr;
@@ -172,6 +182,7 @@ cudaError_t launch_to_soa(Ctx &c, const double *K, double *Ks, float *Ks32);
 // PCG on the padded node vectors c.d_f -> c.d_u; state left in c.h_state
 cudaError_t pcg_fp64(Ctx &c, bool warm, double tol, int maxit, int chunk, int iter0 = 0);
 cudaError_t pcg_mixed(Ctx &c, bool warm, double tol, int maxit, int chunk);
+constexpr int kDoneBarrierTimeout = 6;  // PcgState::done: a grid-barrier wait ran out
 cudaError_t launch_residual(Ctx &c, const double *Ks, const double *f, const double *u, double *r,
                             double *rr_out_dev);
 cudaError_t launch_spmv(Ctx &c, const double *Ks, const double *x, double *y);

@@ -67,6 +67,15 @@ int dgemm_splits(int M, int N, int K);
 cudaError_t dgemm(cudaStream_t s, int M, int N, int K, const double *A, int lda, bool ta, const double *B, int ldb,
                   bool tb, double *C, int ldc, double *ws);
 
+// C[p][q] (row-major, ldc) = sum_i A[i lda + a] B[i ldb + b] over the n rows
+// of two tall, thin row-major matrices (p q <= kSkinnyMaxOut): one pass over
+// the rows by kSkinnyBlocks blocks, partials (ws >= kSkinnyBlocks p q
+// doubles) summed in a fixed order.  Two launches.
+constexpr int kSkinnyBlocks = 296;
+constexpr int kSkinnyMaxOut = 4096;
+cudaError_t skinny_atb(cudaStream_t s, int64_t n, int p, int q, const double *A, int lda, const double *B, int ldb,
+                       double *C, int ldc, double *ws);
+
 // symmetric eigen-decomposition (cyclic Jacobi) of a small n x n matrix:
 // eigenvalues descending in w, eigenvectors as columns of V (row-major n x n)
 void sym_eig(int n, std::vector<double> a, std::vector<double> &w, std::vector<double> &V);

@@ -87,6 +87,59 @@ __global__ void dgemm_reduce(int M, int N, int splits, const double *__restrict_
 
 }  // namespace
 
+// Per-block partial sums of C[a][b] = sum_i A[i lda + a] B[i ldb + b]: with
+// few outputs the block's threads split the rows into groups (combined in
+// shared memory in a fixed order); with many, each thread owns outputs.
+template <int NT>
+__global__ void __launch_bounds__(NT) skinny_atb_part(int64_t n, int p, int q, const double *__restrict__ A, int lda,
+                                                      const double *__restrict__ B, int ldb,
+                                                      double *__restrict__ part) {
+  __shared__ double red[NT];
+  const int pq = p * q, tid = threadIdx.x;
+  if (pq <= NT) {
+    const int groups = NT / pq;
+    const int o = tid % pq, g = tid / pq;
+    double acc = 0.0;
+    if (g < groups) {
+      const int a = o / q, b = o % q;
+      for (int64_t i = (int64_t)blockIdx.x * groups + g; i < n; i += (int64_t)gridDim.x * groups)
+        acc = fma(A[i * lda + a], B[i * ldb + b], acc);
+    }
+    red[tid] = acc;
+    __syncthreads();
+    if (tid < pq) {
+      double t = 0.0;
+      for (int gg = 0; gg < groups; gg++) t += red[gg * pq + tid];
+      part[(int64_t)blockIdx.x * pq + tid] = t;
+    }
+  } else {
+    for (int o = tid; o < pq; o += NT) {
+      const int a = o / q, b = o % q;
+      double acc = 0.0;
+      for (int64_t i = blockIdx.x; i < n; i += gridDim.x) acc = fma(A[i * lda + a], B[i * ldb + b], acc);
+      part[(int64_t)blockIdx.x * pq + o] = acc;
+    }
+  }
+}
+
+__global__ void skinny_finish(int nblk, int p, int q, const double *__restrict__ part, double *__restrict__ C,
+                              int ldc) {
+  const int pq = p * q;
+  for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < pq; o += gridDim.x * blockDim.x) {
+    double t = 0.0;
+    for (int b = 0; b < nblk; b++) t += part[(int64_t)b * pq + o];
+    C[(int64_t)(o / q) * ldc + o % q] = t;
+  }
+}
+
+cudaError_t skinny_atb(cudaStream_t s, int64_t n, int p, int q, const double *A, int lda, const double *B, int ldb,
+                       double *C, int ldc, double *ws) {
+  if (n <= 0 || p <= 0 || q <= 0 || p * q > kSkinnyMaxOut || !ws) return cudaErrorInvalidValue;
+  skinny_atb_part<256><<<kSkinnyBlocks, 256, 0, s>>>(n, p, q, A, lda, B, ldb, ws);
+  skinny_finish<<<(p * q + 255) / 256, 256, 0, s>>>(kSkinnyBlocks, p, q, ws, C, ldc);
+  return cudaGetLastError();
+}
+
 int dgemm_splits(int M, int N, int K) {
   const int tiles = ((M + kT - 1) / kT) * ((N + kT - 1) / kT);
   if (tiles >= 148) return 1;

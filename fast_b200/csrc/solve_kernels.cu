@@ -660,6 +660,329 @@ cudaError_t launch_build_precond(Ctx &c, const double *K, int precond) {
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------- persistent PCG
+// For small systems the iteration is latency-bound (five kernels of a few
+// microseconds each).  There one cooperative launch runs a whole chunk of
+// iterations: each block owns a contiguous range of block-rows (nodes), and
+// three grid barriers per iteration separate w = K p (with the p.w
+// partials), the vector updates (with the r.r and z.r partials) and the new
+// search direction.  Every block sums the per-block partials itself, in the
+// same fixed order, so the scalars agree in every block without a broadcast
+// and a solve stays bit-reproducible.  Data written by other blocks during
+// the launch (p and the partials) is read through L2 (ld.global.cg).  The
+// scalars and the exit codes are exactly those of pcg_alpha/pcg_update/
+// pcg_beta/pcg_pupdate; block 0 writes them back to the PcgState at the end.
+constexpr int kPersistThreads = 512;
+constexpr uint64_t kBarrierWaitNs = 2000000000ull;  // one barrier wait; then the launch gives up
+
+// Flag barrier: block b > 0 posts the barrier's epoch in its own word and
+// waits for the release word; the threads of block 0 poll all posted words
+// in parallel and then release.  Epochs count the barriers of one launch
+// from 1 (the words are cleared before each launch).  Every wait is bounded:
+// when one runs out the error word is set and every block leaves at its
+// next barrier.
+constexpr int kMaxPersistBlocks = 1024;
+struct GridBarrier {
+  unsigned int release;
+  int32_t err;
+  unsigned int pad[2];
+  unsigned int posted[kMaxPersistBlocks];
+};
+static_assert(sizeof(GridBarrier) <= Ctx::kBarrierBytes, "barrier words exceed their allocation");
+
+__device__ __forceinline__ uint64_t now_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ bool grid_barrier(GridBarrier *b, unsigned int epoch, int *ok_sh) {
+  volatile unsigned int *vrel = &b->release;
+  volatile int32_t *verr = &b->err;
+  __syncthreads();
+  if (blockIdx.x == 0) {
+    int ok = 1;
+    const unsigned int t = threadIdx.x;
+    if (t > 0 && t < gridDim.x) {
+      volatile unsigned int *vp = &b->posted[t];
+      const uint64_t t0 = now_ns();
+      while (*vp != epoch) {
+        if (*verr != 0) { ok = 0; break; }
+        if (now_ns() - t0 > kBarrierWaitNs) { atomicExch(&b->err, 1); ok = 0; break; }
+      }
+    }
+    ok = __syncthreads_and(ok);
+    if (threadIdx.x == 0) {
+      __threadfence();
+      if (ok) *vrel = epoch;
+      *ok_sh = ok && *verr == 0;
+    }
+  } else if (threadIdx.x == 0) {
+    int ok = *verr == 0;
+    __threadfence();
+    b->posted[blockIdx.x] = epoch;
+    const uint64_t t0 = now_ns();
+    while (ok && *vrel != epoch) {
+      if (*verr != 0) { ok = 0; break; }
+      if (now_ns() - t0 > kBarrierWaitNs) { atomicExch(&b->err, 1); ok = 0; break; }
+    }
+    __threadfence();
+    *ok_sh = ok;
+  }
+  __syncthreads();
+  return *ok_sh != 0;
+}
+
+template <typename T> struct V4cg;
+template <> struct V4cg<float> {
+  static __device__ __forceinline__ void load(const float *p, float &a, float &b, float &c) {
+    const float4 v = __ldcg(reinterpret_cast<const float4 *>(p));
+    a = v.x; b = v.y; c = v.z;
+  }
+};
+template <> struct V4cg<double> {
+  static __device__ __forceinline__ void load(const double *p, double &a, double &b, double &c) {
+    const double2 v0 = __ldcg(reinterpret_cast<const double2 *>(p));
+    a = v0.x; b = v0.y; c = __ldcg(p + 2);
+  }
+};
+
+// gather of the search direction: x_j = p_j (first iteration of a launch) or
+// x_j = z_j + beta p_j (the direction of this iteration, built from the last
+// one), read through L2
+template <typename T>
+struct DirGather {
+  const T *p, *z;
+  T beta;
+  bool plain;
+  __device__ __forceinline__ void load(int64_t j, T &a, T &b, T &c) const {
+    V4cg<T>::load(p + 4 * j, a, b, c);
+    if (!plain) {
+      T z0, z1, z2;
+      V4cg<T>::load(z + 4 * j, z0, z1, z2);
+      a = z0 + beta * a;
+      b = z1 + beta * b;
+      c = z2 + beta * c;
+    }
+  }
+};
+
+__device__ __forceinline__ void persist_row_dir(const int32_t *__restrict__ scol, const float *__restrict__ vr,
+                                                int32_t s0, int32_t nbp, int q, const DirGather<float> &x, float &a0,
+                                                float &a1, float &a2) {
+  for (int j = 4 * q; j < nbp; j += 64) {
+    const int4 c = *reinterpret_cast<const int4 *>(scol + s0 + j);
+    float4 v[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) v[k] = *reinterpret_cast<const float4 *>(vr + k * nbp + j);
+    float xa0, xa1, xa2, xb0, xb1, xb2, xc0, xc1, xc2, xd0, xd1, xd2;
+    x.load(c.x, xa0, xa1, xa2);
+    x.load(c.y, xb0, xb1, xb2);
+    x.load(c.z, xc0, xc1, xc2);
+    x.load(c.w, xd0, xd1, xd2);
+    a0 += v[0].x * xa0 + v[1].x * xa1 + v[2].x * xa2 + v[0].y * xb0 + v[1].y * xb1 + v[2].y * xb2 +
+          v[0].z * xc0 + v[1].z * xc1 + v[2].z * xc2 + v[0].w * xd0 + v[1].w * xd1 + v[2].w * xd2;
+    a1 += v[3].x * xa0 + v[4].x * xa1 + v[5].x * xa2 + v[3].y * xb0 + v[4].y * xb1 + v[5].y * xb2 +
+          v[3].z * xc0 + v[4].z * xc1 + v[5].z * xc2 + v[3].w * xd0 + v[4].w * xd1 + v[5].w * xd2;
+    a2 += v[6].x * xa0 + v[7].x * xa1 + v[8].x * xa2 + v[6].y * xb0 + v[7].y * xb1 + v[8].y * xb2 +
+          v[6].z * xc0 + v[7].z * xc1 + v[8].z * xc2 + v[6].w * xd0 + v[7].w * xd1 + v[8].w * xd2;
+  }
+}
+__device__ __forceinline__ void persist_row_dir(const int32_t *__restrict__ scol, const double *__restrict__ vr,
+                                                int32_t s0, int32_t nbp, int q, const DirGather<double> &x,
+                                                double &a0, double &a1, double &a2) {
+  for (int j = 2 * q; j < nbp; j += 32) {
+    const int2 c = *reinterpret_cast<const int2 *>(scol + s0 + j);
+    double2 v[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) v[k] = *reinterpret_cast<const double2 *>(vr + k * nbp + j);
+    double xa0, xa1, xa2, xb0, xb1, xb2;
+    x.load(c.x, xa0, xa1, xa2);
+    x.load(c.y, xb0, xb1, xb2);
+    a0 += v[0].x * xa0 + v[1].x * xa1 + v[2].x * xa2 + v[0].y * xb0 + v[1].y * xb1 + v[2].y * xb2;
+    a1 += v[3].x * xa0 + v[4].x * xa1 + v[5].x * xa2 + v[3].y * xb0 + v[4].y * xb1 + v[5].y * xb2;
+    a2 += v[6].x * xa0 + v[7].x * xa1 + v[8].x * xa2 + v[6].y * xb0 + v[7].y * xb1 + v[8].y * xb2;
+  }
+}
+
+// sum of the G per-block partials at part[0..G), the same in every block
+__device__ __forceinline__ double persist_sum(const double *part, int G, double *sbuf, double *bc) {
+  const double v = threadIdx.x < G ? __ldcg(part + threadIdx.x) : 0.0;
+  const double t = block_sum<kPersistThreads>(v, sbuf);
+  if (threadIdx.x == 0) *bc = t;
+  __syncthreads();
+  const double r = *bc;
+  __syncthreads();
+  return r;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kPersistThreads, 1)
+pcg_persistent(int64_t nnode, const int32_t *__restrict__ srow, const int32_t *__restrict__ scol,
+               const T *__restrict__ val, T *u, T *r, T *z, T *p, T *p2, T *w, const T *__restrict__ dinv,
+               PcgState *st, double *part_pw, double *part_rr, double *part_zr, GridBarrier *bar, int iters) {
+  __shared__ double sbuf[32];
+  __shared__ double bc;
+  __shared__ int ok_sh;
+  if (st->done) return;  // the same value in every block: no block waits alone
+  const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, q = lane & 15;
+  double dot0 = st->dot0, alpha = st->alpha, beta = st->beta, rr = st->rr, err = st->err, pw = st->pw;
+  int iter = st->iter, done = 0;
+  const double tol = st->tol, lenf = st->lenf;
+  const int maxit = st->maxit;
+  const int64_t rb = (nnode + G - 1) / G;
+  const int64_t r0 = min(nnode, (int64_t)b * rb), r1 = min(nnode, r0 + rb);
+  unsigned int epoch = 0;
+  // The direction of iteration k+1 is p = z + beta p_k.  Instead of a third
+  // barrier before the SpMV, each block builds it on the fly from z and the
+  // last direction (both final after the second barrier) for every gathered
+  // node, and stores it for its own nodes in the other buffer.
+  T *pcur = p, *pnxt = p2;
+  bool first = true;
+  int it = 0;
+  for (; it < iters; it++) {
+    const DirGather<T> dir{pcur, z, (T)beta, first};
+    T *pdir = first ? pcur : pnxt;
+    // w = K p on the block's rows, partial p.w, own rows of p stored
+    double pacc = 0.0;
+    for (int64_t row0 = r0 + 2 * (tid >> 5); row0 < r1; row0 += 2 * (kPersistThreads / 32)) {
+      const int64_t row = row0 + (lane >> 4);
+      const bool live = row < r1;
+      int32_t s0 = 0, nbp = 0;
+      if (live) {
+        s0 = srow[row];
+        nbp = srow[row + 1] - s0;
+      }
+      T a0 = 0, a1 = 0, a2 = 0;
+      persist_row_dir(scol, val + 9 * (int64_t)s0, s0, nbp, q, dir, a0, a1, a2);
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+      }
+      if (live && q == 0) {
+        V4<T>::store(w + 4 * row, a0, a1, a2);
+        T x0, x1, x2;
+        dir.load(row, x0, x1, x2);
+        if (!first) V4<T>::store(pdir + 4 * row, x0, x1, x2);
+        pacc += (double)x0 * a0 + (double)x1 * a1 + (double)x2 * a2;
+      }
+    }
+    pcur = pdir;
+    pnxt = (pdir == p) ? p2 : p;
+    first = false;
+    double t = block_sum<kPersistThreads>(pacc, sbuf);
+    if (tid == 0) part_pw[b] = t;
+    if (!grid_barrier(bar, ++epoch, &ok_sh)) { done = kDoneBarrierTimeout; break; }
+    pw = persist_sum(part_pw, G, sbuf, &bc);
+    if (!(pw > 0.0) || !isfinite(pw)) { done = 3; break; }
+    alpha = dot0 / pw;
+    // u += alpha p; r -= alpha w; z = Dinv r; partials r.r, z.r
+    const T al = (T)alpha;
+    double rra = 0.0, zra = 0.0;
+    for (int64_t n = r0 + tid; n < r1; n += kPersistThreads) {
+      T u0, u1, u2, p0, p1, p2_, x0, x1, x2, w0, w1, w2, z0, z1, z2;
+      V4<T>::load(u + 4 * n, u0, u1, u2);
+      V4<T>::load(pcur + 4 * n, p0, p1, p2_);
+      V4<T>::load(r + 4 * n, x0, x1, x2);
+      V4<T>::load(w + 4 * n, w0, w1, w2);
+      u0 = u0 + al * p0; u1 = u1 + al * p1; u2 = u2 + al * p2_;
+      x0 = x0 + (-al) * w0; x1 = x1 + (-al) * w1; x2 = x2 + (-al) * w2;
+      apply_dinv(dinv + 12 * n, x0, x1, x2, z0, z1, z2);
+      V4<T>::store(u + 4 * n, u0, u1, u2);
+      V4<T>::store(r + 4 * n, x0, x1, x2);
+      V4<T>::store(z + 4 * n, z0, z1, z2);
+      rra += (double)x0 * x0 + (double)x1 * x1 + (double)x2 * x2;
+      zra += (double)z0 * x0 + (double)z1 * x1 + (double)z2 * x2;
+    }
+    t = block_sum<kPersistThreads>(rra, sbuf);
+    if (tid == 0) part_rr[b] = t;
+    t = block_sum<kPersistThreads>(zra, sbuf);
+    if (tid == 0) part_zr[b] = t;
+    if (!grid_barrier(bar, ++epoch, &ok_sh)) { done = kDoneBarrierTimeout; break; }
+    rr = persist_sum(part_rr, G, sbuf, &bc);
+    const double zr = persist_sum(part_zr, G, sbuf, &bc);
+    iter += 1;
+    err = sqrt(rr) / lenf;
+    if (err < tol) { done = 1; break; }
+    if (!isfinite(err)) { done = 3; break; }
+    if (iter >= maxit) { done = 2; break; }
+    beta = zr / dot0;
+    dot0 = zr;
+  }
+  // leave the direction the per-kernel iteration expects in p: the next one
+  // (z + beta p) when the chunk ran out, else the last one used
+  if (done != kDoneBarrierTimeout) {
+    const bool next = (done == 0);
+    if (next || pcur != p) {
+      const T be = (T)beta;
+      for (int64_t n = r0 + tid; n < r1; n += kPersistThreads) {
+        T p0, p1, p2_, z0, z1, z2;
+        V4<T>::load(pcur + 4 * n, p0, p1, p2_);
+        if (next) {
+          V4<T>::load(z + 4 * n, z0, z1, z2);
+          p0 = z0 + be * p0; p1 = z1 + be * p1; p2_ = z2 + be * p2_;
+        }
+        V4<T>::store(p + 4 * n, p0, p1, p2_);
+      }
+    }
+  }
+  if (b == 0 && tid == 0) {
+    st->dot0 = dot0;
+    st->alpha = alpha;
+    st->beta = beta;
+    st->rr = rr;
+    st->err = err;
+    st->pw = pw;
+    st->iter = iter;
+    st->done = done;
+  }
+}
+
+// k iterations of the persistent kernel; false when the system is too large
+// for it (the caller then uses the per-kernel iteration)
+template <typename T>
+static cudaError_t launch_persistent(Ctx &c, const T *val, T *u, T *r, T *z, T *p, T *p2, T *w, const T *dinv,
+                                     int k) {
+  cudaError_t e = cudaMemsetAsync(c.d_bar, 0, sizeof(GridBarrier), c.stream);
+  if (e != cudaSuccess) return e;
+  int64_t nn = c.nnode;
+  const int32_t *srow = c.d_srow, *scol = c.d_scol;
+  PcgState *st = c.d_state;
+  double *pa = c.d_partials, *pb = c.d_partials + 2048, *pc = c.d_partials + 4096;
+  GridBarrier *bar = static_cast<GridBarrier *>(c.d_bar);
+  void *args[] = {&nn, &srow, &scol, &val, &u, &r, &z, &p, &p2, &w, &dinv, &st, &pa, &pb, &pc, &bar, &k};
+  e = cudaLaunchCooperativeKernel((const void *)pcg_persistent<T>, dim3(c.persist_grid), dim3(kPersistThreads), args,
+                                  0, c.stream);
+  c.launches++;
+  return e;
+}
+
+// small enough, and one block of the kernel fits on every SM (sized once)
+static bool use_persistent(Ctx &c) {
+  if (c.nnode <= 0 || c.nnode > c.persist_max_nodes) return false;
+  if (c.persist_grid == 0) {
+    int a = 0, b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, pcg_persistent<double>, kPersistThreads, 0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, pcg_persistent<float>, kPersistThreads, 0) != cudaSuccess ||
+        a < 1 || b < 1) {
+      cudaGetLastError();
+      c.persist_max_nodes = 0;
+      return false;
+    }
+    c.persist_grid = 1;  // sized per system below
+  }
+  {
+    // about 64 block-rows per block (two passes of the 512 threads), at most one block per SM
+    int64_t g = (c.nnode + 63) / 64;
+    if (g > c.sm_count) g = c.sm_count;
+    if (g > kMaxPersistBlocks) g = kMaxPersistBlocks;
+    c.persist_grid = (int)(g < 1 ? 1 : g);
+  }
+  return true;
+}
+
 // Pipelined host loop: launch a chunk, then look at the state copied after the
 // previous chunk; returns when done or when maxit iterations were launched.
 // Full chunks run as a CUDA graph captured on first use (the scalars live on
@@ -737,6 +1060,12 @@ cudaError_t pcg_fp64(Ctx &c, bool warm, double tol, int maxit, int chunk, int it
   pcg_init_scalar<<<1, 256, 0, c.stream>>>(st, P_C(c), R, P_D(c), R, warm ? P_E(c) : nullptr, G, tol, maxit, iter0);
   c.launches++;
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (use_persistent(c)) {
+    const int pchunk = chunk < 64 ? 64 : chunk;  // each chunk is one launch: read the state back less often
+    return drive(c, maxit, pchunk, nullptr, nullptr, nullptr, [&](int k) -> cudaError_t {
+      return launch_persistent<double>(c, c.d_Ks, c.d_u, c.d_r, c.d_z, c.d_p, c.d_p2, c.d_w, c.d_dinv, k);
+    });
+  }
   return drive(c, maxit, chunk, &c.graph_fp64, &c.graph_fp64_chunk, &c.graph_fp64_kernels, [&](int k) -> cudaError_t {
     for (int i = 0; i < k; i++) {
       c.begin_span(0);
@@ -778,6 +1107,14 @@ cudaError_t pcg_mixed(Ctx &c, bool warm, double tol, int maxit, int chunk) {
   };
   reliable();
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (use_persistent(c)) {
+    return drive(c, maxit, chunk, nullptr, nullptr, nullptr, [&](int k) -> cudaError_t {
+      cudaError_t el = launch_persistent<float>(c, c.d_Ks32, c.s_x, c.s_r, c.s_z, c.s_p, c.s_p2, c.s_w, c.s_dinv, k);
+      if (el != cudaSuccess) return el;
+      reliable();
+      return cudaGetLastError();
+    });
+  }
   return drive(c, maxit, chunk, &c.graph_mixed, &c.graph_mixed_chunk, &c.graph_mixed_kernels,
                [&](int k) -> cudaError_t {
     for (int i = 0; i < k; i++) {

@@ -251,6 +251,7 @@ struct fast_gpu_ws {
   double *d_L = nullptr;         // [64*64] its Cholesky factor
   int32_t *d_ok = nullptr;
   double *d_g = nullptr, *d_r = nullptr;  // [n]
+  double *d_skinny = nullptr;    // [kSkinnyBlocks][kSkinnyMaxOut] partials of the skinny products
   int64_t n_pred = 0, n_gal = 0;
   double pred_ms = 0.0;
 
@@ -274,6 +275,11 @@ struct fast_gpu_ws {
     if (e != cudaSuccess) return e;
     launches += dgemm_splits(M, N, K) > 1 ? 2 : 1;
     return dgemm(c->stream, M, N, K, A, lda, ta, B, ldb, tb, C, ldc, d_ws);
+  }
+  cudaError_t atb(int64_t rows, int p, int q, const double *A, int lda, const double *B, int ldb, double *C,
+                  int ldc) {
+    launches += 2;
+    return skinny_atb(c->stream, rows, p, q, A, lda, B, ldb, C, ldc, d_skinny);
   }
   // Q = Y V_r Lambda_r^{-1/2} from the eigenpairs of Y^T Y (rank-revealing
   // orthonormalisation of the rows x l matrix Y); returns the rank r
@@ -345,6 +351,7 @@ extern "C" int fast_gpu_ws_create(fast_gpu_ctx *ctx, const fast_gpu_ws_opts *opt
   if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_ok, sizeof(int32_t));
   if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_g, sizeof(double) * (size_t)w->n);
   if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_r, sizeof(double) * (size_t)w->n);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_skinny, sizeof(double) * kSkinnyBlocks * kSkinnyMaxOut);
   for (int i = 0; i < fast_gpu_ws::kRing; i++) w->ring_step[i] = -1;
   if (e != cudaSuccess) {
     ctx->err = std::string("ws_create: ") + cudaGetErrorString(e);
@@ -360,7 +367,7 @@ extern "C" void fast_gpu_ws_destroy(fast_gpu_ws *w) {
   if (w->c) cudaStreamSynchronize(w->c->stream);
   for (double *p : w->traj) cudaFree(p);
   for (double *p : {w->d_phi, w->d_ws, w->d_coef, w->d_delta, w->d_ring, w->d_scales, w->d_phin, w->d_Y, w->d_Er,
-                    w->d_L, w->d_g, w->d_r})
+                    w->d_L, w->d_g, w->d_r, w->d_skinny})
     if (p) cudaFree(p);
   if (w->d_ok) cudaFree(w->d_ok);
   w->net.release();
@@ -651,10 +658,10 @@ extern "C" int fast_gpu_ws_predict(void *user, int32_t step, double lambda, cons
   if (w->use_network) {
     // a_{s-1} = Phi^T u_last, a_{s-2} = Phi^T u_prev into the ring
     const int s1 = (step - 1) % R, s2 = (step - 2) % R;
-    WCK(w->gemm(1, k, n, d_u_last, n, false, w->d_phi, k, false, w->d_ring + s1 * 64, k));
+    WCK(w->atb(n, 1, k, d_u_last, 1, w->d_phi, k, w->d_ring + s1 * 64, k));
     w->ring_step[s1] = step - 1;
     if (step - 2 >= 1) {
-      WCK(w->gemm(1, k, n, d_u_prev, n, false, w->d_phi, k, false, w->d_ring + s2 * 64, k));
+      WCK(w->atb(n, 1, k, d_u_prev, 1, w->d_phi, k, w->d_ring + s2 * 64, k));
       w->ring_step[s2] = step - 2;
     }
     FeatArgs fa{};
@@ -692,10 +699,10 @@ extern "C" int fast_gpu_ws_predict(void *user, int32_t step, double lambda, cons
     ws_block_spmm<<<(unsigned)((tot + 127) / 128), 128, 0, c.stream>>>(c.nnode, k, c.d_rowptr, c.d_col, c.d_K,
                                                                          w->d_phin, w->d_Y);
     w->launches++;
-    WCK(w->gemm(k, k, (int)nrow, w->d_phin, k, true, w->d_Y, k, false, w->d_Er, k));
+    WCK(w->atb(nrow, k, k, w->d_phin, k, w->d_Y, k, w->d_Er, k));
     ws_chol<<<1, 64, 0, c.stream>>>(k, w->d_Er, w->d_L, w->d_ok);
     w->launches++;
-    WCK(w->gemm(1, k, n, d_f, n, false, w->d_phi, k, false, w->d_coef + 64, k));
+    WCK(w->atb(n, 1, k, d_f, 1, w->d_phi, k, w->d_coef + 64, k));
     fast_gpu_ctx *fc = static_cast<fast_gpu_ctx *>(w->c);
     for (int it = 0; it < w->gal_iters; it++) {
       int rc = fast_gpu_set_displacement_device(fc, d_u_pred);
@@ -703,7 +710,7 @@ extern "C" int fast_gpu_ws_predict(void *user, int32_t step, double lambda, cons
       if (rc != FAST_GPU_OK) return rc;
       ws_sub<<<148, 256, 0, c.stream>>>(n, d_f, w->d_g, w->d_r);
       w->launches++;
-      WCK(w->gemm(1, k, n, w->d_r, n, false, w->d_phi, k, false, w->d_coef, k));  // Phi^T r
+      WCK(w->atb(n, 1, k, w->d_r, 1, w->d_phi, k, w->d_coef, k));  // Phi^T r
       ws_reduced_solve<<<1, 32, 0, c.stream>>>(k, w->d_L, w->d_ok, w->d_coef, w->d_coef + 64, w->gal_tol,
                                                 w->d_delta);
       ws_add_phi<<<148, 256, 0, c.stream>>>(n, k, w->d_phi, w->d_delta, d_u_pred);

@@ -48,7 +48,9 @@ EXPORTS = [
     "fast_gpu_ws_build_basis", "fast_gpu_ws_train", "fast_gpu_ws_predict", "fast_gpu_ws_report",
     "fast_gpu_ws_get_basis", "fast_gpu_ws_get_samples", "fast_gpu_mlp_params", "fast_gpu_mlp_forward",
     "fast_gpu_mlp_loss_grad", "fast_gpu_mlp_gemm", "fast_gpu_ws_configure", "fast_gpu_ws_last_input",
+    "fast_gpu_set_option",
 ]
+OPT_PERSISTENT_MAX_NODES = 1
 KERNEL_SPMV_FP64, KERNEL_SPMV_FP32, KERNEL_ASSEMBLE = 0, 1, 2
 KERNEL_PREDICT_NET, KERNEL_PREDICT_GALERKIN, KERNEL_INTERNAL_FORCE, KERNEL_LINEAR_SOLVE = 3, 4, 5, 6
 
@@ -152,6 +154,7 @@ def load_library(path: str = LIB_PATH):
     L.fast_gpu_last_error.restype = ctypes.c_char_p
     L.fast_gpu_set_stream.argtypes = [vp, vp]
     L.fast_gpu_synchronize.argtypes = [vp]
+    L.fast_gpu_set_option.argtypes = [vp, ctypes.c_int32, ctypes.c_int64]
     L.fast_gpu_upload_mesh.argtypes = [vp, ctypes.POINTER(Mesh)]
     L.fast_gpu_pattern_info.argtypes = [vp, _lp, _lp, _ip, _dp]
     L.fast_gpu_update_coords.argtypes = [vp, _dp]
@@ -287,6 +290,9 @@ class GpuSystem:
             self.close()
         except Exception:
             pass
+
+    def set_option(self, option: int, value: int):
+        self._ck(self.L.fast_gpu_set_option(self.ctx, int(option), int(value)), "set_option")
 
     def mlp_gemm(self, A, B, ta=False, tb=False):
         """The tensor-core GEMM alone: C = opA(A) opB(B)^T with opA = A^T when ta

@@ -125,6 +125,12 @@ int         fast_gpu_version(void);
 /* Use a caller's CUDA stream (a cudaStream_t passed as void*); NULL = context's own. */
 int         fast_gpu_set_stream(fast_gpu_ctx *ctx, void *cuda_stream);
 int         fast_gpu_synchronize(fast_gpu_ctx *ctx);
+/* Tuning options (no reference counterpart). */
+#define FAST_OPT_PERSISTENT_MAX_NODES 1  /* PCG on systems with at most this many nodes runs each chunk
+                                            of iterations as one persistent cooperative kernel (grid
+                                            barriers instead of kernel boundaries); default 65536,
+                                            0 = always one kernel per step of the iteration */
+int         fast_gpu_set_option(fast_gpu_ctx *ctx, int32_t option, int64_t value);
 
 /* ---- mesh and pattern ---------------------------------------------------
  * Replaces cControl::Init's CompEqs/CompProf (ctrl/ctrl.cpp:2004-2157) for the

@@ -23,10 +23,17 @@ SOLVABLE = ["cfg_hex8_cantilever", "cfg_hex20_lognormal_4x4x2", "cfg_hex20_logno
 SOLVE_TOL = {"cfg_hex8_cantilever": 1e-10}
 
 
-def system(d):
+def system(d, persistent=True):
+    """Device system for deck d.  Small systems iterate in one persistent
+    cooperative kernel per chunk by default; persistent=False keeps the
+    kernel-per-step iteration (the path large systems take)."""
     s = gpu.GpuSystem(0)
+    if not persistent:
+        s.set_option(gpu.OPT_PERSISTENT_MAX_NODES, 0)
     s.upload(d)
     return s
+
+PATHS = pytest.mark.parametrize("persistent", [True, False], ids=["persistent", "per-kernel"])
 
 
 @pytest.mark.parametrize("name", LINEAR)
@@ -60,20 +67,22 @@ def test_assembly_is_bit_identical_run_to_run():
     assert a.tobytes() == b.tobytes()
 
 
+@PATHS
 @pytest.mark.parametrize("name", SOLVABLE)
 @pytest.mark.parametrize("precision", [gpu.PREC_FP64, gpu.PREC_MIXED])
-def test_displacements_match_reference(name, precision):
+def test_displacements_match_reference(name, precision, persistent):
     d, g = gio.load(name)
-    s = system(d)
+    s = system(d, persistent)
     s.assemble()
     u, rep = s.solve(g["ref_f"], tol=SOLVE_TOL.get(name, 1e-12), precision=precision)
     assert rep["converged"]
     assert gio.rel(u, g["ref_u"]) < TOL_U, rep
 
 
-def test_fp64_iterations_match_oracle_pcg():
+@PATHS
+def test_fp64_iterations_match_oracle_pcg(persistent):
     d, g = gio.load("cfg_hex20_lognormal_8x8x4")
-    s = system(d)
+    s = system(d, persistent)
     s.assemble()
     K = fo.assemble(d)
     f = g["ref_f"]
@@ -85,9 +94,10 @@ def test_fp64_iterations_match_oracle_pcg():
         assert gio.rel(u, u_o) < 1e-6
 
 
-def test_solve_is_bit_identical_run_to_run():
+@PATHS
+def test_solve_is_bit_identical_run_to_run(persistent):
     d = decks.box_hex20_lognormal(8, 8, 4, seed=1)
-    s = system(d)
+    s = system(d, persistent)
     s.assemble()
     f = gpu.face_load_vector(d)
     u1, _ = s.solve(f, tol=1e-10)
@@ -123,10 +133,11 @@ def test_mass_matrices_match_reference():
     assert abs(Ml - R).max() / abs(R).max() < TOL_K
 
 
+@PATHS
 @pytest.mark.parametrize("precond", [gpu.PRECOND_JACOBI, gpu.PRECOND_BLOCK_JACOBI])
-def test_medium_hex20_against_oracle(precond):
+def test_medium_hex20_against_oracle(precond, persistent):
     d = decks.box_hex20_lognormal(16, 16, 8, seed=2)
-    s = system(d)
+    s = system(d, persistent)
     s.assemble()
     K = fo.assemble(d)
     Kl = s.lower_csr()
@@ -150,10 +161,11 @@ def test_nonpositive_jacobian_is_reported():
     assert ei.value.rc == -6
 
 
-def test_mixed_escalates_on_ill_conditioned_system():
+@PATHS
+def test_mixed_escalates_on_ill_conditioned_system(persistent):
     # slender cantilever, cond(K) ~ 1e6: FP32 iterates stall, the solve goes on in FP64
     d, g = gio.load("cfg_hex8_cantilever")
-    s = system(d)
+    s = system(d, persistent)
     s.assemble()
     u, rep = s.solve(g["ref_f"], tol=1e-10, precision=gpu.PREC_MIXED)
     assert rep["converged"] and rep["escalated"] == 1
@@ -174,8 +186,9 @@ def test_mixed_does_not_escalate_on_lognormal_box():
 
 
 def test_live_kernel_timing_counts_launches():
+    # per-kernel iteration: every SpMV launch is timed
     d = decks.box_hex20_lognormal(8, 8, 4, seed=1)
-    s = system(d)
+    s = system(d, persistent=False)
     s.kernel_timing(True)
     s.assemble()
     f = gpu.face_load_vector(d)
@@ -196,3 +209,24 @@ def test_nonconvergence_is_reported():
     with pytest.raises(gpu.FastGpuError) as ei:
         s.solve(f, tol=1e-12, maxit=5)
     assert ei.value.rc == -5
+
+
+def test_persistent_and_per_kernel_iterations_agree():
+    """The persistent cooperative kernel runs the same iteration as the
+    kernel-per-step path: same iteration count (the dot products are summed
+    over different block partitions, so the last bits differ) and the same
+    solution to the tolerance."""
+    d = decks.box_hex20_lognormal(10, 10, 5, seed=9)
+    f = gpu.face_load_vector(d)
+    out = {}
+    for persistent in (True, False):
+        s = system(d, persistent)
+        s.assemble()
+        for prec in (gpu.PREC_FP64, gpu.PREC_MIXED):
+            out[persistent, prec] = s.solve(f, tol=1e-10, precision=prec)
+        s.close()
+    for prec in (gpu.PREC_FP64, gpu.PREC_MIXED):
+        (u1, r1), (u2, r2) = out[True, prec], out[False, prec]
+        assert r1["converged"] and r2["converged"]
+        assert abs(r1["iterations"] - r2["iterations"]) <= 2, (r1, r2)
+        assert gio.rel(u1, u2) < 1e-8
