@@ -25,9 +25,13 @@ enum GemmEpi : int {
 //   opA(m, k) = ta ? A[k * lda + m] : A[m * lda + k]
 //   opB(n, k) = tb ? B[k * ldb + n] : B[n * ldb + k]
 // A wait that does not finish within its limit sets *status = 1.
+// With ws (>= splits * M * N floats, see gemm_splits) a store-epilogue GEMM
+// with few output tiles and a long K is split over K across CTAs and the
+// partial tiles are summed in a fixed order by a second kernel.
 cudaError_t gemm_bf16(cudaStream_t s, int M, int N, int K, const float *A, int lda, bool ta, const float *B,
                       int ldb, bool tb, float *C, int ldc, int epi, const float *bias, const float *aux,
-                      int ldaux, int32_t *status);
+                      int ldaux, int32_t *status, float *ws = nullptr);
+int gemm_splits(int M, int N, int K, int epi);
 
 // Fully connected tanh network: dims[0] -> dims[1] -> ... -> dims[L] with
 // tanh on the hidden layers and a linear output.  Parameters are FP32
@@ -43,6 +47,7 @@ struct Mlp {
   float *d_target = nullptr;      // [cap][dims[L]]
   float *d_part = nullptr;        // loss partial sums
   float *d_loss = nullptr;        // [1]
+  float *d_splitws = nullptr;     // split-K partial tiles of the weight gradients
   int32_t *d_status = nullptr;
   int64_t adam_t = 0;
   int64_t launches = 0;

@@ -16,6 +16,7 @@
 // Every mbarrier wait is bounded (1 s); a wait that runs out sets the status
 // flag, waits once more (bounded) for the work in flight, frees the tensor
 // memory and returns.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -94,9 +95,9 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
 
 template <int BN, bool TA, bool TB, int EPI>
 __global__ void __launch_bounds__(128, 1)
-    umma_gemm_bf16(int M, int N, int K, const float *__restrict__ A, int lda, const float *__restrict__ B, int ldb,
-                   float *__restrict__ C, int ldc, const float *__restrict__ bias, const float *__restrict__ aux,
-                   int ldaux, int32_t *__restrict__ status) {
+    umma_gemm_bf16(int M, int N, int K, int kslice, const float *__restrict__ A, int lda, const float *__restrict__ B,
+                   int ldb, float *__restrict__ C, int ldc, const float *__restrict__ bias,
+                   const float *__restrict__ aux, int ldaux, int32_t *__restrict__ status) {
   constexpr int kNcols = BN < 32 ? 32 : BN;            // tensor-memory columns (power of 2, >= 32)
   constexpr int kAbytes = kBM * kBK * 2;
   constexpr int kBbytes = BN * kBK * 2;
@@ -113,7 +114,10 @@ __global__ void __launch_bounds__(128, 1)
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * BN;
-  const int nkb = (K + kBK - 1) / kBK;
+  // split K: this CTA reduces over [kbeg, kend); with several slices the
+  // epilogue (store only) writes slice z's partial tile to C + z M ldc
+  const int kbeg = blockIdx.z * kslice, kend = min(K, kbeg + kslice);
+  const int nkb = (kend - kbeg + kBK - 1) / kBK;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
@@ -143,7 +147,7 @@ __global__ void __launch_bounds__(128, 1)
       __syncthreads();
       if (!ok_sh) break;
     }
-    const int k0 = kb * kBK;
+    const int k0 = kbeg + kb * kBK;
     // A tile: 128 rows x 8 chunks of 8 K-values
     for (int u = tid; u < kBM * (kBK / 8); u += 128) {
       const int r = u % kBM, ch = u / kBM;
@@ -152,7 +156,7 @@ __global__ void __launch_bounds__(128, 1)
 #pragma unroll
       for (int j = 0; j < 8; j++) {
         const int kk = gk + j;
-        f[j] = (gm < M && kk < K) ? (TA ? A[(int64_t)kk * lda + gm] : A[(int64_t)gm * lda + kk]) : 0.f;
+        f[j] = (gm < M && kk < kend) ? (TA ? A[(int64_t)kk * lda + gm] : A[(int64_t)gm * lda + kk]) : 0.f;
       }
       uint4 p = make_uint4(pack_bf16(f[0], f[1]), pack_bf16(f[2], f[3]), pack_bf16(f[4], f[5]), pack_bf16(f[6], f[7]));
       *reinterpret_cast<uint4 *>(sA + ((r >> 3) * (kBK / 8) + ch) * 128 + (r & 7) * 16) = p;
@@ -165,7 +169,7 @@ __global__ void __launch_bounds__(128, 1)
 #pragma unroll
       for (int j = 0; j < 8; j++) {
         const int kk = gk + j;
-        f[j] = (gn < N && kk < K) ? (TB ? B[(int64_t)kk * ldb + gn] : B[(int64_t)gn * ldb + kk]) : 0.f;
+        f[j] = (gn < N && kk < kend) ? (TB ? B[(int64_t)kk * ldb + gn] : B[(int64_t)gn * ldb + kk]) : 0.f;
       }
       uint4 p = make_uint4(pack_bf16(f[0], f[1]), pack_bf16(f[2], f[3]), pack_bf16(f[4], f[5]), pack_bf16(f[6], f[7]));
       *reinterpret_cast<uint4 *>(sB + ((r >> 3) * (kBK / 8) + ch) * 128 + (r & 7) * 16) = p;
@@ -232,7 +236,7 @@ __global__ void __launch_bounds__(128, 1)
               const float h = aux[(int64_t)row * ldaux + col];
               x *= 1.f - h * h;
             }
-            C[(int64_t)row * ldc + col] = x;
+            C[((int64_t)blockIdx.z * M + row) * ldc + col] = x;
           }
         }
       }
@@ -245,8 +249,8 @@ __global__ void __launch_bounds__(128, 1)
 }
 
 template <int BN, bool TA, bool TB, int EPI>
-cudaError_t launch_gemm(cudaStream_t s, int M, int N, int K, const float *A, int lda, const float *B, int ldb,
-                        float *C, int ldc, const float *bias, const float *aux, int ldaux, int32_t *status) {
+cudaError_t launch_gemm(cudaStream_t s, int M, int N, int K, int splits, const float *A, int lda, const float *B,
+                        int ldb, float *C, int ldc, const float *bias, const float *aux, int ldaux, int32_t *status) {
   constexpr int kStage = kBM * kBK * 2 + BN * kBK * 2;
   constexpr int kSmem = 2 * kStage;
   auto kern = umma_gemm_bf16<BN, TA, TB, EPI>;
@@ -256,32 +260,33 @@ cudaError_t launch_gemm(cudaStream_t s, int M, int N, int K, const float *A, int
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  dim3 grid((M + kBM - 1) / kBM, (N + BN - 1) / BN);
-  kern<<<grid, 128, kSmem, s>>>(M, N, K, A, lda, B, ldb, C, ldc, bias, aux, ldaux, status);
+  const int kslice = (K + splits - 1) / splits;
+  dim3 grid((M + kBM - 1) / kBM, (N + BN - 1) / BN, (K + kslice - 1) / kslice);
+  kern<<<grid, 128, kSmem, s>>>(M, N, K, kslice, A, lda, B, ldb, C, ldc, bias, aux, ldaux, status);
   return cudaGetLastError();
 }
 
 template <int BN, bool TA, bool TB>
-cudaError_t launch_epi(cudaStream_t s, int epi, int M, int N, int K, const float *A, int lda, const float *B,
+cudaError_t launch_epi(cudaStream_t s, int epi, int M, int N, int K, int sp, const float *A, int lda, const float *B,
                        int ldb, float *C, int ldc, const float *bias, const float *aux, int ldaux, int32_t *status) {
   switch (epi) {
-    case kEpiStore: return launch_gemm<BN, TA, TB, kEpiStore>(s, M, N, K, A, lda, B, ldb, C, ldc, bias, aux, ldaux, status);
-    case kEpiBias: return launch_gemm<BN, TA, TB, kEpiBias>(s, M, N, K, A, lda, B, ldb, C, ldc, bias, aux, ldaux, status);
+    case kEpiStore: return launch_gemm<BN, TA, TB, kEpiStore>(s, M, N, K, sp, A, lda, B, ldb, C, ldc, bias, aux, ldaux, status);
+    case kEpiBias: return launch_gemm<BN, TA, TB, kEpiBias>(s, M, N, K, sp, A, lda, B, ldb, C, ldc, bias, aux, ldaux, status);
     case kEpiBiasTanh:
-      return launch_gemm<BN, TA, TB, kEpiBiasTanh>(s, M, N, K, A, lda, B, ldb, C, ldc, bias, aux, ldaux, status);
-    case kEpiDTanh: return launch_gemm<BN, TA, TB, kEpiDTanh>(s, M, N, K, A, lda, B, ldb, C, ldc, bias, aux, ldaux, status);
+      return launch_gemm<BN, TA, TB, kEpiBiasTanh>(s, M, N, K, sp, A, lda, B, ldb, C, ldc, bias, aux, ldaux, status);
+    case kEpiDTanh: return launch_gemm<BN, TA, TB, kEpiDTanh>(s, M, N, K, sp, A, lda, B, ldb, C, ldc, bias, aux, ldaux, status);
   }
   return cudaErrorInvalidValue;
 }
 
 template <int BN>
-cudaError_t launch_bn(cudaStream_t s, int epi, bool ta, bool tb, int M, int N, int K, const float *A, int lda,
+cudaError_t launch_bn(cudaStream_t s, int epi, bool ta, bool tb, int M, int N, int K, int sp, const float *A, int lda,
                       const float *B, int ldb, float *C, int ldc, const float *bias, const float *aux, int ldaux,
                       int32_t *status) {
-  if (!ta && !tb) return launch_epi<BN, false, false>(s, epi, M, N, K, A, lda, B, ldb, C, ldc, bias, aux, ldaux, status);
-  if (!ta && tb) return launch_epi<BN, false, true>(s, epi, M, N, K, A, lda, B, ldb, C, ldc, bias, aux, ldaux, status);
-  if (ta && !tb) return launch_epi<BN, true, false>(s, epi, M, N, K, A, lda, B, ldb, C, ldc, bias, aux, ldaux, status);
-  return launch_epi<BN, true, true>(s, epi, M, N, K, A, lda, B, ldb, C, ldc, bias, aux, ldaux, status);
+  if (!ta && !tb) return launch_epi<BN, false, false>(s, epi, M, N, K, sp, A, lda, B, ldb, C, ldc, bias, aux, ldaux, status);
+  if (!ta && tb) return launch_epi<BN, false, true>(s, epi, M, N, K, sp, A, lda, B, ldb, C, ldc, bias, aux, ldaux, status);
+  if (ta && !tb) return launch_epi<BN, true, false>(s, epi, M, N, K, sp, A, lda, B, ldb, C, ldc, bias, aux, ldaux, status);
+  return launch_epi<BN, true, true>(s, epi, M, N, K, sp, A, lda, B, ldb, C, ldc, bias, aux, ldaux, status);
 }
 
 // ---------------------------------------------------------------- MLP pieces
@@ -339,6 +344,16 @@ __global__ void adam_step(int64_t n, float lr, float b1, float b2, float eps, fl
 
 constexpr int kLossBlocks = 64;
 
+// C[m][n] = sum of the split-K partial tiles in slice order
+__global__ void split_reduce(int M, int N, int splits, const float *__restrict__ ws, float *__restrict__ C, int ldc) {
+  const int64_t mn = (int64_t)M * N;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < mn; i += (int64_t)gridDim.x * blockDim.x) {
+    float t = 0.f;
+    for (int z = 0; z < splits; z++) t += ws[z * mn + i];
+    C[(i / N) * ldc + i % N] = t;
+  }
+}
+
 // splitmix64: seeded, platform-independent initial weights
 uint64_t splitmix(uint64_t &x) {
   uint64_t z = (x += 0x9E3779B97F4A7C15ull);
@@ -349,12 +364,29 @@ uint64_t splitmix(uint64_t &x) {
 
 }  // namespace
 
+int gemm_splits(int M, int N, int K, int epi) {
+  if (epi != kEpiStore) return 1;
+  const int tiles = ((M + kBM - 1) / kBM) * ((N + (N <= 64 ? 64 : 128) - 1) / (N <= 64 ? 64 : 128));
+  if (tiles >= 32 || K < 1024) return 1;
+  int sp = (K + 255) / 256;  // at least four K-blocks per slice
+  const int cap = 128 / tiles;
+  return sp < cap ? sp : (cap < 1 ? 1 : cap);
+}
+
 cudaError_t gemm_bf16(cudaStream_t s, int M, int N, int K, const float *A, int lda, bool ta, const float *B, int ldb,
                       bool tb, float *C, int ldc, int epi, const float *bias, const float *aux, int ldaux,
-                      int32_t *status) {
+                      int32_t *status, float *ws) {
   if (M <= 0 || N <= 0 || K <= 0) return cudaErrorInvalidValue;
-  if (N <= 64) return launch_bn<64>(s, epi, ta, tb, M, N, K, A, lda, B, ldb, C, ldc, bias, aux, ldaux, status);
-  return launch_bn<128>(s, epi, ta, tb, M, N, K, A, lda, B, ldb, C, ldc, bias, aux, ldaux, status);
+  const int sp = ws ? gemm_splits(M, N, K, epi) : 1;
+  float *out = sp > 1 ? ws : C;
+  const int ldo = sp > 1 ? N : ldc;
+  cudaError_t e = N <= 64 ? launch_bn<64>(s, epi, ta, tb, M, N, K, sp, A, lda, B, ldb, out, ldo, bias, aux, ldaux, status)
+                          : launch_bn<128>(s, epi, ta, tb, M, N, K, sp, A, lda, B, ldb, out, ldo, bias, aux, ldaux, status);
+  if (e != cudaSuccess || sp == 1) return e;
+  const int kslice = (K + sp - 1) / sp, z = (K + kslice - 1) / kslice;
+  const int64_t mn = (int64_t)M * N;
+  split_reduce<<<(unsigned)std::min<int64_t>(592, (mn + 255) / 256), 256, 0, s>>>(M, N, z, ws, C, ldc);
+  return cudaGetLastError();
 }
 
 cudaError_t Mlp::init(const std::vector<int> &d, uint64_t seed) {
@@ -389,6 +421,12 @@ cudaError_t Mlp::init(const std::vector<int> &d, uint64_t seed) {
   if (e == cudaSuccess) e = cudaMemset(d_v, 0, sizeof(float) * nparams);
   if (e == cudaSuccess) e = cudaMemset(d_grads, 0, sizeof(float) * nparams);
   if (e == cudaSuccess) e = cudaMalloc((void **)&d_part, sizeof(float) * kLossBlocks);
+  {
+    // split-K partials of the weight gradients: at most 128 tiles of 128 x 128
+    int64_t mx = 0;
+    for (int l = 0; l < L; l++) mx = std::max<int64_t>(mx, (int64_t)dims[l + 1] * dims[l]);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&d_splitws, sizeof(float) * std::max<int64_t>(mx * 128, 128 * 128 * 128));
+  }
   if (e == cudaSuccess) e = cudaMalloc((void **)&d_loss, sizeof(float));
   if (e == cudaSuccess) e = cudaMalloc((void **)&d_status, sizeof(int32_t));
   if (e == cudaSuccess) e = cudaMemset(d_status, 0, sizeof(int32_t));
@@ -420,7 +458,7 @@ void Mlp::release() {
   for (float *p : d_g) if (p) cudaFree(p);
   d_h.clear();
   d_g.clear();
-  for (float **p : {&d_params, &d_grads, &d_m, &d_v, &d_target, &d_part, &d_loss})
+  for (float **p : {&d_params, &d_grads, &d_m, &d_v, &d_target, &d_part, &d_loss, &d_splitws})
     if (*p) { cudaFree(*p); *p = nullptr; }
   if (d_status) { cudaFree(d_status); d_status = nullptr; }
   cap = 0;
@@ -450,10 +488,10 @@ cudaError_t Mlp::backward(cudaStream_t s, int batch) {
     const int fi = dims[l], fo = dims[l + 1];
     // dW_l[o][i] = sum_b g[l+1][b][o] h[l][b][i]
     cudaError_t e = gemm_bf16(s, fo, fi, batch, d_g[l + 1], fo, true, d_h[l], fi, true, d_grads + w_off[l], fi,
-                              kEpiStore, nullptr, nullptr, 0, d_status);
+                              kEpiStore, nullptr, nullptr, 0, d_status, d_splitws);
     if (e != cudaSuccess) return e;
     col_sums<<<(fo + 127) / 128, 128, 0, s>>>(batch, fo, d_g[l + 1], d_grads + b_off[l]);
-    launches += 2;
+    launches += gemm_splits(fo, fi, batch, kEpiStore) > 1 ? 3 : 2;
     if (l > 0) {
       // g[l][b][i] = (sum_o g[l+1][b][o] W_l[o][i]) * (1 - h[l][b][i]^2)
       e = gemm_bf16(s, batch, fi, fo, d_g[l + 1], fo, false, d_params + w_off[l], fi, true, d_g[l], fi, kEpiDTanh,

@@ -838,9 +838,11 @@ extern "C" int fast_gpu_mlp_loss_grad(fast_gpu_ws *w, int32_t batch, const float
 extern "C" int fast_gpu_mlp_gemm(fast_gpu_ctx *c, int32_t M, int32_t N, int32_t K, const float *A, int32_t ta,
                                  const float *B, int32_t tb, float *C) {
   if (!c || M <= 0 || N <= 0 || K <= 0 || !A || !B || !C) return FAST_GPU_EINVAL;
-  float *dA = nullptr, *dB = nullptr, *dC = nullptr;
+  float *dA = nullptr, *dB = nullptr, *dC = nullptr, *dW = nullptr;
   int32_t *dst = nullptr, status = 0;
+  const int sp = gemm_splits(M, N, K, kEpiStore);
   cudaError_t e = cudaMalloc((void **)&dA, sizeof(float) * (size_t)M * K);
+  if (e == cudaSuccess && sp > 1) e = cudaMalloc((void **)&dW, sizeof(float) * (size_t)sp * M * N);
   if (e == cudaSuccess) e = cudaMalloc((void **)&dB, sizeof(float) * (size_t)N * K);
   if (e == cudaSuccess) e = cudaMalloc((void **)&dC, sizeof(float) * (size_t)M * N);
   if (e == cudaSuccess) e = cudaMalloc((void **)&dst, sizeof(int32_t));
@@ -849,12 +851,12 @@ extern "C" int fast_gpu_mlp_gemm(fast_gpu_ctx *c, int32_t M, int32_t N, int32_t 
   if (e == cudaSuccess) e = cudaMemcpyAsync(dB, B, sizeof(float) * (size_t)N * K, cudaMemcpyHostToDevice, c->stream);
   if (e == cudaSuccess)
     e = gemm_bf16(c->stream, M, N, K, dA, ta ? M : K, ta != 0, dB, tb ? N : K, tb != 0, dC, N, kEpiStore, nullptr,
-                  nullptr, 0, dst);
+                  nullptr, 0, dst, dW);
   c->launches++;
   if (e == cudaSuccess) e = cudaMemcpyAsync(C, dC, sizeof(float) * (size_t)M * N, cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(&status, dst, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  for (void *p : {(void *)dA, (void *)dB, (void *)dC, (void *)dst})
+  for (void *p : {(void *)dA, (void *)dB, (void *)dC, (void *)dW, (void *)dst})
     if (p) cudaFree(p);
   if (e != cudaSuccess) { c->err = std::string("mlp_gemm: ") + cudaGetErrorString(e); return FAST_GPU_ECUDA; }
   if (status) { c->err = "mlp_gemm: a tensor-core wait timed out"; return FAST_GPU_ECUDA; }

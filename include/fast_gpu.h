@@ -285,7 +285,8 @@ int fast_gpu_mlp_loss_grad(fast_gpu_ws *ws, int32_t batch, const float *x, const
                            float *grad);
 /* The tensor-core GEMM by itself (host buffers): C[M][N] = sum_k opA(m,k) opB(n,k),
  * opA(m,k) = ta ? A[k*M+m] : A[m*K+k], opB(n,k) = tb ? B[k*N+n] : B[n*K+k];
- * FP32 in and out, BF16 products, FP32 accumulation. */
+ * FP32 in and out, BF16 products, FP32 accumulation (split over K across
+ * CTAs, partials summed in a fixed order, when there are few output tiles). */
 int fast_gpu_mlp_gemm(fast_gpu_ctx *ctx, int32_t M, int32_t N, int32_t K, const float *A, int32_t ta,
                       const float *B, int32_t tb, float *C);
 

@@ -58,7 +58,9 @@ def predictor(system, small_plate):
     p.close()
 
 
-def test_mlp_forward_and_gradients_match_oracle(system, small_plate):
+@pytest.mark.parametrize("batch", [300, 2496])
+def test_mlp_forward_and_gradients_match_oracle(system, small_plate, batch):
+    # batch 2496 (the training batch) takes the split-K weight-gradient GEMMs
     dims = [129, 256, 256, 32]
     p = gpu.LearnedPredictor(system, modes=32, history=4, width=256, hidden=2, seed=11)
     try:
@@ -67,8 +69,8 @@ def test_mlp_forward_and_gradients_match_oracle(system, small_plate):
         rng = np.random.default_rng(4)
         params = (rng.standard_normal(p.params().size) * 0.08).astype(np.float32)
         p.params(set_to=params)
-        x = rng.standard_normal((300, 129)).astype(np.float32)
-        t = rng.standard_normal((300, 32)).astype(np.float32)
+        x = rng.standard_normal((batch, 129)).astype(np.float32)
+        t = rng.standard_normal((batch, 32)).astype(np.float32)
         y = p.forward(x)
         ye = net.forward(params, x, emulate=True)[-1]
         assert rel(y, ye) < 1e-4
