@@ -162,14 +162,36 @@ def test_nonpositive_jacobian_is_reported():
 
 
 @PATHS
-def test_mixed_escalates_on_ill_conditioned_system(persistent):
-    # slender cantilever, cond(K) ~ 1e6: FP32 iterates stall, the solve goes on in FP64
+def test_mixed_solves_ill_conditioned_cantilever(persistent):
+    # slender cantilever, cond(K) ~ 1e6: whether the FP32 iterates stall here
+    # depends on rounding order; either way the answer is the reference's
     d, g = gio.load("cfg_hex8_cantilever")
     s = system(d, persistent)
     s.assemble()
     u, rep = s.solve(g["ref_f"], tol=1e-10, precision=gpu.PREC_MIXED)
-    assert rep["converged"] and rep["escalated"] == 1
+    assert rep["converged"] and rep["true_rel_residual"] < 1e-10
     assert gio.rel(u, g["ref_u"]) < TOL_U
+
+
+@PATHS
+def test_mixed_escalates_when_fp32_diverges(persistent):
+    # 40x2x2 hex8 beam of length 40: FP32 PCG with FP64 residual replacement
+    # diverges (simulated on the CPU: residual 67x the load after 500
+    # iterations), so the solve must go on in FP64 and still converge
+    import scipy.sparse.linalg as sla
+    d = decks.cantilever_hex8(40, 2, 2, L=(40.0, 1.0, 1.0))
+    f = gpu.face_load_vector(d)
+    s = system(d, persistent)
+    s.assemble()
+    u, rep = s.solve(f, tol=1e-10, precision=gpu.PREC_MIXED)
+    assert rep["converged"] and rep["escalated"] == 1, rep
+    # cond(D^-1/2 K D^-1/2) = 4e7: the reference's FP64 PCG itself stops at a
+    # true residual of 6e-9 for tol 1e-10 (recurrence drift), and is 1e-10
+    # from the direct solution
+    assert rep["true_rel_residual"] < 2e-8
+    K = fo.assemble(d).tocsc()
+    u_d = sla.spsolve(K, f)
+    assert gio.rel(u, u_d) < 1e-8
 
 
 def test_mixed_does_not_escalate_on_lognormal_box():
