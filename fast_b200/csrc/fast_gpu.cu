@@ -57,12 +57,19 @@ void free_mesh(Ctx &c) {
   c.h_eq_tmp = nullptr;
   c.K_ok = c.M_ok = c.Ks_ok = c.Ms_ok = false;
   c.precond_built = -1;
+  for (void *p : {(void *)c.d_noff, (void *)c.d_order, (void *)c.d_piters, (void *)c.d_pdone, (void *)c.d_perr})
+    if (p) cudaFree(p);
+  c.d_noff = nullptr; c.d_order = nullptr; c.d_piters = nullptr; c.d_pdone = nullptr; c.d_perr = nullptr;
+  c.nprob = 0;
+  c.h_noff.clear();
   c.nnode = 0;
   c.neq = 0;
   c.nnzb = 0;
 }
 
 int check_ctx(const fast_gpu_ctx *c) { return c ? FAST_GPU_OK : FAST_GPU_EINVAL; }
+
+cudaError_t ensure_soa(Ctx &c, int what, bool fp32);
 
 double *target_of(Ctx &c, int what) {
   if (what == FAST_ASM_STIFFNESS) return c.d_K;
@@ -117,6 +124,10 @@ int64_t value_index(const Ctx &c, int32_t i, int32_t j) {
 }
 
 }  // namespace
+
+namespace fastgpu {
+cudaError_t solve_layout(Ctx &c, int what, bool fp32) { return ensure_soa(c, what, fp32); }
+}  // namespace fastgpu
 
 extern "C" {
 

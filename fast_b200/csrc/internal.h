@@ -120,6 +120,14 @@ struct Ctx {
 
   int64_t launches = 0;          // kernels launched by this context (all entry points)
 
+  // independent problems in one mesh (fast_gpu_set_problems)
+  int32_t nprob = 0;
+  std::vector<int64_t> h_noff;    // [nprob+1] node offsets
+  int64_t *d_noff = nullptr;
+  int32_t *d_order = nullptr;     // problems by size, largest first
+  int32_t *d_piters = nullptr, *d_pdone = nullptr;
+  double *d_perr = nullptr;
+
   // persistent PCG: systems with at most persist_max_nodes nodes run each
   // chunk of iterations as one cooperative kernel (grid barriers in d_bar)
   int64_t persist_max_nodes = 65536;
@@ -183,6 +191,12 @@ cudaError_t launch_to_soa(Ctx &c, const double *K, double *Ks, float *Ks32);
 cudaError_t pcg_fp64(Ctx &c, bool warm, double tol, int maxit, int chunk, int iter0 = 0);
 cudaError_t pcg_mixed(Ctx &c, bool warm, double tol, int maxit, int chunk);
 constexpr int kDoneBarrierTimeout = 6;  // PcgState::done: a grid-barrier wait ran out
+// one CTA per independent problem (node ranges d_noff), FP64 Jacobi/block PCG on c.d_Ks
+// from c.d_f into c.d_u; per problem: iterations, |r|/|f| and done (1 conv, 2 cap, 3 breakdown)
+// padded row-local SoA copies of K (what = FAST_ASM_STIFFNESS, FP32 too when fp32) or M, rebuilt if stale
+cudaError_t solve_layout(Ctx &c, int what, bool fp32);
+cudaError_t launch_pcg_batch(Ctx &c, int nprob, const int32_t *d_order, const int64_t *d_noff, double tol, int maxit,
+                             bool warm, int32_t *d_iters, double *d_errs, int32_t *d_done);
 cudaError_t launch_residual(Ctx &c, const double *Ks, const double *f, const double *u, double *r,
                             double *rr_out_dev);
 cudaError_t launch_spmv(Ctx &c, const double *Ks, const double *x, double *y);

@@ -228,6 +228,52 @@ def cantilever_hex8(nx=20, ny=4, nz=4, L=(10.0, 1.0, 1.0), E=1000.0, nu=0.3, q=(
                 title=f"hex8 cantilever {nx}x{ny}x{nz}")
 
 
+def concat_decks(members) -> tuple:
+    """One deck holding independent decks side by side (disjoint node and
+    element ranges, same element kind and Gauss rule).  Returns (deck,
+    node_offsets [m+1], element_offsets [m+1]); equation numbers of member k
+    are then contiguous, in member order."""
+    d0 = members[0]
+    noff, eoff = [0], [0]
+    for m in members:
+        assert m.kind == d0.kind and tuple(m.ngp) == tuple(d0.ngp)
+        noff.append(noff[-1] + m.num_nodes)
+        eoff.append(eoff[-1] + m.num_elems)
+    coords = np.concatenate([m.coords for m in members])
+    conn = np.concatenate([m.conn + o for m, o in zip(members, noff)]).astype(np.int32)
+    fixed = np.concatenate([m.fixed for m in members])
+    has_face = [m.face_elem is not None for m in members]
+    fe = fc = fq = fl = None
+    if any(has_face):
+        fe = np.concatenate([m.face_elem + o for m, o in zip(members, eoff) if m.face_elem is not None]).astype(np.int32)
+        fc = np.concatenate([m.face_corners + o for m, o in zip(members, noff) if m.face_elem is not None]).astype(np.int32)
+        fq = np.concatenate([m.face_q for m in members if m.face_elem is not None])
+        fl = np.concatenate([m.face_local for m in members if m.face_elem is not None]).astype(np.int32)
+    rho = np.concatenate([m.rho for m in members]) if all(m.rho is not None for m in members) else None
+    d = Deck(d0.kind, coords, conn, np.concatenate([m.E for m in members]), np.concatenate([m.nu for m in members]),
+             d0.ngp, fixed, fe, fc, fq, fl, rho=rho, title=f"{len(members)} independent decks")
+    return d, np.asarray(noff, np.int64), np.asarray(eoff, np.int64)
+
+
+def ensemble_cantilevers(count=1024, nmin=6, nmax=20, seed=0, median=1000.0, sigma=0.5, nu=0.3):
+    """Independent hex8 cantilevers with uneven meshes: member k is n x n x 2n
+    elements (n uniform in [nmin, nmax]) on a 2 x 1 x 1 bar (2n along x),
+    2x2x2 Gauss points, x=0 clamped, its own lognormal Young's modulus per
+    element (median, sigma) and a random uniform traction (standard normal
+    components) on the x=2 face.  Returns (deck, node_offsets, sizes n)."""
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(nmin, nmax + 1, size=count)
+    members = []
+    for k, n in enumerate(ns):
+        m = cantilever_hex8(2 * int(n), int(n), int(n), L=(2.0, 1.0, 1.0), nu=nu,
+                            q=tuple(rng.standard_normal(3)))
+        m.E = median * np.exp(sigma * rng.standard_normal(m.num_elems))
+        members.append(m)
+    d, noff, _ = concat_decks(members)
+    d.title = f"{count} hex8 cantilevers n x n x 2n, n in [{nmin}, {nmax}], seed {seed}"
+    return d, noff, ns
+
+
 def box_hex20_lognormal(nx=64, ny=64, nz=32, L=(4.0, 4.0, 2.0), median=1000.0, sigma=0.5, seed=0,
                         nu=0.3, ngp=3, pressure=1.0) -> Deck:
     """hex20 box with a lognormal Young's modulus per element.

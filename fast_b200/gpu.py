@@ -48,7 +48,7 @@ EXPORTS = [
     "fast_gpu_ws_build_basis", "fast_gpu_ws_train", "fast_gpu_ws_predict", "fast_gpu_ws_report",
     "fast_gpu_ws_get_basis", "fast_gpu_ws_get_samples", "fast_gpu_mlp_params", "fast_gpu_mlp_forward",
     "fast_gpu_mlp_loss_grad", "fast_gpu_mlp_gemm", "fast_gpu_ws_configure", "fast_gpu_ws_last_input",
-    "fast_gpu_set_option",
+    "fast_gpu_set_option", "fast_gpu_set_problems", "fast_gpu_solve_batch",
 ]
 OPT_PERSISTENT_MAX_NODES = 1
 KERNEL_SPMV_FP64, KERNEL_SPMV_FP32, KERNEL_ASSEMBLE = 0, 1, 2
@@ -114,6 +114,10 @@ NR_PREDICTOR = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int32, c
 PREDICT_NONE, PREDICT_SECANT, PREDICT_CALLBACK = 0, 1, 2
 
 
+class ProblemReport(ctypes.Structure):
+    _fields_ = [("converged", ctypes.c_int32), ("iterations", ctypes.c_int32), ("rel_residual", ctypes.c_double)]
+
+
 class WsOpts(ctypes.Structure):
     _fields_ = [("modes", ctypes.c_int32), ("history", ctypes.c_int32), ("width", ctypes.c_int32),
                 ("hidden", ctypes.c_int32), ("oversample", ctypes.c_int32), ("power_iters", ctypes.c_int32),
@@ -155,6 +159,8 @@ def load_library(path: str = LIB_PATH):
     L.fast_gpu_set_stream.argtypes = [vp, vp]
     L.fast_gpu_synchronize.argtypes = [vp]
     L.fast_gpu_set_option.argtypes = [vp, ctypes.c_int32, ctypes.c_int64]
+    L.fast_gpu_set_problems.argtypes = [vp, ctypes.c_int32, _lp]
+    L.fast_gpu_solve_batch.argtypes = [vp, _dp, _dp, ctypes.POINTER(SolveOpts), ctypes.POINTER(ProblemReport)]
     L.fast_gpu_upload_mesh.argtypes = [vp, ctypes.POINTER(Mesh)]
     L.fast_gpu_pattern_info.argtypes = [vp, _lp, _lp, _ip, _dp]
     L.fast_gpu_update_coords.argtypes = [vp, _dp]
@@ -290,6 +296,27 @@ class GpuSystem:
             self.close()
         except Exception:
             pass
+
+    def set_problems(self, node_offsets):
+        """Mark the uploaded mesh as independent problems over node ranges."""
+        off = np.ascontiguousarray(node_offsets, dtype=np.int64)
+        self._ck(self.L.fast_gpu_set_problems(self.ctx, len(off) - 1, _p(off, _lp)), "set_problems")
+        self.nprob = len(off) - 1
+
+    def solve_batch(self, f, tol=1e-8, precond=PRECOND_JACOBI, maxit=0, u0=None, raise_on_nonconv=True):
+        """Solve every problem to its own stopping test in one launch;
+        returns u and per-problem (converged, iterations, rel_residual) arrays."""
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        u = np.zeros(self.neq) if u0 is None else np.array(u0, dtype=np.float64)
+        o = SolveOpts(PREC_FP64, precond, int(maxit), int(u0 is not None), float(tol), 0.0, 0, 0)
+        reps = (ProblemReport * self.nprob)()
+        rc = self.L.fast_gpu_solve_batch(self.ctx, _p(f), _p(u), ctypes.byref(o), reps)
+        if rc != FAST_GPU_OK and (raise_on_nonconv or rc != -5):
+            self._ck(rc, "solve_batch")
+        conv = np.array([r.converged for r in reps], bool)
+        its = np.array([r.iterations for r in reps], np.int32)
+        res = np.array([r.rel_residual for r in reps])
+        return u, conv, its, res
 
     def set_option(self, option: int, value: int):
         self._ck(self.L.fast_gpu_set_option(self.ctx, int(option), int(value)), "set_option")

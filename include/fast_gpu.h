@@ -290,6 +290,26 @@ int fast_gpu_mlp_loss_grad(fast_gpu_ws *ws, int32_t batch, const float *x, const
 int fast_gpu_mlp_gemm(fast_gpu_ctx *ctx, int32_t M, int32_t N, int32_t K, const float *A, int32_t ta,
                       const float *B, int32_t tb, float *C);
 
+/* ---- many independent problems -----------------------------------------
+ * Each problem is what one FAST run of cLinStat (ctrl/ctrllins.cpp:46-99)
+ * solves; their meshes are uploaded together as one mesh whose problem k owns
+ * the nodes [node_offsets[k], node_offsets[k+1]) (no element may couple two
+ * problems: checked).  Assembly then covers all problems in one pass, and
+ * fast_gpu_solve_batch solves every problem to its own PCGSolver stopping test
+ * (mlib/sysmat.cpp:1061-1125: |r_k|/|f_k| < tol, |f_k| > 1e11 replaced by 1,
+ * u_k = 0 when |f_k| < tol) in one launch, one CTA per problem. */
+typedef struct {
+  int32_t converged;
+  int32_t iterations;
+  double  rel_residual;   /* recurrence |r_k|/|f_k| at exit */
+} fast_gpu_problem_report;
+
+int fast_gpu_set_problems(fast_gpu_ctx *ctx, int32_t num_problems, const int64_t *node_offsets);
+/* f, u host [num_eq]; FP64 only; reps [num_problems] may be NULL.  Returns
+ * FAST_GPU_ENONCONV when any problem did not converge. */
+int fast_gpu_solve_batch(fast_gpu_ctx *ctx, const double *f, double *u, const fast_gpu_solve_opts *opts,
+                         fast_gpu_problem_report *reps);
+
 /* ---- cSysMatrix replacement (mlib/sysmat.h:60-99) ------------------------ */
 /* cSysMatrix::Zero */
 int fast_gpu_zero(fast_gpu_ctx *ctx, int32_t what);

@@ -252,3 +252,41 @@ def test_persistent_and_per_kernel_iterations_agree():
         assert r1["converged"] and r2["converged"]
         assert abs(r1["iterations"] - r2["iterations"]) <= 2, (r1, r2)
         assert gio.rel(u1, u2) < 1e-8
+
+
+def test_batch_of_independent_problems_matches_single_solves():
+    """Independent cantilevers uploaded as one mesh and solved in one launch
+    (one CTA per problem): every problem reaches its own stopping test and
+    agrees with that problem solved alone and with the oracle's PCG."""
+    d, noff, ns = decks.ensemble_cantilevers(count=12, nmin=2, nmax=5, seed=4)
+    s = system(d)
+    s.assemble()
+    s.set_problems(noff)
+    f = gpu.face_load_vector(d)
+    u, conv, its, res = s.solve_batch(f, tol=1e-10)
+    assert conv.all() and (res < 1e-10).all()
+    eq = d.node_eq()
+    Kall = fo.assemble(d).tocsr()
+    for k in range(len(ns)):
+        n0, n1 = noff[k], noff[k + 1]
+        e = eq[n0:n1].ravel()
+        e = e[e > 0] - 1
+        # the member's own block of K, solved alone by the oracle's PCGSolver
+        K = Kall[e][:, e]
+        u_o, ok, it_o, _ = fo.pcg(K, f[e], 1e-10, 100000)
+        assert ok
+        assert abs(int(its[k]) - it_o) <= 2, (k, its[k], it_o)
+        assert gio.rel(u[e], u_o) < 1e-8
+    # bit-reproducible
+    u2, _, its2, _ = s.solve_batch(f, tol=1e-10)
+    assert u2.tobytes() == u.tobytes() and (its2 == its).all()
+
+
+def test_batch_rejects_coupled_problems():
+    d, noff, ns = decks.ensemble_cantilevers(count=3, nmin=2, nmax=3, seed=1)
+    s = system(d)
+    bad = noff.copy()
+    bad[1] += 1    # a node of problem 1 claimed by problem 0: problem 0 now couples into problem 1
+    with pytest.raises(gpu.FastGpuError) as ei:
+        s.set_problems(bad)
+    assert ei.value.rc == -1
