@@ -293,6 +293,13 @@ cudaError_t launch_zero_matrix(Ctx &c, double *K, bool identity_on_fixed) {
   return cudaGetLastError();
 }
 
+cudaError_t launch_fixed_identity(Ctx &c, double *K) {
+  const int bs = 256;
+  zero_fixed_identity<<<(unsigned)((c.nnode + bs - 1) / bs), bs, 0, c.stream>>>(c.nnode, c.d_fix, c.d_diag, K);
+  c.launches++;
+  return cudaGetLastError();
+}
+
 cudaError_t launch_assemble(Ctx &c, int what, double *target) {
   for (size_t b = 0; b < c.buckets.size(); b++) {
     const Bucket &B = c.buckets[b];

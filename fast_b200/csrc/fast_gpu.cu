@@ -127,6 +127,7 @@ int64_t value_index(const Ctx &c, int32_t i, int32_t j) {
 
 namespace fastgpu {
 cudaError_t solve_layout(Ctx &c, int what, bool fp32) { return ensure_soa(c, what, fp32); }
+void matrix_changed(Ctx &c, int what) { invalidate(c, what); }
 }  // namespace fastgpu
 
 extern "C" {
@@ -580,6 +581,14 @@ int solve_node_space(fast_gpu_ctx *c, const fast_gpu_solve_opts *o, bool warm, f
 }
 
 }  // namespace
+
+extern "C++" {
+namespace fastgpu {
+int solve_nodes(Ctx &c, const fast_gpu_solve_opts *o, bool warm, fast_gpu_solve_report *rep) {
+  return solve_node_space(static_cast<fast_gpu_ctx *>(&c), o, warm, rep);
+}
+}  // namespace fastgpu
+}
 
 int fast_gpu_solve_device(fast_gpu_ctx *c, const double *d_f, double *d_u, const fast_gpu_solve_opts *o,
                           fast_gpu_solve_report *rep) {

@@ -175,6 +175,8 @@ int nodes_of(int type);
 
 // kernels (elem_kernels.cu / solve_kernels.cu); all launched on c.stream
 cudaError_t launch_zero_matrix(Ctx &c, double *K, bool identity_on_fixed);
+// 1 on the diagonal of every fixed DOF (the stiffness slot's convention)
+cudaError_t launch_fixed_identity(Ctx &c, double *K);
 cudaError_t launch_assemble(Ctx &c, int what, double *target);
 cudaError_t launch_element_matrices(Ctx &c, int what, int bucket, int64_t first_sorted, int64_t count,
                                     double *d_out);
@@ -195,6 +197,11 @@ constexpr int kDoneBarrierTimeout = 6;  // PcgState::done: a grid-barrier wait r
 // from c.d_f into c.d_u; per problem: iterations, |r|/|f| and done (1 conv, 2 cap, 3 breakdown)
 // padded row-local SoA copies of K (what = FAST_ASM_STIFFNESS, FP32 too when fp32) or M, rebuilt if stale
 cudaError_t solve_layout(Ctx &c, int what, bool fp32);
+// the values of K (FAST_ASM_STIFFNESS) or M changed: drop their solve copies and preconditioner
+void matrix_changed(Ctx &c, int what);
+// solve K u = f on the node-padded vectors c.d_f -> c.d_u (c.d_u is the first iterate when warm);
+// returns a FAST_GPU_* status
+int solve_nodes(Ctx &c, const fast_gpu_solve_opts *o, bool warm, fast_gpu_solve_report *rep);
 cudaError_t launch_pcg_batch(Ctx &c, int nprob, const int32_t *d_order, const int64_t *d_noff, double tol, int maxit,
                              bool warm, int32_t *d_iters, double *d_errs, int32_t *d_done);
 cudaError_t launch_residual(Ctx &c, const double *Ks, const double *f, const double *u, double *r,

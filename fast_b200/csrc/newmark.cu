@@ -1,0 +1,228 @@
+// newmark.cu - linear Newmark time integration on the device
+// (fast_gpu_newmark), the loop of cCtrlNewmark::Solver
+// (ctrl/ctrlnewmark.cpp:79-254) without damping:
+//
+//   a0 = 1/(beta dt^2), a2 = 1/(beta dt), a3 = 1/(2 beta) - 1,
+//   a6 = (1 - gamma) dt, a7 = gamma dt
+//   f = ExtLoadVector (a step load: the same f at every time), M a = f
+//   K_eff = K + a0 M
+//   each step: f_eff = f + M (a0 u + a2 v + a3 a);  K_eff u_new = f_eff
+//              du = u_new - u;  a <- -a3 a + a0 du - a2 v;  v <- v + a6 a_old + a7 a
+//
+// The reference factors K_eff once (skyline Crout); here every step is a PCG
+// solve warm-started from the last displacements, with K_eff, M and the
+// state vectors resident in HBM and the step's vector work in two fused
+// kernels.  The printout's max norms (umax, vmax, amax) are kept on the
+// device.
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+using namespace fastgpu;
+
+struct fast_gpu_ctx : public Ctx {};
+
+namespace {
+
+constexpr int kNmBlocks = 592;
+
+// K <- K + s M on the AoS block values
+__global__ void nm_axpy(int64_t n, double s, const double *__restrict__ M, double *__restrict__ K) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    K[i] += s * M[i];
+}
+
+// w = a0 u + a2 v + a3 a
+__global__ void nm_inertia(int64_t n, double a0, double a2, double a3, const double *__restrict__ u,
+                           const double *__restrict__ v, const double *__restrict__ a, double *__restrict__ w) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    w[i] = a0 * u[i] + a2 * v[i] + a3 * a[i];
+}
+
+// f_eff = q + z; the solver's first iterate = u
+__global__ void nm_rhs(int64_t n, const double *__restrict__ q, const double *__restrict__ z,
+                       const double *__restrict__ u, double *__restrict__ f, double *__restrict__ x) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    f[i] = q[i] + z[i];
+    x[i] = u[i];
+  }
+}
+
+// ordered bits of a non-negative double (max over them is the max of the values)
+__device__ __forceinline__ unsigned long long dbits(double x) { return (unsigned long long)__double_as_longlong(x); }
+
+// du = x - u; a_new = -a3 a + a0 du - a2 v; v += a6 a_old + a7 a_new; u = x; running inf-norms
+__global__ void nm_update(int64_t n, double a0, double a2, double a3, double a6, double a7, const double *__restrict__ x,
+                          double *__restrict__ u, double *__restrict__ v, double *__restrict__ a,
+                          unsigned long long *__restrict__ maxes) {
+  double mu = 0.0, mv = 0.0, ma = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double un = x[i], du = un - u[i], ao = a[i], vo = v[i];
+    double an = -a3 * ao;
+    an += a0 * du;
+    an += -a2 * vo;
+    double vn = vo + a6 * ao;
+    vn += a7 * an;
+    u[i] = un;
+    v[i] = vn;
+    a[i] = an;
+    mu = fmax(mu, fabs(un));
+    mv = fmax(mv, fabs(vn));
+    ma = fmax(ma, fabs(an));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mu = fmax(mu, __shfl_xor_sync(0xffffffffu, mu, o));
+    mv = fmax(mv, __shfl_xor_sync(0xffffffffu, mv, o));
+    ma = fmax(ma, __shfl_xor_sync(0xffffffffu, ma, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(maxes + 0, dbits(mu));
+    atomicMax(maxes + 1, dbits(mv));
+    atomicMax(maxes + 2, dbits(ma));
+  }
+}
+
+__global__ void nm_amax0(int64_t n, const double *__restrict__ a, unsigned long long *__restrict__ maxes) {
+  double ma = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    ma = fmax(ma, fabs(a[i]));
+  for (int o = 16; o > 0; o >>= 1) ma = fmax(ma, __shfl_xor_sync(0xffffffffu, ma, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(maxes + 2, dbits(ma));
+}
+
+// probe_hist[step][k] = u at equation probe[k] (node-padded index dof[probe[k]])
+__global__ void nm_probe(int nprobe, const int32_t *__restrict__ probe, const int32_t *__restrict__ dof,
+                         const double *__restrict__ u, double *__restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < nprobe) out[k] = u[dof[probe[k]]];
+}
+
+}  // namespace
+
+#define NMCK(call)                                                            \
+  do {                                                                        \
+    cudaError_t _e = (call);                                                  \
+    if (_e != cudaSuccess) {                                                  \
+      c->err = std::string("newmark: ") + #call + ": " + cudaGetErrorString(_e); \
+      rc = FAST_GPU_ECUDA;                                                    \
+      goto done;                                                              \
+    }                                                                         \
+  } while (0)
+
+extern "C" int fast_gpu_newmark(fast_gpu_ctx *c, const double *q, const fast_gpu_newmark_opts *o, double *u_out,
+                                double *v_out, double *a_out, int32_t nprobe, const int32_t *probe_eq,
+                                double *probe_hist, fast_gpu_newmark_report *rep) {
+  if (!c || !q || !o || o->steps <= 0 || !(o->dt > 0) || !(o->beta > 0) || nprobe < 0 ||
+      (nprobe > 0 && (!probe_eq || !probe_hist)))
+    return FAST_GPU_EINVAL;
+  if (!c->d_K) { c->err = "newmark: no mesh"; return FAST_GPU_ESTATE; }
+  for (int k = 0; k < nprobe; k++)
+    if (probe_eq[k] < 0 || probe_eq[k] >= c->neq) { c->err = "newmark: probe equation out of range"; return FAST_GPU_EINVAL; }
+  const int64_t n4 = 4 * c->nnode;
+  const double dt = o->dt, gamma = o->gamma, beta = o->beta;
+  const double a0 = 1.0 / (beta * dt * dt), a2 = 1.0 / (beta * dt), a3 = 0.5 / beta - 1.0;
+  const double a6 = (1.0 - gamma) * dt, a7 = gamma * dt;
+  int rc = FAST_GPU_OK;
+  fast_gpu_newmark_report R{};
+  double *d_q = nullptr, *d_u = nullptr, *d_v = nullptr, *d_a = nullptr, *d_w = nullptr, *d_z = nullptr,
+         *d_hist = nullptr;
+  int32_t *d_probe = nullptr;
+  unsigned long long *d_max = nullptr;
+  unsigned long long h_max[3] = {0, 0, 0};
+  fast_gpu_solve_report lr{};
+  std::vector<double> tmp;
+  {
+    cudaError_t e = cudaSuccess;
+    for (double **b : {&d_q, &d_u, &d_v, &d_a, &d_w, &d_z})
+      if (e == cudaSuccess) e = cudaMalloc((void **)b, sizeof(double) * n4);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&d_max, sizeof(unsigned long long) * 3);
+    if (e == cudaSuccess && nprobe > 0) e = cudaMalloc((void **)&d_probe, sizeof(int32_t) * nprobe);
+    if (e == cudaSuccess && nprobe > 0) e = cudaMalloc((void **)&d_hist, sizeof(double) * (size_t)nprobe * o->steps);
+    NMCK(e);
+  }
+  for (double *b : {d_u, d_v, d_a}) NMCK(cudaMemsetAsync(b, 0, sizeof(double) * n4, c->stream));
+  NMCK(cudaMemsetAsync(d_max, 0, sizeof(unsigned long long) * 3, c->stream));
+  if (nprobe > 0)
+    NMCK(cudaMemcpyAsync(d_probe, probe_eq, sizeof(int32_t) * nprobe, cudaMemcpyHostToDevice, c->stream));
+  // the load, node-padded
+  NMCK(cudaMemcpyAsync(c->d_eq_tmp, q, sizeof(double) * c->neq, cudaMemcpyHostToDevice, c->stream));
+  NMCK(launch_eq_to_node(*c, c->d_eq_tmp, d_q));
+
+  // M, then a(0) from M a = f (the solver works on the K slot: M is copied there)
+  rc = fast_gpu_assemble(c, FAST_ASM_MASS);
+  if (rc != FAST_GPU_OK) goto done;
+  NMCK(cudaMemcpyAsync(c->d_K, c->d_M, sizeof(double) * 9 * c->nnzb, cudaMemcpyDeviceToDevice, c->stream));
+  NMCK(launch_fixed_identity(*c, c->d_K));  // fixed DOFs: identity rows, as in the stiffness slot
+  c->K_ok = true;
+  matrix_changed(*c, FAST_ASM_STIFFNESS);
+  NMCK(cudaMemcpyAsync(c->d_f, d_q, sizeof(double) * n4, cudaMemcpyDeviceToDevice, c->stream));
+  rc = solve_nodes(*c, &o->mass, false, &lr);
+  R.mass_iterations = lr.iterations;
+  if (rc != FAST_GPU_OK) goto done;
+  NMCK(cudaMemcpyAsync(d_a, c->d_u, sizeof(double) * n4, cudaMemcpyDeviceToDevice, c->stream));
+  nm_amax0<<<kNmBlocks, 256, 0, c->stream>>>(n4, d_a, d_max);
+  c->launches++;
+
+  // K_eff = K + a0 M
+  rc = fast_gpu_assemble(c, FAST_ASM_STIFFNESS);
+  if (rc != FAST_GPU_OK) goto done;
+  nm_axpy<<<kNmBlocks, 256, 0, c->stream>>>(9 * c->nnzb, a0, c->d_M, c->d_K);
+  c->launches++;
+  matrix_changed(*c, FAST_ASM_STIFFNESS);
+  NMCK(solve_layout(*c, FAST_ASM_MASS, false));
+
+  for (int s = 0; s < o->steps; s++) {
+    nm_inertia<<<kNmBlocks, 256, 0, c->stream>>>(n4, a0, a2, a3, d_u, d_v, d_a, d_w);
+    c->launches++;
+    NMCK(launch_spmv(*c, c->d_Ms, d_w, d_z));  // z = M w
+    nm_rhs<<<kNmBlocks, 256, 0, c->stream>>>(n4, d_q, d_z, d_u, c->d_f, c->d_u);
+    c->launches++;
+    rc = solve_nodes(*c, &o->lin, o->lin.warm_start != 0, &lr);
+    R.linear_iterations += lr.iterations;
+    if (lr.iterations > R.max_step_iterations) R.max_step_iterations = lr.iterations;
+    if (lr.escalated) R.escalated_steps++;
+    if (rc != FAST_GPU_OK) { R.failed_step = s + 1; goto done; }
+    nm_update<<<kNmBlocks, 256, 0, c->stream>>>(n4, a0, a2, a3, a6, a7, c->d_u, d_u, d_v, d_a, d_max);
+    c->launches++;
+    if (nprobe > 0) {
+      nm_probe<<<(nprobe + 127) / 128, 128, 0, c->stream>>>(nprobe, d_probe, c->d_dof_of_eq, d_u,
+                                                             d_hist + (size_t)s * nprobe);
+      c->launches++;
+    }
+    R.steps_done = s + 1;
+  }
+  NMCK(cudaGetLastError());
+  tmp.resize(c->neq);
+  for (int k = 0; k < 3; k++) {
+    double *src = k == 0 ? d_u : (k == 1 ? d_v : d_a);
+    double *dst = k == 0 ? u_out : (k == 1 ? v_out : a_out);
+    if (!dst) continue;
+    NMCK(launch_node_to_eq(*c, src, c->d_eq_tmp));
+    NMCK(cudaMemcpyAsync(dst, c->d_eq_tmp, sizeof(double) * c->neq, cudaMemcpyDeviceToHost, c->stream));
+    NMCK(cudaStreamSynchronize(c->stream));
+  }
+  if (nprobe > 0)
+    NMCK(cudaMemcpyAsync(probe_hist, d_hist, sizeof(double) * (size_t)nprobe * o->steps, cudaMemcpyDeviceToHost,
+                         c->stream));
+  NMCK(cudaMemcpyAsync(h_max, d_max, sizeof(h_max), cudaMemcpyDeviceToHost, c->stream));
+  NMCK(cudaStreamSynchronize(c->stream));
+  {
+    double m[3];
+    std::memcpy(m, h_max, sizeof(m));
+    R.umax = m[0];
+    R.vmax = m[1];
+    R.amax = m[2];
+  }
+done:
+  if (rep) *rep = R;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (double *b : {d_q, d_u, d_v, d_a, d_w, d_z, d_hist})
+    if (b) cudaFree(b);
+  if (d_probe) cudaFree(d_probe);
+  if (d_max) cudaFree(d_max);
+  // the K slot now holds K_eff (or M): the next stiffness assembly rebuilds K
+  return rc;
+}

@@ -77,6 +77,9 @@ class Deck:
     maxit: int = 0
     maxstep: int = 1
     step_factor: float = 1.0
+    time_step: float = 0.0                    # Newmark: %HEADER.ANALYSIS.TIME.STEP
+    newmark: tuple = (0.5, 0.25)              # Newmark: (gamma, beta), cCtrlNewmark defaults
+    print_step: int = 1                       # %HEADER.ANALYSIS.PRINT.STEPS
     node_labels: Optional[np.ndarray] = None  # [nnode] labels used in a .dat
     title: str = "deck"
 
@@ -330,18 +333,18 @@ def plate_variant_params(seed: int, num_elems: int, E: float = 1000.0, p_range=(
     return ps, E * es * np.exp(e_sigma * rng.standard_normal(num_elems))
 
 
-def read_pos_displacements(path: str, labels=None) -> np.ndarray:
-    """Nodal displacements of every printed step of a FAST .pos file: [steps][nnode][3].
-
-    Reads the %RESULT.CASE.STEP.NODAL.DISPLACEMENT blocks (written by
-    cControl::PrintResult); rows are ordered by node label.
-    """
+def read_pos_block(path: str, key: str = "NODAL.DISPLACEMENT") -> np.ndarray:
+    """Nodal vectors of one result block (``%RESULT.CASE.STEP.<key>``) of every
+    printed step of a FAST .pos file: [steps][nnode][3], rows ordered by node
+    label.  Keys written by cControl::PrintResult / cCtrlNewmark::PrintVelAcc:
+    NODAL.DISPLACEMENT, VELOCITY, ACCELERATION."""
     steps = []
     with open(path) as fp:
         lines = fp.read().splitlines()
+    tag = "%RESULT.CASE.STEP." + key
     i = 0
     while i < len(lines):
-        if lines[i].strip() == "%RESULT.CASE.STEP.NODAL.DISPLACEMENT":
+        if lines[i].strip() == tag:
             n = int(lines[i + 1].split()[0])
             rows = [lines[i + 2 + k].split() for k in range(n)]
             lab = np.array([int(r[0]) for r in rows])
@@ -351,6 +354,11 @@ def read_pos_displacements(path: str, labels=None) -> np.ndarray:
         else:
             i += 1
     return np.asarray(steps)
+
+
+def read_pos_displacements(path: str, labels=None) -> np.ndarray:
+    """Nodal displacements of every printed step of a FAST .pos file: [steps][nnode][3]."""
+    return read_pos_block(path, "NODAL.DISPLACEMENT")
 
 
 # --------------------------------------------------------------------------
@@ -376,6 +384,10 @@ def write_dat(deck: Deck, base: str) -> str:
         lines += ["%HEADER.ANALYSIS.MAXIMUM.STEPS", str(int(deck.maxstep)), ""]
     if deck.step_factor != 1.0:
         lines += ["%HEADER.ANALYSIS.STEP.FACTOR", _fmt(deck.step_factor), ""]
+    if deck.algorithm.lower() == "newmark":
+        lines += ["%HEADER.ANALYSIS.TIME.STEP", _fmt(deck.time_step), ""]
+        lines += ["%HEADER.ANALYSIS.NEWMARK.PARAMETERS", f"{_fmt(deck.newmark[0])} {_fmt(deck.newmark[1])}", ""]
+        lines += ["%HEADER.ANALYSIS.PRINT.STEPS", str(int(deck.print_step)), ""]
     lines += ["%HEADER.OUTPUT.PRECISION", "15", ""]
     lines += ["%NODE", str(deck.num_nodes), "", "%NODE.COORD", str(deck.num_nodes)]
     lines += [f"{int(l)} {_fmt(x)} {_fmt(y)} {_fmt(z)}" for l, (x, y, z) in zip(lab, deck.coords)]

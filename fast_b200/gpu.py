@@ -48,7 +48,7 @@ EXPORTS = [
     "fast_gpu_ws_build_basis", "fast_gpu_ws_train", "fast_gpu_ws_predict", "fast_gpu_ws_report",
     "fast_gpu_ws_get_basis", "fast_gpu_ws_get_samples", "fast_gpu_mlp_params", "fast_gpu_mlp_forward",
     "fast_gpu_mlp_loss_grad", "fast_gpu_mlp_gemm", "fast_gpu_ws_configure", "fast_gpu_ws_last_input",
-    "fast_gpu_set_option", "fast_gpu_set_problems", "fast_gpu_solve_batch",
+    "fast_gpu_set_option", "fast_gpu_set_problems", "fast_gpu_solve_batch", "fast_gpu_newmark",
 ]
 OPT_PERSISTENT_MAX_NODES = 1
 KERNEL_SPMV_FP64, KERNEL_SPMV_FP32, KERNEL_ASSEMBLE = 0, 1, 2
@@ -114,6 +114,21 @@ NR_PREDICTOR = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int32, c
 PREDICT_NONE, PREDICT_SECANT, PREDICT_CALLBACK = 0, 1, 2
 
 
+class NewmarkOpts(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_int32), ("reserved", ctypes.c_int32), ("dt", ctypes.c_double),
+                ("gamma", ctypes.c_double), ("beta", ctypes.c_double), ("lin", SolveOpts), ("mass", SolveOpts)]
+
+
+class NewmarkReport(ctypes.Structure):
+    _fields_ = [("steps_done", ctypes.c_int32), ("failed_step", ctypes.c_int32),
+                ("linear_iterations", ctypes.c_int32), ("max_step_iterations", ctypes.c_int32),
+                ("mass_iterations", ctypes.c_int32), ("escalated_steps", ctypes.c_int32),
+                ("umax", ctypes.c_double), ("vmax", ctypes.c_double), ("amax", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class ProblemReport(ctypes.Structure):
     _fields_ = [("converged", ctypes.c_int32), ("iterations", ctypes.c_int32), ("rel_residual", ctypes.c_double)]
 
@@ -160,6 +175,8 @@ def load_library(path: str = LIB_PATH):
     L.fast_gpu_synchronize.argtypes = [vp]
     L.fast_gpu_set_option.argtypes = [vp, ctypes.c_int32, ctypes.c_int64]
     L.fast_gpu_set_problems.argtypes = [vp, ctypes.c_int32, _lp]
+    L.fast_gpu_newmark.argtypes = [vp, _dp, ctypes.POINTER(NewmarkOpts), _dp, _dp, _dp, ctypes.c_int32, _ip, _dp,
+                                   ctypes.POINTER(NewmarkReport)]
     L.fast_gpu_solve_batch.argtypes = [vp, _dp, _dp, ctypes.POINTER(SolveOpts), ctypes.POINTER(ProblemReport)]
     L.fast_gpu_upload_mesh.argtypes = [vp, ctypes.POINTER(Mesh)]
     L.fast_gpu_pattern_info.argtypes = [vp, _lp, _lp, _ip, _dp]
@@ -296,6 +313,24 @@ class GpuSystem:
             self.close()
         except Exception:
             pass
+
+    def newmark(self, q, steps, dt, gamma=0.5, beta=0.25, precision=PREC_FP64, precond=PRECOND_JACOBI, tol=1e-10,
+                warm=True, mass_tol=1e-12, probes=None, check_every=0):
+        """Linear Newmark (cCtrlNewmark::Solver) under the step load q.
+        Returns (u, v, a) at the last step, u at the probe equations per step
+        ([steps][len(probes)], or None) and the report."""
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        lin = SolveOpts(precision, precond, 0, int(bool(warm)), float(tol), 0.0, 0, int(check_every))
+        mass = SolveOpts(PREC_FP64, PRECOND_JACOBI, 0, 0, float(mass_tol), 0.0, 0, 0)
+        o = NewmarkOpts(int(steps), 0, float(dt), float(gamma), float(beta), lin, mass)
+        u, v, a = np.zeros(self.neq), np.zeros(self.neq), np.zeros(self.neq)
+        pr = np.ascontiguousarray(probes if probes is not None else [], dtype=np.int32)
+        hist = np.zeros((steps, len(pr))) if len(pr) else None
+        rep = NewmarkReport()
+        self._ck(self.L.fast_gpu_newmark(self.ctx, _p(q), ctypes.byref(o), _p(u), _p(v), _p(a), len(pr),
+                                         _p(pr, _ip) if len(pr) else _ip(), _p(hist) if hist is not None else _dp(),
+                                         ctypes.byref(rep)), "newmark")
+        return (u, v, a), hist, rep.as_dict()
 
     def set_problems(self, node_offsets):
         """Mark the uploaded mesh as independent problems over node ranges."""

@@ -290,6 +290,37 @@ int fast_gpu_mlp_loss_grad(fast_gpu_ws *ws, int32_t batch, const float *x, const
 int fast_gpu_mlp_gemm(fast_gpu_ctx *ctx, int32_t M, int32_t N, int32_t K, const float *A, int32_t ta,
                       const float *B, int32_t tb, float *C);
 
+/* ---- linear Newmark time integration -----------------------------------
+ * cCtrlNewmark::Solver (ctrl/ctrlnewmark.cpp:79-254) without damping, under
+ * the step load q (the same external load at every time, t = 0 included):
+ * M a(0) = q, K_eff = K + M/(beta dt^2), per step the effective load
+ * q + M (a0 u + a2 v + a3 a), a solve with K_eff and the reference's update
+ * of a and v.  Each solve is a PCG (opts->lin, warm-started from the last
+ * displacements when lin.warm_start) where the reference factors K_eff
+ * once.  Needs densities on the buckets.  Leaves K_eff in the stiffness
+ * slot (the next fast_gpu_assemble rebuilds K). */
+typedef struct {
+  int32_t steps;              /* MAXIMUM.STEPS                                        */
+  int32_t reserved;
+  double  dt;                 /* TIME.STEP                                            */
+  double  gamma, beta;        /* NEWMARK.PARAMETERS (0.5, 0.25: average acceleration) */
+  fast_gpu_solve_opts lin;    /* the step solves                                      */
+  fast_gpu_solve_opts mass;   /* M a(0) = q                                           */
+} fast_gpu_newmark_opts;
+
+typedef struct {
+  int32_t steps_done, failed_step;
+  int32_t linear_iterations, max_step_iterations;
+  int32_t mass_iterations, escalated_steps;
+  double  umax, vmax, amax;   /* max over the steps of the inf-norms (the reference's printout) */
+} fast_gpu_newmark_report;
+
+/* q host [num_eq]; u_out, v_out, a_out [num_eq] (final state) may be NULL;
+ * probe_hist [steps][nprobe] receives u at the equations probe_eq[k]. */
+int fast_gpu_newmark(fast_gpu_ctx *ctx, const double *q, const fast_gpu_newmark_opts *opts, double *u_out,
+                     double *v_out, double *a_out, int32_t nprobe, const int32_t *probe_eq, double *probe_hist,
+                     fast_gpu_newmark_report *rep);
+
 /* ---- many independent problems -----------------------------------------
  * Each problem is what one FAST run of cLinStat (ctrl/ctrllins.cpp:46-99)
  * solves; their meshes are uploaded together as one mesh whose problem k owns

@@ -159,3 +159,43 @@ def pcg(K, f, tol, maxit):
     ok = lib().fo_pcg(n, _p(rp, ctypes.POINTER(ctypes.c_int64)), _p(ci, ctypes.POINTER(ctypes.c_int32)), _p(v),
                       _p(f), _p(u), int(maxit), float(tol), ctypes.byref(it), ctypes.byref(err))
     return u, bool(ok), it.value, err.value
+
+
+def mass_matrix(deck):
+    """Equation-space consistent mass matrix (scipy CSR) from elem_mass."""
+    Me = np.array([elem_mass(deck.nn, deck.ngp, deck.coords[deck.conn[e]], deck.rho[e])[0]
+                   for e in range(deck.num_elems)])
+    return assemble(deck, Me)
+
+
+def newmark(K, M, f, dt, steps, gamma=0.5, beta=0.25):
+    """Linear Newmark of cCtrlNewmark::Solver (ctrl/ctrlnewmark.cpp:79-254),
+    without damping, under the constant (step) load f from t = 0, with direct
+    solves: a(0) from M a = f, K_eff = K + a0 M, then per step
+    f_eff = f + M (a0 u + a2 v + a3 a), u = K_eff^-1 f_eff,
+    a <- -a3 a + a0 du - a2 v, v <- v + a6 a_old + a7 a.
+    Returns u, v, a per step: three [steps][neq] arrays."""
+    import scipy.sparse.linalg as sla
+    a0 = 1.0 / (beta * dt * dt)
+    a2 = 1.0 / (beta * dt)
+    a3 = 0.5 / beta - 1.0
+    a6 = (1.0 - gamma) * dt
+    a7 = gamma * dt
+    n = K.shape[0]
+    u = np.zeros(n)
+    v = np.zeros(n)
+    a = sla.spsolve(M.tocsc(), f)
+    lu = sla.splu((K + a0 * M).tocsc())
+    U, V, A = [], [], []
+    for _ in range(steps):
+        fe = f + M @ (a0 * u + a2 * v + a3 * a)
+        un = lu.solve(fe)
+        du = un - u
+        a_old = a
+        a = -a3 * a + a0 * du - a2 * v
+        v = v + a6 * a_old + a7 * a
+        u = un
+        U.append(u.copy())
+        V.append(v.copy())
+        A.append(a.copy())
+    return np.array(U), np.array(V), np.array(A)

@@ -149,6 +149,29 @@ def main():
                    maxit=np.array(d.maxit))
         np.savez_compressed(os.path.join(HERE, "nr_plate_tl.npz"), **out)
         print("nr_plate_tl:", us.shape, "max |w|", np.abs(us[..., 2]).max())
+
+        # the reference's own linear Newmark (cCtrlNewmark, unmodified `fast`
+        # binary, skyline): displacements, velocities and accelerations of every
+        # step of a hex20 box with density under a step load
+        d = decks.box_hex20_lognormal(4, 4, 2, seed=7)
+        d.rho = np.full(d.num_elems, 1e-3)
+        d.algorithm = "newmark"
+        d.time_step = 2e-4
+        d.maxstep = 20
+        base = os.path.join(tmp, "nm_hex20_box")
+        decks.write_dat(d, base)
+        subprocess.run([refdump.FAST, base, "-silent"], check=True, stdout=subprocess.DEVNULL)
+        # read the printed steps before the harness reuses the deck's output file
+        blocks = {k: decks.read_pos_block(base + ".pos", k) for k in ("NODAL.DISPLACEMENT", "VELOCITY", "ACCELERATION")}
+        ref = refdump.run_dump(base, base + ".bin", "--no-solve", "--no-triplets")
+        out = deck_arrays(d)
+        out.update(ref_neq=ref["neq"], ref_node_eq=ref["node_eq"], ref_f=ref["f"],
+                   ref_u_steps=blocks["NODAL.DISPLACEMENT"], ref_v_steps=blocks["VELOCITY"],
+                   ref_a_steps=blocks["ACCELERATION"],
+                   steps=np.array(d.maxstep), time_step=np.array(d.time_step),
+                   gamma=np.array(d.newmark[0]), beta=np.array(d.newmark[1]))
+        np.savez_compressed(os.path.join(HERE, "nm_hex20_box.npz"), **out)
+        print("nm_hex20_box:", out["ref_u_steps"].shape)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
 

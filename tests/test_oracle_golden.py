@@ -7,7 +7,7 @@ import scipy.sparse as sp
 from oracle import fem_oracle as fo
 from tests import golden_io as gio
 
-CASES = [n for n in gio.names() if not n.startswith("nr_")]
+CASES = [n for n in gio.names() if not n.startswith(("nr_", "nm_"))]
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -181,3 +181,21 @@ def test_oracle_newton_matches_reference_nr():
         unode = np.zeros((d.num_nodes, 3))
         unode[m] = us[k][eq[m] - 1]
         assert gio.rel(unode, g["ref_u_steps"][k]) < 1e-8, k
+
+
+def test_oracle_newmark_matches_reference():
+    """The oracle's restatement of cCtrlNewmark::Solver (with the oracle's K
+    and consistent M) reproduces the displacements, velocities and
+    accelerations the reference's own `fast` binary printed for every step."""
+    d, g = gio.load("nm_hex20_box")
+    K = fo.assemble(d)
+    M = fo.mass_matrix(d)
+    U, V, A = fo.newmark(K, M, g["ref_f"], float(g["time_step"]), int(g["steps"]), float(g["gamma"]),
+                         float(g["beta"]))
+    eq = g["ref_node_eq"].reshape(-1, 3)
+    m = eq > 0
+    for name, X, R in (("u", U, g["ref_u_steps"]), ("v", V, g["ref_v_steps"]), ("a", A, g["ref_a_steps"])):
+        for s in range(X.shape[0]):
+            node = np.zeros(eq.shape)
+            node[m] = X[s][eq[m] - 1]
+            assert gio.rel(node, R[s]) < 1e-9, (name, s, gio.rel(node, R[s]))
