@@ -1,0 +1,262 @@
+// bsp_kernels.cu - Bezier-extracted B-spline / NURBS solid elements (sm_100a).
+//
+// Computes what cElmParam::StiffMat (elc/elmparam.cpp:539-597) computes for an
+// element of %ELEMENT.BSPLINE.SOLID: the same Gauss loop and isotropic B^T C B
+// as the hex kernels, on the shape functions of cShapeBspSolid
+// (shp/shpbsp.cpp:928-1067):
+//   B_a(g)   = Nr_i(r_g) Ns_j(s_g) Nt_k(t_g)     a = i + Qr j + Qr Qs k,  Qd = (degree in d) + 1
+//   rational: N_a = B_a w_a / W,  W = sum_a B_a w_a,
+//             dN_a/dxi = (dB_a/dxi w_a - N_a dW/dxi) / W
+// where the univariate factors of the element's knot span are the Bezier-
+// extracted tables built on the host (one table per direction, span and
+// Gauss point; see bspline_gauss_tables).  For non-rational patches the plain
+// tensor-product derivative is used: the reference's non-rational branch
+// (shp/shpbsp.cpp:1015-1030) never advances its node index, so only its
+// rational branch is a usable oracle, and with unit weights both agree.
+//
+// Layout per CTA (one element at a time, grid-stride over one colour):
+//   sD  [NG][3][NN]  natural derivatives, overwritten in place by dN/dx
+//   sB  [NG][NN]     rational numerators (rational patches only)
+// Thread t owns node pairs t, t+NT, ...: M_ij = sum_g c_g dNa/dx_i dNb/dx_j,
+// turned into the isotropic 3x3 block and added into K through the slot map
+// (elements of one colour share no node, so the adds need no atomics and K
+// is bit-identical from run to run).
+#include <cstdint>
+
+#include "elem_common.cuh"
+#include "internal.h"
+
+namespace fastgpu {
+
+template <int PR, int PS, int PT, int NG1>
+struct BspSmem {
+  static constexpr int QR = PR + 1, QS = PS + 1, QT = PT + 1;
+  static constexpr int NN = QR * QS * QT;
+  static constexpr int NG = NG1 * NG1 * NG1;
+  static constexpr int NP = NN * (NN + 1) / 2;
+  static constexpr int kX = NN * 3, kW = NN, kB = NG * NN, kD = NG * 3 * NN, kJ = NG * 9, kC = NG, kWg = NG * 4;
+  static constexpr size_t doubles = kX + kW + kB + kD + kJ + kC + kWg;
+  static constexpr size_t bytes = doubles * sizeof(double) + NP * 2 + NN + 16;
+};
+
+template <int PR, int PS, int PT, int NG1, int NT>
+__global__ void __launch_bounds__(NT, 1) bsp_elem_kernel(ElemArgs A) {
+  using S = BspSmem<PR, PS, PT, NG1>;
+  constexpr int QR = S::QR, QS = S::QS, QT = S::QT, NN = S::NN, NG = S::NG, NP = S::NP, ND = 3 * NN;
+  extern __shared__ __align__(16) double sm[];
+  double *sX = sm;
+  double *sW = sX + S::kX;
+  double *sB = sW + S::kW;
+  double *sD = sB + S::kB;
+  double *sJ = sD + S::kD;
+  double *sc = sJ + S::kJ;
+  double *sWg = sc + S::kC;
+  uint8_t *spair = reinterpret_cast<uint8_t *>(sWg + S::kWg);
+  uint8_t *sfix = spair + 2 * NP;
+  const int tid = threadIdx.x;
+  for (int q = tid; q < NP; q += NT) {
+    int a, b;
+    pair_of(q, NN, a, b);
+    spair[2 * q] = (uint8_t)a;
+    spair[2 * q + 1] = (uint8_t)b;
+  }
+  const double *__restrict__ gw = A.w;
+  const bool rat = A.rational != 0;
+
+  for (int64_t it = blockIdx.x; it < A.ne; it += gridDim.x) {
+    const int64_t e = A.index ? (int64_t)A.index[it] : A.offset + it;
+    __syncthreads();
+    const int32_t *en = A.conn + e * NN;
+    for (int i = tid; i < NN * 3; i += NT) sX[i] = A.X[3 * (int64_t)en[i / 3] + (i % 3)];
+    for (int i = tid; i < NN; i += NT) {
+      sfix[i] = A.fix[en[i]];
+      sW[i] = (rat && A.wt) ? A.wt[en[i]] : 1.0;
+    }
+    const int sr = A.span[4 * e], ss = A.span[4 * e + 1], st = A.span[4 * e + 2];
+    const double *br = A.bas[0] + (size_t)sr * NG1 * QR * 2;
+    const double *bs = A.bas[1] + (size_t)ss * NG1 * QS * 2;
+    const double *bt = A.bas[2] + (size_t)st * NG1 * QT * 2;
+    __syncthreads();
+
+    // tensor-product basis (cShapeBspSolid::DrvShpRST, shp/shpbsp.cpp:985-1067)
+    for (int t = tid; t < NG * NN; t += NT) {
+      const int g = t / NN, a = t - NN * g;
+      const int gl = g % NG1, gj = (g / NG1) % NG1, gi = g / (NG1 * NG1);
+      const int ia = a % QR, ja = (a / QR) % QS, ka = a / (QR * QS);
+      const double *fr = br + (gl * QR + ia) * 2, *fs = bs + (gj * QS + ja) * 2, *ft = bt + (gi * QT + ka) * 2;
+      double *D = sD + g * ND;
+      if (rat) {
+        const double w = sW[a];
+        sB[g * NN + a] = fr[0] * fs[0] * ft[0] * w;
+        D[a] = fr[1] * fs[0] * ft[0] * w;
+        D[NN + a] = fr[0] * fs[1] * ft[0] * w;
+        D[2 * NN + a] = fr[0] * fs[0] * ft[1] * w;
+      } else {
+        D[a] = fr[1] * fs[0] * ft[0];
+        D[NN + a] = fr[0] * fs[1] * ft[0];
+        D[2 * NN + a] = fr[0] * fs[0] * ft[1];
+      }
+    }
+    if (rat) {
+      __syncthreads();
+      // W and dW/dxi per Gauss point, summed in node order as the reference
+      for (int g = tid; g < NG; g += NT) {
+        const double *D = sD + g * ND;
+        double w = 0.0, wr = 0.0, ws = 0.0, wt = 0.0;
+        for (int a = 0; a < NN; a++) {
+          w += sB[g * NN + a];
+          wr += D[a];
+          ws += D[NN + a];
+          wt += D[2 * NN + a];
+        }
+        sWg[4 * g] = w;
+        sWg[4 * g + 1] = wr;
+        sWg[4 * g + 2] = ws;
+        sWg[4 * g + 3] = wt;
+      }
+      __syncthreads();
+      for (int t = tid; t < NG * NN; t += NT) {
+        const int g = t / NN, a = t - NN * g;
+        const double *Wg = sWg + 4 * g;
+        const double n = sB[g * NN + a] / Wg[0];
+        double *D = sD + g * ND;
+        D[a] = (D[a] - n * Wg[1]) / Wg[0];
+        D[NN + a] = (D[NN + a] - n * Wg[2]) / Wg[0];
+        D[2 * NN + a] = (D[2 * NN + a] - n * Wg[3]) / Wg[0];
+      }
+    }
+    __syncthreads();
+
+    // Jacobians J[g][p][q] = sum_a dN_a/dxi_p X_a,q (cShapeSolid::DrvShpXYZ, shp/shpsolid.cpp:58-126)
+    for (int t = tid; t < NG * 9; t += NT) {
+      const int g = t / 9, pq = t - 9 * g, p = pq / 3, q = pq - 3 * p;
+      const double *d = sD + g * ND + p * NN;
+      double s = 0.0;
+      for (int a = 0; a < NN; a++) s += d[a] * sX[3 * a + q];
+      sJ[t] = s;
+    }
+    __syncthreads();
+    // determinant and inverse by cofactors (cShape::ShpMatInv, shp/shape.cpp:360-393)
+    for (int g = tid; g < NG; g += NT) {
+      double *J = sJ + 9 * g;
+      const double j00 = J[0], j01 = J[1], j02 = J[2], j10 = J[3], j11 = J[4], j12 = J[5], j20 = J[6],
+                   j21 = J[7], j22 = J[8];
+      const double det = j00 * (j11 * j22 - j12 * j21) - j01 * (j10 * j22 - j12 * j20) + j02 * (j10 * j21 - j11 * j20);
+      if (!(det > 0.0)) atomicOr(A.status, 1);
+      const double id = 1.0 / ((det != 0.0) ? det : 1.0);
+      J[0] = (j11 * j22 - j12 * j21) * id;
+      J[1] = -(j01 * j22 - j02 * j21) * id;
+      J[2] = (j01 * j12 - j02 * j11) * id;
+      J[3] = -(j10 * j22 - j12 * j20) * id;
+      J[4] = (j00 * j22 - j02 * j20) * id;
+      J[5] = -(j00 * j12 - j02 * j10) * id;
+      J[6] = (j10 * j21 - j11 * j20) * id;
+      J[7] = -(j00 * j21 - j01 * j20) * id;
+      J[8] = (j00 * j11 - j01 * j10) * id;
+      sc[g] = gw[g] * det;
+    }
+    __syncthreads();
+    // dN/dx in place: each (g, a) reads and writes only its own three entries
+    for (int t = tid; t < NG * NN; t += NT) {
+      const int g = t / NN, a = t - NN * g;
+      const double *J = sJ + 9 * g;
+      double *D = sD + g * ND;
+      const double d0 = D[a], d1 = D[NN + a], d2 = D[2 * NN + a];
+      D[a] = J[0] * d0 + J[1] * d1 + J[2] * d2;
+      D[NN + a] = J[3] * d0 + J[4] * d1 + J[5] * d2;
+      D[2 * NN + a] = J[6] * d0 + J[7] * d1 + J[8] * d2;
+    }
+    __syncthreads();
+
+    const double E = A.E[e], nu = A.nu[e];
+    const double dd = (1.0 + nu) * (1.0 - 2.0 * nu);
+    const double C00 = E * (1.0 - nu) / dd, C01 = E * nu / dd, G = 0.5 * E / (1.0 + nu);
+    for (int q = tid; q < NP; q += NT) {
+      const int pa = spair[2 * q], pb = spair[2 * q + 1];
+      double M[9];
+#pragma unroll
+      for (int k = 0; k < 9; k++) M[k] = 0.0;
+      for (int g = 0; g < NG; g++) {
+        const double *D = sD + g * ND;
+        const double cg = sc[g];
+        const double a0 = cg * D[pa], a1 = cg * D[NN + pa], a2 = cg * D[2 * NN + pa];
+        const double b0 = D[pb], b1 = D[NN + pb], b2 = D[2 * NN + pb];
+        M[0] = fma(a0, b0, M[0]); M[1] = fma(a0, b1, M[1]); M[2] = fma(a0, b2, M[2]);
+        M[3] = fma(a1, b0, M[3]); M[4] = fma(a1, b1, M[4]); M[5] = fma(a1, b2, M[5]);
+        M[6] = fma(a2, b0, M[6]); M[7] = fma(a2, b1, M[7]); M[8] = fma(a2, b2, M[8]);
+      }
+      // isotropic block (cSolid::QMatrix elc/anmodel.cpp:1286-1298, BMatrix :1418-1447)
+      double v[9];
+      const double tr = M[0] + M[4] + M[8];
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+          v[3 * i + j] = (i == j) ? C00 * M[4 * i] + G * (tr - M[4 * i]) : C01 * M[3 * i + j] + G * M[3 * j + i];
+      if (A.Ke_out) {
+        double *Ko = A.Ke_out + it * ND * ND;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+          for (int j = 0; j < 3; j++) {
+            Ko[(3 * pa + i) * ND + 3 * pb + j] = v[3 * i + j];
+            Ko[(3 * pb + j) * ND + 3 * pa + i] = v[3 * i + j];
+          }
+      }
+      if (A.K) {
+        double *Kab = A.K + (int64_t)A.slot[(e * NN + pa) * NN + pb] * 9;
+        double *Kba = pa != pb ? A.K + (int64_t)A.slot[(e * NN + pb) * NN + pa] * 9 : nullptr;
+        const uint8_t fa = sfix[pa], fb = sfix[pb];
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+          for (int j = 0; j < 3; j++)
+            if (!((fa >> i) & 1) && !((fb >> j) & 1)) {
+              Kab[3 * i + j] += v[3 * i + j];
+              if (Kba) Kba[3 * j + i] += v[3 * i + j];
+            }
+      }
+    }
+  }
+}
+
+template <int PR, int PS, int PT, int NG1, int NT>
+static cudaError_t run_bsp(Ctx &c, ElemArgs a, int64_t count) {
+  if (count <= 0) return cudaSuccess;
+  using S = BspSmem<PR, PS, PT, NG1>;
+  auto kern = bsp_elem_kernel<PR, PS, PT, NG1, NT>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, S::bytes);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  int64_t grid = (int64_t)per_sm * c.sm_count;
+  if (grid > count) grid = count;
+  a.ne = count;
+  kern<<<(unsigned)grid, NT, S::bytes, c.stream>>>(a);
+  c.launches++;
+  return cudaGetLastError();
+}
+
+bool bsp_supported(const int pd[3], int ngp) {
+  if (pd[0] == 2 && pd[1] == 2 && pd[2] == 2) return ngp == 3 || ngp == 4;
+  if (pd[0] == 3 && pd[1] == 3 && (pd[2] == 3 || pd[2] == 2)) return ngp == 4;
+  return false;
+}
+
+cudaError_t launch_bsp_elements(Ctx &c, const Bucket &B, ElemArgs a, int64_t count) {
+  a.span = B.d_span;
+  for (int d = 0; d < 3; d++) a.bas[d] = B.d_bas + B.bas_off[d];
+  a.wt = B.d_wt;
+  a.rational = B.rational;
+  const int ng = B.ngp[0];
+  const int *p = B.pd;
+  if (p[0] == 2 && p[1] == 2 && p[2] == 2 && ng == 3) return run_bsp<2, 2, 2, 3, 384>(c, a, count);
+  if (p[0] == 2 && p[1] == 2 && p[2] == 2 && ng == 4) return run_bsp<2, 2, 2, 4, 384>(c, a, count);
+  if (p[0] == 3 && p[1] == 3 && p[2] == 3 && ng == 4) return run_bsp<3, 3, 3, 4, 512>(c, a, count);
+  if (p[0] == 3 && p[1] == 3 && p[2] == 2 && ng == 4) return run_bsp<3, 3, 2, 4, 512>(c, a, count);
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace fastgpu

@@ -3,6 +3,8 @@
 
 #include <cstdint>
 
+#include <cuda_runtime.h>
+
 namespace fastgpu {
 
 struct ElemArgs {
@@ -22,7 +24,17 @@ struct ElemArgs {
   int32_t *status;            // bit 0: non-positive Jacobian determinant
   const double *U;            // [nnode][4] nodal displacements (total-Lagrangian / internal force)
   double *G;                  // [nnode][4] internal force, added to (colour-safe) or null
+  // B-spline solids
+  const int32_t *span;        // [*][4] colour-sorted knot spans (r, s, t, unused)
+  const double *bas[3];       // per direction [nspan][ngp][p+1][2] {N, dN/dt}
+  const double *wt;           // [nnode] control-point weights (rational patches)
+  int rational;
 };
+
+struct Ctx;
+struct Bucket;
+// B-spline solid buckets (bsp_kernels.cu): stiffness scatter or element matrices
+cudaError_t launch_bsp_elements(Ctx &c, const Bucket &B, ElemArgs a, int64_t count);
 
 // (a, b) pair index -> a <= b, row-major over the upper triangle
 __device__ __forceinline__ void pair_of(int p, int n, int &a, int &b) {

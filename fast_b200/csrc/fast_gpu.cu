@@ -42,6 +42,7 @@ void free_mesh(Ctx &c) {
   for (Bucket &B : c.buckets) {
     dfree(B.d_conn); dfree(B.d_E); dfree(B.d_nu); dfree(B.d_rho); dfree(B.d_slot);
     dfree(B.d_dN); dfree(B.d_N); dfree(B.d_w);
+    dfree(B.d_span); dfree(B.d_bas); dfree(B.d_wt);
   }
   c.buckets.clear();
   dfree(c.d_X); dfree(c.d_fix); dfree(c.d_dof_of_eq);
@@ -243,13 +244,21 @@ int fast_gpu_upload_mesh(fast_gpu_ctx *c, const fast_gpu_mesh *m) {
     const fast_gpu_bucket &bk = m->buckets[b];
     Bucket &B = c->buckets[b];
     B.type = bk.elem_type;
-    B.nn = nodes_of(bk.elem_type);
-    if (!B.nn) { c->err = "upload_mesh: unsupported element type"; return FAST_GPU_ENOTSUP; }
+    B.nn = bucket_nodes(bk);
+    if (!B.nn) {
+      c->err = bk.elem_type == FAST_ELEM_BSP_SOLID
+                   ? "upload_mesh: B-spline solid bucket needs a patch of degree 2 or 3 in all directions"
+                   : "upload_mesh: unsupported element type";
+      return FAST_GPU_ENOTSUP;
+    }
     for (int k = 0; k < 3; k++) B.ngp[k] = bk.ngp[k];
     B.ng = B.ngp[0] * B.ngp[1] * B.ngp[2];
+    if (B.type == FAST_ELEM_BSP_SOLID)
+      for (int d = 0; d < 3; d++) B.pd[d] = bk.patch->degree[d];
     const bool ok_rule = (B.ngp[0] == B.ngp[1] && B.ngp[1] == B.ngp[2]) &&
                          ((B.type == FAST_ELEM_HEX8 && (B.ngp[0] == 1 || B.ngp[0] == 2 || B.ngp[0] == 3)) ||
-                          (B.type == FAST_ELEM_HEX20 && (B.ngp[0] >= 2 && B.ngp[0] <= 4)));
+                          (B.type == FAST_ELEM_HEX20 && (B.ngp[0] >= 2 && B.ngp[0] <= 4)) ||
+                          (B.type == FAST_ELEM_BSP_SOLID && bsp_supported(B.pd, B.ngp[0])));
     if (!ok_rule) { c->err = "upload_mesh: unsupported Gauss rule for this element type"; return FAST_GPU_ENOTSUP; }
     B.ne = bk.num_elems;
     if (B.ne <= 0 || !bk.conn || !bk.E || !bk.nu) { c->err = "upload_mesh: empty bucket"; return FAST_GPU_EINVAL; }
@@ -259,6 +268,28 @@ int fast_gpu_upload_mesh(fast_gpu_ctx *c, const fast_gpu_mesh *m) {
       return FAST_GPU_ENOTSUP;
     }
     B.tl = bk.formulation == FAST_FORM_TOTAL_LAGRANGIAN;
+    if (B.type == FAST_ELEM_BSP_SOLID) {
+      const fast_gpu_patch &P = *bk.patch;
+      if (B.tl || B.has_rho) {
+        c->err = "upload_mesh: B-spline solids support the small-strain stiffness only";
+        return FAST_GPU_ENOTSUP;
+      }
+      if (!P.span) { c->err = "upload_mesh: B-spline solid bucket without element spans"; return FAST_GPU_EINVAL; }
+      for (int d = 0; d < 3; d++) {
+        std::vector<double> tab;
+        if (!bspline_gauss_tables(B.pd[d], P.num_knots[d], P.knots[d], B.ngp[d], B.nspan[d], tab)) {
+          c->err = "upload_mesh: invalid knot vector in patch direction " + std::to_string(d);
+          return FAST_GPU_EINVAL;
+        }
+      }
+      for (int64_t e = 0; e < B.ne; e++)
+        for (int d = 0; d < 3; d++)
+          if (P.span[3 * e + d] < 0 || P.span[3 * e + d] >= B.nspan[d]) {
+            c->err = "upload_mesh: element " + std::to_string(e) + " names a knot span outside its patch";
+            return FAST_GPU_EINVAL;
+          }
+      B.rational = P.rational ? 1 : 0;
+    }
   }
   if (!build_pattern(*c, *m)) return FAST_GPU_EINVAL;
 
@@ -304,6 +335,39 @@ int fast_gpu_upload_mesh(fast_gpu_ctx *c, const fast_gpu_mesh *m) {
       CK(cudaMemcpy(B.d_rho, rho.data(), sizeof(double) * ne, cudaMemcpyHostToDevice));
     }
     std::vector<double> N, dN, w;
+    if (B.type == FAST_ELEM_BSP_SOLID) {
+      const fast_gpu_patch &P = *bk.patch;
+      std::vector<double> all;
+      for (int d = 0; d < 3; d++) {
+        std::vector<double> tab;
+        int ns = 0;
+        bspline_gauss_tables(B.pd[d], P.num_knots[d], P.knots[d], B.ngp[d], ns, tab);
+        B.bas_off[d] = (int64_t)all.size();
+        all.insert(all.end(), tab.begin(), tab.end());
+      }
+      CK(dalloc(&B.d_bas, all.size()));
+      CK(cudaMemcpy(B.d_bas, all.data(), sizeof(double) * all.size(), cudaMemcpyHostToDevice));
+      std::vector<int32_t> sp(4 * ne, 0);
+      for (int64_t s = 0; s < ne; s++)
+        for (int d = 0; d < 3; d++) sp[4 * s + d] = P.span[3 * (int64_t)B.perm[s] + d];
+      CK(dalloc(&B.d_span, 4 * ne));
+      CK(cudaMemcpy(B.d_span, sp.data(), sizeof(int32_t) * sp.size(), cudaMemcpyHostToDevice));
+      if (B.rational && P.weights) {
+        CK(dalloc(&B.d_wt, nnode));
+        CK(cudaMemcpy(B.d_wt, P.weights, sizeof(double) * nnode, cudaMemcpyHostToDevice));
+      }
+      // Gauss weights only: the shape functions come from the span tables
+      double r[6], wr[6], ws[6], wt[6];
+      gauss_rule(B.ngp[0], r, wr);
+      gauss_rule(B.ngp[1], r, ws);
+      gauss_rule(B.ngp[2], r, wt);
+      for (int i = 0; i < B.ngp[2]; i++)
+        for (int j = 0; j < B.ngp[1]; j++)
+          for (int l = 0; l < B.ngp[0]; l++) w.push_back(wr[l] * ws[j] * wt[i]);
+      CK(dalloc(&B.d_w, w.size()));
+      CK(cudaMemcpy(B.d_w, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice));
+      continue;
+    }
     gauss_point_tables(B.type, B.ngp, N, dN, w);
     CK(dalloc(&B.d_N, N.size()));
     CK(cudaMemcpy(B.d_N, N.data(), sizeof(double) * N.size(), cudaMemcpyHostToDevice));
@@ -667,6 +731,10 @@ int fast_gpu_element_matrices(fast_gpu_ctx *c, int32_t what, int32_t b, int64_t 
   if (first < 0 || count <= 0 || first + count > B.ne) return FAST_GPU_EINVAL;
   if (what == FAST_ASM_MASS && !B.has_rho) { c->err = "element_matrices: bucket has no density"; return FAST_GPU_ESTATE; }
   if (what != FAST_ASM_STIFFNESS && what != FAST_ASM_MASS && what != FAST_ASM_INTERNAL_FORCE) return FAST_GPU_EINVAL;
+  if (B.type == FAST_ELEM_BSP_SOLID && what != FAST_ASM_STIFFNESS) {
+    c->err = "element_matrices: B-spline solids provide the stiffness matrix only";
+    return FAST_GPU_ENOTSUP;
+  }
   const int nd = 3 * B.nn;
   const size_t mat_bytes = sizeof(double) * (size_t)count * (what == FAST_ASM_INTERNAL_FORCE ? nd : nd * nd);
   double *buf = nullptr;
@@ -697,7 +765,7 @@ int fast_gpu_inspect_pattern(const fast_gpu_mesh *m, int64_t *nnzb, int64_t *nnz
   c.buckets.resize(m->num_buckets);
   for (int b = 0; b < m->num_buckets; b++) {
     c.buckets[b].type = m->buckets[b].elem_type;
-    c.buckets[b].nn = nodes_of(m->buckets[b].elem_type);
+    c.buckets[b].nn = bucket_nodes(m->buckets[b]);
     c.buckets[b].ne = m->buckets[b].num_elems;
     if (!c.buckets[b].nn || !m->buckets[b].conn) return FAST_GPU_ENOTSUP;
   }

@@ -59,6 +59,14 @@ struct Bucket {
   double *d_dN = nullptr;          // [ng][nn][3] natural derivatives at the Gauss points
   double *d_N = nullptr;           // [ng][nn] shape functions
   double *d_w = nullptr;           // [ng] Gauss weights
+  // B-spline solids (FAST_ELEM_BSP_SOLID)
+  int pd[3] = {0, 0, 0};           // degree per direction
+  int rational = 0;
+  int nspan[3] = {0, 0, 0};
+  int32_t *d_span = nullptr;       // [ne][4] colour-sorted spans per direction (4th unused)
+  double *d_bas = nullptr;         // per direction d at offset bas_off[d]: [nspan][ngp_d][p+1][2] (N, dN/dt)
+  int64_t bas_off[3] = {0, 0, 0};
+  double *d_wt = nullptr;          // [nnode] control-point weights (rational patches)
 };
 
 struct Ctx {
@@ -172,6 +180,14 @@ bool gauss_rule(int n, double *r, double *w);
 void gauss_point_tables(int type, const int ngp[3], std::vector<double> &N, std::vector<double> &dN,
                         std::vector<double> &w);
 int nodes_of(int type);
+// B-spline solid kernels exist for these (degree per direction, Gauss order)
+bool bsp_supported(const int pd[3], int ngp);
+// nodes per element of a bucket description (B-spline solids: product of p+1); 0 = unsupported
+int bucket_nodes(const fast_gpu_bucket &bk);
+// Per-span univariate basis tables of one patch direction at the Gauss
+// points: out[(s * ng + g) * (p + 1) + i] = {N_i, dN_i/dt} of span s.  False
+// when the knot vector is not a valid open or clamped vector of this degree.
+bool bspline_gauss_tables(int p, int nknots, const double *knots, int ng, int &nspan, std::vector<double> &out);
 
 // kernels (elem_kernels.cu / solve_kernels.cu); all launched on c.stream
 cudaError_t launch_zero_matrix(Ctx &c, double *K, bool identity_on_fixed);

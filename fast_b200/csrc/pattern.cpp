@@ -41,7 +41,7 @@ bool build_pattern(Ctx &c, const fast_gpu_mesh &m) {
   std::vector<int64_t> ecount(nnode + 1, 0);
   for (int b = 0; b < m.num_buckets; b++) {
     const fast_gpu_bucket &bk = m.buckets[b];
-    const int nn = nodes_of(bk.elem_type);
+    const int nn = bucket_nodes(bk);
     for (int64_t e = 0; e < bk.num_elems; e++)
       for (int a = 0; a < nn; a++) {
         int32_t n = bk.conn[e * nn + a];
@@ -56,7 +56,7 @@ bool build_pattern(Ctx &c, const fast_gpu_mesh &m) {
     std::vector<int64_t> fill(ecount.begin(), ecount.end() - 1);
     for (int b = 0; b < m.num_buckets; b++) {
       const fast_gpu_bucket &bk = m.buckets[b];
-      const int nn = nodes_of(bk.elem_type);
+      const int nn = bucket_nodes(bk);
       for (int64_t e = 0; e < bk.num_elems; e++)
         for (int a = 0; a < nn; a++) elist[fill[bk.conn[e * nn + a]]++] = ((int64_t)b << 40) | e;
     }
@@ -76,7 +76,7 @@ bool build_pattern(Ctx &c, const fast_gpu_mesh &m) {
           const int b = (int)(elist[k] >> 40);
           const int64_t e = elist[k] & ((1LL << 40) - 1);
           const fast_gpu_bucket &bk = m.buckets[b];
-          const int nn = nodes_of(bk.elem_type);
+          const int nn = bucket_nodes(bk);
           for (int a = 0; a < nn; a++) {
             int32_t n = bk.conn[e * nn + a];
             if (mark[n] != i) { mark[n] = i; cnt++; }
@@ -104,7 +104,7 @@ bool build_pattern(Ctx &c, const fast_gpu_mesh &m) {
           const int b = (int)(elist[k] >> 40);
           const int64_t e = elist[k] & ((1LL << 40) - 1);
           const fast_gpu_bucket &bk = m.buckets[b];
-          const int nn = nodes_of(bk.elem_type);
+          const int nn = bucket_nodes(bk);
           for (int a = 0; a < nn; a++) {
             int32_t n = bk.conn[e * nn + a];
             if (mark[n] != i) { mark[n] = i; out[cnt++] = n; }
@@ -165,18 +165,24 @@ bool build_pattern(Ctx &c, const fast_gpu_mesh &m) {
   for (int b = 0; b < m.num_buckets; b++) {
     const fast_gpu_bucket &bk = m.buckets[b];
     Bucket &B = c.buckets[b];
-    std::vector<uint64_t> node_colors(nnode, 0);  // bit k: a colour-k element uses the node
+    // bit k of a node's mask: a colour-k element uses the node.  B-spline
+    // solids of degree p need at least (p+1)^3 colours (64 for p = 3).
+    constexpr int kWords = 4;  // up to 256 colours
+    std::vector<uint64_t> node_colors((size_t)nnode * kWords, 0);
     const int nn = B.nn;
     std::vector<int32_t> color(bk.num_elems);
     int ncol = 0;
     for (int64_t e = 0; e < bk.num_elems; e++) {
-      uint64_t used = 0;
-      for (int a = 0; a < nn; a++) used |= node_colors[bk.conn[e * nn + a]];
-      if (~used == 0) return c.set_error("element colouring needs more than 64 colours");
-      int col = __builtin_ctzll(~used);
+      uint64_t used[kWords] = {0, 0, 0, 0};
+      for (int a = 0; a < nn; a++)
+        for (int w = 0; w < kWords; w++) used[w] |= node_colors[(size_t)bk.conn[e * nn + a] * kWords + w];
+      int col = -1;
+      for (int w = 0; w < kWords && col < 0; w++)
+        if (~used[w] != 0) col = 64 * w + __builtin_ctzll(~used[w]);
+      if (col < 0) return c.set_error("element colouring needs more than 256 colours");
       color[e] = col;
       ncol = std::max(ncol, col + 1);
-      for (int a = 0; a < nn; a++) node_colors[bk.conn[e * nn + a]] |= (1ULL << col);
+      for (int a = 0; a < nn; a++) node_colors[(size_t)bk.conn[e * nn + a] * kWords + col / 64] |= (1ULL << (col % 64));
     }
     c.ncolors = std::max(c.ncolors, ncol);
     // stable counting sort by colour

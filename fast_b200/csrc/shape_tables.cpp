@@ -11,6 +11,7 @@
 // FAST's local node order, written here from the standard closed forms
 //   corner  N = 1/8 (1+r ri)(1+s si)(1+t ti)(r ri + s si + t ti - 2)
 //   edge    N = 1/4 (1-r^2)(1+s si)(1+t ti)   (and permutations).
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -97,6 +98,155 @@ int nodes_of(int type) {
     case FAST_ELEM_HEX20: return 20;
     default: return 0;
   }
+}
+
+int bucket_nodes(const fast_gpu_bucket &bk) {
+  if (bk.elem_type != FAST_ELEM_BSP_SOLID) return nodes_of(bk.elem_type);
+  if (!bk.patch) return 0;
+  int nn = 1;
+  for (int d = 0; d < 3; d++) {
+    const int p = bk.patch->degree[d];
+    if (p < 2 || p > 3) return 0;
+    nn *= p + 1;
+  }
+  return nn;
+}
+
+namespace {
+
+// The p+1 B-splines of degree p that are non-zero on knot span [U[k], U[k+1]),
+// evaluated at u by the Cox-de Boor recurrence, built up one degree at a time:
+//   N_{i,q}(u) = (u - U_i)/(U_{i+q} - U_i) N_{i,q-1} + (U_{i+q+1} - u)/(U_{i+q+1} - U_{i+1}) N_{i+1,q-1}
+// (de Boor 1972; 0/0 := 0).  out[i] = N_{k-p+i,p}(u).  The span is given, so u
+// may sit on its right end and the value is that of the span's polynomial piece.
+void span_basis(int p, const double *U, int k, double u, double *out) {
+  double N[8] = {0.0};
+  N[p] = 1.0;  // degree 0: only N_{k,0} = 1 on the span
+  for (int q = 1; q <= p; q++) {
+    // degree q functions N_{k-q..k, q} stored at N[p-q .. p]
+    for (int t = p - q; t <= p; t++) {
+      const int i = k - p + t;  // global index of the function at slot t
+      double v = 0.0;
+      const double dl = U[i + q] - U[i];
+      if (t >= p - q + 1 && dl > 0.0) v += (u - U[i]) / dl * N[t];
+      const double dr = U[i + q + 1] - U[i + 1];
+      if (t + 1 <= p && dr > 0.0) v += (U[i + q + 1] - u) / dr * N[t + 1];
+      N[t] = v;
+    }
+  }
+  for (int i = 0; i <= p; i++) out[i] = N[i];
+}
+
+double binom(int n, int k) {
+  double r = 1.0;
+  for (int i = 1; i <= k; i++) r = r * (n - k + i) / i;
+  return r;
+}
+
+// Bernstein polynomials of degree p on [0, 1] and their derivatives
+void bernstein(int p, double x, double *B, double *dB) {
+  for (int j = 0; j <= p; j++) B[j] = binom(p, j) * std::pow(x, j) * std::pow(1.0 - x, p - j);
+  if (!dB) return;
+  double lo[8];
+  for (int j = 0; j < p; j++) lo[j] = binom(p - 1, j) * std::pow(x, j) * std::pow(1.0 - x, p - 1 - j);
+  for (int j = 0; j <= p; j++) dB[j] = p * ((j > 0 ? lo[j - 1] : 0.0) - (j < p ? lo[j] : 0.0));
+}
+
+// Solve A x = b (n <= 8) by Gaussian elimination with partial pivoting
+bool small_solve(int n, double A[8][8], double *b) {
+  for (int c = 0; c < n; c++) {
+    int piv = c;
+    for (int r = c + 1; r < n; r++)
+      if (std::fabs(A[r][c]) > std::fabs(A[piv][c])) piv = r;
+    if (A[piv][c] == 0.0) return false;
+    if (piv != c) {
+      for (int k = 0; k < n; k++) std::swap(A[c][k], A[piv][k]);
+      std::swap(b[c], b[piv]);
+    }
+    for (int r = c + 1; r < n; r++) {
+      const double f = A[r][c] / A[c][c];
+      for (int k = c; k < n; k++) A[r][k] -= f * A[c][k];
+      b[r] -= f * b[c];
+    }
+  }
+  for (int c = n - 1; c >= 0; c--) {
+    double v = b[c];
+    for (int k = c + 1; k < n; k++) v -= A[c][k] * b[k];
+    b[c] = v / A[c][c];
+  }
+  return true;
+}
+
+}  // namespace
+
+// Bezier extraction of one knot span: the span's B-splines as combinations of
+// the degree-p Bernstein polynomials in xi = (u - U_k)/(U_{k+1} - U_k),
+//   N_{k-p+i}(u) = sum_j C[i][j] B_j(xi)
+// (the operator cKnotVector::CompBezExtMat builds by knot insertion,
+// geom/knotvec.cpp:415-493).  Here it is found by collocation instead: both
+// sides are degree-p polynomials on the span, so matching them at the p+1
+// points xi_c = c/p determines C.  Then the Gauss-point tables follow the
+// reference's evaluation (cShapeBsp::EvalBspBas/EvalBspBasDerv,
+// shp/shpbsp.cpp:254-300): xi = (t+1)/2, and dN/dt takes the Bernstein
+// derivative halved.
+bool bspline_gauss_tables(int p, int nknots, const double *U, int ng, int &nspan, std::vector<double> &out) {
+  nspan = 0;
+  out.clear();
+  if (p < 1 || p > 7 || ng < 1 || ng > 6 || !U || nknots < 2 * (p + 1)) return false;
+  for (int i = 1; i < nknots; i++)
+    if (!(U[i] >= U[i - 1])) return false;
+  // non-zero spans as the reference counts them (knot gap above 1e-5,
+  // cKnotVector::FindSpan(int), geom/knotvec.cpp:303-313)
+  std::vector<int> left;
+  for (int i = 1; i < nknots; i++)
+    if (U[i] - U[i - 1] > 1e-5) left.push_back(i - 1);
+  if (left.empty()) return false;
+  for (int k : left)
+    if (k < p || k > nknots - p - 2) return false;  // needs p functions on each side
+  nspan = (int)left.size();
+  double tr[6], tw[6];
+  gauss_rule(ng, tr, tw);
+  out.assign((size_t)nspan * ng * (p + 1) * 2, 0.0);
+  for (int s = 0; s < nspan; s++) {
+    const int k = left[s];
+    const double u0 = U[k], h = U[k + 1] - U[k];
+    // collocation: V[c][j] = B_j(xi_c), rhs columns N_i(u_c)
+    double V[8][8], Nc[8][8];
+    for (int c = 0; c <= p; c++) {
+      const double xi = (double)c / p;
+      bernstein(p, xi, V[c], nullptr);
+      double nb[8];
+      span_basis(p, U, k, u0 + xi * h, nb);
+      for (int i = 0; i <= p; i++) Nc[i][c] = nb[i];
+    }
+    double C[8][8];
+    for (int i = 0; i <= p; i++) {
+      double A[8][8], x[8];
+      for (int r = 0; r <= p; r++) {
+        for (int cc = 0; cc <= p; cc++) A[r][cc] = V[r][cc];
+        x[r] = Nc[i][r];
+      }
+      if (!small_solve(p + 1, A, x)) return false;
+      for (int j = 0; j <= p; j++) C[i][j] = x[j];
+    }
+    for (int g = 0; g < ng; g++) {
+      const double xi = 0.5 * (tr[g] + 1.0);
+      double B[8], dB[8];
+      bernstein(p, xi, B, dB);
+      for (int j = 0; j <= p; j++) dB[j] /= 2.0;
+      for (int i = 0; i <= p; i++) {
+        double n = 0.0, d = 0.0;
+        for (int j = 0; j <= p; j++) {
+          n += C[i][j] * B[j];
+          d += C[i][j] * dB[j];
+        }
+        double *o = &out[(((size_t)s * ng + g) * (p + 1) + i) * 2];
+        o[0] = n;
+        o[1] = d;
+      }
+    }
+  }
+  return true;
 }
 
 bool gauss_rule(int n, double *r, double *w) {

@@ -355,6 +355,10 @@ static ElemArgs tl_args(Ctx &c, const Bucket &B, double *K, double *G) {
 cudaError_t launch_tl(Ctx &c, double *K, double *G, bool want_k, bool want_g) {
   for (size_t b = 0; b < c.buckets.size(); b++) {
     const Bucket &B = c.buckets[b];
+    if (B.type == FAST_ELEM_BSP_SOLID) {
+      if (want_g) return cudaErrorNotSupported;  // B-spline solids: stiffness only
+      continue;
+    }
     int mode;
     if (B.tl) {
       if (!want_k && !want_g) continue;

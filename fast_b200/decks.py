@@ -57,8 +57,21 @@ KINDS = {"hex8": (8, HEX8_NAT, HEX8_FACES), "hex20": (20, HEX20_NAT, HEX20_FACES
 
 
 @dataclasses.dataclass
+class Patch:
+    """A B-spline solid patch (cBspPat, geom/patch.cpp:1459-1484) and the knot
+    spans of its elements (%ELEMENT.BSPLINE.SOLID, shp/shpbsp.cpp:57-116)."""
+    degree: tuple                   # polynomial degree in r, s and t
+    knots: list                     # three knot vectors, multiplicities expanded
+    span: np.ndarray                # [ne, 3] 0-based non-zero span per direction
+    grid: tuple                     # control points per direction (r fastest in the patch list)
+    cps: np.ndarray                 # [grid product] node index of each patch control point
+    weights: Optional[np.ndarray] = None  # [nnode] control-point weights, None = 1
+    rational: bool = True           # the reference deck's rational flag
+
+
+@dataclasses.dataclass
 class Deck:
-    kind: str                       # "hex8" | "hex20"
+    kind: str                       # "hex8" | "hex20" | "bsp" (B-spline solid)
     coords: np.ndarray              # [nnode, 3] float64
     conn: np.ndarray                # [ne, nn] int32, 0-based node index
     E: np.ndarray                   # [ne] float64
@@ -82,10 +95,21 @@ class Deck:
     print_step: int = 1                       # %HEADER.ANALYSIS.PRINT.STEPS
     node_labels: Optional[np.ndarray] = None  # [nnode] labels used in a .dat
     title: str = "deck"
+    patch: Optional[Patch] = None             # kind "bsp": the element patch
+    nodal_f: Optional[np.ndarray] = None      # [nnode, 3] nodal forces (%LOAD.CASE.NODAL.FORCE)
+    blocks: list = dataclasses.field(default_factory=list)  # further element buckets on the same nodes
+    solver_rank: Optional[np.ndarray] = None  # [nnode] %NODE.SOLVER.ORDER position of each node (1-based)
 
     @property
     def nn(self) -> int:
+        if self.kind == "bsp":
+            d = self.patch.degree
+            return (d[0] + 1) * (d[1] + 1) * (d[2] + 1)
         return KINDS[self.kind][0]
+
+    def buckets(self) -> list:
+        """This deck's own elements followed by its extra blocks."""
+        return [self] + list(self.blocks)
 
     @property
     def num_nodes(self) -> int:
@@ -105,13 +129,16 @@ class Deck:
 
         Follows cControl::InitDofs/CompEqs (ctrl/ctrl.cpp:2004-2104): DOFs
         are activated by the elements that use the node, supports remove
-        them, and numbering runs over nodes in label order, x, y, z.
+        them, and numbering runs over nodes in solver order, x, y, z.
         """
         active = np.zeros((self.num_nodes, 3), dtype=bool)
-        active[np.unique(self.conn.ravel())] = True
+        for b in self.buckets():
+            active[np.unique(b.conn.ravel())] = True
         if self.fixed is not None:
             active &= ~self.fixed
-        order = np.argsort(self.labels(), kind="stable")
+        # nodes in solver order (cNode::GetNodeInSolverOrder, node/node.cpp:543-552):
+        # ascending %NODE.SOLVER.ORDER position when given, else label order
+        order = np.argsort(self.labels() if self.solver_rank is None else self.solver_rank, kind="stable")
         eq = np.zeros((self.num_nodes, 3), dtype=np.int32)
         flat = active[order].ravel()
         nums = np.cumsum(flat, dtype=np.int64)
@@ -333,6 +360,71 @@ def plate_variant_params(seed: int, num_elems: int, E: float = 1000.0, p_range=(
     return ps, E * es * np.exp(e_sigma * rng.standard_normal(num_elems))
 
 
+def open_knots(p: int, n: int) -> np.ndarray:
+    """Open uniform knot vector of degree p with n unit spans: p+1 zeros,
+    1..n-1, p+1 values n (multiplicities expanded)."""
+    return np.concatenate([np.zeros(p), np.arange(n + 1, dtype=np.float64), np.full(p, float(n))])
+
+
+def bspline_box(p: int, n=(4, 4, 2), L=(4.0, 4.0, 2.0), origin=(0.0, 0.0, 0.0), jitter=0.05, seed=0,
+                E=1000.0, nu=0.3, ngp=None, clamp_axis=0, load=(0.0, 0.0, -1.0)) -> Deck:
+    """B-spline solid block of degree p with n[d] elements (knot spans) per
+    direction on open uniform knot vectors.
+
+    Control points sit on a uniform grid of (n[d] + p) points per direction
+    over the box, each coordinate moved by uniform[-jitter h, jitter h]
+    (h = L[d]/n[d], the element size) except along the direction in which the
+    point is on a face of the box, so the faces stay plane.  The face
+    x[clamp_axis] = origin is clamped and the opposite face carries nodal
+    forces summing to ``load``.  Elements are numbered with the r span
+    fastest; local nodes are the element's (p+1)^3 control points, r index
+    fastest (cShapeBspSolid::Init, shp/shpbsp.cpp:873-902).
+    """
+    n = tuple(int(v) for v in n)
+    nb = tuple(v + p for v in n)
+    rng = np.random.default_rng(seed)
+    axes = [origin[d] + L[d] * np.arange(nb[d]) / (nb[d] - 1) for d in range(3)]
+    I, J, K = np.meshgrid(np.arange(nb[0]), np.arange(nb[1]), np.arange(nb[2]), indexing="ij")
+    idx = np.stack([I.ravel(order="F"), J.ravel(order="F"), K.ravel(order="F")], axis=1)  # r fastest
+    coords = np.stack([axes[d][idx[:, d]] for d in range(3)], axis=1)
+    for d in range(3):
+        h = L[d] / n[d]
+        inner = (idx[:, d] > 0) & (idx[:, d] < nb[d] - 1)
+        coords[inner, d] += rng.uniform(-jitter * h, jitter * h, int(inner.sum()))
+    ids = np.arange(len(coords)).reshape(nb[2], nb[1], nb[0])  # [k][j][i]
+    Q = p + 1
+    el = []
+    span = []
+    for ek in range(n[2]):
+        for ej in range(n[1]):
+            for ei in range(n[0]):
+                el.append(ids[ek:ek + Q, ej:ej + Q, ei:ei + Q].ravel())
+                span.append((ei, ej, ek))
+    conn = np.asarray(el, dtype=np.int32)
+    ne = len(conn)
+    fixed = np.zeros((len(coords), 3), bool)
+    fixed[idx[:, clamp_axis] == 0] = True
+    nodal = np.zeros((len(coords), 3))
+    far = idx[:, clamp_axis] == nb[clamp_axis] - 1
+    nodal[far] = np.asarray(load, dtype=np.float64) / int(far.sum())
+    patch = Patch((p, p, p), [open_knots(p, n[d]) for d in range(3)], np.asarray(span, dtype=np.int32), nb,
+                  np.arange(len(coords), dtype=np.int64))
+    g = (p + 1,) * 3 if ngp is None else tuple(ngp)
+    return Deck("bsp", coords, conn, np.full(ne, float(E)), np.full(ne, float(nu)), g, fixed,
+                matrix_type="sparse", patch=patch, nodal_f=nodal, title=f"bspline p={p} {n}")
+
+
+def nodal_load_vector(deck: Deck) -> np.ndarray:
+    """Equation-space vector of the deck's nodal forces (cNodalLoad)."""
+    f = np.zeros(deck.num_eq())
+    if deck.nodal_f is None:
+        return f
+    eq = deck.node_eq()
+    m = eq > 0
+    np.add.at(f, eq[m] - 1, deck.nodal_f[m])
+    return f
+
+
 def read_pos_block(path: str, key: str = "NODAL.DISPLACEMENT") -> np.ndarray:
     """Nodal vectors of one result block (``%RESULT.CASE.STEP.<key>``) of every
     printed step of a FAST .pos file: [steps][nnode][3], rows ordered by node
@@ -392,6 +484,8 @@ def write_dat(deck: Deck, base: str) -> str:
     lines += ["%NODE", str(deck.num_nodes), "", "%NODE.COORD", str(deck.num_nodes)]
     lines += [f"{int(l)} {_fmt(x)} {_fmt(y)} {_fmt(z)}" for l, (x, y, z) in zip(lab, deck.coords)]
     lines.append("")
+    if deck.solver_rank is not None:
+        lines += ["%NODE.SOLVER.ORDER", str(deck.num_nodes)] + [" ".join(str(int(v)) for v in deck.solver_rank), ""]
     if deck.fixed is not None and deck.fixed.any():
         sup = np.nonzero(deck.fixed.any(axis=1))[0]
         lines += ["%NODE.SUPPORT", str(len(sup))]
@@ -415,14 +509,45 @@ def write_dat(deck: Deck, base: str) -> str:
     lines.append("")
     g = deck.ngp
     lines += ["%INTEGRATION.ORDER", "1", f"1 {g[0]} {g[1]} {g[2]} {g[0]} {g[1]} {g[2]}", ""]
-    key = {"hex8": "BRICK8", "hex20": "BRICK20"}[deck.kind] + ("TL" if deck.total_lagrangian else "")
-    lines += ["%ELEMENT", str(ne), "", f"%ELEMENT.{key}", str(ne)]
-    cl = lab[deck.conn]
-    lines += [f"{e+1} {inv[e]+1} 1 " + " ".join(str(int(v)) for v in cl[e]) for e in range(ne)]
-    lines.append("")
-    if deck.face_elem is not None and len(deck.face_elem):
+    if deck.kind == "bsp":
+        # one B-spline solid patch (cBspPat::Read, geom/patch.cpp:1459-1484): rational
+        # flag, then per direction degree 'General' #knots values multiplicities,
+        # then the control-point node labels, r fastest
+        P = deck.patch
+        lines += ["%PATCH", "1", f"1 'bspsol' {int(bool(P.rational))}"]
+        for d in range(3):
+            vals, mult = np.unique(np.asarray(P.knots[d]), return_counts=True)
+            lines.append(f"{P.degree[d]} 'General' {len(vals)} " + " ".join(_fmt(v) for v in vals) + " " +
+                         " ".join(str(int(m)) for m in mult))
+        lines.append(" ".join(str(int(v)) for v in lab[P.cps]))
+        lines.append("")
+        if P.weights is not None:
+            lines += ["%CONTROL.POINT.WEIGHT", str(deck.num_nodes)]
+            lines += [f"{int(l)} {_fmt(w)}" for l, w in zip(lab, P.weights)]
+            lines.append("")
+        lines += ["%ELEMENT", str(ne), "", "%ELEMENT.BSPLINE.SOLID", str(ne)]
+        lines += [f"{e+1} {inv[e]+1} 1 1 {int(P.span[e,0])+1} {int(P.span[e,1])+1} {int(P.span[e,2])+1}"
+                  for e in range(ne)]
+        lines.append("")
+    else:
+        key = {"hex8": "BRICK8", "hex20": "BRICK20"}[deck.kind] + ("TL" if deck.total_lagrangian else "")
+        lines += ["%ELEMENT", str(ne), "", f"%ELEMENT.{key}", str(ne)]
+        cl = lab[deck.conn]
+        lines += [f"{e+1} {inv[e]+1} 1 " + " ".join(str(int(v)) for v in cl[e]) for e in range(ne)]
+        lines.append("")
+    has_face = deck.face_elem is not None and len(deck.face_elem)
+    has_nodal = deck.nodal_f is not None and bool(np.any(deck.nodal_f))
+    if has_face or has_nodal:
+        lines += ["%LOAD", "1", "1 'Load_Case_1'", "%LOAD.CASE", "1"]
+    if has_nodal:
+        nz = np.nonzero(np.any(deck.nodal_f != 0.0, axis=1))[0]
+        lines += ["%LOAD.CASE.NODAL.FORCE", str(len(nz))]
+        lines += [f"{int(lab[i])} {_fmt(deck.nodal_f[i,0])} {_fmt(deck.nodal_f[i,1])} {_fmt(deck.nodal_f[i,2])} 0 0 0"
+                  for i in nz]
+        lines.append("")
+    if has_face:
         nf = len(deck.face_elem)
-        lines += ["%LOAD", "1", "1 'Load_Case_1'", "%LOAD.CASE", "1", "%LOAD.CASE.AREA.UNIFORM", str(nf)]
+        lines += ["%LOAD.CASE.AREA.UNIFORM", str(nf)]
         for k in range(nf):
             c = lab[deck.face_corners[k]]
             q = deck.face_q[k]
@@ -489,6 +614,8 @@ def read_dat(path: str) -> Deck:
     for k in range(int(t[0])):
         row = [int(v) for v in t[1 + 7 * k: 8 + 7 * k]]
         ords[row[0]] = tuple(row[1:4])
+    if "ELEMENT.BSPLINE.SOLID" in blk:
+        return _read_bsp(blk, coords, labels, l2i, fixed, mats, secs, ords, path)
     kind, tl, key = None, False, None
     for k, (kd, t_) in {"ELEMENT.BRICK8": ("hex8", False), "ELEMENT.BRICK20": ("hex20", False),
                         "ELEMENT.BRICK8TL": ("hex8", True), "ELEMENT.BRICK20TL": ("hex20", True)}.items():
@@ -533,4 +660,78 @@ def read_dat(path: str) -> Deck:
                 maxit=s1("HEADER.ANALYSIS.MAXIMUM.ITERATIONS", 0, int),
                 maxstep=s1("HEADER.ANALYSIS.MAXIMUM.STEPS", 1, int),
                 step_factor=s1("HEADER.ANALYSIS.STEP.FACTOR", 1.0, float),
-                node_labels=labels, title=os.path.basename(path))
+                node_labels=labels, title=os.path.basename(path), solver_rank=_solver_rank(blk, n))
+
+
+def _read_bsp(blk, coords, labels, l2i, fixed, mats, secs, ords, path) -> Deck:
+    """%PATCH (one 'bspsol' patch, 'General' knot vectors), %CONTROL.POINT.WEIGHT
+    and %ELEMENT.BSPLINE.SOLID (cBspPat::Read geom/patch.cpp:1459-1484,
+    cKnotVector::ReadKnot/ReadMult geom/knotvec.cpp:91-170, cShapeBsp::ReadIGA
+    shp/shpbsp.cpp:57-116)."""
+    t = blk["PATCH"]
+    if int(t[0]) != 1 or t[2] != "'bspsol'":
+        raise ValueError("one 'bspsol' patch per deck is read here")
+    rational = bool(int(t[3]))
+    pos = 4
+    degs, knots, nbas = [], [], []
+    for d in range(3):
+        deg = int(t[pos]); kind = t[pos + 1]; nk = int(t[pos + 2])
+        if kind != "'General'":
+            raise ValueError(f"knot vector format {kind} is not read here")
+        vals = [float(v) for v in t[pos + 3: pos + 3 + nk]]
+        mult = [int(v) for v in t[pos + 3 + nk: pos + 3 + 2 * nk]]
+        pos += 3 + 2 * nk
+        U = np.repeat(np.asarray(vals), mult)
+        degs.append(deg)
+        knots.append(U)
+        nbas.append(len(U) - deg - 1)
+    ncp = nbas[0] * nbas[1] * nbas[2]
+    cps = np.array([l2i[int(v)] for v in t[pos: pos + ncp]], dtype=np.int64)
+    weights = None
+    if "CONTROL.POINT.WEIGHT" in blk:
+        w = blk["CONTROL.POINT.WEIGHT"]
+        nw = int(w[0])
+        weights = np.ones(len(coords))
+        for k in range(nw):
+            weights[l2i[int(w[1 + 2 * k])]] = float(w[2 + 2 * k])
+    t = blk["ELEMENT.BSPLINE.SOLID"]
+    ne = int(t[0])
+    a = np.array(t[1:1 + 7 * ne], dtype=np.int64).reshape(ne, 7)
+    a = a[np.argsort(a[:, 0])]
+    span = (a[:, 4:7] - 1).astype(np.int32)
+    # first basis function of each non-zero span (cBSplineBasis::getBasInd, geom/bspbasis.cpp:59-62)
+    first = []
+    for d in range(3):
+        U = knots[d]
+        left = [i - 1 for i in range(1, len(U)) if U[i] - U[i - 1] > 1e-5]
+        first.append(np.asarray(left) - degs[d])
+    Qr, Qs, Qt = (v + 1 for v in degs)
+    conn = np.zeros((ne, Qr * Qs * Qt), dtype=np.int32)
+    for e in range(ne):
+        b0, b1, b2 = (int(first[d][span[e, d]]) for d in range(3))
+        loc = 0
+        for k in range(Qt):
+            for j in range(Qs):
+                for i in range(Qr):
+                    cp = (b0 + i) + nbas[0] * (b1 + j) + nbas[0] * nbas[1] * (b2 + k)
+                    conn[e, loc] = cps[cp]
+                    loc += 1
+    E = np.array([mats[secs[int(s_)]][0] for s_ in a[:, 1]])
+    nu = np.array([mats[secs[int(s_)]][1] for s_ in a[:, 1]])
+    ordset = {ords[int(o)] for o in a[:, 2]}
+    if len(ordset) != 1:
+        raise ValueError("one integration order per deck is read here")
+    patch = Patch(tuple(degs), knots, span, tuple(nbas), cps, weights, rational)
+    return Deck("bsp", coords, conn, E, nu, ordset.pop(), fixed, matrix_type="sparse", patch=patch,
+                node_labels=labels, title=os.path.basename(path), solver_rank=_solver_rank(blk, len(coords)))
+
+
+def _solver_rank(blk, nnode):
+    """%NODE.SOLVER.ORDER: the i-th entry is the solver position of the i-th
+    node (cNode::ReadSolverOrder, node/node.cpp:248-284)."""
+    if "NODE.SOLVER.ORDER" not in blk:
+        return None
+    t = blk["NODE.SOLVER.ORDER"]
+    if int(t[0]) != nnode:
+        raise ValueError("NODE.SOLVER.ORDER must list every node")
+    return np.array([int(v) for v in t[1:1 + nnode]], dtype=np.int64)

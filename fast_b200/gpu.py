@@ -29,7 +29,7 @@ LIB_PATH = os.path.join(HERE, "libfastgpu.so")
 FAST_GPU_OK = 0
 ERRORS = {-1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ESTATE", -5: "ENONCONV", -6: "EDETJ", -7: "ENOTSUP",
           -8: "ENOTFOUND", -9: "ETOOBIG"}
-ELEM = {"hex8": 1, "hex20": 2}
+ELEM = {"hex8": 1, "hex20": 2, "bsp": 3}
 ASM_K, ASM_M, ASM_G = 1, 2, 3
 FORM_SMALL, FORM_TL = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
@@ -61,11 +61,19 @@ class FastGpuError(RuntimeError):
         self.rc = rc
 
 
+class Patch(ctypes.Structure):
+    _fields_ = [("degree", ctypes.c_int32 * 3), ("num_knots", ctypes.c_int32 * 3),
+                ("knots", ctypes.POINTER(ctypes.c_double) * 3), ("span", ctypes.POINTER(ctypes.c_int32)),
+                ("weights", ctypes.POINTER(ctypes.c_double)), ("rational", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
 class Bucket(ctypes.Structure):
     _fields_ = [("elem_type", ctypes.c_int32), ("ngp", ctypes.c_int32 * 3), ("num_elems", ctypes.c_int64),
                 ("conn", ctypes.POINTER(ctypes.c_int32)), ("E", ctypes.POINTER(ctypes.c_double)),
                 ("nu", ctypes.POINTER(ctypes.c_double)), ("rho", ctypes.POINTER(ctypes.c_double)),
-                ("formulation", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("formulation", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("patch", ctypes.POINTER(Patch))]
 
 
 class Mesh(ctypes.Structure):
@@ -250,19 +258,36 @@ def face_load_vector(deck: _decks.Deck) -> np.ndarray:
     return f
 
 
+def _bucket_struct(b: _decks.Deck, keep: list) -> Bucket:
+    conn = np.ascontiguousarray(b.conn, dtype=np.int32)
+    E = np.ascontiguousarray(b.E, dtype=np.float64)
+    nu = np.ascontiguousarray(b.nu, dtype=np.float64)
+    rho = None if b.rho is None else np.ascontiguousarray(b.rho, dtype=np.float64)
+    keep += [conn, E, nu, rho]
+    pat = ctypes.POINTER(Patch)()
+    if b.kind == "bsp":
+        P = b.patch
+        knots = [np.ascontiguousarray(k, dtype=np.float64) for k in P.knots]
+        span = np.ascontiguousarray(P.span, dtype=np.int32)
+        w = None if P.weights is None else np.ascontiguousarray(P.weights, dtype=np.float64)
+        ps = Patch((ctypes.c_int32 * 3)(*P.degree), (ctypes.c_int32 * 3)(*[len(k) for k in knots]),
+                   (ctypes.POINTER(ctypes.c_double) * 3)(*[_p(k) for k in knots]), _p(span, _ip),
+                   _p(w) if w is not None else ctypes.POINTER(ctypes.c_double)(), int(bool(P.rational)), 0)
+        keep += [knots, span, w, ps]
+        pat = ctypes.pointer(ps)
+    return Bucket(ELEM[b.kind], (ctypes.c_int32 * 3)(*b.ngp), b.num_elems, _p(conn, _ip), _p(E), _p(nu),
+                  _p(rho) if rho is not None else ctypes.POINTER(ctypes.c_double)(),
+                  FORM_TL if b.total_lagrangian else FORM_SMALL, 0, pat)
+
+
 def _mesh_struct(deck: _decks.Deck):
     coords = np.ascontiguousarray(deck.coords, dtype=np.float64)
     eq = np.ascontiguousarray(deck.node_eq(), dtype=np.int32)
-    conn = np.ascontiguousarray(deck.conn, dtype=np.int32)
-    E = np.ascontiguousarray(deck.E, dtype=np.float64)
-    nu = np.ascontiguousarray(deck.nu, dtype=np.float64)
-    rho = None if deck.rho is None else np.ascontiguousarray(deck.rho, dtype=np.float64)
-    b = Bucket(ELEM[deck.kind], (ctypes.c_int32 * 3)(*deck.ngp), deck.num_elems, _p(conn, _ip), _p(E), _p(nu),
-               _p(rho) if rho is not None else ctypes.POINTER(ctypes.c_double)(),
-               FORM_TL if deck.total_lagrangian else FORM_SMALL, 0)
-    buckets = (Bucket * 1)(b)
-    m = Mesh(deck.num_nodes, _p(coords), _p(eq, _ip), int(eq.max(initial=0)), 1, buckets)
-    return m, (coords, eq, conn, E, nu, rho, buckets)
+    keep = []
+    bl = deck.buckets()
+    buckets = (Bucket * len(bl))(*[_bucket_struct(b, keep) for b in bl])
+    m = Mesh(deck.num_nodes, _p(coords), _p(eq, _ip), int(eq.max(initial=0)), len(bl), buckets)
+    return m, (coords, eq, keep, buckets)
 
 
 def inspect_pattern(deck: _decks.Deck) -> dict:
@@ -514,9 +539,10 @@ class GpuSystem:
         return sp.csr_matrix((v, ci, rp), shape=(self.neq, self.neq))
 
     def element_matrices(self, first=0, count=None, what=ASM_K, bucket=0):
-        nn = _decks.KINDS[self.deck.kind][0]
+        b = self.deck.buckets()[bucket]
+        nn = b.nn
         if count is None:
-            count = self.deck.num_elems - first
+            count = b.num_elems - first
         out = np.zeros((count, 3 * nn) if what == ASM_G else (count, 3 * nn, 3 * nn))
         self._ck(self.L.fast_gpu_element_matrices(self.ctx, what, bucket, int(first), int(count), _p(out)),
                  "element_matrices")

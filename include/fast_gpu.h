@@ -48,6 +48,10 @@ extern "C" {
 /* ---- element types (FAST readers elc/element.cpp:1985-2101) ----------- */
 #define FAST_ELEM_HEX8      1   /* %ELEMENT.BRICK8   cElmParam,  SHAPE_BRICK8  */
 #define FAST_ELEM_HEX20     2   /* %ELEMENT.BRICK20  cElmParam,  SHAPE_BRICK20 */
+#define FAST_ELEM_BSP_SOLID 3   /* %ELEMENT.BSPLINE.SOLID cElmParam, SHAPE_BSP_SOLID: Bezier-extracted
+                                   B-spline / NURBS solid (shp/shpbsp.cpp:873-1067); degrees
+                                   (2,2,2) with 3 or 4 Gauss points per direction, (3,3,3) and
+                                   (3,3,2) with 4; needs a patch */
 
 /* ---- element formulation --------------------------------------------- */
 #define FAST_FORM_SMALL_STRAIN       0  /* cElmParam   (%ELEMENT.BRICK8 / BRICK20)     */
@@ -73,6 +77,23 @@ extern "C" {
 
 typedef struct fast_gpu_ctx fast_gpu_ctx;
 
+/* The B-spline patch of a FAST_ELEM_BSP_SOLID bucket (cBspPat, geom/patch.cpp:
+ * 1459-1484, read from %PATCH; element spans from %ELEMENT.BSPLINE.SOLID,
+ * shp/shpbsp.cpp:57-116).  The element's local nodes are its (p+1)^3 control
+ * points with the r index fastest, then s, then t (cShapeBspSolid::Init,
+ * shp/shpbsp.cpp:873-902). */
+typedef struct {
+  int32_t        degree[3];     /* polynomial degree per direction                      */
+  int32_t        num_knots[3];  /* knot vector lengths, repeated knots included          */
+  const double  *knots[3];      /* knot vectors with multiplicities expanded (cKnotVector::Val) */
+  const int32_t *span;          /* [num_elems][3] 0-based non-zero knot span per direction */
+  const double  *weights;       /* [num_nodes] control-point weights (%CONTROL.POINT.WEIGHT)
+                                   or NULL for unit weights (cNode::GetW, node/node.cpp:656-662) */
+  int32_t        rational;      /* patch rational flag: 1 = NURBS quotient N_a w_a / W,
+                                   0 = plain tensor-product B-spline                        */
+  int32_t        reserved;
+} fast_gpu_patch;
+
 /* One bucket = one element type with one Gauss rule (a FAST element reader
  * block with one %INTEGRATION.ORDER). */
 typedef struct {
@@ -85,6 +106,7 @@ typedef struct {
   const double  *rho;           /* [num_elems] density, or NULL                */
   int32_t        formulation;   /* FAST_FORM_*                                 */
   int32_t        reserved;
+  const fast_gpu_patch *patch;  /* FAST_ELEM_BSP_SOLID: its patch; NULL otherwise  */
 } fast_gpu_bucket;
 
 typedef struct {

@@ -1,0 +1,132 @@
+"""B-spline / NURBS solid element stiffness on the CPU (TEST INFRASTRUCTURE ONLY).
+
+A numpy restatement of what FAST computes for %ELEMENT.BSPLINE.SOLID:
+cElmParam::StiffMat (elc/elmparam.cpp:539-597) on the shape functions of
+cShapeBspSolid::DrvShpRST (shp/shpbsp.cpp:985-1067), with B and C as
+cSolid::BMatrix / QMatrix (elc/anmodel.cpp:1418-1447, 1286-1298):
+
+    K_e = sum_g w_g detJ_g B_g^T C B_g .
+
+The univariate B-splines are evaluated directly from the knot vector by the
+Cox-de Boor recurrence (no Bezier extraction), so this checker shares no code
+path with the library, which contracts extraction operators with Bernstein
+polynomials.  The parameter of the knot span is mapped from the Gauss
+coordinate t in [-1, 1] as u = U_k + (t+1)/2 (U_{k+1} - U_k), and the natural
+derivative is dN/dt = (U_{k+1} - U_k)/2 dN/du, which is what the reference's
+extraction form (Bernstein derivative halved, shp/shpbsp.cpp:277-300) equals.
+Rational patches use the quotient N_a = B_a w_a / W; non-rational patches the
+plain tensor product (the reference's non-rational derivative branch,
+shp/shpbsp.cpp:1015-1030, does not advance its node index, so the reference
+itself is only usable as an oracle through its rational branch).
+
+Only ``tests/`` and the golden-fixture script import this module.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+# FAST's 15-digit Gauss tables (elc/intpoint.cpp:742-800) as numbers
+_GR = {2: [-0.577350269189626, 0.577350269189626],
+       3: [-0.774596669241483, 0.0, 0.774596669241483],
+       4: [-0.861136311594053, -0.339981043584856, 0.339981043584856, 0.861136311594053],
+       5: [-0.906179845938664, -0.538469310105683, 0.0, 0.538469310105683, 0.906179845938664]}
+_GW = {2: [1.0, 1.0],
+       3: [0.555555555555556, 0.888888888888889, 0.555555555555556],
+       4: [0.347854845137454, 0.652145154862546, 0.652145154862546, 0.347854845137454],
+       5: [0.236926885056189, 0.478628670499367, 0.568888888888889, 0.478628670499367, 0.236926885056189]}
+
+
+def spans(U):
+    """Left knot index of every non-zero span (gap above 1e-5, as the reference)."""
+    return [i - 1 for i in range(1, len(U)) if U[i] - U[i - 1] > 1e-5]
+
+
+def basis(U, p, k, u):
+    """Values and u-derivatives of the p+1 B-splines non-zero on span k at u."""
+    def N(i, q, x):
+        if q == 0:
+            return 1.0 if i == k else 0.0
+        a = 0.0
+        if U[i + q] - U[i] > 0:
+            a += (x - U[i]) / (U[i + q] - U[i]) * N(i, q - 1, x)
+        if U[i + q + 1] - U[i + 1] > 0:
+            a += (U[i + q + 1] - x) / (U[i + q + 1] - U[i + 1]) * N(i + 1, q - 1, x)
+        return a
+
+    def dN(i, q, x):
+        # dN_{i,q}/du = q/(U_{i+q}-U_i) N_{i,q-1} - q/(U_{i+q+1}-U_{i+1}) N_{i+1,q-1}
+        d = 0.0
+        if U[i + q] - U[i] > 0:
+            d += q / (U[i + q] - U[i]) * N(i, q - 1, x)
+        if U[i + q + 1] - U[i + 1] > 0:
+            d -= q / (U[i + q + 1] - U[i + 1]) * N(i + 1, q - 1, x)
+        return d
+
+    idx = range(k - p, k + 1)
+    return np.array([N(i, p, u) for i in idx]), np.array([dN(i, p, u) for i in idx])
+
+
+def elem_stiff(deck, e):
+    """Stiffness matrix of element e of a "bsp" deck (local DOFs node-major, x y z)."""
+    P = deck.patch
+    deg = P.degree
+    ng = deck.ngp
+    X = deck.coords[deck.conn[e]]
+    w = np.ones(len(X)) if (P.weights is None or not P.rational) else P.weights[deck.conn[e]]
+    tabs = []
+    for d in range(3):
+        U = np.asarray(P.knots[d], dtype=np.float64)
+        k = spans(U)[int(P.span[e, d])]
+        h = U[k + 1] - U[k]
+        vals = []
+        for t in _GR[ng[d]]:
+            n, dn = basis(U, deg[d], k, U[k] + 0.5 * (t + 1.0) * h)
+            vals.append((n, 0.5 * h * dn))
+        tabs.append(vals)
+    E, nu = float(deck.E[e]), float(deck.nu[e])
+    dd = (1 + nu) * (1 - 2 * nu)
+    C = np.zeros((6, 6))
+    C[:3, :3] = E * nu / dd
+    np.fill_diagonal(C[:3, :3], E * (1 - nu) / dd)
+    C[3, 3] = C[4, 4] = C[5, 5] = E / (2 * (1 + nu))
+    nn = len(X)
+    K = np.zeros((3 * nn, 3 * nn))
+    for gt in range(ng[2]):
+        for gs in range(ng[1]):
+            for gr in range(ng[0]):
+                wg = _GW[ng[0]][gr] * _GW[ng[1]][gs] * _GW[ng[2]][gt]
+                nr, dr = tabs[0][gr]
+                ns, ds = tabs[1][gs]
+                nt, dt = tabs[2][gt]
+                # a = i + Qr j + Qr Qs k (r fastest)
+                B = np.einsum("k,j,i->kji", nt, ns, nr).ravel()
+                dB = np.stack([np.einsum("k,j,i->kji", nt, ns, dr).ravel(),
+                               np.einsum("k,j,i->kji", nt, ds, nr).ravel(),
+                               np.einsum("k,j,i->kji", dt, ns, nr).ravel()])
+                if P.rational:
+                    Bw, dBw = B * w, dB * w
+                    W, dW = Bw.sum(), dBw.sum(axis=1)
+                    N = Bw / W
+                    dN = (dBw - np.outer(dW, N)) / W
+                else:
+                    dN = dB
+                J = dN @ X
+                det = np.linalg.det(J)
+                dx = np.linalg.solve(J, dN)
+                Bm = np.zeros((6, 3 * nn))
+                Bm[0, 0::3] = dx[0]
+                Bm[1, 1::3] = dx[1]
+                Bm[2, 2::3] = dx[2]
+                Bm[3, 0::3] = dx[1]
+                Bm[3, 1::3] = dx[0]
+                Bm[4, 0::3] = dx[2]
+                Bm[4, 2::3] = dx[0]
+                Bm[5, 1::3] = dx[2]
+                Bm[5, 2::3] = dx[1]
+                K += wg * det * Bm.T @ C @ Bm
+    return K
+
+
+def elems_stiff(deck, elems=None):
+    elems = range(deck.num_elems) if elems is None else elems
+    return np.array([elem_stiff(deck, int(e)) for e in elems])

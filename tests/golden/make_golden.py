@@ -4,7 +4,8 @@ program itself.
 Run in a container that has the reference tree (default /root/reference,
 override with FAST_REF):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          (all fixtures)
+    python tests/golden/make_golden.py iga      (B-spline solid fixtures only)
 
 It builds ``oracle/_ref/fastref`` (the reference's own sources compiled by
 ``oracle/Makefile``, plus a dump harness), writes each deck with
@@ -43,6 +44,17 @@ def deck_arrays(d: decks.Deck) -> dict:
         out["rho"] = d.rho
     if d.node_labels is not None:
         out["node_labels"] = d.node_labels
+    if d.nodal_f is not None:
+        out["nodal_f"] = d.nodal_f
+    if d.solver_rank is not None:
+        out["solver_rank"] = d.solver_rank
+    if d.patch is not None:
+        P = d.patch
+        out.update(patch_degree=np.array(P.degree, np.int32), patch_span=P.span, patch_grid=np.array(P.grid),
+                   patch_cps=P.cps, patch_rational=np.array(int(bool(P.rational))),
+                   **{f"patch_knots{k}": np.asarray(P.knots[k]) for k in range(3)})
+        if P.weights is not None:
+            out["patch_weights"] = P.weights
     return out
 
 
@@ -88,10 +100,45 @@ def run_case(name, deck, tmp, keep_elems=None, triplets=True, extra=(), uvec=Non
           f"-> {os.path.getsize(os.path.join(HERE, name + '.npz')) / 1e6:.2f} MB")
 
 
+def iga_cases(tmp):
+    """B-spline solids: two seeded blocks with jittered control points (rational
+    flag with unit weights, the reference's usable shape branch) solved by the
+    reference's sparse PCG, and the reference's own NURBS deck
+    dat/iga/ScordelisLoDeg3.dat (weights, degrees 3 x 3 x 2)."""
+    d = decks.bspline_box(2, (3, 2, 2), L=(3.0, 2.0, 1.0), jitter=0.05, seed=1)
+    d.tol = 1e-13
+    d.maxit = 100000
+    run_case("iga_p2_box", d, tmp)
+    d = decks.bspline_box(3, (2, 2, 1), L=(2.0, 2.0, 0.5), jitter=0.05, seed=2)
+    d.tol = 1e-13
+    d.maxit = 100000
+    run_case("iga_p3_box", d, tmp, keep_elems=np.array([0, 3]))
+    src = os.path.join(FAST_REF, "dat/iga/ScordelisLoDeg3.dat")
+    d = decks.read_dat(src)
+    base = os.path.join(tmp, "iga_scordelis_deg3")
+    shutil.copy(src, base + ".dat")
+    os.chmod(base + ".dat", 0o644)
+    ref = refdump.run_dump(base, base + ".bin")
+    out = deck_arrays(d)
+    keep = np.array([0, 9, 63])
+    out.update(ref_neq=ref["neq"], ref_node_eq=ref["node_eq"], ref_elems=keep, ref_elm_K=ref["elm_K"][keep],
+               ref_elm_dofs=ref["elm_dofs"], ref_f=ref["f"], ref_u=ref["u"])
+    out.update({"ref_" + k: v for k, v in lower_csr(ref).items()})
+    np.savez_compressed(os.path.join(HERE, "iga_scordelis_deg3.npz"), **out)
+    print("iga_scordelis_deg3 written")
+
+
 def main():
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"FAST_REF={FAST_REF}", "ref"], check=True)
     tmp = tempfile.mkdtemp(prefix="golden_")
+    if len(sys.argv) > 1 and sys.argv[1] == "iga":
+        try:
+            iga_cases(tmp)
+        finally:
+            shutil.rmtree(tmp, ignore_errors=True)
+        return
     try:
+        iga_cases(tmp)
         # known-answer decks shipped with the reference
         for nm, rel in [("ref_testb8", "dat/continuum/TestB8.dat"), ("ref_beamb20", "dat/continuum/BeamB20.dat")]:
             src = os.path.join(FAST_REF, rel)

@@ -20,7 +20,12 @@ def load(name):
     d = decks.Deck(str(g["kind"]), g["coords"], g["conn"].astype(np.int32), g["E"], g["nu"],
                    tuple(int(v) for v in g["ngp"]), g["fixed"].astype(bool),
                    g.get("face_elem"), g.get("face_corners"), fq, g.get("face_local"),
-                   g.get("rho"), bool(int(g["tl"])), node_labels=g.get("node_labels"), title=name)
+                   g.get("rho"), bool(int(g["tl"])), node_labels=g.get("node_labels"), title=name,
+                   nodal_f=g.get("nodal_f"), solver_rank=g.get("solver_rank"))
+    if "patch_degree" in g:
+        d.patch = decks.Patch(tuple(int(v) for v in g["patch_degree"]), [g[f"patch_knots{k}"] for k in range(3)],
+                              g["patch_span"].astype(np.int32), tuple(int(v) for v in g["patch_grid"]),
+                              g["patch_cps"], g.get("patch_weights"), bool(int(g["patch_rational"])))
     return d, g
 
 

@@ -45,7 +45,7 @@ def test_abi_version(lib):
     assert lib.fast_gpu_version() == 1
 
 
-@pytest.mark.parametrize("name", [n for n in gio.names() if not n.startswith("nr_")])
+@pytest.mark.parametrize("name", [n for n in gio.names() if not n.startswith(("nr_", "iga_"))])
 def test_face_load_vector_matches_reference(lib, name):
     d, g = gio.load(name)
     f = gpu.face_load_vector(d)
@@ -67,7 +67,8 @@ def test_create_without_device_fails_cleanly(lib):
     assert rc == -3 and not ctx.value
 
 
-@pytest.mark.parametrize("name", ["cfg_hex8_cantilever", "cfg_hex20_lognormal_4x4x2", "ref_beamb20"])
+@pytest.mark.parametrize("name", ["cfg_hex8_cantilever", "cfg_hex20_lognormal_4x4x2", "ref_beamb20", "iga_p2_box",
+                                  "iga_p3_box", "iga_scordelis_deg3"])
 def test_host_pattern_matches_reference_structure(lib, name):
     """Node-block pattern covers exactly the reference's stored lower triangle,
     and no two elements of one colour share a node."""

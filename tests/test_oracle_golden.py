@@ -7,7 +7,7 @@ import scipy.sparse as sp
 from oracle import fem_oracle as fo
 from tests import golden_io as gio
 
-CASES = [n for n in gio.names() if not n.startswith(("nr_", "nm_"))]
+CASES = [n for n in gio.names() if not n.startswith(("nr_", "nm_", "iga_"))]
 
 
 @pytest.mark.parametrize("name", CASES)
