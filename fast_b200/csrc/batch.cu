@@ -43,6 +43,7 @@ void free_problems(Ctx &c) {
   } while (0)
 
 extern "C" int fast_gpu_set_problems(fast_gpu_ctx *c, int32_t num_problems, const int64_t *node_offsets) {
+  if (c && c->has_ties()) { c->err = "tied interfaces support linear static solves only"; return FAST_GPU_ENOTSUP; }
   if (!c || num_problems <= 0 || !node_offsets) return FAST_GPU_EINVAL;
   if (c->nnode <= 0) { c->err = "set_problems: no mesh"; return FAST_GPU_ESTATE; }
   std::vector<int64_t> off(node_offsets, node_offsets + num_problems + 1);

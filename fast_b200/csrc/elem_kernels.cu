@@ -301,6 +301,20 @@ cudaError_t launch_fixed_identity(Ctx &c, double *K) {
   return cudaGetLastError();
 }
 
+cudaError_t launch_tied_element_matrices(Ctx &c) {
+  const TiedSet &T = c.tied;
+  for (size_t b = 0; b < c.buckets.size(); b++) {
+    if (T.bucket_pos[b].empty()) continue;
+    const Bucket &B = c.buckets[b];
+    ElemArgs a = base_args(c, B, nullptr);
+    a.Ke_out = T.d_ke + T.bucket_keoff[b];
+    a.index = T.d_bucket_pos[b];
+    cudaError_t e = dispatch<false>(c, B, a, (int64_t)T.bucket_pos[b].size());
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 cudaError_t launch_assemble(Ctx &c, int what, double *target) {
   for (size_t b = 0; b < c.buckets.size(); b++) {
     const Bucket &B = c.buckets[b];
@@ -314,6 +328,7 @@ cudaError_t launch_assemble(Ctx &c, int what, double *target) {
       if (e != cudaSuccess) return e;
     }
   }
+  if (what == FAST_ASM_STIFFNESS) return launch_tied_assemble(c, target);
   return cudaSuccess;
 }
 

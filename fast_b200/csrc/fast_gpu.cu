@@ -45,6 +45,7 @@ void free_mesh(Ctx &c) {
     dfree(B.d_span); dfree(B.d_bas); dfree(B.d_wt);
   }
   c.buckets.clear();
+  free_ties(c);
   dfree(c.d_X); dfree(c.d_fix); dfree(c.d_dof_of_eq);
   dfree(c.d_rowptr); dfree(c.d_col); dfree(c.d_diag); dfree(c.d_srow); dfree(c.d_scol);
   dfree(c.d_K); dfree(c.d_M); dfree(c.d_Ks); dfree(c.d_Ms); dfree(c.d_Ks32);
@@ -291,7 +292,16 @@ int fast_gpu_upload_mesh(fast_gpu_ctx *c, const fast_gpu_mesh *m) {
       B.rational = P.rational ? 1 : 0;
     }
   }
+  if (m->ties && m->ties->num_slaves > 0)
+    for (const Bucket &B : c->buckets)
+      if (B.tl || B.has_rho) {
+        c->err = "upload_mesh: tied interfaces support small-strain stiffness buckets only";
+        return FAST_GPU_ENOTSUP;
+      }
   if (!build_pattern(*c, *m)) return FAST_GPU_EINVAL;
+  // slave DOFs leave the system: flagged like fixed ones (identity diagonal)
+  for (int64_t n = 0; n < nnode; n++)
+    if (c->h_slave_of[n] >= 0) fix[n] = 7;
 
   CK(dalloc(&c->d_X, 3 * nnode));
   CK(cudaMemcpy(c->d_X, m->coords, sizeof(double) * 3 * nnode, cudaMemcpyHostToDevice));
@@ -376,6 +386,7 @@ int fast_gpu_upload_mesh(fast_gpu_ctx *c, const fast_gpu_mesh *m) {
     CK(dalloc(&B.d_w, w.size()));
     CK(cudaMemcpy(B.d_w, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice));
   }
+  CK(upload_ties(*c));
   const int64_t n4 = 4 * nnode;
   CK(dalloc(&c->d_K, 9 * c->nnzb));
   CK(dalloc(&c->d_u, n4)); CK(dalloc(&c->d_r, n4)); CK(dalloc(&c->d_z, n4)); CK(dalloc(&c->d_p, n4));
@@ -465,6 +476,7 @@ int fast_gpu_set_displacement(fast_gpu_ctx *c, const double *u) {
 }
 
 int fast_gpu_internal_force_device(fast_gpu_ctx *c, double *d_g) {
+  if (c && c->has_ties()) { c->err = "internal_force: not available with tied interfaces"; return FAST_GPU_ENOTSUP; }
   if (check_ctx(c) || !d_g || !c->d_gint) return FAST_GPU_EINVAL;
   const int64_t sp = c->begin_span(FAST_KERNEL_INTERNAL_FORCE);
   CK(cudaMemsetAsync(c->d_status, 0, sizeof(int32_t), c->stream));
@@ -661,9 +673,16 @@ int fast_gpu_solve_device(fast_gpu_ctx *c, const double *d_f, double *d_u, const
   const bool warm = o && o->warm_start;
   const int64_t sp = c->begin_span(FAST_KERNEL_LINEAR_SOLVE);
   CK(launch_eq_to_node(*c, d_f, c->d_f));
-  if (warm) CK(launch_eq_to_node(*c, d_u, c->d_u));
+  CK(launch_tie_restrict(*c, c->d_f));
+  if (warm) {
+    CK(launch_eq_to_node(*c, d_u, c->d_u));
+    CK(launch_tie_zero(*c, c->d_u));
+  }
   const int rc = solve_node_space(c, o, warm, rep);
-  if (rc == FAST_GPU_OK || rc == FAST_GPU_ENONCONV) CK(launch_node_to_eq(*c, c->d_u, d_u));
+  if (rc == FAST_GPU_OK || rc == FAST_GPU_ENONCONV) {
+    CK(launch_tie_prolong(*c, c->d_u));
+    CK(launch_node_to_eq(*c, c->d_u, d_u));
+  }
   c->end_span(sp);
   return rc;
 }
@@ -779,11 +798,12 @@ int fast_gpu_inspect_pattern(const fast_gpu_mesh *m, int64_t *nnzb, int64_t *nnz
     const Bucket &B = c.buckets[0];
     for (size_t k = 0; k + 1 < B.color_off.size(); k++)
       for (int64_t s = B.color_off[k]; s < B.color_off[k + 1]; s++) color[B.perm[s]] = (int32_t)k;
+    for (int64_t s = B.ne_regular; s < B.ne; s++) color[B.perm[s]] = -1;  // tied: scattered separately
   }
-  // the slot map must cover every element node pair
+  // the slot map must cover every node pair of the colour-scheduled elements
   for (const Bucket &B : c.buckets)
-    for (int32_t v : B.h_slot)
-      if (v < 0) return FAST_GPU_EINVAL;
+    for (int64_t k = 0; k < B.ne_regular * B.nn * B.nn; k++)
+      if (B.h_slot[k] < 0) return FAST_GPU_EINVAL;
   return FAST_GPU_OK;
 }
 

@@ -59,6 +59,7 @@ struct Bucket {
   double *d_dN = nullptr;          // [ng][nn][3] natural derivatives at the Gauss points
   double *d_N = nullptr;           // [ng][nn] shape functions
   double *d_w = nullptr;           // [ng] Gauss weights
+  int64_t ne_regular = 0;          // colour-scheduled elements; the tied ones follow in perm order
   // B-spline solids (FAST_ELEM_BSP_SOLID)
   int pd[3] = {0, 0, 0};           // degree per direction
   int rational = 0;
@@ -67,6 +68,44 @@ struct Bucket {
   double *d_bas = nullptr;         // per direction d at offset bas_off[d]: [nspan][ngp_d][p+1][2] (N, dN/dt)
   int64_t bas_off[3] = {0, 0, 0};
   double *d_wt = nullptr;          // [nnode] control-point weights (rational patches)
+};
+
+// Elements that touch a tied (slave) node.  Their element matrices go to a
+// scratch buffer and are scattered as T_e^T K_e T_e onto their expanded node
+// list (the non-slave nodes plus the masters of their slave nodes).
+struct TiedSet {
+  int64_t n = 0;                          // tied elements
+  std::vector<int64_t> color_off;         // [ncolors+1] over colour-sorted tied elements
+  std::vector<int64_t> h_nptr;            // [n+1] offsets into h_nodes (expanded node lists)
+  std::vector<int32_t> h_nodes;
+  std::vector<int64_t> h_sptr;            // [n+1] offsets into h_slot (m_e^2 block slots, row-major)
+  std::vector<int32_t> h_slot;
+  std::vector<int64_t> h_pptr;            // [h_nodes.size()+1] pre-image of each expanded node
+  std::vector<int32_t> h_pa;              //   local node of the element
+  std::vector<double> h_pt;               //   weight (1 for a non-slave node)
+  std::vector<int64_t> h_keoff;           // [n] element matrix offset in the scratch buffer
+  std::vector<int32_t> h_nn;              // [n] nodes per element
+  int64_t ke_total = 0;
+  std::vector<std::vector<int32_t>> bucket_pos;  // per bucket: colour-sorted positions, scratch order
+  std::vector<int64_t> bucket_keoff;             // per bucket: first scratch offset
+  int64_t *d_nptr = nullptr, *d_sptr = nullptr, *d_pptr = nullptr, *d_keoff = nullptr;
+  int32_t *d_nodes = nullptr, *d_slot = nullptr, *d_pa = nullptr, *d_nn = nullptr;
+  double *d_pt = nullptr, *d_ke = nullptr;
+  std::vector<int32_t *> d_bucket_pos;
+};
+
+// Slave / master maps of the ties, for the load restriction T^T f and the
+// displacement prolongation u_s = sum w u_m (gather forms, deterministic).
+struct TieMaps {
+  int64_t nslave = 0, nmaster = 0;
+  int32_t *d_slave = nullptr;   // [nslave]
+  int64_t *d_sptr = nullptr;    // [nslave+1]
+  int32_t *d_smaster = nullptr; // masters of each slave
+  double *d_sw = nullptr;
+  int32_t *d_master = nullptr;  // [nmaster] distinct master nodes
+  int64_t *d_mptr = nullptr;    // [nmaster+1]
+  int32_t *d_mslave = nullptr;  // slaves of each master
+  double *d_mw = nullptr;
 };
 
 struct Ctx {
@@ -85,6 +124,13 @@ struct Ctx {
   uint8_t *d_fix = nullptr;       // [nnode] bit i set: DOF i has no equation
   int32_t *d_dof_of_eq = nullptr; // [neq] padded vector index 4*n+i of equation k+1
   std::vector<Bucket> buckets;
+  // tied interfaces
+  std::vector<int64_t> h_tslave, h_tptr, h_tmaster;  // copies of fast_gpu_ties
+  std::vector<double> h_tweight;
+  std::vector<int32_t> h_slave_of;                   // [nnode] tie index of a slave node, -1 otherwise
+  TiedSet tied;
+  TieMaps tmaps;
+  bool has_ties() const { return !h_tslave.empty(); }
 
   // node-block (3x3) CSR pattern, full (both triangles)
   int64_t nnzb = 0;
@@ -194,6 +240,14 @@ cudaError_t launch_zero_matrix(Ctx &c, double *K, bool identity_on_fixed);
 // 1 on the diagonal of every fixed DOF (the stiffness slot's convention)
 cudaError_t launch_fixed_identity(Ctx &c, double *K);
 cudaError_t launch_assemble(Ctx &c, int what, double *target);
+// tied interfaces (ties.cu)
+cudaError_t upload_ties(Ctx &c);
+void free_ties(Ctx &c);
+cudaError_t launch_tied_element_matrices(Ctx &c);   // dense K_e of every tied element into the scratch buffer
+cudaError_t launch_tied_assemble(Ctx &c, double *K);
+cudaError_t launch_tie_restrict(Ctx &c, double *f);  // f <- T^T f (padded node layout)
+cudaError_t launch_tie_zero(Ctx &c, double *v);      // v[slave DOFs] = 0
+cudaError_t launch_tie_prolong(Ctx &c, double *u);   // u[slave] = sum w u[master]
 cudaError_t launch_element_matrices(Ctx &c, int what, int bucket, int64_t first_sorted, int64_t count,
                                     double *d_out);
 

@@ -115,6 +115,7 @@ __global__ void nm_probe(int nprobe, const int32_t *__restrict__ probe, const in
 extern "C" int fast_gpu_newmark(fast_gpu_ctx *c, const double *q, const fast_gpu_newmark_opts *o, double *u_out,
                                 double *v_out, double *a_out, int32_t nprobe, const int32_t *probe_eq,
                                 double *probe_hist, fast_gpu_newmark_report *rep) {
+  if (c && c->has_ties()) { c->err = "tied interfaces support linear static solves only"; return FAST_GPU_ENOTSUP; }
   if (!c || !q || !o || o->steps <= 0 || !(o->dt > 0) || !(o->beta > 0) || nprobe < 0 ||
       (nprobe > 0 && (!probe_eq || !probe_hist)))
     return FAST_GPU_EINVAL;

@@ -125,6 +125,7 @@ struct fast_gpu_ctx : public Ctx {};
 extern "C" int fast_gpu_nr_solve(fast_gpu_ctx *c, const double *q_host, const fast_gpu_nr_opts *o,
                                  fast_gpu_nr_predictor predictor, void *predictor_user, double *u_hist,
                                  int32_t *iters, fast_gpu_nr_report *rep) {
+  if (c && c->has_ties()) { c->err = "tied interfaces support linear static solves only"; return FAST_GPU_ENOTSUP; }
   if (!c || !q_host || !o || o->steps <= 0 || o->max_iter <= 0) return FAST_GPU_EINVAL;
   if (!c->d_K) { c->err = "nr_solve: no mesh"; return FAST_GPU_ESTATE; }
   const int32_t n = c->neq;

@@ -122,21 +122,26 @@ __global__ void __launch_bounds__(NT) skinny_atb_part(int64_t n, int p, int q, c
   }
 }
 
+// one warp per output entry: lane l sums the partials l, l+32, ... in order,
+// then a fixed butterfly combines the lanes (deterministic)
 __global__ void skinny_finish(int nblk, int p, int q, const double *__restrict__ part, double *__restrict__ C,
                               int ldc) {
   const int pq = p * q;
-  for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < pq; o += gridDim.x * blockDim.x) {
-    double t = 0.0;
-    for (int b = 0; b < nblk; b++) t += part[(int64_t)b * pq + o];
-    C[(int64_t)(o / q) * ldc + o % q] = t;
-  }
+  const int lane = threadIdx.x & 31;
+  const int o = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (o >= pq) return;
+  double t = 0.0;
+  for (int b = lane; b < nblk; b += 32) t += part[(int64_t)b * pq + o];
+#pragma unroll
+  for (int m = 16; m > 0; m >>= 1) t += __shfl_xor_sync(0xffffffffu, t, m);
+  if (lane == 0) C[(int64_t)(o / q) * ldc + o % q] = t;
 }
 
 cudaError_t skinny_atb(cudaStream_t s, int64_t n, int p, int q, const double *A, int lda, const double *B, int ldb,
                        double *C, int ldc, double *ws) {
   if (n <= 0 || p <= 0 || q <= 0 || p * q > kSkinnyMaxOut || !ws) return cudaErrorInvalidValue;
   skinny_atb_part<256><<<kSkinnyBlocks, 256, 0, s>>>(n, p, q, A, lda, B, ldb, ws);
-  skinny_finish<<<(p * q + 255) / 256, 256, 0, s>>>(kSkinnyBlocks, p, q, ws, C, ldc);
+  skinny_finish<<<(p * q + 7) / 8, 256, 0, s>>>(kSkinnyBlocks, p, q, ws, C, ldc);
   return cudaGetLastError();
 }
 

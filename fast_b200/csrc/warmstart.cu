@@ -164,34 +164,45 @@ __global__ void ws_chol(int k, const double *__restrict__ E, double *__restrict_
     }
     __syncthreads();
   }
-  for (int t = threadIdx.x; t < k * k; t += blockDim.x) {
-    const int i = t / k, j = t % k;
-    L[t] = j <= i ? A[i][j] : 0.0;
+  __syncthreads();
+  // explicit inverse (L L^T)^-1, one column per thread, so that every reduced
+  // solve of the step is a k x k product
+  for (int c = threadIdx.x; c < k; c += blockDim.x) {
+    double y[64];
+    for (int i = 0; i < k; i++) {
+      double v = (i == c) ? 1.0 : 0.0;
+      for (int p = 0; p < i; p++) v -= A[i][p] * y[p];
+      y[i] = v / A[i][i];
+    }
+    for (int i = k - 1; i >= 0; i--) {
+      double v = y[i];
+      for (int p = i + 1; p < k; p++) v -= A[p][i] * y[p];
+      y[i] = v / A[i][i];
+    }
+    for (int i = 0; i < k; i++) L[i * k + c] = y[i];
   }
   if (threadIdx.x == 0) *ok = bad ? 0 : 1;
 }
 
-// da = (L L^T)^-1 t, or 0 when the factor failed or |t| <= tol |tf|
-__global__ void ws_reduced_solve(int k, const double *__restrict__ L, const int32_t *__restrict__ ok,
+// da = Ainv t (Ainv from ws_chol), or 0 when the factor failed or |t| <= tol |tf|;
+// one warp, thread i forms row i
+__global__ void ws_reduced_solve(int k, const double *__restrict__ Ainv, const int32_t *__restrict__ ok,
                                  const double *__restrict__ t, const double *__restrict__ tf, double tol,
                                  double *__restrict__ da) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int lane = threadIdx.x;
   double tn = 0.0, fn = 0.0;
-  for (int j = 0; j < k; j++) { tn += t[j] * t[j]; fn += tf[j] * tf[j]; }
-  if (!*ok || !(sqrt(tn) > tol * sqrt(fn))) {
-    for (int j = 0; j < k; j++) da[j] = 0.0;
-    return;
+  for (int j = lane; j < k; j += 32) { tn += t[j] * t[j]; fn += tf[j] * tf[j]; }
+#pragma unroll
+  for (int m = 16; m > 0; m >>= 1) {
+    tn += __shfl_xor_sync(0xffffffffu, tn, m);
+    fn += __shfl_xor_sync(0xffffffffu, fn, m);
   }
-  double y[64];
-  for (int i = 0; i < k; i++) {
-    double v = t[i];
-    for (int p = 0; p < i; p++) v -= L[i * k + p] * y[p];
-    y[i] = v / L[i * k + i];
-  }
-  for (int i = k - 1; i >= 0; i--) {
-    double v = y[i];
-    for (int p = i + 1; p < k; p++) v -= L[p * k + i] * da[p];
-    da[i] = v / L[i * k + i];
+  const bool skip = !*ok || !(sqrt(tn) > tol * sqrt(fn));
+  for (int i = lane; i < k; i += 32) {
+    double v = 0.0;
+    if (!skip)
+      for (int j = 0; j < k; j++) v += Ainv[i * k + j] * t[j];
+    da[i] = v;
   }
 }
 
@@ -248,7 +259,7 @@ struct fast_gpu_ws {
   double *d_phin = nullptr;      // [nnode*4][k] basis in the node-padded layout
   double *d_Y = nullptr;         // [nnode*4][k] K Phi
   double *d_Er = nullptr;        // [64*64] Phi^T K Phi
-  double *d_L = nullptr;         // [64*64] its Cholesky factor
+  double *d_L = nullptr;         // [64*64] its inverse (from the Cholesky factor)
   int32_t *d_ok = nullptr;
   double *d_g = nullptr, *d_r = nullptr;  // [n]
   double *d_skinny = nullptr;    // [kSkinnyBlocks][kSkinnyMaxOut] partials of the skinny products

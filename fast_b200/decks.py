@@ -70,6 +70,17 @@ class Patch:
 
 
 @dataclasses.dataclass
+class Ties:
+    """Slave nodes tied to master surfaces: u_s = sum_k w_k u_(m_k) in x, y
+    and z (three %NODE.MULTI-POINT.CONSTRAINT equations per slave,
+    node/node.cpp:459-509)."""
+    slave: np.ndarray               # [ns] node index
+    ptr: np.ndarray                 # [ns+1] offsets into master / weight
+    master: np.ndarray              # master node indices
+    weight: np.ndarray              # interpolation weights
+
+
+@dataclasses.dataclass
 class Deck:
     kind: str                       # "hex8" | "hex20" | "bsp" (B-spline solid)
     coords: np.ndarray              # [nnode, 3] float64
@@ -99,6 +110,7 @@ class Deck:
     nodal_f: Optional[np.ndarray] = None      # [nnode, 3] nodal forces (%LOAD.CASE.NODAL.FORCE)
     blocks: list = dataclasses.field(default_factory=list)  # further element buckets on the same nodes
     solver_rank: Optional[np.ndarray] = None  # [nnode] %NODE.SOLVER.ORDER position of each node (1-based)
+    ties: Optional["Ties"] = None             # tied interfaces (slave nodes follow master surfaces)
 
     @property
     def nn(self) -> int:
@@ -412,6 +424,199 @@ def bspline_box(p: int, n=(4, 4, 2), L=(4.0, 4.0, 2.0), origin=(0.0, 0.0, 0.0), 
     g = (p + 1,) * 3 if ngp is None else tuple(ngp)
     return Deck("bsp", coords, conn, np.full(ne, float(E)), np.full(ne, float(nu)), g, fixed,
                 matrix_type="sparse", patch=patch, nodal_f=nodal, title=f"bspline p={p} {n}")
+
+
+def hex_shape(kind: str, r: float, s: float, t: float) -> np.ndarray:
+    """hex8 / hex20 shape functions at (r, s, t) in FAST's local node order
+    (cShapeBrick8 / cShapeBrick20, shp/shpsolid.cpp:188-238, 329-433)."""
+    nat = KINDS[kind][1]
+    N = np.zeros(len(nat))
+    for a, (ri, si, ti) in enumerate(nat):
+        fr, fs, ft = 1 + ri * r, 1 + si * s, 1 + ti * t
+        if kind == "hex8":
+            N[a] = 0.125 * fr * fs * ft
+        elif ri and si and ti:
+            N[a] = 0.125 * fr * fs * ft * (ri * r + si * s + ti * t - 2.0)
+        elif ri == 0:
+            N[a] = 0.25 * (1 - r * r) * fs * ft
+        elif si == 0:
+            N[a] = 0.25 * fr * (1 - s * s) * ft
+        else:
+            N[a] = 0.25 * fr * fs * (1 - t * t)
+    return N
+
+
+def bspline_eval(U: np.ndarray, p: int, u: float):
+    """(first basis index, values, u-derivatives) of the p+1 B-splines that are
+    non-zero at u on the open knot vector U (Cox-de Boor recurrence)."""
+    U = np.asarray(U, dtype=np.float64)
+    nb = len(U) - p - 1
+    k = int(np.searchsorted(U, u, side="right")) - 1
+    k = min(max(k, p), nb - 1)
+
+    def table(q):
+        # degree-q functions N_{k-q..k}
+        N = np.array([1.0])
+        for d in range(1, q + 1):
+            M = np.zeros(d + 1)
+            for t in range(d + 1):
+                i = k - d + t
+                v = 0.0
+                if t >= 1 and U[i + d] > U[i]:
+                    v += (u - U[i]) / (U[i + d] - U[i]) * N[t - 1]
+                if t <= d - 1 and U[i + d + 1] > U[i + 1]:
+                    v += (U[i + d + 1] - u) / (U[i + d + 1] - U[i + 1]) * N[t]
+                M[t] = v
+            N = M
+        return N
+
+    N = table(p)
+    Nm = table(p - 1)
+    dN = np.zeros(p + 1)
+    for t in range(p + 1):
+        i = k - p + t
+        if t >= 1 and U[i + p] > U[i]:
+            dN[t] += p / (U[i + p] - U[i]) * Nm[t - 1]
+        if t <= p - 1 and U[i + p + 1] > U[i + 1]:
+            dN[t] -= p / (U[i + p + 1] - U[i + 1]) * Nm[t]
+    return k - p, N, dN
+
+
+def _hex_face_weights(kind, coords, conn, n, L, origin, pts, top):
+    """(masters, weights) of each point (x, y) on the z-top / z-bottom face of a
+    structured hex block made by box_mesh (its elements in (x, y, z) cells)."""
+    nx, ny, nz = n
+    # cell -> element: the element whose lower corner node sits at the cell corner
+    X = coords[conn]                       # [ne, nn, 3]
+    lo = X.min(axis=1)
+    h = np.array([L[0] / nx, L[1] / ny, L[2] / nz])
+    cell = np.rint((lo - np.asarray(origin)) / h).astype(np.int64)
+    lut = {tuple(c): e for e, c in enumerate(cell)}
+    res = []
+    for x, y in pts:
+        fx = (x - origin[0]) / h[0]
+        fy = (y - origin[1]) / h[1]
+        ix = min(max(int(np.floor(fx)), 0), nx - 1)
+        iy = min(max(int(np.floor(fy)), 0), ny - 1)
+        e = lut[(ix, iy, nz - 1 if top else 0)]
+        r, s_ = 2 * (fx - ix) - 1, 2 * (fy - iy) - 1
+        N = hex_shape(kind, r, s_, 1.0 if top else -1.0)
+        keep = np.abs(N) > 1e-14
+        res.append((conn[e][keep], N[keep]))
+    return res
+
+
+def _bsp_face_weights(deck, node_off, pts, top, tol=1e-13):
+    """(masters, weights) of each point (x, y) on the t = 1 (top) or t = 0
+    (bottom) surface of a B-spline block from bspline_box: the surface
+    parameters (u, v) of the point by Newton's method, then the tensor
+    products N_i(u) N_j(v) of the face's control points (unit weights)."""
+    P = deck.patch
+    p = P.degree
+    nb0, nb1, nb2 = P.grid
+    k = nb2 - 1 if top else 0
+    Xf = np.array([[deck.coords[node_off + P.cps[i + nb0 * j + nb0 * nb1 * k], :2]
+                    for i in range(nb0)] for j in range(nb1)])  # [j][i][2]
+    U, V = np.asarray(P.knots[0]), np.asarray(P.knots[1])
+    x0 = deck.coords[node_off + P.cps[0]]
+    span = np.ptp(deck.coords[node_off + P.cps], axis=0)
+    res = []
+    for x, y in pts:
+        u = U[-1] * (x - x0[0]) / span[0]
+        v = V[-1] * (y - x0[1]) / span[1]
+        for _ in range(50):
+            iu, Nu, dNu = bspline_eval(U, p[0], u)
+            iv, Nv, dNv = bspline_eval(V, p[1], v)
+            blk = Xf[iv:iv + p[1] + 1, iu:iu + p[0] + 1]        # [j][i][2]
+            pos = np.einsum("j,i,jic->c", Nv, Nu, blk)
+            Ju = np.einsum("j,i,jic->c", Nv, dNu, blk)
+            Jv = np.einsum("j,i,jic->c", dNv, Nu, blk)
+            J = np.stack([Ju, Jv], axis=1)
+            d = np.linalg.solve(J, np.array([x, y]) - pos)
+            u = min(max(u + d[0], U[0]), U[-1])
+            v = min(max(v + d[1], V[0]), V[-1])
+            if np.abs(d).max() < tol:
+                break
+        iu, Nu, _ = bspline_eval(U, p[0], u)
+        iv, Nv, _ = bspline_eval(V, p[1], v)
+        ms, ws = [], []
+        for j in range(p[1] + 1):
+            for i in range(p[0] + 1):
+                w = Nu[i] * Nv[j]
+                if abs(w) > 1e-14:
+                    ms.append(node_off + P.cps[(iu + i) + nb0 * (iv + j) + nb0 * nb1 * k])
+                    ws.append(w)
+        res.append((np.asarray(ms), np.asarray(ws)))
+    return res
+
+
+def tied_column(hex8=(40, 40, 20), hex20=(24, 24, 12), p2=(32, 32, 8), p3=(24, 24, 6), width=1.0, jitter=0.05,
+                seed=0, E=1000.0, nu=0.3, load=(0.0, 0.0, -1.0)) -> Deck:
+    """Four blocks on one width x width footprint, stacked in z and joined by
+    tied interfaces: a B-spline p=2 patch (bottom, clamped at z=0), a hex8 box,
+    a hex20 box and a B-spline p=3 patch (top, nodal forces summing to
+    ``load`` on its top control points).  Each block's height is its element
+    count in z times its element size.  Ties: the hex8 box's bottom nodes
+    follow the p=2 patch's top surface, its top nodes follow the hex20 box's
+    bottom faces, and the hex20 box's top nodes follow the p=3 patch's bottom
+    surface (slaves on the finer or interpolating side).  Control points are
+    jittered as in bspline_box; the hex boxes are regular."""
+    W = float(width)
+    z = 0.0
+    parts = []
+    # p=2 patch
+    hz = W / p2[0] * p2[2]
+    b2 = bspline_box(2, p2, L=(W, W, hz), origin=(0.0, 0.0, z), jitter=jitter, seed=seed, E=E, nu=nu,
+                     clamp_axis=2, load=(0.0, 0.0, 0.0))
+    parts.append(b2); z += hz
+    h8z = W / hex8[0] * hex8[2]
+    c8, k8, _ = box_mesh("hex8", hex8, (W, W, h8z), origin=(0.0, 0.0, z))
+    z8 = (z, z + h8z); z += h8z
+    h20z = W / hex20[0] * hex20[2]
+    c20, k20, _ = box_mesh("hex20", hex20, (W, W, h20z), origin=(0.0, 0.0, z))
+    z20 = (z, z + h20z); z += h20z
+    h3z = W / p3[0] * p3[2]
+    b3 = bspline_box(3, p3, L=(W, W, h3z), origin=(0.0, 0.0, z), jitter=jitter, seed=seed + 1, E=E, nu=nu,
+                     clamp_axis=2, load=load)
+    z += h3z
+    off = np.cumsum([0, b2.num_nodes, len(c8), len(c20), b3.num_nodes])
+    coords = np.concatenate([b2.coords, c8, c20, b3.coords])
+    nn = len(coords)
+    fixed = np.zeros((nn, 3), bool)
+    fixed[:b2.num_nodes] = b2.fixed          # p=2 patch: z = 0 face clamped
+    nodal = np.zeros((nn, 3))
+    far = np.isclose(b3.coords[:, 2], z)     # p=3 patch: load on its top face
+    nodal[off[3]:off[4]][far] = np.asarray(load, dtype=np.float64) / int(far.sum())
+
+    def sub(kind, conn, ngp, patch=None):
+        ne = len(conn)
+        return Deck(kind, coords, conn.astype(np.int32), np.full(ne, float(E)), np.full(ne, float(nu)), ngp,
+                    patch=patch)
+
+    p3patch = dataclasses.replace(b3.patch, cps=b3.patch.cps + off[3])
+    blocks = [sub("hex8", k8 + off[1], (2, 2, 2)), sub("hex20", k20 + off[2], (3, 3, 3)),
+              sub("bsp", b3.conn + off[3], (4, 4, 4), p3patch)]
+    main = Deck("bsp", coords, b2.conn.copy(), b2.E.copy(), b2.nu.copy(), (3, 3, 3), fixed, matrix_type="sparse",
+                patch=b2.patch, nodal_f=nodal, blocks=blocks, title="tied column")
+    # ties
+    slaves, masters, weights = [], [], []
+
+    def add(nodes, res):
+        for n_, (ms, ws) in zip(nodes, res):
+            slaves.append(int(n_)); masters.append(np.asarray(ms, dtype=np.int64)); weights.append(ws)
+
+    bot8 = off[1] + np.nonzero(np.isclose(c8[:, 2], z8[0]))[0]
+    add(bot8, _bsp_face_weights(main, 0, coords[bot8, :2], top=True))
+    top8 = off[1] + np.nonzero(np.isclose(c8[:, 2], z8[1]))[0]
+    add(top8, [(off[2] + ms, ws) for ms, ws in
+               _hex_face_weights("hex20", c20, k20, hex20, (W, W, h20z), (0.0, 0.0, z20[0]), coords[top8, :2], top=False)])
+    top20 = off[2] + np.nonzero(np.isclose(c20[:, 2], z20[1]))[0]
+    add(top20, _bsp_face_weights(dataclasses.replace(b3, coords=coords, patch=p3patch), 0, coords[top20, :2],
+                                 top=False))
+    ptr = np.concatenate([[0], np.cumsum([len(m) for m in masters])]).astype(np.int64)
+    main.ties = Ties(np.asarray(slaves, dtype=np.int64), ptr, np.concatenate(masters).astype(np.int64),
+                     np.concatenate(weights).astype(np.float64))
+    return main
 
 
 def nodal_load_vector(deck: Deck) -> np.ndarray:

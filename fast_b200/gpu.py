@@ -76,10 +76,17 @@ class Bucket(ctypes.Structure):
                 ("patch", ctypes.POINTER(Patch))]
 
 
+class Ties(ctypes.Structure):
+    _fields_ = [("num_slaves", ctypes.c_int64), ("slave", ctypes.POINTER(ctypes.c_int64)),
+                ("ptr", ctypes.POINTER(ctypes.c_int64)), ("master", ctypes.POINTER(ctypes.c_int64)),
+                ("weight", ctypes.POINTER(ctypes.c_double))]
+
+
 class Mesh(ctypes.Structure):
     _fields_ = [("num_nodes", ctypes.c_int64), ("coords", ctypes.POINTER(ctypes.c_double)),
                 ("node_eq", ctypes.POINTER(ctypes.c_int32)), ("num_eq", ctypes.c_int32),
-                ("num_buckets", ctypes.c_int32), ("buckets", ctypes.POINTER(Bucket))]
+                ("num_buckets", ctypes.c_int32), ("buckets", ctypes.POINTER(Bucket)),
+                ("ties", ctypes.POINTER(Ties))]
 
 
 class SolveOpts(ctypes.Structure):
@@ -286,7 +293,15 @@ def _mesh_struct(deck: _decks.Deck):
     keep = []
     bl = deck.buckets()
     buckets = (Bucket * len(bl))(*[_bucket_struct(b, keep) for b in bl])
-    m = Mesh(deck.num_nodes, _p(coords), _p(eq, _ip), int(eq.max(initial=0)), len(bl), buckets)
+    tp = ctypes.POINTER(Ties)()
+    if deck.ties is not None and len(deck.ties.slave):
+        t = deck.ties
+        arrs = [np.ascontiguousarray(a, dtype=np.int64) for a in (t.slave, t.ptr, t.master)]
+        w = np.ascontiguousarray(t.weight, dtype=np.float64)
+        ts = Ties(len(arrs[0]), _p(arrs[0], _lp), _p(arrs[1], _lp), _p(arrs[2], _lp), _p(w))
+        keep += [arrs, w, ts]
+        tp = ctypes.pointer(ts)
+    m = Mesh(deck.num_nodes, _p(coords), _p(eq, _ip), int(eq.max(initial=0)), len(bl), buckets, tp)
     return m, (coords, eq, keep, buckets)
 
 

@@ -109,6 +109,24 @@ typedef struct {
   const fast_gpu_patch *patch;  /* FAST_ELEM_BSP_SOLID: its patch; NULL otherwise  */
 } fast_gpu_bucket;
 
+/* Tied interfaces between non-matching meshes.  Each tie is the three linear
+ * constraints  u_s,i - sum_k w_k u_(m_k),i = 0  (i = x, y, z) of one slave node
+ * s on the surface of its master elements; in the reference they are
+ * %NODE.MULTI-POINT.CONSTRAINT equations (cNode::ReadNodeMPC, node/node.cpp:
+ * 459-509) solved with dense Lagrange multipliers by cSysMatrix::SolveMPC
+ * (mlib/sysmat.cpp:72-143).  Here the slave DOFs are eliminated: with u = T u~,
+ * the library assembles K~ = T^T K T directly into the node-block matrix and
+ * solves K~ u~ = T^T f; slave displacements are interpolated back.  A slave
+ * must not be a master, and its equations (if any) stay in the caller's
+ * numbering: loads on them are carried to the masters. */
+typedef struct {
+  int64_t        num_slaves;
+  const int64_t *slave;         /* [num_slaves] tied nodes (0-based, distinct)        */
+  const int64_t *ptr;           /* [num_slaves + 1] offsets into master / weight      */
+  const int64_t *master;        /* master nodes of each slave                         */
+  const double  *weight;        /* interpolation weights w_k                         */
+} fast_gpu_ties;
+
 typedef struct {
   int64_t                num_nodes;
   const double          *coords;    /* [num_nodes][3]                          */
@@ -116,6 +134,7 @@ typedef struct {
   int32_t                num_eq;
   int32_t                num_buckets;
   const fast_gpu_bucket *buckets;
+  const fast_gpu_ties   *ties;      /* NULL: no tied interfaces (linear statics only) */
 } fast_gpu_mesh;
 
 typedef struct {
