@@ -349,8 +349,13 @@ def tied_blocks(local, args):
     S.kernel_timing(False)
     a_ms /= max(1, a_n)
     runs = {}
-    for name, prec, tol in (("mixed", gpu.PREC_MIXED, 1e-8), ("fp64", gpu.PREC_FP64, 1e-8),
-                            ("fp64_1e-12", gpu.PREC_FP64, 1e-12)):
+    # the 84,647-node system iterates per kernel by default; the persistent
+    # cooperative iteration is also measured with its node limit raised
+    for name, prec, tol, persist in (("mixed", gpu.PREC_MIXED, 1e-8, 65536), ("fp64", gpu.PREC_FP64, 1e-8, 65536),
+                                     ("mixed_persistent", gpu.PREC_MIXED, 1e-8, 1 << 20),
+                                     ("fp64_persistent", gpu.PREC_FP64, 1e-8, 1 << 20),
+                                     ("fp64_1e-12", gpu.PREC_FP64, 1e-12, 65536)):
+        S.set_option(gpu.OPT_PERSISTENT_MAX_NODES, persist)
         best = None
         for _ in range(2 if name != "fp64_1e-12" else 1):
             t1 = time.perf_counter()
@@ -359,6 +364,7 @@ def tied_blocks(local, args):
             if best is None or dt < best[0]:
                 best = (dt, u, rep)
         runs[name] = best
+    S.set_option(gpu.OPT_PERSISTENT_MAX_NODES, 65536)
     clk = clocks.stop()
     u_ref = runs["fp64_1e-12"][1]
     err = {k: float(np.abs(v[1] - u_ref).max() / np.abs(u_ref).max()) for k, v in runs.items() if k != "fp64_1e-12"}

@@ -21,6 +21,7 @@
 // turned into the isotropic 3x3 block and added into K through the slot map
 // (elements of one colour share no node, so the adds need no atomics and K
 // is bit-identical from run to run).
+#include <algorithm>
 #include <cstdint>
 
 #include "elem_common.cuh"
@@ -39,8 +40,12 @@ struct BspSmem {
   static constexpr size_t bytes = doubles * sizeof(double) + NP * 2 + NN + 16;
 };
 
+// split > 1: `split` CTAs share one element, each taking every split-th block
+// of NT node pairs (they write disjoint blocks of K); the geometry is
+// recomputed by each.  Fills the GPU when a colour holds few elements (a
+// degree-3 patch needs 64 colours).
 template <int PR, int PS, int PT, int NG1, int NT>
-__global__ void __launch_bounds__(NT, 1) bsp_elem_kernel(ElemArgs A) {
+__global__ void __launch_bounds__(NT, 1) bsp_elem_kernel(ElemArgs A, int split) {
   using S = BspSmem<PR, PS, PT, NG1>;
   constexpr int QR = S::QR, QS = S::QS, QT = S::QT, NN = S::NN, NG = S::NG, NP = S::NP, ND = 3 * NN;
   extern __shared__ __align__(16) double sm[];
@@ -63,7 +68,9 @@ __global__ void __launch_bounds__(NT, 1) bsp_elem_kernel(ElemArgs A) {
   const double *__restrict__ gw = A.w;
   const bool rat = A.rational != 0;
 
-  for (int64_t it = blockIdx.x; it < A.ne; it += gridDim.x) {
+  for (int64_t wi = blockIdx.x; wi < A.ne * split; wi += gridDim.x) {
+    const int64_t it = wi / split;
+    const int part = (int)(wi - it * split);
     const int64_t e = A.index ? (int64_t)A.index[it] : A.offset + it;
     __syncthreads();
     const int32_t *en = A.conn + e * NN;
@@ -97,22 +104,34 @@ __global__ void __launch_bounds__(NT, 1) bsp_elem_kernel(ElemArgs A) {
         D[2 * NN + a] = fr[0] * fs[0] * ft[1];
       }
     }
+    constexpr int NW = NT / 32;
+    const int lane = tid & 31, warp = tid >> 5;
     if (rat) {
       __syncthreads();
-      // W and dW/dxi per Gauss point, summed in node order as the reference
-      for (int g = tid; g < NG; g += NT) {
+      // W and dW/dxi per Gauss point: one warp per point, lanes over the nodes
+      // (consecutive addresses), then a fixed butterfly
+      for (int g = warp; g < NG; g += NW) {
         const double *D = sD + g * ND;
         double w = 0.0, wr = 0.0, ws = 0.0, wt = 0.0;
-        for (int a = 0; a < NN; a++) {
+        for (int a = lane; a < NN; a += 32) {
           w += sB[g * NN + a];
           wr += D[a];
           ws += D[NN + a];
           wt += D[2 * NN + a];
         }
-        sWg[4 * g] = w;
-        sWg[4 * g + 1] = wr;
-        sWg[4 * g + 2] = ws;
-        sWg[4 * g + 3] = wt;
+#pragma unroll
+        for (int m = 16; m > 0; m >>= 1) {
+          w += __shfl_xor_sync(0xffffffffu, w, m);
+          wr += __shfl_xor_sync(0xffffffffu, wr, m);
+          ws += __shfl_xor_sync(0xffffffffu, ws, m);
+          wt += __shfl_xor_sync(0xffffffffu, wt, m);
+        }
+        if (lane == 0) {
+          sWg[4 * g] = w;
+          sWg[4 * g + 1] = wr;
+          sWg[4 * g + 2] = ws;
+          sWg[4 * g + 3] = wt;
+        }
       }
       __syncthreads();
       for (int t = tid; t < NG * NN; t += NT) {
@@ -127,13 +146,34 @@ __global__ void __launch_bounds__(NT, 1) bsp_elem_kernel(ElemArgs A) {
     }
     __syncthreads();
 
-    // Jacobians J[g][p][q] = sum_a dN_a/dxi_p X_a,q (cShapeSolid::DrvShpXYZ, shp/shpsolid.cpp:58-126)
-    for (int t = tid; t < NG * 9; t += NT) {
-      const int g = t / 9, pq = t - 9 * g, p = pq / 3, q = pq - 3 * p;
-      const double *d = sD + g * ND + p * NN;
-      double s = 0.0;
-      for (int a = 0; a < NN; a++) s += d[a] * sX[3 * a + q];
-      sJ[t] = s;
+    // Jacobians J[g][p][q] = sum_a dN_a/dxi_p X_a,q (cShapeSolid::DrvShpXYZ, shp/shpsolid.cpp:58-126):
+    // one warp per Gauss point, lanes over the nodes
+    for (int g = warp; g < NG; g += NW) {
+      const double *D = sD + g * ND;
+      double j[9];
+#pragma unroll
+      for (int k = 0; k < 9; k++) j[k] = 0.0;
+      for (int a = lane; a < NN; a += 32) {
+        const double x0 = sX[3 * a], x1 = sX[3 * a + 1], x2 = sX[3 * a + 2];
+#pragma unroll
+        for (int p = 0; p < 3; p++) {
+          const double d = D[p * NN + a];
+          j[3 * p] = fma(d, x0, j[3 * p]);
+          j[3 * p + 1] = fma(d, x1, j[3 * p + 1]);
+          j[3 * p + 2] = fma(d, x2, j[3 * p + 2]);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 9; k++)
+#pragma unroll
+        for (int m = 16; m > 0; m >>= 1) j[k] += __shfl_xor_sync(0xffffffffu, j[k], m);
+      if (lane < 9) {
+        double v = j[0];
+#pragma unroll
+        for (int k = 1; k < 9; k++)
+          if (lane == k) v = j[k];
+        sJ[9 * g + lane] = v;
+      }
     }
     __syncthreads();
     // determinant and inverse by cofactors (cShape::ShpMatInv, shp/shape.cpp:360-393)
@@ -142,7 +182,10 @@ __global__ void __launch_bounds__(NT, 1) bsp_elem_kernel(ElemArgs A) {
       const double j00 = J[0], j01 = J[1], j02 = J[2], j10 = J[3], j11 = J[4], j12 = J[5], j20 = J[6],
                    j21 = J[7], j22 = J[8];
       const double det = j00 * (j11 * j22 - j12 * j21) - j01 * (j10 * j22 - j12 * j20) + j02 * (j10 * j21 - j11 * j20);
-      if (!(det > 0.0)) atomicOr(A.status, 1);
+      // a B-spline patch may be parametrised left-handed: the reference keeps the
+      // signed determinant (and so a negative definite K and load); only a
+      // vanishing or non-finite Jacobian is an error here
+      if (!(fabs(det) > 0.0) || !isfinite(det)) atomicOr(A.status, 1);
       const double id = 1.0 / ((det != 0.0) ? det : 1.0);
       J[0] = (j11 * j22 - j12 * j21) * id;
       J[1] = -(j01 * j22 - j02 * j21) * id;
@@ -171,7 +214,7 @@ __global__ void __launch_bounds__(NT, 1) bsp_elem_kernel(ElemArgs A) {
     const double E = A.E[e], nu = A.nu[e];
     const double dd = (1.0 + nu) * (1.0 - 2.0 * nu);
     const double C00 = E * (1.0 - nu) / dd, C01 = E * nu / dd, G = 0.5 * E / (1.0 + nu);
-    for (int q = tid; q < NP; q += NT) {
+    for (int q = tid + part * NT; q < NP; q += NT * split) {
       const int pa = spair[2 * q], pb = spair[2 * q + 1];
       double M[9];
 #pragma unroll
@@ -231,10 +274,13 @@ static cudaError_t run_bsp(Ctx &c, ElemArgs a, int64_t count) {
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, S::bytes);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
-  int64_t grid = (int64_t)per_sm * c.sm_count;
-  if (grid > count) grid = count;
+  // as many CTAs per element as fit in one wave (a second, partial wave would
+  // double the launch time), at most one per block of NT node pairs
+  const int64_t slots = (int64_t)per_sm * c.sm_count;
+  int split = (int)std::min<int64_t>((S::NP + NT - 1) / NT, std::max<int64_t>(1, slots / count));
+  int64_t grid = std::min<int64_t>(slots, count * split);
   a.ne = count;
-  kern<<<(unsigned)grid, NT, S::bytes, c.stream>>>(a);
+  kern<<<(unsigned)grid, NT, S::bytes, c.stream>>>(a, split);
   c.launches++;
   return cudaGetLastError();
 }

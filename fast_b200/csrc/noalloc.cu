@@ -155,8 +155,9 @@ __global__ void __launch_bounds__(kNoAllocThreads) na_alpha(double *S) {
   __shared__ double sbuf[32];
   const double pw = na_sum_partials(S + kOffPart, sbuf);
   if (threadIdx.x == 0) {
-    if (!(pw > 0.0) || !isfinite(pw)) { st->done = 3; return; }
-    st->alpha = st->dot0 / pw;
+    const double al = st->dot0 / pw;
+    if (!(al > 0.0) || !isfinite(pw) || !isfinite(al)) { st->done = 3; return; }
+    st->alpha = al;
   }
 }
 

@@ -256,8 +256,12 @@ __global__ void __launch_bounds__(256) pcg_alpha(PcgState *st, const double *par
   const double pw = sum_partials(part, n, sbuf);
   if (threadIdx.x == 0) {
     st->pw = pw;
-    if (!(pw > 0.0) || !isfinite(pw)) { st->done = 3; return; }
-    st->alpha = st->dot0 / pw;
+    // breakdown unless alpha > 0: p.Kp and z.r of one sign (an SPD system, or a
+    // negative definite one such as the stiffness of a left-handed B-spline
+    // parametrisation, which the reference's signed det J produces)
+    const double al = st->dot0 / pw;
+    if (!(al > 0.0) || !isfinite(pw) || !isfinite(al)) { st->done = 3; return; }
+    st->alpha = al;
   }
 }
 
@@ -868,8 +872,8 @@ pcg_persistent(int64_t nnode, const int32_t *__restrict__ srow, const int32_t *_
     if (tid == 0) part_pw[b] = t;
     if (!grid_barrier(bar, &ok_sh)) { done = kDoneBarrierTimeout; break; }
     pw = persist_sum(part_pw, G, sbuf, &bc);
-    if (!(pw > 0.0) || !isfinite(pw)) { done = 3; break; }
     alpha = dot0 / pw;
+    if (!(alpha > 0.0) || !isfinite(pw) || !isfinite(alpha)) { done = 3; break; }
     // u += alpha p; r -= alpha w; z = Dinv r; partials r.r, z.r
     const T al = (T)alpha;
     double rra = 0.0, zra = 0.0;
@@ -1060,8 +1064,8 @@ pcg_batch(const int32_t *__restrict__ order, const int64_t *__restrict__ noff, c
     double dot0 = csum(zr);  // its cluster barrier also publishes p
     while (!done && it < maxit) {
       const double pw = spmv(p, nullptr, w);
-      if (!(pw > 0.0) || !isfinite(pw)) { done = 3; break; }
       const double alpha = dot0 / pw;
+      if (!(alpha > 0.0) || !isfinite(pw) || !isfinite(alpha)) { done = 3; break; }
       double rra = 0.0, zra = 0.0;
       for (int64_t n = n0 + tid; n < n1; n += kBatchThreads) {
         double u0, u1, u2, p0, p1, p2, r0, r1, r2, w0, w1, w2, z0, z1, z2;

@@ -30,18 +30,26 @@ namespace fastgpu {
 
 namespace {
 
+// STAGE: the element matrix is first copied to shared memory (when it fits)
+template <bool STAGE>
 __global__ void tied_scatter(int64_t first, int64_t count, const int64_t *__restrict__ nptr,
                              const int32_t *__restrict__ nodes, const int64_t *__restrict__ sptr,
                              const int32_t *__restrict__ slot, const int64_t *__restrict__ pptr,
                              const int32_t *__restrict__ pa, const double *__restrict__ pt,
                              const int64_t *__restrict__ keoff, const int32_t *__restrict__ nn_of,
                              const double *__restrict__ ke, const uint8_t *__restrict__ fix, double *__restrict__ K) {
+  extern __shared__ double sKe[];
   for (int64_t it = blockIdx.x; it < count; it += gridDim.x) {
     const int64_t x = first + it;
     const int64_t n0 = nptr[x];
     const int m = (int)(nptr[x + 1] - n0);
     const int nd = 3 * nn_of[x];
     const double *Ke = ke + keoff[x];
+    if (STAGE) {
+      for (int i = threadIdx.x; i < nd * nd; i += blockDim.x) sKe[i] = Ke[i];
+      __syncthreads();
+      Ke = sKe;
+    }
     const int32_t *sl = slot + sptr[x];
     for (int q = threadIdx.x; q < m * m; q += blockDim.x) {
       const int A = q / m, B = q - A * m;
@@ -215,8 +223,18 @@ cudaError_t launch_tied_assemble(Ctx &c, double *K) {
     const int64_t first = T.color_off[k], cnt = T.color_off[k + 1] - first;
     if (cnt <= 0) continue;
     const unsigned grid = (unsigned)std::min<int64_t>(cnt, 4LL * c.sm_count);
-    tied_scatter<<<grid, 256, 0, c.stream>>>(first, cnt, T.d_nptr, T.d_nodes, T.d_sptr, T.d_slot, T.d_pptr, T.d_pa,
-                                             T.d_pt, T.d_keoff, T.d_nn, T.d_ke, c.d_fix, K);
+    int maxnn = 0;
+    for (int32_t v : T.h_nn) maxnn = std::max(maxnn, v);
+    const size_t smem = sizeof(double) * 9 * maxnn * maxnn;
+    if (smem <= 96 * 1024) {
+      e = cudaFuncSetAttribute(tied_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      tied_scatter<true><<<grid, 256, smem, c.stream>>>(first, cnt, T.d_nptr, T.d_nodes, T.d_sptr, T.d_slot, T.d_pptr,
+                                                        T.d_pa, T.d_pt, T.d_keoff, T.d_nn, T.d_ke, c.d_fix, K);
+    } else {
+      tied_scatter<false><<<grid, 256, 0, c.stream>>>(first, cnt, T.d_nptr, T.d_nodes, T.d_sptr, T.d_slot, T.d_pptr,
+                                                      T.d_pa, T.d_pt, T.d_keoff, T.d_nn, T.d_ke, c.d_fix, K);
+    }
     c.launches++;
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;

@@ -5,6 +5,8 @@ under ncu (each one GPU, a few hundred MB at most):
     python -m fast_b200.profile_cases mlp_grad      # tcgen05 BF16 GEMMs: MLP forward + backward,
                                                     #   batch 2496, 129 -> 256 -> 256 -> 32
     python -m fast_b200.profile_cases box N         # hex20 box N x N x N/2: assemble + mixed solve
+    python -m fast_b200.profile_cases tied          # tied four-block column (B-spline p=2, hex8, hex20,
+                                                    #   B-spline p=3): two assemblies
 
 Each prints one line of results; none measures anything itself.
 """
@@ -50,12 +52,24 @@ def box(n):
     print("box", n, r)
 
 
+def tied():
+    d = decks.tied_column()
+    s = gpu.GpuSystem(0)
+    s.upload(d)
+    for _ in range(2):
+        s.assemble()
+    s.synchronize()
+    print("tied", d.num_eq())
+
+
 if __name__ == "__main__":
     case = sys.argv[1] if len(sys.argv) > 1 else "plate_solve"
     if case == "plate_solve":
         plate_solve()
     elif case == "mlp_grad":
         mlp_grad()
+    elif case == "tied":
+        tied()
     elif case == "box":
         box(int(sys.argv[2]) if len(sys.argv) > 2 else 40)
     else:
