@@ -216,6 +216,20 @@ __global__ void __launch_bounds__(NT, 1) bsp_elem_kernel(ElemArgs A, int split) 
     const double C00 = E * (1.0 - nu) / dd, C01 = E * nu / dd, G = 0.5 * E / (1.0 + nu);
     for (int q = tid + part * NT; q < NP; q += NT * split) {
       const int pa = spair[2 * q], pb = spair[2 * q + 1];
+      // the pair's two K blocks are loaded before its Gauss-point sum, so the
+      // read latency overlaps the arithmetic
+      double *Kab = nullptr, *Kba = nullptr;
+      double oab[9], oba[9];
+      if (A.K) {
+        Kab = A.K + (int64_t)A.slot[(e * NN + pa) * NN + pb] * 9;
+        Kba = pa != pb ? A.K + (int64_t)A.slot[(e * NN + pb) * NN + pa] * 9 : nullptr;
+#pragma unroll
+        for (int k = 0; k < 9; k++) oab[k] = Kab[k];
+        if (Kba) {
+#pragma unroll
+          for (int k = 0; k < 9; k++) oba[k] = Kba[k];
+        }
+      }
       double M[9];
 #pragma unroll
       for (int k = 0; k < 9; k++) M[k] = 0.0;
@@ -247,16 +261,14 @@ __global__ void __launch_bounds__(NT, 1) bsp_elem_kernel(ElemArgs A, int split) 
           }
       }
       if (A.K) {
-        double *Kab = A.K + (int64_t)A.slot[(e * NN + pa) * NN + pb] * 9;
-        double *Kba = pa != pb ? A.K + (int64_t)A.slot[(e * NN + pb) * NN + pa] * 9 : nullptr;
         const uint8_t fa = sfix[pa], fb = sfix[pb];
 #pragma unroll
         for (int i = 0; i < 3; i++)
 #pragma unroll
           for (int j = 0; j < 3; j++)
             if (!((fa >> i) & 1) && !((fb >> j) & 1)) {
-              Kab[3 * i + j] += v[3 * i + j];
-              if (Kba) Kba[3 * j + i] += v[3 * i + j];
+              Kab[3 * i + j] = oab[3 * i + j] + v[3 * i + j];
+              if (Kba) Kba[3 * j + i] = oba[3 * j + i] + v[3 * i + j];
             }
       }
     }
@@ -300,8 +312,8 @@ cudaError_t launch_bsp_elements(Ctx &c, const Bucket &B, ElemArgs a, int64_t cou
   const int *p = B.pd;
   if (p[0] == 2 && p[1] == 2 && p[2] == 2 && ng == 3) return run_bsp<2, 2, 2, 3, 384>(c, a, count);
   if (p[0] == 2 && p[1] == 2 && p[2] == 2 && ng == 4) return run_bsp<2, 2, 2, 4, 384>(c, a, count);
-  if (p[0] == 3 && p[1] == 3 && p[2] == 3 && ng == 4) return run_bsp<3, 3, 3, 4, 512>(c, a, count);
-  if (p[0] == 3 && p[1] == 3 && p[2] == 2 && ng == 4) return run_bsp<3, 3, 2, 4, 512>(c, a, count);
+  if (p[0] == 3 && p[1] == 3 && p[2] == 3 && ng == 4) return run_bsp<3, 3, 3, 4, 384>(c, a, count);
+  if (p[0] == 3 && p[1] == 3 && p[2] == 2 && ng == 4) return run_bsp<3, 3, 2, 4, 384>(c, a, count);
   return cudaErrorInvalidValue;
 }
 
