@@ -338,6 +338,7 @@ def tied_blocks(local, args):
     setup_s = time.perf_counter() - t0
     pinfo = S.pattern_info()
     S.assemble()
+    tune = S.autotune()
     S.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
@@ -351,10 +352,11 @@ def tied_blocks(local, args):
     runs = {}
     # the 84,647-node system iterates per kernel by default; the persistent
     # cooperative iteration is also measured with its node limit raised
-    for name, prec, tol, persist in (("mixed", gpu.PREC_MIXED, 1e-8, 65536), ("fp64", gpu.PREC_FP64, 1e-8, 65536),
+    tuned = tune["persistent_max_nodes"]
+    for name, prec, tol, persist in (("mixed", gpu.PREC_MIXED, 1e-8, tuned), ("fp64", gpu.PREC_FP64, 1e-8, tuned),
                                      ("mixed_persistent", gpu.PREC_MIXED, 1e-8, 1 << 20),
                                      ("fp64_persistent", gpu.PREC_FP64, 1e-8, 1 << 20),
-                                     ("fp64_1e-12", gpu.PREC_FP64, 1e-12, 65536)):
+                                     ("fp64_1e-12", gpu.PREC_FP64, 1e-12, tuned)):
         S.set_option(gpu.OPT_PERSISTENT_MAX_NODES, persist)
         best = None
         for _ in range(2 if name != "fp64_1e-12" else 1):
@@ -364,7 +366,7 @@ def tied_blocks(local, args):
             if best is None or dt < best[0]:
                 best = (dt, u, rep)
         runs[name] = best
-    S.set_option(gpu.OPT_PERSISTENT_MAX_NODES, 65536)
+    S.set_option(gpu.OPT_PERSISTENT_MAX_NODES, tuned)
     clk = clocks.stop()
     u_ref = runs["fp64_1e-12"][1]
     err = {k: float(np.abs(v[1] - u_ref).max() / np.abs(u_ref).max()) for k, v in runs.items() if k != "fp64_1e-12"}
@@ -378,6 +380,7 @@ def tied_blocks(local, args):
                     "on the p=3 patch's top control points; non-matching interfaces tied (slave DOFs eliminated)",
         "elements": kinds, "nodes": int(d.num_nodes), "equations": int(d.num_eq()),
         "tied_slave_nodes": int(len(d.ties.slave)), "pattern": pinfo, "generate_s": gen_s, "setup_s": setup_s,
+        "autotune": tune,
         "assembly": {"ms": a_ms, "launches_timed": int(a_n), "elements_per_s": sum(kinds.values()) / (a_ms / 1e3),
                      "algorithmic_bytes": a_bytes, "GB_per_s": a_bytes / (a_ms / 1e3) / 1e9,
                      "frac": a_bytes / (a_ms / 1e3) / 1e9 / hbm},
@@ -471,6 +474,9 @@ def run_ours(args):
         S.assemble()
         return S.solve_device(d_f.data_ptr(), d_u.data_ptr(), tol=TOL, precision=precision, precond=precond)
 
+    # launch shapes measured on this system before the warm-up (untimed)
+    S.assemble()
+    tune = S.autotune()
     for _ in range(args.warmup):
         rep = step()
 
@@ -632,6 +638,7 @@ def run_ours(args):
             "assembly": {"ms": a_ms, "launches_timed": a_n, "elements_per_s": deck.num_elems / (a_ms / 1e3),
                          "algorithmic_bytes": a_bytes, "GB_per_s": a_gbs, "frac": a_gbs / hbm},
             "pattern": {**pinfo, "setup_s": setup_s},
+            "autotune": tune,
             "tied_blocks": cfg2,
             "newton_plate": plate,
             "ensemble_and_dynamics": cfg4,

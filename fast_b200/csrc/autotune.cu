@@ -1,0 +1,111 @@
+// autotune.cu - launch shapes chosen by measurement on the system at hand
+// (fast_gpu_autotune; no reference counterpart).
+//
+// What is tuned, and why it is worth measuring:
+//   * lanes per block-row of the FP32 and FP64 SpMV: the best split of a row's
+//     blocks over lanes depends on the row length (27 blocks for hex8 meshes,
+//     ~57 for hex20, ~125 for degree-3 B-spline patches) and on how many rows a
+//     warp then covers;
+//   * the PCG iteration path: one persistent cooperative kernel per chunk
+//     (latency-bound small systems) or a CUDA graph of kernels (bandwidth-
+//     bound large ones).  The crossover depends on the system, so both are
+//     timed on the same 64 FP64 iterations.
+// The choices become the context's options (fast_gpu_set_option); the caller
+// may cache them per device and mesh type.
+#include <algorithm>
+#include <functional>
+#include <vector>
+
+#include "internal.h"
+
+using namespace fastgpu;
+
+struct fast_gpu_ctx : public Ctx {};
+
+namespace {
+
+// median over `reps` launches, each bracketed by events on the context stream
+cudaError_t median_ms(Ctx &c, const std::function<cudaError_t()> &launch, int reps, double &ms) {
+  cudaEvent_t a, b;
+  cudaError_t e = cudaEventCreate(&a);
+  if (e == cudaSuccess) e = cudaEventCreate(&b);
+  std::vector<double> t;
+  for (int r = 0; r < reps + 1 && e == cudaSuccess; r++) {  // the first launch warms up
+    e = cudaEventRecord(a, c.stream);
+    if (e == cudaSuccess) e = launch();
+    if (e == cudaSuccess) e = cudaEventRecord(b, c.stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(b);
+    float f = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&f, a, b);
+    if (e == cudaSuccess && r > 0) t.push_back(f);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (e != cudaSuccess) return e;
+  std::sort(t.begin(), t.end());
+  ms = t[t.size() / 2];
+  return cudaSuccess;
+}
+
+}  // namespace
+
+#define ATK(call)                                                                     \
+  do {                                                                                \
+    cudaError_t _e = (call);                                                          \
+    if (_e != cudaSuccess) {                                                          \
+      c->err = std::string("autotune: ") + #call + ": " + cudaGetErrorString(_e);    \
+      return FAST_GPU_ECUDA;                                                          \
+    }                                                                                 \
+  } while (0)
+
+extern "C" int fast_gpu_autotune(fast_gpu_ctx *c, fast_gpu_tune_report *rep) {
+  if (!c || !rep) return FAST_GPU_EINVAL;
+  if (!c->K_ok) { c->err = "autotune: matrix not assembled"; return FAST_GPU_ESTATE; }
+  fast_gpu_tune_report R{};
+  ATK(solve_layout(*c, FAST_ASM_STIFFNESS, true));
+  const size_t n4 = 4 * (size_t)c->nnode;
+  ATK(cudaMemsetAsync(c->d_p, 0x3F, sizeof(double) * n4, c->stream));  // any finite vector
+  ATK(cudaMemsetAsync(c->s_p, 0x3F, sizeof(float) * n4, c->stream));
+  const int lanes[4] = {4, 8, 16, 32};
+  int best32 = c->lpr32, best64 = c->lpr64;
+  double b32 = 1e300, b64 = 1e300;
+  for (int i = 0; i < 4; i++) {
+    c->lpr32 = c->lpr64 = lanes[i];
+    ATK(median_ms(*c, [&] { return launch_spmv32(*c, c->d_Ks32, c->s_p, c->s_w); }, 9, R.ms_fp32[i]));
+    ATK(median_ms(*c, [&] { return launch_spmv(*c, c->d_Ks, c->d_p, c->d_w); }, 9, R.ms_fp64[i]));
+    if (R.ms_fp32[i] < b32) { b32 = R.ms_fp32[i]; best32 = lanes[i]; }
+    if (R.ms_fp64[i] < b64) { b64 = R.ms_fp64[i]; best64 = lanes[i]; }
+  }
+  c->lpr32 = best32;
+  c->lpr64 = best64;
+  c->drop_graphs();
+  R.lanes_fp32 = best32;
+  R.lanes_fp64 = best64;
+
+  // PCG path: both timed on 64 FP64 iterations with a dummy load (tol 0 never
+  // stops early), for systems within reach of one co-resident grid
+  R.persistent_max_nodes = c->persist_max_nodes;
+  const int64_t saved = c->persist_max_nodes;
+  int coop = 0;
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device);
+  if (coop && c->nnode <= (int64_t)1 << 20) {
+    if (c->precond_built != FAST_PRECOND_JACOBI) ATK(launch_build_precond(*c, c->d_K, FAST_PRECOND_JACOBI));
+    ATK(cudaMemsetAsync(c->d_f, 0x3F, sizeof(double) * n4, c->stream));
+    constexpr int kIt = 64;
+    double ms_p = 0.0, ms_k = 0.0;
+    c->persist_max_nodes = (int64_t)1 << 40;
+    ATK(median_ms(*c, [&] { return pcg_fp64(*c, false, 0.0, kIt, kIt); }, 3, ms_p));
+    c->persist_max_nodes = 0;
+    ATK(median_ms(*c, [&] { return pcg_fp64(*c, false, 0.0, kIt, kIt); }, 3, ms_k));
+    R.us_iter_persistent = ms_p * 1e3 / kIt;
+    R.us_iter_kernels = ms_k * 1e3 / kIt;
+    c->persist_max_nodes = (ms_p < ms_k) ? std::max<int64_t>(saved, c->nnode) : std::min<int64_t>(saved, c->nnode - 1);
+    R.persistent_max_nodes = c->persist_max_nodes;
+    c->drop_graphs();
+  }
+  ATK(cudaMemsetAsync(c->d_p, 0, sizeof(double) * n4, c->stream));
+  ATK(cudaMemsetAsync(c->s_p, 0, sizeof(float) * n4, c->stream));
+  ATK(cudaStreamSynchronize(c->stream));
+  *rep = R;
+  return FAST_GPU_OK;
+}

@@ -175,6 +175,13 @@ int fast_gpu_set_option(fast_gpu_ctx *c, int32_t option, int64_t value) {
     c->persist_max_nodes = coop ? value : 0;
     return FAST_GPU_OK;
   }
+  if (option == FAST_OPT_SPMV_LANES_FP32 || option == FAST_OPT_SPMV_LANES_FP64) {
+    if (value != 4 && value != 8 && value != 16 && value != 32) return FAST_GPU_EINVAL;
+    CK(cudaStreamSynchronize(c->stream));
+    c->drop_graphs();  // captured iterations hold the old launch shape
+    (option == FAST_OPT_SPMV_LANES_FP32 ? c->lpr32 : c->lpr64) = (int)value;
+    return FAST_GPU_OK;
+  }
   return FAST_GPU_EINVAL;
 }
 

@@ -185,6 +185,10 @@ struct Ctx {
   // persistent PCG: systems with at most persist_max_nodes nodes run each
   // chunk of iterations as one cooperative kernel (grid barriers in d_bar)
   int64_t persist_max_nodes = 65536;
+  // SpMV lanes per block-row (4, 8, 16 or 32): FP32 takes 4 blocks and FP64 2
+  // blocks per lane trip; defaults measured best on a hex20 box (64 blocks per
+  // padded row), fast_gpu_autotune measures them on the system at hand
+  int lpr32 = 8, lpr64 = 16;
   int persist_grid = 0;           // blocks of that kernel (0: not yet sized)
   void *d_bar = nullptr;          // grid barrier words (kBarrierBytes)
   static constexpr size_t kBarrierBytes = 8192;

@@ -42,8 +42,6 @@ namespace fastgpu {
 
 constexpr int kSpmvThreads = 256;
 constexpr int kVecThreads = 256;
-constexpr int kLPR32 = 8;   // lanes per block-row, FP32 SpMV (4 blocks per lane trip; 8 measured 7 % faster than 16 or 4)
-constexpr int kLPR64 = 16;  // lanes per block-row, FP64 SpMV (2 blocks per lane trip; 16 measured faster than 8 or 4)
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -599,6 +597,27 @@ static double *P_C(Ctx &c) { return c.d_partials + 4096; }    // [R]  z.r
 static double *P_D(Ctx &c) { return c.d_partials + 6144; }    // [R]  f.f
 static double *P_E(Ctx &c) { return c.d_partials + 8192; }    // [G]  true r.r
 
+// lanes per block-row chosen at run time (fast_gpu_set_option / fast_gpu_autotune)
+template <int MODE>
+static void spmv64_go(const Ctx &c, int G, int64_t nn, const double *Ks, const double *x, const double *b, double *y,
+                      double *part, const int32_t *skip) {
+  switch (c.lpr64) {
+    case 4: spmv_f64<MODE, 4><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, Ks, x, b, y, part, skip); break;
+    case 8: spmv_f64<MODE, 8><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, Ks, x, b, y, part, skip); break;
+    case 32: spmv_f64<MODE, 32><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, Ks, x, b, y, part, skip); break;
+    default: spmv_f64<MODE, 16><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, Ks, x, b, y, part, skip);
+  }
+}
+static void spmv32_go(const Ctx &c, int G, int64_t nn, const float *Ks, const float *x, float *y, double *part,
+                      const int32_t *skip) {
+  switch (c.lpr32) {
+    case 4: spmv_f32<0, 4><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, Ks, x, nullptr, y, part, skip); break;
+    case 16: spmv_f32<0, 16><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, Ks, x, nullptr, y, part, skip); break;
+    case 32: spmv_f32<0, 32><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, Ks, x, nullptr, y, part, skip); break;
+    default: spmv_f32<0, 8><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, Ks, x, nullptr, y, part, skip);
+  }
+}
+
 cudaError_t launch_to_soa(Ctx &c, const double *K, double *Ks, float *Ks32) {
   aos_to_soa<<<spmv_grid(c), 256, 0, c.stream>>>(c.nnode, c.d_rowptr, c.d_srow, K, Ks, Ks32);
   c.launches++;
@@ -606,23 +625,20 @@ cudaError_t launch_to_soa(Ctx &c, const double *K, double *Ks, float *Ks32) {
 }
 
 cudaError_t launch_spmv(Ctx &c, const double *Ks, const double *x, double *y) {
-  spmv_f64<0, kLPR64><<<spmv_grid(c), kSpmvThreads, 0, c.stream>>>(
-      c.nnode, c.d_srow, c.d_scol, Ks, x, nullptr, y, nullptr, nullptr);
+  spmv64_go<0>(c, spmv_grid(c), c.nnode, Ks, x, nullptr, y, nullptr, nullptr);
   c.launches++;
   return cudaGetLastError();
 }
 
 cudaError_t launch_spmv32(Ctx &c, const float *Ks, const float *x, float *y) {
-  spmv_f32<0, kLPR32><<<spmv_grid(c), kSpmvThreads, 0, c.stream>>>(
-      c.nnode, c.d_srow, c.d_scol, Ks, x, nullptr, y, nullptr, nullptr);
+  spmv32_go(c, spmv_grid(c), c.nnode, Ks, x, y, nullptr, nullptr);
   c.launches++;
   return cudaGetLastError();
 }
 
 cudaError_t launch_residual(Ctx &c, const double *Ks, const double *f, const double *u, double *r, double *rr_out) {
   double *part = P_E(c);
-  spmv_f64<1, kLPR64><<<spmv_grid(c), kSpmvThreads, 0, c.stream>>>(
-      c.nnode, c.d_srow, c.d_scol, Ks, u, f, r, part, nullptr);
+  spmv64_go<1>(c, spmv_grid(c), c.nnode, Ks, u, f, r, part, nullptr);
   c.launches++;
   finish_sum<<<1, 256, 0, c.stream>>>(part, spmv_grid(c), rr_out);
   c.launches++;
@@ -1225,8 +1241,7 @@ cudaError_t pcg_fp64(Ctx &c, bool warm, double tol, int maxit, int chunk, int it
   PcgState *st = c.d_state;
   cudaError_t e;
   if (warm) {
-    spmv_f64<1, kLPR64><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, c.d_Ks, c.d_u, c.d_f,
-                                                                   c.d_r, P_E(c), nullptr);
+    spmv64_go<1>(c, G, nn, c.d_Ks, c.d_u, c.d_f, c.d_r, P_E(c), nullptr);
     c.launches++;
   } else {
     cudaMemsetAsync(c.d_u, 0, sizeof(double) * 4 * nn, c.stream);
@@ -1246,8 +1261,7 @@ cudaError_t pcg_fp64(Ctx &c, bool warm, double tol, int maxit, int chunk, int it
   return drive(c, maxit, chunk, &c.graph_fp64, &c.graph_fp64_chunk, &c.graph_fp64_kernels, [&](int k) -> cudaError_t {
     for (int i = 0; i < k; i++) {
       c.begin_span(0);
-      spmv_f64<0, kLPR64><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, c.d_Ks, c.d_p, nullptr,
-                                                                     c.d_w, P_A(c), &st->done);
+      spmv64_go<0>(c, G, nn, c.d_Ks, c.d_p, nullptr, c.d_w, P_A(c), &st->done);
       c.end_span();
       pcg_alpha<<<1, 256, 0, c.stream>>>(st, P_A(c), G);
       pcg_update<double><<<R, kVecThreads, 0, c.stream>>>(nn, c.d_u, c.d_r, c.d_z, c.d_p, c.d_w, c.d_dinv, st,
@@ -1274,8 +1288,7 @@ cudaError_t pcg_mixed(Ctx &c, bool warm, double tol, int maxit, int chunk) {
   auto reliable = [&]() {
     flush_correction<<<R, 256, 0, c.stream>>>(4 * nn, c.d_u, c.s_x, st);
     c.begin_span(0);
-    spmv_f64<1, kLPR64><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, c.d_Ks, c.d_u, c.d_f,
-                                                                   c.d_r, P_E(c), &st->final);
+    spmv64_go<1>(c, G, nn, c.d_Ks, c.d_u, c.d_f, c.d_r, P_E(c), &st->final);
     c.end_span();
     replace_residual<<<R, kVecThreads, 0, c.stream>>>(nn, c.d_r, c.s_r, c.s_z, c.s_p, c.s_dinv, st, P_C(c));
     reliable_scalar<<<1, 256, 0, c.stream>>>(st, P_E(c), G, P_C(c), R);
@@ -1296,8 +1309,7 @@ cudaError_t pcg_mixed(Ctx &c, bool warm, double tol, int maxit, int chunk) {
                [&](int k) -> cudaError_t {
     for (int i = 0; i < k; i++) {
       c.begin_span(1);
-      spmv_f32<0, kLPR32><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, c.d_Ks32, c.s_p, nullptr,
-                                                                   c.s_w, P_A(c), &st->done);
+      spmv32_go(c, G, nn, c.d_Ks32, c.s_p, c.s_w, P_A(c), &st->done);
       c.end_span();
       pcg_alpha<<<1, 256, 0, c.stream>>>(st, P_A(c), G);
       pcg_update<float><<<R, kVecThreads, 0, c.stream>>>(nn, c.s_x, c.s_r, c.s_z, c.s_p, c.s_w, c.s_dinv, st,

@@ -45,12 +45,12 @@ EXPORTS = [
     "fast_gpu_inspect_pattern", "fast_gpu_pcg_solve_noalloc", "fast_gpu_set_displacement",
     "fast_gpu_set_displacement_device", "fast_gpu_internal_force", "fast_gpu_internal_force_device",
     "fast_gpu_nr_solve", "fast_gpu_ws_create", "fast_gpu_ws_destroy", "fast_gpu_ws_add_trajectory",
-    "fast_gpu_ws_build_basis", "fast_gpu_ws_train", "fast_gpu_ws_predict", "fast_gpu_ws_report",
+    "fast_gpu_ws_build_basis", "fast_gpu_ws_train", "fast_gpu_ws_predict", "fast_gpu_ws_report", "fast_gpu_autotune",
     "fast_gpu_ws_get_basis", "fast_gpu_ws_get_samples", "fast_gpu_mlp_params", "fast_gpu_mlp_forward",
     "fast_gpu_mlp_loss_grad", "fast_gpu_mlp_gemm", "fast_gpu_ws_configure", "fast_gpu_ws_last_input",
     "fast_gpu_set_option", "fast_gpu_set_problems", "fast_gpu_solve_batch", "fast_gpu_newmark",
 ]
-OPT_PERSISTENT_MAX_NODES = 1
+OPT_PERSISTENT_MAX_NODES, OPT_SPMV_LANES_FP32, OPT_SPMV_LANES_FP64 = 1, 2, 3
 KERNEL_SPMV_FP64, KERNEL_SPMV_FP32, KERNEL_ASSEMBLE = 0, 1, 2
 KERNEL_PREDICT_NET, KERNEL_PREDICT_GALERKIN, KERNEL_INTERNAL_FORCE, KERNEL_LINEAR_SOLVE = 3, 4, 5, 6
 
@@ -144,6 +144,18 @@ class NewmarkReport(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class TuneReport(ctypes.Structure):
+    _fields_ = [("lanes_fp32", ctypes.c_int32), ("lanes_fp64", ctypes.c_int32), ("ms_fp32", ctypes.c_double * 4),
+                ("ms_fp64", ctypes.c_double * 4), ("persistent_max_nodes", ctypes.c_int64),
+                ("us_iter_persistent", ctypes.c_double), ("us_iter_kernels", ctypes.c_double)]
+
+    def as_dict(self):
+        return {"lanes_fp32": self.lanes_fp32, "lanes_fp64": self.lanes_fp64,
+                "ms_fp32_lanes_4_8_16_32": list(self.ms_fp32), "ms_fp64_lanes_4_8_16_32": list(self.ms_fp64),
+                "persistent_max_nodes": self.persistent_max_nodes, "us_iter_persistent": self.us_iter_persistent,
+                "us_iter_kernels": self.us_iter_kernels}
+
+
 class ProblemReport(ctypes.Structure):
     _fields_ = [("converged", ctypes.c_int32), ("iterations", ctypes.c_int32), ("rel_residual", ctypes.c_double)]
 
@@ -189,6 +201,7 @@ def load_library(path: str = LIB_PATH):
     L.fast_gpu_set_stream.argtypes = [vp, vp]
     L.fast_gpu_synchronize.argtypes = [vp]
     L.fast_gpu_set_option.argtypes = [vp, ctypes.c_int32, ctypes.c_int64]
+    L.fast_gpu_autotune.argtypes = [vp, vp]
     L.fast_gpu_set_problems.argtypes = [vp, ctypes.c_int32, _lp]
     L.fast_gpu_newmark.argtypes = [vp, _dp, ctypes.POINTER(NewmarkOpts), _dp, _dp, _dp, ctypes.c_int32, _ip, _dp,
                                    ctypes.POINTER(NewmarkReport)]
@@ -392,6 +405,13 @@ class GpuSystem:
         its = np.array([r.iterations for r in reps], np.int32)
         res = np.array([r.rel_residual for r in reps])
         return u, conv, its, res
+
+    def autotune(self) -> dict:
+        """Measure the SpMV lanes-per-row choices and the PCG iteration path on
+        this (assembled) system and keep the fastest (fast_gpu_autotune)."""
+        r = TuneReport()
+        self._ck(self.L.fast_gpu_autotune(self.ctx, ctypes.byref(r)), "autotune")
+        return r.as_dict()
 
     def set_option(self, option: int, value: int):
         self._ck(self.L.fast_gpu_set_option(self.ctx, int(option), int(value)), "set_option")

@@ -171,7 +171,23 @@ int         fast_gpu_synchronize(fast_gpu_ctx *ctx);
                                             of iterations as one persistent cooperative kernel (grid
                                             barriers instead of kernel boundaries); default 65536,
                                             0 = always one kernel per step of the iteration */
+#define FAST_OPT_SPMV_LANES_FP32      2  /* lanes per block-row of the FP32 SpMV: 4, 8 (default), 16, 32 */
+#define FAST_OPT_SPMV_LANES_FP64      3  /* lanes per block-row of the FP64 SpMV: 4, 8, 16 (default), 32 */
 int         fast_gpu_set_option(fast_gpu_ctx *ctx, int32_t option, int64_t value);
+
+/* Autotuner (no reference counterpart): times the SpMV of the assembled
+ * stiffness for every lanes-per-row choice in both precisions (CUDA events,
+ * median of 9 launches each) and, for systems small enough for the persistent
+ * PCG kernel, one 64-iteration FP64 PCG chunk on each iteration path; keeps
+ * the fastest choices as the context's options.  Needs an assembled K; uses
+ * the solver's work vectors (call it before a solve, not during one). */
+typedef struct {
+  int32_t lanes_fp32, lanes_fp64;       /* chosen lanes per block-row                      */
+  double  ms_fp32[4], ms_fp64[4];       /* per launch for 4, 8, 16, 32 lanes              */
+  int64_t persistent_max_nodes;         /* chosen limit for the persistent PCG kernel     */
+  double  us_iter_persistent, us_iter_kernels;  /* FP64 PCG per iteration, or 0 if not timed */
+} fast_gpu_tune_report;
+int         fast_gpu_autotune(fast_gpu_ctx *ctx, fast_gpu_tune_report *rep);
 
 /* ---- mesh and pattern ---------------------------------------------------
  * Replaces cControl::Init's CompEqs/CompProf (ctrl/ctrl.cpp:2004-2157) for the
