@@ -544,8 +544,9 @@ def run_ours(args):
 
     # ---- dominant kernel and assembly: CUDA events around each launch in the timed region
     hbm, hbm_kind = measured_hbm()
-    achieved = k_bytes / (k_ms / 1e3) / 1e9
-    a_gbs = a_bytes / (a_ms / 1e3) / 1e9
+    # (a zero duration only happens under a profiler that replays the kernels)
+    achieved = k_bytes / (k_ms / 1e3) / 1e9 if k_ms > 0 else 0.0
+    a_gbs = a_bytes / (a_ms / 1e3) / 1e9 if a_ms > 0 else 0.0
     traffic = None
     tp = os.path.join(ROOT, "profiles", "spmv_soa_fp32_hex20_64x64x32.txt" if spmv_which == gpu.KERNEL_SPMV_FP32
                       else "spmv_soa_fp64_hex20_64x64x32.txt")
