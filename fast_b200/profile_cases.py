@@ -7,6 +7,8 @@ under ncu (each one GPU, a few hundred MB at most):
     python -m fast_b200.profile_cases box N         # hex20 box N x N x N/2: assemble + mixed solve
     python -m fast_b200.profile_cases tied          # tied four-block column (B-spline p=2, hex8, hex20,
                                                     #   B-spline p=3): two assemblies
+    python -m fast_b200.profile_cases ensemble N    # N hex8 cantilevers (n in [6, 20]): assemble + batch solve
+    python -m fast_b200.profile_cases newmark       # hex20 box 16x16x8 with density: 20 Newmark steps (mixed)
 
 Each prints one line of results; none measures anything itself.
 """
@@ -62,6 +64,27 @@ def tied():
     print("tied", d.num_eq())
 
 
+def ensemble(count):
+    d, noff, _ = decks.ensemble_cantilevers(count, 6, 20, seed=0)
+    s = gpu.GpuSystem(0)
+    s.upload(d)
+    s.set_problems(noff)
+    f = gpu.face_load_vector(d)
+    s.assemble()
+    u, conv, its, res = s.solve_batch(f, tol=1e-8)
+    print("ensemble", count, int(conv.sum()), int(its.max()))
+
+
+def newmark():
+    d = decks.box_hex20_lognormal(16, 16, 8, seed=0)
+    d.rho = np.full(d.num_elems, 1e-3)
+    q = gpu.face_load_vector(d)
+    s = gpu.GpuSystem(0)
+    s.upload(d)
+    _, _, rep = s.newmark(q, 20, 1e-4, precision=gpu.PREC_MIXED, tol=1e-8, warm=True, mass_tol=1e-10)
+    print("newmark", rep)
+
+
 if __name__ == "__main__":
     case = sys.argv[1] if len(sys.argv) > 1 else "plate_solve"
     if case == "plate_solve":
@@ -70,6 +93,10 @@ if __name__ == "__main__":
         mlp_grad()
     elif case == "tied":
         tied()
+    elif case == "ensemble":
+        ensemble(int(sys.argv[2]) if len(sys.argv) > 2 else 128)
+    elif case == "newmark":
+        newmark()
     elif case == "box":
         box(int(sys.argv[2]) if len(sys.argv) > 2 else 40)
     else:
