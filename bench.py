@@ -218,6 +218,35 @@ def newton_plate(local, args):
     }
 
 
+def ensemble_members(rank, world, count=1024, seed=0):
+    """This rank's members (index, deck) of the configs[4] ensemble: member k
+    (n x n x 2n hex8 cantilever, n uniform in [6, 20], lognormal E per element,
+    random tip traction, all drawn in member order from one seeded stream)
+    belongs to rank k mod world.  No exchange is needed between ranks."""
+    from fast_b200 import decks
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(6, 21, size=count)
+    out = []
+    for k, n in enumerate(ns):
+        m = decks.cantilever_hex8(2 * int(n), int(n), int(n), L=(2.0, 1.0, 1.0), q=tuple(rng.standard_normal(3)))
+        m.E = 1000.0 * np.exp(0.5 * rng.standard_normal(m.num_elems))
+        if k % world == rank:
+            out.append((k, m))
+    return out
+
+
+def reduce_over_ranks(values, op, world, dev):
+    """All-reduce a list of numbers over the ranks (op "max" or "sum"); the
+    identity for one rank.  Every rank must call it at the same point."""
+    if world == 1:
+        return list(values)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(list(values), dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return [float(v) for v in t.tolist()]
+
+
 def ensemble_and_dynamics(local, rank, world, args, dev):
     """(a) 1024 independent hex8 cantilevers n x n x 2n, n uniform
     in [6, 20], lognormal E per element, random tip traction: assembled in one
@@ -231,15 +260,7 @@ def ensemble_and_dynamics(local, rank, world, args, dev):
     import torch.distributed as dist
     from fast_b200 import decks, gpu
     out = {}
-    # this rank's members of decks.ensemble_cantilevers(1024, 6, 20, seed 0), drawn in the same order
-    rng = np.random.default_rng(0)
-    ns = rng.integers(6, 21, size=1024)
-    members = []
-    for k, n in enumerate(ns):
-        m = decks.cantilever_hex8(2 * int(n), int(n), int(n), L=(2.0, 1.0, 1.0), q=tuple(rng.standard_normal(3)))
-        m.E = 1000.0 * np.exp(0.5 * rng.standard_normal(m.num_elems))
-        if k % world == rank:
-            members.append(m)
+    members = [m for _, m in ensemble_members(rank, world)]
     d, noff, _ = decks.concat_decks(members)
     f = gpu.face_load_vector(d)
     S = gpu.GpuSystem(local)
@@ -264,15 +285,8 @@ def ensemble_and_dynamics(local, rank, world, args, dev):
         ts.append(t2 - t1)
     clk = clocks.stop()
     tot = min(a + b for a, b in zip(ta, ts))
-    if world > 1:
-        t = torch.tensor([tot], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot = float(t.item())
-        cnt = torch.tensor([int(conv.sum()), int(d.num_eq())], dtype=torch.int64, device=dev)
-        dist.all_reduce(cnt)
-        nconv, neq_total = int(cnt[0].item()), int(cnt[1].item())
-    else:
-        nconv, neq_total = int(conv.sum()), int(d.num_eq())
+    tot = reduce_over_ranks([tot], "max", world, dev)[0]
+    nconv, neq_total = (int(v) for v in reduce_over_ranks([int(conv.sum()), int(d.num_eq())], "sum", world, dev))
     out["ensemble"] = {
         "workload": "1024 hex8 cantilevers n x n x 2n on 2x1x1, n uniform in [6, 20] (seed 0), 2x2x2 Gauss, "
                     "lognormal E (median 1000, sigma 0.5) per element, random tip traction; assemble all, solve "
@@ -485,11 +499,7 @@ def run_ours(args):
             dist.barrier()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_over_ranks([x], "max", world, dev)[0]
 
     # ---- timed region: device-resident inputs, no instrumentation
     clocks = ClockSampler(local)
