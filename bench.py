@@ -219,7 +219,7 @@ def newton_plate(local, args):
 
 
 def ensemble_members(rank, world, count=1024, seed=0):
-    """This rank's members (index, deck) of the configs[4] ensemble: member k
+    """This rank's members (index, deck) of the cantilever ensemble: member k
     (n x n x 2n hex8 cantilever, n uniform in [6, 20], lognormal E per element,
     random tip traction, all drawn in member order from one seeded stream)
     belongs to rank k mod world.  No exchange is needed between ranks."""
@@ -248,7 +248,7 @@ def reduce_over_ranks(values, op, world, dev):
 
 
 def ensemble_and_dynamics(local, rank, world, args, dev):
-    """(a) 1024 independent hex8 cantilevers n x n x 2n, n uniform
+    """Ensemble and dynamics: (a) 1024 independent hex8 cantilevers n x n x 2n, n uniform
     in [6, 20], lognormal E per element, random tip traction: assembled in one
     pass and solved in one launch (one thread-block cluster per problem) to
     |r_k|/|f_k| <= 1e-8 each; with N ranks the members are split by index
@@ -333,7 +333,7 @@ def ensemble_and_dynamics(local, rank, world, args, dev):
 
 
 def tied_blocks(local, args):
-    """one model of four blocks joined by tied interfaces (a
+    """Tied multi-block model: four blocks joined by tied interfaces (a
     B-spline p=2 patch 32x32x8 with 3^3 Gauss points, a hex8 box 40x40x20 with
     2^3, a hex20 box 24x24x12 with 3^3 and a B-spline p=3 patch 24x24x6 with
     4^3, control points jittered by uniform[-0.05h, 0.05h]); the slave DOFs
