@@ -134,7 +134,6 @@ extern "C" int fast_gpu_nr_solve(fast_gpu_ctx *c, const double *q_host, const fa
   int rc = FAST_GPU_OK;
   fast_gpu_nr_report R{};
   double lam = 0.0, flen2 = 0.0, rlen2 = 0.0, glen2 = 0.0, best = 0.0;
-  bool use_secant = true;
   std::vector<double> hq;
   const double tol = o->tol > 0 ? o->tol : 1e-5;
   if (n <= 0) return FAST_GPU_EINVAL;
@@ -156,7 +155,6 @@ extern "C" int fast_gpu_nr_solve(fast_gpu_ctx *c, const double *q_host, const fa
   NRRC(fast_gpu_internal_force_device(c, w.g));  // initial stresses (zero for these models)
 
   for (int step = 1; step <= o->steps; step++) {
-    const double lam_prev = lam;
     lam += o->step_factor;
     NRCK(axpby(*c, lam, w.q, 0.0, w.q, w.f));  // f = lambda q
 
@@ -171,7 +169,6 @@ extern "C" int fast_gpu_nr_solve(fast_gpu_ctx *c, const double *q_host, const fa
       NRCK(axpby(*c, 1.0, w.f, -1.0, w.g, w.r));
       NRCK(norms2(*c, w, w.r, nullptr, &best, nullptr));
       R.secant_starts++;
-      use_secant = true;
       if (o->predictor == FAST_NR_PREDICT_CALLBACK && predictor) {
         // the caller writes its prediction of u at this load level into du
         const int prc = predictor(predictor_user, step, lam, w.u, w.up, w.f, w.du);
@@ -183,7 +180,6 @@ extern "C" int fast_gpu_nr_solve(fast_gpu_ctx *c, const double *q_host, const fa
           NRCK(norms2(*c, w, w.r, nullptr, &rl, nullptr));
           R.predictions++;
           if (rl < best) {
-            use_secant = false;
             R.predictions_accepted++;
             NRCK(cudaMemcpyAsync(w.ucand, w.du, nb, cudaMemcpyDeviceToDevice, c->stream));
           }
@@ -196,7 +192,6 @@ extern "C" int fast_gpu_nr_solve(fast_gpu_ctx *c, const double *q_host, const fa
     NRRC(fast_gpu_internal_force_device(c, w.g));
     NRCK(axpby(*c, 1.0, w.f, -1.0, w.g, w.r));  // r = f - g
     NRCK(norms2(*c, w, w.r, w.f, &rlen2, &flen2));
-    (void)use_secant;
 
     int conv = 0, it = 0;
     bool start_ok = false;

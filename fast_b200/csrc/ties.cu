@@ -30,9 +30,11 @@ namespace fastgpu {
 
 namespace {
 
+constexpr int kTiedThreads = 1024;
+
 // STAGE: the element matrix is first copied to shared memory (when it fits)
 template <bool STAGE>
-__global__ void tied_scatter(int64_t first, int64_t count, const int64_t *__restrict__ nptr,
+__global__ void __launch_bounds__(kTiedThreads) tied_scatter(int64_t first, int64_t count, const int64_t *__restrict__ nptr,
                              const int32_t *__restrict__ nodes, const int64_t *__restrict__ sptr,
                              const int32_t *__restrict__ slot, const int64_t *__restrict__ pptr,
                              const int32_t *__restrict__ pa, const double *__restrict__ pt,
@@ -222,17 +224,19 @@ cudaError_t launch_tied_assemble(Ctx &c, double *K) {
   for (size_t k = 0; k + 1 < T.color_off.size(); k++) {
     const int64_t first = T.color_off[k], cnt = T.color_off[k + 1] - first;
     if (cnt <= 0) continue;
-    const unsigned grid = (unsigned)std::min<int64_t>(cnt, 4LL * c.sm_count);
+    // one element per CTA; 1024 threads share its expanded pairs, whose K
+    // read-modify-writes are latency-bound
+    const unsigned grid = (unsigned)std::min<int64_t>(cnt, 2LL * c.sm_count);
     int maxnn = 0;
     for (int32_t v : T.h_nn) maxnn = std::max(maxnn, v);
     const size_t smem = sizeof(double) * 9 * maxnn * maxnn;
     if (smem <= 96 * 1024) {
       e = cudaFuncSetAttribute(tied_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e != cudaSuccess) return e;
-      tied_scatter<true><<<grid, 256, smem, c.stream>>>(first, cnt, T.d_nptr, T.d_nodes, T.d_sptr, T.d_slot, T.d_pptr,
+      tied_scatter<true><<<grid, kTiedThreads, smem, c.stream>>>(first, cnt, T.d_nptr, T.d_nodes, T.d_sptr, T.d_slot, T.d_pptr,
                                                         T.d_pa, T.d_pt, T.d_keoff, T.d_nn, T.d_ke, c.d_fix, K);
     } else {
-      tied_scatter<false><<<grid, 256, 0, c.stream>>>(first, cnt, T.d_nptr, T.d_nodes, T.d_sptr, T.d_slot, T.d_pptr,
+      tied_scatter<false><<<grid, kTiedThreads, 0, c.stream>>>(first, cnt, T.d_nptr, T.d_nodes, T.d_sptr, T.d_slot, T.d_pptr,
                                                       T.d_pa, T.d_pt, T.d_keoff, T.d_nn, T.d_ke, c.d_fix, K);
     }
     c.launches++;
