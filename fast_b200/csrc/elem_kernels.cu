@@ -42,17 +42,37 @@ struct ElemSmem {
   static constexpr int kJ = NG * 9;               // Jacobian, then its inverse
   static constexpr int kC = NG;
   static constexpr int kD = MASS ? 0 : NG * ND;   // dN/dx at the Gauss points
-  static constexpr int total = kN + kX + kJ + kC + kD;
-  static constexpr size_t bytes = total * sizeof(double) + 2 * 256 + 64;
+  // hex20 and larger stage the scatter through shared memory (coalesced);
+  // hex8 (64 blocks per element) keeps per-pair register scatter, measured faster
+  static constexpr bool STAGE = NN > 8;
+  static constexpr int NP = NN * (NN + 1) / 2;
+  static constexpr int kK = STAGE ? NN * NN * 9 : 0;   // current K blocks of the element's node pairs
+  static constexpr int kV = STAGE ? NP * 9 : 0;        // the element's 3x3 blocks, a <= b
+  static constexpr int total = kN + kX + kJ + kC + kD + kK + kV;
+  static constexpr size_t bytes = total * sizeof(double) + (STAGE ? NN * NN : 0) * sizeof(int32_t) + 2 * 256 + 64;
 };
 
+// asynchronous 8-byte global -> shared copy
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // One CTA integrates one element at a time (grid-stride over the colour).
-// Thread p < NP owns node pair (a, b), a <= b: it loads the pair's two slot
-// indices and the current 3x3 blocks (a,b) and (b,a) at the start of the
-// element, so the global read latency overlaps the Jacobian and derivative
-// work, then forms
+// Thread p < NP owns node pair (a, b), a <= b, and forms
 //     M_ij = sum_g c_g dN_a/dx_i dN_b/dx_j
-// in registers, turns M into the 3x3 stiffness block and adds it.
+// in registers, turns M into the 3x3 stiffness block and adds it to K.  The
+// current values of the element's K blocks are read at the start of the
+// element, so the read latency overlaps the Jacobian and derivative work:
+//   * hex8: each pair thread loads its blocks (a,b) and (b,a) to registers and
+//     writes them back itself;
+//   * hex20 (STAGE): the CTA copies all NN^2 blocks to shared memory with
+//     cp.async, consecutive threads taking consecutive entries of a block, and
+//     writes old + new back the same way (block (b, a) is the transpose of
+//     (a, b)): coalesced, where per-pair accesses touch one cache line per
+//     thread and instruction.
 template <int NN, int NG, int NT, bool MASS>
 __global__ void __launch_bounds__(NT, (NT >= 128 ? 3 : 8)) elem_kernel(ElemArgs A) {
   using S = ElemSmem<NN, NG, MASS>;
@@ -63,9 +83,10 @@ __global__ void __launch_bounds__(NT, (NT >= 128 ? 3 : 8)) elem_kernel(ElemArgs 
   double *sJ = sX + S::kX;
   double *sc = sJ + S::kJ;
   double *sD = sc + S::kC;
-  uint8_t *sfix = reinterpret_cast<uint8_t *>(sD + S::kD);
-  uint8_t *spa = sfix + 64;
-  uint8_t *spb = spa + 256;
+  double *sKo = sD + S::kD;
+  double *sV = sKo + S::kK;
+  int32_t *sSlot = reinterpret_cast<int32_t *>(sV + S::kV);
+  uint8_t *sfix = reinterpret_cast<uint8_t *>(sSlot + (S::STAGE ? NN * NN : 0));
   constexpr int NP = NN * (NN + 1) / 2;
   static_assert(NP <= NT, "one thread per node pair");
   // Gauss-point tables are read through the L1 cache (read-only, shared by all blocks)
@@ -77,8 +98,6 @@ __global__ void __launch_bounds__(NT, (NT >= 128 ? 3 : 8)) elem_kernel(ElemArgs 
     for (int i = tid; i < S::kN; i += NT) sN[i] = A.N[i];
   int pa = 0, pb = 0;
   if (tid < NP) pair_of(tid, NN, pa, pb);
-  (void)spa;
-  (void)spb;
 
   for (int64_t it = blockIdx.x; it < A.ne; it += gridDim.x) {
     const int64_t e = A.index ? (int64_t)A.index[it] : A.offset + it;
@@ -93,7 +112,16 @@ __global__ void __launch_bounds__(NT, (NT >= 128 ? 3 : 8)) elem_kernel(ElemArgs 
     // early scatter loads: slots, then the current block values
     double *Kab = nullptr, *Kba = nullptr;
     double oab[9], oba[9];
-    if (A.K && tid < NP) {
+    if (S::STAGE && A.K) {
+      const int32_t *es = A.slot + e * NN * NN;
+      for (int t = tid; t < NN * NN * 9; t += NT) {
+        const int q = t / 9, k = t - 9 * q;
+        const int32_t sl = es[q];
+        if (k == 0) sSlot[q] = sl;
+        cp_async8(sKo + t, A.K + (int64_t)sl * 9 + k);
+      }
+      cp_async_commit();
+    } else if (A.K && tid < NP) {
       Kab = A.K + (int64_t)A.slot[(e * NN + pa) * NN + pb] * 9;
       if (pa != pb) Kba = A.K + (int64_t)A.slot[(e * NN + pb) * NN + pa] * 9;
 #pragma unroll
@@ -201,6 +229,10 @@ __global__ void __launch_bounds__(NT, (NT >= 128 ? 3 : 8)) elem_kernel(ElemArgs 
             Ko[(3 * pb + j) * ND + 3 * pa + i] = v[3 * i + j];
           }
       }
+      if (S::STAGE && A.K) {
+#pragma unroll
+        for (int k = 0; k < 9; k++) sV[9 * tid + k] = v[k];
+      }
       if (Kab) {
         const uint8_t fa = sfix[pa], fb = sfix[pb];
 #pragma unroll
@@ -211,6 +243,19 @@ __global__ void __launch_bounds__(NT, (NT >= 128 ? 3 : 8)) elem_kernel(ElemArgs 
               Kab[3 * i + j] = oab[3 * i + j] + v[3 * i + j];
               if (Kba) Kba[3 * j + i] = oba[3 * j + i] + v[3 * i + j];
             }
+      }
+    }
+    if (S::STAGE && A.K) {
+      cp_async_wait_all();
+      __syncthreads();
+      // old + new for every entry whose two DOFs have equations
+      for (int t = tid; t < NN * NN * 9; t += NT) {
+        const int q = t / 9, k = t - 9 * q;
+        const int a = q / NN, b = q - NN * a, i = k / 3, j = k - 3 * i;
+        if (((sfix[a] >> i) & 1) || ((sfix[b] >> j) & 1)) continue;
+        const double add = (a <= b) ? sV[9 * (a * NN - a * (a - 1) / 2 + (b - a)) + k]
+                                    : sV[9 * (b * NN - b * (b - 1) / 2 + (a - b)) + 3 * j + i];
+        A.K[(int64_t)sSlot[q] * 9 + k] = sKo[t] + add;
       }
     }
   }
