@@ -178,16 +178,19 @@ __global__ void __launch_bounds__(NT, (NT >= 128 ? 3 : 8)) elem_kernel(ElemArgs 
         for (int k = 0; k < 9; k++) v[k] = (k % 4 == 0) ? s : 0.0;
       }
     } else {
-      // D[g][i*NN + a] = dN_a/dx_i at Gauss point g
+      // D[g][i*NN + a] = sqrt(c_g) dN_a/dx_i at Gauss point g: the weight
+      // w_g detJ_g is split between the two factors of every product below
+      // (detJ > 0 is required; a non-positive one is reported as EDETJ)
       for (int t = tid; t < NG * NN; t += NT) {
         const int g = t / NN, a = t - NN * g;
         const double *J = sJ + 9 * g;
         const double *dn = gdN + (g * NN + a) * 3;
         const double d0 = dn[0], d1 = dn[1], d2 = dn[2];
+        const double sq = sqrt(sc[g]);
         double *D = sD + g * ND;
-        D[a] = J[0] * d0 + J[1] * d1 + J[2] * d2;
-        D[NN + a] = J[3] * d0 + J[4] * d1 + J[5] * d2;
-        D[2 * NN + a] = J[6] * d0 + J[7] * d1 + J[8] * d2;
+        D[a] = sq * (J[0] * d0 + J[1] * d1 + J[2] * d2);
+        D[NN + a] = sq * (J[3] * d0 + J[4] * d1 + J[5] * d2);
+        D[2 * NN + a] = sq * (J[6] * d0 + J[7] * d1 + J[8] * d2);
       }
       __syncthreads();
       if (tid < NP) {
@@ -199,8 +202,7 @@ __global__ void __launch_bounds__(NT, (NT >= 128 ? 3 : 8)) elem_kernel(ElemArgs 
         for (int k = 0; k < 9; k++) M[k] = 0.0;
         for (int g = 0; g < NG; g++) {
           const double *D = sD + g * ND;
-          const double cg = sc[g];
-          const double a0 = cg * D[pa], a1 = cg * D[NN + pa], a2 = cg * D[2 * NN + pa];
+          const double a0 = D[pa], a1 = D[NN + pa], a2 = D[2 * NN + pa];
           const double b0 = D[pb], b1 = D[NN + pb], b2 = D[2 * NN + pb];
           M[0] = fma(a0, b0, M[0]); M[1] = fma(a0, b1, M[1]); M[2] = fma(a0, b2, M[2]);
           M[3] = fma(a1, b0, M[3]); M[4] = fma(a1, b1, M[4]); M[5] = fma(a1, b2, M[5]);
