@@ -118,7 +118,9 @@ typedef struct {
  * the library assembles K~ = T^T K T directly into the node-block matrix and
  * solves K~ u~ = T^T f; slave displacements are interpolated back.  A slave
  * must not be a master, and its equations (if any) stay in the caller's
- * numbering: loads on them are carried to the masters. */
+ * numbering: loads on them are carried to the masters.  fast_gpu_get_lower_csr
+ * and fast_gpu_mult_vect then see K~, with an identity diagonal on the slave
+ * equations. */
 typedef struct {
   int64_t        num_slaves;
   const int64_t *slave;         /* [num_slaves] tied nodes (0-based, distinct)        */
