@@ -46,6 +46,7 @@ void free_mesh(Ctx &c) {
   }
   c.buckets.clear();
   free_ties(c);
+  free_face_loads(c);
   dfree(c.d_X); dfree(c.d_fix); dfree(c.d_dof_of_eq);
   dfree(c.d_rowptr); dfree(c.d_col); dfree(c.d_diag); dfree(c.d_srow); dfree(c.d_scol);
   dfree(c.d_K); dfree(c.d_M); dfree(c.d_Ks); dfree(c.d_Ms); dfree(c.d_Ks32);

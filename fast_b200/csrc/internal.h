@@ -124,6 +124,12 @@ struct Ctx {
   uint8_t *d_fix = nullptr;       // [nnode] bit i set: DOF i has no equation
   int32_t *d_dof_of_eq = nullptr; // [neq] padded vector index 4*n+i of equation k+1
   std::vector<Bucket> buckets;
+  // face tractions on the device (fast_gpu_set_face_loads)
+  int32_t nface = 0, nfn = 0, face_ngp = 0, nfnode = 0;
+  int32_t *d_fn = nullptr, *d_floc = nullptr;    // [nface][nfn] nodes, [nface] Local flags
+  double *d_fq = nullptr, *d_fe = nullptr;       // [nface][3] tractions, [nface][nfn][3] face forces
+  int32_t *d_fnode = nullptr, *d_feq = nullptr;  // [nfnode] loaded nodes, [nfnode][3] their equations
+  int32_t *d_fptr = nullptr, *d_fidx = nullptr;  // [nfnode+1] / [nface*nfn]: face-node entries per node
   // tied interfaces
   std::vector<int64_t> h_tslave, h_tptr, h_tmaster;  // copies of fast_gpu_ties
   std::vector<double> h_tweight;
@@ -244,6 +250,8 @@ cudaError_t launch_zero_matrix(Ctx &c, double *K, bool identity_on_fixed);
 // 1 on the diagonal of every fixed DOF (the stiffness slot's convention)
 cudaError_t launch_fixed_identity(Ctx &c, double *K);
 cudaError_t launch_assemble(Ctx &c, int what, double *target);
+// device face loads (face_loads.cu)
+void free_face_loads(Ctx &c);
 // tied interfaces (ties.cu)
 cudaError_t upload_ties(Ctx &c);
 void free_ties(Ctx &c);

@@ -45,7 +45,8 @@ EXPORTS = [
     "fast_gpu_inspect_pattern", "fast_gpu_pcg_solve_noalloc", "fast_gpu_set_displacement",
     "fast_gpu_set_displacement_device", "fast_gpu_internal_force", "fast_gpu_internal_force_device",
     "fast_gpu_nr_solve", "fast_gpu_ws_create", "fast_gpu_ws_destroy", "fast_gpu_ws_add_trajectory",
-    "fast_gpu_ws_build_basis", "fast_gpu_ws_train", "fast_gpu_ws_predict", "fast_gpu_ws_report", "fast_gpu_autotune",
+    "fast_gpu_ws_build_basis", "fast_gpu_ws_train", "fast_gpu_ws_predict", "fast_gpu_ws_report", "fast_gpu_autotune", "fast_gpu_set_face_loads",
+    "fast_gpu_face_load_device",
     "fast_gpu_ws_get_basis", "fast_gpu_ws_get_samples", "fast_gpu_mlp_params", "fast_gpu_mlp_forward",
     "fast_gpu_mlp_loss_grad", "fast_gpu_mlp_gemm", "fast_gpu_ws_configure", "fast_gpu_ws_last_input",
     "fast_gpu_set_option", "fast_gpu_set_problems", "fast_gpu_solve_batch", "fast_gpu_newmark",
@@ -202,6 +203,8 @@ def load_library(path: str = LIB_PATH):
     L.fast_gpu_synchronize.argtypes = [vp]
     L.fast_gpu_set_option.argtypes = [vp, ctypes.c_int32, ctypes.c_int64]
     L.fast_gpu_autotune.argtypes = [vp, vp]
+    L.fast_gpu_set_face_loads.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, vp, vp, vp, ctypes.c_int32]
+    L.fast_gpu_face_load_device.argtypes = [vp, ctypes.c_double, vp]
     L.fast_gpu_set_problems.argtypes = [vp, ctypes.c_int32, _lp]
     L.fast_gpu_newmark.argtypes = [vp, _dp, ctypes.POINTER(NewmarkOpts), _dp, _dp, _dp, ctypes.c_int32, _ip, _dp,
                                    ctypes.POINTER(NewmarkReport)]
@@ -405,6 +408,23 @@ class GpuSystem:
         its = np.array([r.iterations for r in reps], np.int32)
         res = np.array([r.rel_residual for r in reps])
         return u, conv, its, res
+
+    def set_face_loads(self, deck: _decks.Deck = None):
+        """Store the deck's face tractions on the device (fast_gpu_set_face_loads)."""
+        deck = self.deck if deck is None else deck
+        if deck.face_elem is None or not len(deck.face_elem):
+            self._ck(self.L.fast_gpu_set_face_loads(self.ctx, 0, 4, None, None, None, 2), "set_face_loads")
+            return
+        fn = np.ascontiguousarray(deck.face_nodes(), dtype=np.int32)
+        q = np.ascontiguousarray(deck.face_q, dtype=np.float64)
+        loc = np.ascontiguousarray(deck.face_local, dtype=np.int32)
+        self._ck(self.L.fast_gpu_set_face_loads(self.ctx, fn.shape[0], fn.shape[1], fn.ctypes.data, q.ctypes.data,
+                                                loc.ctypes.data, int(max(deck.ngp))), "set_face_loads")
+
+    def face_load_device(self, d_f_ptr: int, scale: float = 1.0):
+        """scale * f into the device vector at d_f_ptr (num_eq doubles)."""
+        self._ck(self.L.fast_gpu_face_load_device(self.ctx, float(scale), ctypes.c_void_p(d_f_ptr)),
+                 "face_load_device")
 
     def autotune(self) -> dict:
         """Measure the SpMV lanes-per-row choices and the PCG iteration path on

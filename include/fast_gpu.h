@@ -434,6 +434,17 @@ int fast_gpu_face_load_vector(int64_t num_nodes, const double *coords, const int
                               int32_t num_faces, int32_t nodes_per_face, const int32_t *face_nodes,
                               const double *q, const int32_t *local, int32_t ngp1d, double *f);
 
+/* The same load on the device, from the context's current coordinates (so a
+ * fast_gpu_update_coords is followed): fast_gpu_set_face_loads stores the
+ * faces once per load case (same arguments as above, node indices of the
+ * uploaded mesh); fast_gpu_face_load_device writes scale * f into d_f
+ * (device, num_eq).  Every face is integrated by one thread, then each loaded
+ * node sums its faces' contributions in face order, so f is bit-identical run
+ * to run. */
+int fast_gpu_set_face_loads(fast_gpu_ctx *ctx, int32_t num_faces, int32_t nodes_per_face, const int32_t *face_nodes,
+                            const double *q, const int32_t *local, int32_t ngp1d);
+int fast_gpu_face_load_device(fast_gpu_ctx *ctx, double scale, double *d_f);
+
 /* ---- parity / inspection ---------------------------------------------- */
 /* Host-only: builds the node-block pattern and element colouring of a mesh
  * without a device and reports them.  rowptr [num_nodes+1], col [nnz_blocks]
