@@ -1,0 +1,143 @@
+// stress.cu - Gauss-point strains and stresses at the current displacements
+// (fast_gpu_gauss_stress): what cElmParam::IntPntStress (elc/elmparam.cpp:
+// 859-935) returns for an isotropic small-strain solid, e = B u_e at each
+// integration point (cSolid::BMatrix, elc/anmodel.cpp:1418-1447: Voigt xx yy
+// zz xy xz yz, engineering shears) and s = C e (cSolid::QMatrix,
+// elc/anmodel.cpp:1286-1298).  It is the per-point work FAST repeats on the
+// CPU for every printed step (stress recovery).
+//
+// One thread per (element, Gauss point): the point's Jacobian from the
+// element's coordinates, its inverse by cofactors, then the strain summed
+// over the element's nodes; the threads of one element read the same nodes,
+// which the L1 cache serves.
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+using namespace fastgpu;
+
+struct fast_gpu_ctx : public Ctx {};
+
+namespace {
+
+template <int NN, int NG>
+__global__ void gauss_stress(int64_t count, const int32_t *__restrict__ index, const int32_t *__restrict__ conn,
+                             const double *__restrict__ E, const double *__restrict__ nu,
+                             const double *__restrict__ X, const double *__restrict__ U,
+                             const double *__restrict__ dN, double *__restrict__ strain,
+                             double *__restrict__ stress, int32_t *__restrict__ status) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= count * NG) return;
+  const int64_t k = t / NG;
+  const int g = (int)(t - k * NG);
+  const int64_t e = index[k];
+  const int32_t *en = conn + e * NN;
+  const double *d = dN + (int64_t)g * NN * 3;
+  double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int a = 0; a < NN; a++) {
+    const double *x = X + 3 * (int64_t)en[a];
+#pragma unroll
+    for (int p = 0; p < 3; p++)
+#pragma unroll
+      for (int q = 0; q < 3; q++) J[3 * p + q] = fma(d[3 * a + p], x[q], J[3 * p + q]);
+  }
+  const double det = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) +
+                     J[2] * (J[3] * J[7] - J[4] * J[6]);
+  if (!(det > 0.0)) atomicOr(status, 1);
+  const double id = 1.0 / ((det != 0.0) ? det : 1.0);
+  const double I[9] = {(J[4] * J[8] - J[5] * J[7]) * id,  -(J[1] * J[8] - J[2] * J[7]) * id,
+                       (J[1] * J[5] - J[2] * J[4]) * id,  -(J[3] * J[8] - J[5] * J[6]) * id,
+                       (J[0] * J[8] - J[2] * J[6]) * id,  -(J[0] * J[5] - J[2] * J[3]) * id,
+                       (J[3] * J[7] - J[4] * J[6]) * id,  -(J[0] * J[7] - J[1] * J[6]) * id,
+                       (J[0] * J[4] - J[1] * J[3]) * id};
+  // displacement gradient G[i][j] = du_i/dx_j
+  double G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int a = 0; a < NN; a++) {
+    const double d0 = d[3 * a], d1 = d[3 * a + 1], d2 = d[3 * a + 2];
+    const double gx = I[0] * d0 + I[1] * d1 + I[2] * d2;
+    const double gy = I[3] * d0 + I[4] * d1 + I[5] * d2;
+    const double gz = I[6] * d0 + I[7] * d1 + I[8] * d2;
+    const double *u = U + 4 * (int64_t)en[a];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      G[3 * i] = fma(u[i], gx, G[3 * i]);
+      G[3 * i + 1] = fma(u[i], gy, G[3 * i + 1]);
+      G[3 * i + 2] = fma(u[i], gz, G[3 * i + 2]);
+    }
+  }
+  const double ev[6] = {G[0], G[4], G[8], G[1] + G[3], G[2] + G[6], G[5] + G[7]};
+  const double En = E[e], v = nu[e];
+  const double dd = (1.0 + v) * (1.0 - 2.0 * v);
+  const double C00 = En * (1.0 - v) / dd, C01 = En * v / dd, Gs = 0.5 * En / (1.0 + v);
+  double *so = stress + t * 6, *eo = strain + t * 6;
+#pragma unroll
+  for (int c = 0; c < 6; c++) eo[c] = ev[c];
+  so[0] = C00 * ev[0] + C01 * (ev[1] + ev[2]);
+  so[1] = C00 * ev[1] + C01 * (ev[0] + ev[2]);
+  so[2] = C00 * ev[2] + C01 * (ev[0] + ev[1]);
+  so[3] = Gs * ev[3];
+  so[4] = Gs * ev[4];
+  so[5] = Gs * ev[5];
+}
+
+template <int NN, int NG>
+cudaError_t run(Ctx &c, const Bucket &B, int64_t count, const int32_t *idx, double *st, double *ss) {
+  const int64_t n = count * NG;
+  gauss_stress<NN, NG><<<(unsigned)((n + 127) / 128), 128, 0, c.stream>>>(count, idx, B.d_conn, B.d_E, B.d_nu, c.d_X,
+                                                                          c.d_disp, B.d_dN, st, ss, c.d_status);
+  c.launches++;
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+#define SCK(call)                                                                 \
+  do {                                                                            \
+    cudaError_t _e = (call);                                                      \
+    if (_e != cudaSuccess) {                                                      \
+      c->err = std::string("gauss_stress: ") + #call + ": " + cudaGetErrorString(_e); \
+      if (buf) cudaFree(buf);                                                     \
+      return FAST_GPU_ECUDA;                                                      \
+    }                                                                             \
+  } while (0)
+
+extern "C" int fast_gpu_gauss_stress(fast_gpu_ctx *c, int32_t b, int64_t first, int64_t count, double *strain,
+                                     double *stress) {
+  if (!c || b < 0 || b >= (int)c->buckets.size() || !strain || !stress) return FAST_GPU_EINVAL;
+  const Bucket &B = c->buckets[b];
+  if (first < 0 || count <= 0 || first + count > B.ne) return FAST_GPU_EINVAL;
+  if (B.tl || B.type == FAST_ELEM_BSP_SOLID) {
+    c->err = "gauss_stress: small-strain hex buckets only";
+    return FAST_GPU_ENOTSUP;
+  }
+  const int ng = B.ng;
+  const size_t vals = (size_t)count * ng * 6;
+  double *buf = nullptr;
+  SCK(cudaMalloc((void **)&buf, sizeof(double) * 2 * vals + sizeof(int32_t) * count + 16));
+  std::vector<int32_t> idx(count);
+  for (int64_t k = 0; k < count; k++) idx[k] = B.inv[first + k];
+  int32_t *d_idx = reinterpret_cast<int32_t *>(buf + 2 * vals);
+  SCK(cudaMemcpyAsync(d_idx, idx.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice, c->stream));
+  SCK(cudaMemsetAsync(c->d_status, 0, sizeof(int32_t), c->stream));
+  cudaError_t e = cudaErrorInvalidValue;
+  if (B.type == FAST_ELEM_HEX8 && ng == 8) e = run<8, 8>(*c, B, count, d_idx, buf, buf + vals);
+  else if (B.type == FAST_ELEM_HEX8 && ng == 27) e = run<8, 27>(*c, B, count, d_idx, buf, buf + vals);
+  else if (B.type == FAST_ELEM_HEX8 && ng == 1) e = run<8, 1>(*c, B, count, d_idx, buf, buf + vals);
+  else if (B.type == FAST_ELEM_HEX20 && ng == 27) e = run<20, 27>(*c, B, count, d_idx, buf, buf + vals);
+  else if (B.type == FAST_ELEM_HEX20 && ng == 8) e = run<20, 8>(*c, B, count, d_idx, buf, buf + vals);
+  else if (B.type == FAST_ELEM_HEX20 && ng == 64) e = run<20, 64>(*c, B, count, d_idx, buf, buf + vals);
+  SCK(e);
+  SCK(cudaMemcpyAsync(strain, buf, sizeof(double) * vals, cudaMemcpyDeviceToHost, c->stream));
+  SCK(cudaMemcpyAsync(stress, buf + vals, sizeof(double) * vals, cudaMemcpyDeviceToHost, c->stream));
+  int32_t status = 0;
+  SCK(cudaMemcpyAsync(&status, c->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  SCK(cudaStreamSynchronize(c->stream));
+  cudaFree(buf);
+  if (status) {
+    c->err = "gauss_stress: non-positive Jacobian determinant in at least one element";
+    return FAST_GPU_EDETJ;
+  }
+  return FAST_GPU_OK;
+}

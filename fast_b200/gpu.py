@@ -45,7 +45,7 @@ EXPORTS = [
     "fast_gpu_inspect_pattern", "fast_gpu_pcg_solve_noalloc", "fast_gpu_set_displacement",
     "fast_gpu_set_displacement_device", "fast_gpu_internal_force", "fast_gpu_internal_force_device",
     "fast_gpu_nr_solve", "fast_gpu_ws_create", "fast_gpu_ws_destroy", "fast_gpu_ws_add_trajectory",
-    "fast_gpu_ws_build_basis", "fast_gpu_ws_train", "fast_gpu_ws_predict", "fast_gpu_ws_report", "fast_gpu_autotune", "fast_gpu_set_face_loads",
+    "fast_gpu_ws_build_basis", "fast_gpu_ws_train", "fast_gpu_ws_predict", "fast_gpu_ws_report", "fast_gpu_autotune", "fast_gpu_set_face_loads", "fast_gpu_gauss_stress",
     "fast_gpu_face_load_device",
     "fast_gpu_ws_get_basis", "fast_gpu_ws_get_samples", "fast_gpu_mlp_params", "fast_gpu_mlp_forward",
     "fast_gpu_mlp_loss_grad", "fast_gpu_mlp_gemm", "fast_gpu_ws_configure", "fast_gpu_ws_last_input",
@@ -203,6 +203,7 @@ def load_library(path: str = LIB_PATH):
     L.fast_gpu_synchronize.argtypes = [vp]
     L.fast_gpu_set_option.argtypes = [vp, ctypes.c_int32, ctypes.c_int64]
     L.fast_gpu_autotune.argtypes = [vp, vp]
+    L.fast_gpu_gauss_stress.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, vp, vp]
     L.fast_gpu_set_face_loads.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, vp, vp, vp, ctypes.c_int32]
     L.fast_gpu_face_load_device.argtypes = [vp, ctypes.c_double, vp]
     L.fast_gpu_set_problems.argtypes = [vp, ctypes.c_int32, _lp]
@@ -425,6 +426,18 @@ class GpuSystem:
         """scale * f into the device vector at d_f_ptr (num_eq doubles)."""
         self._ck(self.L.fast_gpu_face_load_device(self.ctx, float(scale), ctypes.c_void_p(d_f_ptr)),
                  "face_load_device")
+
+    def gauss_stress(self, first=0, count=None, bucket=0):
+        """Gauss-point (strain, stress) [count][points][6] at the current
+        displacements (fast_gpu_gauss_stress)."""
+        b = self.deck.buckets()[bucket]
+        count = b.num_elems - first if count is None else count
+        ng = int(np.prod(b.ngp))
+        st = np.zeros((count, ng, 6))
+        ss = np.zeros((count, ng, 6))
+        self._ck(self.L.fast_gpu_gauss_stress(self.ctx, bucket, int(first), int(count), st.ctypes.data,
+                                              ss.ctypes.data), "gauss_stress")
+        return st, ss
 
     def autotune(self) -> dict:
         """Measure the SpMV lanes-per-row choices and the PCG iteration path on

@@ -445,6 +445,16 @@ int fast_gpu_set_face_loads(fast_gpu_ctx *ctx, int32_t num_faces, int32_t nodes_
                             const double *q, const int32_t *local, int32_t ngp1d);
 int fast_gpu_face_load_device(fast_gpu_ctx *ctx, double scale, double *d_f);
 
+/* ---- stress recovery ----------------------------------------------------
+ * Gauss-point strains and stresses at the current displacements
+ * (fast_gpu_set_displacement): cElmParam::IntPntStress (elc/elmparam.cpp:
+ * 859-935) for elements first .. first+count-1 of a small-strain hex bucket,
+ * in the caller's element order; strain and stress are host arrays
+ * [count][points][6], Voigt xx yy zz xy xz yz (engineering shears), points in
+ * the Gauss rule's order (r fastest). */
+int fast_gpu_gauss_stress(fast_gpu_ctx *ctx, int32_t bucket, int64_t first, int64_t count, double *strain,
+                          double *stress);
+
 /* ---- parity / inspection ---------------------------------------------- */
 /* Host-only: builds the node-block pattern and element colouring of a mesh
  * without a device and reports them.  rowptr [num_nodes+1], col [nnz_blocks]

@@ -233,6 +233,28 @@ int fo_elem_intforce(int nn, const int *ngp, const double *X, double E, double n
   return bad;
 }
 
+/* Gauss-point strains e = B u_e and stresses s = C e, point by point in the
+ * rule's order (cElmParam::IntPntStress, elc/elmparam.cpp:859-935; the
+ * isotropic section's Stress, sec/secanalysis.cpp:219-224). */
+int fo_elem_stress(int nn, const int *ngp, const double *X, double E, double nu,
+                   const double *ue, double *strain, double *stress)
+{
+  int nd = 3 * nn, bad = 0;
+  double pts[216 * 3], wts[216], N[20], dN[60], dX[60], B[6 * 60], C[36];
+  int np = gauss_pts(ngp, pts, wts);
+  qmatrix(E, nu, C);
+  for (int g = 0; g < np; g++)
+  {
+    double detJ, *e = strain + 6 * g, *s = stress + 6 * g;
+    shape(nn, pts[3 * g], pts[3 * g + 1], pts[3 * g + 2], N, dN);
+    if (drv_xyz(nn, dN, X, &detJ, dX)) bad = -1;
+    bmatrix(nn, dX, B);
+    for (int k = 0; k < 6; k++) { e[k] = 0; for (int j = 0; j < nd; j++) e[k] += B[k * nd + j] * ue[j]; }
+    for (int k = 0; k < 6; k++) { s[k] = 0; for (int j = 0; j < 6; j++) s[k] += C[k * 6 + j] * e[j]; }
+  }
+  return bad;
+}
+
 int fo_elem_mass(int nn, const int *ngp, const double *X, double rho, double *Me)
 {
   int nd = 3 * nn, bad = 0;

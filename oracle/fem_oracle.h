@@ -37,6 +37,8 @@ int fo_elems_stiff(int nn, const int *ngp, int64_t ne, const int32_t *conn, cons
  * elc/elmparam.cpp:449-535). */
 int fo_elem_intforce(int nn, const int *ngp, const double *X, double E, double nu,
                      const double *ue, double *ge);
+int fo_elem_stress(int nn, const int *ngp, const double *X, double E, double nu,
+                   const double *ue, double *strain, double *stress);
 
 /* Consistent mass M = sum_g w detJ rho N^T N (cElmParam::MassMat, elc/elmparam.cpp:672-739). */
 int fo_elem_mass(int nn, const int *ngp, const double *X, double rho, double *Me);

@@ -36,6 +36,7 @@ def lib():
         L.fo_elem_stiff.argtypes = [ctypes.c_int, _ip, _dp, ctypes.c_double, ctypes.c_double, _dp]
         L.fo_elems_stiff.argtypes = [ctypes.c_int, _ip, ctypes.c_int64, ctypes.POINTER(ctypes.c_int32), _dp, _dp, _dp, _dp]
         L.fo_elem_intforce.argtypes = [ctypes.c_int, _ip, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp]
+        L.fo_elem_stress.argtypes = [ctypes.c_int, _ip, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp]
         L.fo_elem_mass.argtypes = [ctypes.c_int, _ip, _dp, ctypes.c_double, _dp]
         L.fo_elem_tl.argtypes = [ctypes.c_int, _ip, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp]
         L.fo_face_load.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp]
@@ -82,6 +83,17 @@ def elem_intforce(nn, ngp, X, E, nu, ue):
     ue = np.ascontiguousarray(ue, dtype=np.float64)
     rc = lib().fo_elem_intforce(nn, _ngp(ngp), _p(X), float(E), float(nu), _p(ue), _p(g))
     return g, rc
+
+
+def elem_stress(nn, ngp, X, E, nu, ue):
+    """Gauss-point strains and stresses [ngp][6] (Voigt xx yy zz xy xz yz)."""
+    n = int(np.prod(ngp))
+    e = np.zeros((n, 6))
+    s = np.zeros((n, 6))
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    ue = np.ascontiguousarray(ue, dtype=np.float64)
+    rc = lib().fo_elem_stress(nn, _ngp(ngp), _p(X), float(E), float(nu), _p(ue), _p(e), _p(s))
+    return e, s, rc
 
 
 def elem_mass(nn, ngp, X, rho):

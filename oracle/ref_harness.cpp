@@ -25,7 +25,10 @@
 //                                  cLinStat::Solver does (ctrl/ctrllins.cpp:46-70)
 //         g_of_u    [neq]          cControl::IntForceVector after AssignDispl(u)
 //       With --u the element quantities are evaluated at the given nodal state
-//       (for total-Lagrangian elements).
+//       (for total-Lagrangian elements).  With --stress, at the solved (or the
+//       --u) state:
+//         elm_strain, elm_stress [ne][nip][6]  cElement::IntPntStress
+//                                  (elc/elmparam.cpp:859-935), Voigt xx yy zz xy xz yz
 //
 //   fastref bench <deck> <pcg_iters> [reps]
 //       Times the reference CPU path on one host thread: StiffnessMatrix into
@@ -134,7 +137,7 @@ static int mode_dump(int argc, char **argv)
 {
   string deck = argv[2];
   const char *outp = argv[3];
-  bool trip = true, solve = true, mass = false;
+  bool trip = true, solve = true, mass = false, stress = false;
   const char *ufile = 0;
   double stol = -1.0;
   for (int a = 4; a < argc; a++)
@@ -143,6 +146,7 @@ static int mode_dump(int argc, char **argv)
     if (s == "--no-triplets") trip = false;
     else if (s == "--no-solve") solve = false;
     else if (s == "--mass") mass = true;
+    else if (s == "--stress") stress = true;
     else if (s == "--u" && a + 1 < argc) ufile = argv[++a];
     else if (s == "--solver-tol" && a + 1 < argc) stol = atof(argv[++a]);
   }
@@ -243,6 +247,26 @@ static int mode_dump(int argc, char **argv)
     cControl::IntForceVector(g);
     w.f8("g_of_u", {neq}, g.Val( ), neq);
     delete K;
+  }
+  if (stress && (ufile || solve))
+  {
+    const int nip = ne > 0 ? cElement::GetElm(0)->GetNumIntPnt( ) : 0;
+    vector<double> SE((size_t)ne * nip * 6), SS((size_t)ne * nip * 6);
+    cMatrix Strain(nip, 6), Stress(nip, 6);
+    for (int e = 0; e < ne; e++)
+    {
+      cElement *elm = cElement::GetElm(e);
+      if (elm->GetNumIntPnt( ) != nip) { fprintf(stderr, "mixed integration orders are not dumped\n"); return 2; }
+      elm->IntPntStress(Strain, Stress);
+      for (int i = 0; i < nip; i++)
+        for (int k = 0; k < 6; k++)
+        {
+          SE[((size_t)e * nip + i) * 6 + k] = Strain[i][k];
+          SS[((size_t)e * nip + i) * 6 + k] = Stress[i][k];
+        }
+    }
+    w.f8("elm_strain", {ne, nip, 6}, SE.data( ), SE.size( ));
+    w.f8("elm_stress", {ne, nip, 6}, SS.data( ), SS.size( ));
   }
   cout.rdbuf(coutbuf);
   return 0;

@@ -6,6 +6,7 @@ override with FAST_REF):
 
     python tests/golden/make_golden.py          (all fixtures)
     python tests/golden/make_golden.py iga      (B-spline solid fixtures only)
+    python tests/golden/make_golden.py stress   (the two fixtures with Gauss-point stresses)
 
 It builds ``oracle/_ref/fastref`` (the reference's own sources compiled by
 ``oracle/Makefile``, plus a dump harness), writes each deck with
@@ -64,10 +65,12 @@ def lower_csr(ref: dict):
     return dict(K_indptr=K.indptr.astype(np.int64), K_indices=K.indices.astype(np.int32), K_data=K.data)
 
 
-def run_case(name, deck, tmp, keep_elems=None, triplets=True, extra=(), uvec=None, mass=False):
+def run_case(name, deck, tmp, keep_elems=None, triplets=True, extra=(), uvec=None, mass=False, stress=False):
     base = os.path.join(tmp, name)
     decks.write_dat(deck, base)
     opts = list(extra)
+    if stress:
+        opts.append("--stress")
     if not triplets:
         opts.append("--no-triplets")
     if mass:
@@ -87,6 +90,9 @@ def run_case(name, deck, tmp, keep_elems=None, triplets=True, extra=(), uvec=Non
     out["ref_elm_dofs"] = ref["elm_dofs"]
     if "elm_M" in ref:
         out["ref_elm_M"] = ref["elm_M"][sel]
+    if "elm_stress" in ref:
+        out["ref_elm_strain"] = ref["elm_strain"][sel]
+        out["ref_elm_stress"] = ref["elm_stress"][sel]
     out["ref_f"] = ref["f"]
     if triplets:
         out.update({"ref_" + k: v for k, v in lower_csr(ref).items()})
@@ -128,9 +134,27 @@ def iga_cases(tmp):
     print("iga_scordelis_deg3 written")
 
 
+def stress_cases(tmp):
+    """Decks whose fixtures also hold the reference's Gauss-point strains and
+    stresses at its solution (cElement::IntPntStress)."""
+    # hex8 cantilever 20x4x4 (1500 equations), skyline + Crout
+    run_case("cfg_hex8_cantilever", decks.cantilever_hex8(), tmp, stress=True)
+
+    # hex20 lognormal boxes (sparse Jacobi-PCG in the reference), small enough for full dumps
+    d = decks.box_hex20_lognormal(4, 4, 2, seed=7)
+    d.tol = 1e-13
+    run_case("cfg_hex20_lognormal_4x4x2", d, tmp, stress=True)
+
+
 def main():
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"FAST_REF={FAST_REF}", "ref"], check=True)
     tmp = tempfile.mkdtemp(prefix="golden_")
+    if len(sys.argv) > 1 and sys.argv[1] == "stress":
+        try:
+            stress_cases(tmp)
+        finally:
+            shutil.rmtree(tmp, ignore_errors=True)
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "iga":
         try:
             iga_cases(tmp)
@@ -157,13 +181,7 @@ def main():
             np.savez_compressed(os.path.join(HERE, nm + ".npz"), **out)
             print(nm, "written")
 
-        # hex8 cantilever 20x4x4 (1500 equations), skyline + Crout
-        run_case("cfg_hex8_cantilever", decks.cantilever_hex8(), tmp)
-
-        # hex20 lognormal boxes (sparse Jacobi-PCG in the reference), small enough for full dumps
-        d = decks.box_hex20_lognormal(4, 4, 2, seed=7)
-        d.tol = 1e-13
-        run_case("cfg_hex20_lognormal_4x4x2", d, tmp)
+        stress_cases(tmp)
         d = decks.box_hex20_lognormal(8, 8, 4, seed=11)
         d.tol = 1e-12
         run_case("cfg_hex20_lognormal_8x8x4", d, tmp, keep_elems=np.arange(0, 256, 17), triplets=False)

@@ -199,3 +199,19 @@ def test_oracle_newmark_matches_reference():
             node = np.zeros(eq.shape)
             node[m] = X[s][eq[m] - 1]
             assert gio.rel(node, R[s]) < 1e-9, (name, s, gio.rel(node, R[s]))
+
+
+@pytest.mark.parametrize("name", [c for c in CASES if "ref_elm_stress" in gio.load(c)[1]])
+def test_gauss_point_stresses(name):
+    """Strains and stresses at the Gauss points of the reference's solution
+    (cElement::IntPntStress) from the C restatement."""
+    d, g = gio.load(name)
+    eq = d.node_eq()
+    u = g["ref_u"]
+    for k, e in enumerate(g["ref_elems"]):
+        dofs = eq[d.conn[e]].ravel()
+        ue = np.where(dofs > 0, u[np.maximum(dofs - 1, 0)], 0.0)
+        st, ss, rc = fo.elem_stress(d.nn, d.ngp, d.coords[d.conn[e]], d.E[e], d.nu[e], ue)
+        assert rc == 0
+        assert np.abs(st - g["ref_elm_strain"][k]).max() <= 1e-12 * np.abs(g["ref_elm_strain"]).max()
+        assert np.abs(ss - g["ref_elm_stress"][k]).max() <= 1e-12 * np.abs(g["ref_elm_stress"]).max()
