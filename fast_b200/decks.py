@@ -102,6 +102,8 @@ class Deck:
     maxstep: int = 1
     step_factor: float = 1.0
     time_step: float = 0.0                    # Newmark: %HEADER.ANALYSIS.TIME.STEP
+    arc_load_coeff: Optional[float] = None    # arc-length: %HEADER.ANALYSIS.ARC-LENGTH (load coefficient)
+    target_iter: Optional[int] = None         # %HEADER.ANALYSIS.TARGET.ITERATIONS (reference default 1)
     newmark: tuple = (0.5, 0.25)              # Newmark: (gamma, beta), cCtrlNewmark defaults
     print_step: int = 1                       # %HEADER.ANALYSIS.PRINT.STEPS
     node_labels: Optional[np.ndarray] = None  # [nnode] labels used in a .dat
@@ -630,6 +632,18 @@ def nodal_load_vector(deck: Deck) -> np.ndarray:
     return f
 
 
+def read_pos_factors(path: str) -> np.ndarray:
+    """Load factor of every printed step of a FAST .pos file
+    (%RESULT.CASE.STEP.FACTOR, cControl::PrintResult ctrl/ctrl.cpp:1154-1155)."""
+    out = []
+    with open(path) as fp:
+        lines = fp.read().splitlines()
+    for i, ln in enumerate(lines):
+        if ln.strip() == "%RESULT.CASE.STEP.FACTOR":
+            out.append(float(lines[i + 1].split()[0]))
+    return np.asarray(out)
+
+
 def read_pos_block(path: str, key: str = "NODAL.DISPLACEMENT") -> np.ndarray:
     """Nodal vectors of one result block (``%RESULT.CASE.STEP.<key>``) of every
     printed step of a FAST .pos file: [steps][nnode][3], rows ordered by node
@@ -681,6 +695,10 @@ def write_dat(deck: Deck, base: str) -> str:
         lines += ["%HEADER.ANALYSIS.MAXIMUM.STEPS", str(int(deck.maxstep)), ""]
     if deck.step_factor != 1.0:
         lines += ["%HEADER.ANALYSIS.STEP.FACTOR", _fmt(deck.step_factor), ""]
+    if deck.arc_load_coeff is not None:
+        lines += ["%HEADER.ANALYSIS.ARC-LENGTH", _fmt(deck.arc_load_coeff), ""]
+    if deck.target_iter is not None:
+        lines += ["%HEADER.ANALYSIS.TARGET.ITERATIONS", str(int(deck.target_iter)), ""]
     if deck.algorithm.lower() == "newmark":
         lines += ["%HEADER.ANALYSIS.TIME.STEP", _fmt(deck.time_step), ""]
         lines += ["%HEADER.ANALYSIS.NEWMARK.PARAMETERS", f"{_fmt(deck.newmark[0])} {_fmt(deck.newmark[1])}", ""]

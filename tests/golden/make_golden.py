@@ -7,6 +7,7 @@ override with FAST_REF):
     python tests/golden/make_golden.py          (all fixtures)
     python tests/golden/make_golden.py iga      (B-spline solid fixtures only)
     python tests/golden/make_golden.py stress   (the two fixtures with Gauss-point stresses)
+    python tests/golden/make_golden.py arc      (the path-following fixture)
 
 It builds ``oracle/_ref/fastref`` (the reference's own sources compiled by
 ``oracle/Makefile``, plus a dump harness), writes each deck with
@@ -134,6 +135,34 @@ def iga_cases(tmp):
     print("iga_scordelis_deg3 written")
 
 
+def arc_cases(tmp):
+    """The reference's own path-following controller (cCtrlPath with the
+    'ioal', 'uoal' and 'clinal' arc-length rules, unmodified `fast` binary) on
+    a small TL plate: displacements and load factors of every step."""
+    out = None
+    for alg in ("ioal", "uoal", "clinal"):
+        d = decks.plate_tl_hex8(6, 6, 2, L=4.0, t=0.4, pressure=8.0, steps=8, tol=1e-10, maxit=30)
+        d.algorithm = alg
+        d.step_factor = 0.15
+        d.arc_load_coeff = 0.0
+        d.target_iter = 4
+        base = os.path.join(tmp, "arc_" + alg)
+        decks.write_dat(d, base)
+        subprocess.run([refdump.FAST, base, "-silent"], check=True, stdout=subprocess.DEVNULL)
+        us = decks.read_pos_displacements(base + ".pos")
+        lam = decks.read_pos_factors(base + ".pos")
+        if out is None:
+            ref = refdump.run_dump(base, base + ".bin", "--no-solve", "--no-triplets")
+            out = deck_arrays(d)
+            out.update(ref_neq=ref["neq"], ref_node_eq=ref["node_eq"], ref_f=ref["f"], steps=np.array(d.maxstep),
+                       step_factor=np.array(d.step_factor), tol=np.array(d.tol), maxit=np.array(d.maxit),
+                       load_coeff=np.array(d.arc_load_coeff), target_iter=np.array(d.target_iter))
+        out["ref_u_steps_" + alg] = us
+        out["ref_lam_" + alg] = lam
+    np.savez_compressed(os.path.join(HERE, "arc_plate_tl.npz"), **out)
+    print("arc_plate_tl:", out["ref_u_steps_clinal"].shape, out["ref_lam_clinal"])
+
+
 def stress_cases(tmp):
     """Decks whose fixtures also hold the reference's Gauss-point strains and
     stresses at its solution (cElement::IntPntStress)."""
@@ -149,6 +178,12 @@ def stress_cases(tmp):
 def main():
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"FAST_REF={FAST_REF}", "ref"], check=True)
     tmp = tempfile.mkdtemp(prefix="golden_")
+    if len(sys.argv) > 1 and sys.argv[1] == "arc":
+        try:
+            arc_cases(tmp)
+        finally:
+            shutil.rmtree(tmp, ignore_errors=True)
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "stress":
         try:
             stress_cases(tmp)
@@ -182,6 +217,7 @@ def main():
             print(nm, "written")
 
         stress_cases(tmp)
+        arc_cases(tmp)
         d = decks.box_hex20_lognormal(8, 8, 4, seed=11)
         d.tol = 1e-12
         run_case("cfg_hex20_lognormal_8x8x4", d, tmp, keep_elems=np.arange(0, 256, 17), triplets=False)

@@ -7,7 +7,7 @@ import scipy.sparse as sp
 from oracle import fem_oracle as fo
 from tests import golden_io as gio
 
-CASES = [n for n in gio.names() if not n.startswith(("nr_", "nm_", "iga_"))]
+CASES = [n for n in gio.names() if not n.startswith(("nr_", "nm_", "iga_", "arc_"))]
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -215,3 +215,22 @@ def test_gauss_point_stresses(name):
         assert rc == 0
         assert np.abs(st - g["ref_elm_strain"][k]).max() <= 1e-12 * np.abs(g["ref_elm_strain"]).max()
         assert np.abs(ss - g["ref_elm_stress"][k]).max() <= 1e-12 * np.abs(g["ref_elm_stress"]).max()
+
+
+@pytest.mark.parametrize("method", ["ioal", "uoal", "clinal"])
+def test_oracle_arclength_matches_reference(method):
+    """The oracle's restatement of cCtrlPath with the arc-length rules
+    reproduces the displacements and load factors that the reference's own
+    `fast` binary printed for every step."""
+    from oracle import path_oracle as po
+    d, g = gio.load("arc_plate_tl")
+    us, lams, its = po.arclength(d, g["ref_f"], method, int(g["steps"]), float(g["step_factor"]), int(g["maxit"]),
+                                 float(g["tol"]), float(g["load_coeff"]), int(g["target_iter"]))
+    assert len(lams) == len(g["ref_lam_" + method])
+    assert np.abs(lams - g["ref_lam_" + method]).max() < 1e-10
+    eq = d.node_eq()
+    m = eq > 0
+    for k in range(len(us)):
+        unode = np.zeros((d.num_nodes, 3))
+        unode[m] = us[k][eq[m] - 1]
+        assert gio.rel(unode, g["ref_u_steps_" + method][k]) < 1e-9, k
