@@ -46,7 +46,7 @@ EXPORTS = [
     "fast_gpu_set_displacement_device", "fast_gpu_internal_force", "fast_gpu_internal_force_device",
     "fast_gpu_nr_solve", "fast_gpu_ws_create", "fast_gpu_ws_destroy", "fast_gpu_ws_add_trajectory",
     "fast_gpu_ws_build_basis", "fast_gpu_ws_train", "fast_gpu_ws_predict", "fast_gpu_ws_report", "fast_gpu_autotune", "fast_gpu_set_face_loads", "fast_gpu_gauss_stress",
-    "fast_gpu_face_load_device",
+    "fast_gpu_face_load_device", "fast_gpu_arclength_solve",
     "fast_gpu_ws_get_basis", "fast_gpu_ws_get_samples", "fast_gpu_mlp_params", "fast_gpu_mlp_forward",
     "fast_gpu_mlp_loss_grad", "fast_gpu_mlp_gemm", "fast_gpu_ws_configure", "fast_gpu_ws_last_input",
     "fast_gpu_set_option", "fast_gpu_set_problems", "fast_gpu_solve_batch", "fast_gpu_newmark",
@@ -100,6 +100,25 @@ class SolveReport(ctypes.Structure):
     _fields_ = [("converged", ctypes.c_int32), ("iterations", ctypes.c_int32), ("outer", ctypes.c_int32),
                 ("escalated", ctypes.c_int32), ("rel_residual", ctypes.c_double),
                 ("true_rel_residual", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+ARC_INITIAL_NORMAL, ARC_UPDATED_NORMAL, ARC_LINEARIZED = 1, 2, 3
+ARC_METHODS = {"ioal": ARC_INITIAL_NORMAL, "uoal": ARC_UPDATED_NORMAL, "clinal": ARC_LINEARIZED}
+
+
+class ArcOpts(ctypes.Structure):
+    _fields_ = [("method", ctypes.c_int32), ("steps", ctypes.c_int32), ("max_iter", ctypes.c_int32),
+                ("target_iter", ctypes.c_int32), ("step_factor", ctypes.c_double), ("tol", ctypes.c_double),
+                ("load_coeff", ctypes.c_double), ("lin", SolveOpts)]
+
+
+class ArcReport(ctypes.Structure):
+    _fields_ = [("converged_steps", ctypes.c_int32), ("failed_step", ctypes.c_int32),
+                ("iterations", ctypes.c_int32), ("linear_iterations", ctypes.c_int32),
+                ("last_err", ctypes.c_double), ("arc_length", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -235,6 +254,8 @@ def load_library(path: str = LIB_PATH):
     L.fast_gpu_internal_force_device.argtypes = [vp, vp]
     L.fast_gpu_nr_solve.argtypes = [vp, _dp, ctypes.POINTER(NrOpts), NR_PREDICTOR, vp, _dp, _ip,
                                     ctypes.POINTER(NrReport)]
+    L.fast_gpu_arclength_solve.argtypes = [vp, _dp, ctypes.POINTER(ArcOpts), _dp, _dp, _ip,
+                                           ctypes.POINTER(ArcReport)]
     _fp = ctypes.POINTER(ctypes.c_float)
     L.fast_gpu_ws_create.argtypes = [vp, ctypes.POINTER(WsOpts), ctypes.POINTER(vp)]
     L.fast_gpu_ws_destroy.argtypes = [vp]
@@ -529,6 +550,28 @@ class GpuSystem:
         if rc != FAST_GPU_OK and raise_on_fail:
             self._ck(rc, "nr_solve")
         return hist, iters, rep.as_dict()
+
+    # -- path following (cCtrlPath::Solver with the arc-length rules)
+    def arclength_solve(self, q, method, steps, step_factor, tol=1e-8, max_iter=30, load_coeff=0.0, target_iter=1,
+                        precision=PREC_FP64, precond=PRECOND_JACOBI, lin_tol=1e-12, raise_on_fail=True):
+        """Arc-length path following.  ``method``: "ioal", "uoal" or "clinal"
+        (the reference's cIniOrtArcLength, cUpOrtArcLength, cConLinArcLength).
+        Returns (displacements [steps][neq], load factors [steps], iterations
+        per step, report)."""
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        lin = SolveOpts(precision, precond, 0, 0, float(lin_tol), 0.0, 0, 0)
+        o = ArcOpts(ARC_METHODS.get(method, method), int(steps), int(max_iter), int(target_iter), float(step_factor),
+                    float(tol), float(load_coeff), lin)
+        hist = np.zeros((steps, self.neq))
+        lams = np.zeros(steps)
+        iters = np.zeros(steps, np.int32)
+        rep = ArcReport()
+        rc = self.L.fast_gpu_arclength_solve(self.ctx, _p(q), ctypes.byref(o), _p(hist), _p(lams), _p(iters, _ip),
+                                             ctypes.byref(rep))
+        if rc != FAST_GPU_OK and raise_on_fail:
+            self._ck(rc, "arclength_solve")
+        n = rep.converged_steps
+        return hist[:n], lams[:n], iters[:n], rep.as_dict()
 
     # -- cSysMatrix
     def zero(self, what=ASM_K):

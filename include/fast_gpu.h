@@ -264,6 +264,47 @@ int fast_gpu_nr_solve(fast_gpu_ctx *ctx, const double *q, const fast_gpu_nr_opts
                       fast_gpu_nr_predictor predictor, void *predictor_user, double *u_hist, int32_t *iters,
                       fast_gpu_nr_report *rep);
 
+/* ---- path following (arc length) ---------------------------------------
+ * cCtrlPath::Solver (ctrl/ctrlpath.cpp:63-265) with the load-increment rules
+ * of the reference's arc-length classes (ctrl/ctrlarclen.cpp:95-250), on the
+ * device: per iteration the tangent at u, K du1 = q and K du2 = r (two PCG
+ * solves on unit right-hand sides), the rule's load increment dlf,
+ * du = dlf du1 - du2, r = g(u) - lambda q, converged when
+ * |r| / max(1, |q|) < tol (cControl::Convergence, ctrl/ctrl.cpp:1366-1380).
+ * The arc length is StepFactor (|du1| + LoadCoeff) at the first step and is
+ * scaled by sqrt(TargetIter / iterations of the last step) afterwards
+ * (%HEADER.ANALYSIS.ARC-LENGTH gives LoadCoeff, TARGET.ITERATIONS TargetIter,
+ * whose reference default is 1).  No strain loads, critical points or large
+ * rotations (the reference's options around this loop). */
+#define FAST_ARC_INITIAL_NORMAL 1   /* 'ioal'   cIniOrtArcLength */
+#define FAST_ARC_UPDATED_NORMAL 2   /* 'uoal'   cUpOrtArcLength  */
+#define FAST_ARC_LINEARIZED     3   /* 'clinal' cConLinArcLength */
+
+typedef struct {
+  int32_t method;             /* FAST_ARC_*                                          */
+  int32_t steps;              /* MAXIMUM.STEPS                                       */
+  int32_t max_iter;           /* MAXIMUM.ITERATIONS                                  */
+  int32_t target_iter;        /* TARGET.ITERATIONS (0: keep the arc length)          */
+  double  step_factor;        /* STEP.FACTOR: first load increment                   */
+  double  tol;                /* TOLERANCE                                           */
+  double  load_coeff;         /* ARC-LENGTH load coefficient                          */
+  fast_gpu_solve_opts lin;    /* the inner solves (tol relative to the unit rhs)     */
+} fast_gpu_arc_opts;
+
+typedef struct {
+  int32_t converged_steps;
+  int32_t failed_step;        /* 0, or the step that did not converge                */
+  int32_t iterations;         /* tangent assemblies, all steps                       */
+  int32_t linear_iterations;  /* PCG iterations, all steps                           */
+  double  last_err;           /* |r| / max(1, |q|) at the last iteration              */
+  double  arc_length;         /* at the last step                                    */
+} fast_gpu_arc_report;
+
+/* q: reference load (host, num_eq).  u_hist (host, [steps][num_eq]),
+ * lambda_hist ([steps]) and iters ([steps]) may be NULL. */
+int fast_gpu_arclength_solve(fast_gpu_ctx *ctx, const double *q, const fast_gpu_arc_opts *opts, double *u_hist,
+                             double *lambda_hist, int32_t *iters, fast_gpu_arc_report *rep);
+
 /* ---- learned load-step predictor ------------------------------------------
  * No counterpart in the reference (cCtrlNR starts every step from the last
  * converged u).  A POD basis Phi (num_eq x modes) of converged displacements

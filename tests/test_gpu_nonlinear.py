@@ -92,3 +92,33 @@ def test_newton_reports_failure():
     with pytest.raises(gpu.FastGpuError) as ei:
         s.nr_solve(q, 2, 0.5, tol=1e-30, max_iter=3)
     assert ei.value.rc == -5
+
+
+@pytest.mark.parametrize("method", ["ioal", "uoal", "clinal"])
+def test_arclength_matches_reference_cctrlpath(method):
+    """Every step of the device arc-length driver equals the displacements and
+    load factors the reference's own cCtrlPath printed (TL hex8 plate, 8
+    steps, TargetIter 4)."""
+    d, g = gio.load("arc_plate_tl")
+    s = system(d)
+    hist, lams, iters, rep = s.arclength_solve(g["ref_f"], method, int(g["steps"]), float(g["step_factor"]),
+                                               tol=float(g["tol"]), max_iter=int(g["maxit"]),
+                                               load_coeff=float(g["load_coeff"]), target_iter=int(g["target_iter"]))
+    ref_lam = g["ref_lam_" + method]
+    assert rep["converged_steps"] == len(ref_lam), rep
+    assert np.abs(lams - ref_lam).max() < 1e-9, (lams, ref_lam)
+    eq = d.node_eq()
+    m = eq > 0
+    for k in range(hist.shape[0]):
+        unode = np.zeros((d.num_nodes, 3))
+        unode[m] = hist[k][eq[m] - 1]
+        assert gio.rel(unode, g["ref_u_steps_" + method][k]) < 1e-8, (k, iters, rep)
+
+
+def test_arclength_reports_failure():
+    d = decks.plate_tl_hex8(4, 4, 2, L=4.0, t=0.4, pressure=8.0, steps=2, tol=1e-14)
+    s = system(d)
+    q = gpu.face_load_vector(d)
+    with pytest.raises(gpu.FastGpuError) as ei:
+        s.arclength_solve(q, "clinal", 2, 0.5, tol=1e-30, max_iter=3)
+    assert ei.value.rc == -5
