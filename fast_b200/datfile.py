@@ -1,0 +1,105 @@
+"""FAST ``.dat`` decks read by the library's parallel reader (fast_dat_*).
+
+``read_dat(path)`` returns the same :class:`fast_b200.decks.Deck` as the
+pure-Python reader, for hex8 / hex20 (small-strain or total-Lagrangian)
+decks, with the reference's record semantics (the i-th %NODE.COORD record is
+node i+1; sections, materials and elements by label; integration orders by
+position).  Decks outside that subset raise :class:`DatError` with the
+library's status (``rc == -7`` for B-spline patches, ties, mixed types).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import decks, gpu
+
+
+class DatInfo(ctypes.Structure):
+    _fields_ = [("num_nodes", ctypes.c_int64), ("num_elems", ctypes.c_int64), ("num_faces", ctypes.c_int64),
+                ("nodes_per_face", ctypes.c_int32), ("elem_type", ctypes.c_int32),
+                ("nodes_per_elem", ctypes.c_int32), ("formulation", ctypes.c_int32),
+                ("ngp", ctypes.c_int32 * 3), ("has_density", ctypes.c_int32), ("has_solver_order", ctypes.c_int32),
+                ("has_nodal_forces", ctypes.c_int32), ("max_iter", ctypes.c_int32), ("max_steps", ctypes.c_int32),
+                ("target_iter", ctypes.c_int32), ("print_step", ctypes.c_int32), ("has_arc_length", ctypes.c_int32),
+                ("tol", ctypes.c_double), ("step_factor", ctypes.c_double), ("arc_load_coeff", ctypes.c_double),
+                ("time_step", ctypes.c_double), ("newmark", ctypes.c_double * 2),
+                ("algorithm", ctypes.c_char * 32), ("matrix_type", ctypes.c_char * 32), ("title", ctypes.c_char * 128)]
+
+
+EXPORTS = ["fast_dat_read", "fast_dat_error", "fast_dat_free", "fast_dat_get_info", "fast_dat_get_nodes",
+           "fast_dat_get_elements", "fast_dat_get_faces", "fast_dat_bucket"]
+
+
+class DatError(RuntimeError):
+    def __init__(self, rc, msg):
+        super().__init__(f"fast_dat_read failed ({rc}): {msg}")
+        self.rc = rc
+
+
+def _lib():
+    L = gpu.load_library()
+    if getattr(L, "_dat_bound", False):
+        return L
+    vp = ctypes.c_void_p
+    L.fast_dat_read.argtypes = [ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(vp)]
+    L.fast_dat_error.argtypes = [vp]
+    L.fast_dat_error.restype = ctypes.c_char_p
+    L.fast_dat_free.argtypes = [vp]
+    L.fast_dat_free.restype = None
+    L.fast_dat_get_info.argtypes = [vp, ctypes.POINTER(DatInfo)]
+    L.fast_dat_get_nodes.argtypes = [vp, vp, vp, vp, vp]
+    L.fast_dat_get_elements.argtypes = [vp, vp, vp, vp, vp]
+    L.fast_dat_get_faces.argtypes = [vp, vp, vp, vp, vp, vp]
+    L._dat_bound = True
+    return L
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def read_dat(path: str, threads: int = 0) -> decks.Deck:
+    """Read a hex8 / hex20 FAST deck with ``threads`` host threads (0: all)."""
+    L = _lib()
+    h = ctypes.c_void_p()
+    rc = L.fast_dat_read(os.fsencode(path), int(threads), ctypes.byref(h))
+    try:
+        if rc != 0:
+            msg = L.fast_dat_error(h).decode(errors="replace") if h else "out of memory"
+            raise DatError(rc, msg)
+        I = DatInfo()
+        L.fast_dat_get_info(h, ctypes.byref(I))
+        n, ne, nf, nn = I.num_nodes, I.num_elems, I.num_faces, I.nodes_per_elem
+        coords = np.empty((n, 3))
+        fixed = np.empty((n, 3), np.uint8)
+        rank = np.empty(n, np.int64)
+        nodal = np.empty((n, 3))
+        L.fast_dat_get_nodes(h, _ptr(coords), _ptr(fixed), _ptr(rank), _ptr(nodal))
+        conn = np.empty((ne, nn), np.int32)
+        E, nu, rho = np.empty(ne), np.empty(ne), np.empty(ne)
+        L.fast_dat_get_elements(h, _ptr(conn), _ptr(E), _ptr(nu), _ptr(rho))
+        fe = fc = fq = fl = None
+        if nf:
+            fe = np.empty(nf, np.int32)
+            fc = np.empty((nf, 3), np.int32)
+            fnodes = np.empty((nf, I.nodes_per_face), np.int32)
+            fl = np.empty(nf, np.int32)
+            fq = np.empty((nf, 3))
+            L.fast_dat_get_faces(h, _ptr(fe), _ptr(fc), _ptr(fnodes), _ptr(fl), _ptr(fq))
+    finally:
+        if h:
+            L.fast_dat_free(h)
+    kind = {gpu_elem: k for k, gpu_elem in (("hex8", 1), ("hex20", 2))}[I.elem_type]
+    return decks.Deck(kind, coords, conn, E, nu, tuple(int(v) for v in I.ngp), fixed.astype(bool), fe, fc, fq, fl,
+                      rho if I.has_density else None, bool(I.formulation == 1),
+                      algorithm=I.algorithm.decode() or "linear", matrix_type=I.matrix_type.decode() or "skyline",
+                      tol=I.tol, maxit=I.max_iter, maxstep=I.max_steps, step_factor=I.step_factor,
+                      time_step=I.time_step, arc_load_coeff=I.arc_load_coeff if I.has_arc_length else None,
+                      target_iter=I.target_iter if I.target_iter >= 0 else None,
+                      newmark=(I.newmark[0], I.newmark[1]), print_step=I.print_step,
+                      node_labels=np.arange(1, n + 1, dtype=np.int64), title=os.path.basename(path),
+                      nodal_f=nodal if I.has_nodal_forces else None,
+                      solver_rank=rank if I.has_solver_order else None)
