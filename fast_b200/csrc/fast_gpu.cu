@@ -43,6 +43,7 @@ void free_mesh(Ctx &c) {
     dfree(B.d_conn); dfree(B.d_E); dfree(B.d_nu); dfree(B.d_rho); dfree(B.d_slot);
     dfree(B.d_dN); dfree(B.d_N); dfree(B.d_w);
     dfree(B.d_span); dfree(B.d_bas); dfree(B.d_wt);
+    dfree(B.d_tr); dfree(B.d_nptr); dfree(B.d_nent);
   }
   c.buckets.clear();
   free_ties(c);

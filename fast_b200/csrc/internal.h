@@ -68,6 +68,11 @@ struct Bucket {
   double *d_bas = nullptr;         // per direction d at offset bas_off[d]: [nspan][ngp_d][p+1][2] (N, dN/dt)
   int64_t bas_off[3] = {0, 0, 0};
   double *d_wt = nullptr;          // [nnode] control-point weights (rational patches)
+  // nodal stress recovery (built on first use): extrapolation matrix and the
+  // node -> (element, local node) incidence in element order
+  double *d_tr = nullptr;          // [nn][ng]
+  int64_t *d_nptr = nullptr;       // [nnode+1]
+  int64_t *d_nent = nullptr;       // [ne*nn] entries k*nn + a, ascending k per node
 };
 
 // Elements that touch a tied (slave) node.  Their element matrices go to a
@@ -235,6 +240,8 @@ bool build_pattern(Ctx &c, const fast_gpu_mesh &m);
 bool gauss_rule(int n, double *r, double *w);
 void gauss_point_tables(int type, const int ngp[3], std::vector<double> &N, std::vector<double> &dN,
                         std::vector<double> &w);
+// stress extrapolation TR [nn][ng] of a hex type and Gauss rule
+bool extrapolation_matrix(int type, const int ngp[3], std::vector<double> &TR);
 int nodes_of(int type);
 // B-spline solid kernels exist for these (degree per direction, Gauss order)
 bool bsp_supported(const int pd[3], int ngp);

@@ -249,6 +249,48 @@ bool bspline_gauss_tables(int p, int nknots, const double *U, int ng, int &nspan
   return true;
 }
 
+// Stress extrapolation to the nodes (cElmParam::CompTRMatrix,
+// elc/elmparam.cpp:1444-1535): the linear field a0 + a1 r + a2 s + a3 t that
+// fits the Gauss-point values in the least-squares sense, evaluated at the
+// node: TR[a][g] = c_a^T A^-1 u_g with A = sum_g u_g u_g^T, u = (1, r, s, t),
+// c_a the node's (1, r, s, t).  A is symmetric, so each row is one 4x4 solve
+// A y = c_a followed by y . u_g.  A one-point first order gives the average.
+bool extrapolation_matrix(int type, const int ngp[3], std::vector<double> &TR) {
+  const int nn = nodes_of(type);
+  const int ng = ngp[0] * ngp[1] * ngp[2];
+  if (nn <= 0 || ng <= 0) return false;
+  TR.assign((size_t)nn * ng, 0.0);
+  if (ngp[0] == 1) {
+    for (double &v : TR) v = 1.0 / ng;
+    return true;
+  }
+  std::vector<double> u((size_t)ng * 4);
+  int k = 0;
+  for (int i = 0; i < ngp[2]; i++)
+    for (int j = 0; j < ngp[1]; j++)
+      for (int l = 0; l < ngp[0]; l++, k++) {
+        u[4 * k] = 1.0;
+        u[4 * k + 1] = kGaussR[ngp[0] - 1][l];
+        u[4 * k + 2] = kGaussR[ngp[1] - 1][j];
+        u[4 * k + 3] = kGaussR[ngp[2] - 1][i];
+      }
+  double A0[4][4] = {};
+  for (int g = 0; g < ng; g++)
+    for (int p = 0; p < 4; p++)
+      for (int q = 0; q < 4; q++) A0[p][q] += u[4 * g + p] * u[4 * g + q];
+  for (int a = 0; a < nn; a++) {
+    const int *nat = type == FAST_ELEM_HEX8 ? kHex8Nat[a] : kHex20Nat[a];
+    double A[8][8] = {};
+    for (int p = 0; p < 4; p++)
+      for (int q = 0; q < 4; q++) A[p][q] = A0[p][q];
+    double y[8] = {1.0, (double)nat[0], (double)nat[1], (double)nat[2]};
+    if (!small_solve(4, A, y)) return false;
+    for (int g = 0; g < ng; g++)
+      TR[(size_t)a * ng + g] = y[0] * u[4 * g] + y[1] * u[4 * g + 1] + y[2] * u[4 * g + 2] + y[3] * u[4 * g + 3];
+  }
+  return true;
+}
+
 bool gauss_rule(int n, double *r, double *w) {
   if (n < 1 || n > 6) return false;
   for (int i = 0; i < n; i++) {

@@ -10,6 +10,12 @@
 // element's coordinates, its inverse by cofactors, then the strain summed
 // over the element's nodes; the threads of one element read the same nodes,
 // which the L1 cache serves.
+//
+// fast_gpu_nodal_stress goes on to the printing step's nodal values: the
+// element-nodal stresses extrapolated from the Gauss points
+// (cElmParam::NodalStress with CompTRMatrix, elc/elmparam.cpp:1304-1312,
+// 1444-1535) and their average at each node over the elements sharing it
+// (cControl::PrintAvrNodalStress, ctrl/ctrl.cpp:2397-2440).
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -26,7 +32,7 @@ template <int NN, int NG>
 __global__ void gauss_stress(int64_t count, const int32_t *__restrict__ index, const int32_t *__restrict__ conn,
                              const double *__restrict__ E, const double *__restrict__ nu,
                              const double *__restrict__ X, const double *__restrict__ U,
-                             const double *__restrict__ dN, double *__restrict__ strain,
+                             const double *__restrict__ dN, double *__restrict__ strain /* or NULL */,
                              double *__restrict__ stress, int32_t *__restrict__ status) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= count * NG) return;
@@ -71,9 +77,12 @@ __global__ void gauss_stress(int64_t count, const int32_t *__restrict__ index, c
   const double En = E[e], v = nu[e];
   const double dd = (1.0 + v) * (1.0 - 2.0 * v);
   const double C00 = En * (1.0 - v) / dd, C01 = En * v / dd, Gs = 0.5 * En / (1.0 + v);
-  double *so = stress + t * 6, *eo = strain + t * 6;
+  double *so = stress + t * 6;
+  if (strain) {
+    double *eo = strain + t * 6;
 #pragma unroll
-  for (int c = 0; c < 6; c++) eo[c] = ev[c];
+    for (int c = 0; c < 6; c++) eo[c] = ev[c];
+  }
   so[0] = C00 * ev[0] + C01 * (ev[1] + ev[2]);
   so[1] = C00 * ev[1] + C01 * (ev[0] + ev[2]);
   so[2] = C00 * ev[2] + C01 * (ev[0] + ev[1]);
@@ -88,6 +97,61 @@ cudaError_t run(Ctx &c, const Bucket &B, int64_t count, const int32_t *idx, doub
   gauss_stress<NN, NG><<<(unsigned)((n + 127) / 128), 128, 0, c.stream>>>(count, idx, B.d_conn, B.d_E, B.d_nu, c.d_X,
                                                                           c.d_disp, B.d_dN, st, ss, c.d_status);
   c.launches++;
+  return cudaGetLastError();
+}
+
+// element-nodal stresses [ne][NN][6] = TR [NN][NG] x Gauss-point stresses
+// [ne][NG][6] (cElmParam::NodalStress, elc/elmparam.cpp:1304-1312): one
+// thread per (element, local node)
+template <int NN, int NG>
+__global__ void extrapolate_to_nodes(int64_t ne, const double *__restrict__ TR, const double *__restrict__ Sg,
+                                     double *__restrict__ Sn) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= ne * NN) return;
+  const int64_t k = t / NN;
+  const int a = (int)(t - k * NN);
+  const double *sg = Sg + k * NG * 6;
+  const double *tr = TR + a * NG;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int g = 0; g < NG; g++) {
+    const double w = tr[g];
+#pragma unroll
+    for (int c = 0; c < 6; c++) acc[c] = fma(w, sg[6 * g + c], acc[c]);
+  }
+#pragma unroll
+  for (int c = 0; c < 6; c++) Sn[t * 6 + c] = acc[c];
+}
+
+// averaged nodal stresses (cControl::PrintAvrNodalStress, ctrl/ctrl.cpp:
+// 2397-2440): one thread per node gathers its (element, local node) entries
+// in element order, so the sum is the reference's and the same every run
+__global__ void average_at_nodes(int64_t nnode, const int64_t *__restrict__ ptr, const int64_t *__restrict__ ent,
+                                 const double *__restrict__ Sn, double *__restrict__ out) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= nnode) return;
+  const int64_t p0 = ptr[n], p1 = ptr[n + 1];
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int64_t p = p0; p < p1; p++) {
+    const double *v = Sn + ent[p] * 6;
+#pragma unroll
+    for (int c = 0; c < 6; c++) acc[c] += v[c];
+  }
+  const double cnt = (double)(p1 - p0);
+#pragma unroll
+  for (int c = 0; c < 6; c++) out[n * 6 + c] = p1 > p0 ? acc[c] / cnt : 0.0;
+}
+
+template <int NN, int NG>
+cudaError_t run_nodal(Ctx &c, const Bucket &B, const int32_t *idx, double *Sg, double *Sn, double *avg) {
+  const int64_t ne = B.ne;
+  gauss_stress<NN, NG><<<(unsigned)((ne * NG + 127) / 128), 128, 0, c.stream>>>(
+      ne, idx, B.d_conn, B.d_E, B.d_nu, c.d_X, c.d_disp, B.d_dN, nullptr, Sg, c.d_status);
+  extrapolate_to_nodes<NN, NG><<<(unsigned)((ne * NN + 127) / 128), 128, 0, c.stream>>>(ne, B.d_tr, Sg, Sn);
+  c.launches += 2;
+  if (avg) {
+    average_at_nodes<<<(unsigned)((c.nnode + 127) / 128), 128, 0, c.stream>>>(c.nnode, B.d_nptr, B.d_nent, Sn, avg);
+    c.launches++;
+  }
   return cudaGetLastError();
 }
 
@@ -137,6 +201,82 @@ extern "C" int fast_gpu_gauss_stress(fast_gpu_ctx *c, int32_t b, int64_t first, 
   cudaFree(buf);
   if (status) {
     c->err = "gauss_stress: non-positive Jacobian determinant in at least one element";
+    return FAST_GPU_EDETJ;
+  }
+  return FAST_GPU_OK;
+}
+
+// Extrapolation matrix and node incidence of a bucket, built once.
+static int nodal_tables(Ctx &c, Bucket &B) {
+  if (B.d_tr) return FAST_GPU_OK;
+  std::vector<double> TR;
+  if (!extrapolation_matrix(B.type, B.ngp, TR)) {
+    c.err = "nodal_stress: no extrapolation for this element and rule";
+    return FAST_GPU_ENOTSUP;
+  }
+  const int nn = B.nn;
+  const int64_t ne = B.ne, nnode = c.nnode;
+  std::vector<int64_t> ptr(nnode + 1, 0), ent((size_t)ne * nn);
+  for (int64_t k = 0; k < ne; k++)
+    for (int a = 0; a < nn; a++) ptr[B.h_conn[(size_t)B.inv[k] * nn + a] + 1]++;
+  for (int64_t n = 0; n < nnode; n++) ptr[n + 1] += ptr[n];
+  std::vector<int64_t> fill(ptr.begin(), ptr.end() - 1);
+  for (int64_t k = 0; k < ne; k++)  // element order: each node's entries ascend in k
+    for (int a = 0; a < nn; a++) ent[fill[B.h_conn[(size_t)B.inv[k] * nn + a]]++] = k * nn + a;
+  cudaError_t e = cudaMalloc((void **)&B.d_tr, sizeof(double) * TR.size());
+  if (e == cudaSuccess) e = cudaMalloc((void **)&B.d_nptr, sizeof(int64_t) * ptr.size());
+  if (e == cudaSuccess) e = cudaMalloc((void **)&B.d_nent, sizeof(int64_t) * ent.size());
+  if (e == cudaSuccess) e = cudaMemcpy(B.d_tr, TR.data(), sizeof(double) * TR.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(B.d_nptr, ptr.data(), sizeof(int64_t) * ptr.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(B.d_nent, ent.data(), sizeof(int64_t) * ent.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    for (void *p : {(void *)B.d_tr, (void *)B.d_nptr, (void *)B.d_nent})
+      if (p) cudaFree(p);
+    B.d_tr = nullptr;
+    B.d_nptr = B.d_nent = nullptr;
+    c.err = std::string("nodal_stress: ") + cudaGetErrorString(e);
+    return FAST_GPU_ECUDA;
+  }
+  return FAST_GPU_OK;
+}
+
+extern "C" int fast_gpu_nodal_stress(fast_gpu_ctx *c, int32_t b, double *elem_nodal, double *nodal) {
+  if (!c || b < 0 || b >= (int)c->buckets.size() || (!elem_nodal && !nodal)) return FAST_GPU_EINVAL;
+  Bucket &B = c->buckets[b];
+  if (B.tl || B.type == FAST_ELEM_BSP_SOLID) {
+    c->err = "nodal_stress: small-strain hex buckets only";
+    return FAST_GPU_ENOTSUP;
+  }
+  if (!c->d_disp) {
+    c->err = "nodal_stress: no displacement state";
+    return FAST_GPU_ESTATE;
+  }
+  int rc = nodal_tables(*c, B);
+  if (rc != FAST_GPU_OK) return rc;
+  const int64_t ne = B.ne, nn = B.nn, ng = B.ng;
+  const size_t nsg = (size_t)ne * ng * 6, nsn = (size_t)ne * nn * 6, nav = (size_t)c->nnode * 6;
+  double *buf = nullptr;
+  SCK(cudaMalloc((void **)&buf, sizeof(double) * (nsg + nsn + nav) + sizeof(int32_t) * ne + 16));
+  double *Sg = buf, *Sn = buf + nsg, *avg = nodal ? buf + nsg + nsn : nullptr;
+  int32_t *d_idx = reinterpret_cast<int32_t *>(buf + nsg + nsn + nav);
+  SCK(cudaMemcpyAsync(d_idx, B.inv.data(), sizeof(int32_t) * ne, cudaMemcpyHostToDevice, c->stream));
+  SCK(cudaMemsetAsync(c->d_status, 0, sizeof(int32_t), c->stream));
+  cudaError_t e = cudaErrorInvalidValue;
+  if (B.type == FAST_ELEM_HEX8 && ng == 8) e = run_nodal<8, 8>(*c, B, d_idx, Sg, Sn, avg);
+  else if (B.type == FAST_ELEM_HEX8 && ng == 27) e = run_nodal<8, 27>(*c, B, d_idx, Sg, Sn, avg);
+  else if (B.type == FAST_ELEM_HEX8 && ng == 1) e = run_nodal<8, 1>(*c, B, d_idx, Sg, Sn, avg);
+  else if (B.type == FAST_ELEM_HEX20 && ng == 27) e = run_nodal<20, 27>(*c, B, d_idx, Sg, Sn, avg);
+  else if (B.type == FAST_ELEM_HEX20 && ng == 8) e = run_nodal<20, 8>(*c, B, d_idx, Sg, Sn, avg);
+  else if (B.type == FAST_ELEM_HEX20 && ng == 64) e = run_nodal<20, 64>(*c, B, d_idx, Sg, Sn, avg);
+  SCK(e);
+  if (elem_nodal) SCK(cudaMemcpyAsync(elem_nodal, Sn, sizeof(double) * nsn, cudaMemcpyDeviceToHost, c->stream));
+  if (nodal) SCK(cudaMemcpyAsync(nodal, avg, sizeof(double) * nav, cudaMemcpyDeviceToHost, c->stream));
+  int32_t status = 0;
+  SCK(cudaMemcpyAsync(&status, c->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  SCK(cudaStreamSynchronize(c->stream));
+  cudaFree(buf);
+  if (status) {
+    c->err = "nodal_stress: non-positive Jacobian determinant in at least one element";
     return FAST_GPU_EDETJ;
   }
   return FAST_GPU_OK;

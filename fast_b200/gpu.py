@@ -46,7 +46,7 @@ EXPORTS = [
     "fast_gpu_set_displacement_device", "fast_gpu_internal_force", "fast_gpu_internal_force_device",
     "fast_gpu_nr_solve", "fast_gpu_ws_create", "fast_gpu_ws_destroy", "fast_gpu_ws_add_trajectory",
     "fast_gpu_ws_build_basis", "fast_gpu_ws_train", "fast_gpu_ws_predict", "fast_gpu_ws_report", "fast_gpu_autotune", "fast_gpu_set_face_loads", "fast_gpu_gauss_stress",
-    "fast_gpu_face_load_device", "fast_gpu_arclength_solve",
+    "fast_gpu_face_load_device", "fast_gpu_arclength_solve", "fast_gpu_nodal_stress",
     "fast_gpu_ws_get_basis", "fast_gpu_ws_get_samples", "fast_gpu_mlp_params", "fast_gpu_mlp_forward",
     "fast_gpu_mlp_loss_grad", "fast_gpu_mlp_gemm", "fast_gpu_ws_configure", "fast_gpu_ws_last_input",
     "fast_gpu_set_option", "fast_gpu_set_problems", "fast_gpu_solve_batch", "fast_gpu_newmark",
@@ -223,6 +223,7 @@ def load_library(path: str = LIB_PATH):
     L.fast_gpu_set_option.argtypes = [vp, ctypes.c_int32, ctypes.c_int64]
     L.fast_gpu_autotune.argtypes = [vp, vp]
     L.fast_gpu_gauss_stress.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, vp, vp]
+    L.fast_gpu_nodal_stress.argtypes = [vp, ctypes.c_int32, vp, vp]
     L.fast_gpu_set_face_loads.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, vp, vp, vp, ctypes.c_int32]
     L.fast_gpu_face_load_device.argtypes = [vp, ctypes.c_double, vp]
     L.fast_gpu_set_problems.argtypes = [vp, ctypes.c_int32, _lp]
@@ -459,6 +460,15 @@ class GpuSystem:
         self._ck(self.L.fast_gpu_gauss_stress(self.ctx, bucket, int(first), int(count), st.ctypes.data,
                                               ss.ctypes.data), "gauss_stress")
         return st, ss
+
+    def nodal_stress(self, bucket=0):
+        """(element-nodal [ne][nn][6], averaged nodal [nnode][6]) stresses at the
+        current displacements (fast_gpu_nodal_stress)."""
+        b = self.deck.buckets()[bucket]
+        en = np.zeros((b.num_elems, b.nn, 6))
+        avg = np.zeros((self.deck.num_nodes, 6))
+        self._ck(self.L.fast_gpu_nodal_stress(self.ctx, bucket, en.ctypes.data, avg.ctypes.data), "nodal_stress")
+        return en, avg
 
     def autotune(self) -> dict:
         """Measure the SpMV lanes-per-row choices and the PCG iteration path on

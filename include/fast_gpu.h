@@ -495,6 +495,16 @@ int fast_gpu_face_load_device(fast_gpu_ctx *ctx, double scale, double *d_f);
  * the Gauss rule's order (r fastest). */
 int fast_gpu_gauss_stress(fast_gpu_ctx *ctx, int32_t bucket, int64_t first, int64_t count, double *strain,
                           double *stress);
+/* The printing step's nodal stresses at the current displacements, for a
+ * whole small-strain hex bucket: elem_nodal [num_elems][nn][6] (caller's
+ * element order) = TR x the Gauss-point stresses, TR the extrapolation of
+ * cElmParam::CompTRMatrix (elc/elmparam.cpp:1444-1535: least-squares linear
+ * field in r, s, t evaluated at the nodes; the average for a one-point rule),
+ * as cElmParam::NodalStress returns them (:1304-1312); nodal [num_nodes][6]
+ * their average at each node over the bucket's elements, summed in element
+ * order as cControl::PrintAvrNodalStress does (ctrl/ctrl.cpp:2397-2440),
+ * 0 at nodes of no element.  Either output may be NULL. */
+int fast_gpu_nodal_stress(fast_gpu_ctx *ctx, int32_t bucket, double *elem_nodal, double *nodal);
 
 /* ---- parity / inspection ---------------------------------------------- */
 /* Host-only: builds the node-block pattern and element colouring of a mesh

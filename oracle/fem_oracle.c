@@ -255,6 +255,81 @@ int fo_elem_stress(int nn, const int *ngp, const double *X, double E, double nu,
   return bad;
 }
 
+/* Extrapolation matrix TR [nn][ng] (cElmParam::CompTRMatrix,
+ * elc/elmparam.cpp:1444-1535): a linear field a0 + a1 r + a2 s + a3 t fitted
+ * by least squares to the Gauss-point values and evaluated at the nodes,
+ * TR = CN A^-1 CI with A = sum_i u_i u_i^T, u = (1, r, s, t); a one-point
+ * rule (first order 1) gives the average.  The 4x4 system is solved by
+ * Gaussian elimination with partial pivoting. */
+int fo_extrap_matrix(int nn, const int *ngp, double *TR)
+{
+  double pts[216 * 3], wts[216];
+  int np = gauss_pts(ngp, pts, wts);
+  if (ngp[0] == 1)
+  {
+    for (int i = 0; i < nn * np; i++) TR[i] = 1.0 / np;
+    return 0;
+  }
+  double A[4][4] = {{0}};
+  for (int g = 0; g < np; g++)
+  {
+    double u[4] = {1.0, pts[3 * g], pts[3 * g + 1], pts[3 * g + 2]};
+    for (int k = 0; k < 4; k++)
+      for (int l = 0; l < 4; l++) A[k][l] += u[k] * u[l];
+  }
+  /* Q = A^-1 CI, one Gauss point (column) at a time */
+  double Q[4][216];
+  for (int g = 0; g < np; g++)
+  {
+    double M[4][5];
+    double u[4] = {1.0, pts[3 * g], pts[3 * g + 1], pts[3 * g + 2]};
+    for (int k = 0; k < 4; k++)
+    {
+      for (int l = 0; l < 4; l++) M[k][l] = A[k][l];
+      M[k][4] = u[k];
+    }
+    for (int c = 0; c < 4; c++)
+    {
+      int piv = c;
+      for (int r = c + 1; r < 4; r++)
+        if (fabs(M[r][c]) > fabs(M[piv][c])) piv = r;
+      if (M[piv][c] == 0.0) return -1;
+      for (int l = 0; l < 5; l++) { double t = M[c][l]; M[c][l] = M[piv][l]; M[piv][l] = t; }
+      for (int r = c + 1; r < 4; r++)
+      {
+        double f = M[r][c] / M[c][c];
+        for (int l = c; l < 5; l++) M[r][l] -= f * M[c][l];
+      }
+    }
+    for (int c = 3; c >= 0; c--)
+    {
+      double v = M[c][4];
+      for (int l = c + 1; l < 4; l++) v -= M[c][l] * Q[l][g];
+      Q[c][g] = v / M[c][c];
+    }
+  }
+  for (int a = 0; a < nn; a++)
+  {
+    double r, s, t;
+    if (nn == 8)
+    {
+      static const int sr[8] = {-1, 1, 1, -1, -1, 1, 1, -1};
+      static const int ss[8] = {-1, -1, 1, 1, -1, -1, 1, 1};
+      static const int st[8] = { 1, 1, 1, 1, -1, -1, -1, -1};
+      r = sr[a]; s = ss[a]; t = st[a];
+    }
+    else { r = H20[a][0]; s = H20[a][1]; t = H20[a][2]; }
+    double cn[4] = {1.0, r, s, t};
+    for (int g = 0; g < np; g++)
+    {
+      double v = 0.0;
+      for (int k = 0; k < 4; k++) v += cn[k] * Q[k][g];
+      TR[a * np + g] = v;
+    }
+  }
+  return 0;
+}
+
 int fo_elem_mass(int nn, const int *ngp, const double *X, double rho, double *Me)
 {
   int nd = 3 * nn, bad = 0;

@@ -40,6 +40,11 @@ int fo_elem_intforce(int nn, const int *ngp, const double *X, double E, double n
 int fo_elem_stress(int nn, const int *ngp, const double *X, double E, double nu,
                    const double *ue, double *strain, double *stress);
 
+/* Stress extrapolation matrix TR [nn][ng] of cElmParam::CompTRMatrix
+ * (elc/elmparam.cpp:1444-1535): element-nodal stresses = TR x Gauss-point
+ * stresses (cElmParam::NodalStress, :1304-1312). */
+int fo_extrap_matrix(int nn, const int *ngp, double *TR);
+
 /* Consistent mass M = sum_g w detJ rho N^T N (cElmParam::MassMat, elc/elmparam.cpp:672-739). */
 int fo_elem_mass(int nn, const int *ngp, const double *X, double rho, double *Me);
 

@@ -38,6 +38,7 @@ def lib():
         L.fo_elem_intforce.argtypes = [ctypes.c_int, _ip, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp]
         L.fo_elem_stress.argtypes = [ctypes.c_int, _ip, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp]
         L.fo_elem_mass.argtypes = [ctypes.c_int, _ip, _dp, ctypes.c_double, _dp]
+        L.fo_extrap_matrix.argtypes = [ctypes.c_int, _ip, _dp]
         L.fo_elem_tl.argtypes = [ctypes.c_int, _ip, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp]
         L.fo_face_load.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp]
         L.fo_pcg.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32), _dp,
@@ -94,6 +95,28 @@ def elem_stress(nn, ngp, X, E, nu, ue):
     ue = np.ascontiguousarray(ue, dtype=np.float64)
     rc = lib().fo_elem_stress(nn, _ngp(ngp), _p(X), float(E), float(nu), _p(ue), _p(e), _p(s))
     return e, s, rc
+
+
+def extrap_matrix(nn, ngp):
+    """TR [nn][ngp] of cElmParam::CompTRMatrix: element-nodal = TR @ Gauss-point values."""
+    TR = np.zeros((nn, int(np.prod(ngp))))
+    rc = lib().fo_extrap_matrix(nn, _ngp(ngp), _p(TR))
+    return TR, rc
+
+
+def averaged_nodal_stress(num_nodes, conn, elem_nodal):
+    """cControl::PrintAvrNodalStress (ctrl/ctrl.cpp:2397-2440): every node's
+    element-nodal values summed over its elements in element order, divided
+    by their count; 0 at nodes of no element.  elem_nodal [ne][nn][6]."""
+    s = np.zeros((num_nodes, elem_nodal.shape[2]))
+    c = np.zeros(num_nodes)
+    for e in range(conn.shape[0]):
+        for a, n in enumerate(conn[e]):
+            s[n] += elem_nodal[e, a]
+            c[n] += 1
+    m = c > 0
+    s[m] /= c[m][:, None]
+    return s
 
 
 def elem_mass(nn, ngp, X, rho):

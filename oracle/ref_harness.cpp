@@ -29,6 +29,8 @@
 //       --u) state:
 //         elm_strain, elm_stress [ne][nip][6]  cElement::IntPntStress
 //                                  (elc/elmparam.cpp:859-935), Voigt xx yy zz xy xz yz
+//         elm_nodal_stress [ne][nn][6]  cElmParam::NodalStress with extrapolation
+//                                  (elc/elmparam.cpp:1304-1312, CompTRMatrix :1444-1535)
 //
 //   fastref bench <deck> <pcg_iters> [reps]
 //       Times the reference CPU path on one host thread: StiffnessMatrix into
@@ -251,8 +253,9 @@ static int mode_dump(int argc, char **argv)
   if (stress && (ufile || solve))
   {
     const int nip = ne > 0 ? cElement::GetElm(0)->GetNumIntPnt( ) : 0;
-    vector<double> SE((size_t)ne * nip * 6), SS((size_t)ne * nip * 6);
-    cMatrix Strain(nip, 6), Stress(nip, 6);
+    const int nen = ne > 0 ? cElement::GetElm(0)->GetShape( )->GetNumNode( ) : 0;
+    vector<double> SE((size_t)ne * nip * 6), SS((size_t)ne * nip * 6), SN((size_t)ne * nen * 6);
+    cMatrix Strain(nip, 6), Stress(nip, 6), Nodal(nen, 6);
     for (int e = 0; e < ne; e++)
     {
       cElement *elm = cElement::GetElm(e);
@@ -264,9 +267,15 @@ static int mode_dump(int argc, char **argv)
           SE[((size_t)e * nip + i) * 6 + k] = Strain[i][k];
           SS[((size_t)e * nip + i) * 6 + k] = Stress[i][k];
         }
+      // extrapolated nodal stresses from the stresses just stored (the
+      // printing step's cElmParam::NodalStress)
+      elm->NodalStress(Nodal);
+      for (int a = 0; a < nen; a++)
+        for (int k = 0; k < 6; k++) SN[((size_t)e * nen + a) * 6 + k] = Nodal[a][k];
     }
     w.f8("elm_strain", {ne, nip, 6}, SE.data( ), SE.size( ));
     w.f8("elm_stress", {ne, nip, 6}, SS.data( ), SS.size( ));
+    w.f8("elm_nodal_stress", {ne, nen, 6}, SN.data( ), SN.size( ));
   }
   cout.rdbuf(coutbuf);
   return 0;

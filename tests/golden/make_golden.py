@@ -94,6 +94,7 @@ def run_case(name, deck, tmp, keep_elems=None, triplets=True, extra=(), uvec=Non
     if "elm_stress" in ref:
         out["ref_elm_strain"] = ref["elm_strain"][sel]
         out["ref_elm_stress"] = ref["elm_stress"][sel]
+        out["ref_elm_nodal_stress"] = ref["elm_nodal_stress"][sel]
     out["ref_f"] = ref["f"]
     if triplets:
         out.update({"ref_" + k: v for k, v in lower_csr(ref).items()})
@@ -163,16 +164,63 @@ def arc_cases(tmp):
     print("arc_plate_tl:", out["ref_u_steps_clinal"].shape, out["ref_lam_clinal"])
 
 
+def read_pos_nodal_stresses(path):
+    """The last step's element-nodal stresses (%RESULT.CASE.STEP.ELEMENT.NODAL.
+    SCALAR.DATA, cControl::PrintNodalStress ctrl/ctrl.cpp:2264-2320) and averaged
+    nodal stresses (%RESULT.CASE.STEP.NODAL.SCALAR.DATA, PrintAvrNodalStress
+    :2397-2470) of a .pos file, with their scalar labels."""
+    lines = open(path).read().splitlines()
+    out = {}
+    for i, ln in enumerate(lines):
+        t = ln.strip()
+        if t in ("%RESULT.CASE.STEP.ELEMENT.NODAL.SCALAR", "%RESULT.CASE.STEP.NODAL.SCALAR"):
+            out[t[18:] + ".labels"] = lines[i + 2].replace("'", " ").split()
+        elif t == "%RESULT.CASE.STEP.ELEMENT.NODAL.SCALAR.DATA":
+            ne = int(lines[i + 1].split()[0])
+            rows, j = [], i + 2
+            for _ in range(ne):
+                j += 1  # element label
+                blk = []
+                while j < len(lines) and lines[j].strip() and not lines[j].strip().lstrip("+-").isdigit():
+                    blk.append([float(v) for v in lines[j].split()])
+                    j += 1
+                rows.append(blk)
+            out["ELEMENT.NODAL"] = np.array(rows)
+        elif t == "%RESULT.CASE.STEP.NODAL.SCALAR.DATA":
+            n = int(lines[i + 1].split()[0])
+            rows = [lines[i + 2 + k].split() for k in range(n)]
+            lab = np.array([int(r[0]) for r in rows])
+            out["NODAL"] = np.array([[float(v) for v in r[1:]] for r in rows])[np.argsort(lab)]
+    return out
+
+
 def stress_cases(tmp):
     """Decks whose fixtures also hold the reference's Gauss-point strains and
-    stresses at its solution (cElement::IntPntStress)."""
+    stresses at its solution (cElement::IntPntStress), its extrapolated
+    element-nodal stresses (cElmParam::NodalStress) and, from the unmodified
+    `fast` binary's .pos with %HEADER.PRINT.AVERAGE.NODAL.STRESS, the printed
+    element-nodal and averaged nodal stresses."""
     # hex8 cantilever 20x4x4 (1500 equations), skyline + Crout
-    run_case("cfg_hex8_cantilever", decks.cantilever_hex8(), tmp, stress=True)
-
+    cases = [("cfg_hex8_cantilever", decks.cantilever_hex8())]
     # hex20 lognormal boxes (sparse Jacobi-PCG in the reference), small enough for full dumps
     d = decks.box_hex20_lognormal(4, 4, 2, seed=7)
     d.tol = 1e-13
-    run_case("cfg_hex20_lognormal_4x4x2", d, tmp, stress=True)
+    cases.append(("cfg_hex20_lognormal_4x4x2", d))
+    for name, d in cases:
+        run_case(name, d, tmp, stress=True)
+        base = os.path.join(tmp, name + "_pos")
+        path = decks.write_dat(d, base)
+        text = open(path).read().replace("%END", "%HEADER.PRINT.AVERAGE.NODAL.STRESS\n1\n\n%END")
+        open(path, "w").write(text)
+        subprocess.run([refdump.FAST, base, "-silent"], check=True, stdout=subprocess.DEVNULL)
+        pos = read_pos_nodal_stresses(base + ".pos")
+        f = os.path.join(HERE, name + ".npz")
+        z = dict(np.load(f))
+        z["ref_pos_elm_nodal_stress"] = pos["ELEMENT.NODAL"]
+        z["ref_pos_nodal_stress_avg"] = pos["NODAL"]
+        z["ref_pos_stress_labels"] = np.array(pos["NODAL.SCALAR.labels"])
+        np.savez_compressed(f, **z)
+        print(name, "pos stresses", pos["ELEMENT.NODAL"].shape, pos["NODAL"].shape, pos["NODAL.SCALAR.labels"])
 
 
 def main():

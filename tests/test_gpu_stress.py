@@ -49,3 +49,43 @@ def test_gauss_stress_rejects_total_lagrangian():
     with pytest.raises(gpu.FastGpuError):
         s.gauss_stress()
     s.close()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_nodal_stress_matches_reference_printout(name):
+    """Element-nodal (cElmParam::NodalStress) and averaged nodal stresses
+    (cControl::PrintAvrNodalStress) against the reference harness and the
+    values the reference's `fast` binary printed to its .pos file."""
+    d, g = gio.load(name)
+    s = gpu.GpuSystem(0)
+    s.upload(d)
+    s.set_displacement(g["ref_u"])
+    en, avg = s.nodal_stress()
+    ref_en = g["ref_elm_nodal_stress"]
+    scale = np.abs(ref_en).max()
+    assert np.abs(en[g["ref_elems"]] - ref_en).max() <= 1e-12 * scale
+    assert np.abs(en - g["ref_pos_elm_nodal_stress"]).max() <= 1e-12 * scale
+    assert np.abs(avg - g["ref_pos_nodal_stress_avg"]).max() <= 1e-12 * scale
+    # run to run the same bits (gather in element order, no atomics)
+    en2, avg2 = s.nodal_stress()
+    assert np.array_equal(en, en2) and np.array_equal(avg, avg2)
+    s.close()
+
+
+def test_nodal_stress_average_on_a_mesh_with_unused_nodes():
+    """Nodes of no element get zero; the averaged values are the oracle's
+    arithmetic on the device's own element-nodal values."""
+    from oracle import fem_oracle as fo
+    d = decks.cantilever_hex8(6, 2, 2)
+    extra = np.array([[50.0, 50.0, 50.0]])
+    d.coords = np.vstack([d.coords, extra])
+    d.fixed = np.vstack([d.fixed, [[True, True, True]]])
+    s = gpu.GpuSystem(0)
+    s.upload(d)
+    u = np.random.default_rng(5).standard_normal(d.num_eq()) * 1e-3
+    s.set_displacement(u)
+    en, avg = s.nodal_stress()
+    assert np.all(avg[-1] == 0.0)
+    ref = fo.averaged_nodal_stress(d.num_nodes, d.conn, en)
+    assert np.abs(avg - ref).max() <= 1e-14 * np.abs(ref).max()
+    s.close()

@@ -217,6 +217,32 @@ def test_gauss_point_stresses(name):
         assert np.abs(ss - g["ref_elm_stress"][k]).max() <= 1e-12 * np.abs(g["ref_elm_stress"]).max()
 
 
+@pytest.mark.parametrize("name", [c for c in CASES if "ref_elm_nodal_stress" in gio.load(c)[1]])
+def test_extrapolated_and_averaged_nodal_stresses(name):
+    """cElmParam::NodalStress (TR x Gauss-point stresses, CompTRMatrix) and
+    cControl::PrintAvrNodalStress from the oracle at the reference's
+    solution, against the harness dump and the `fast` binary's .pos print."""
+    d, g = gio.load(name)
+    assert list(g["ref_pos_stress_labels"]) == ["STRESS_XX", "STRESS_YY", "STRESS_ZZ", "STRESS_XY", "STRESS_XZ",
+                                                "STRESS_YZ"]
+    TR, rc = fo.extrap_matrix(d.nn, d.ngp)
+    assert rc == 0
+    np.testing.assert_allclose(TR.sum(axis=1), 1.0, rtol=0, atol=1e-14)  # constants extrapolate exactly
+    eq = d.node_eq()
+    u = g["ref_u"]
+    en = np.zeros((d.num_elems, d.nn, 6))
+    for e in range(d.num_elems):
+        dofs = eq[d.conn[e]].ravel()
+        ue = np.where(dofs > 0, u[np.maximum(dofs - 1, 0)], 0.0)
+        _, ss, rc = fo.elem_stress(d.nn, d.ngp, d.coords[d.conn[e]], d.E[e], d.nu[e], ue)
+        en[e] = TR @ ss
+    scale = np.abs(g["ref_elm_nodal_stress"]).max()
+    assert np.abs(en[g["ref_elems"]] - g["ref_elm_nodal_stress"]).max() <= 1e-12 * scale
+    assert np.abs(en - g["ref_pos_elm_nodal_stress"]).max() <= 1e-12 * scale
+    avg = fo.averaged_nodal_stress(d.num_nodes, d.conn, en)
+    assert np.abs(avg - g["ref_pos_nodal_stress_avg"]).max() <= 1e-12 * scale
+
+
 @pytest.mark.parametrize("method", ["ioal", "uoal", "clinal"])
 def test_oracle_arclength_matches_reference(method):
     """The oracle's restatement of cCtrlPath with the arc-length rules
