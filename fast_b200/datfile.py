@@ -1,4 +1,5 @@
-"""FAST ``.dat`` decks read by the library's parallel reader (fast_dat_*).
+"""FAST ``.dat`` decks read by the library's parallel reader (fast_dat_*),
+and ``.pos`` result files written by its parallel writer (fast_pos_*).
 
 ``read_dat(path)`` returns the same :class:`fast_b200.decks.Deck` as the
 pure-Python reader, for hex8 / hex20 (small-strain or total-Lagrangian)
@@ -29,6 +30,13 @@ class DatInfo(ctypes.Structure):
                 ("algorithm", ctypes.c_char * 32), ("matrix_type", ctypes.c_char * 32), ("title", ctypes.c_char * 128)]
 
 
+class PosOpts(ctypes.Structure):
+    _fields_ = [("header_line", ctypes.c_char_p), ("precision", ctypes.c_int32), ("max_steps", ctypes.c_int32),
+                ("print_average", ctypes.c_int32), ("threads", ctypes.c_int32)]
+
+
+POS_EXPORTS = ["fast_pos_open", "fast_pos_step", "fast_pos_finish", "fast_pos_error", "fast_pos_free"]
+
 EXPORTS = ["fast_dat_read", "fast_dat_error", "fast_dat_free", "fast_dat_get_info", "fast_dat_get_nodes",
            "fast_dat_get_elements", "fast_dat_get_faces", "fast_dat_bucket"]
 
@@ -53,6 +61,14 @@ def _lib():
     L.fast_dat_get_nodes.argtypes = [vp, vp, vp, vp, vp]
     L.fast_dat_get_elements.argtypes = [vp, vp, vp, vp, vp]
     L.fast_dat_get_faces.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.fast_pos_open.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(PosOpts), ctypes.POINTER(vp)]
+    L.fast_pos_step.argtypes = [vp, ctypes.c_double, ctypes.c_int64, vp, ctypes.c_int64, ctypes.c_int32, vp,
+                                ctypes.c_int32, vp, vp]
+    L.fast_pos_finish.argtypes = [vp]
+    L.fast_pos_error.argtypes = [vp]
+    L.fast_pos_error.restype = ctypes.c_char_p
+    L.fast_pos_free.argtypes = [vp]
+    L.fast_pos_free.restype = None
     L._dat_bound = True
     return L
 
@@ -103,3 +119,44 @@ def read_dat(path: str, threads: int = 0) -> decks.Deck:
                       node_labels=np.arange(1, n + 1, dtype=np.int64), title=os.path.basename(path),
                       nodal_f=nodal if I.has_nodal_forces else None,
                       solver_rank=rank if I.has_solver_order else None)
+
+
+def _arr(a, shape=None):
+    if a is None:
+        return None, None
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if shape is not None:
+        a = a.reshape(shape)
+    return a, a.ctypes.data_as(ctypes.c_void_p)
+
+
+def write_pos(pos_path: str, dat_path: str, steps, precision: int = 5, max_steps: int = 1,
+              print_average: bool = False, header_line: str = None, threads: int = 0) -> None:
+    """Write a FAST ``.pos`` file: the deck's echo, then one printed step per
+    entry of ``steps`` (dicts with ``factor``, ``displ`` [nnode][3] and
+    optionally ``gauss_stress`` [ne][points][6], ``elem_nodal`` [ne][nn][6],
+    ``nodal_avg`` [nnode][6])."""
+    L = _lib()
+    o = PosOpts(header_line.encode() if header_line is not None else None, int(precision), int(max_steps),
+                int(bool(print_average)), int(threads))
+    h = ctypes.c_void_p()
+    try:
+        rc = L.fast_pos_open(os.fsencode(pos_path), os.fsencode(dat_path), ctypes.byref(o), ctypes.byref(h))
+        if rc != 0:
+            raise DatError(rc, L.fast_pos_error(h).decode(errors="replace") if h else "out of memory")
+        for st in steps:
+            u, up = _arr(st["displ"])
+            gs, gp = _arr(st.get("gauss_stress"))
+            en, ep = _arr(st.get("elem_nodal"))
+            av, ap = _arr(st.get("nodal_avg"))
+            ne = gs.shape[0] if gs is not None else (en.shape[0] if en is not None else 0)
+            rc = L.fast_pos_step(h, float(st["factor"]), u.shape[0], up, ne, gs.shape[1] if gs is not None else 0,
+                                 gp, en.shape[1] if en is not None else 0, ep, ap)
+            if rc != 0:
+                raise DatError(rc, L.fast_pos_error(h).decode(errors="replace"))
+        rc = L.fast_pos_finish(h)
+        if rc != 0:
+            raise DatError(rc, L.fast_pos_error(h).decode(errors="replace"))
+    finally:
+        if h:
+            L.fast_pos_free(h)

@@ -1,0 +1,64 @@
+/* fast_pos.h - C ABI of the result writer in libfastgpu.so: FAST's .pos
+ * output for solid decks, formatted on all host cores.
+ *
+ * It writes what the reference's main program and controller write
+ * (main/main.cpp:108-121, cControl::PrintResult ctrl/ctrl.cpp:1117-1304,
+ * cControl::End :597-622), byte for byte for the blocks below:
+ *   "%HEADER", the generator line, the deck's own text from its second line
+ *   up to "%END" (InpCopyData, main/input.cpp:405-420);
+ *   at the first step "%RESULT" and "%RESULT.CASE" with the blank step-list
+ *   area (13 spaces per line, floor(1.1 * max_steps) + 1 lines);
+ *   per step: %RESULT.CASE.STEP, .FACTOR, .NODAL.DISPLACEMENT (six values,
+ *   the rotations 0 for solids), .ELEMENT.GAUSS.SCALAR(.DATA)
+ *   (cControl::PrintIntPntStress :2189-2260), .ELEMENT.NODAL.SCALAR(.DATA)
+ *   (PrintNodalStress :2264-2320) and, when asked for, .NODAL.SCALAR(.DATA)
+ *   (PrintAvrNodalStress :2397-2470);
+ *   at the end "%END" and the step list written over the blank area.
+ * Numbers are printed as iostream prints them with scientific, showpos and
+ * setprecision(precision): a sign, one digit, the point, `precision` digits,
+ * the exponent with at least two digits.  Node i is label i+1, element k
+ * label k+1, stresses in Voigt order xx yy zz xy xz yz.  Support reactions,
+ * Newmark velocities and accelerations and the IGA and micro-model blocks are
+ * not written.  Status codes are fast_gpu.h's (FAST_GPU_EINVAL for bad
+ * arguments or an I/O error). */
+#ifndef FAST_POS_H
+#define FAST_POS_H
+
+#include <stdint.h>
+
+#include "fast_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fast_pos fast_pos;
+
+typedef struct {
+  const char *header_line;  /* the file's second line, without newline (NULL: the library's own) */
+  int32_t precision;        /* %HEADER.OUTPUT.PRECISION (the reference's default is 5) */
+  int32_t max_steps;        /* MAXIMUM.STEPS: sizes the step-list area                 */
+  int32_t print_average;    /* %HEADER.PRINT.AVERAGE.NODAL.STRESS: write .NODAL.SCALAR  */
+  int32_t threads;          /* formatting threads, 0: all cores                         */
+} fast_pos_opts;
+
+/* Creates pos_path and writes the header and the echo of the deck at
+ * dat_path.  *out is set whenever it is not NULL and memory allowed; on an
+ * error fast_pos_error() says why; release it with fast_pos_free. */
+int fast_pos_open(const char *pos_path, const char *dat_path, const fast_pos_opts *opts, fast_pos **out);
+/* One printed step.  displ [num_nodes][3]; gauss_stress [num_elems][points][6]
+ * and elem_nodal [num_elems][nodes_per_elem][6] may be NULL (block not
+ * written); nodal_avg [num_nodes][6] is required when print_average. */
+int fast_pos_step(fast_pos *pos, double factor, int64_t num_nodes, const double *displ, int64_t num_elems,
+                  int32_t points, const double *gauss_stress, int32_t nodes_per_elem, const double *elem_nodal,
+                  const double *nodal_avg);
+/* "%END" and the step list; the file is complete after this. */
+int fast_pos_finish(fast_pos *pos);
+const char *fast_pos_error(const fast_pos *pos);
+void fast_pos_free(fast_pos *pos);   /* closes the file if still open */
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FAST_POS_H */

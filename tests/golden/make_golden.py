@@ -8,6 +8,7 @@ override with FAST_REF):
     python tests/golden/make_golden.py iga      (B-spline solid fixtures only)
     python tests/golden/make_golden.py stress   (the two fixtures with Gauss-point stresses)
     python tests/golden/make_golden.py arc      (the path-following fixture)
+    python tests/golden/make_golden.py pos      (.pos files next to the numbers they print)
 
 It builds ``oracle/_ref/fastref`` (the reference's own sources compiled by
 ``oracle/Makefile``, plus a dump harness), writes each deck with
@@ -223,9 +224,51 @@ def stress_cases(tmp):
         print(name, "pos stresses", pos["ELEMENT.NODAL"].shape, pos["NODAL"].shape, pos["NODAL.SCALAR.labels"])
 
 
+def pos_cases(tmp):
+    """The unmodified `fast` binary's .pos files next to the numbers they
+    print: two linear static decks with every stress block (the harness's
+    displacements and stresses of the same run), and a three-step Newton run
+    on small-strain bricks whose numbers are read back from the file
+    (precision 14, so every printed value survives the round trip)."""
+    out = {}
+    for name, d in (("hex8", decks.cantilever_hex8(3, 2, 2)),
+                    ("hex20", decks.box_hex20_lognormal(2, 2, 1, seed=3))):
+        base = os.path.join(tmp, "pos_" + name)
+        path = decks.write_dat(d, base)
+        text = open(path).read().replace("%END", "%HEADER.PRINT.AVERAGE.NODAL.STRESS\n1\n\n%END")
+        open(path, "w").write(text)
+        ref = refdump.run_dump(base, base + ".bin", "--stress", "--no-triplets")
+        subprocess.run([refdump.FAST, base, "-silent"], check=True, stdout=subprocess.DEVNULL)
+        for k, v in deck_arrays(d).items():
+            out[f"{name}_{k}"] = v
+        out[f"{name}_dat"] = np.frombuffer(open(path, "rb").read(), np.uint8)
+        out[f"{name}_pos"] = np.frombuffer(open(base + ".pos", "rb").read(), np.uint8)
+        out[f"{name}_ref_node_eq"] = ref["node_eq"]
+        out[f"{name}_ref_u"] = ref["u"]
+        out[f"{name}_ref_elm_stress"] = ref["elm_stress"]
+        out[f"{name}_ref_elm_nodal_stress"] = ref["elm_nodal_stress"]
+    d = decks.cantilever_hex8(3, 2, 2)
+    d.algorithm, d.maxstep, d.step_factor, d.maxit, d.tol = "lcm", 3, 1.0 / 3.0, 10, 1e-10
+    base = os.path.join(tmp, "pos_steps")
+    path = decks.write_dat(d, base)
+    text = open(path).read().replace("%HEADER.OUTPUT.PRECISION\n15", "%HEADER.OUTPUT.PRECISION\n14")
+    open(path, "w").write(text)
+    subprocess.run([refdump.FAST, base, "-silent"], check=True, stdout=subprocess.DEVNULL)
+    out["steps_dat"] = np.frombuffer(open(path, "rb").read(), np.uint8)
+    out["steps_pos"] = np.frombuffer(open(base + ".pos", "rb").read(), np.uint8)
+    np.savez_compressed(os.path.join(HERE, "pos_output.npz"), **out)
+    print("pos_output:", {k: v.shape for k, v in out.items() if k.endswith("pos")})
+
+
 def main():
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"FAST_REF={FAST_REF}", "ref"], check=True)
     tmp = tempfile.mkdtemp(prefix="golden_")
+    if len(sys.argv) > 1 and sys.argv[1] == "pos":
+        try:
+            pos_cases(tmp)
+        finally:
+            shutil.rmtree(tmp, ignore_errors=True)
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "arc":
         try:
             arc_cases(tmp)
@@ -266,6 +309,7 @@ def main():
 
         stress_cases(tmp)
         arc_cases(tmp)
+        pos_cases(tmp)
         d = decks.box_hex20_lognormal(8, 8, 4, seed=11)
         d.tol = 1e-12
         run_case("cfg_hex20_lognormal_8x8x4", d, tmp, keep_elems=np.arange(0, 256, 17), triplets=False)
