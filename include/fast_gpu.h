@@ -264,6 +264,34 @@ int fast_gpu_nr_solve(fast_gpu_ctx *ctx, const double *q, const fast_gpu_nr_opts
                       fast_gpu_nr_predictor predictor, void *predictor_user, double *u_hist, int32_t *iters,
                       fast_gpu_nr_report *rep);
 
+/* ---- modal analysis ------------------------------------------------------
+ * cCtrlModal::Solver (ctrl/ctrlmodal.cpp:48-128) with the subspace iteration
+ * of cGenEigSubSpaces::Solver (mlib/eig.cpp:377-510): M and K assembled on
+ * the device, q = max(2p, p + 8) vectors (at most 32, so p <= 16), each
+ * iteration K Y = M X by PCG, the projected pencil Y^T K Y, Y^T M Y solved on
+ * the host, X = Y Phi; converged when sqrt(|1 - lambda^2 / |phi|^2|) <= tol for
+ * the p lowest, the reference's measure.  lambda [num_modes] are the
+ * eigenvalues (natural frequencies sqrt(lambda)); modes [num_modes][num_eq]
+ * (may be NULL) the M-normalised mode shapes, sign arbitrary.  Needs
+ * densities in every bucket (fast_gpu_bucket.rho). */
+typedef struct {
+  int32_t num_modes;          /* EIGEN.NUMBER.MODES (the reference's default is 5)  */
+  int32_t max_iter;           /* MAXIMUM.ITERATIONS of the subspace loop             */
+  double  tol;                /* TOLERANCE on the reference's convergence measure    */
+  fast_gpu_solve_opts lin;    /* the K solves (tol relative to the right-hand side)  */
+} fast_gpu_modal_opts;
+
+typedef struct {
+  int32_t converged;
+  int32_t iterations;         /* subspace iterations                                 */
+  int32_t linear_iterations;  /* PCG iterations, all solves                          */
+  int32_t subspace;           /* q                                                   */
+  double  max_err;            /* the convergence measure at the last iteration        */
+} fast_gpu_modal_report;
+
+int fast_gpu_modal(fast_gpu_ctx *ctx, const fast_gpu_modal_opts *opts, double *lambda, double *modes,
+                   fast_gpu_modal_report *rep);
+
 /* ---- path following (arc length) ---------------------------------------
  * cCtrlPath::Solver (ctrl/ctrlpath.cpp:63-265) with the load-increment rules
  * of the reference's arc-length classes (ctrl/ctrlarclen.cpp:95-250), on the

@@ -9,6 +9,7 @@ override with FAST_REF):
     python tests/golden/make_golden.py stress   (the two fixtures with Gauss-point stresses)
     python tests/golden/make_golden.py arc      (the path-following fixture)
     python tests/golden/make_golden.py pos      (.pos files next to the numbers they print)
+    python tests/golden/make_golden.py modal    (natural frequencies and mode shapes)
 
 It builds ``oracle/_ref/fastref`` (the reference's own sources compiled by
 ``oracle/Makefile``, plus a dump harness), writes each deck with
@@ -260,9 +261,57 @@ def pos_cases(tmp):
     print("pos_output:", {k: v.shape for k, v in out.items() if k.endswith("pos")})
 
 
+def read_pos_modes(path):
+    """Natural frequencies and eigenvectors of a modal .pos
+    (cCtrlModal::PrintMode, ctrl/ctrlmodal.cpp:128-155): [modes], [modes][nnode][3]."""
+    lines = open(path).read().splitlines()
+    freq, modes = [], []
+    for i, ln in enumerate(lines):
+        if ln.strip() == "%RESULT.CASE.STEP.NATURAL.FREQUENCY":
+            freq.append(float(lines[i + 1].split()[1]))
+        elif ln.strip() == "%RESULT.CASE.STEP.NODAL.EIGENVECTOR":
+            n = int(lines[i + 1].split()[0])
+            rows = [lines[i + 2 + k].split() for k in range(n)]
+            lab = np.array([int(r[0]) for r in rows])
+            modes.append(np.array([[float(v) for v in r[1:4]] for r in rows])[np.argsort(lab)])
+    return np.array(freq), np.array(modes)
+
+
+def modal_cases(tmp):
+    """The reference's modal analysis (cCtrlModal with cGenEigSubSpaces,
+    unmodified `fast` binary): natural frequencies and mode shapes of a
+    cantilever with an oblong section (distinct modes) and of a hex20 block."""
+    d8 = decks.cantilever_hex8(6, 2, 3, L=(6.0, 1.0, 1.6))
+    d8.rho = np.full(d8.num_elems, 2.0)
+    d20 = decks.box_hex20_lognormal(3, 2, 2, L=(3.0, 2.0, 1.3), seed=5)
+    d20.rho = np.full(d20.num_elems, 1.5)
+    for name, d, nm in (("modal_hex8_cantilever", d8, 5), ("modal_hex20_block", d20, 6)):
+        d.algorithm, d.tol, d.maxit = "ModalAnalysis", 1e-6, 200
+        base = os.path.join(tmp, name)
+        path = decks.write_dat(d, base)
+        text = open(path).read().replace(
+            "%END", f"%HEADER.ANALYSIS.EIGEN.ALGORITHM\n'SubspaceIteration'\n\n"
+                    f"%HEADER.ANALYSIS.EIGEN.NUMBER.MODES\n{nm}\n\n%END")
+        open(path, "w").write(text)
+        subprocess.run([refdump.FAST, base, "-silent"], check=True, stdout=subprocess.DEVNULL)
+        freq, modes = read_pos_modes(base + ".pos")
+        ref = refdump.run_dump(base, base + ".bin", "--no-solve", "--no-triplets")
+        out = deck_arrays(d)
+        out.update(ref_neq=ref["neq"], ref_node_eq=ref["node_eq"], ref_freq=freq, ref_modes=modes,
+                   num_modes=np.array(nm), tol=np.array(d.tol), maxit=np.array(d.maxit))
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+        print(name, freq)
+
+
 def main():
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"FAST_REF={FAST_REF}", "ref"], check=True)
     tmp = tempfile.mkdtemp(prefix="golden_")
+    if len(sys.argv) > 1 and sys.argv[1] == "modal":
+        try:
+            modal_cases(tmp)
+        finally:
+            shutil.rmtree(tmp, ignore_errors=True)
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "pos":
         try:
             pos_cases(tmp)
@@ -310,6 +359,7 @@ def main():
         stress_cases(tmp)
         arc_cases(tmp)
         pos_cases(tmp)
+        modal_cases(tmp)
         d = decks.box_hex20_lognormal(8, 8, 4, seed=11)
         d.tol = 1e-12
         run_case("cfg_hex20_lognormal_8x8x4", d, tmp, keep_elems=np.arange(0, 256, 17), triplets=False)

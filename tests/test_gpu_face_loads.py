@@ -12,7 +12,7 @@ from tests import golden_io as gio
 
 pytestmark = pytest.mark.gpu
 
-CASES = [n for n in gio.names() if not n.startswith(("nr_", "iga_", "arc_"))]
+CASES = [n for n in gio.names() if not n.startswith(("nr_", "iga_", "arc_", "modal_"))]
 
 
 def device_f(s, scale=1.0):

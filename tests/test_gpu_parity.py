@@ -15,7 +15,7 @@ TOL_K = 1e-12
 # displacement parity bound for well-conditioned decks
 TOL_U = 1e-9
 
-LINEAR = [n for n in gio.names() if n != "cfg_hex8_tl_state" and not n.startswith(("nr_", "nm_", "iga_", "arc_"))]
+LINEAR = [n for n in gio.names() if n != "cfg_hex8_tl_state" and not n.startswith(("nr_", "nm_", "iga_", "arc_", "modal_"))]
 WITH_K = [n for n in LINEAR if "ref_K_data" in gio.load(n)[1]]
 SOLVABLE = ["cfg_hex8_cantilever", "cfg_hex20_lognormal_4x4x2", "cfg_hex20_lognormal_8x8x4"]
 # solver tolerance per deck: the slender cantilever's attainable FP64 residual

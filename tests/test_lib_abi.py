@@ -45,7 +45,7 @@ def test_abi_version(lib):
     assert lib.fast_gpu_version() == 1
 
 
-@pytest.mark.parametrize("name", [n for n in gio.names() if not n.startswith(("nr_", "iga_", "arc_"))])
+@pytest.mark.parametrize("name", [n for n in gio.names() if not n.startswith(("nr_", "iga_", "arc_", "modal_"))])
 def test_face_load_vector_matches_reference(lib, name):
     d, g = gio.load(name)
     f = gpu.face_load_vector(d)

@@ -7,7 +7,7 @@ import scipy.sparse as sp
 from oracle import fem_oracle as fo
 from tests import golden_io as gio
 
-CASES = [n for n in gio.names() if not n.startswith(("nr_", "nm_", "iga_", "arc_"))]
+CASES = [n for n in gio.names() if not n.startswith(("nr_", "nm_", "iga_", "arc_", "modal_"))]
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -260,3 +260,25 @@ def test_oracle_arclength_matches_reference(method):
         unode = np.zeros((d.num_nodes, 3))
         unode[m] = us[k][eq[m] - 1]
         assert gio.rel(unode, g["ref_u_steps_" + method][k]) < 1e-9, k
+
+
+@pytest.mark.parametrize("name", ["modal_hex8_cantilever", "modal_hex20_block"])
+def test_oracle_modal_matches_reference(name):
+    """The oracle's subspace iteration (cGenEigSubSpaces) on the oracle's K
+    and M reproduces the natural frequencies and mode shapes the reference's
+    `fast` binary printed (ModalAnalysis, SubspaceIteration)."""
+    from oracle import eig_oracle as eo
+    d, g = gio.load(name)
+    K = fo.assemble(d)
+    M = fo.mass_matrix(d)
+    lam, X, it, ok = eo.subspace(K, M, int(g["num_modes"]), float(g["tol"]), int(g["maxit"]))
+    assert ok
+    assert np.abs(np.sqrt(lam) / g["ref_freq"] - 1.0).max() < 1e-11
+    eq = d.node_eq()
+    m = eq > 0
+    for k in range(len(lam)):
+        node = np.zeros((d.num_nodes, 3))
+        node[m] = X[k][eq[m] - 1]
+        R = g["ref_modes"][k]
+        sgn = np.sign(np.sum(node * R))
+        assert np.abs(sgn * node - R).max() <= 1e-5 * np.abs(R).max(), k
