@@ -11,6 +11,11 @@ cCtrlModal::Solver (ctrl/ctrlmodal.cpp:48-128) drives it:
   phi^T Mp phi = 1 ascending, X = Y Phi; converged when every one of the p
   lowest has sqrt(|1 - lambda^2 / |phi|^2|) <= tol.
 
+cCtrlLinStab::Solver (ctrl/ctrllinstab.cpp:46-140) runs the same iteration
+on K v = lambda (-G) v, G the geometric stiffness at the linear solution of
+the reference load (cControl::GeomStiffMatrix); lambda are the buckling
+factors.
+
 Here the K solves are sparse LU and the projected problem is solved by a
 Cholesky reduction and a symmetric eigensolver instead of the reference's
 generalized Jacobi sweeps (cGenEigJacobi, mlib/eig.cpp:528-722): the same
@@ -30,7 +35,9 @@ def start_vectors(K, M, q, seed=1):
     """[q][n] starting vectors of cGenEigSubSpaces::Solver."""
     n = K.shape[0]
     kd, md = K.diagonal(), M.diagonal()
-    order = sorted(range(n), key=lambda i: (kd[i] / md[i], i))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ratio = np.where(md != 0.0, kd / np.where(md != 0.0, md, 1.0), np.inf)
+    order = sorted(range(n), key=lambda i: (ratio[i], i))
     X = np.zeros((q, n))
     for j in range(q):
         X[j, order[j]] = 1.0
@@ -46,8 +53,22 @@ def projected_eigen(Kp, Mp):
     return lam, Phi
 
 
-def subspace(K, M, p, tol, maxit, X0=None):
-    """(lambda [p], modes [p][n] with v^T M v = 1, iterations, converged)."""
+def projected_eigen_swapped(Kp, Bp):
+    """The same pencil when Bp need not be definite (buckling, Bp = -Y^T G Y):
+    Bp z = mu Kp z with z^T Kp z = 1, lambda = 1 / mu, phi = z / sqrt(|mu|),
+    ascending in lambda as sEigPair::ComparePair orders them."""
+    mu, Z = sl.eigh(0.5 * (Bp + Bp.T), 0.5 * (Kp + Kp.T))
+    with np.errstate(divide="ignore"):
+        lam = np.where(mu != 0.0, 1.0 / mu, np.inf)
+    Phi = Z / np.sqrt(np.where(mu != 0.0, np.abs(mu), 1.0))
+    order = np.argsort(lam, kind="stable")
+    return lam[order], Phi[:, order]
+
+
+def subspace(K, M, p, tol, maxit, X0=None, swapped=False):
+    """(lambda [p], modes [p][n] with v^T M v = 1, iterations, converged).
+    M is the right-hand matrix of the pencil: the mass for modal analysis,
+    minus the geometric stiffness for linear buckling (swapped=True)."""
     n = K.shape[0]
     q = min(max(2 * p, p + 8), n)
     X = start_vectors(K, M, q) if X0 is None else X0
@@ -57,7 +78,7 @@ def subspace(K, M, p, tol, maxit, X0=None):
         Y = np.array([lu.solve(X[i] if it == 0 else M @ X[i]) for i in range(q)])
         Kp = Y @ (K @ Y.T)
         Mp = Y @ (M @ Y.T)
-        lam, Phi = projected_eigen(Kp, Mp)
+        lam, Phi = projected_eigen_swapped(Kp, Mp) if swapped else projected_eigen(Kp, Mp)
         X = (Y.T @ Phi).T
         err = np.sqrt(np.abs(1.0 - lam[:p] ** 2 / np.sum(Phi[:, :p] ** 2, axis=0)))
         if np.all(err <= tol):

@@ -255,6 +255,40 @@ int fo_elem_stress(int nn, const int *ngp, const double *X, double E, double nu,
   return bad;
 }
 
+/* Geometric stiffness at the displacements ue (cElmParam::GeomStiff,
+ * elc/elmparam.cpp:743-830, with cSolid::BnlMatrix / SMatrix,
+ * elc/anmodel.cpp:1514-1560): G = sum_g w detJ Bnl^T S Bnl, Bnl the 9 x 3nn
+ * gradient operator and S three copies of the stress tensor of s = C B ue,
+ * i.e. G[3a+i][3b+j] = delta_ij sum_g w detJ dN_a^T sigma dN_b. */
+int fo_elem_geom(int nn, const int *ngp, const double *X, double E, double nu, const double *ue, double *Ge)
+{
+  int nd = 3 * nn, bad = 0;
+  double pts[216 * 3], wts[216], N[20], dN[60], dX[60], B[6 * 60], C[36];
+  int np = gauss_pts(ngp, pts, wts);
+  qmatrix(E, nu, C);
+  for (int i = 0; i < nd * nd; i++) Ge[i] = 0.0;
+  for (int g = 0; g < np; g++)
+  {
+    double detJ, e[6], s[6];
+    shape(nn, pts[3 * g], pts[3 * g + 1], pts[3 * g + 2], N, dN);
+    if (drv_xyz(nn, dN, X, &detJ, dX)) bad = -1;
+    bmatrix(nn, dX, B);
+    for (int k = 0; k < 6; k++) { e[k] = 0; for (int j = 0; j < nd; j++) e[k] += B[k * nd + j] * ue[j]; }
+    for (int k = 0; k < 6; k++) { s[k] = 0; for (int j = 0; j < 6; j++) s[k] += C[k * 6 + j] * e[j]; }
+    const double S[3][3] = {{s[0], s[3], s[4]}, {s[3], s[1], s[5]}, {s[4], s[5], s[2]}};
+    const double c = wts[g] * detJ;
+    for (int a = 0; a < nn; a++)
+      for (int b = 0; b < nn; b++)
+      {
+        double v = 0.0;
+        for (int p = 0; p < 3; p++)
+          for (int q = 0; q < 3; q++) v += dX[3 * a + p] * S[p][q] * dX[3 * b + q];
+        for (int i = 0; i < 3; i++) Ge[(3 * a + i) * nd + 3 * b + i] += c * v;
+      }
+  }
+  return bad;
+}
+
 /* Extrapolation matrix TR [nn][ng] (cElmParam::CompTRMatrix,
  * elc/elmparam.cpp:1444-1535): a linear field a0 + a1 r + a2 s + a3 t fitted
  * by least squares to the Gauss-point values and evaluated at the nodes,

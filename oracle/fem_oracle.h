@@ -40,6 +40,10 @@ int fo_elem_intforce(int nn, const int *ngp, const double *X, double E, double n
 int fo_elem_stress(int nn, const int *ngp, const double *X, double E, double nu,
                    const double *ue, double *strain, double *stress);
 
+/* Geometric stiffness Ge [3nn][3nn] at element displacements ue
+ * (cElmParam::GeomStiff, elc/elmparam.cpp:743-830). */
+int fo_elem_geom(int nn, const int *ngp, const double *X, double E, double nu, const double *ue, double *Ge);
+
 /* Stress extrapolation matrix TR [nn][ng] of cElmParam::CompTRMatrix
  * (elc/elmparam.cpp:1444-1535): element-nodal stresses = TR x Gauss-point
  * stresses (cElmParam::NodalStress, :1304-1312). */

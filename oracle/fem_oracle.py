@@ -39,6 +39,7 @@ def lib():
         L.fo_elem_stress.argtypes = [ctypes.c_int, _ip, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp]
         L.fo_elem_mass.argtypes = [ctypes.c_int, _ip, _dp, ctypes.c_double, _dp]
         L.fo_extrap_matrix.argtypes = [ctypes.c_int, _ip, _dp]
+        L.fo_elem_geom.argtypes = [ctypes.c_int, _ip, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp]
         L.fo_elem_tl.argtypes = [ctypes.c_int, _ip, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp]
         L.fo_face_load.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp]
         L.fo_pcg.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32), _dp,
@@ -95,6 +96,37 @@ def elem_stress(nn, ngp, X, E, nu, ue):
     ue = np.ascontiguousarray(ue, dtype=np.float64)
     rc = lib().fo_elem_stress(nn, _ngp(ngp), _p(X), float(E), float(nu), _p(ue), _p(e), _p(s))
     return e, s, rc
+
+
+def elem_geom(nn, ngp, X, E, nu, ue):
+    """Element geometric stiffness [3nn][3nn] at displacements ue (cElmParam::GeomStiff)."""
+    G = np.zeros((3 * nn, 3 * nn))
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    ue = np.ascontiguousarray(ue, dtype=np.float64)
+    rc = lib().fo_elem_geom(nn, _ngp(ngp), _p(X), float(E), float(nu), _p(ue), _p(G))
+    return G, rc
+
+
+def geom_matrix(d, u):
+    """Assembled geometric stiffness (equation space, scipy CSR) of a deck at
+    the equation vector u (cControl::GeomStiffMatrix, ctrl/ctrl.cpp:1031-1063)."""
+    import scipy.sparse as sp
+    eq = d.node_eq()
+    neq = d.num_eq()
+    dofs = eq[d.conn].reshape(d.num_elems, -1)
+    unode = np.zeros((d.num_nodes, 3))
+    m = eq > 0
+    unode[m] = u[eq[m] - 1]
+    I, J, V = [], [], []
+    for e in range(d.num_elems):
+        Ge, rc = elem_geom(d.nn, d.ngp, d.coords[d.conn[e]], d.E[e], d.nu[e], unode[d.conn[e]].ravel())
+        dd = dofs[e]
+        mm = dd > 0
+        ii = np.repeat(dd, len(dd)) - 1
+        jj = np.tile(dd, len(dd)) - 1
+        keep = np.repeat(mm, len(dd)) & np.tile(mm, len(dd))
+        I.append(ii[keep]); J.append(jj[keep]); V.append(Ge.ravel()[keep])
+    return sp.csr_matrix((np.concatenate(V), (np.concatenate(I), np.concatenate(J))), shape=(neq, neq))
 
 
 def extrap_matrix(nn, ngp):

@@ -31,6 +31,8 @@
 //                                  (elc/elmparam.cpp:859-935), Voigt xx yy zz xy xz yz
 //         elm_nodal_stress [ne][nn][6]  cElmParam::NodalStress with extrapolation
 //                                  (elc/elmparam.cpp:1304-1312, CompTRMatrix :1444-1535)
+//       With --geom, at the same state:
+//         elm_G [ne][ndof][ndof]   cElmParam::GeomStiff (elc/elmparam.cpp:743-830)
 //
 //   fastref bench <deck> <pcg_iters> [reps]
 //       Times the reference CPU path on one host thread: StiffnessMatrix into
@@ -139,7 +141,7 @@ static int mode_dump(int argc, char **argv)
 {
   string deck = argv[2];
   const char *outp = argv[3];
-  bool trip = true, solve = true, mass = false, stress = false;
+  bool trip = true, solve = true, mass = false, stress = false, geom = false;
   const char *ufile = 0;
   double stol = -1.0;
   for (int a = 4; a < argc; a++)
@@ -149,6 +151,7 @@ static int mode_dump(int argc, char **argv)
     else if (s == "--no-solve") solve = false;
     else if (s == "--mass") mass = true;
     else if (s == "--stress") stress = true;
+    else if (s == "--geom") geom = true;
     else if (s == "--u" && a + 1 < argc) ufile = argv[++a];
     else if (s == "--solver-tol" && a + 1 < argc) stol = atof(argv[++a]);
   }
@@ -276,6 +279,22 @@ static int mode_dump(int argc, char **argv)
     w.f8("elm_strain", {ne, nip, 6}, SE.data( ), SE.size( ));
     w.f8("elm_stress", {ne, nip, 6}, SS.data( ), SS.size( ));
     w.f8("elm_nodal_stress", {ne, nen, 6}, SN.data( ), SN.size( ));
+  }
+  if (geom && (ufile || solve))
+  {
+    // element geometric stiffness at the solved (or --u) state, the matrix
+    // cControl::GeomStiffMatrix assembles for linear buckling
+    const int nd = ne > 0 ? cElement::GetElm(0)->GetNumElmDof( ) : 0;
+    vector<double> GE((size_t)ne * nd * nd);
+    cMatrix Gelm(nd, nd);
+    for (int e = 0; e < ne; e++)
+    {
+      cElement *elm = cElement::GetElm(e);
+      elm->GeomStiff(Gelm);
+      for (int i = 0; i < nd; i++)
+        for (int j = 0; j < nd; j++) GE[((size_t)e * nd + i) * nd + j] = Gelm[i][j];
+    }
+    w.f8("elm_G", {ne, nd, nd}, GE.data( ), GE.size( ));
   }
   cout.rdbuf(coutbuf);
   return 0;

@@ -10,6 +10,7 @@ override with FAST_REF):
     python tests/golden/make_golden.py arc      (the path-following fixture)
     python tests/golden/make_golden.py pos      (.pos files next to the numbers they print)
     python tests/golden/make_golden.py modal    (natural frequencies and mode shapes)
+    python tests/golden/make_golden.py buckling (buckling factors, modes, geometric stiffness)
 
 It builds ``oracle/_ref/fastref`` (the reference's own sources compiled by
 ``oracle/Makefile``, plus a dump harness), writes each deck with
@@ -97,6 +98,8 @@ def run_case(name, deck, tmp, keep_elems=None, triplets=True, extra=(), uvec=Non
         out["ref_elm_strain"] = ref["elm_strain"][sel]
         out["ref_elm_stress"] = ref["elm_stress"][sel]
         out["ref_elm_nodal_stress"] = ref["elm_nodal_stress"][sel]
+    if "elm_G" in ref:
+        out["ref_elm_G"] = ref["elm_G"][sel]
     out["ref_f"] = ref["f"]
     if triplets:
         out.update({"ref_" + k: v for k, v in lower_csr(ref).items()})
@@ -303,9 +306,46 @@ def modal_cases(tmp):
         print(name, freq)
 
 
+def buckling_cases(tmp):
+    """The reference's linear buckling (cCtrlLinStab with cGenEigSubSpaces,
+    unmodified `fast` binary) of two compressed columns: buckling factors and
+    modes from its .pos, and from the harness the linear solution and the
+    element geometric stiffness at it (cElmParam::GeomStiff)."""
+    d8 = decks.cantilever_hex8(12, 2, 3, L=(12.0, 1.0, 1.6), q=(-1.0, 0.0, 0.0))
+    d20 = decks.box_hex20_lognormal(2, 2, 10, L=(1.0, 1.3, 10.0), seed=9)
+    d20.matrix_type = "skyline"  # the linear solve direct, as for the eigen solves
+    for name, d, nm, keep in (("buck_hex8_column", d8, 3, np.array([0, 5, 40, 71])),
+                              ("buck_hex20_column", d20, 3, np.array([0, 7, 39]))):
+        d.algorithm, d.tol, d.maxit = "LinearStability", 1e-6, 200
+        run_case(name, d, tmp, keep_elems=keep, triplets=False, extra=("--geom",))
+        base = os.path.join(tmp, name + "_buck")
+        path = decks.write_dat(d, base)
+        text = open(path).read().replace(
+            "%END", f"%HEADER.ANALYSIS.EIGEN.ALGORITHM\n'SubspaceIteration'\n\n"
+                    f"%HEADER.ANALYSIS.EIGEN.NUMBER.MODES\n{nm}\n\n%END")
+        open(path, "w").write(text)
+        subprocess.run([refdump.FAST, base, "-silent"], check=True, stdout=subprocess.DEVNULL)
+        lines = open(base + ".pos").read().splitlines()
+        lam = [float(lines[i + 1].split()[1]) for i, ln in enumerate(lines)
+               if ln.strip() == "%RESULT.CASE.STEP.BUCKLING.FACTOR"]
+        _, modes = read_pos_modes(base + ".pos")
+        f = os.path.join(HERE, name + ".npz")
+        z = dict(np.load(f))
+        z.update(ref_lambda=np.array(lam), ref_modes=modes, num_modes=np.array(nm), tol=np.array(d.tol),
+                 maxit=np.array(d.maxit))
+        np.savez_compressed(f, **z)
+        print(name, lam)
+
+
 def main():
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"FAST_REF={FAST_REF}", "ref"], check=True)
     tmp = tempfile.mkdtemp(prefix="golden_")
+    if len(sys.argv) > 1 and sys.argv[1] == "buckling":
+        try:
+            buckling_cases(tmp)
+        finally:
+            shutil.rmtree(tmp, ignore_errors=True)
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "modal":
         try:
             modal_cases(tmp)
@@ -360,6 +400,7 @@ def main():
         arc_cases(tmp)
         pos_cases(tmp)
         modal_cases(tmp)
+        buckling_cases(tmp)
         d = decks.box_hex20_lognormal(8, 8, 4, seed=11)
         d.tol = 1e-12
         run_case("cfg_hex20_lognormal_8x8x4", d, tmp, keep_elems=np.arange(0, 256, 17), triplets=False)

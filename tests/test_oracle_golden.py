@@ -282,3 +282,41 @@ def test_oracle_modal_matches_reference(name):
         R = g["ref_modes"][k]
         sgn = np.sign(np.sum(node * R))
         assert np.abs(sgn * node - R).max() <= 1e-5 * np.abs(R).max(), k
+
+
+@pytest.mark.parametrize("name", ["buck_hex8_column", "buck_hex20_column"])
+def test_element_geometric_stiffness(name):
+    """cElmParam::GeomStiff at the reference's linear solution."""
+    d, g = gio.load(name)
+    eq = d.node_eq()
+    unode = np.zeros((d.num_nodes, 3))
+    m = eq > 0
+    unode[m] = g["ref_u"][eq[m] - 1]
+    for k, e in enumerate(g["ref_elems"]):
+        Ge, rc = fo.elem_geom(d.nn, d.ngp, d.coords[d.conn[e]], d.E[e], d.nu[e], unode[d.conn[e]].ravel())
+        assert rc == 0
+        assert gio.rel(Ge, g["ref_elm_G"][k]) < 1e-13, e
+
+
+@pytest.mark.parametrize("name", ["buck_hex8_column", "buck_hex20_column"])
+def test_oracle_buckling_matches_reference(name):
+    """Linear buckling (cCtrlLinStab): the oracle's subspace iteration on K and
+    minus the geometric stiffness at the linear solution reproduces the
+    buckling factors and modes the reference's `fast` binary printed."""
+    import scipy.sparse.linalg as sla
+    from oracle import eig_oracle as eo
+    d, g = gio.load(name)
+    K = fo.assemble(d)
+    u = sla.spsolve(K.tocsc(), fo.face_loads(d))
+    G = fo.geom_matrix(d, u)
+    lam, X, it, ok = eo.subspace(K, -G, int(g["num_modes"]), float(g["tol"]), int(g["maxit"]), swapped=True)
+    assert ok
+    assert np.abs(lam / g["ref_lambda"] - 1.0).max() < 1e-9
+    eq = d.node_eq()
+    m = eq > 0
+    for k in range(len(lam)):
+        node = np.zeros((d.num_nodes, 3))
+        node[m] = X[k][eq[m] - 1]
+        R = g["ref_modes"][k]
+        sgn = np.sign(np.sum(node * R))
+        assert np.abs(sgn * node - R).max() <= 1e-5 * np.abs(R).max(), k
