@@ -270,6 +270,10 @@ cudaError_t launch_tie_prolong(Ctx &c, double *u);   // u[slave] = sum w u[maste
 cudaError_t launch_element_matrices(Ctx &c, int what, int bucket, int64_t first_sorted, int64_t count,
                                     double *d_out);
 
+// geom.cu: G += sign * geometric stiffness at c.d_disp (small-strain hex
+// buckets, colour by colour; fixed rows and columns untouched)
+cudaError_t launch_geom_stiffness(Ctx &c, double *G, double sign);
+
 // tl_kernels.cu
 cudaError_t launch_tl(Ctx &c, double *K, double *G, bool want_k, bool want_g);
 cudaError_t launch_tl_element(Ctx &c, int what, int bucket, int64_t count, double *d_out_and_index);

@@ -1,6 +1,8 @@
-// modal.cu - natural frequencies and mode shapes on the device
-// (fast_gpu_modal): cCtrlModal::Solver (ctrl/ctrlmodal.cpp:48-128) with the
-// subspace iteration of cGenEigSubSpaces::Solver (mlib/eig.cpp:377-510).
+// modal.cu - natural frequencies and mode shapes (fast_gpu_modal) and linear
+// buckling factors and modes (fast_gpu_buckling) on the device:
+// cCtrlModal::Solver (ctrl/ctrlmodal.cpp:48-128) and cCtrlLinStab::Solver
+// (ctrl/ctrllinstab.cpp:46-140) with the subspace iteration of
+// cGenEigSubSpaces::Solver (mlib/eig.cpp:377-510).
 //
 //   q = max(2p, p + 8) vectors (at most 32); start: unit vectors at the q
 //   smallest K_ii / M_ii, the last one an alternating-sign pseudo-random
@@ -37,7 +39,8 @@ constexpr int kGramBlocks = 296;  // 2 x 148 SMs
 constexpr int kGramRows = 32;     // rows per shared-memory tile
 
 // K_ii / M_ii of every DOF of the node-padded layout (+inf where M_ii = 0:
-// fixed DOFs and pads)
+// fixed DOFs and pads; M is minus the geometric stiffness for buckling,
+// whose diagonal may be negative)
 __global__ void modal_ratio(int64_t nnode, const int32_t *__restrict__ diag, const double *__restrict__ K,
                             const double *__restrict__ M, double *__restrict__ out) {
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -45,7 +48,7 @@ __global__ void modal_ratio(int64_t nnode, const int32_t *__restrict__ diag, con
   const int64_t b = (int64_t)diag[n] * 9;
   for (int i = 0; i < 3; i++) {
     const double m = M[b + 4 * i];
-    out[4 * n + i] = m > 0.0 ? K[b + 4 * i] / m : INFINITY;
+    out[4 * n + i] = m != 0.0 ? K[b + 4 * i] / m : INFINITY;
   }
   out[4 * n + 3] = INFINITY;
 }
@@ -162,27 +165,31 @@ bool sym_eigen(int q, std::vector<double> &C, std::vector<double> &V) {
   return false;
 }
 
-// Kp phi = lambda Mp phi: Mp = L L^T, C = L^-1 Kp L^-T, C z = lambda z,
-// phi = L^-T z (so phi^T Mp phi = 1); ascending.  Phi k-major [q][q].
+// Kp phi = lambda Mp phi, ascending, phi^T Mp phi = 1.  Mp definite (modal):
+// Mp = L L^T, C = L^-1 Kp L^-T, C z = lambda z, phi = L^-T z.  Swapped (the
+// buckling pencil, Mp = -Y^T G Y need not be definite, Kp is): Kp = L L^T,
+// C = L^-1 Mp L^-T, C z = mu z, lambda = 1/mu, phi = L^-T z / sqrt(|mu|)
+// (so phi^T Mp phi = 1 where mu > 0).  Phi k-major [q][q].
 bool projected_eigen(int q, const std::vector<double> &Kp, const std::vector<double> &Mp, std::vector<double> &lam,
-                     std::vector<double> &Phi) {
+                     std::vector<double> &Phi, bool swapped = false) {
+  const std::vector<double> &S = swapped ? Kp : Mp, &T = swapped ? Mp : Kp;
   std::vector<double> L((size_t)q * q, 0.0);
   for (int j = 0; j < q; j++) {
-    double d = 0.5 * (Mp[(size_t)j * q + j] + Mp[(size_t)j * q + j]);
+    double d = S[(size_t)j * q + j];
     for (int k = 0; k < j; k++) d -= L[(size_t)j * q + k] * L[(size_t)j * q + k];
     if (!(d > 0.0)) return false;
     L[(size_t)j * q + j] = std::sqrt(d);
     for (int i = j + 1; i < q; i++) {
-      double s = 0.5 * (Mp[(size_t)i * q + j] + Mp[(size_t)j * q + i]);
+      double s = 0.5 * (S[(size_t)i * q + j] + S[(size_t)j * q + i]);
       for (int k = 0; k < j; k++) s -= L[(size_t)i * q + k] * L[(size_t)j * q + k];
       L[(size_t)i * q + j] = s / L[(size_t)j * q + j];
     }
   }
-  // W = L^-1 Ks (Ks the symmetric part of Kp), then C = W L^-T = L^-1 W^T
+  // W = L^-1 Ts (Ts the symmetric part of T), then C = W L^-T = L^-1 W^T
   std::vector<double> W((size_t)q * q), C((size_t)q * q);
   for (int col = 0; col < q; col++)
     for (int i = 0; i < q; i++) {
-      double s = 0.5 * (Kp[(size_t)i * q + col] + Kp[(size_t)col * q + i]);
+      double s = 0.5 * (T[(size_t)i * q + col] + T[(size_t)col * q + i]);
       for (int k = 0; k < i; k++) s -= L[(size_t)i * q + k] * W[(size_t)k * q + col];
       W[(size_t)i * q + col] = s / L[(size_t)i * q + i];
     }
@@ -199,22 +206,30 @@ bool projected_eigen(int q, const std::vector<double> &Kp, const std::vector<dou
     }
   std::vector<double> V;
   if (!sym_eigen(q, C, V)) return false;
+  std::vector<double> val(q);
+  for (int j = 0; j < q; j++) {
+    const double mu = C[(size_t)j * q + j];
+    val[j] = swapped ? (mu != 0.0 ? 1.0 / mu : INFINITY) : mu;
+  }
   std::vector<int> order(q);
   for (int i = 0; i < q; i++) order[i] = i;
-  std::sort(order.begin(), order.end(), [&](int a, int b) {
-    return C[(size_t)a * q + a] < C[(size_t)b * q + b] || (C[(size_t)a * q + a] == C[(size_t)b * q + b] && a < b);
-  });
+  std::sort(order.begin(), order.end(),
+            [&](int a, int b) { return val[a] < val[b] || (val[a] == val[b] && a < b); });
   lam.resize(q);
   Phi.assign((size_t)q * q, 0.0);
   for (int jj = 0; jj < q; jj++) {
     const int j = order[jj];
-    lam[jj] = C[(size_t)j * q + j];
+    lam[jj] = val[j];
+    const double mu = C[(size_t)j * q + j];
+    const double sc = (swapped && mu != 0.0) ? 1.0 / std::sqrt(std::fabs(mu)) : 1.0;
     // phi = L^-T z: back substitution
     for (int i = q - 1; i >= 0; i--) {
       double s = V[(size_t)i * q + j];
       for (int k = i + 1; k < q; k++) s -= L[(size_t)k * q + i] * Phi[(size_t)k * q + jj];
       Phi[(size_t)i * q + jj] = s / L[(size_t)i * q + i];
     }
+    if (sc != 1.0)
+      for (int i = 0; i < q; i++) Phi[(size_t)i * q + jj] *= sc;
   }
   return true;
 }
@@ -242,17 +257,12 @@ double start_value(int64_t j) {
     }                                                                         \
   } while (0)
 
-extern "C" int fast_gpu_modal(fast_gpu_ctx *c, const fast_gpu_modal_opts *o, double *lambda, double *modes,
-                              fast_gpu_modal_report *rep) {
-  if (!c || !o || !lambda || o->num_modes <= 0 || o->max_iter <= 0) return FAST_GPU_EINVAL;
-  if (c->has_ties()) { c->err = "tied interfaces support linear static solves only"; return FAST_GPU_ENOTSUP; }
-  if (!c->d_K || c->neq <= 0) { c->err = "modal: no mesh"; return FAST_GPU_ESTATE; }
+// The subspace iteration on the pencil (K in the stiffness slot, the
+// right-hand matrix in the mass slot), both assembled.
+static int subspace_iteration(fast_gpu_ctx *c, const fast_gpu_modal_opts *o, bool swapped, double *lambda,
+                              double *modes, fast_gpu_modal_report *rep) {
   const int p = o->num_modes;
   const int q = (int)std::min<int64_t>(std::max(2 * p, p + 8), c->neq);
-  if (q > kMaxSub || p > q) {
-    c->err = "modal: at most 16 modes (a subspace of 32 vectors)";
-    return FAST_GPU_ENOTSUP;
-  }
   const int64_t n4 = 4 * c->nnode;
   const size_t vb = sizeof(double) * n4;
   int rc = FAST_GPU_OK;
@@ -270,11 +280,6 @@ extern "C" int fast_gpu_modal(fast_gpu_ctx *c, const fast_gpu_modal_opts *o, dou
     if (e == cudaSuccess) e = cudaMalloc((void **)&d_phi, sizeof(double) * q * q);
     MCK(e);
   }
-  // cCtrlModal::Solver: M, then K (identity rows on fixed DOFs)
-  rc = fast_gpu_assemble(c, FAST_ASM_MASS);
-  if (rc != FAST_GPU_OK) goto done;
-  rc = fast_gpu_assemble(c, FAST_ASM_STIFFNESS);
-  if (rc != FAST_GPU_OK) goto done;
   MCK(solve_layout(*c, FAST_ASM_MASS, false));
   MCK(solve_layout(*c, FAST_ASM_STIFFNESS, false));
 
@@ -350,8 +355,8 @@ extern "C" int fast_gpu_modal(fast_gpu_ctx *c, const fast_gpu_modal_opts *o, dou
                           c->stream));
     }
     MCK(cudaStreamSynchronize(c->stream));
-    if (!projected_eigen(q, Kp, Mp, lam, Phi)) {
-      c->err = "modal: projected problem not positive definite (vectors lost independence)";
+    if (!projected_eigen(q, Kp, Mp, lam, Phi, swapped)) {
+      c->err = "subspace iteration: projected problem not definite (vectors lost independence)";
       rc = FAST_GPU_ENONCONV;
       goto done;
     }
@@ -374,7 +379,7 @@ extern "C" int fast_gpu_modal(fast_gpu_ctx *c, const fast_gpu_modal_opts *o, dou
     }
   }
   if (!R.converged) {
-    c->err = "modal: subspace iteration did not converge";
+    c->err = "subspace iteration did not converge";
     rc = FAST_GPU_ENONCONV;
   }
   for (int j = 0; j < p && j < (int)lam.size(); j++) lambda[j] = lam[j];
@@ -391,5 +396,94 @@ done:
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (double *b : {d_X, d_Y, d_T, d_part, d_G, d_phi})
     if (b) cudaFree(b);
+  return rc;
+}
+
+static int eigen_checks(fast_gpu_ctx *c, const fast_gpu_modal_opts *o, const double *lambda) {
+  if (!c || !o || !lambda || o->num_modes <= 0 || o->max_iter <= 0) return FAST_GPU_EINVAL;
+  if (c->has_ties()) { c->err = "tied interfaces support linear static solves only"; return FAST_GPU_ENOTSUP; }
+  if (!c->d_K || c->neq <= 0) { c->err = "eigen solve: no mesh"; return FAST_GPU_ESTATE; }
+  const int p = o->num_modes;
+  const int q = (int)std::min<int64_t>(std::max(2 * p, p + 8), c->neq);
+  if (q > kMaxSub || p > q) {
+    c->err = "eigen solve: at most 16 modes (a subspace of 32 vectors)";
+    return FAST_GPU_ENOTSUP;
+  }
+  return FAST_GPU_OK;
+}
+
+extern "C" int fast_gpu_modal(fast_gpu_ctx *c, const fast_gpu_modal_opts *o, double *lambda, double *modes,
+                              fast_gpu_modal_report *rep) {
+  int rc = eigen_checks(c, o, lambda);
+  if (rc != FAST_GPU_OK) return rc;
+  // cCtrlModal::Solver: M, then K (identity rows on fixed DOFs)
+  rc = fast_gpu_assemble(c, FAST_ASM_MASS);
+  if (rc == FAST_GPU_OK) rc = fast_gpu_assemble(c, FAST_ASM_STIFFNESS);
+  if (rc != FAST_GPU_OK) return rc;
+  return subspace_iteration(c, o, false, lambda, modes, rep);
+}
+
+// cCtrlLinStab::Solver (ctrl/ctrllinstab.cpp:46-140): K u = f, the geometric
+// stiffness G at u, then K v = lambda (-G) v.  -G goes to the mass slot (the
+// slot is marked stale afterwards, so a later mass assembly rebuilds M).
+extern "C" int fast_gpu_buckling(fast_gpu_ctx *c, const double *f, const fast_gpu_modal_opts *o, double *lambda,
+                                 double *modes, double *u, fast_gpu_modal_report *rep) {
+  int rc = eigen_checks(c, o, lambda);
+  if (rc != FAST_GPU_OK) return rc;
+  if (!f) return FAST_GPU_EINVAL;
+  for (const Bucket &B : c->buckets)
+    if (B.tl || B.type == FAST_ELEM_BSP_SOLID) {
+      c->err = "buckling: small-strain hex buckets only";
+      return FAST_GPU_ENOTSUP;
+    }
+  rc = fast_gpu_assemble(c, FAST_ASM_STIFFNESS);
+  if (rc != FAST_GPU_OK) return rc;
+  fast_gpu_solve_report lr{};
+  cudaError_t e = cudaMemcpyAsync(c->d_eq_tmp, f, sizeof(double) * c->neq, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = launch_eq_to_node(*c, c->d_eq_tmp, c->d_f);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_u, 0, sizeof(double) * 4 * c->nnode, c->stream);
+  if (e != cudaSuccess) {
+    c->err = std::string("buckling: ") + cudaGetErrorString(e);
+    return FAST_GPU_ECUDA;
+  }
+  fast_gpu_solve_opts lin = o->lin;
+  lin.warm_start = 0;
+  rc = solve_nodes(*c, &lin, false, &lr);
+  if (rc != FAST_GPU_OK) return rc;
+  e = launch_node_to_eq(*c, c->d_u, c->d_eq_tmp);
+  if (e == cudaSuccess && u)
+    e = cudaMemcpyAsync(u, c->d_eq_tmp, sizeof(double) * c->neq, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) {
+    c->err = std::string("buckling: ") + cudaGetErrorString(e);
+    return FAST_GPU_ECUDA;
+  }
+  rc = fast_gpu_set_displacement_device(c, c->d_eq_tmp);
+  if (rc != FAST_GPU_OK) return rc;
+  if (!c->d_M) {
+    e = cudaMalloc((void **)&c->d_M, sizeof(double) * 9 * c->nnzb);
+    if (e != cudaSuccess) {
+      c->err = std::string("buckling: ") + cudaGetErrorString(e);
+      return FAST_GPU_ENOMEM;
+    }
+  }
+  e = cudaMemsetAsync(c->d_status, 0, sizeof(int32_t), c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_M, 0, sizeof(double) * 9 * c->nnzb, c->stream);
+  if (e == cudaSuccess) e = launch_geom_stiffness(*c, c->d_M, -1.0);
+  int32_t status = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&status, c->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  c->M_ok = false;  // the mass slot holds -G now
+  matrix_changed(*c, FAST_ASM_MASS);
+  if (e != cudaSuccess) {
+    c->err = std::string("buckling: ") + cudaGetErrorString(e);
+    return FAST_GPU_ECUDA;
+  }
+  if (status & 1) {
+    c->err = "buckling: non-positive Jacobian determinant in at least one element";
+    return FAST_GPU_EDETJ;
+  }
+  rc = subspace_iteration(c, o, true, lambda, modes, rep);
+  matrix_changed(*c, FAST_ASM_MASS);
   return rc;
 }

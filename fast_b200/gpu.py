@@ -46,7 +46,7 @@ EXPORTS = [
     "fast_gpu_set_displacement_device", "fast_gpu_internal_force", "fast_gpu_internal_force_device",
     "fast_gpu_nr_solve", "fast_gpu_ws_create", "fast_gpu_ws_destroy", "fast_gpu_ws_add_trajectory",
     "fast_gpu_ws_build_basis", "fast_gpu_ws_train", "fast_gpu_ws_predict", "fast_gpu_ws_report", "fast_gpu_autotune", "fast_gpu_set_face_loads", "fast_gpu_gauss_stress",
-    "fast_gpu_face_load_device", "fast_gpu_arclength_solve", "fast_gpu_nodal_stress", "fast_gpu_modal",
+    "fast_gpu_face_load_device", "fast_gpu_arclength_solve", "fast_gpu_nodal_stress", "fast_gpu_modal", "fast_gpu_buckling",
     "fast_gpu_ws_get_basis", "fast_gpu_ws_get_samples", "fast_gpu_mlp_params", "fast_gpu_mlp_forward",
     "fast_gpu_mlp_loss_grad", "fast_gpu_mlp_gemm", "fast_gpu_ws_configure", "fast_gpu_ws_last_input",
     "fast_gpu_set_option", "fast_gpu_set_problems", "fast_gpu_solve_batch", "fast_gpu_newmark",
@@ -269,6 +269,7 @@ def load_library(path: str = LIB_PATH):
     L.fast_gpu_nr_solve.argtypes = [vp, _dp, ctypes.POINTER(NrOpts), NR_PREDICTOR, vp, _dp, _ip,
                                     ctypes.POINTER(NrReport)]
     L.fast_gpu_modal.argtypes = [vp, ctypes.POINTER(ModalOpts), _dp, _dp, ctypes.POINTER(ModalReport)]
+    L.fast_gpu_buckling.argtypes = [vp, _dp, ctypes.POINTER(ModalOpts), _dp, _dp, _dp, ctypes.POINTER(ModalReport)]
     L.fast_gpu_arclength_solve.argtypes = [vp, _dp, ctypes.POINTER(ArcOpts), _dp, _dp, _ip,
                                            ctypes.POINTER(ArcReport)]
     _fp = ctypes.POINTER(ctypes.c_float)
@@ -588,6 +589,22 @@ class GpuSystem:
         if rc != FAST_GPU_OK and raise_on_fail:
             self._ck(rc, "modal")
         return lam, modes, rep.as_dict()
+
+    def buckling(self, f, num_modes=5, tol=1e-6, max_iter=200, lin_tol=1e-12, precision=PREC_FP64,
+                 precond=PRECOND_JACOBI, raise_on_fail=True):
+        """Linear buckling under the reference load f: (factors [num_modes],
+        modes [num_modes][neq], linear solution u [neq], report)."""
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        lin = SolveOpts(precision, precond, 0, 0, float(lin_tol), 0.0, 0, 0)
+        o = ModalOpts(int(num_modes), int(max_iter), float(tol), lin)
+        lam = np.zeros(num_modes)
+        modes = np.zeros((num_modes, self.neq))
+        u = np.zeros(self.neq)
+        rep = ModalReport()
+        rc = self.L.fast_gpu_buckling(self.ctx, _p(f), ctypes.byref(o), _p(lam), _p(modes), _p(u), ctypes.byref(rep))
+        if rc != FAST_GPU_OK and raise_on_fail:
+            self._ck(rc, "buckling")
+        return lam, modes, u, rep.as_dict()
 
     # -- path following (cCtrlPath::Solver with the arc-length rules)
     def arclength_solve(self, q, method, steps, step_factor, tol=1e-8, max_iter=30, load_coeff=0.0, target_iter=1,

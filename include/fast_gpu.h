@@ -292,6 +292,19 @@ typedef struct {
 int fast_gpu_modal(fast_gpu_ctx *ctx, const fast_gpu_modal_opts *opts, double *lambda, double *modes,
                    fast_gpu_modal_report *rep);
 
+/* Linear buckling: cCtrlLinStab::Solver (ctrl/ctrllinstab.cpp:46-140).
+ * K u = f (f host, num_eq: the reference load), the geometric stiffness G
+ * at u assembled on the device (cControl::GeomStiffMatrix ctrl/ctrl.cpp:
+ * 1031-1063, cElmParam::GeomStiff elc/elmparam.cpp:743-830), then the same
+ * subspace iteration on K v = lambda (-G) v.  lambda ascending as the
+ * reference orders them (a state with tension can give negative factors
+ * first); modes normalised v^T (-G) v = 1; u (num_eq, may be NULL) gets the
+ * linear solution.  opts.lin serves the linear solve and the iteration's
+ * solves.  Small-strain hex buckets; the mass slot is overwritten (the next
+ * mass assembly rebuilds it). */
+int fast_gpu_buckling(fast_gpu_ctx *ctx, const double *f, const fast_gpu_modal_opts *opts, double *lambda,
+                      double *modes, double *u, fast_gpu_modal_report *rep);
+
 /* ---- path following (arc length) ---------------------------------------
  * cCtrlPath::Solver (ctrl/ctrlpath.cpp:63-265) with the load-increment rules
  * of the reference's arc-length classes (ctrl/ctrlarclen.cpp:95-250), on the

@@ -60,3 +60,27 @@ def test_modal_needs_density():
     with pytest.raises(gpu.FastGpuError):
         s.modal(3)
     s.close()
+
+
+@pytest.mark.parametrize("name", ["buck_hex8_column", "buck_hex20_column"])
+def test_buckling_matches_reference(name):
+    """Linear buckling (fast_gpu_buckling, cCtrlLinStab) against the
+    factors and modes the reference's `fast` binary printed; the geometric
+    stiffness is assembled on the device at the device's linear solution."""
+    d, g = gio.load(name)
+    s = gpu.GpuSystem(0)
+    s.upload(d)
+    nm = int(g["num_modes"])
+    lam, modes, u, rep = s.buckling(g["ref_f"], nm, tol=float(g["tol"]), max_iter=int(g["maxit"]), lin_tol=1e-13)
+    assert rep["converged"] == 1, rep
+    assert gio.rel(u, g["ref_u"]) < 1e-9
+    assert np.abs(lam / g["ref_lambda"] - 1.0).max() < 1e-9, (lam, g["ref_lambda"])
+    eq = d.node_eq()
+    m = eq > 0
+    for k in range(nm):
+        node = np.zeros((d.num_nodes, 3))
+        node[m] = modes[k][eq[m] - 1]
+        R = g["ref_modes"][k]
+        sgn = np.sign(np.sum(node * R))
+        assert np.abs(sgn * node - R).max() <= 1e-5 * np.abs(R).max(), k
+    s.close()
