@@ -233,6 +233,51 @@ extern "C" int fast_pos_step(fast_pos *pp, double factor, int64_t nnode, const d
   return FAST_GPU_OK;
 }
 
+extern "C" int fast_pos_modes(fast_pos *pp, int32_t kind, int32_t nmodes, const double *values, int64_t nnode,
+                              const double *modes) {
+  if (!pp || !pp->fp) return FAST_GPU_EINVAL;
+  fast_pos &p = *pp;
+  if ((kind != FAST_POS_VIBRATION && kind != FAST_POS_BUCKLING) || nmodes < 0 || nnode <= 0 ||
+      (nmodes > 0 && (!values || !modes))) {
+    p.err = "bad arguments";
+    return FAST_GPU_EINVAL;
+  }
+  const bool vib = kind == FAST_POS_VIBRATION;
+  const int prec = p.prec;
+  const size_t num = (size_t)prec + 11;
+  std::string s = std::string("\n%RESULT.CASE.STEP.") + (vib ? "VIBRATION" : "BUCKLING") + ".MODES\n" +
+                  std::to_string(nmodes) + "\n";
+  if (!put(p, s)) return FAST_GPU_EINVAL;
+  for (int m = 0; m < nmodes; m++) {
+    // mode + 1 << "  " << showpos << right << scientific << setw(14) << value
+    char fb[64];
+    const int len = (int)(put_num(fb, values[m], prec, true) - fb);
+    s = std::string("\n%RESULT.CASE.STEP.") + (vib ? "NATURAL.FREQUENCY" : "BUCKLING.FACTOR") + "\n" +
+        std::to_string(m + 1) + "  ";
+    for (int k = len; k < 14; k++) s += ' ';
+    s.append(fb, len);
+    s += "\n\n%RESULT.CASE.STEP.NODAL.EIGENVECTOR\n" + std::to_string(nnode) +
+         (vib ? "  'Vibration mode'\n" : "  'Buckling mode'\n");
+    if (!put(p, s)) return FAST_GPU_EINVAL;
+    const double *v = modes + (size_t)m * nnode * 3;
+    // left << setw(4) << label << " ", then " " before each of the six values
+    const bool ok = rows(p, nnode, 6 * num + 32, [&](int64_t i, char *o) {
+      char *b = o;
+      o = put_int(o, i + 1);
+      while (o - b < 4) *o++ = ' ';
+      *o++ = ' ';
+      for (int j = 0; j < 6; j++) {
+        *o++ = ' ';
+        o = put_num(o, j < 3 ? v[3 * i + j] : 0.0, prec, true);
+      }
+      *o++ = '\n';
+      return o;
+    });
+    if (!ok || !put(p, "\n", 1)) return FAST_GPU_EINVAL;
+  }
+  return FAST_GPU_OK;
+}
+
 extern "C" int fast_pos_finish(fast_pos *pp) {
   if (!pp || !pp->fp) return FAST_GPU_EINVAL;
   fast_pos &p = *pp;

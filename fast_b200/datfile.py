@@ -35,7 +35,9 @@ class PosOpts(ctypes.Structure):
                 ("print_average", ctypes.c_int32), ("threads", ctypes.c_int32)]
 
 
-POS_EXPORTS = ["fast_pos_open", "fast_pos_step", "fast_pos_finish", "fast_pos_error", "fast_pos_free"]
+POS_EXPORTS = ["fast_pos_open", "fast_pos_step", "fast_pos_modes", "fast_pos_finish", "fast_pos_error",
+               "fast_pos_free"]
+POS_VIBRATION, POS_BUCKLING = 0, 1
 
 EXPORTS = ["fast_dat_read", "fast_dat_error", "fast_dat_free", "fast_dat_get_info", "fast_dat_get_nodes",
            "fast_dat_get_elements", "fast_dat_get_faces", "fast_dat_bucket"]
@@ -64,6 +66,7 @@ def _lib():
     L.fast_pos_open.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(PosOpts), ctypes.POINTER(vp)]
     L.fast_pos_step.argtypes = [vp, ctypes.c_double, ctypes.c_int64, vp, ctypes.c_int64, ctypes.c_int32, vp,
                                 ctypes.c_int32, vp, vp]
+    L.fast_pos_modes.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, vp, ctypes.c_int64, vp]
     L.fast_pos_finish.argtypes = [vp]
     L.fast_pos_error.argtypes = [vp]
     L.fast_pos_error.restype = ctypes.c_char_p
@@ -131,11 +134,14 @@ def _arr(a, shape=None):
 
 
 def write_pos(pos_path: str, dat_path: str, steps, precision: int = 5, max_steps: int = 1,
-              print_average: bool = False, header_line: str = None, threads: int = 0) -> None:
+              print_average: bool = False, header_line: str = None, threads: int = 0, modes=None) -> None:
     """Write a FAST ``.pos`` file: the deck's echo, then one printed step per
     entry of ``steps`` (dicts with ``factor``, ``displ`` [nnode][3] and
     optionally ``gauss_stress`` [ne][points][6], ``elem_nodal`` [ne][nn][6],
-    ``nodal_avg`` [nnode][6])."""
+    ``nodal_avg`` [nnode][6]), then, when ``modes`` is given, the modes of an
+    eigen analysis: a dict with ``kind`` (POS_VIBRATION / POS_BUCKLING),
+    ``values`` [p] (frequencies or buckling factors) and ``shapes``
+    [p][nnode][3]."""
     L = _lib()
     o = PosOpts(header_line.encode() if header_line is not None else None, int(precision), int(max_steps),
                 int(bool(print_average)), int(threads))
@@ -152,6 +158,12 @@ def write_pos(pos_path: str, dat_path: str, steps, precision: int = 5, max_steps
             ne = gs.shape[0] if gs is not None else (en.shape[0] if en is not None else 0)
             rc = L.fast_pos_step(h, float(st["factor"]), u.shape[0], up, ne, gs.shape[1] if gs is not None else 0,
                                  gp, en.shape[1] if en is not None else 0, ep, ap)
+            if rc != 0:
+                raise DatError(rc, L.fast_pos_error(h).decode(errors="replace"))
+        if modes is not None:
+            vals, vp_ = _arr(modes["values"])
+            shp, sp_ = _arr(modes["shapes"])
+            rc = L.fast_pos_modes(h, int(modes["kind"]), len(vals), vp_, shp.shape[1], sp_)
             if rc != 0:
                 raise DatError(rc, L.fast_pos_error(h).decode(errors="replace"))
         rc = L.fast_pos_finish(h)

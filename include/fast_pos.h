@@ -13,7 +13,9 @@
  *   (cControl::PrintIntPntStress :2189-2260), .ELEMENT.NODAL.SCALAR(.DATA)
  *   (PrintNodalStress :2264-2320) and, when asked for, .NODAL.SCALAR(.DATA)
  *   (PrintAvrNodalStress :2397-2470);
- *   at the end "%END" and the step list written over the blank area.
+ *   the vibration or buckling modes of an eigen analysis;
+ *   at the end "%END" and the step list written over the blank area (after
+ *   it when no step was printed, as for a modal analysis).
  * Numbers are printed as iostream prints them with scientific, showpos and
  * setprecision(precision): a sign, one digit, the point, `precision` digits,
  * the exponent with at least two digits.  Node i is label i+1, element k
@@ -52,6 +54,14 @@ int fast_pos_open(const char *pos_path, const char *dat_path, const fast_pos_opt
 int fast_pos_step(fast_pos *pos, double factor, int64_t num_nodes, const double *displ, int64_t num_elems,
                   int32_t points, const double *gauss_stress, int32_t nodes_per_elem, const double *elem_nodal,
                   const double *nodal_avg);
+/* Eigen-analysis output (cCtrlModal::PrintMode ctrl/ctrlmodal.cpp:129-156,
+ * cCtrlLinStab::PrintMode ctrl/ctrllinstab.cpp:156-185): the .MODES header,
+ * then per mode its value (natural frequency, or buckling factor) and its
+ * eigenvector block.  modes [num_modes][num_nodes][3] (rotations printed 0). */
+#define FAST_POS_VIBRATION 0
+#define FAST_POS_BUCKLING  1
+int fast_pos_modes(fast_pos *pos, int32_t kind, int32_t num_modes, const double *values, int64_t num_nodes,
+                   const double *modes);
 /* "%END" and the step list; the file is complete after this. */
 int fast_pos_finish(fast_pos *pos);
 const char *fast_pos_error(const fast_pos *pos);

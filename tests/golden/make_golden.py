@@ -260,6 +260,23 @@ def pos_cases(tmp):
     subprocess.run([refdump.FAST, base, "-silent"], check=True, stdout=subprocess.DEVNULL)
     out["steps_dat"] = np.frombuffer(open(path, "rb").read(), np.uint8)
     out["steps_pos"] = np.frombuffer(open(base + ".pos", "rb").read(), np.uint8)
+    # eigen analyses: modal (no printed step) and linear buckling (the linear
+    # step, then the modes), precision 14
+    dm = decks.cantilever_hex8(6, 2, 3, L=(6.0, 1.0, 1.6))
+    dm.rho = np.full(dm.num_elems, 2.0)
+    dm.algorithm, dm.tol, dm.maxit = "ModalAnalysis", 1e-6, 200
+    db = decks.cantilever_hex8(12, 2, 3, L=(12.0, 1.0, 1.6), q=(-1.0, 0.0, 0.0))
+    db.algorithm, db.tol, db.maxit = "LinearStability", 1e-6, 200
+    for key, d in (("modal", dm), ("buck", db)):
+        base = os.path.join(tmp, "pos_" + key)
+        path = decks.write_dat(d, base)
+        text = open(path).read().replace("%HEADER.OUTPUT.PRECISION\n15", "%HEADER.OUTPUT.PRECISION\n14").replace(
+            "%END", "%HEADER.ANALYSIS.EIGEN.ALGORITHM\n'SubspaceIteration'\n\n"
+                    "%HEADER.ANALYSIS.EIGEN.NUMBER.MODES\n3\n\n%END")
+        open(path, "w").write(text)
+        subprocess.run([refdump.FAST, base, "-silent"], check=True, stdout=subprocess.DEVNULL)
+        out[key + "_dat"] = np.frombuffer(open(path, "rb").read(), np.uint8)
+        out[key + "_pos"] = np.frombuffer(open(base + ".pos", "rb").read(), np.uint8)
     np.savez_compressed(os.path.join(HERE, "pos_output.npz"), **out)
     print("pos_output:", {k: v.shape for k, v in out.items() if k.endswith("pos")})
 

@@ -149,3 +149,33 @@ def test_echo_without_end_keeps_the_reference_quirk(tmp_path):
 def test_bad_arguments(tmp_path):
     with pytest.raises(datfile.DatError):
         datfile.write_pos(str(tmp_path / "o.pos"), str(tmp_path / "missing.dat"), [])
+
+
+def _parse_modes(text):
+    lines = text.decode().split("\n")
+    vals, shapes, kind = [], [], None
+    for i, t in enumerate(lines):
+        if t in ("%RESULT.CASE.STEP.NATURAL.FREQUENCY", "%RESULT.CASE.STEP.BUCKLING.FACTOR"):
+            kind = datfile.POS_VIBRATION if "NATURAL" in t else datfile.POS_BUCKLING
+            vals.append(float(lines[i + 1].split()[1]))
+        elif t == "%RESULT.CASE.STEP.NODAL.EIGENVECTOR":
+            n = int(lines[i + 1].split()[0])
+            shapes.append([[float(v) for v in lines[i + 2 + k].split()[1:4]] for k in range(n)])
+    return dict(kind=kind, values=np.array(vals), shapes=np.array(shapes))
+
+
+@pytest.mark.parametrize("key", ["modal", "buck"])
+def test_eigen_analysis_file_is_the_reference_file(key, tmp_path):
+    """Modal (modes only, the step list after %END) and linear buckling (the
+    linear step, then the modes): every value read back from the
+    reference's print at precision 14 and re-printed."""
+    dat = tmp_path / "deck.dat"
+    dat.write_bytes(_text(key + "_dat"))
+    ref = _text(key + "_pos")
+    steps = _parse_steps(ref)
+    modes = _parse_modes(ref)
+    assert len(modes["values"]) == 3
+    out = tmp_path / "out.pos"
+    datfile.write_pos(str(out), str(dat), steps, precision=14, max_steps=1, modes=modes,
+                      header_line=ref.split(b"\n")[1].decode())
+    assert out.read_bytes() == ref
