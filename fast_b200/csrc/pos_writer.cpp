@@ -233,6 +233,35 @@ extern "C" int fast_pos_step(fast_pos *pp, double factor, int64_t nnode, const d
   return FAST_GPU_OK;
 }
 
+extern "C" int fast_pos_velacc(fast_pos *pp, int64_t nnode, const double *v, const double *a) {
+  if (!pp || !pp->fp) return FAST_GPU_EINVAL;
+  fast_pos &p = *pp;
+  if (nnode <= 0 || !v || !a) {
+    p.err = "bad arguments";
+    return FAST_GPU_EINVAL;
+  }
+  const int prec = p.prec;
+  const size_t num = (size_t)prec + 11;
+  for (int k = 0; k < 2; k++) {
+    const double *x = k == 0 ? v : a;
+    const std::string s = std::string(k == 0 ? "%RESULT.CASE.STEP.VELOCITY\n" : "%RESULT.CASE.STEP.ACCELERATION\n") +
+                          std::to_string(nnode) + (k == 0 ? "  'velocity'\n" : "  'acceleration'\n");
+    if (!put(p, s)) return FAST_GPU_EINVAL;
+    const bool ok = rows(p, nnode, 6 * num + 32, [&](int64_t i, char *o) {
+      o = put_label(o, i + 1);
+      for (int j = 0; j < 6; j++) {
+        o = put_num(o, j < 3 ? x[3 * i + j] : 0.0, prec, true);
+        *o++ = ' ';
+        *o++ = ' ';
+      }
+      *o++ = '\n';
+      return o;
+    });
+    if (!ok || !put(p, "\n", 1)) return FAST_GPU_EINVAL;
+  }
+  return FAST_GPU_OK;
+}
+
 extern "C" int fast_pos_modes(fast_pos *pp, int32_t kind, int32_t nmodes, const double *values, int64_t nnode,
                               const double *modes) {
   if (!pp || !pp->fp) return FAST_GPU_EINVAL;

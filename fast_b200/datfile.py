@@ -35,7 +35,7 @@ class PosOpts(ctypes.Structure):
                 ("print_average", ctypes.c_int32), ("threads", ctypes.c_int32)]
 
 
-POS_EXPORTS = ["fast_pos_open", "fast_pos_step", "fast_pos_modes", "fast_pos_finish", "fast_pos_error",
+POS_EXPORTS = ["fast_pos_open", "fast_pos_step", "fast_pos_velacc", "fast_pos_modes", "fast_pos_finish", "fast_pos_error",
                "fast_pos_free"]
 POS_VIBRATION, POS_BUCKLING = 0, 1
 
@@ -66,6 +66,7 @@ def _lib():
     L.fast_pos_open.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(PosOpts), ctypes.POINTER(vp)]
     L.fast_pos_step.argtypes = [vp, ctypes.c_double, ctypes.c_int64, vp, ctypes.c_int64, ctypes.c_int32, vp,
                                 ctypes.c_int32, vp, vp]
+    L.fast_pos_velacc.argtypes = [vp, ctypes.c_int64, vp, vp]
     L.fast_pos_modes.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, vp, ctypes.c_int64, vp]
     L.fast_pos_finish.argtypes = [vp]
     L.fast_pos_error.argtypes = [vp]
@@ -138,7 +139,8 @@ def write_pos(pos_path: str, dat_path: str, steps, precision: int = 5, max_steps
     """Write a FAST ``.pos`` file: the deck's echo, then one printed step per
     entry of ``steps`` (dicts with ``factor``, ``displ`` [nnode][3] and
     optionally ``gauss_stress`` [ne][points][6], ``elem_nodal`` [ne][nn][6],
-    ``nodal_avg`` [nnode][6]), then, when ``modes`` is given, the modes of an
+    ``nodal_avg`` [nnode][6], and for Newmark ``velocity`` and
+    ``acceleration`` [nnode][3]), then, when ``modes`` is given, the modes of an
     eigen analysis: a dict with ``kind`` (POS_VIBRATION / POS_BUCKLING),
     ``values`` [p] (frequencies or buckling factors) and ``shapes``
     [p][nnode][3]."""
@@ -160,6 +162,12 @@ def write_pos(pos_path: str, dat_path: str, steps, precision: int = 5, max_steps
                                  gp, en.shape[1] if en is not None else 0, ep, ap)
             if rc != 0:
                 raise DatError(rc, L.fast_pos_error(h).decode(errors="replace"))
+            if st.get("velocity") is not None:
+                v, vp2 = _arr(st["velocity"])
+                a, ap2 = _arr(st["acceleration"])
+                rc = L.fast_pos_velacc(h, v.shape[0], vp2, ap2)
+                if rc != 0:
+                    raise DatError(rc, L.fast_pos_error(h).decode(errors="replace"))
         if modes is not None:
             vals, vp_ = _arr(modes["values"])
             shp, sp_ = _arr(modes["shapes"])

@@ -12,7 +12,8 @@
  *   the rotations 0 for solids), .ELEMENT.GAUSS.SCALAR(.DATA)
  *   (cControl::PrintIntPntStress :2189-2260), .ELEMENT.NODAL.SCALAR(.DATA)
  *   (PrintNodalStress :2264-2320) and, when asked for, .NODAL.SCALAR(.DATA)
- *   (PrintAvrNodalStress :2397-2470);
+ *   (PrintAvrNodalStress :2397-2470), and for Newmark the .VELOCITY and
+ *   .ACCELERATION blocks;
  *   the vibration or buckling modes of an eigen analysis;
  *   at the end "%END" and the step list written over the blank area (after
  *   it when no step was printed, as for a modal analysis).
@@ -54,6 +55,10 @@ int fast_pos_open(const char *pos_path, const char *dat_path, const fast_pos_opt
 int fast_pos_step(fast_pos *pos, double factor, int64_t num_nodes, const double *displ, int64_t num_elems,
                   int32_t points, const double *gauss_stress, int32_t nodes_per_elem, const double *elem_nodal,
                   const double *nodal_avg);
+/* Nodal velocities and accelerations of a printed Newmark step, after its
+ * fast_pos_step (cCtrlNewmark::PrintVelAcc, ctrl/ctrlnewmark.cpp:282-330):
+ * v, a [num_nodes][3], rotations printed 0. */
+int fast_pos_velacc(fast_pos *pos, int64_t num_nodes, const double *v, const double *a);
 /* Eigen-analysis output (cCtrlModal::PrintMode ctrl/ctrlmodal.cpp:129-156,
  * cCtrlLinStab::PrintMode ctrl/ctrllinstab.cpp:156-185): the .MODES header,
  * then per mode its value (natural frequency, or buckling factor) and its

@@ -277,6 +277,17 @@ def pos_cases(tmp):
         subprocess.run([refdump.FAST, base, "-silent"], check=True, stdout=subprocess.DEVNULL)
         out[key + "_dat"] = np.frombuffer(open(path, "rb").read(), np.uint8)
         out[key + "_pos"] = np.frombuffer(open(base + ".pos", "rb").read(), np.uint8)
+    # Newmark: three printed steps with velocities and accelerations
+    dn = decks.cantilever_hex8(4, 2, 2)
+    dn.rho = np.full(dn.num_elems, 1e-3)
+    dn.algorithm, dn.maxstep, dn.time_step, dn.print_step, dn.matrix_type = "newmark", 3, 1e-3, 1, "skyline"
+    base = os.path.join(tmp, "pos_newmark")
+    path = decks.write_dat(dn, base)
+    text = open(path).read().replace("%HEADER.OUTPUT.PRECISION\n15", "%HEADER.OUTPUT.PRECISION\n14")
+    open(path, "w").write(text)
+    subprocess.run([refdump.FAST, base, "-silent"], check=True, stdout=subprocess.DEVNULL)
+    out["newmark_dat"] = np.frombuffer(open(path, "rb").read(), np.uint8)
+    out["newmark_pos"] = np.frombuffer(open(base + ".pos", "rb").read(), np.uint8)
     np.savez_compressed(os.path.join(HERE, "pos_output.npz"), **out)
     print("pos_output:", {k: v.shape for k, v in out.items() if k.endswith("pos")})
 

@@ -71,9 +71,11 @@ def _parse_steps(text):
         t = lines[i]
         if t == "%RESULT.CASE.STEP.FACTOR":
             steps.append({"factor": float(lines[i + 1])})
-        elif t == "%RESULT.CASE.STEP.NODAL.DISPLACEMENT":
+        elif t in ("%RESULT.CASE.STEP.NODAL.DISPLACEMENT", "%RESULT.CASE.STEP.VELOCITY",
+                   "%RESULT.CASE.STEP.ACCELERATION"):
             n = int(lines[i + 1].split()[0])
-            steps[-1]["displ"] = np.array([[float(v) for v in lines[i + 2 + k].split()[1:4]] for k in range(n)])
+            key = {"DISPLACEMENT": "displ", "VELOCITY": "velocity", "ACCELERATION": "acceleration"}[t.split(".")[-1]]
+            steps[-1][key] = np.array([[float(v) for v in lines[i + 2 + k].split()[1:4]] for k in range(n)])
         elif t in ("%RESULT.CASE.STEP.ELEMENT.GAUSS.SCALAR.DATA", "%RESULT.CASE.STEP.ELEMENT.NODAL.SCALAR.DATA"):
             ne, j, blocks = int(lines[i + 1]), i + 2, []
             gauss = "GAUSS" in t
@@ -178,4 +180,17 @@ def test_eigen_analysis_file_is_the_reference_file(key, tmp_path):
     out = tmp_path / "out.pos"
     datfile.write_pos(str(out), str(dat), steps, precision=14, max_steps=1, modes=modes,
                       header_line=ref.split(b"\n")[1].decode())
+    assert out.read_bytes() == ref
+
+
+def test_newmark_file_is_the_reference_file(tmp_path):
+    """Three printed Newmark steps: displacements, stresses, velocities and
+    accelerations (cCtrlNewmark::PrintVelAcc), re-printed from the values."""
+    dat = tmp_path / "deck.dat"
+    dat.write_bytes(_text("newmark_dat"))
+    ref = _text("newmark_pos")
+    steps = _parse_steps(ref)
+    assert len(steps) == 3 and all("velocity" in st and "acceleration" in st for st in steps)
+    out = tmp_path / "out.pos"
+    datfile.write_pos(str(out), str(dat), steps, precision=14, max_steps=3, header_line=ref.split(b"\n")[1].decode())
     assert out.read_bytes() == ref
