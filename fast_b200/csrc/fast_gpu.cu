@@ -257,7 +257,7 @@ int fast_gpu_upload_mesh(fast_gpu_ctx *c, const fast_gpu_mesh *m) {
     B.nn = bucket_nodes(bk);
     if (!B.nn) {
       c->err = bk.elem_type == FAST_ELEM_BSP_SOLID
-                   ? "upload_mesh: B-spline solid bucket needs a patch of degree 2 or 3 in all directions"
+                   ? "upload_mesh: B-spline solid bucket needs a patch of degree 2 to 5 in every direction"
                    : "upload_mesh: unsupported element type";
       return FAST_GPU_ENOTSUP;
     }

@@ -106,7 +106,7 @@ int bucket_nodes(const fast_gpu_bucket &bk) {
   int nn = 1;
   for (int d = 0; d < 3; d++) {
     const int p = bk.patch->degree[d];
-    if (p < 2 || p > 3) return 0;
+    if (p < 2 || p > 5) return 0;
     nn *= p + 1;
   }
   return nn;

@@ -29,11 +29,15 @@ import numpy as np
 _GR = {2: [-0.577350269189626, 0.577350269189626],
        3: [-0.774596669241483, 0.0, 0.774596669241483],
        4: [-0.861136311594053, -0.339981043584856, 0.339981043584856, 0.861136311594053],
-       5: [-0.906179845938664, -0.538469310105683, 0.0, 0.538469310105683, 0.906179845938664]}
+       5: [-0.906179845938664, -0.538469310105683, 0.0, 0.538469310105683, 0.906179845938664],
+       6: [-0.932469514203152, -0.661209386466264, -0.238619186083197, 0.238619186083197, 0.661209386466264,
+           0.932469514203152]}
 _GW = {2: [1.0, 1.0],
        3: [0.555555555555556, 0.888888888888889, 0.555555555555556],
        4: [0.347854845137454, 0.652145154862546, 0.652145154862546, 0.347854845137454],
-       5: [0.236926885056189, 0.478628670499367, 0.568888888888889, 0.478628670499367, 0.236926885056189]}
+       5: [0.236926885056189, 0.478628670499367, 0.568888888888889, 0.478628670499367, 0.236926885056189],
+       6: [0.171324492379170, 0.360761573048139, 0.467913934572691, 0.467913934572691, 0.360761573048139,
+           0.171324492379170]}
 
 
 def spans(U):

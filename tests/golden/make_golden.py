@@ -139,6 +139,29 @@ def iga_cases(tmp):
     out.update({"ref_" + k: v for k, v in lower_csr(ref).items()})
     np.savez_compressed(os.path.join(HERE, "iga_scordelis_deg3.npz"), **out)
     print("iga_scordelis_deg3 written")
+    # the reference's higher-degree NURBS cylinders: degrees (4, 2, 4) with a
+    # 5-point rule and (5, 2, 5) with a 6-point rule
+    for nm, deck, keep in (("iga_pincyl_deg4", "PinCylDeg4.dat", np.array([0, 31, 63])),
+                           ("iga_thincyl_deg5", "ThinCylinderDeg5.dat", np.array([0, 40, 79]))):
+        iga_reference_deck(tmp, nm, deck, keep)
+
+
+def iga_reference_deck(tmp, name, deck, keep):
+    """A deck shipped with the reference under dat/iga, with the harness's
+    element matrices (elements ``keep``), load and solution (the recorded K
+    of these dense patches would be megabytes: the assembled K is checked
+    against the oracle's assembly of element matrices pinned here)."""
+    src = os.path.join(FAST_REF, "dat/iga", deck)
+    d = decks.read_dat(src)
+    base = os.path.join(tmp, name)
+    shutil.copy(src, base + ".dat")
+    os.chmod(base + ".dat", 0o644)
+    ref = refdump.run_dump(base, base + ".bin")
+    out = deck_arrays(d)
+    out.update(ref_neq=ref["neq"], ref_node_eq=ref["node_eq"], ref_elems=keep, ref_elm_K=ref["elm_K"][keep],
+               ref_elm_dofs=ref["elm_dofs"], ref_f=ref["f"], ref_u=ref["u"])
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, "written", d.patch.degree, d.ngp, d.num_elems, int(ref["neq"][0]))
 
 
 def arc_cases(tmp):

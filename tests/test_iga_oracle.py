@@ -10,7 +10,7 @@ from oracle import fem_oracle as fo
 from oracle import iga_oracle as io
 from tests import golden_io as gio
 
-CASES = ["iga_p2_box", "iga_p3_box", "iga_scordelis_deg3"]
+CASES = ["iga_p2_box", "iga_p3_box", "iga_scordelis_deg3", "iga_pincyl_deg4", "iga_thincyl_deg5"]
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -78,3 +78,16 @@ def test_unit_weight_nurbs_equals_bspline():
     d.patch.rational = False
     Kp = io.elem_stiff(d, 3)
     assert gio.rel(Kp, Kr) < 1e-13
+
+
+@pytest.mark.parametrize("name", ["iga_pincyl_deg4", "iga_thincyl_deg5"])
+def test_high_degree_cylinders_solution(name):
+    """dat/iga/PinCylDeg4.dat and ThinCylinderDeg5.dat: K assembled from the
+    oracle's element matrices solves the reference's load to the reference's
+    skyline solution."""
+    import scipy.sparse.linalg as sla
+    d, g = gio.load(name)
+    assert d.patch.rational and d.patch.degree in ((4, 2, 4), (5, 2, 5))
+    K = fo.assemble(d, io.elems_stiff(d))
+    u = sla.spsolve(K.tocsc(), g["ref_f"])
+    assert gio.rel(u, g["ref_u"]) < 1e-8
