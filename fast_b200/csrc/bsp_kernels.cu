@@ -565,6 +565,7 @@ bool bsp_supported(const int pd[3], int ngp) {
   if (pd[0] == 2 && pd[1] == 2 && pd[2] == 2) return ngp == 3 || ngp == 4;
   if (pd[0] == 3 && pd[1] == 3 && (pd[2] == 3 || pd[2] == 2)) return ngp == 4;
   if (pd[0] == 4 && pd[1] == 2 && pd[2] == 4) return ngp == 5;
+  if (pd[0] == 4 && pd[1] == 2 && pd[2] == 2) return ngp == 5;
   if (pd[0] == 5 && pd[1] == 2 && pd[2] == 5) return ngp == 6;
   return false;
 }
@@ -581,6 +582,7 @@ cudaError_t launch_bsp_elements(Ctx &c, const Bucket &B, ElemArgs a, int64_t cou
   if (p[0] == 3 && p[1] == 3 && p[2] == 3 && ng == 4) return run_bsp<3, 3, 3, 4, 384>(c, a, count);
   if (p[0] == 3 && p[1] == 3 && p[2] == 2 && ng == 4) return run_bsp<3, 3, 2, 4, 384>(c, a, count);
   if (p[0] == 4 && p[1] == 2 && p[2] == 4 && ng == 5) return run_bsp_big<4, 2, 4, 5, 256, 2>(c, a, count);
+  if (p[0] == 4 && p[1] == 2 && p[2] == 2 && ng == 5) return run_bsp_big<4, 2, 2, 5, 256, 2>(c, a, count);
   if (p[0] == 5 && p[1] == 2 && p[2] == 5 && ng == 6) return run_bsp_big<5, 2, 5, 6, 256, 2>(c, a, count);
   return cudaErrorInvalidValue;
 }

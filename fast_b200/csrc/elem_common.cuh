@@ -35,6 +35,9 @@ struct Ctx;
 struct Bucket;
 // B-spline solid buckets (bsp_kernels.cu): stiffness scatter or element matrices
 cudaError_t launch_bsp_elements(Ctx &c, const Bucket &B, ElemArgs a, int64_t count);
+// B-spline solid buckets (bsp_tl.cu): total-Lagrangian tangent and / or
+// internal force (mode 0 both, 1 tangent, 2 force), small-strain internal force
+cudaError_t launch_bsp_tl(Ctx &c, const Bucket &B, ElemArgs a, int64_t count, int mode);
 
 // (a, b) pair index -> a <= b, row-major over the upper triangle
 __device__ __forceinline__ void pair_of(int p, int n, int &a, int &b) {

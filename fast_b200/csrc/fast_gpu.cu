@@ -268,7 +268,8 @@ int fast_gpu_upload_mesh(fast_gpu_ctx *c, const fast_gpu_mesh *m) {
     const bool ok_rule = (B.ngp[0] == B.ngp[1] && B.ngp[1] == B.ngp[2]) &&
                          ((B.type == FAST_ELEM_HEX8 && (B.ngp[0] == 1 || B.ngp[0] == 2 || B.ngp[0] == 3)) ||
                           (B.type == FAST_ELEM_HEX20 && (B.ngp[0] >= 2 && B.ngp[0] <= 4)) ||
-                          (B.type == FAST_ELEM_BSP_SOLID && bsp_supported(B.pd, B.ngp[0])));
+                          (B.type == FAST_ELEM_BSP_SOLID && bsp_supported(B.pd, B.ngp[0]) &&
+                           (bk.formulation != FAST_FORM_TOTAL_LAGRANGIAN || bsp_tl_supported(B.pd, B.ngp[0]))));
     if (!ok_rule) { c->err = "upload_mesh: unsupported Gauss rule for this element type"; return FAST_GPU_ENOTSUP; }
     B.ne = bk.num_elems;
     if (B.ne <= 0 || !bk.conn || !bk.E || !bk.nu) { c->err = "upload_mesh: empty bucket"; return FAST_GPU_EINVAL; }
@@ -280,8 +281,8 @@ int fast_gpu_upload_mesh(fast_gpu_ctx *c, const fast_gpu_mesh *m) {
     B.tl = bk.formulation == FAST_FORM_TOTAL_LAGRANGIAN;
     if (B.type == FAST_ELEM_BSP_SOLID) {
       const fast_gpu_patch &P = *bk.patch;
-      if (B.tl || B.has_rho) {
-        c->err = "upload_mesh: B-spline solids support the small-strain stiffness only";
+      if (B.has_rho) {
+        c->err = "upload_mesh: B-spline solids have no mass matrix here (no density)";
         return FAST_GPU_ENOTSUP;
       }
       if (!P.span) { c->err = "upload_mesh: B-spline solid bucket without element spans"; return FAST_GPU_EINVAL; }
@@ -759,8 +760,10 @@ int fast_gpu_element_matrices(fast_gpu_ctx *c, int32_t what, int32_t b, int64_t 
   if (first < 0 || count <= 0 || first + count > B.ne) return FAST_GPU_EINVAL;
   if (what == FAST_ASM_MASS && !B.has_rho) { c->err = "element_matrices: bucket has no density"; return FAST_GPU_ESTATE; }
   if (what != FAST_ASM_STIFFNESS && what != FAST_ASM_MASS && what != FAST_ASM_INTERNAL_FORCE) return FAST_GPU_EINVAL;
-  if (B.type == FAST_ELEM_BSP_SOLID && what != FAST_ASM_STIFFNESS) {
-    c->err = "element_matrices: B-spline solids provide the stiffness matrix only";
+  if (B.type == FAST_ELEM_BSP_SOLID && (what == FAST_ASM_MASS || (what == FAST_ASM_INTERNAL_FORCE &&
+                                                                 !bsp_tl_supported(B.pd, B.ngp[0])))) {
+    c->err = "element_matrices: B-spline solids provide the stiffness matrix (and, for the tangent kernels' "
+             "degrees, the internal force) only";
     return FAST_GPU_ENOTSUP;
   }
   const int nd = 3 * B.nn;

@@ -245,6 +245,8 @@ bool extrapolation_matrix(int type, const int ngp[3], std::vector<double> &TR);
 int nodes_of(int type);
 // B-spline solid kernels exist for these (degree per direction, Gauss order)
 bool bsp_supported(const int pd[3], int ngp);
+// ... and total-Lagrangian tangents / internal forces (bsp_tl.cu)
+bool bsp_tl_supported(const int pd[3], int ngp);
 // nodes per element of a bucket description (B-spline solids: product of p+1); 0 = unsupported
 int bucket_nodes(const fast_gpu_bucket &bk);
 // Per-span univariate basis tables of one patch direction at the Gauss

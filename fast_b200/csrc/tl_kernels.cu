@@ -355,10 +355,6 @@ static ElemArgs tl_args(Ctx &c, const Bucket &B, double *K, double *G) {
 cudaError_t launch_tl(Ctx &c, double *K, double *G, bool want_k, bool want_g) {
   for (size_t b = 0; b < c.buckets.size(); b++) {
     const Bucket &B = c.buckets[b];
-    if (B.type == FAST_ELEM_BSP_SOLID) {
-      if (want_g) return cudaErrorNotSupported;  // B-spline solids: stiffness only
-      continue;
-    }
     int mode;
     if (B.tl) {
       if (!want_k && !want_g) continue;
@@ -371,7 +367,9 @@ cudaError_t launch_tl(Ctx &c, double *K, double *G, bool want_k, bool want_g) {
       ElemArgs a = tl_args(c, B, (B.tl && want_k) ? K : nullptr, want_g ? G : nullptr);
       a.offset = B.color_off[k];
       const int64_t cnt = B.color_off[k + 1] - B.color_off[k];
-      cudaError_t e = B.tl ? dispatch_tl<true>(c, B, a, cnt, mode) : dispatch_tl<false>(c, B, a, cnt, mode);
+      cudaError_t e = B.type == FAST_ELEM_BSP_SOLID ? launch_bsp_tl(c, B, a, cnt, mode)
+                      : B.tl                         ? dispatch_tl<true>(c, B, a, cnt, mode)
+                                                     : dispatch_tl<false>(c, B, a, cnt, mode);
       if (e != cudaSuccess) return e;
     }
   }
@@ -387,6 +385,10 @@ cudaError_t launch_tl_element(Ctx &c, int what, int bucket, int64_t count, doubl
   a.Ke_out = d_out_and_index;
   const size_t per = (what == 0) ? (size_t)nd * nd : (size_t)nd;
   a.index = reinterpret_cast<const int32_t *>(d_out_and_index + (size_t)count * per);
+  if (B.type == FAST_ELEM_BSP_SOLID) {
+    if (what == 0 && !B.tl) return cudaErrorInvalidValue;
+    return launch_bsp_tl(c, B, a, count, what == 0 ? 1 : 2);
+  }
   if (what == 0) return B.tl ? dispatch_tl<true>(c, B, a, count, 1) : cudaErrorInvalidValue;
   return B.tl ? dispatch_tl<true>(c, B, a, count, 2) : dispatch_tl<false>(c, B, a, count, 2);
 }

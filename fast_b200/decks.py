@@ -748,7 +748,7 @@ def write_dat(deck: Deck, base: str) -> str:
             lines += ["%CONTROL.POINT.WEIGHT", str(deck.num_nodes)]
             lines += [f"{int(l)} {_fmt(w)}" for l, w in zip(lab, P.weights)]
             lines.append("")
-        lines += ["%ELEMENT", str(ne), "", "%ELEMENT.BSPLINE.SOLID", str(ne)]
+        lines += ["%ELEMENT", str(ne), "", "%ELEMENT.BSPLINE.SOLID" + ("TL" if deck.total_lagrangian else ""), str(ne)]
         lines += [f"{e+1} {inv[e]+1} 1 1 {int(P.span[e,0])+1} {int(P.span[e,1])+1} {int(P.span[e,2])+1}"
                   for e in range(ne)]
         lines.append("")
@@ -837,7 +837,7 @@ def read_dat(path: str) -> Deck:
     for k in range(int(t[0])):
         row = [int(v) for v in t[1 + 7 * k: 8 + 7 * k]]
         ords[row[0]] = tuple(row[1:4])
-    if "ELEMENT.BSPLINE.SOLID" in blk:
+    if "ELEMENT.BSPLINE.SOLID" in blk or "ELEMENT.BSPLINE.SOLIDTL" in blk:
         return _read_bsp(blk, coords, labels, l2i, fixed, mats, secs, ords, path)
     kind, tl, key = None, False, None
     for k, (kd, t_) in {"ELEMENT.BRICK8": ("hex8", False), "ELEMENT.BRICK20": ("hex20", False),
@@ -917,7 +917,9 @@ def _read_bsp(blk, coords, labels, l2i, fixed, mats, secs, ords, path) -> Deck:
         weights = np.ones(len(coords))
         for k in range(nw):
             weights[l2i[int(w[1 + 2 * k])]] = float(w[2 + 2 * k])
-    t = blk["ELEMENT.BSPLINE.SOLID"]
+    # %ELEMENT.BSPLINE.SOLIDTL: the same elements with cElmParamTL
+    tl = "ELEMENT.BSPLINE.SOLIDTL" in blk
+    t = blk["ELEMENT.BSPLINE.SOLIDTL" if tl else "ELEMENT.BSPLINE.SOLID"]
     ne = int(t[0])
     a = np.array(t[1:1 + 7 * ne], dtype=np.int64).reshape(ne, 7)
     a = a[np.argsort(a[:, 0])]
@@ -945,7 +947,7 @@ def _read_bsp(blk, coords, labels, l2i, fixed, mats, secs, ords, path) -> Deck:
     if len(ordset) != 1:
         raise ValueError("one integration order per deck is read here")
     patch = Patch(tuple(degs), knots, span, tuple(nbas), cps, weights, rational)
-    return Deck("bsp", coords, conn, E, nu, ordset.pop(), fixed, matrix_type="sparse", patch=patch,
+    return Deck("bsp", coords, conn, E, nu, ordset.pop(), fixed, matrix_type="sparse", patch=patch, total_lagrangian=tl,
                 node_labels=labels, title=os.path.basename(path), solver_rank=_solver_rank(blk, len(coords)))
 
 

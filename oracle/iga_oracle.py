@@ -70,8 +70,9 @@ def basis(U, p, k, u):
     return np.array([N(i, p, u) for i in idx]), np.array([dN(i, p, u) for i in idx])
 
 
-def elem_stiff(deck, e):
-    """Stiffness matrix of element e of a "bsp" deck (local DOFs node-major, x y z)."""
+def _points(deck, e):
+    """(c_g = w_g detJ_g, dN/dx [3][nn]) at every Gauss point of element e of
+    a "bsp" deck, points in the rule's order (r fastest)."""
     P = deck.patch
     deg = P.degree
     ng = deck.ngp
@@ -87,14 +88,6 @@ def elem_stiff(deck, e):
             n, dn = basis(U, deg[d], k, U[k] + 0.5 * (t + 1.0) * h)
             vals.append((n, 0.5 * h * dn))
         tabs.append(vals)
-    E, nu = float(deck.E[e]), float(deck.nu[e])
-    dd = (1 + nu) * (1 - 2 * nu)
-    C = np.zeros((6, 6))
-    C[:3, :3] = E * nu / dd
-    np.fill_diagonal(C[:3, :3], E * (1 - nu) / dd)
-    C[3, 3] = C[4, 4] = C[5, 5] = E / (2 * (1 + nu))
-    nn = len(X)
-    K = np.zeros((3 * nn, 3 * nn))
     for gt in range(ng[2]):
         for gs in range(ng[1]):
             for gr in range(ng[0]):
@@ -115,20 +108,68 @@ def elem_stiff(deck, e):
                 else:
                     dN = dB
                 J = dN @ X
-                det = np.linalg.det(J)
-                dx = np.linalg.solve(J, dN)
-                Bm = np.zeros((6, 3 * nn))
-                Bm[0, 0::3] = dx[0]
-                Bm[1, 1::3] = dx[1]
-                Bm[2, 2::3] = dx[2]
-                Bm[3, 0::3] = dx[1]
-                Bm[3, 1::3] = dx[0]
-                Bm[4, 0::3] = dx[2]
-                Bm[4, 2::3] = dx[0]
-                Bm[5, 1::3] = dx[2]
-                Bm[5, 2::3] = dx[1]
-                K += wg * det * Bm.T @ C @ Bm
+                yield wg * np.linalg.det(J), np.linalg.solve(J, dN)
+
+
+def _cmatrix(E, nu):
+    dd = (1 + nu) * (1 - 2 * nu)
+    C = np.zeros((6, 6))
+    C[:3, :3] = E * nu / dd
+    np.fill_diagonal(C[:3, :3], E * (1 - nu) / dd)
+    C[3, 3] = C[4, 4] = C[5, 5] = E / (2 * (1 + nu))
+    return C
+
+
+def elem_stiff(deck, e):
+    """Stiffness matrix of element e of a "bsp" deck (local DOFs node-major, x y z)."""
+    C = _cmatrix(float(deck.E[e]), float(deck.nu[e]))
+    nn = deck.conn.shape[1]
+    K = np.zeros((3 * nn, 3 * nn))
+    for c, dx in _points(deck, e):
+        Bm = np.zeros((6, 3 * nn))
+        Bm[0, 0::3] = dx[0]
+        Bm[1, 1::3] = dx[1]
+        Bm[2, 2::3] = dx[2]
+        Bm[3, 0::3] = dx[1]
+        Bm[3, 1::3] = dx[0]
+        Bm[4, 0::3] = dx[2]
+        Bm[4, 2::3] = dx[0]
+        Bm[5, 1::3] = dx[2]
+        Bm[5, 2::3] = dx[1]
+        K += c * Bm.T @ C @ Bm
     return K
+
+
+def elem_tl(deck, e, ue):
+    """Total-Lagrangian tangent and internal force of element e of a "bsp"
+    deck at element displacements ue (cElmParamTL::StiffMat / IntForce,
+    elc/elmparam.cpp:1615-1807, with cSolid::BlMatrix / BnlMatrix / SMatrix,
+    elc/anmodel.cpp:1451-1568): F = I + grad u, Green strain E = (F^T F - I)/2,
+    S = C E, B_L the strain variation (rows xx yy zz xy xz yz, engineering
+    shears), K = sum c (B_L^T C B_L + grad N^T S grad N (x) I), g = sum c B_L^T S."""
+    C = _cmatrix(float(deck.E[e]), float(deck.nu[e]))
+    nn = deck.conn.shape[1]
+    U = np.asarray(ue, dtype=np.float64).reshape(nn, 3)
+    K = np.zeros((3 * nn, 3 * nn))
+    g = np.zeros(3 * nn)
+    voigt = [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]
+    for c, dx in _points(deck, e):
+        F = np.eye(3) + U.T @ dx.T
+        Eg = 0.5 * (F.T @ F - np.eye(3))
+        ev = np.array([Eg[0, 0], Eg[1, 1], Eg[2, 2], 2 * Eg[0, 1], 2 * Eg[0, 2], 2 * Eg[1, 2]])
+        sv = C @ ev
+        S = np.array([[sv[0], sv[3], sv[4]], [sv[3], sv[1], sv[5]], [sv[4], sv[5], sv[2]]])
+        BL = np.zeros((6, 3 * nn))
+        for r, (j, k) in enumerate(voigt):
+            for i in range(3):
+                if j == k:
+                    BL[r, i::3] = F[i, j] * dx[j]
+                else:
+                    BL[r, i::3] = F[i, j] * dx[k] + F[i, k] * dx[j]
+        Gn = dx.T @ S @ dx
+        K += c * (BL.T @ C @ BL + np.kron(Gn, np.eye(3)))
+        g += c * BL.T @ sv
+    return K, g
 
 
 def elems_stiff(deck, elems=None):

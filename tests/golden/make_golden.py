@@ -144,6 +144,42 @@ def iga_cases(tmp):
     for nm, deck, keep in (("iga_pincyl_deg4", "PinCylDeg4.dat", np.array([0, 31, 63])),
                            ("iga_thincyl_deg5", "ThinCylinderDeg5.dat", np.array([0, 40, 79]))):
         iga_reference_deck(tmp, nm, deck, keep)
+    iga_tl_cases(tmp)
+
+
+def iga_tl_cases(tmp):
+    """dat/iga/CurvedBeamDeg4.dat: total-Lagrangian NURBS solid (degrees
+    4, 2, 2, 5-point rule) under load control.  The unmodified `fast`
+    binary's displacements and load factor of every printed step (15 digits),
+    and from
+    the harness the element tangents and internal forces at one of those
+    states, the load vector and the equation numbering."""
+    src = os.path.join(FAST_REF, "dat/iga/CurvedBeamDeg4.dat")
+    d = decks.read_dat(src)
+    base = os.path.join(tmp, "iga_curvedbeam_tl")
+    # the deck as shipped, with 15 printed digits (it asks for the default 5)
+    text = open(src).read().replace("%END", "%HEADER.OUTPUT.PRECISION\n15\n\n%END")
+    with open(base + ".dat", "w") as fp:
+        fp.write(text)
+    subprocess.run([refdump.FAST, base, "-silent"], check=True, stdout=subprocess.DEVNULL)
+    us = decks.read_pos_displacements(base + ".pos")
+    lam = decks.read_pos_factors(base + ".pos")
+    ref0 = refdump.run_dump(base, base + "0.bin", "--no-solve", "--no-triplets")
+    eq = ref0["node_eq"].reshape(-1, 3)
+    k = len(us) // 2
+    u_state = np.zeros(int(ref0["neq"][0]))
+    m = eq > 0
+    u_state[eq[m] - 1] = us[k][m]
+    upath = base + ".u.f8"
+    u_state.astype("<f8").tofile(upath)
+    ref = refdump.run_dump(base, base + ".bin", "--u", upath, "--no-triplets")
+    out = deck_arrays(d)
+    out.update(ref_neq=ref0["neq"], ref_node_eq=ref0["node_eq"], ref_elm_dofs=ref0["elm_dofs"], ref_f=ref0["f"],
+               ref_elems=np.arange(d.num_elems), ref_elm_K0=ref0["elm_K"], u_state=u_state,
+               ref_elm_K=ref["elm_K"], ref_elm_g=ref["elm_g"], ref_u_steps=us, ref_lam=lam, state_step=np.array(k),
+               steps=np.array(200), step_factor=np.array(0.005), tol=np.array(1e-8), maxit=np.array(100))
+    np.savez_compressed(os.path.join(HERE, "iga_curvedbeam_tl.npz"), **out)
+    print("iga_curvedbeam_tl:", us.shape, lam[:3], lam[-1])
 
 
 def iga_reference_deck(tmp, name, deck, keep):

@@ -131,3 +131,40 @@ def test_high_degree_nurbs_cylinders(name):
     assert rep["converged"]
     assert gio.rel(u, g["ref_u"]) < 1e-8
     s.close()
+
+
+def test_total_lagrangian_bspline_curved_beam():
+    """The reference's TL NURBS curved beam (dat/iga/CurvedBeamDeg4.dat,
+    degrees 4, 2, 2, 5-point rule, load control 200 x 0.005): element
+    tangents and internal forces against the reference's dumps, then the
+    device Newton driver against every step the reference's `fast` binary
+    printed, and the tip displacements its deck lists as expected results."""
+    d, g, s = loaded("iga_curvedbeam_tl")
+    n = d.num_elems
+    s.set_displacement(np.zeros(d.num_eq()))
+    K0 = s.element_matrices(0, n, what=gpu.ASM_K)
+    for e in range(n):
+        assert gio.rel(K0[e], g["ref_elm_K0"][e]) < TOL_K, e
+    s.set_displacement(g["u_state"])
+    Kt = s.element_matrices(0, n, what=gpu.ASM_K)
+    ge = s.element_matrices(0, n, what=gpu.ASM_G)
+    for e in range(n):
+        assert gio.rel(Kt[e], g["ref_elm_K"][e]) < TOL_K, e
+        assert gio.rel(ge[e], g["ref_elm_g"][e]) < 1e-9, e
+    steps = int(g["steps"])
+    hist, iters, rep = s.nr_solve(g["ref_f"], steps, float(g["step_factor"]), tol=float(g["tol"]),
+                                  max_iter=int(g["maxit"]), lin_tol=1e-13)
+    assert rep["converged_steps"] == steps, rep
+    eq = d.node_eq()
+    m = eq > 0
+    tip = {}
+    for k in range(steps):
+        unode = np.zeros((d.num_nodes, 3))
+        unode[m] = hist[k][eq[m] - 1]
+        assert gio.rel(unode, g["ref_u_steps"][k]) < 1e-7, k
+        tip[round(float(g["ref_lam"][k]), 6)] = unode[29]
+    # "Expected displacements at the end (FAST)" in the deck's header (6 digits)
+    for lf, v in ((0.30, (-5.83285, 3.49059, 28.8182)), (0.50, (-11.8457, 7.08783, 39.8952)),
+                  (0.95, (-22.0535, 13.1954, 51.6480))):
+        assert np.abs(tip[lf] - np.array(v)).max() <= 5e-6 * np.abs(v).max(), (lf, tip[lf])
+    s.close()

@@ -91,3 +91,24 @@ def test_high_degree_cylinders_solution(name):
     K = fo.assemble(d, io.elems_stiff(d))
     u = sla.spsolve(K.tocsc(), g["ref_f"])
     assert gio.rel(u, g["ref_u"]) < 1e-8
+
+
+def test_total_lagrangian_bspline_element():
+    """dat/iga/CurvedBeamDeg4.dat (%ELEMENT.BSPLINE.SOLIDTL, degrees 4, 2, 2):
+    the oracle's TL tangent at u = 0 and the TL tangent and internal force at
+    a state of the reference's own load path, against the harness dumps."""
+    d, g = gio.load("iga_curvedbeam_tl")
+    assert d.total_lagrangian and d.patch.degree == (4, 2, 2)
+    np.testing.assert_array_equal(d.node_eq(), g["ref_node_eq"])
+    eq = d.node_eq()
+    m = eq > 0
+    unode = np.zeros((d.num_nodes, 3))
+    unode[m] = g["u_state"][eq[m] - 1]
+    for e in range(d.num_elems):
+        K0, _ = io.elem_tl(d, e, np.zeros(3 * d.nn))
+        assert gio.rel(K0, g["ref_elm_K0"][e]) < 1e-13
+        Kt, ge = io.elem_tl(d, e, unode[d.conn[e]].ravel())
+        assert gio.rel(Kt, g["ref_elm_K"][e]) < 1e-13
+        # the force at a large-rotation, small-strain state loses digits to
+        # cancellation in F^T F - I
+        assert gio.rel(ge, g["ref_elm_g"][e]) < 1e-9
