@@ -51,7 +51,9 @@ extern "C" {
 #define FAST_ELEM_BSP_SOLID 3   /* %ELEMENT.BSPLINE.SOLID cElmParam, SHAPE_BSP_SOLID: Bezier-extracted
                                    B-spline / NURBS solid (shp/shpbsp.cpp:873-1067); degrees
                                    (2,2,2) with 3 or 4 Gauss points per direction, (3,3,3) and
-                                   (3,3,2) with 4, (4,2,4) with 5, (5,2,5) with 6; needs a patch */
+                                   (3,3,2) with 4, (4,2,4) and (4,2,2) with 5, (5,2,5) with 6;
+                                   FAST_FORM_TOTAL_LAGRANGIAN (%ELEMENT.BSPLINE.SOLIDTL) for
+                                   (2,2,2), (3,3,3), (3,3,2) and (4,2,2); no mass; needs a patch */
 
 /* ---- element formulation --------------------------------------------- */
 #define FAST_FORM_SMALL_STRAIN       0  /* cElmParam   (%ELEMENT.BRICK8 / BRICK20)     */
