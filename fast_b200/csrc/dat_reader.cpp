@@ -60,6 +60,11 @@ struct fast_dat {
   std::vector<uint8_t> fixed;
   std::vector<int64_t> solver_rank;
   std::vector<int32_t> conn, face_elem, face_corner, face_nodes, face_local;
+  // B-spline solid decks: the patch (knots expanded) and the element spans
+  std::vector<double> knots[3], weights;
+  std::vector<int32_t> span;  // [ne][3]
+  std::vector<int32_t> cps;   // node index of each patch control point, r fastest
+  fast_gpu_patch patch{};
 };
 
 namespace {
@@ -258,12 +263,90 @@ struct Reader {
     return FAST_GPU_OK;
   }
 
+  // %PATCH (cBspPat::Read, geom/patch.cpp:1459-1484): one 'bspsol' patch:
+  // id, type, rational flag, per direction degree 'General' #knots values
+  // multiplicities (cKnotVector::ReadKnot / ReadMult, geom/knotvec.cpp:91-170),
+  // then the control-point node labels, r fastest.  Quoted words are tokens.
+  int read_patch(int64_t nnode, int deg[3], int64_t nbas[3], std::vector<int32_t> &cps) {
+    const Block *b = find("PATCH");
+    if (!b) return fail("B-spline elements without %PATCH", nullptr);
+    std::vector<std::string> tok;
+    for (const char *p = b->b; p < b->e;) {
+      while (p < b->e && is_ws(*p)) p++;
+      if (p >= b->e) break;
+      const char *q = p;
+      if (*p == '\'') {
+        q = (const char *)memchr(p + 1, '\'', b->e - p - 1);
+        q = q ? q + 1 : b->e;
+      } else {
+        while (q < b->e && !is_ws(*q)) q++;
+      }
+      tok.emplace_back(p, q);
+      p = q;
+    }
+    size_t pos = 0;
+    auto num = [&](double &v) -> bool { return pos < tok.size() && parse_one(tok[pos].data(), tok[pos].data() + tok[pos].size(), v) && ++pos; };
+    double v;
+    if (!num(v) || v != 1.0) {
+      d.err = "one B-spline patch per deck is read here";
+      return FAST_GPU_ENOTSUP;
+    }
+    if (!num(v) || pos >= tok.size() || tok[pos] != "'bspsol'") {
+      d.err = "the patch must be a 'bspsol' B-spline solid";
+      return FAST_GPU_ENOTSUP;
+    }
+    pos++;
+    double rat;
+    if (!num(rat)) return fail("error in the input of the patch rational flag", b->b);
+    d.patch.rational = rat != 0.0;
+    for (int k = 0; k < 3; k++) {
+      double p_, nk;
+      if (!num(p_) || pos >= tok.size()) return fail("error in the input of the patch degrees", b->b);
+      if (tok[pos] != "'General'") {
+        d.err = "knot vector format " + tok[pos] + " is not read here";
+        return FAST_GPU_ENOTSUP;
+      }
+      pos++;
+      if (!num(nk) || nk < 1) return fail("error in the input of the knot vector", b->b);
+      std::vector<double> vals((size_t)nk), mult((size_t)nk);
+      for (auto &x : vals)
+        if (!num(x)) return fail("error in the input of the knot values", b->b);
+      for (auto &x : mult)
+        if (!num(x) || x < 1) return fail("error in the input of the knot multiplicities", b->b);
+      deg[k] = (int)p_;
+      d.knots[k].clear();
+      for (size_t i = 0; i < vals.size(); i++)
+        for (int m = 0; m < (int)mult[i]; m++) d.knots[k].push_back(vals[i]);
+      nbas[k] = (int64_t)d.knots[k].size() - deg[k] - 1;
+      if (deg[k] < 1 || nbas[k] < 1) return fail("invalid knot vector / degree in the patch", b->b);
+    }
+    const int64_t ncp = nbas[0] * nbas[1] * nbas[2];
+    cps.resize(ncp);
+    for (int64_t i = 0; i < ncp; i++) {
+      if (!num(v) || v < 1 || v > nnode) return fail("invalid control point in the patch", b->b);
+      cps[i] = (int32_t)v - 1;
+    }
+    d.weights.clear();
+    if (const Block *w = find("CONTROL.POINT.WEIGHT")) {
+      std::vector<double> t;
+      int rc;
+      if ((rc = tokens(*w, -2, t, "control point weights"))) return rc;
+      d.weights.assign(nnode, 1.0);
+      for (int64_t r = 0; r < (int64_t)t[0]; r++) {
+        const double id = t[1 + 2 * r];
+        if (!(id >= 1 && id <= (double)nnode)) return fail("weight of an invalid control point", w->b);
+        d.weights[(int64_t)id - 1] = t[2 + 2 * r];
+      }
+    }
+    return FAST_GPU_OK;
+  }
+
   int run() {
     split();
     int rc = header();
     if (rc) return rc;
     fast_dat_info &I = d.info;
-    for (const char *unsup : {"PATCH", "ELEMENT.BSPLINE.SOLID", "NODE.MULTI-POINT.CONSTRAINT"})
+    for (const char *unsup : {"NODE.MULTI-POINT.CONSTRAINT"})
       if (find(unsup)) {
         d.err = std::string("%") + unsup + " decks are not read here";
         return FAST_GPU_ENOTSUP;
@@ -361,7 +444,9 @@ struct Reader {
     const Kind kinds[] = {{"ELEMENT.BRICK8", FAST_ELEM_HEX8, 8, FAST_FORM_SMALL_STRAIN},
                           {"ELEMENT.BRICK20", FAST_ELEM_HEX20, 20, FAST_FORM_SMALL_STRAIN},
                           {"ELEMENT.BRICK8TL", FAST_ELEM_HEX8, 8, FAST_FORM_TOTAL_LAGRANGIAN},
-                          {"ELEMENT.BRICK20TL", FAST_ELEM_HEX20, 20, FAST_FORM_TOTAL_LAGRANGIAN}};
+                          {"ELEMENT.BRICK20TL", FAST_ELEM_HEX20, 20, FAST_FORM_TOTAL_LAGRANGIAN},
+                          {"ELEMENT.BSPLINE.SOLID", FAST_ELEM_BSP_SOLID, 0, FAST_FORM_SMALL_STRAIN},
+                          {"ELEMENT.BSPLINE.SOLIDTL", FAST_ELEM_BSP_SOLID, 0, FAST_FORM_TOTAL_LAGRANGIAN}};
     const Kind *kind = nullptr;
     for (auto &k : kinds)
       if (find(k.label)) {
@@ -372,10 +457,30 @@ struct Reader {
         kind = &k;
       }
     if (!kind) {
-      d.err = "no %ELEMENT.BRICK8 / BRICK20 (TL) block";
+      d.err = "no %ELEMENT.BRICK8 / BRICK20 (TL) or BSPLINE.SOLID (TL) block";
       return FAST_GPU_ENOTSUP;
     }
-    const int nn = kind->nn, rec = 3 + nn;
+    const bool bsp = kind->type == FAST_ELEM_BSP_SOLID;
+    int deg[3] = {0, 0, 0};
+    int64_t nbas[3] = {0, 0, 0};
+    std::vector<int32_t> cps;
+    std::vector<int64_t> first[3];  // first basis function of each non-zero span
+    if (bsp) {
+      if ((rc = read_patch(nnode, deg, nbas, cps))) return rc;
+      // cBSplineBasis::getBasInd (geom/bspbasis.cpp:59-62): spans with a gap above 1e-5
+      for (int k = 0; k < 3; k++) {
+        const std::vector<double> &U = d.knots[k];
+        for (size_t i = 1; i < U.size(); i++)
+          if (U[i] - U[i - 1] > 1e-5) first[k].push_back((int64_t)i - 1 - deg[k]);
+      }
+      if (find("LOAD.CASE.AREA.UNIFORM")) {
+        d.err = "area loads on B-spline solids are not read here";
+        return FAST_GPU_ENOTSUP;
+      }
+    }
+    const int nn = bsp ? (deg[0] + 1) * (deg[1] + 1) * (deg[2] + 1) : kind->nn;
+    // cShapeBsp::ReadIGA (shp/shpbsp.cpp:57-116): id section order patch span_r span_s span_t
+    const int rec = bsp ? 7 : 3 + nn;
     std::vector<std::vector<int64_t>> eblk;
     int64_t nrec = 0;
     for (const Block *b : find_all(kind->label)) {
@@ -395,8 +500,9 @@ struct Reader {
     I.elem_type = kind->type;
     I.nodes_per_elem = nn;
     I.formulation = kind->form;
-    I.nodes_per_face = nn == 8 ? 4 : 8;
+    I.nodes_per_face = bsp ? 0 : (nn == 8 ? 4 : 8);
     d.conn.assign((size_t)nelem * nn, -1);
+    if (bsp) d.span.assign((size_t)nelem * 3, 0);
     d.E.assign(nelem, 0.0);
     d.nu.assign(nelem, 0.0);
     if (I.has_density) d.rho.assign(nelem, 0.0);
@@ -415,6 +521,26 @@ struct Reader {
         seen[e] = 1;
         elem_sec[e] = row[1];
         elem_ord[e] = row[2];
+        if (bsp) {
+          // the element's control points, r fastest (cShapeBspSolid::Init, shp/shpbsp.cpp:873-902)
+          int64_t b0[3];
+          bool ok = true;
+          for (int k = 0; k < 3; k++) {
+            const int64_t sp = row[4 + k] - 1;
+            if (sp < 0 || sp >= (int64_t)first[k].size()) { ok = false; break; }
+            d.span[3 * e + k] = (int32_t)sp;
+            b0[k] = first[k][sp];
+          }
+          if (!ok) { bad = 2; continue; }
+          int loc = 0;
+          for (int kk = 0; kk <= deg[2]; kk++)
+            for (int jj = 0; jj <= deg[1]; jj++)
+              for (int ii = 0; ii <= deg[0]; ii++, loc++) {
+                const int64_t cp = (b0[0] + ii) + nbas[0] * (b0[1] + jj) + nbas[0] * nbas[1] * (b0[2] + kk);
+                d.conn[(size_t)e * nn + loc] = (cp >= 0 && cp < (int64_t)cps.size()) ? cps[cp] : (bad = 2, 0);
+              }
+          continue;
+        }
         for (int k = 0; k < nn; k++) {
           const int64_t v = row[3 + k];
           if (v < 1 || v > nnode) bad = 2;
@@ -423,7 +549,8 @@ struct Reader {
       }
     }
     if (bad == 1) return fail(std::string("error in the input of ") + (kind->label + 8) + " elements (label)", nullptr);
-    if (bad == 2) return fail("element incidence names an invalid node", nullptr);
+    if (bad == 2) return fail(bsp ? "element knot span outside the patch" : "element incidence names an invalid node",
+                              nullptr);
     if (bad == 3 || std::count(seen.begin(), seen.end(), 0))
       return fail("the element blocks do not define every element exactly once", nullptr);
     // cElmParam::Read: section by label, integration order by position
@@ -516,6 +643,21 @@ struct Reader {
       if (fbad == 2) return fail("error in the input of uniform face (area) loads: corners match no face", b->b);
     }
     I.num_faces = (int64_t)d.face_elem.size();
+    if (bsp) {
+      for (int k = 0; k < 3; k++) {
+        I.patch_degree[k] = deg[k];
+        I.patch_num_knots[k] = (int32_t)d.knots[k].size();
+        d.patch.degree[k] = deg[k];
+        d.patch.num_knots[k] = (int32_t)d.knots[k].size();
+        d.patch.knots[k] = d.knots[k].data();
+      }
+      d.patch.span = d.span.data();
+      d.cps = cps;
+      I.patch_num_cps = (int64_t)cps.size();
+      d.patch.weights = d.weights.empty() ? nullptr : d.weights.data();
+      I.patch_rational = d.patch.rational;
+      I.has_weights = !d.weights.empty();
+    }
     return FAST_GPU_OK;
   }
 };
@@ -604,6 +746,23 @@ extern "C" int fast_dat_get_faces(const fast_dat *d, int32_t *elem, int32_t *cor
   return FAST_GPU_OK;
 }
 
+extern "C" int fast_dat_get_patch(const fast_dat *d, double *knots, int32_t *span, double *weights, int32_t *cps) {
+  if (!d || !d->err.empty() || d->info.elem_type != FAST_ELEM_BSP_SOLID) return FAST_GPU_EINVAL;
+  if (knots)
+    for (int k = 0; k < 3; k++) {
+      memcpy(knots, d->knots[k].data(), d->knots[k].size() * sizeof(double));
+      knots += d->knots[k].size();
+    }
+  if (span) memcpy(span, d->span.data(), d->span.size() * sizeof(int32_t));
+  if (weights) {
+    if (d->weights.empty())
+      for (int64_t i = 0; i < d->info.num_nodes; i++) weights[i] = 1.0;
+    else memcpy(weights, d->weights.data(), d->weights.size() * sizeof(double));
+  }
+  if (cps) memcpy(cps, d->cps.data(), d->cps.size() * sizeof(int32_t));
+  return FAST_GPU_OK;
+}
+
 extern "C" int fast_dat_bucket(const fast_dat *d, fast_gpu_bucket *b) {
   if (!d || !b || !d->err.empty()) return FAST_GPU_EINVAL;
   memset(b, 0, sizeof *b);
@@ -615,6 +774,6 @@ extern "C" int fast_dat_bucket(const fast_dat *d, fast_gpu_bucket *b) {
   b->nu = d->nu.data();
   b->rho = d->rho.empty() ? nullptr : d->rho.data();
   b->formulation = d->info.formulation;
-  b->patch = nullptr;
+  b->patch = d->info.elem_type == FAST_ELEM_BSP_SOLID ? &d->patch : nullptr;
   return FAST_GPU_OK;
 }

@@ -1,4 +1,5 @@
-"""FAST ``.dat`` decks read by the library's parallel reader (fast_dat_*),
+"""FAST ``.dat`` decks (hex8 / hex20 / B-spline solids) read by the library's
+parallel reader (fast_dat_*),
 and ``.pos`` result files written by its parallel writer (fast_pos_*).
 
 ``read_dat(path)`` returns the same :class:`fast_b200.decks.Deck` as the
@@ -27,7 +28,9 @@ class DatInfo(ctypes.Structure):
                 ("target_iter", ctypes.c_int32), ("print_step", ctypes.c_int32), ("has_arc_length", ctypes.c_int32),
                 ("tol", ctypes.c_double), ("step_factor", ctypes.c_double), ("arc_load_coeff", ctypes.c_double),
                 ("time_step", ctypes.c_double), ("newmark", ctypes.c_double * 2),
-                ("algorithm", ctypes.c_char * 32), ("matrix_type", ctypes.c_char * 32), ("title", ctypes.c_char * 128)]
+                ("algorithm", ctypes.c_char * 32), ("matrix_type", ctypes.c_char * 32), ("title", ctypes.c_char * 128),
+                ("patch_degree", ctypes.c_int32 * 3), ("patch_num_knots", ctypes.c_int32 * 3),
+                ("patch_rational", ctypes.c_int32), ("has_weights", ctypes.c_int32), ("patch_num_cps", ctypes.c_int64)]
 
 
 class PosOpts(ctypes.Structure):
@@ -40,7 +43,7 @@ POS_EXPORTS = ["fast_pos_open", "fast_pos_step", "fast_pos_velacc", "fast_pos_mo
 POS_VIBRATION, POS_BUCKLING = 0, 1
 
 EXPORTS = ["fast_dat_read", "fast_dat_error", "fast_dat_free", "fast_dat_get_info", "fast_dat_get_nodes",
-           "fast_dat_get_elements", "fast_dat_get_faces", "fast_dat_bucket"]
+           "fast_dat_get_elements", "fast_dat_get_faces", "fast_dat_get_patch", "fast_dat_bucket"]
 
 
 class DatError(RuntimeError):
@@ -63,6 +66,7 @@ def _lib():
     L.fast_dat_get_nodes.argtypes = [vp, vp, vp, vp, vp]
     L.fast_dat_get_elements.argtypes = [vp, vp, vp, vp, vp]
     L.fast_dat_get_faces.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.fast_dat_get_patch.argtypes = [vp, vp, vp, vp, vp]
     L.fast_pos_open.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(PosOpts), ctypes.POINTER(vp)]
     L.fast_pos_step.argtypes = [vp, ctypes.c_double, ctypes.c_int64, vp, ctypes.c_int64, ctypes.c_int32, vp,
                                 ctypes.c_int32, vp, vp]
@@ -101,6 +105,19 @@ def read_dat(path: str, threads: int = 0) -> decks.Deck:
         conn = np.empty((ne, nn), np.int32)
         E, nu, rho = np.empty(ne), np.empty(ne), np.empty(ne)
         L.fast_dat_get_elements(h, _ptr(conn), _ptr(E), _ptr(nu), _ptr(rho))
+        patch = None
+        if I.elem_type == 3:
+            nk = list(I.patch_num_knots)
+            knots = np.empty(sum(nk))
+            span = np.empty((ne, 3), np.int32)
+            wts = np.empty(n)
+            cps = np.empty(I.patch_num_cps, np.int32)
+            L.fast_dat_get_patch(h, _ptr(knots), _ptr(span), _ptr(wts), _ptr(cps))
+            deg = tuple(int(v) for v in I.patch_degree)
+            kv = [knots[sum(nk[:k]):sum(nk[:k + 1])].copy() for k in range(3)]
+            grid = tuple(len(kv[k]) - deg[k] - 1 for k in range(3))
+            patch = decks.Patch(deg, kv, span, grid, cps.astype(np.int64), wts if I.has_weights else None,
+                                bool(I.patch_rational))
         fe = fc = fq = fl = None
         if nf:
             fe = np.empty(nf, np.int32)
@@ -112,7 +129,7 @@ def read_dat(path: str, threads: int = 0) -> decks.Deck:
     finally:
         if h:
             L.fast_dat_free(h)
-    kind = {gpu_elem: k for k, gpu_elem in (("hex8", 1), ("hex20", 2))}[I.elem_type]
+    kind = {gpu_elem: k for k, gpu_elem in (("hex8", 1), ("hex20", 2), ("bsp", 3))}[I.elem_type]
     return decks.Deck(kind, coords, conn, E, nu, tuple(int(v) for v in I.ngp), fixed.astype(bool), fe, fc, fq, fl,
                       rho if I.has_density else None, bool(I.formulation == 1),
                       algorithm=I.algorithm.decode() or "linear", matrix_type=I.matrix_type.decode() or "skyline",
@@ -122,7 +139,7 @@ def read_dat(path: str, threads: int = 0) -> decks.Deck:
                       newmark=(I.newmark[0], I.newmark[1]), print_step=I.print_step,
                       node_labels=np.arange(1, n + 1, dtype=np.int64), title=os.path.basename(path),
                       nodal_f=nodal if I.has_nodal_forces else None,
-                      solver_rank=rank if I.has_solver_order else None)
+                      solver_rank=rank if I.has_solver_order else None, patch=patch)
 
 
 def _arr(a, shape=None):

@@ -871,19 +871,24 @@ def read_dat(path: str) -> Deck:
         fl = np.array([int(r[4]) for r in rows], np.int32)
         fq = np.array([[float(v) for v in r[5:8]] for r in rows])
 
+    return Deck(kind, coords, conn, E, nu, ngp, fixed, fe, fc, fq, fl, rho, tl,
+                node_labels=labels, title=os.path.basename(path), solver_rank=_solver_rank(blk, n),
+                **_analysis_header(blk))
+
+
+def _analysis_header(blk) -> dict:
+    """%HEADER.ANALYSIS.* fields of a deck (defaults as the reference's)."""
     def s1(label, default, cast):
         if label in blk and blk[label]:
             return cast(blk[label][0].strip("'"))
         return default
 
-    return Deck(kind, coords, conn, E, nu, ngp, fixed, fe, fc, fq, fl, rho, tl,
-                algorithm=s1("HEADER.ANALYSIS.ALGORITHM", "linear", str),
+    return dict(algorithm=s1("HEADER.ANALYSIS.ALGORITHM", "linear", str),
                 matrix_type=s1("HEADER.ANALYSIS.MATRIX.TYPE", "skyline", str),
                 tol=s1("HEADER.ANALYSIS.TOLERANCE", 1e-5, float),
                 maxit=s1("HEADER.ANALYSIS.MAXIMUM.ITERATIONS", 0, int),
                 maxstep=s1("HEADER.ANALYSIS.MAXIMUM.STEPS", 1, int),
-                step_factor=s1("HEADER.ANALYSIS.STEP.FACTOR", 1.0, float),
-                node_labels=labels, title=os.path.basename(path), solver_rank=_solver_rank(blk, n))
+                step_factor=s1("HEADER.ANALYSIS.STEP.FACTOR", 1.0, float))
 
 
 def _read_bsp(blk, coords, labels, l2i, fixed, mats, secs, ords, path) -> Deck:
@@ -947,8 +952,9 @@ def _read_bsp(blk, coords, labels, l2i, fixed, mats, secs, ords, path) -> Deck:
     if len(ordset) != 1:
         raise ValueError("one integration order per deck is read here")
     patch = Patch(tuple(degs), knots, span, tuple(nbas), cps, weights, rational)
-    return Deck("bsp", coords, conn, E, nu, ordset.pop(), fixed, matrix_type="sparse", patch=patch, total_lagrangian=tl,
-                node_labels=labels, title=os.path.basename(path), solver_rank=_solver_rank(blk, len(coords)))
+    return Deck("bsp", coords, conn, E, nu, ordset.pop(), fixed, patch=patch, total_lagrangian=tl,
+                node_labels=labels, title=os.path.basename(path), solver_rank=_solver_rank(blk, len(coords)),
+                **_analysis_header(blk))
 
 
 def _solver_rank(blk, nnode):

@@ -15,6 +15,9 @@
  *   %ELEMENT, %ELEMENT.BRICK8/BRICK8TL/BRICK20/BRICK20TL
  *                               cElement::ReadNumElm / ReadBrick* (elc/element.cpp:301-316,
  *                               1985-2090) with cElmParam::Read (elc/elmparam.cpp:221-247)
+ *   %PATCH, %CONTROL.POINT.WEIGHT, %ELEMENT.BSPLINE.SOLID(TL)
+ *                               one 'bspsol' patch with 'General' knot vectors (cBspPat::Read
+ *                               geom/patch.cpp:1459-1484, cShapeBsp::ReadIGA shp/shpbsp.cpp:57-116)
  *   %LOAD.CASE.NODAL.FORCE      cLoad::ReadNodalLoads (load/load.cpp:53-87)
  *   %LOAD.CASE.AREA.UNIFORM     cLoad::ReadFaceUnifLoads + cFaceUnifLoad::Read
  *                               (load/load.cpp:229-248, 1440-1478)
@@ -28,8 +31,9 @@
  * Other blocks are skipped, as the reference skips labels it does not know.
  *
  * Status codes are fast_gpu.h's (FAST_GPU_OK, FAST_GPU_EINVAL for a deck
- * error, FAST_GPU_ENOTSUP for decks outside this subset: B-spline patches,
- * more than one element type or integration order, ties). */
+ * error, FAST_GPU_ENOTSUP for decks outside this subset: more than one
+ * element type or integration order, ties, other patch kinds, area loads on
+ * B-spline solids). */
 #ifndef FAST_DAT_H
 #define FAST_DAT_H
 
@@ -48,8 +52,8 @@ typedef struct {
   int64_t num_elems;
   int64_t num_faces;          /* %LOAD.CASE.AREA.UNIFORM records                     */
   int32_t nodes_per_face;     /* 4 (Q4 faces of hex8) or 8 (Q8 faces of hex20)       */
-  int32_t elem_type;          /* FAST_ELEM_HEX8 or FAST_ELEM_HEX20                     */
-  int32_t nodes_per_elem;     /* 8 or 20                                             */
+  int32_t elem_type;          /* FAST_ELEM_HEX8, FAST_ELEM_HEX20 or FAST_ELEM_BSP_SOLID  */
+  int32_t nodes_per_elem;     /* 8, 20 or the patch's (p+1)(q+1)(r+1)                */
   int32_t formulation;        /* FAST_FORM_SMALL_STRAIN or FAST_FORM_TOTAL_LAGRANGIAN */
   int32_t ngp[3];             /* Gauss points per direction (the deck's one order)   */
   int32_t has_density;        /* %MATERIAL.DENSITY present                           */
@@ -68,6 +72,12 @@ typedef struct {
   char    algorithm[32];      /* ALGORITHM, without quotes ("" when absent)          */
   char    matrix_type[32];    /* MATRIX.TYPE, without quotes                         */
   char    title[128];         /* first line after %HEADER                            */
+  /* B-spline solid decks (elem_type FAST_ELEM_BSP_SOLID) */
+  int32_t patch_degree[3];
+  int32_t patch_num_knots[3]; /* knot vector lengths, multiplicities expanded         */
+  int32_t patch_rational;
+  int32_t has_weights;        /* %CONTROL.POINT.WEIGHT present                       */
+  int64_t patch_num_cps;      /* control points of the patch                         */
 } fast_dat_info;
 
 /* Reads the deck at path with up to `threads` host threads (0: all cores).
@@ -96,6 +106,11 @@ int fast_dat_get_elements(const fast_dat *dat, int32_t *conn, double *E, double 
  * output may be NULL. */
 int fast_dat_get_faces(const fast_dat *dat, int32_t *elem, int32_t *corners, int32_t *face_nodes, int32_t *local,
                        double *q);
+/* B-spline solid decks: knots (the three expanded vectors one after the
+ * other), span [num_elems][3] 0-based non-zero knot spans, weights
+ * [num_nodes] (1 where none is given), cps [patch_num_cps] the node of each
+ * patch control point (r fastest); any may be NULL. */
+int fast_dat_get_patch(const fast_dat *dat, double *knots, int32_t *span, double *weights, int32_t *cps);
 /* A bucket whose arrays point into the deck (valid until fast_dat_free):
  * uploads without copies through fast_gpu_mesh.buckets. */
 int fast_dat_bucket(const fast_dat *dat, fast_gpu_bucket *bucket);

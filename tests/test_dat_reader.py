@@ -17,6 +17,7 @@ from tests import golden_io as gio
 
 ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
 HEX = [n for n in gio.names() if gio.load(n)[0].kind in ("hex8", "hex20")]
+BSP = [n for n in gio.names() if gio.load(n)[0].kind == "bsp"]
 FIELDS = ["coords", "conn", "E", "nu", "fixed", "face_elem", "face_corners", "face_q", "face_local", "rho",
           "solver_rank"]
 
@@ -224,7 +225,10 @@ def test_deck_errors_are_reported_with_their_line(tmp_path):
 def test_decks_outside_the_subset_are_refused(tmp_path):
     d, _ = gio.load("iga_p2_box")
     p = decks.write_dat(d, str(tmp_path / "bsp"))
-    assert _err(p).rc == -7
+    txt = open(p).read()
+    q = tmp_path / "bsp_patch_kind.dat"
+    q.write_text(txt.replace("'bspsol'", "'bspsurf'"))
+    assert _err(str(q)).rc == -7
 
     def two_types(t):
         return t.replace("%END", "%ELEMENT.BRICK20\n0\n\n%END")
@@ -246,5 +250,44 @@ def test_bucket_points_into_the_deck(tmp_path):
         np.testing.assert_array_equal(conn, d.conn)
         np.testing.assert_array_equal(np.ctypeslib.as_array(b.E, shape=(d.num_elems,)), d.E)
         assert not b.rho and b.formulation == 0
+    finally:
+        L.fast_dat_free(h)
+
+
+def same_patch(P, Q):
+    assert P.degree == Q.degree and tuple(P.grid) == tuple(Q.grid) and P.rational == Q.rational
+    for k in range(3):
+        np.testing.assert_array_equal(P.knots[k], Q.knots[k])
+    np.testing.assert_array_equal(P.span, Q.span)
+    np.testing.assert_array_equal(P.cps, Q.cps)
+    assert (P.weights is None) == (Q.weights is None)
+    if P.weights is not None:
+        np.testing.assert_array_equal(P.weights, Q.weights)
+
+
+@pytest.mark.parametrize("name", BSP)
+def test_bspline_decks_match_python_reader_and_reference(name, tmp_path):
+    """%PATCH / %CONTROL.POINT.WEIGHT / %ELEMENT.BSPLINE.SOLID(TL): the native
+    reader builds the same patch, spans and control-point incidence as the
+    Python reader, and the reference's equation numbering."""
+    d, g = gio.load(name)
+    p = decks.write_dat(d, str(tmp_path / name))
+    nat = datfile.read_dat(p)
+    py = decks.read_dat(p)
+    same(nat, py)
+    same_patch(nat.patch, py.patch)
+    np.testing.assert_array_equal(nat.node_eq(), g["ref_node_eq"])
+    # the bucket view carries the patch
+    L = datfile._lib()
+    L.fast_dat_bucket.argtypes = [ctypes.c_void_p, ctypes.POINTER(gpu.Bucket)]
+    h = ctypes.c_void_p()
+    assert L.fast_dat_read(os.fsencode(p), 2, ctypes.byref(h)) == 0
+    try:
+        b = gpu.Bucket()
+        assert L.fast_dat_bucket(h, ctypes.byref(b)) == 0
+        assert b.elem_type == 3 and bool(b.patch)
+        assert tuple(b.patch.contents.degree) == tuple(d.patch.degree)
+        span = np.ctypeslib.as_array(b.patch.contents.span, shape=(d.num_elems, 3))
+        np.testing.assert_array_equal(span, d.patch.span)
     finally:
         L.fast_dat_free(h)
