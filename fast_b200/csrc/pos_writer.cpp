@@ -27,6 +27,9 @@ struct fast_pos {
   int prec = 5, max_steps = 1, avg = 0, threads = 1;
   int steps = 0;
   long case_pos = 0;
+  bool left = false;                // the stream's adjustfield after the last block
+  std::vector<int64_t> reac_nodes;  // staged for the next step
+  std::vector<double> reac_vals;
 };
 
 namespace {
@@ -174,6 +177,33 @@ extern "C" int fast_pos_step(fast_pos *pp, double factor, int64_t nnode, const d
     return o;
   });
   if (!ok || !put(p, "\n", 1)) return FAST_GPU_EINVAL;
+  p.left = true;
+  if (!p.reac_nodes.empty()) {
+    // left << setw(4) << label << " ", then scientific << right <<
+    // setprecision(5) << setw(13) << value << " " for the six components
+    s = "%RESULT.CASE.STEP.NODAL.REACTIONS\n" + std::to_string(p.reac_nodes.size()) + "\n";
+    if (!put(p, s)) return FAST_GPU_EINVAL;
+    ok = rows(p, (int64_t)p.reac_nodes.size(), 6 * 24 + 32, [&](int64_t r, char *o) {
+      char *b = o;
+      o = put_int(o, p.reac_nodes[r] + 1);
+      while (o - b < 4) *o++ = ' ';
+      *o++ = ' ';
+      for (int j = 0; j < 6; j++) {
+        char nb[40];
+        const int len = (int)(put_num(nb, j < 3 ? p.reac_vals[3 * r + j] : 0.0, 5, false) - nb);
+        for (int k = len; k < 13; k++) *o++ = ' ';
+        memcpy(o, nb, len);
+        o += len;
+        *o++ = ' ';
+      }
+      *o++ = '\n';
+      return o;
+    });
+    if (!ok || !put(p, "\n", 1)) return FAST_GPU_EINVAL;
+    p.left = false;
+    p.reac_nodes.clear();
+    p.reac_vals.clear();
+  }
   if (gs) {
     s = std::string("%RESULT.CASE.STEP.ELEMENT.GAUSS.SCALAR\n6\n") + kLabels +
         "\n%RESULT.CASE.STEP.ELEMENT.GAUSS.SCALAR.DATA\n" + std::to_string(ne) + "\n";
@@ -229,7 +259,15 @@ extern "C" int fast_pos_step(fast_pos *pp, double factor, int64_t nnode, const d
       return o;
     });
     if (!ok || !put(p, "\n", 1)) return FAST_GPU_EINVAL;
+    p.left = true;
   }
+  return FAST_GPU_OK;
+}
+
+extern "C" int fast_pos_reactions(fast_pos *pp, int64_t count, const int64_t *nodes, const double *R) {
+  if (!pp || !pp->fp || count < 0 || (count > 0 && (!nodes || !R))) return FAST_GPU_EINVAL;
+  pp->reac_nodes.assign(nodes, nodes + count);
+  pp->reac_vals.assign(R, R + 3 * count);
   return FAST_GPU_OK;
 }
 
@@ -259,6 +297,7 @@ extern "C" int fast_pos_velacc(fast_pos *pp, int64_t nnode, const double *v, con
     });
     if (!ok || !put(p, "\n", 1)) return FAST_GPU_EINVAL;
   }
+  p.left = true;
   return FAST_GPU_OK;
 }
 
@@ -303,6 +342,7 @@ extern "C" int fast_pos_modes(fast_pos *pp, int32_t kind, int32_t nmodes, const 
       return o;
     });
     if (!ok || !put(p, "\n", 1)) return FAST_GPU_EINVAL;
+    p.left = true;
   }
   return FAST_GPU_OK;
 }
@@ -310,8 +350,9 @@ extern "C" int fast_pos_modes(fast_pos *pp, int32_t kind, int32_t nmodes, const 
 extern "C" int fast_pos_finish(fast_pos *pp) {
   if (!pp || !pp->fp) return FAST_GPU_EINVAL;
   fast_pos &p = *pp;
-  // cControl::End: "%END", then the step list over the reserved area (the
-  // labels still left-aligned from the displacement rows: setw(2) pads "1 ")
+  // cControl::End: "%END", then the step list over the reserved area;
+  // setw(2) pads under the adjustfield the last block left behind ("1 "
+  // after displacement rows, " 1" after support reactions)
   bool ok = put(p, "\n%END\n", 6);
   if (ok && p.case_pos != 0 && fseek(p.fp, p.case_pos, SEEK_SET) != 0) {
     p.err = "seek error";
@@ -321,7 +362,7 @@ extern "C" int fast_pos_finish(fast_pos *pp) {
     std::string s = "1   " + std::to_string(p.steps) + "\n";
     for (int i = 1; i <= p.steps; i++) {
       std::string n = std::to_string(i);
-      if (n.size() < 2) n += " ";
+      if (n.size() < 2) n = p.left ? n + " " : " " + n;  // setw(2) under the stream's adjustfield
       s += n + "  'step" + std::to_string(i) + "'\n";
     }
     ok = put(p, s);

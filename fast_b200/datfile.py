@@ -38,7 +38,7 @@ class PosOpts(ctypes.Structure):
                 ("print_average", ctypes.c_int32), ("threads", ctypes.c_int32)]
 
 
-POS_EXPORTS = ["fast_pos_open", "fast_pos_step", "fast_pos_velacc", "fast_pos_modes", "fast_pos_finish", "fast_pos_error",
+POS_EXPORTS = ["fast_pos_open", "fast_pos_step", "fast_pos_reactions", "fast_pos_velacc", "fast_pos_modes", "fast_pos_finish", "fast_pos_error",
                "fast_pos_free"]
 POS_VIBRATION, POS_BUCKLING = 0, 1
 
@@ -71,6 +71,7 @@ def _lib():
     L.fast_pos_step.argtypes = [vp, ctypes.c_double, ctypes.c_int64, vp, ctypes.c_int64, ctypes.c_int32, vp,
                                 ctypes.c_int32, vp, vp]
     L.fast_pos_velacc.argtypes = [vp, ctypes.c_int64, vp, vp]
+    L.fast_pos_reactions.argtypes = [vp, ctypes.c_int64, vp, vp]
     L.fast_pos_modes.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, vp, ctypes.c_int64, vp]
     L.fast_pos_finish.argtypes = [vp]
     L.fast_pos_error.argtypes = [vp]
@@ -156,8 +157,9 @@ def write_pos(pos_path: str, dat_path: str, steps, precision: int = 5, max_steps
     """Write a FAST ``.pos`` file: the deck's echo, then one printed step per
     entry of ``steps`` (dicts with ``factor``, ``displ`` [nnode][3] and
     optionally ``gauss_stress`` [ne][points][6], ``elem_nodal`` [ne][nn][6],
-    ``nodal_avg`` [nnode][6], and for Newmark ``velocity`` and
-    ``acceleration`` [nnode][3]), then, when ``modes`` is given, the modes of an
+    ``nodal_avg`` [nnode][6], ``reaction_nodes`` [k] with ``reactions``
+    [k][3], and for Newmark ``velocity`` and ``acceleration`` [nnode][3]),
+    then, when ``modes`` is given, the modes of an
     eigen analysis: a dict with ``kind`` (POS_VIBRATION / POS_BUCKLING),
     ``values`` [p] (frequencies or buckling factors) and ``shapes``
     [p][nnode][3]."""
@@ -170,6 +172,12 @@ def write_pos(pos_path: str, dat_path: str, steps, precision: int = 5, max_steps
         if rc != 0:
             raise DatError(rc, L.fast_pos_error(h).decode(errors="replace") if h else "out of memory")
         for st in steps:
+            if st.get("reactions") is not None:
+                rn = np.ascontiguousarray(st["reaction_nodes"], dtype=np.int64)
+                rv, rp_ = _arr(st["reactions"])
+                rc = L.fast_pos_reactions(h, len(rn), rn.ctypes.data_as(ctypes.c_void_p), rp_)
+                if rc != 0:
+                    raise DatError(rc, L.fast_pos_error(h).decode(errors="replace"))
             u, up = _arr(st["displ"])
             gs, gp = _arr(st.get("gauss_stress"))
             en, ep = _arr(st.get("elem_nodal"))

@@ -46,7 +46,7 @@ EXPORTS = [
     "fast_gpu_set_displacement_device", "fast_gpu_internal_force", "fast_gpu_internal_force_device",
     "fast_gpu_nr_solve", "fast_gpu_ws_create", "fast_gpu_ws_destroy", "fast_gpu_ws_add_trajectory",
     "fast_gpu_ws_build_basis", "fast_gpu_ws_train", "fast_gpu_ws_predict", "fast_gpu_ws_report", "fast_gpu_autotune", "fast_gpu_set_face_loads", "fast_gpu_gauss_stress",
-    "fast_gpu_face_load_device", "fast_gpu_arclength_solve", "fast_gpu_nodal_stress", "fast_gpu_modal", "fast_gpu_buckling",
+    "fast_gpu_face_load_device", "fast_gpu_arclength_solve", "fast_gpu_nodal_stress", "fast_gpu_modal", "fast_gpu_buckling", "fast_gpu_support_reactions",
     "fast_gpu_ws_get_basis", "fast_gpu_ws_get_samples", "fast_gpu_mlp_params", "fast_gpu_mlp_forward",
     "fast_gpu_mlp_loss_grad", "fast_gpu_mlp_gemm", "fast_gpu_ws_configure", "fast_gpu_ws_last_input",
     "fast_gpu_set_option", "fast_gpu_set_problems", "fast_gpu_solve_batch", "fast_gpu_newmark",
@@ -237,6 +237,8 @@ def load_library(path: str = LIB_PATH):
     L.fast_gpu_autotune.argtypes = [vp, vp]
     L.fast_gpu_gauss_stress.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, vp, vp]
     L.fast_gpu_nodal_stress.argtypes = [vp, ctypes.c_int32, vp, vp]
+    L.fast_gpu_support_reactions.argtypes = [vp, vp, ctypes.c_int32, ctypes.c_int32, vp, vp, vp, ctypes.c_int32, vp,
+                                             ctypes.c_double, vp]
     L.fast_gpu_set_face_loads.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, vp, vp, vp, ctypes.c_int32]
     L.fast_gpu_face_load_device.argtypes = [vp, ctypes.c_double, vp]
     L.fast_gpu_set_problems.argtypes = [vp, ctypes.c_int32, _lp]
@@ -475,6 +477,25 @@ class GpuSystem:
         self._ck(self.L.fast_gpu_gauss_stress(self.ctx, bucket, int(first), int(count), st.ctypes.data,
                                               ss.ctypes.data), "gauss_stress")
         return st, ss
+
+    def support_reactions(self, load_factor=1.0, supported=None):
+        """Support reactions [nnode][3] at the current displacements under the
+        deck's face and nodal loads scaled by load_factor (fast_gpu_support_reactions)."""
+        d = self.deck
+        R = np.zeros((d.num_nodes, 3))
+        sup = None if supported is None else np.ascontiguousarray(supported, dtype=np.uint8)
+        nf = 0 if d.face_elem is None else len(d.face_elem)
+        fn = q = loc = None
+        if nf:
+            fn = np.ascontiguousarray(d.face_nodes(), dtype=np.int32)
+            q = np.ascontiguousarray(d.face_q, dtype=np.float64)
+            loc = np.ascontiguousarray(d.face_local, dtype=np.int32)
+        nod = None if d.nodal_f is None else np.ascontiguousarray(d.nodal_f, dtype=np.float64)
+        ptr = lambda a: None if a is None else a.ctypes.data
+        self._ck(self.L.fast_gpu_support_reactions(self.ctx, ptr(sup), nf, fn.shape[1] if nf else 4, ptr(fn), ptr(q),
+                                                   ptr(loc), int(d.ngp[0]), ptr(nod), float(load_factor),
+                                                   R.ctypes.data), "support_reactions")
+        return R
 
     def nodal_stress(self, bucket=0):
         """(element-nodal [ne][nn][6], averaged nodal [nnode][6]) stresses at the

@@ -529,6 +529,19 @@ int fast_gpu_set_face_loads(fast_gpu_ctx *ctx, int32_t num_faces, int32_t nodes_
                             const double *q, const int32_t *local, int32_t ngp1d);
 int fast_gpu_face_load_device(fast_gpu_ctx *ctx, double scale, double *d_f);
 
+/* Support reactions at the current displacements (cControl::SuppReactions,
+ * ctrl/ctrl.cpp:844-882): the internal force of every element with a
+ * supported node (device) added to all its nodes in element order, minus the
+ * face loads with a supported node (same arguments as
+ * fast_gpu_face_load_vector) and the nodal loads nodal_f [num_nodes][3] (may
+ * be NULL) on supported nodes, both scaled by load_factor.  supported
+ * [num_nodes] (NULL: every node with a DOF without an equation).  R
+ * [num_nodes][3] out (host); the rows of supported nodes are the reactions. */
+int fast_gpu_support_reactions(fast_gpu_ctx *ctx, const uint8_t *supported, int32_t num_faces,
+                               int32_t nodes_per_face, const int32_t *face_nodes, const double *q,
+                               const int32_t *local, int32_t ngp1d, const double *nodal_f, double load_factor,
+                               double *R);
+
 /* ---- stress recovery ----------------------------------------------------
  * Gauss-point strains and stresses at the current displacements
  * (fast_gpu_set_displacement): cElmParam::IntPntStress (elc/elmparam.cpp:

@@ -9,7 +9,7 @@
  *   at the first step "%RESULT" and "%RESULT.CASE" with the blank step-list
  *   area (13 spaces per line, floor(1.1 * max_steps) + 1 lines);
  *   per step: %RESULT.CASE.STEP, .FACTOR, .NODAL.DISPLACEMENT (six values,
- *   the rotations 0 for solids), .ELEMENT.GAUSS.SCALAR(.DATA)
+ *   the rotations 0 for solids), .NODAL.REACTIONS when given, .ELEMENT.GAUSS.SCALAR(.DATA)
  *   (cControl::PrintIntPntStress :2189-2260), .ELEMENT.NODAL.SCALAR(.DATA)
  *   (PrintNodalStress :2264-2320) and, when asked for, .NODAL.SCALAR(.DATA)
  *   (PrintAvrNodalStress :2397-2470), and for Newmark the .VELOCITY and
@@ -20,9 +20,8 @@
  * Numbers are printed as iostream prints them with scientific, showpos and
  * setprecision(precision): a sign, one digit, the point, `precision` digits,
  * the exponent with at least two digits.  Node i is label i+1, element k
- * label k+1, stresses in Voigt order xx yy zz xy xz yz.  Support reactions,
- * Newmark velocities and accelerations and the IGA and micro-model blocks are
- * not written.  Status codes are fast_gpu.h's (FAST_GPU_EINVAL for bad
+ * label k+1, stresses in Voigt order xx yy zz xy xz yz.  The IGA and
+ * micro-model blocks are not written.  Status codes are fast_gpu.h's (FAST_GPU_EINVAL for bad
  * arguments or an I/O error). */
 #ifndef FAST_POS_H
 #define FAST_POS_H
@@ -55,6 +54,12 @@ int fast_pos_open(const char *pos_path, const char *dat_path, const fast_pos_opt
 int fast_pos_step(fast_pos *pos, double factor, int64_t num_nodes, const double *displ, int64_t num_elems,
                   int32_t points, const double *gauss_stress, int32_t nodes_per_elem, const double *elem_nodal,
                   const double *nodal_avg);
+/* Support reactions for the next fast_pos_step, printed after its
+ * displacements (%RESULT.CASE.STEP.NODAL.REACTIONS, ctrl/ctrl.cpp:1222-1257,
+ * when %HEADER.PRINT.SUPPORT.REACTIONS is set): nodes [count] the 0-based
+ * supported nodes in ascending order, R [count][3] (e.g. the supported rows
+ * of fast_gpu_support_reactions); five digits as the reference prints them. */
+int fast_pos_reactions(fast_pos *pos, int64_t count, const int64_t *nodes, const double *R);
 /* Nodal velocities and accelerations of a printed Newmark step, after its
  * fast_pos_step (cCtrlNewmark::PrintVelAcc, ctrl/ctrlnewmark.cpp:282-330):
  * v, a [num_nodes][3], rotations printed 0. */

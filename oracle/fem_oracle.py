@@ -213,6 +213,39 @@ def face_loads(deck):
     return f
 
 
+def support_reactions(deck, u, load_factor=1.0):
+    """cControl::SuppReactions (ctrl/ctrl.cpp:844-882) at the equation vector
+    u: internal forces of the elements with a supported node added to all
+    their nodes, minus the face and nodal loads with a supported node.
+    [nnode][3]; supported = a node with a DOF without an equation."""
+    eq = deck.node_eq()
+    sup = (eq == 0).any(axis=1)
+    unode = np.zeros((deck.num_nodes, 3))
+    m = eq > 0
+    unode[m] = u[eq[m] - 1]
+    R = np.zeros((deck.num_nodes, 3))
+    for e in range(deck.num_elems):
+        en = deck.conn[e]
+        if not sup[en].any():
+            continue
+        ge, rc = elem_intforce(deck.nn, deck.ngp, deck.coords[en], deck.E[e], deck.nu[e], unode[en].ravel())
+        R[en] += ge.reshape(-1, 3)
+    if deck.face_elem is not None and len(deck.face_elem):
+        fn = deck.face_nodes()
+        nf = fn.shape[1]
+        for k in range(len(fn)):
+            if not sup[fn[k]].any():
+                continue
+            fe = np.zeros(3 * nf)
+            q = np.ascontiguousarray(deck.face_q[k], dtype=np.float64)
+            lib().fo_face_load(nf, max(deck.ngp), _p(np.ascontiguousarray(deck.coords[fn[k]])), _p(q),
+                               int(deck.face_local[k]), _p(fe))
+            R[fn[k]] -= load_factor * fe.reshape(-1, 3)
+    if deck.nodal_f is not None:
+        R[sup] -= load_factor * deck.nodal_f[sup]
+    return R
+
+
 def pcg(K, f, tol, maxit):
     """FAST's Jacobi PCG on a scipy CSR matrix; returns (u, converged, iters, err)."""
     n = K.shape[0]

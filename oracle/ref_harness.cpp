@@ -31,6 +31,8 @@
 //                                  (elc/elmparam.cpp:859-935), Voigt xx yy zz xy xz yz
 //         elm_nodal_stress [ne][nn][6]  cElmParam::NodalStress with extrapolation
 //                                  (elc/elmparam.cpp:1304-1312, CompTRMatrix :1444-1535)
+//       With --reactions, at the same state:
+//         reactions [nnode][6]     cControl::SuppReactions (ctrl/ctrl.cpp:844-882)
 //       With --geom, at the same state:
 //         elm_G [ne][ndof][ndof]   cElmParam::GeomStiff (elc/elmparam.cpp:743-830)
 //
@@ -141,7 +143,7 @@ static int mode_dump(int argc, char **argv)
 {
   string deck = argv[2];
   const char *outp = argv[3];
-  bool trip = true, solve = true, mass = false, stress = false, geom = false;
+  bool trip = true, solve = true, mass = false, stress = false, geom = false, reac = false;
   const char *ufile = 0;
   double stol = -1.0;
   for (int a = 4; a < argc; a++)
@@ -152,6 +154,7 @@ static int mode_dump(int argc, char **argv)
     else if (s == "--mass") mass = true;
     else if (s == "--stress") stress = true;
     else if (s == "--geom") geom = true;
+    else if (s == "--reactions") reac = true;
     else if (s == "--u" && a + 1 < argc) ufile = argv[++a];
     else if (s == "--solver-tol" && a + 1 < argc) stol = atof(argv[++a]);
   }
@@ -279,6 +282,19 @@ static int mode_dump(int argc, char **argv)
     w.f8("elm_strain", {ne, nip, 6}, SE.data( ), SE.size( ));
     w.f8("elm_stress", {ne, nip, 6}, SS.data( ), SS.size( ));
     w.f8("elm_nodal_stress", {ne, nen, 6}, SN.data( ), SN.size( ));
+  }
+  if (reac && (ufile || solve))
+  {
+    // support reactions at the same state (cControl::SuppReactions): element
+    // internal forces of the elements touching a support minus the loads
+    // touching one, per node label and direction (all nodes, 6 columns)
+    const int nnode = cNode::GetNumNode( );
+    cMatrix R(nnode, 6);
+    cControl::SuppReactions(R);
+    vector<double> RR((size_t)nnode * 6);
+    for (int i = 0; i < nnode; i++)
+      for (int j = 0; j < 6; j++) RR[(size_t)i * 6 + j] = R(i, j);
+    w.f8("reactions", {nnode, 6}, RR.data( ), RR.size( ));
   }
   if (geom && (ufile || solve))
   {

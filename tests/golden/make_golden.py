@@ -74,7 +74,7 @@ def run_case(name, deck, tmp, keep_elems=None, triplets=True, extra=(), uvec=Non
     decks.write_dat(deck, base)
     opts = list(extra)
     if stress:
-        opts.append("--stress")
+        opts += ["--stress", "--reactions"]
     if not triplets:
         opts.append("--no-triplets")
     if mass:
@@ -100,6 +100,8 @@ def run_case(name, deck, tmp, keep_elems=None, triplets=True, extra=(), uvec=Non
         out["ref_elm_nodal_stress"] = ref["elm_nodal_stress"][sel]
     if "elm_G" in ref:
         out["ref_elm_G"] = ref["elm_G"][sel]
+    if "reactions" in ref:
+        out["ref_reactions"] = ref["reactions"]
     out["ref_f"] = ref["f"]
     if triplets:
         out.update({"ref_" + k: v for k, v in lower_csr(ref).items()})
@@ -336,6 +338,16 @@ def pos_cases(tmp):
         subprocess.run([refdump.FAST, base, "-silent"], check=True, stdout=subprocess.DEVNULL)
         out[key + "_dat"] = np.frombuffer(open(path, "rb").read(), np.uint8)
         out[key + "_pos"] = np.frombuffer(open(base + ".pos", "rb").read(), np.uint8)
+    # support reactions (%HEADER.PRINT.SUPPORT.REACTIONS), precision 14
+    dr = decks.cantilever_hex8(3, 2, 2)
+    base = os.path.join(tmp, "pos_reac")
+    path = decks.write_dat(dr, base)
+    text = open(path).read().replace("%HEADER.OUTPUT.PRECISION\n15", "%HEADER.OUTPUT.PRECISION\n14").replace(
+        "%END", "%HEADER.PRINT.SUPPORT.REACTIONS\n1\n\n%END")
+    open(path, "w").write(text)
+    subprocess.run([refdump.FAST, base, "-silent"], check=True, stdout=subprocess.DEVNULL)
+    out["reac_dat"] = np.frombuffer(open(path, "rb").read(), np.uint8)
+    out["reac_pos"] = np.frombuffer(open(base + ".pos", "rb").read(), np.uint8)
     # Newmark: three printed steps with velocities and accelerations
     dn = decks.cantilever_hex8(4, 2, 2)
     dn.rho = np.full(dn.num_elems, 1e-3)

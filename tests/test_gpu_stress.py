@@ -89,3 +89,20 @@ def test_nodal_stress_average_on_a_mesh_with_unused_nodes():
     ref = fo.averaged_nodal_stress(d.num_nodes, d.conn, en)
     assert np.abs(avg - ref).max() <= 1e-14 * np.abs(ref).max()
     s.close()
+
+
+@pytest.mark.parametrize("name", [n for n in CASES if "ref_reactions" in gio.load(n)[1]])
+def test_support_reactions_match_reference(name):
+    """fast_gpu_support_reactions (device element forces, host loads) at the
+    reference's solution against the reference's cControl::SuppReactions."""
+    d, g = gio.load(name)
+    s = gpu.GpuSystem(0)
+    s.upload(d)
+    s.set_displacement(g["ref_u"])
+    R = s.support_reactions()
+    sup = (d.node_eq() == 0).any(axis=1)
+    ref = g["ref_reactions"][:, :3]
+    assert np.abs(R[sup] - ref[sup]).max() <= 1e-12 * np.abs(ref[sup]).max()
+    # balance: the reactions carry the applied load
+    np.testing.assert_allclose(R[sup].sum(axis=0), ref[sup].sum(axis=0), rtol=0, atol=1e-10 * np.abs(ref).max())
+    s.close()

@@ -320,3 +320,13 @@ def test_oracle_buckling_matches_reference(name):
         R = g["ref_modes"][k]
         sgn = np.sign(np.sum(node * R))
         assert np.abs(sgn * node - R).max() <= 1e-5 * np.abs(R).max(), k
+
+
+@pytest.mark.parametrize("name", [c for c in CASES if "ref_reactions" in gio.load(c)[1]])
+def test_support_reactions(name):
+    """cControl::SuppReactions at the reference's solution from the oracle's
+    element forces and face loads, against the reference's own."""
+    d, g = gio.load(name)
+    R = fo.support_reactions(d, g["ref_u"])
+    ref = g["ref_reactions"][:, :3]
+    assert np.abs(R - ref).max() <= 1e-13 * np.abs(ref).max()

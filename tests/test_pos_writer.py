@@ -76,6 +76,11 @@ def _parse_steps(text):
             n = int(lines[i + 1].split()[0])
             key = {"DISPLACEMENT": "displ", "VELOCITY": "velocity", "ACCELERATION": "acceleration"}[t.split(".")[-1]]
             steps[-1][key] = np.array([[float(v) for v in lines[i + 2 + k].split()[1:4]] for k in range(n)])
+        elif t == "%RESULT.CASE.STEP.NODAL.REACTIONS":
+            n = int(lines[i + 1].split()[0])
+            rows = [lines[i + 2 + k].split() for k in range(n)]
+            steps[-1]["reaction_nodes"] = np.array([int(r[0]) - 1 for r in rows])
+            steps[-1]["reactions"] = np.array([[float(v) for v in r[1:4]] for r in rows])
         elif t in ("%RESULT.CASE.STEP.ELEMENT.GAUSS.SCALAR.DATA", "%RESULT.CASE.STEP.ELEMENT.NODAL.SCALAR.DATA"):
             ne, j, blocks = int(lines[i + 1]), i + 2, []
             gauss = "GAUSS" in t
@@ -193,4 +198,18 @@ def test_newmark_file_is_the_reference_file(tmp_path):
     assert len(steps) == 3 and all("velocity" in st and "acceleration" in st for st in steps)
     out = tmp_path / "out.pos"
     datfile.write_pos(str(out), str(dat), steps, precision=14, max_steps=3, header_line=ref.split(b"\n")[1].decode())
+    assert out.read_bytes() == ref
+
+
+def test_support_reactions_file_is_the_reference_file(tmp_path):
+    """%HEADER.PRINT.SUPPORT.REACTIONS: the reactions block (five digits,
+    right-aligned) after the displacements, and the step list padded the way
+    the stream's alignment leaves it."""
+    dat = tmp_path / "deck.dat"
+    dat.write_bytes(_text("reac_dat"))
+    ref = _text("reac_pos")
+    steps = _parse_steps(ref)
+    assert "reactions" in steps[0]
+    out = tmp_path / "out.pos"
+    datfile.write_pos(str(out), str(dat), steps, precision=14, max_steps=1, header_line=ref.split(b"\n")[1].decode())
     assert out.read_bytes() == ref
