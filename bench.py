@@ -405,6 +405,49 @@ def tied_blocks(local, args):
         "clocks": clk}
 
 
+def deck_io_and_output(S, deck, u, args):
+    """The host side around the hot path, on this box: the .dat deck of the
+    workload read by the library's parallel reader (beside the pure-Python
+    reader), and the printing step: Gauss-point and nodal stresses on the
+    device, then the .pos blocks formatted on all host cores (written to
+    /dev/null, so the figure is formatting, not disk)."""
+    from fast_b200 import datfile, decks
+    out = {"threads": os.cpu_count()}
+    with tempfile.TemporaryDirectory() as td:
+        path = decks.write_dat(deck, os.path.join(td, "deck"))
+        out["deck_bytes"] = os.path.getsize(path)
+        ts = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            dn = datfile.read_dat(path)
+            ts.append(time.perf_counter() - t0)
+        out["native_read_s"] = min(ts)
+        t0 = time.perf_counter()
+        dp = decks.read_dat(path)
+        out["python_read_s"] = time.perf_counter() - t0
+        out["readers_agree"] = bool(np.array_equal(dn.conn, dp.conn) and np.array_equal(dn.coords, dp.coords)
+                                    and np.array_equal(dn.E, dp.E))
+        S.set_displacement(u)
+        t0 = time.perf_counter()
+        _, gs = S.gauss_stress()
+        out["gauss_stress_s"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        en, avg = S.nodal_stress()
+        out["nodal_stress_s"] = time.perf_counter() - t0
+        eq = deck.node_eq()
+        displ = np.zeros((deck.num_nodes, 3))
+        m = eq > 0
+        displ[m] = u[eq[m] - 1]
+        t0 = time.perf_counter()
+        datfile.write_pos(os.devnull, path, [dict(factor=1.0, displ=displ, gauss_stress=gs, elem_nodal=en,
+                                                  nodal_avg=avg)], precision=15, print_average=True)
+        out["pos_format_s"] = time.perf_counter() - t0
+        out["pos_numbers"] = int(6 * (2 * deck.num_nodes + gs.shape[0] * gs.shape[1] + en.shape[0] * en.shape[1]))
+    out["note"] = ("stress times include the device-to-host copy of the results; the reference prints the same "
+                   "blocks through iostream one number at a time")
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -601,6 +644,12 @@ def run_ours(args):
         except Exception as ex:  # reported, not fatal
             base = {"value": None, "error": str(ex)[:200]}
 
+    io = None
+    if rank == 0 and world == 1 and not args.no_io:
+        try:
+            io = deck_io_and_output(S, deck, u_main, args)
+        except Exception as ex:  # reported, not fatal
+            io = {"error": str(ex)[:300]}
     S.close()
     cfg4 = None
     if not args.no_ensemble:
@@ -653,6 +702,7 @@ def run_ours(args):
             "tied_blocks": cfg2,
             "newton_plate": plate,
             "ensemble_and_dynamics": cfg4,
+            "deck_io_and_output": io,
         }
         print(json.dumps(line))
     if world > 1:
@@ -674,6 +724,7 @@ def main():
     ap.add_argument("--no-newton", action="store_true", help="skip the nonlinear plate (learned start) section")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the ensemble + Newmark section")
     ap.add_argument("--no-tied", action="store_true", help="skip the tied multi-block (hex8, hex20, B-spline) section")
+    ap.add_argument("--no-io", action="store_true", help="skip the deck reading / result formatting section")
     args = ap.parse_args()
     global NX, NY, NZ
     NX = NY = args.size
