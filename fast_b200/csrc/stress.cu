@@ -91,6 +91,119 @@ __global__ void gauss_stress(int64_t count, const int32_t *__restrict__ index, c
   so[5] = Gs * ev[5];
 }
 
+// B-spline / NURBS solids: the same per point, with the shape-function
+// derivatives of the element's knot spans from the Bezier-extracted span
+// tables (rational quotient N_a = B_a w_a / W as cShapeBspSolid), three
+// passes over the nodes: W and dW, the Jacobian, the displacement gradient.
+// A B-spline patch may be parametrised left-handed: only a zero or
+// non-finite det J is flagged, as in the stiffness kernels.
+template <int PR, int PS, int PT, int NG1>
+__global__ void bsp_gauss_stress(int64_t count, const int32_t *__restrict__ index, const int32_t *__restrict__ conn,
+                                 const double *__restrict__ E, const double *__restrict__ nu,
+                                 const double *__restrict__ X, const double *__restrict__ U,
+                                 const int32_t *__restrict__ span, const double *__restrict__ bas_r,
+                                 const double *__restrict__ bas_s, const double *__restrict__ bas_t,
+                                 const double *__restrict__ wt, int rational, double *__restrict__ strain,
+                                 double *__restrict__ stress, int32_t *__restrict__ status) {
+  constexpr int QR = PR + 1, QS = PS + 1, QT = PT + 1, NN = QR * QS * QT, NG = NG1 * NG1 * NG1;
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= count * NG) return;
+  const int64_t k = t / NG;
+  const int g = (int)(t - k * NG);
+  const int64_t e = index[k];
+  const int gl = g % NG1, gj = (g / NG1) % NG1, gi = g / (NG1 * NG1);
+  const double *br = bas_r + (size_t)span[4 * e] * NG1 * QR * 2 + gl * QR * 2;
+  const double *bs = bas_s + (size_t)span[4 * e + 1] * NG1 * QS * 2 + gj * QS * 2;
+  const double *bt = bas_t + (size_t)span[4 * e + 2] * NG1 * QT * 2 + gi * QT * 2;
+  const int32_t *en = conn + e * NN;
+  const bool rat = rational != 0;
+  double W = 1.0, Wr = 0.0, Ws = 0.0, Wt = 0.0;
+  if (rat) {
+    W = 0.0;
+    for (int a = 0; a < NN; a++) {
+      const int ia = a % QR, ja = (a / QR) % QS, ka = a / (QR * QS);
+      const double *fr = br + 2 * ia, *fs = bs + 2 * ja, *ft = bt + 2 * ka;
+      const double w = wt ? wt[en[a]] : 1.0;
+      W += fr[0] * fs[0] * ft[0] * w;
+      Wr += fr[1] * fs[0] * ft[0] * w;
+      Ws += fr[0] * fs[1] * ft[0] * w;
+      Wt += fr[0] * fs[0] * ft[1] * w;
+    }
+  }
+  auto dnat = [&](int a, double &d0, double &d1, double &d2) {
+    const int ia = a % QR, ja = (a / QR) % QS, ka = a / (QR * QS);
+    const double *fr = br + 2 * ia, *fs = bs + 2 * ja, *ft = bt + 2 * ka;
+    d0 = fr[1] * fs[0] * ft[0];
+    d1 = fr[0] * fs[1] * ft[0];
+    d2 = fr[0] * fs[0] * ft[1];
+    if (rat) {
+      const double w = wt ? wt[en[a]] : 1.0;
+      const double n = fr[0] * fs[0] * ft[0] * w / W;
+      d0 = (d0 * w - n * Wr) / W;
+      d1 = (d1 * w - n * Ws) / W;
+      d2 = (d2 * w - n * Wt) / W;
+    }
+  };
+  double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int a = 0; a < NN; a++) {
+    double d[3];
+    dnat(a, d[0], d[1], d[2]);
+    const double *x = X + 3 * (int64_t)en[a];
+#pragma unroll
+    for (int p = 0; p < 3; p++)
+#pragma unroll
+      for (int q = 0; q < 3; q++) J[3 * p + q] = fma(d[p], x[q], J[3 * p + q]);
+  }
+  const double det = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) +
+                     J[2] * (J[3] * J[7] - J[4] * J[6]);
+  if (!(fabs(det) > 0.0) || !isfinite(det)) atomicOr(status, 1);
+  const double id = 1.0 / ((det != 0.0) ? det : 1.0);
+  const double I[9] = {(J[4] * J[8] - J[5] * J[7]) * id,  -(J[1] * J[8] - J[2] * J[7]) * id,
+                       (J[1] * J[5] - J[2] * J[4]) * id,  -(J[3] * J[8] - J[5] * J[6]) * id,
+                       (J[0] * J[8] - J[2] * J[6]) * id,  -(J[0] * J[5] - J[2] * J[3]) * id,
+                       (J[3] * J[7] - J[4] * J[6]) * id,  -(J[0] * J[7] - J[1] * J[6]) * id,
+                       (J[0] * J[4] - J[1] * J[3]) * id};
+  double G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int a = 0; a < NN; a++) {
+    double d0, d1, d2;
+    dnat(a, d0, d1, d2);
+    const double gx = I[0] * d0 + I[1] * d1 + I[2] * d2;
+    const double gy = I[3] * d0 + I[4] * d1 + I[5] * d2;
+    const double gz = I[6] * d0 + I[7] * d1 + I[8] * d2;
+    const double *u = U + 4 * (int64_t)en[a];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      G[3 * i] = fma(u[i], gx, G[3 * i]);
+      G[3 * i + 1] = fma(u[i], gy, G[3 * i + 1]);
+      G[3 * i + 2] = fma(u[i], gz, G[3 * i + 2]);
+    }
+  }
+  const double ev[6] = {G[0], G[4], G[8], G[1] + G[3], G[2] + G[6], G[5] + G[7]};
+  const double En = E[e], v = nu[e];
+  const double dd = (1.0 + v) * (1.0 - 2.0 * v);
+  const double C00 = En * (1.0 - v) / dd, C01 = En * v / dd, Gs = 0.5 * En / (1.0 + v);
+  double *so = stress + t * 6, *eo = strain + t * 6;
+#pragma unroll
+  for (int c = 0; c < 6; c++) eo[c] = ev[c];
+  so[0] = C00 * ev[0] + C01 * (ev[1] + ev[2]);
+  so[1] = C00 * ev[1] + C01 * (ev[0] + ev[2]);
+  so[2] = C00 * ev[2] + C01 * (ev[0] + ev[1]);
+  so[3] = Gs * ev[3];
+  so[4] = Gs * ev[4];
+  so[5] = Gs * ev[5];
+}
+
+template <int PR, int PS, int PT, int NG1>
+cudaError_t run_bsp(Ctx &c, const Bucket &B, int64_t count, const int32_t *idx, double *st, double *ss) {
+  constexpr int NG = NG1 * NG1 * NG1;
+  const int64_t n = count * NG;
+  bsp_gauss_stress<PR, PS, PT, NG1><<<(unsigned)((n + 127) / 128), 128, 0, c.stream>>>(
+      count, idx, B.d_conn, B.d_E, B.d_nu, c.d_X, c.d_disp, B.d_span, B.d_bas + B.bas_off[0],
+      B.d_bas + B.bas_off[1], B.d_bas + B.bas_off[2], B.d_wt, B.rational, st, ss, c.d_status);
+  c.launches++;
+  return cudaGetLastError();
+}
+
 template <int NN, int NG>
 cudaError_t run(Ctx &c, const Bucket &B, int64_t count, const int32_t *idx, double *st, double *ss) {
   const int64_t n = count * NG;
@@ -172,8 +285,8 @@ extern "C" int fast_gpu_gauss_stress(fast_gpu_ctx *c, int32_t b, int64_t first, 
   if (!c || b < 0 || b >= (int)c->buckets.size() || !strain || !stress) return FAST_GPU_EINVAL;
   const Bucket &B = c->buckets[b];
   if (first < 0 || count <= 0 || first + count > B.ne) return FAST_GPU_EINVAL;
-  if (B.tl || B.type == FAST_ELEM_BSP_SOLID) {
-    c->err = "gauss_stress: small-strain hex buckets only";
+  if (B.tl) {
+    c->err = "gauss_stress: small-strain buckets only";
     return FAST_GPU_ENOTSUP;
   }
   const int ng = B.ng;
@@ -192,6 +305,16 @@ extern "C" int fast_gpu_gauss_stress(fast_gpu_ctx *c, int32_t b, int64_t first, 
   else if (B.type == FAST_ELEM_HEX20 && ng == 27) e = run<20, 27>(*c, B, count, d_idx, buf, buf + vals);
   else if (B.type == FAST_ELEM_HEX20 && ng == 8) e = run<20, 8>(*c, B, count, d_idx, buf, buf + vals);
   else if (B.type == FAST_ELEM_HEX20 && ng == 64) e = run<20, 64>(*c, B, count, d_idx, buf, buf + vals);
+  else if (B.type == FAST_ELEM_BSP_SOLID) {
+    const int *p = B.pd, g1 = B.ngp[0];
+    if (p[0] == 2 && p[1] == 2 && p[2] == 2 && g1 == 3) e = run_bsp<2, 2, 2, 3>(*c, B, count, d_idx, buf, buf + vals);
+    else if (p[0] == 2 && p[1] == 2 && p[2] == 2 && g1 == 4) e = run_bsp<2, 2, 2, 4>(*c, B, count, d_idx, buf, buf + vals);
+    else if (p[0] == 3 && p[1] == 3 && p[2] == 3 && g1 == 4) e = run_bsp<3, 3, 3, 4>(*c, B, count, d_idx, buf, buf + vals);
+    else if (p[0] == 3 && p[1] == 3 && p[2] == 2 && g1 == 4) e = run_bsp<3, 3, 2, 4>(*c, B, count, d_idx, buf, buf + vals);
+    else if (p[0] == 4 && p[1] == 2 && p[2] == 4 && g1 == 5) e = run_bsp<4, 2, 4, 5>(*c, B, count, d_idx, buf, buf + vals);
+    else if (p[0] == 4 && p[1] == 2 && p[2] == 2 && g1 == 5) e = run_bsp<4, 2, 2, 5>(*c, B, count, d_idx, buf, buf + vals);
+    else if (p[0] == 5 && p[1] == 2 && p[2] == 5 && g1 == 6) e = run_bsp<5, 2, 5, 6>(*c, B, count, d_idx, buf, buf + vals);
+  }
   SCK(e);
   SCK(cudaMemcpyAsync(strain, buf, sizeof(double) * vals, cudaMemcpyDeviceToHost, c->stream));
   SCK(cudaMemcpyAsync(stress, buf + vals, sizeof(double) * vals, cudaMemcpyDeviceToHost, c->stream));

@@ -545,7 +545,8 @@ int fast_gpu_support_reactions(fast_gpu_ctx *ctx, const uint8_t *supported, int3
 /* ---- stress recovery ----------------------------------------------------
  * Gauss-point strains and stresses at the current displacements
  * (fast_gpu_set_displacement): cElmParam::IntPntStress (elc/elmparam.cpp:
- * 859-935) for elements first .. first+count-1 of a small-strain hex bucket,
+ * 859-935) for elements first .. first+count-1 of a small-strain hex or
+ * B-spline bucket,
  * in the caller's element order; strain and stress are host arrays
  * [count][points][6], Voigt xx yy zz xy xz yz (engineering shears), points in
  * the Gauss rule's order (r fastest). */

@@ -140,6 +140,22 @@ def elem_stiff(deck, e):
     return K
 
 
+def elem_stress(deck, e, ue):
+    """Gauss-point strains and stresses [ngp][6] (Voigt xx yy zz xy xz yz,
+    engineering shears) of element e of a "bsp" deck at element displacements
+    ue (cElmParam::IntPntStress, elc/elmparam.cpp:859-935)."""
+    C = _cmatrix(float(deck.E[e]), float(deck.nu[e]))
+    nn = deck.conn.shape[1]
+    U = np.asarray(ue, dtype=np.float64).reshape(nn, 3)
+    st, ss = [], []
+    for c, dx in _points(deck, e):
+        H = U.T @ dx.T
+        ev = np.array([H[0, 0], H[1, 1], H[2, 2], H[0, 1] + H[1, 0], H[0, 2] + H[2, 0], H[1, 2] + H[2, 1]])
+        st.append(ev)
+        ss.append(C @ ev)
+    return np.array(st), np.array(ss)
+
+
 def elem_tl(deck, e, ue):
     """Total-Lagrangian tangent and internal force of element e of a "bsp"
     deck at element displacements ue (cElmParamTL::StiffMat / IntForce,

@@ -29,7 +29,7 @@
 //       --u) state:
 //         elm_strain, elm_stress [ne][nip][6]  cElement::IntPntStress
 //                                  (elc/elmparam.cpp:859-935), Voigt xx yy zz xy xz yz
-//         elm_nodal_stress [ne][nn][6]  cElmParam::NodalStress with extrapolation
+//         elm_nodal_stress [ne][nn][6]  (with --nodal) cElmParam::NodalStress with extrapolation
 //                                  (elc/elmparam.cpp:1304-1312, CompTRMatrix :1444-1535)
 //       With --reactions, at the same state:
 //         reactions [nnode][6]     cControl::SuppReactions (ctrl/ctrl.cpp:844-882)
@@ -143,7 +143,7 @@ static int mode_dump(int argc, char **argv)
 {
   string deck = argv[2];
   const char *outp = argv[3];
-  bool trip = true, solve = true, mass = false, stress = false, geom = false, reac = false;
+  bool trip = true, solve = true, mass = false, stress = false, geom = false, reac = false, nodal = false;
   const char *ufile = 0;
   double stol = -1.0;
   for (int a = 4; a < argc; a++)
@@ -155,6 +155,7 @@ static int mode_dump(int argc, char **argv)
     else if (s == "--stress") stress = true;
     else if (s == "--geom") geom = true;
     else if (s == "--reactions") reac = true;
+    else if (s == "--nodal") nodal = true;
     else if (s == "--u" && a + 1 < argc) ufile = argv[++a];
     else if (s == "--solver-tol" && a + 1 < argc) stol = atof(argv[++a]);
   }
@@ -275,13 +276,16 @@ static int mode_dump(int argc, char **argv)
         }
       // extrapolated nodal stresses from the stresses just stored (the
       // printing step's cElmParam::NodalStress)
-      elm->NodalStress(Nodal);
-      for (int a = 0; a < nen; a++)
-        for (int k = 0; k < 6; k++) SN[((size_t)e * nen + a) * 6 + k] = Nodal[a][k];
+      if (nodal)
+      {
+        elm->NodalStress(Nodal);
+        for (int a = 0; a < nen; a++)
+          for (int k = 0; k < 6; k++) SN[((size_t)e * nen + a) * 6 + k] = Nodal[a][k];
+      }
     }
     w.f8("elm_strain", {ne, nip, 6}, SE.data( ), SE.size( ));
     w.f8("elm_stress", {ne, nip, 6}, SS.data( ), SS.size( ));
-    w.f8("elm_nodal_stress", {ne, nen, 6}, SN.data( ), SN.size( ));
+    if (nodal) w.f8("elm_nodal_stress", {ne, nen, 6}, SN.data( ), SN.size( ));
   }
   if (reac && (ufile || solve))
   {

@@ -1,6 +1,6 @@
-"""Gauss-point strains and stresses on the device (fast_gpu_gauss_stress)
-against the reference's cElement::IntPntStress at its own solution.  Needs a
-B200."""
+"""Gauss-point strains and stresses on the device (fast_gpu_gauss_stress),
+hex and B-spline buckets, against the reference's cElement::IntPntStress at
+its own solution; nodal stresses and support reactions.  Needs a B200."""
 import numpy as np
 import pytest
 
@@ -51,7 +51,7 @@ def test_gauss_stress_rejects_total_lagrangian():
     s.close()
 
 
-@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("name", [n for n in CASES if "ref_elm_nodal_stress" in gio.load(n)[1]])
 def test_nodal_stress_matches_reference_printout(name):
     """Element-nodal (cElmParam::NodalStress) and averaged nodal stresses
     (cControl::PrintAvrNodalStress) against the reference harness and the

@@ -112,3 +112,17 @@ def test_total_lagrangian_bspline_element():
         # the force at a large-rotation, small-strain state loses digits to
         # cancellation in F^T F - I
         assert gio.rel(ge, g["ref_elm_g"][e]) < 1e-9
+
+
+def test_bspline_gauss_point_stresses():
+    """cElement::IntPntStress of a B-spline solid at the reference's solution
+    (strains and stresses of every Gauss point) from the oracle."""
+    d, g = gio.load("iga_p2_box")
+    eq = d.node_eq()
+    m = eq > 0
+    un = np.zeros((d.num_nodes, 3))
+    un[m] = g["ref_u"][eq[m] - 1]
+    for k, e in enumerate(g["ref_elems"]):
+        st, ss = io.elem_stress(d, int(e), un[d.conn[e]].ravel())
+        assert np.abs(st - g["ref_elm_strain"][k]).max() <= 1e-12 * np.abs(g["ref_elm_strain"]).max()
+        assert np.abs(ss - g["ref_elm_stress"][k]).max() <= 1e-12 * np.abs(g["ref_elm_stress"]).max()
