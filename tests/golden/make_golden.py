@@ -1,10 +1,9 @@
 """Regenerate the golden fixtures in this directory from the reference FAST
 program itself.
 
-Run in a container that has the reference tree (default /root/reference,
-override with FAST_REF):
+Run where the reference tree is present, with FAST_REF set to it:
 
-    python tests/golden/make_golden.py          (all fixtures)
+    FAST_REF=<reference tree> python tests/golden/make_golden.py          (all fixtures)
     python tests/golden/make_golden.py iga      (B-spline solid fixtures only)
     python tests/golden/make_golden.py stress   (the two fixtures with Gauss-point stresses)
     python tests/golden/make_golden.py arc      (the path-following fixture)
@@ -36,7 +35,9 @@ sys.path.insert(0, ROOT)
 from fast_b200 import decks  # noqa: E402
 from oracle import refdump  # noqa: E402
 
-FAST_REF = os.environ.get("FAST_REF", "/root/reference")
+FAST_REF = os.environ.get("FAST_REF", "")
+if __name__ == "__main__" and not os.path.isdir(FAST_REF):
+    sys.exit("set FAST_REF to the reference FAST source tree")
 
 
 def deck_arrays(d: decks.Deck) -> dict:
