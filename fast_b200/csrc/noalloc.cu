@@ -7,7 +7,20 @@
 // other stream of the process.  fast_gpu_pcg_solve_noalloc serves them: the
 // caller passes the matrix, the load and the solution buffer in device
 // memory; every work vector and reduction buffer of the solve lives in one
-// file-scope __device__ array below, reserved when the library is loaded.
+// file-scope __device__ array below.
+//
+// When that array gets its memory: it belongs to this file's module of the
+// library.  Under CUDA's lazy module loading (the default of the CUDA 12
+// runtime unless CUDA_MODULE_LOADING=EAGER is set) the module, and with it the
+// array, is loaded onto a device the first time anything in this file is used
+// there, i.e. inside the first call made on that device.  That first call may
+// therefore take device memory for the array (and fail with FAST_GPU_ECUDA if
+// the device has none left) and may synchronise the device.  A caller whose
+// own pool takes the device should make the first call, for instance the
+// set-up-only call with num_eq = 0, before the pool is created, and before any
+// stream capture; every later call allocates nothing and does not synchronise
+// the device (it synchronises only its own stream, to read the convergence
+// state).
 //
 // The solve is the same FP64 Jacobi PCG as fast_gpu_solve with
 // FAST_PREC_FP64 / FAST_PRECOND_JACOBI (same iteration, same stopping test
@@ -16,12 +29,12 @@
 // and result agree with that entry point to rounding.
 //
 // Limits and sharing: at most kNoAllocMaxEq equations (the array holds five
-// vectors of that length, 20 MB in all, on every device that loads the
-// library, until the process exits).  Every call uses the same array and it
-// keeps the previous call's contents; everything a solve needs is
-// re-initialised at the start of each call.  Two calls whose work overlaps on
-// the GPU (different streams, or different host threads) race on the array
-// and must not be issued.
+// vectors of that length, 20 MB in all, on every device that has loaded it,
+// until the process exits).  Every call uses the same array and it keeps the
+// previous call's contents; everything a solve needs is re-initialised at the
+// start of each call.  Two calls whose work overlaps on the GPU (different
+// streams, or different host threads) race on the array and must not be
+// issued.
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -33,7 +46,6 @@ namespace {
 constexpr int64_t kNoAllocMaxEq = 500000;
 constexpr int kNoAllocBlocks = 592;      // fixed reduction grid (4 x 148 SMs)
 constexpr int kNoAllocThreads = 256;
-constexpr int kNoAllocMaxDevices = 64;
 // scratch layout (doubles): r, z, p, w, dinv [kNoAllocMaxEq each];
 // partials [4][kNoAllocBlocks]; solver state
 constexpr size_t kOffR = 0, kOffZ = kNoAllocMaxEq, kOffP = 2 * kNoAllocMaxEq, kOffW = 3 * kNoAllocMaxEq,
@@ -43,10 +55,8 @@ constexpr size_t kScratchDoubles = kOffState + 32;
 
 __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
-// device address of g_noalloc_scratch per device ordinal, set on the first
-// call made with that device current
-double *g_scratch_addr[kNoAllocMaxDevices] = {};
-
+// done: 0 running, 1 converged, 2 maxit reached, 3 breakdown (p.Kp not
+// positive, or a non-finite value), 4 a row without a usable diagonal
 struct NaState {
   double dot0, alpha, beta, lenf, rr, err, tol;
   int32_t iter, done, maxit, pad;
@@ -76,18 +86,22 @@ __device__ __forceinline__ double na_sum_partials(const double *p, double *sbuf)
   return na_block_sum(v, sbuf);
 }
 
-// r = f, u = 0, dinv = 1/diag(K), z = dinv r, p = z; partials z.r and f.f
+// r = f, u = 0, dinv = 1/diag(K), z = dinv r, p = z; partials z.r, f.f and
+// the number of rows whose diagonal is not stored, zero or not finite (Jacobi
+// is undefined there; such a row gets dinv = 0 and the solve is rejected)
 __global__ void __launch_bounds__(kNoAllocThreads)
 na_init(int32_t n, const int64_t *__restrict__ rowptr, const int32_t *__restrict__ col,
         const double *__restrict__ val, const double *__restrict__ f, double *__restrict__ u, double *S) {
   __shared__ double sbuf[32];
   double *r = S + kOffR, *z = S + kOffZ, *p = S + kOffP, *dinv = S + kOffD, *part = S + kOffPart;
-  double zr = 0.0, ff = 0.0;
+  double zr = 0.0, ff = 0.0, bad = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double d = 0.0;
     for (int64_t k = rowptr[i]; k < rowptr[i + 1]; k++)
       if (col[k] == i) d = val[k];
-    const double di = 1.0 / d;
+    const bool usable = d != 0.0 && isfinite(d);
+    bad += usable ? 0.0 : 1.0;
+    const double di = usable ? 1.0 / d : 0.0;
     const double fi = f[i];
     dinv[i] = di;
     u[i] = 0.0;
@@ -101,6 +115,8 @@ na_init(int32_t n, const int64_t *__restrict__ rowptr, const int32_t *__restrict
   if (threadIdx.x == 0) part[blockIdx.x] = t1;
   const double t2 = na_block_sum(ff, sbuf);
   if (threadIdx.x == 0) part[kNoAllocBlocks + blockIdx.x] = t2;
+  const double t3 = na_block_sum(bad, sbuf);
+  if (threadIdx.x == 0) part[2 * kNoAllocBlocks + blockIdx.x] = t3;
 }
 
 __global__ void __launch_bounds__(kNoAllocThreads) na_init_scalar(double *S, double tol, int maxit) {
@@ -108,6 +124,7 @@ __global__ void __launch_bounds__(kNoAllocThreads) na_init_scalar(double *S, dou
   const double *part = S + kOffPart;
   const double zr = na_sum_partials(part, sbuf);
   const double ff = na_sum_partials(part + kNoAllocBlocks, sbuf);
+  const double bad = na_sum_partials(part + 2 * kNoAllocBlocks, sbuf);
   if (threadIdx.x == 0) {
     NaState s{};
     double lenf = sqrt(ff);
@@ -119,6 +136,7 @@ __global__ void __launch_bounds__(kNoAllocThreads) na_init_scalar(double *S, dou
     s.lenf = lenf;
     s.rr = ff;
     s.err = sqrt(ff) / (lenf > 0 ? lenf : 1.0);
+    if (bad > 0.0) s.done = 4;
     *reinterpret_cast<NaState *>(S + kOffState) = s;
   }
 }
@@ -220,22 +238,19 @@ extern "C" int fast_gpu_pcg_solve_noalloc(int32_t num_eq, const int64_t *d_rowpt
                                           int32_t maxit, void *cuda_stream, fast_gpu_solve_report *rep) {
   // the size limit is checked first, before any CUDA call
   if (num_eq > kNoAllocMaxEq) return FAST_GPU_ETOOBIG;
-  if (num_eq <= 0 || !d_rowptr || !d_col || !d_val || !d_f || !d_u) return FAST_GPU_EINVAL;
-  if (!(tol > 0)) tol = 1e-5;
-  if (maxit <= 0) maxit = 20 * num_eq;
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return FAST_GPU_ECUDA;
-  if (dev < 0 || dev >= kNoAllocMaxDevices) return FAST_GPU_EINVAL;
-  // once per device, with that device current: the device address of the
-  // scratch array (its host-side name is not a device address)
-  if (!g_scratch_addr[dev]) {
-    double *ptr = nullptr;
-    e = cudaGetSymbolAddress((void **)&ptr, g_noalloc_scratch);
-    if (e != cudaSuccess || !ptr) return FAST_GPU_ECUDA;
-    g_scratch_addr[dev] = ptr;
-  }
-  double *S = g_scratch_addr[dev];
+  if (num_eq < 0) return FAST_GPU_EINVAL;
+  if (num_eq > 0 && (!d_rowptr || !d_col || !d_val || !d_f || !d_u)) return FAST_GPU_EINVAL;
+  if (!(tol > 0)) tol = 1e-5;           // cSysMatrix's default tolerance
+  if (maxit <= 0) maxit = num_eq;       // cSysMatrix(n) sets maxit = n
+  // The device address of the scratch array, looked up on every call with
+  // the caller's device current: the array's host-side name is not a device
+  // address, and the address can change if the context is torn down and
+  // re-created (cudaDeviceReset), so it is never cached.  On the first call
+  // on a device this lookup is what loads this file's module there.
+  double *S = nullptr;
+  cudaError_t e = cudaGetSymbolAddress((void **)&S, g_noalloc_scratch);
+  if (e != cudaSuccess || !S) return FAST_GPU_ECUDA;
+  if (num_eq == 0) return FAST_GPU_OK;  // set-up only
   cudaStream_t s = (cudaStream_t)cuda_stream;
   const int G = kNoAllocBlocks, T = kNoAllocThreads;
   na_init<<<G, T, 0, s>>>(num_eq, d_rowptr, d_col, d_val, d_f, d_u, S);
@@ -267,6 +282,7 @@ extern "C" int fast_gpu_pcg_solve_noalloc(int32_t num_eq, const int64_t *d_rowpt
     rep->rel_residual = h.err;
     rep->true_rel_residual = -1.0;  // not recomputed here
   }
-  if (h.done != 1) return FAST_GPU_ENONCONV;
+  if (h.done == 4) return FAST_GPU_EINVAL;  // a row without a usable diagonal
+  if (h.done != 1) return FAST_GPU_ENONCONV;  // maxit reached (2) or breakdown (3)
   return FAST_GPU_OK;
 }
