@@ -10,6 +10,8 @@
 #include "fem_oracle.h"
 
 #include <math.h>
+#include <pthread.h>
+#include <unistd.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -566,6 +568,122 @@ int fo_pcg(int n, const int64_t *rowptr, const int32_t *col, const double *val,
   }
   *iters = conv ? k : maxit;
   *err_out = err;
+  free(r); free(p); free(d); free(w); free(z);
+  return conv;
+}
+
+/* The same iteration with every vector operation and the SpMV split over the
+ * host threads (pthreads, one static range of rows per thread): a
+ * large-system checker, not a restatement of the reference's loop order.
+ * Sums are per-thread partials combined in thread order, so a run is
+ * reproducible for a fixed thread count. */
+enum { PT_SPMV_DOT, PT_UPDATE, PT_PUPDATE, PT_INIT };
+typedef struct {
+  int op, n, t, nt;
+  const int64_t *rowptr; const int32_t *col; const double *val;
+  const double *f; double *u, *r, *p, *d, *w, *z;
+  double alpha, beta, s1, s2;
+} pt_job;
+
+static void *pt_run(void *arg)
+{
+  pt_job *j = (pt_job *)arg;
+  const int i0 = (int)((int64_t)j->n * j->t / j->nt), i1 = (int)((int64_t)j->n * (j->t + 1) / j->nt);
+  double s1 = 0.0, s2 = 0.0;
+  switch (j->op)
+  {
+    case PT_INIT:
+      for (int i = i0; i < i1; i++)
+      {
+        j->d[i] = 0.0;
+        for (int64_t k = j->rowptr[i]; k < j->rowptr[i + 1]; k++) if (j->col[k] == i) j->d[i] = j->val[k];
+        j->r[i] = j->f[i]; j->z[i] = j->r[i] / j->d[i]; j->p[i] = j->z[i];
+        s1 += j->z[i] * j->r[i];
+        s2 += j->f[i] * j->f[i];
+      }
+      break;
+    case PT_SPMV_DOT:   /* w = K p, p.w */
+      for (int i = i0; i < i1; i++)
+      {
+        double s = 0.0;
+        for (int64_t k = j->rowptr[i]; k < j->rowptr[i + 1]; k++) s += j->val[k] * j->p[j->col[k]];
+        j->w[i] = s;
+        s1 += j->p[i] * s;
+      }
+      break;
+    case PT_UPDATE:     /* u += a p; r -= a w; z = r / d; r.r, z.r */
+      for (int i = i0; i < i1; i++)
+      {
+        j->u[i] = j->u[i] + j->alpha * j->p[i];
+        j->r[i] = j->r[i] + (-j->alpha) * j->w[i];
+        j->z[i] = j->r[i] / j->d[i];
+        s1 += j->r[i] * j->r[i];
+        s2 += j->z[i] * j->r[i];
+      }
+      break;
+    case PT_PUPDATE:    /* p = z + b p */
+      for (int i = i0; i < i1; i++) j->p[i] = j->z[i] + j->beta * j->p[i];
+      break;
+  }
+  j->s1 = s1;
+  j->s2 = s2;
+  return NULL;
+}
+
+/* run one operation on nt threads; *s1, *s2 = partial sums combined in thread order */
+static void pt_parallel(pt_job *jobs, int nt, int op, double alpha, double beta, double *s1, double *s2)
+{
+  pthread_t th[64];
+  for (int t = 0; t < nt; t++)
+  {
+    jobs[t].op = op; jobs[t].alpha = alpha; jobs[t].beta = beta;
+    if (t > 0) pthread_create(&th[t], NULL, pt_run, &jobs[t]);
+  }
+  pt_run(&jobs[0]);
+  for (int t = 1; t < nt; t++) pthread_join(th[t], NULL);
+  double a = 0.0, b = 0.0;
+  for (int t = 0; t < nt; t++) { a += jobs[t].s1; b += jobs[t].s2; }
+  if (s1) *s1 = a;
+  if (s2) *s2 = b;
+}
+
+int fo_pcg_threaded(int n, const int64_t *rowptr, const int32_t *col, const double *val,
+                    const double *f, double *u, int maxit, double tol, int *iters, double *err_out)
+{
+  long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
+  int nt = ncpu < 1 ? 1 : (ncpu > 64 ? 64 : (int)ncpu);
+  memset(u, 0, sizeof(double) * n);
+  *iters = 0;
+  *err_out = 0.0;
+  double *r = malloc(sizeof(double) * n), *p = malloc(sizeof(double) * n);
+  double *d = malloc(sizeof(double) * n), *w = malloc(sizeof(double) * n), *z = malloc(sizeof(double) * n);
+  pt_job jobs[64];
+  for (int t = 0; t < nt; t++)
+  {
+    pt_job j = {0, n, t, nt, rowptr, col, val, f, u, r, p, d, w, z, 0.0, 0.0, 0.0, 0.0};
+    jobs[t] = j;
+  }
+  double dot0 = 0.0, ff = 0.0, err = 0.0;
+  pt_parallel(jobs, nt, PT_INIT, 0.0, 0.0, &dot0, &ff);
+  double lenf = sqrt(ff);
+  int conv = 0, k = 0;
+  if (lenf < tol) { conv = 1; goto out; }
+  if (lenf > 10e+10) lenf = 1.0;
+  for (k = 1; k <= maxit; k++)
+  {
+    double pw = 0.0, rr = 0.0, zr = 0.0;
+    pt_parallel(jobs, nt, PT_SPMV_DOT, 0.0, 0.0, &pw, NULL);
+    double alpha = dot0 / pw;
+    pt_parallel(jobs, nt, PT_UPDATE, alpha, 0.0, &rr, &zr);
+    err = sqrt(rr) / lenf;
+    if (err < tol) { conv = 1; break; }
+    double beta = zr / dot0;
+    dot0 = zr;
+    pt_parallel(jobs, nt, PT_PUPDATE, 0.0, beta, NULL, NULL);
+  }
+  *iters = conv ? k : maxit;
+  *err_out = err;
+out:
   free(r); free(p); free(d); free(w); free(z);
   return conv;
 }

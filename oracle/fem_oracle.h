@@ -70,6 +70,11 @@ int fo_face_load(int nf, int ngp1d, const double *Xf, const double *q, int local
 int fo_pcg(int n, const int64_t *rowptr, const int32_t *col, const double *val,
            const double *f, double *u, int maxit, double tol, int *iters, double *err);
 
+/* The same PCG with its vector operations and SpMV on all host threads
+ * (pthreads): a checker for systems of millions of equations. */
+int fo_pcg_threaded(int n, const int64_t *rowptr, const int32_t *col, const double *val,
+                    const double *f, double *u, int maxit, double tol, int *iters, double *err);
+
 /* y = A x for a full CSR matrix. */
 void fo_spmv(int n, const int64_t *rowptr, const int32_t *col, const double *val,
              const double *x, double *y);

@@ -44,6 +44,7 @@ def lib():
         L.fo_face_load.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp]
         L.fo_pcg.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32), _dp,
                              _dp, _dp, ctypes.c_int, ctypes.c_double, _ip, _dp]
+        L.fo_pcg_threaded.argtypes = L.fo_pcg.argtypes
         L.fo_spmv.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32), _dp, _dp, _dp]
         _lib = L
     return _lib
@@ -259,6 +260,58 @@ def pcg(K, f, tol, maxit):
     ok = lib().fo_pcg(n, _p(rp, ctypes.POINTER(ctypes.c_int64)), _p(ci, ctypes.POINTER(ctypes.c_int32)), _p(v),
                       _p(f), _p(u), int(maxit), float(tol), ctypes.byref(it), ctypes.byref(err))
     return u, bool(ok), it.value, err.value
+
+
+def pcg_threaded(K, f, tol, maxit):
+    """pcg() with the SpMV and vector operations on all host threads;
+    returns (u, iterations, recurrence error)."""
+    n = K.shape[0]
+    rp = np.ascontiguousarray(K.indptr, dtype=np.int64)
+    ci = np.ascontiguousarray(K.indices, dtype=np.int32)
+    v = np.ascontiguousarray(K.data, dtype=np.float64)
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    u = np.zeros(n)
+    it = ctypes.c_int(0)
+    err = ctypes.c_double(0)
+    ok = lib().fo_pcg_threaded(n, _p(rp, ctypes.POINTER(ctypes.c_int64)), _p(ci, ctypes.POINTER(ctypes.c_int32)),
+                               _p(v), _p(f), _p(u), int(maxit), float(tol), ctypes.byref(it), ctypes.byref(err))
+    if not ok:
+        raise RuntimeError("pcg_threaded: no convergence in %d iterations (err %.3e)" % (it.value, err.value))
+    return u, it.value, err.value
+
+
+def assemble_chunked(deck, chunk=16384, threads=None):
+    """assemble() for large meshes: element matrices computed in chunks on
+    all host threads (the C restatement releases the GIL), each chunk summed
+    into the equation-space CSR matrix as it is produced."""
+    import scipy.sparse as sp
+    from concurrent.futures import ThreadPoolExecutor
+    neq = deck.num_eq()
+    dofs_all = elem_dofs(deck)
+    nd = dofs_all.shape[1]
+    ne = deck.num_elems
+    starts = list(range(0, ne, chunk))
+
+    def work(a):
+        b = min(ne, a + chunk)
+        Ke, rc = elems_stiff(deck, np.arange(a, b))
+        if rc != 0:
+            raise RuntimeError("element stiffness failed in elements %d..%d" % (a, b))
+        dofs = dofs_all[a:b]
+        I = np.repeat(dofs, nd, axis=1).ravel()
+        J = np.tile(dofs, (1, nd)).ravel()
+        m = (I > 0) & (J > 0)
+        C = sp.csr_matrix((Ke.reshape(b - a, -1).ravel()[m], (I[m] - 1, J[m] - 1)), shape=(neq, neq))
+        C.sum_duplicates()
+        return C
+
+    K = None
+    with ThreadPoolExecutor(max_workers=threads or os.cpu_count()) as ex:
+        for C in ex.map(work, starts):
+            K = C if K is None else K + C
+    K.sum_duplicates()
+    K.sort_indices()
+    return K
 
 
 def mass_matrix(deck):

@@ -36,11 +36,12 @@
 //       With --geom, at the same state:
 //         elm_G [ne][ndof][ndof]   cElmParam::GeomStiff (elc/elmparam.cpp:743-830)
 //
-//   fastref bench <deck> <pcg_iters> [reps]
+//   fastref bench <deck> <pcg_iters> [reps] [pcg_iters2]
 //       Times the reference CPU path on one host thread: StiffnessMatrix into
 //       the deck's sparse matrix (cSymSprsMatrix, mlib/sysmat.cpp:889) once,
 //       then [reps] (default 1) runs of <pcg_iters> iterations of PCGSolver
-//       (mlib/sysmat.cpp:1061), each timed.  Prints one JSON line.
+//       (mlib/sysmat.cpp:1061), each timed, each followed (when given) by a
+//       run of <pcg_iters2> iterations.  Prints one JSON line.
 
 #include <chrono>
 #include <cmath>
@@ -325,6 +326,7 @@ static int mode_bench(int argc, char **argv)
   string deck = argv[2];
   int iters = argc > 3 ? atoi(argv[3]) : 5;
   int reps = argc > 4 ? atoi(argv[4]) : 1;
+  int iters2 = argc > 5 ? atoi(argv[5]) : 0;
   if (reps < 1) reps = 1;
   streambuf *coutbuf = cout.rdbuf( );
   ofstream devnull("/dev/null");
@@ -351,19 +353,30 @@ static int mode_bench(int argc, char **argv)
   for (int e = 0; e < ne; e++) cElement::GetElm(e)->StiffMat(Ke);
   double t_int = now_s( ) - t2;
 
+  // each rep runs PCGSolver with `iters` iterations and, when a second count
+  // is given, once more with `iters2`: the difference separates the cost per
+  // iteration from the solver's set-up (its diagonal read through Get)
   cVector u(neq);
-  vector<double> t_pcg(reps);
+  vector<double> t_pcg(reps), t_pcg2(iters2 > 0 ? reps : 0);
   for (int r = 0; r < reps; r++)
   {
     double t3 = now_s( );
     PCGSolver(iters, 1e-300, K, f, u);
     t_pcg[r] = now_s( ) - t3;
+    if (iters2 > 0)
+    {
+      double t4 = now_s( );
+      PCGSolver(iters2, 1e-300, K, f, u);
+      t_pcg2[r] = now_s( ) - t4;
+    }
   }
   cout.rdbuf(coutbuf);
   printf("{\"neq\": %d, \"ne\": %d, \"nnz_lower\": %lld, \"read_s\": %.6f, \"assembly_s\": %.6f, "
          "\"integration_s\": %.6f, \"pcg_iters\": %d, \"pcg_s\": %.6f, \"pcg_rep_s\": [",
          neq, ne, nnz_lower, t_read, t_asm, t_int, iters, t_pcg[0]);
   for (int r = 0; r < reps; r++) printf("%s%.6f", r ? ", " : "", t_pcg[r]);
+  printf("], \"pcg_iters2\": %d, \"pcg_rep2_s\": [", iters2);
+  for (size_t r = 0; r < t_pcg2.size( ); r++) printf("%s%.6f", r ? ", " : "", t_pcg2[r]);
   printf("]}\n");
   return 0;
 }

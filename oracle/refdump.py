@@ -51,8 +51,8 @@ def run_dump(deck_base: str, out_path: str, *opts: str) -> dict:
     return read(out_path)
 
 
-def run_bench(deck_base: str, pcg_iters: int, reps: int = 1) -> dict:
-    r = subprocess.run([FASTREF, "bench", deck_base, str(pcg_iters), str(reps)], check=True,
+def run_bench(deck_base: str, pcg_iters: int, reps: int = 1, pcg_iters2: int = 0) -> dict:
+    r = subprocess.run([FASTREF, "bench", deck_base, str(pcg_iters), str(reps), str(pcg_iters2)], check=True,
                        capture_output=True, text=True)
     return json.loads(r.stdout.strip().splitlines()[-1])
 

@@ -91,3 +91,19 @@ def solve(deck, f, tol=1e-13, maxit=200000, K=None):
     ft[slave] = 0.0
     ut, ok, it, err = fo.pcg(Kt, ft, tol, maxit)
     return T @ ut, ok, it
+
+
+def solve_full(deck, tol=1e-13, maxit=500000):
+    """solve() for the full-size column: nodal load of the deck, the PCG on all
+    host threads; returns u and a dict of what the fixture records."""
+    from fast_b200 import decks
+    f = decks.nodal_load_vector(deck)
+    K = assemble(deck)
+    Kt, T, slave = reduced(deck, K)
+    ft = T.T @ f
+    ft[slave] = 0.0
+    ut, it, err = fo.pcg_threaded(Kt, ft, tol, maxit)
+    u = T @ ut
+    true_res = np.linalg.norm(ft - Kt @ ut) / np.linalg.norm(ft)
+    return u, dict(iterations=it, rec_err=err, true_rel_residual=true_res, neq=K.shape[0],
+                   f_norm2=np.linalg.norm(f), nnz_reduced=Kt.nnz)

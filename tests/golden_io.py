@@ -10,7 +10,7 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 # fixtures that hold no deck (.pos files with the numbers they print)
-NOT_DECKS = {"pos_output"}
+NOT_DECKS = {"pos_output", "full_hex20_64x64x32", "full_plate_tl_40x40x4", "full_tied_column"}
 
 
 def names():
