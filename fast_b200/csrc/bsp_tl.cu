@@ -68,6 +68,7 @@ __global__ void __launch_bounds__(NT, 1) bsp_tl_kernel(ElemArgs A, int split) {
   constexpr int NW = NT / 32;
   const int lane = tid & 31, warp = tid >> 5;
 
+  if (A.skip && *A.skip) return;
   for (int64_t wi = blockIdx.x; wi < A.ne * split; wi += gridDim.x) {
     const int64_t it = wi / split;
     const int part = (int)(wi - it * split);

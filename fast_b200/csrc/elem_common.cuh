@@ -24,6 +24,7 @@ struct ElemArgs {
   int32_t *status;            // bit 0: non-positive Jacobian determinant
   const double *U;            // [nnode][4] nodal displacements (total-Lagrangian / internal force)
   double *G;                  // [nnode][4] internal force, added to (colour-safe) or null
+  const int32_t *skip;        // optional device flag: the launch does nothing when it is non-zero
   // B-spline solids
   const int32_t *span;        // [*][4] colour-sorted knot spans (r, s, t, unused)
   const double *bas[3];       // per direction [nspan][ngp][p+1][2] {N, dN/dt}

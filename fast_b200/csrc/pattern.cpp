@@ -332,6 +332,8 @@ bool build_pattern(Ctx &c, const fast_gpu_mesh &m) {
         for (size_t x = 0; x < tids.size(); x++) order[fill[color[x]]++] = tids[x];
       }
       T.h_nptr.assign(T.n + 1, 0);
+      T.h_eptr.assign(1, 0);
+      T.h_econn.clear();
       T.h_sptr.assign(T.n + 1, 0);
       T.h_pptr.assign(1, 0);
       for (int64_t x = 0; x < T.n; x++) {
@@ -372,6 +374,9 @@ bool build_pattern(Ctx &c, const fast_gpu_mesh &m) {
         T.h_sptr[x + 1] = (int64_t)T.h_slot.size();
         T.h_keoff.push_back(keoff_of[g]);
         T.h_nn.push_back(nn);
+        // its own nodes, in the element's local order (node-space products)
+        T.h_econn.insert(T.h_econn.end(), bk.conn + e * nn, bk.conn + (e + 1) * nn);
+        T.h_eptr.push_back((int64_t)T.h_econn.size());
       }
     }
   }

@@ -33,13 +33,13 @@ namespace {
 constexpr int kTiedThreads = 1024;
 
 // STAGE: the element matrix is first copied to shared memory (when it fits)
-template <bool STAGE>
+template <bool STAGE, typename KT>
 __global__ void __launch_bounds__(kTiedThreads) tied_scatter(int64_t first, int64_t count, const int64_t *__restrict__ nptr,
                              const int32_t *__restrict__ nodes, const int64_t *__restrict__ sptr,
                              const int32_t *__restrict__ slot, const int64_t *__restrict__ pptr,
                              const int32_t *__restrict__ pa, const double *__restrict__ pt,
                              const int64_t *__restrict__ keoff, const int32_t *__restrict__ nn_of,
-                             const double *__restrict__ ke, const uint8_t *__restrict__ fix, double *__restrict__ K) {
+                             const double *__restrict__ ke, const uint8_t *__restrict__ fix, KT *__restrict__ K) {
   extern __shared__ double sKe[];
   for (int64_t it = blockIdx.x; it < count; it += gridDim.x) {
     const int64_t x = first + it;
@@ -72,12 +72,12 @@ __global__ void __launch_bounds__(kTiedThreads) tied_scatter(int64_t first, int6
         }
       }
       const uint8_t fa = fix[nodes[n0 + A]], fb = fix[nodes[n0 + B]];
-      double *Kb = K + (int64_t)sl[q] * 9;
+      KT *Kb = K + (int64_t)sl[q] * 9;
 #pragma unroll
       for (int i = 0; i < 3; i++)
 #pragma unroll
         for (int j = 0; j < 3; j++)
-          if (!((fa >> i) & 1) && !((fb >> j) & 1)) Kb[3 * i + j] += v[3 * i + j];
+          if (!((fa >> i) & 1) && !((fb >> j) & 1)) Kb[3 * i + j] += (KT)v[3 * i + j];
     }
     __syncthreads();
   }
@@ -161,6 +161,8 @@ cudaError_t upload_ties(Ctx &c) {
     if (e == cudaSuccess) e = upload(&T.d_pt, T.h_pt);
     if (e == cudaSuccess) e = upload(&T.d_keoff, T.h_keoff);
     if (e == cudaSuccess) e = upload(&T.d_nn, nn);
+    if (e == cudaSuccess) e = upload(&T.d_eptr, T.h_eptr);
+    if (e == cudaSuccess) e = upload(&T.d_econn, T.h_econn);
     if (e == cudaSuccess) e = cudaMalloc((void **)&T.d_ke, sizeof(double) * std::max<int64_t>(1, T.ke_total));
     T.d_bucket_pos.assign(T.bucket_pos.size(), nullptr);
     for (size_t b = 0; b < T.bucket_pos.size() && e == cudaSuccess; b++)
@@ -207,6 +209,7 @@ void free_ties(Ctx &c) {
   TiedSet &T = c.tied;
   release(T.d_nptr); release(T.d_nodes); release(T.d_sptr); release(T.d_slot); release(T.d_pptr);
   release(T.d_pa); release(T.d_pt); release(T.d_keoff); release(T.d_nn); release(T.d_ke);
+  release(T.d_eptr); release(T.d_econn);
   for (int32_t *&p : T.d_bucket_pos) release(p);
   T = TiedSet();
   TieMaps &M = c.tmaps;
@@ -216,11 +219,12 @@ void free_ties(Ctx &c) {
   c.h_tslave.clear(); c.h_tptr.clear(); c.h_tmaster.clear(); c.h_tweight.clear(); c.h_slave_of.clear();
 }
 
-cudaError_t launch_tied_assemble(Ctx &c, double *K) {
+// the tied scatter of every tied colour into K (element matrices already in
+// the scratch buffer)
+template <typename KT>
+static cudaError_t tied_scatter_all(Ctx &c, KT *K) {
   TiedSet &T = c.tied;
-  if (T.n == 0) return cudaSuccess;
-  cudaError_t e = launch_tied_element_matrices(c);
-  if (e != cudaSuccess) return e;
+  cudaError_t e = cudaSuccess;
   for (size_t k = 0; k + 1 < T.color_off.size(); k++) {
     const int64_t first = T.color_off[k], cnt = T.color_off[k + 1] - first;
     if (cnt <= 0) continue;
@@ -231,16 +235,79 @@ cudaError_t launch_tied_assemble(Ctx &c, double *K) {
     for (int32_t v : T.h_nn) maxnn = std::max(maxnn, v);
     const size_t smem = sizeof(double) * 9 * maxnn * maxnn;
     if (smem <= 96 * 1024) {
-      e = cudaFuncSetAttribute(tied_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      e = cudaFuncSetAttribute(tied_scatter<true, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e != cudaSuccess) return e;
-      tied_scatter<true><<<grid, kTiedThreads, smem, c.stream>>>(first, cnt, T.d_nptr, T.d_nodes, T.d_sptr, T.d_slot, T.d_pptr,
-                                                        T.d_pa, T.d_pt, T.d_keoff, T.d_nn, T.d_ke, c.d_fix, K);
+      tied_scatter<true, KT><<<grid, kTiedThreads, smem, c.stream>>>(first, cnt, T.d_nptr, T.d_nodes, T.d_sptr,
+                                                                      T.d_slot, T.d_pptr, T.d_pa, T.d_pt, T.d_keoff,
+                                                                      T.d_nn, T.d_ke, c.d_fix, K);
     } else {
-      tied_scatter<false><<<grid, kTiedThreads, 0, c.stream>>>(first, cnt, T.d_nptr, T.d_nodes, T.d_sptr, T.d_slot, T.d_pptr,
-                                                      T.d_pa, T.d_pt, T.d_keoff, T.d_nn, T.d_ke, c.d_fix, K);
+      tied_scatter<false, KT><<<grid, kTiedThreads, 0, c.stream>>>(first, cnt, T.d_nptr, T.d_nodes, T.d_sptr, T.d_slot,
+                                                                    T.d_pptr, T.d_pa, T.d_pt, T.d_keoff, T.d_nn,
+                                                                    T.d_ke, c.d_fix, K);
     }
     c.launches++;
     e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_tied_assemble(Ctx &c, double *K) {
+  TiedSet &T = c.tied;
+  if (T.n == 0) return cudaSuccess;
+  cudaError_t e = launch_tied_element_matrices(c);
+  if (e != cudaSuccess) return e;
+  return tied_scatter_all<double>(c, K);
+}
+
+cudaError_t launch_tied_assemble32(Ctx &c, float *K32) {
+  TiedSet &T = c.tied;
+  if (T.n == 0) return cudaSuccess;
+  cudaError_t e = launch_tied_element_matrices(c);
+  if (e != cudaSuccess) return e;
+  return tied_scatter_all<float>(c, K32);
+}
+
+// G += K_e u_e per tied element, one CTA per element of one colour: the
+// element's displacements gathered to shared memory, one thread per row of
+// K_e, the node sums written by the rows of that node (colour-safe)
+__global__ void __launch_bounds__(256) tied_matvec(int64_t first, int64_t count, const int64_t *__restrict__ eptr,
+                                                   const int32_t *__restrict__ econn,
+                                                   const int64_t *__restrict__ keoff, const int32_t *__restrict__ nn_of,
+                                                   const double *__restrict__ ke, const double *__restrict__ u,
+                                                   const uint8_t *__restrict__ fix, double *__restrict__ G,
+                                                   const int32_t *__restrict__ skip) {
+  if (skip && *skip) return;
+  __shared__ double su[3 * 64];
+  for (int64_t it = blockIdx.x; it < count; it += gridDim.x) {
+    const int64_t x = first + it;
+    const int nn = nn_of[x], nd = 3 * nn;
+    const int32_t *en = econn + eptr[x];
+    const double *Ke = ke + keoff[x];
+    __syncthreads();
+    for (int i = threadIdx.x; i < nd; i += blockDim.x) su[i] = u[4 * (int64_t)en[i / 3] + (i % 3)];
+    __syncthreads();
+    for (int r = threadIdx.x; r < nd; r += blockDim.x) {
+      const int a = r / 3, i = r - 3 * a;
+      if ((fix[en[a]] >> i) & 1) continue;
+      const double *row = Ke + (int64_t)r * nd;
+      double g = 0.0;
+      for (int k = 0; k < nd; k++) g = fma(row[k], su[k], g);
+      G[4 * (int64_t)en[a] + i] += g;
+    }
+  }
+}
+
+cudaError_t launch_tied_matvec(Ctx &c, const double *u, double *G, const int32_t *skip) {
+  TiedSet &T = c.tied;
+  for (size_t k = 0; k + 1 < T.color_off.size(); k++) {
+    const int64_t first = T.color_off[k], cnt = T.color_off[k + 1] - first;
+    if (cnt <= 0) continue;
+    const unsigned grid = (unsigned)std::min<int64_t>(cnt, 4LL * c.sm_count);
+    tied_matvec<<<grid, 256, 0, c.stream>>>(first, cnt, T.d_eptr, T.d_econn, T.d_keoff, T.d_nn, T.d_ke, u, c.d_fix,
+                                            G, skip);
+    c.launches++;
+    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;

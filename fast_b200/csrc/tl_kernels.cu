@@ -59,6 +59,7 @@ __global__ void __launch_bounds__(NT, (NT >= 128 ? 3 : 8)) tl_kernel(ElemArgs A)
   int pa = 0, pb = 0;
   if (tid < NP) pair_of(tid, NN, pa, pb);
 
+  if (A.skip && *A.skip) return;
   for (int64_t it = blockIdx.x; it < A.ne; it += gridDim.x) {
     const int64_t e = A.index ? (int64_t)A.index[it] : A.offset + it;
     __syncthreads();
@@ -353,6 +354,10 @@ static ElemArgs tl_args(Ctx &c, const Bucket &B, double *K, double *G) {
 // current displacements.  Small-strain buckets: internal force only (their
 // stiffness comes from launch_assemble).
 cudaError_t launch_tl(Ctx &c, double *K, double *G, bool want_k, bool want_g) {
+  return launch_tl_at(c, K, G, want_k, want_g, c.d_disp, nullptr);
+}
+
+cudaError_t launch_tl_at(Ctx &c, double *K, double *G, bool want_k, bool want_g, const double *U, const int32_t *skip) {
   for (size_t b = 0; b < c.buckets.size(); b++) {
     const Bucket &B = c.buckets[b];
     int mode;
@@ -365,6 +370,8 @@ cudaError_t launch_tl(Ctx &c, double *K, double *G, bool want_k, bool want_g) {
     }
     for (size_t k = 0; k + 1 < B.color_off.size(); k++) {
       ElemArgs a = tl_args(c, B, (B.tl && want_k) ? K : nullptr, want_g ? G : nullptr);
+      a.U = U;
+      a.skip = skip;
       a.offset = B.color_off[k];
       const int64_t cnt = B.color_off[k + 1] - B.color_off[k];
       cudaError_t e = B.type == FAST_ELEM_BSP_SOLID ? launch_bsp_tl(c, B, a, cnt, mode)
