@@ -76,6 +76,18 @@ extern "C" int fast_gpu_autotune(fast_gpu_ctx *c, fast_gpu_tune_report *rep) {
     if (R.ms_fp32[i] < b32) { b32 = R.ms_fp32[i]; best32 = lanes[i]; }
     if (R.ms_fp64[i] < b64) { b64 = R.ms_fp64[i]; best64 = lanes[i]; }
   }
+  // the bulk-staged FP32 SpMV (matrix through shared memory), 8 and 16 lanes
+  bool bulk = false;
+  const bool tiles = ensure_bulk_tiles(*c) == cudaSuccess;  // rows too long for shared memory: not offered
+  (void)cudaGetLastError();
+  c->spmv32_bulk = tiles;
+  for (int i = 0; i < 2 && tiles; i++) {
+    c->lpr32 = i == 0 ? 8 : 16;
+    ATK(median_ms(*c, [&] { return launch_spmv32(*c, c->d_Ks32, c->s_p, c->s_w); }, 9, R.ms_fp32_bulk[i]));
+    if (R.ms_fp32_bulk[i] < b32) { b32 = R.ms_fp32_bulk[i]; best32 = c->lpr32; bulk = true; }
+  }
+  c->spmv32_bulk = bulk;
+  R.bulk_fp32 = bulk ? 1 : 0;
   c->lpr32 = best32;
   c->lpr64 = best64;
   c->drop_graphs();

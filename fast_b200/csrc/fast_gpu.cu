@@ -50,6 +50,9 @@ void free_mesh(Ctx &c) {
   free_face_loads(c);
   dfree(c.d_X); dfree(c.d_fix); dfree(c.d_dof_of_eq);
   dfree(c.d_rowptr); dfree(c.d_col); dfree(c.d_diag); dfree(c.d_srow); dfree(c.d_scol);
+  dfree(c.d_tile_row);
+  c.bulk_ntiles = 0;
+  c.spmv32_bulk = false;
   dfree(c.d_K); dfree(c.d_M); dfree(c.d_Ks); dfree(c.d_Ms); dfree(c.d_Ks32);
   dfree(c.d_u); dfree(c.d_r); dfree(c.d_z); dfree(c.d_p); dfree(c.d_w); dfree(c.d_f); dfree(c.d_dinv);
   dfree(c.d_p2); dfree(c.s_p2);
@@ -99,6 +102,20 @@ cudaError_t ensure_soa(Ctx &c, int what, bool fp32) {
     if (!c.Ms_ok) { e = launch_to_soa(c, c.d_M, c.d_Ms, nullptr); c.Ms_ok = (e == cudaSuccess); }
     return e;
   }
+  if (c.K32_current) {
+    // the tensor-core stiffness: FP32 copy only (there is no FP64 stiffness)
+    if (!fp32) return cudaErrorInvalidValue;
+    if (!c.d_Ks32) {
+      if ((e = cudaMalloc((void **)&c.d_Ks32, sizeof(float) * nv)) != cudaSuccess) return e;
+      if ((e = cudaMemsetAsync(c.d_Ks32, 0, sizeof(float) * nv, c.stream)) != cudaSuccess) return e;
+      c.Ks_ok = false;
+    }
+    if (!c.Ks_ok) {
+      e = launch_to_soa32(c, c.d_K32, c.d_Ks32);
+      c.Ks_ok = (e == cudaSuccess);
+    }
+    return e;
+  }
   if (!c.d_Ks) {
     if ((e = cudaMalloc((void **)&c.d_Ks, sizeof(double) * nv)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(c.d_Ks, 0, sizeof(double) * nv, c.stream)) != cudaSuccess) return e;
@@ -125,6 +142,12 @@ int64_t value_index(const Ctx &c, int32_t i, int32_t j) {
   const int32_t *p = std::lower_bound(b0, b1, nj);
   if (p == b1 || *p != nj) return -1;
   return (int64_t)(p - c.h_col.data()) * 9 + pi * 3 + pj;
+}
+
+// dst += a src over 9 * nnzb block entries (both slots share the pattern)
+__global__ void add_mat_kernel(int64_t n, double a, const double *__restrict__ src, double *__restrict__ dst) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = dst[i] + a * src[i];
 }
 
 }  // namespace
@@ -184,6 +207,19 @@ int fast_gpu_set_option(fast_gpu_ctx *c, int32_t option, int64_t value) {
     (option == FAST_OPT_SPMV_LANES_FP32 ? c->lpr32 : c->lpr64) = (int)value;
     return FAST_GPU_OK;
   }
+  if (option == FAST_OPT_SPMV_BULK_FP32) {
+    if (value != 0 && value != 1) return FAST_GPU_EINVAL;
+    CK(cudaStreamSynchronize(c->stream));
+    if (value) CK(ensure_bulk_tiles(*c));
+    c->drop_graphs();
+    c->spmv32_bulk = value != 0;
+    return FAST_GPU_OK;
+  }
+  if (option == FAST_OPT_GRAPH_STEPS) {
+    if (value != 0 && value != 1) return FAST_GPU_EINVAL;
+    c->graph_steps = value != 0;
+    return FAST_GPU_OK;
+  }
   return FAST_GPU_EINVAL;
 }
 
@@ -199,6 +235,7 @@ int fast_gpu_destroy(fast_gpu_ctx *c) {
   dfree(c->d_partials);
   if (c->d_bar) cudaFree(c->d_bar);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  if (c->side_stream) cudaStreamDestroy(c->side_stream);
   delete c;
   return FAST_GPU_OK;
 }
@@ -519,14 +556,45 @@ int fast_gpu_zero(fast_gpu_ctx *c, int32_t what) {
   double *T = target_of(*c, what);
   if (!T) return FAST_GPU_EINVAL;
   CK(launch_zero_matrix(*c, T, what == FAST_ASM_STIFFNESS));
-  if (what == FAST_ASM_STIFFNESS) c->K_ok = true; else c->M_ok = true;
+  if (what == FAST_ASM_STIFFNESS) { c->K_ok = true; c->K32_current = false; } else c->M_ok = true;
   invalidate(*c, what);
   return FAST_GPU_OK;
 }
 
+namespace {
+// FAST_ASM_STIFFNESS_TF32: the stiffness on the tensor cores, FP32 blocks
+int assemble_tf32(fast_gpu_ctx *c) {
+  for (const Bucket &B : c->buckets)
+    if (!tc_supported(B)) {
+      c->err = "assemble: the tensor-core stiffness takes small-strain hex8 / hex20 and B-spline (2,2,2), "
+               "(3,3,3), (3,3,2) buckets only";
+      return FAST_GPU_ENOTSUP;
+    }
+  if (!c->d_K32) CK(cudaMalloc((void **)&c->d_K32, sizeof(float) * 9 * (size_t)c->nnzb));
+  CK(cudaMemsetAsync(c->d_status, 0, sizeof(int32_t), c->stream));
+  c->begin_span(FAST_KERNEL_ASSEMBLE_TF32);
+  CK(launch_assemble_tc(*c, c->d_K32));
+  c->end_span();
+  CK(cudaMemcpyAsync(c->h_status, c->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->harvest();
+  c->K32_current = true;
+  c->K_ok = false;          // the FP64 stiffness slot no longer holds the current stiffness
+  invalidate(*c, FAST_ASM_STIFFNESS);
+  if (c->h_status[0] & 4) { c->err = "assemble: a tensor-core kernel's wait timed out"; return FAST_GPU_ECUDA; }
+  if (c->h_status[0] & 1) {
+    c->err = "assemble: non-positive Jacobian determinant in at least one element";
+    return FAST_GPU_EDETJ;
+  }
+  return FAST_GPU_OK;
+}
+}  // namespace
+
 int fast_gpu_assemble(fast_gpu_ctx *c, int32_t what) {
   if (check_ctx(c) || !c->d_K) { if (c) c->err = "assemble: no mesh"; return FAST_GPU_ESTATE; }
+  if (what == FAST_ASM_STIFFNESS_TF32) return assemble_tf32(c);
   if (what != FAST_ASM_STIFFNESS && what != FAST_ASM_MASS) return FAST_GPU_EINVAL;
+  if (what == FAST_ASM_STIFFNESS) c->K32_current = false;
   if (what == FAST_ASM_MASS && !c->d_M) CK(dalloc(&c->d_M, 9 * c->nnzb));
   double *T = target_of(*c, what);
   CK(cudaMemsetAsync(c->d_status, 0, sizeof(int32_t), c->stream));
@@ -549,6 +617,10 @@ int fast_gpu_assemble(fast_gpu_ctx *c, int32_t what) {
 
 int fast_gpu_add(fast_gpu_ctx *c, int32_t what, int32_t i, int32_t j, double v) {
   if (check_ctx(c)) return FAST_GPU_EINVAL;
+  if (what == FAST_ASM_STIFFNESS && c->K32_current) {
+    c->err = "add: the current stiffness is the tensor-core FP32 one; assemble FAST_ASM_STIFFNESS to edit entries";
+    return FAST_GPU_ESTATE;
+  }
   double *T = target_of(*c, what);
   if (!T) return FAST_GPU_ESTATE;
   const int64_t k1 = value_index(*c, i, j);
@@ -567,6 +639,21 @@ int fast_gpu_add(fast_gpu_ctx *c, int32_t what, int32_t i, int32_t j, double v) 
   }
   CK(cudaStreamSynchronize(c->stream));
   invalidate(*c, what);
+  return FAST_GPU_OK;
+}
+
+int fast_gpu_add_mat(fast_gpu_ctx *c, int32_t dst, double a, int32_t src) {
+  if (check_ctx(c)) return FAST_GPU_EINVAL;
+  if (dst != FAST_ASM_STIFFNESS || src != FAST_ASM_MASS) {
+    c->err = "add_mat: only K += a M (dst FAST_ASM_STIFFNESS, src FAST_ASM_MASS)";
+    return FAST_GPU_EINVAL;
+  }
+  if (!c->d_K || !c->d_M || !c->K_ok || !c->M_ok) { c->err = "add_mat: K and M must be assembled"; return FAST_GPU_ESTATE; }
+  const int64_t n = 9 * c->nnzb;
+  add_mat_kernel<<<4 * c->sm_count, 256, 0, c->stream>>>(n, a, c->d_M, c->d_K);
+  c->launches++;
+  CK(cudaGetLastError());
+  invalidate(*c, FAST_ASM_STIFFNESS);
   return FAST_GPU_OK;
 }
 
@@ -611,7 +698,14 @@ int solve_node_space(fast_gpu_ctx *c, const fast_gpu_solve_opts *o, bool warm, f
   if (precond != FAST_PRECOND_JACOBI && precond != FAST_PRECOND_BLOCK_JACOBI) return FAST_GPU_EINVAL;
   const bool mixed = opts.precision == FAST_PREC_MIXED;
   if (!mixed && opts.precision != FAST_PREC_FP64) return FAST_GPU_EINVAL;
-  if (c->precond_built != precond) CK(launch_build_precond(*c, c->d_K, precond));
+  const bool k32 = c->K32_current;
+  if (k32 && !mixed) {
+    c->err = "solve: the tensor-core stiffness serves the mixed-precision solve; assemble FAST_ASM_STIFFNESS "
+             "for an FP64 solve";
+    return FAST_GPU_ESTATE;
+  }
+  if (c->precond_built != precond)
+    CK(k32 ? launch_build_precond32(*c, c->d_K32, precond) : launch_build_precond(*c, c->d_K, precond));
   CK(ensure_soa(*c, FAST_ASM_STIFFNESS, mixed));
   const int chunk = opts.check_every > 0 ? opts.check_every : (mixed ? 50 : 32);
   fast_gpu_solve_report R{};
@@ -619,7 +713,7 @@ int solve_node_space(fast_gpu_ctx *c, const fast_gpu_solve_opts *o, bool warm, f
     CK(pcg_mixed(*c, warm, tol, maxit, chunk));
     R.outer = c->h_state->updates;
     const int done = c->h_state->done, it = c->h_state->iter;
-    if ((done == 3 || done == 4) && it < maxit) {
+    if ((done == 3 || done == 4) && it < maxit && !k32) {
       // FP32 iterates stopped making progress (ill-conditioned system): go on
       // with the FP64 iteration from the best FP64 iterate seen
       R.escalated = 1;
@@ -639,7 +733,7 @@ int solve_node_space(fast_gpu_ctx *c, const fast_gpu_solve_opts *o, bool warm, f
   {
     double *d_rr = c->d_partials + 12290;
     double *d_ff = c->d_partials + 12291;
-    CK(launch_residual(*c, c->d_Ks, c->d_f, c->d_u, c->d_r, d_rr));
+    CK(launch_residual(*c, k32 ? nullptr : c->d_Ks, c->d_f, c->d_u, c->d_r, d_rr));  // null: element by element
     CK(launch_norm2(*c, c->d_f, 4 * c->nnode, d_ff));
     double h[2] = {0, 0};
     CK(cudaMemcpyAsync(h, d_rr, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -679,7 +773,7 @@ int solve_nodes(Ctx &c, const fast_gpu_solve_opts *o, bool warm, fast_gpu_solve_
 int fast_gpu_solve_device(fast_gpu_ctx *c, const double *d_f, double *d_u, const fast_gpu_solve_opts *o,
                           fast_gpu_solve_report *rep) {
   if (check_ctx(c) || !d_f || !d_u) return FAST_GPU_EINVAL;
-  if (!c->K_ok) { c->err = "solve: matrix not assembled"; return FAST_GPU_ESTATE; }
+  if (!c->K_ok && !c->K32_current) { c->err = "solve: matrix not assembled"; return FAST_GPU_ESTATE; }
   const bool warm = o && o->warm_start;
   const int64_t sp = c->begin_span(FAST_KERNEL_LINEAR_SOLVE);
   CK(launch_eq_to_node(*c, d_f, c->d_f));
@@ -700,7 +794,7 @@ int fast_gpu_solve_device(fast_gpu_ctx *c, const double *d_f, double *d_u, const
 int fast_gpu_solve(fast_gpu_ctx *c, const double *f, double *u, const fast_gpu_solve_opts *o,
                    fast_gpu_solve_report *rep) {
   if (check_ctx(c) || !f || !u) return FAST_GPU_EINVAL;
-  if (!c->K_ok) { c->err = "solve: matrix not assembled"; return FAST_GPU_ESTATE; }
+  if (!c->K_ok && !c->K32_current) { c->err = "solve: matrix not assembled"; return FAST_GPU_ESTATE; }
   const size_t nb = sizeof(double) * c->neq;
   double *d_feq = c->d_eq_tmp, *d_ueq = c->d_eq_tmp + c->neq;
   CK(cudaStreamSynchronize(c->stream));
@@ -718,8 +812,10 @@ int fast_gpu_solve(fast_gpu_ctx *c, const double *f, double *u, const fast_gpu_s
 
 int fast_gpu_get_lower_csr(fast_gpu_ctx *c, int32_t what, int64_t *nnz, int64_t *rowptr, int32_t *col, double *val) {
   if (check_ctx(c) || !nnz) return FAST_GPU_EINVAL;
-  double *T = target_of(*c, what);
-  if (!T) return FAST_GPU_ESTATE;
+  const bool k32 = what == FAST_ASM_STIFFNESS_TF32;
+  if (k32 && !c->K32_current) { c->err = "get_lower_csr: no tensor-core stiffness assembled"; return FAST_GPU_ESTATE; }
+  double *T = k32 ? nullptr : target_of(*c, what);
+  if (!T && !k32) return FAST_GPU_ESTATE;
   // count per equation row
   const int32_t neq = c->neq;
   std::vector<int64_t> cnt(neq + 1, 0);
@@ -735,8 +831,15 @@ int fast_gpu_get_lower_csr(fast_gpu_ctx *c, int32_t what, int64_t *nnz, int64_t 
   *nnz = cnt[neq];
   if (!col || !val || !rowptr) return FAST_GPU_OK;
   std::vector<double> hv((size_t)9 * c->nnzb);
-  CK(cudaMemcpyAsync(hv.data(), T, sizeof(double) * hv.size(), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+  if (k32) {
+    std::vector<float> hf(hv.size());
+    CK(cudaMemcpyAsync(hf.data(), c->d_K32, sizeof(float) * hf.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (size_t k = 0; k < hv.size(); k++) hv[k] = (double)hf[k];
+  } else {
+    CK(cudaMemcpyAsync(hv.data(), T, sizeof(double) * hv.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
   std::memcpy(rowptr, cnt.data(), sizeof(int64_t) * (neq + 1));
   std::vector<std::pair<int32_t, double>> row;
   for (int32_t i = 0; i < neq; i++) {
@@ -759,7 +862,14 @@ int fast_gpu_element_matrices(fast_gpu_ctx *c, int32_t what, int32_t b, int64_t 
   const Bucket &B = c->buckets[b];
   if (first < 0 || count <= 0 || first + count > B.ne) return FAST_GPU_EINVAL;
   if (what == FAST_ASM_MASS && !B.has_rho) { c->err = "element_matrices: bucket has no density"; return FAST_GPU_ESTATE; }
-  if (what != FAST_ASM_STIFFNESS && what != FAST_ASM_MASS && what != FAST_ASM_INTERNAL_FORCE) return FAST_GPU_EINVAL;
+  if (what != FAST_ASM_STIFFNESS && what != FAST_ASM_MASS && what != FAST_ASM_INTERNAL_FORCE &&
+      what != FAST_ASM_STIFFNESS_TF32)
+    return FAST_GPU_EINVAL;
+  if (what == FAST_ASM_STIFFNESS_TF32 && !tc_supported(B)) {
+    c->err = "element_matrices: the tensor-core stiffness takes small-strain hex8 / hex20 and B-spline (2,2,2), "
+             "(3,3,3), (3,3,2) buckets only";
+    return FAST_GPU_ENOTSUP;
+  }
   if (B.type == FAST_ELEM_BSP_SOLID && (what == FAST_ASM_MASS || (what == FAST_ASM_INTERNAL_FORCE &&
                                                                  !bsp_tl_supported(B.pd, B.ngp[0])))) {
     c->err = "element_matrices: B-spline solids provide the stiffness matrix (and, for the tangent kernels' "
@@ -777,6 +887,7 @@ int fast_gpu_element_matrices(fast_gpu_ctx *c, int32_t what, int32_t b, int64_t 
   if (e == cudaSuccess) e = cudaMemsetAsync(c->d_status, 0, sizeof(int32_t), c->stream);
   if (e == cudaSuccess) {
     if (what == FAST_ASM_INTERNAL_FORCE) e = launch_tl_element(*c, 1, b, count, buf);
+    else if (what == FAST_ASM_STIFFNESS_TF32) e = launch_element_matrices_tc(*c, b, count, buf);
     else if (what == FAST_ASM_STIFFNESS && B.tl) e = launch_tl_element(*c, 0, b, count, buf);
     else e = launch_element_matrices(*c, what, b, 0, count, buf);
   }
@@ -855,6 +966,14 @@ int fast_gpu_kernel_stats(fast_gpu_ctx *c, int32_t which, int64_t *launches, dou
         algo += (double)B.ne * (nn * (4 + 24 + 1) + 16 + nn * nn * (4 + 2 * 72));
       }
       algo += 72.0 * c->nnzb;
+    }
+    if (which == FAST_KERNEL_ASSEMBLE_TF32) {
+      // the same model with FP32 blocks (36 bytes)
+      for (const Bucket &B : c->buckets) {
+        const double nn = B.nn;
+        algo += (double)B.ne * (nn * (4 + 24 + 1) + 16 + nn * nn * (4 + 2 * 36));
+      }
+      algo += 36.0 * c->nnzb;
     }
     *bytes = algo;
   }

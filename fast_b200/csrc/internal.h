@@ -38,6 +38,8 @@ struct PcgState {
   int32_t stall;    // FP64 residual replacements without a 2x improvement
   int32_t final;    // converged on the FP64 residual: later launches do nothing
   int32_t best;     // the last FP64 residual was the smallest so far (mixed path)
+  uint32_t arrive_update;   // blocks finished in the fused update kernel (the last one commits)
+  uint32_t arrive_dir;      // blocks finished in the fused direction kernel
 };
 
 struct Bucket {
@@ -89,11 +91,14 @@ struct TiedSet {
   std::vector<int32_t> h_pa;              //   local node of the element
   std::vector<double> h_pt;               //   weight (1 for a non-slave node)
   std::vector<int64_t> h_keoff;           // [n] element matrix offset in the scratch buffer
+  std::vector<int64_t> h_eptr;            // [n+1] offsets into h_econn
+  std::vector<int32_t> h_econn;           //   each tied element's own nodes, local order
   std::vector<int32_t> h_nn;              // [n] nodes per element
   int64_t ke_total = 0;
   std::vector<std::vector<int32_t>> bucket_pos;  // per bucket: colour-sorted positions, scratch order
   std::vector<int64_t> bucket_keoff;             // per bucket: first scratch offset
-  int64_t *d_nptr = nullptr, *d_sptr = nullptr, *d_pptr = nullptr, *d_keoff = nullptr;
+  int64_t *d_nptr = nullptr, *d_sptr = nullptr, *d_pptr = nullptr, *d_keoff = nullptr, *d_eptr = nullptr;
+  int32_t *d_econn = nullptr;
   int32_t *d_nodes = nullptr, *d_slot = nullptr, *d_pa = nullptr, *d_nn = nullptr;
   double *d_pt = nullptr, *d_ke = nullptr;
   std::vector<int32_t *> d_bucket_pos;
@@ -117,6 +122,7 @@ struct Ctx {
   int device = 0;
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
+  cudaStream_t side_stream = nullptr;  // captures the bodies of conditional graph nodes
   std::string err;
   int sm_count = 148;
 
@@ -158,6 +164,11 @@ struct Ctx {
 
   // assembled matrices: [nnzb][3][3] blocks (assembly target, AoS)
   double *d_K = nullptr, *d_M = nullptr;
+  // FP32 stiffness from the tensor cores (FAST_ASM_STIFFNESS_TF32), same layout;
+  // while K32_current is set it is the stiffness of the context: the FP64 slot
+  // is stale and the mixed solve takes its FP64 residuals element by element
+  float *d_K32 = nullptr;
+  bool K32_current = false;
   // solve copies in row-local SoA layout (FP64 and FP32), rebuilt after each assembly
   double *d_Ks = nullptr, *d_Ms = nullptr;
   float *d_Ks32 = nullptr;
@@ -200,6 +211,13 @@ struct Ctx {
   // blocks per lane trip; defaults measured best on a hex20 box (64 blocks per
   // padded row), fast_gpu_autotune measures them on the system at hand
   int lpr32 = 8, lpr64 = 16;
+  // Newmark steps and Newton iterations replayed as captured CUDA graphs
+  bool graph_steps = true;
+  // FP32 SpMV with the matrix streamed through shared memory by bulk copies
+  // (spmv_f32_bulk): its row tiles, their largest value / column bytes and grid
+  bool spmv32_bulk = false;
+  int32_t *d_tile_row = nullptr;
+  int bulk_ntiles = 0, bulk_vbytes = 0, bulk_cbytes = 0, bulk_grid = 0;
   int persist_grid = 0;           // blocks of that kernel (0: not yet sized)
   void *d_bar = nullptr;          // grid barrier words (kBarrierBytes)
   static constexpr size_t kBarrierBytes = 8192;
@@ -217,7 +235,7 @@ struct Ctx {
   // live kernel timing: CUDA events around SpMV launches, assemblies, the
   // learned predictor, internal forces and linear solves (the FAST_KERNEL_*
   // kinds), harvested at each host sync; spans may nest
-  static constexpr int kSpanKinds = 7;
+  static constexpr int kSpanKinds = 8;
   bool timing = false;
   std::vector<cudaEvent_t> ev_pool;
   struct Span { int kind; int64_t id; bool closed; cudaEvent_t a, b; };
@@ -266,6 +284,13 @@ cudaError_t upload_ties(Ctx &c);
 void free_ties(Ctx &c);
 cudaError_t launch_tied_element_matrices(Ctx &c);   // dense K_e of every tied element into the scratch buffer
 cudaError_t launch_tied_assemble(Ctx &c, double *K);
+// the tied elements into the FP32 tensor-core stiffness: their FP64 element
+// matrices (the scratch buffer) scattered as T_e^T K_e T_e in FP32
+cudaError_t launch_tied_assemble32(Ctx &c, float *K32);
+// G += K_e u_e of every tied element (node space, u with its slave values,
+// from the scratch buffer of the last assembly); DOFs without an equation take
+// nothing; nothing is done while *skip is non-zero
+cudaError_t launch_tied_matvec(Ctx &c, const double *u, double *G, const int32_t *skip);
 cudaError_t launch_tie_restrict(Ctx &c, double *f);  // f <- T^T f (padded node layout)
 cudaError_t launch_tie_zero(Ctx &c, double *v);      // v[slave DOFs] = 0
 cudaError_t launch_tie_prolong(Ctx &c, double *u);   // u[slave] = sum w u[master]
@@ -278,15 +303,43 @@ cudaError_t launch_geom_stiffness(Ctx &c, double *G, double sign);
 
 // tl_kernels.cu
 cudaError_t launch_tl(Ctx &c, double *K, double *G, bool want_k, bool want_g);
+// the same at the nodal displacements U ([nnode][4]); every launch does
+// nothing while *skip (a device flag, may be null) is non-zero
+cudaError_t launch_tl_at(Ctx &c, double *K, double *G, bool want_k, bool want_g, const double *U, const int32_t *skip);
+
+// elem_tc.cu: stiffness on the tensor cores (3xTF32, FP32 blocks), small-strain hex buckets
+bool tc_supported(const Bucket &B);
+cudaError_t launch_assemble_tc(Ctx &c, float *K32);
+cudaError_t launch_element_matrices_tc(Ctx &c, int bucket, int64_t count, double *d_out_and_index);
 cudaError_t launch_tl_element(Ctx &c, int what, int bucket, int64_t count, double *d_out_and_index);
 
 constexpr int kRedBlocks = 592;   // fixed reduction grid: 4 x 148 SMs
 cudaError_t launch_build_precond(Ctx &c, const double *K, int precond);
+// the same from the FP32 blocks of the tensor-core stiffness
+cudaError_t launch_build_precond32(Ctx &c, const float *K32, int precond);
+// row tiles of the bulk-staged FP32 SpMV (once per pattern)
+cudaError_t ensure_bulk_tiles(Ctx &c);
+// FP32 blocks -> the FP32 row-local SoA copy
+cudaError_t launch_to_soa32(Ctx &c, const float *K32, float *Ks32);
+// r = f - K u in FP64 without the assembled matrix: the small-strain internal
+// force of every element at u (K u for a linear elastic solid), tie
+// restriction / prolongation included; r.r per block into part[spmv grid];
+// nothing is done while *skip is non-zero
+cudaError_t launch_matfree_residual(Ctx &c, const double *f, const double *u, double *r, double *part,
+                                    const int32_t *skip);
 // AoS blocks -> row-local SoA copies (either output may be null)
 cudaError_t launch_to_soa(Ctx &c, const double *K, double *Ks, float *Ks32);
 // PCG on the padded node vectors c.d_f -> c.d_u; state left in c.h_state
 cudaError_t pcg_fp64(Ctx &c, bool warm, double tol, int maxit, int chunk, int iter0 = 0);
 cudaError_t pcg_mixed(Ctx &c, bool warm, double tol, int maxit, int chunk);
+// Records a whole solve of c.d_f -> c.d_u (kernel-per-step form: the
+// preconditioner and solve copies must be current) into the graph being
+// captured on c.stream: the initialisation, then a WHILE conditional node
+// whose body is `chunk` iterations (plus the FP64 residual replacement of the
+// mixed path) and a kernel that keeps the loop going while the state is
+// running.  The tolerance is read from tol_dev when that is not null.  The
+// loop ends at the state's maxit at the latest (the kernels stop there).
+cudaError_t record_pcg(Ctx &c, bool mixed, bool warm, double tol, const double *tol_dev, int maxit, int chunk);
 constexpr int kDoneBarrierTimeout = 6;  // PcgState::done: a grid-barrier wait ran out
 // one CTA per independent problem (node ranges d_noff), FP64 Jacobi/block PCG on c.d_Ks
 // from c.d_f into c.d_u; per problem: iterations, |r|/|f| and done (1 conv, 2 cap, 3 breakdown)

@@ -14,6 +14,7 @@
 // state vectors resident in HBM and the step's vector work in two fused
 // kernels.  The printout's max norms (umax, vmax, amax) are kept on the
 // device.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -100,6 +101,23 @@ __global__ void nm_probe(int nprobe, const int32_t *__restrict__ probe, const in
   if (k < nprobe) out[k] = u[dof[probe[k]]];
 }
 
+// graph replays: the step number lives on the device.  stats: [0] steps done,
+// [1] PCG iterations, [2] largest step count, [3] first failed step (0: none)
+__global__ void nm_step_end(const PcgState *__restrict__ st, int32_t *__restrict__ stats) {
+  const int32_t it = st->iter;
+  stats[1] += it;
+  if (it > stats[2]) stats[2] = it;
+  if (st->done != 1 && stats[3] == 0) stats[3] = stats[0] + 1;
+  stats[0] += 1;
+}
+
+__global__ void nm_probe_step(int nprobe, const int32_t *__restrict__ probe, const int32_t *__restrict__ dof,
+                              const double *__restrict__ u, double *__restrict__ hist, const int32_t *__restrict__ stats) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  // written after nm_step_end: the step just done is stats[0] - 1
+  if (k < nprobe) hist[(size_t)(stats[0] - 1) * nprobe + k] = u[dof[probe[k]]];
+}
+
 }  // namespace
 
 #define NMCK(call)                                                            \
@@ -111,6 +129,67 @@ __global__ void nm_probe(int nprobe, const int32_t *__restrict__ probe, const in
       goto done;                                                              \
     }                                                                         \
   } while (0)
+
+// Steps first .. steps-1 as replays of one captured step graph (the first
+// step has run directly: the preconditioner and solve copies of K_eff exist).
+static int graph_steps(fast_gpu_ctx *c, const fast_gpu_newmark_opts *o, int first, int64_t n4, double a0, double a2,
+                       double a3, double a6, double a7, const double *d_q, double *d_u, double *d_v, double *d_a,
+                       double *d_w, double *d_z, unsigned long long *d_max, int32_t nprobe, const int32_t *d_probe,
+                       double *d_hist, const fast_gpu_solve_report &last, fast_gpu_newmark_report &R) {
+  int rc = FAST_GPU_OK;
+  int32_t *d_stats = nullptr;
+  int32_t h_stats[4] = {first, R.linear_iterations, R.max_step_iterations, 0};
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ge = nullptr;
+  const fast_gpu_solve_opts &lo = o->lin;
+  const bool mixed = lo.precision == FAST_PREC_MIXED;
+  const int maxit = lo.maxit > 0 ? lo.maxit : std::max(20 * c->neq, 100);
+  const double tol = lo.tol > 0 ? lo.tol : 1e-5;
+  const int chunk = lo.check_every > 0 ? lo.check_every : 16;
+  const int64_t before = c->launches;
+  int64_t per_step = 0;
+  (void)last;
+  NMCK(cudaMalloc((void **)&d_stats, sizeof(h_stats)));
+  NMCK(cudaMemcpyAsync(d_stats, h_stats, sizeof(h_stats), cudaMemcpyHostToDevice, c->stream));
+  NMCK(cudaStreamSynchronize(c->stream));
+  NMCK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  {
+    nm_inertia<<<kNmBlocks, 256, 0, c->stream>>>(n4, a0, a2, a3, d_u, d_v, d_a, d_w);
+    launch_spmv(*c, c->d_Ms, d_w, d_z);  // z = M w
+    nm_rhs<<<kNmBlocks, 256, 0, c->stream>>>(n4, d_q, d_z, d_u, c->d_f, c->d_u);
+    cudaError_t e = record_pcg(*c, mixed, lo.warm_start != 0, tol, nullptr, maxit, chunk);
+    nm_step_end<<<1, 1, 0, c->stream>>>(c->d_state, d_stats);
+    nm_update<<<kNmBlocks, 256, 0, c->stream>>>(n4, a0, a2, a3, a6, a7, c->d_u, d_u, d_v, d_a, d_max);
+    if (nprobe > 0)
+      nm_probe_step<<<(nprobe + 127) / 128, 128, 0, c->stream>>>(nprobe, d_probe, c->d_dof_of_eq, d_u, d_hist, d_stats);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
+    NMCK(e);
+    NMCK(ec);
+  }
+  per_step = c->launches - before + 4 + (nprobe > 0 ? 1 : 0);
+  c->launches = before;
+  NMCK(cudaGraphInstantiate(&ge, g, 0));
+  for (int s = first; s < o->steps; s++) {
+    NMCK(cudaGraphLaunch(ge, c->stream));
+    c->launches += per_step;   // the kernels of the chunks the loop ran are not counted
+  }
+  NMCK(cudaMemcpyAsync(h_stats, d_stats, sizeof(h_stats), cudaMemcpyDeviceToHost, c->stream));
+  NMCK(cudaStreamSynchronize(c->stream));
+  R.linear_iterations = h_stats[1];
+  R.max_step_iterations = h_stats[2];
+  R.steps_done = h_stats[3] ? h_stats[3] - 1 : h_stats[0];
+  if (h_stats[3]) {
+    R.failed_step = h_stats[3];
+    c->err = "newmark: a step's PCG did not converge";
+    rc = FAST_GPU_ENONCONV;
+  }
+done:
+  if (ge) cudaGraphExecDestroy(ge);
+  if (g) cudaGraphDestroy(g);
+  if (d_stats) cudaFree(d_stats);
+  return rc;
+}
 
 extern "C" int fast_gpu_newmark(fast_gpu_ctx *c, const double *q, const fast_gpu_newmark_opts *o, double *u_out,
                                 double *v_out, double *a_out, int32_t nprobe, const int32_t *probe_eq,
@@ -176,6 +255,14 @@ extern "C" int fast_gpu_newmark(fast_gpu_ctx *c, const double *q, const fast_gpu
   NMCK(solve_layout(*c, FAST_ASM_MASS, false));
 
   for (int s = 0; s < o->steps; s++) {
+    if (s == 1 && c->graph_steps) {
+      // every later step replays one captured graph: right-hand side, the
+      // whole PCG (a WHILE node over chunks of iterations), update, probes
+      rc = graph_steps(c, o, s, n4, a0, a2, a3, a6, a7, d_q, d_u, d_v, d_a, d_w, d_z, d_max, nprobe, d_probe, d_hist,
+                       lr, R);
+      if (rc != FAST_GPU_OK) goto done;
+      break;
+    }
     nm_inertia<<<kNmBlocks, 256, 0, c->stream>>>(n4, a0, a2, a3, d_u, d_v, d_a, d_w);
     c->launches++;
     NMCK(launch_spmv(*c, c->d_Ms, d_w, d_z));  // z = M w

@@ -10,11 +10,16 @@
 //                         (cControl::Convergence, ctrl/ctrl.cpp:1366-1413)
 //
 // Everything stays on the device; the host reads two norms per iteration.
+// After the first iteration of a solve, every iteration is replayed as one
+// captured CUDA graph (tangent assembly, preconditioner, the whole PCG as a
+// conditional WHILE node, update, internal force, residual norms): one host
+// wait per Newton iteration.
 // The reference starts each step from the last converged u; a secant
 // predictor (u_k + (u_k - u_{k-1}) for equal steps) and a caller-supplied
 // predictor (e.g. a learned one) can start it elsewhere.  A predicted start is
 // only taken if its residual is smaller than the residual of the secant
 // start; Newton always iterates to the same tolerance.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -76,12 +81,116 @@ __global__ void __launch_bounds__(256) nr_finish2(const double *__restrict__ par
   }
 }
 
+// graph-replayed iteration: the linear tolerance (inexact Newton, the same
+// formula as the host path) and the right-hand side scaling from the device
+// norms; par[0] tolerance, par[1] 1/|r|, par[2] |r| (1 when r = 0)
+__global__ void nr_lin_params(const double *__restrict__ sums, double tol, double rel, double tmin, double tmax,
+                              double fixed_tol, double *__restrict__ par) {
+  const double rlen = sqrt(sums[0]), flen = sqrt(sums[1]);
+  double lt = fixed_tol;
+  if (rel > 0) {
+    const double err = rlen / fmax(1.0, flen);
+    const double eta = fmax(rel * err, err > 0 ? 0.5 * tol / err : 1.0);
+    lt = fmin(tmax, fmax(tmin, eta));
+  }
+  par[0] = lt;
+  par[1] = rlen > 0 ? 1.0 / rlen : 1.0;
+  par[2] = rlen > 0 ? rlen : 1.0;
+}
+
+// z = par[k] x (+ y when y is given)
+__global__ void nr_scaled(int32_t n, const double *__restrict__ par, int k, const double *__restrict__ x,
+                          const double *__restrict__ y, double *__restrict__ z) {
+  const double a = par[k];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    z[i] = y ? 1.0 * y[i] + a * x[i] : a * x[i] + 0.0 * x[i];
+}
+
+// what the host reads after a replayed iteration
+struct NrIterOut {
+  double rlen2, flen2;
+  int32_t lin_iters, lin_done, status, pad;
+};
+
+__global__ void nr_collect(const double *__restrict__ sums, const PcgState *__restrict__ st,
+                           const int32_t *__restrict__ status, NrIterOut *__restrict__ out) {
+  out->rlen2 = sums[0];
+  out->flen2 = sums[1];
+  out->lin_iters = st->iter;
+  out->lin_done = st->done;
+  out->status = *status;
+}
+
 }  // namespace
 
 struct NrWork {
   double *q = nullptr, *f = nullptr, *g = nullptr, *r = nullptr, *u = nullptr, *du = nullptr, *up = nullptr,
          *ucand = nullptr, *part = nullptr, *sums = nullptr, *hsums = nullptr;
+  double *par = nullptr;                 // [3] linear tolerance, 1/|r|, |r|
+  NrIterOut *d_out = nullptr, *h_out = nullptr;
+  cudaGraphExec_t graph = nullptr;       // one Newton iteration, captured
 };
+
+// Records one Newton iteration (after the residual norms of the current u are
+// in w.sums) as a graph: tangent at u (zero, every colour, TL buckets), its
+// solve copies and preconditioner, the linear tolerance and the scaled
+// right-hand side on the device, the whole PCG (conditional WHILE node),
+// u += |r| du, the internal force at the new u, r = f - g, its norms, and a
+// copy of what the host needs into pinned memory.
+static cudaError_t capture_iteration(Ctx &c, NrWork &w, const fast_gpu_nr_opts *o, bool mixed, int64_t *kernels) {
+  const fast_gpu_solve_opts &lo = o->lin;
+  const int32_t n = c.neq;
+  const int maxit = lo.maxit > 0 ? lo.maxit : std::max(20 * c.neq, 100);
+  const int chunk = lo.check_every > 0 ? lo.check_every : 16;
+  const double tol = o->tol > 0 ? o->tol : 1e-5;
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return e;
+  const int64_t before = c.launches;
+  cudaError_t el = cudaMemsetAsync(c.d_status, 0, sizeof(int32_t), c.stream);
+  // tangent at u (c.d_disp already holds u)
+  if (el == cudaSuccess) el = launch_zero_matrix(c, c.d_K, true);
+  if (el == cudaSuccess) el = launch_assemble(c, FAST_ASM_STIFFNESS, c.d_K);
+  if (el == cudaSuccess) el = launch_tl(c, c.d_K, nullptr, true, false);
+  if (el == cudaSuccess) el = launch_to_soa(c, c.d_K, c.d_Ks, mixed ? c.d_Ks32 : nullptr);
+  if (el == cudaSuccess) el = launch_build_precond(c, c.d_K, lo.precond);
+  // K du = r / |r| with the inexact-Newton tolerance
+  if (el == cudaSuccess) {
+    nr_lin_params<<<1, 1, 0, c.stream>>>(w.sums, tol, o->lin_tol_rel, o->lin_tol_min > 0 ? o->lin_tol_min : 1e-12,
+                                         o->lin_tol_max > 0 ? o->lin_tol_max : 1e-2, lo.tol > 0 ? lo.tol : 1e-5,
+                                         w.par);
+    nr_scaled<<<kNrBlocks, 256, 0, c.stream>>>(n, w.par, 1, w.r, nullptr, w.ucand);
+    c.launches += 2;
+    el = launch_eq_to_node(c, w.ucand, c.d_f);
+  }
+  if (el == cudaSuccess) el = record_pcg(c, mixed, false, 1e-5, w.par, maxit, chunk);
+  if (el == cudaSuccess) el = launch_node_to_eq(c, c.d_u, w.du);
+  if (el == cudaSuccess) {
+    nr_scaled<<<kNrBlocks, 256, 0, c.stream>>>(n, w.par, 2, w.du, w.u, w.u);  // u += |r| du
+    c.launches++;
+    el = launch_eq_to_node(c, w.u, c.d_disp);
+  }
+  // internal force at the new u, residual and norms
+  if (el == cudaSuccess) el = cudaMemsetAsync(c.d_gint, 0, sizeof(double) * 4 * c.nnode, c.stream);
+  if (el == cudaSuccess) el = launch_tl(c, nullptr, c.d_gint, false, true);
+  if (el == cudaSuccess) el = launch_node_to_eq(c, c.d_gint, w.g);
+  if (el == cudaSuccess) {
+    nr_axpby<<<kNrBlocks, 256, 0, c.stream>>>(n, 1.0, w.f, -1.0, w.g, w.r);
+    nr_sumsq2<<<kNrBlocks, 256, 0, c.stream>>>(n, w.r, w.f, w.part);
+    nr_finish2<<<1, 256, 0, c.stream>>>(w.part, w.sums);
+    nr_collect<<<1, 1, 0, c.stream>>>(w.sums, c.d_state, c.d_status, w.d_out);
+    c.launches += 4;
+    el = cudaMemcpyAsync(w.h_out, w.d_out, sizeof(NrIterOut), cudaMemcpyDeviceToHost, c.stream);
+  }
+  if (el == cudaSuccess) el = cudaGetLastError();
+  e = cudaStreamEndCapture(c.stream, &g);
+  *kernels = c.launches - before;   // kernels of one replay outside the PCG loop's chunks
+  c.launches = before;
+  if (el != cudaSuccess) e = el;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&w.graph, g, 0);
+  if (g) cudaGraphDestroy(g);
+  return e;
+}
 
 static cudaError_t axpby(Ctx &c, double a, const double *x, double b, const double *y, double *z) {
   nr_axpby<<<kNrBlocks, 256, 0, c.stream>>>(c.neq, a, x, b, y, z);
@@ -134,6 +243,7 @@ extern "C" int fast_gpu_nr_solve(fast_gpu_ctx *c, const double *q_host, const fa
   int rc = FAST_GPU_OK;
   fast_gpu_nr_report R{};
   double lam = 0.0, flen2 = 0.0, rlen2 = 0.0, glen2 = 0.0, best = 0.0;
+  int64_t graph_kernels = 0;
   std::vector<double> hq;
   const double tol = o->tol > 0 ? o->tol : 1e-5;
   if (n <= 0) return FAST_GPU_EINVAL;
@@ -145,6 +255,9 @@ extern "C" int fast_gpu_nr_solve(fast_gpu_ctx *c, const double *q_host, const fa
     if (e == cudaSuccess) e = cudaMalloc((void **)&w.part, sizeof(double) * 2 * kNrBlocks);
     if (e == cudaSuccess) e = cudaMalloc((void **)&w.sums, sizeof(double) * 2);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&w.hsums, sizeof(double) * 2);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&w.par, sizeof(double) * 3);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&w.d_out, sizeof(NrIterOut));
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&w.h_out, sizeof(NrIterOut));
     NRCK(e);
   }
   hq.assign(q_host, q_host + n);
@@ -214,6 +327,25 @@ extern "C" int fast_gpu_nr_solve(fast_gpu_ctx *c, const double *q_host, const fa
       }
     }
     for (it = 1; !conv && it <= o->max_iter; it++) {
+      if (w.graph) {
+        // the iteration replayed as one graph: one host wait per iteration
+        NRCK(cudaGraphLaunch(w.graph, c->stream));
+        c->launches += graph_kernels;
+        NRCK(cudaStreamSynchronize(c->stream));
+        const NrIterOut &io = *w.h_out;
+        c->K_ok = true;
+        c->K32_current = false;
+        c->Ks_ok = true;
+        c->precond_built = o->lin.precond;
+        if (io.status & 1) {
+          c->err = "assemble: non-positive Jacobian determinant in at least one element";
+          rc = FAST_GPU_EDETJ;
+          goto done;
+        }
+        R.linear_iterations += io.lin_iters;
+        rlen2 = io.rlen2;
+        flen2 = io.flen2;
+      } else {
       NRRC(fast_gpu_assemble(c, FAST_ASM_STIFFNESS));  // tangent at u
       fast_gpu_solve_opts lo = o->lin;
       if (o->lin_tol_rel > 0) {
@@ -245,6 +377,11 @@ extern "C" int fast_gpu_nr_solve(fast_gpu_ctx *c, const double *q_host, const fa
       NRRC(fast_gpu_internal_force_device(c, w.g));
       NRCK(axpby(*c, 1.0, w.f, -1.0, w.g, w.r));  // r = f - g
       NRCK(norms2(*c, w, w.r, w.f, &rlen2, &flen2));
+      // every later iteration replays this one as a captured graph (the
+      // solve copies and work buffers exist now)
+      if (c->graph_steps && !c->timing && !w.graph)
+        NRCK(capture_iteration(*c, w, o, o->lin.precision == FAST_PREC_MIXED, &graph_kernels));
+      }
       R.iterations++;
       const double flen = std::sqrt(flen2), rlen = std::sqrt(rlen2);
       double err;
@@ -274,7 +411,11 @@ extern "C" int fast_gpu_nr_solve(fast_gpu_ctx *c, const double *q_host, const fa
   }
 done:
   if (rep) *rep = R;
+  if (w.graph) cudaGraphExecDestroy(w.graph);
   if (w.hsums) cudaFreeHost(w.hsums);
+  if (w.h_out) cudaFreeHost(w.h_out);
+  if (w.par) cudaFree(w.par);
+  if (w.d_out) cudaFree(w.d_out);
   for (double *p : {w.q, w.f, w.g, w.r, w.u, w.du, w.up, w.ucand, w.part, w.sums})
     if (p) cudaFree(p);
   return rc;

@@ -31,8 +31,10 @@
 // fixed grid and a fixed combination order, so the host never waits inside
 // an iteration and a solve is bit-reproducible.  Kernels check state->done
 // first, so iterations launched past convergence cost only their launch.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <vector>
 
 #include <cooperative_groups.h>
 
@@ -92,10 +94,12 @@ template <> struct V4<double> {
   }
 };
 
-// AoS blocks -> padded row-local SoA, FP64 and FP32 copies
+// AoS blocks (FP64, or the FP32 tensor-core stiffness) -> padded row-local
+// SoA, FP64 and FP32 copies
+template <typename KT>
 __global__ void __launch_bounds__(256)
 aos_to_soa(int64_t nrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ srow,
-           const double *__restrict__ K, double *__restrict__ Ks, float *__restrict__ Ks32) {
+           const KT *__restrict__ K, double *__restrict__ Ks, float *__restrict__ Ks32) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -104,10 +108,10 @@ aos_to_soa(int64_t nrows, const int32_t *__restrict__ rowptr, const int32_t *__r
     const int32_t s0 = srow[row], nbp = srow[row + 1] - s0;
     const int64_t dst = 9 * (int64_t)s0;
     for (int p = lane; p < nb; p += 32) {
-      const double *src = K + 9 * ((int64_t)b0 + p);
+      const KT *src = K + 9 * ((int64_t)b0 + p);
 #pragma unroll
       for (int k = 0; k < 9; k++) {
-        const double v = src[k];
+        const double v = (double)src[k];
         if (Ks) Ks[dst + (int64_t)k * nbp + p] = v;
         if (Ks32) Ks32[dst + (int64_t)k * nbp + p] = (float)v;
       }
@@ -190,6 +194,139 @@ spmv_f32(int64_t nrows, const int32_t *__restrict__ srow, const int32_t *__restr
   }
 }
 
+// FP32 SpMV with the matrix streamed through shared memory.  In the
+// row-local SoA layout the values of consecutive block-rows are one
+// contiguous range (and so are their column indices), so a tile of rows
+// arrives with two cp.async.bulk copies (completion on an mbarrier, this
+// GPU's memory only): the tile after the current one is requested before
+// the current one is computed (two stages), and the bytes in flight are not
+// bounded by registers.  Lanes then read values and columns from shared
+// memory and gather x (L2-resident) from global memory; LPR lanes per row,
+// 4 blocks per lane per trip, the same sums as spmv_f32.  Tiles and the grid
+// are fixed per pattern, so the p.w partials (one per CTA) are too.  A wait
+// that runs out (bounded) sets *status and the CTA stops.
+constexpr int kBulkThreads = 256;
+constexpr uint64_t kBulkWaitNs = 1000000000ull;
+
+template <int LPR>
+__global__ void __launch_bounds__(kBulkThreads, 2)
+spmv_f32_bulk(int ntiles, const int32_t *__restrict__ tile_row, const int32_t *__restrict__ srow,
+              const int32_t *__restrict__ scol, const float *__restrict__ val, const float *__restrict__ x,
+              float *__restrict__ y, double *__restrict__ part, const int32_t *__restrict__ skip,
+              int32_t *__restrict__ status, int vbytes, int cbytes) {
+  if (skip && *skip) return;
+  extern __shared__ __align__(128) uint8_t bsm[];
+  __shared__ double sbuf[32];
+  __shared__ __align__(8) uint64_t bars[2];
+  __shared__ int fail_sh;
+  constexpr int RPW = 32 / LPR;
+  constexpr int NWARP = kBulkThreads / 32;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, q = lane % LPR;
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((unsigned)__cvta_generic_to_shared(&bars[0])) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((unsigned)__cvta_generic_to_shared(&bars[1])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    fail_sh = 0;
+  }
+  __syncthreads();
+  auto issue = [&](int t, int st) {
+    const int32_t b0 = srow[tile_row[t]], b1 = srow[tile_row[t + 1]];
+    const uint32_t nv = 36u * (uint32_t)(b1 - b0), nc = 4u * (uint32_t)(b1 - b0);
+    const unsigned bar = (unsigned)__cvta_generic_to_shared(&bars[st]);
+    uint8_t *dv = bsm + st * (vbytes + cbytes), *dc = dv + vbytes;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(nv + nc) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     (unsigned)__cvta_generic_to_shared(dv)),
+                 "l"(val + 9 * (int64_t)b0), "r"(nv), "r"(bar)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     (unsigned)__cvta_generic_to_shared(dc)),
+                 "l"(scol + b0), "r"(nc), "r"(bar)
+                 : "memory");
+  };
+  auto wait = [&](int st, uint32_t parity) -> bool {
+    const unsigned bar = (unsigned)__cvta_generic_to_shared(&bars[st]);
+    uint32_t ok = 0;
+    uint64_t t0 = 0;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    while (true) {
+      asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                   "selp.b32 %0, 1, 0, p;\n\t}"
+                   : "=r"(ok)
+                   : "r"(bar), "r"(parity)
+                   : "memory");
+      if (ok) return true;
+      uint64_t t1;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
+      if (t1 - t0 > kBulkWaitNs) return false;
+    }
+  };
+  const float4 *__restrict__ x4 = reinterpret_cast<const float4 *>(x);
+  double pacc = 0.0;
+  bool next_issued = false;
+  if (tid == 0 && (int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+  int k = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, k++) {
+    const int st = k & 1;
+    const int tn = t + gridDim.x;
+    next_issued = tn < ntiles;
+    if (tid == 0 && next_issued) issue(tn, st ^ 1);
+    if (!wait(st, (uint32_t)((k >> 1) & 1))) atomicExch(&fail_sh, 1);
+    __syncthreads();
+    if (fail_sh) break;
+    const float *sv = reinterpret_cast<const float *>(bsm + st * (vbytes + cbytes));
+    const int32_t *sc = reinterpret_cast<const int32_t *>(bsm + st * (vbytes + cbytes) + vbytes);
+    const int32_t r0 = tile_row[t], r1 = tile_row[t + 1];
+    const int32_t base = srow[r0];
+    for (int32_t rr = r0 + warp * RPW; rr < r1; rr += NWARP * RPW) {
+      const int32_t row = rr + lane / LPR;
+      const bool live = row < r1;
+      int32_t s0 = 0, nbp = 0;
+      if (live) {
+        s0 = srow[row] - base;
+        nbp = srow[row + 1] - srow[row];
+      }
+      const float *vr = sv + 9 * s0;
+      float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+      for (int j = 4 * q; j < nbp; j += 4 * LPR) {
+        const int4 c = *reinterpret_cast<const int4 *>(sc + s0 + j);
+        const float4 xa = x4[c.x], xb = x4[c.y], xc = x4[c.z], xd = x4[c.w];
+        float4 v[9];
+#pragma unroll
+        for (int kk = 0; kk < 9; kk++) v[kk] = *reinterpret_cast<const float4 *>(vr + kk * nbp + j);
+        a0 += v[0].x * xa.x + v[1].x * xa.y + v[2].x * xa.z + v[0].y * xb.x + v[1].y * xb.y + v[2].y * xb.z +
+              v[0].z * xc.x + v[1].z * xc.y + v[2].z * xc.z + v[0].w * xd.x + v[1].w * xd.y + v[2].w * xd.z;
+        a1 += v[3].x * xa.x + v[4].x * xa.y + v[5].x * xa.z + v[3].y * xb.x + v[4].y * xb.y + v[5].y * xb.z +
+              v[3].z * xc.x + v[4].z * xc.y + v[5].z * xc.z + v[3].w * xd.x + v[4].w * xd.y + v[5].w * xd.z;
+        a2 += v[6].x * xa.x + v[7].x * xa.y + v[8].x * xa.z + v[6].y * xb.x + v[7].y * xb.y + v[8].y * xb.z +
+              v[6].z * xc.x + v[7].z * xc.y + v[8].z * xc.z + v[6].w * xd.x + v[7].w * xd.y + v[8].w * xd.z;
+      }
+#pragma unroll
+      for (int o = LPR / 2; o > 0; o >>= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+      }
+      if (live && q == 0) spmv_row_out<float, 0>(row, a0, a1, a2, x, nullptr, y, part != nullptr, pacc);
+    }
+    __syncthreads();  // this stage may be refilled by the next prefetch
+  }
+  if (fail_sh) {
+    if (tid == 0) {
+      atomicExch(status, 1);
+      // copies in flight land before the shared memory goes away (bounded)
+      wait(k & 1, (uint32_t)((k >> 1) & 1));
+      if (next_issued) wait((k + 1) & 1, (uint32_t)(((k + 1) >> 1) & 1));
+    }
+    __syncthreads();
+    return;
+  }
+  if (part) {
+    const double tsum = block_sum<kBulkThreads>(pacc, sbuf);
+    if (threadIdx.x == 0) part[blockIdx.x] = tsum;
+  }
+}
+
 // FP64 SpMV: LPR lanes per block-row; a lane takes 2 blocks per trip (one
 // int2 of columns, nine double2 of values, two gathers of x).
 template <int MODE, int LPR>
@@ -247,22 +384,6 @@ __device__ __forceinline__ double sum_partials(const double *p, int n, double *s
   return block_sum<256>(v, sbuf);
 }
 
-// alpha = dot0 / (p.w)
-__global__ void __launch_bounds__(256) pcg_alpha(PcgState *st, const double *part, int n) {
-  if (st->done) return;
-  __shared__ double sbuf[32];
-  const double pw = sum_partials(part, n, sbuf);
-  if (threadIdx.x == 0) {
-    st->pw = pw;
-    // breakdown unless alpha > 0: p.Kp and z.r of one sign (an SPD system, or a
-    // negative definite one such as the stiffness of a left-handed B-spline
-    // parametrisation, which the reference's signed det J produces)
-    const double al = st->dot0 / pw;
-    if (!(al > 0.0) || !isfinite(pw) || !isfinite(al)) { st->done = 3; return; }
-    st->alpha = al;
-  }
-}
-
 // z = Dinv r with Dinv stored as 3 padded rows per node
 template <typename T>
 __device__ __forceinline__ void apply_dinv(const T *D, T r0, T r1, T r2, T &z0, T &z1, T &z2) {
@@ -271,65 +392,129 @@ __device__ __forceinline__ void apply_dinv(const T *D, T r0, T r1, T r2, T &z0, 
   z2 = D[8] * r0 + D[9] * r1 + D[10] * r2;
 }
 
-// u += alpha p; r -= alpha w; z = Dinv r; partials r.r, z.r
-template <typename T>
-__global__ void __launch_bounds__(kVecThreads)
-pcg_update(int64_t nnode, T *__restrict__ u, T *__restrict__ r, T *__restrict__ z, const T *__restrict__ p,
-           const T *__restrict__ w, const T *__restrict__ dinv, const PcgState *__restrict__ st,
-           double *__restrict__ part_rr, double *__restrict__ part_zr) {
-  if (st->done) return;
-  __shared__ double sbuf[32];
-  const T alpha = (T)st->alpha;
-  double rr = 0.0, zr = 0.0;
-  for (int64_t n = blockIdx.x * (int64_t)kVecThreads + threadIdx.x; n < nnode; n += (int64_t)gridDim.x * kVecThreads) {
-    T u0, u1, u2, p0, p1, p2, r0, r1, r2, w0, w1, w2, z0, z1, z2;
-    V4<T>::load(u + 4 * n, u0, u1, u2);
-    V4<T>::load(p + 4 * n, p0, p1, p2);
-    V4<T>::load(r + 4 * n, r0, r1, r2);
-    V4<T>::load(w + 4 * n, w0, w1, w2);
-    u0 = u0 + alpha * p0; u1 = u1 + alpha * p1; u2 = u2 + alpha * p2;
-    r0 = r0 + (-alpha) * w0; r1 = r1 + (-alpha) * w1; r2 = r2 + (-alpha) * w2;
-    apply_dinv(dinv + 12 * n, r0, r1, r2, z0, z1, z2);
-    V4<T>::store(u + 4 * n, u0, u1, u2);
-    V4<T>::store(r + 4 * n, r0, r1, r2);
-    V4<T>::store(z + 4 * n, z0, z1, z2);
-    rr += (double)r0 * r0 + (double)r1 * r1 + (double)r2 * r2;
-    zr += (double)z0 * r0 + (double)z1 * r1 + (double)z2 * r2;
+// ---- fused iteration kernels (kernel-per-step path)
+// The scalars of one iteration come from fixed-order sums of per-block
+// partials.  Instead of a single-block kernel between the vector kernels,
+// every block of the next vector kernel forms the same sum itself (same block
+// size, same order, hence the same bits) and takes the same decision; the
+// last block to finish (a counter in the state) commits the scalars, so no
+// block ever reads a value another block of the same launch has overwritten.
+
+// true in exactly one thread of the last block to reach this point
+__device__ __forceinline__ bool last_block(uint32_t *counter) {
+  __shared__ bool is_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint32_t t = atomicAdd(counter, 1u);
+    is_last = (t == gridDim.x - 1);
+    if (is_last) *counter = 0;
   }
-  const double t1 = block_sum<kVecThreads>(rr, sbuf);
-  if (threadIdx.x == 0) part_rr[blockIdx.x] = t1;
-  const double t2 = block_sum<kVecThreads>(zr, sbuf);
-  if (threadIdx.x == 0) part_zr[blockIdx.x] = t2;
+  __syncthreads();
+  return is_last && threadIdx.x == 0;
 }
 
-// err, convergence, beta
-__global__ void __launch_bounds__(256) pcg_beta(PcgState *st, const double *part_rr, const double *part_zr, int n) {
+// alpha = dot0 / p.w (every block), then u += alpha p; r -= alpha w;
+// z = Dinv r; partials r.r, z.r.  The last block stores p.w and alpha, or
+// the breakdown state, which every block detects alike.
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads)
+pcg_update_fused(int64_t nnode, T *__restrict__ u, T *__restrict__ r, T *__restrict__ z, const T *__restrict__ p,
+                 const T *__restrict__ w, const T *__restrict__ dinv, PcgState *__restrict__ st,
+                 const double *__restrict__ part_pw, int npw, double *__restrict__ part_rr,
+                 double *__restrict__ part_zr) {
   if (st->done) return;
   __shared__ double sbuf[32];
+  __shared__ double alpha_sh;
+  __shared__ int bad_sh;
+  const double pw = sum_partials(part_pw, npw, sbuf);
+  if (threadIdx.x == 0) {
+    const double al = st->dot0 / pw;
+    // breakdown unless alpha > 0: p.Kp and z.r of one sign (an SPD system, or
+    // a negative definite one such as the stiffness of a left-handed B-spline
+    // parametrisation, which the reference's signed det J produces)
+    bad_sh = (!(al > 0.0) || !isfinite(pw) || !isfinite(al)) ? 1 : 0;
+    alpha_sh = al;
+  }
+  __syncthreads();
+  const int bad = bad_sh;
+  const double al = alpha_sh;
+  double rr = 0.0, zr = 0.0;
+  if (!bad) {
+    const T alpha = (T)al;
+    for (int64_t n = blockIdx.x * (int64_t)kVecThreads + threadIdx.x; n < nnode;
+         n += (int64_t)gridDim.x * kVecThreads) {
+      T u0, u1, u2, p0, p1, p2, r0, r1, r2, w0, w1, w2, z0, z1, z2;
+      V4<T>::load(u + 4 * n, u0, u1, u2);
+      V4<T>::load(p + 4 * n, p0, p1, p2);
+      V4<T>::load(r + 4 * n, r0, r1, r2);
+      V4<T>::load(w + 4 * n, w0, w1, w2);
+      u0 = u0 + alpha * p0; u1 = u1 + alpha * p1; u2 = u2 + alpha * p2;
+      r0 = r0 + (-alpha) * w0; r1 = r1 + (-alpha) * w1; r2 = r2 + (-alpha) * w2;
+      apply_dinv(dinv + 12 * n, r0, r1, r2, z0, z1, z2);
+      V4<T>::store(u + 4 * n, u0, u1, u2);
+      V4<T>::store(r + 4 * n, r0, r1, r2);
+      V4<T>::store(z + 4 * n, z0, z1, z2);
+      rr += (double)r0 * r0 + (double)r1 * r1 + (double)r2 * r2;
+      zr += (double)z0 * r0 + (double)z1 * r1 + (double)z2 * r2;
+    }
+    const double t1 = block_sum<kVecThreads>(rr, sbuf);
+    if (threadIdx.x == 0) part_rr[blockIdx.x] = t1;
+    const double t2 = block_sum<kVecThreads>(zr, sbuf);
+    if (threadIdx.x == 0) part_zr[blockIdx.x] = t2;
+  }
+  if (last_block(&st->arrive_update)) {
+    st->pw = pw;
+    if (bad) st->done = 3;
+    else st->alpha = al;
+  }
+}
+
+// err, convergence and beta from the r.r / z.r partials (every block), then
+// p = z + beta p; the last block commits iter, rr, err, done, beta, dot0.
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads)
+pcg_direction_fused(int64_t nnode, T *__restrict__ p, const T *__restrict__ z, PcgState *__restrict__ st,
+                    const double *__restrict__ part_rr, const double *__restrict__ part_zr, int n) {
+  if (st->done) return;
+  __shared__ double sbuf[32];
+  __shared__ double beta_sh, err_sh;
+  __shared__ int done_sh;
   const double rr = sum_partials(part_rr, n, sbuf);
   const double zr = sum_partials(part_zr, n, sbuf);
   if (threadIdx.x == 0) {
+    const int iter = st->iter + 1;
+    const double err = sqrt(rr) / st->lenf;
+    int done = 0;
+    if (err < st->tol) done = 1;
+    else if (!isfinite(err)) done = 3;
+    else if (iter >= st->maxit) done = 2;
+    done_sh = done;
+    err_sh = err;
+    beta_sh = zr / st->dot0;
+  }
+  __syncthreads();
+  const int done = done_sh;
+  if (!done) {
+    const T beta = (T)beta_sh;
+    for (int64_t k = blockIdx.x * (int64_t)kVecThreads + threadIdx.x; k < nnode;
+         k += (int64_t)gridDim.x * kVecThreads) {
+      T p0, p1, p2, z0, z1, z2;
+      V4<T>::load(p + 4 * k, p0, p1, p2);
+      V4<T>::load(z + 4 * k, z0, z1, z2);
+      V4<T>::store(p + 4 * k, z0 + beta * p0, z1 + beta * p1, z2 + beta * p2);
+    }
+  }
+  if (last_block(&st->arrive_dir)) {
     st->iter += 1;
     st->rr = rr;
-    st->err = sqrt(rr) / st->lenf;
-    if (st->err < st->tol) { st->done = 1; return; }
-    if (!isfinite(st->err)) { st->done = 3; return; }
-    if (st->iter >= st->maxit) { st->done = 2; return; }
-    st->beta = zr / st->dot0;
-    st->dot0 = zr;
-  }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kVecThreads)
-pcg_pupdate(int64_t nnode, T *__restrict__ p, const T *__restrict__ z, const PcgState *__restrict__ st) {
-  if (st->done) return;
-  const T beta = (T)st->beta;
-  for (int64_t n = blockIdx.x * (int64_t)kVecThreads + threadIdx.x; n < nnode; n += (int64_t)gridDim.x * kVecThreads) {
-    T p0, p1, p2, z0, z1, z2;
-    V4<T>::load(p + 4 * n, p0, p1, p2);
-    V4<T>::load(z + 4 * n, z0, z1, z2);
-    V4<T>::store(p + 4 * n, z0 + beta * p0, z1 + beta * p1, z2 + beta * p2);
+    st->err = err_sh;
+    if (done) {
+      st->done = done;
+    } else {
+      st->beta = beta_sh;
+      st->dot0 = zr;
+    }
   }
 }
 
@@ -364,7 +549,8 @@ pcg_precond(int64_t nnode, const T *__restrict__ r, T *__restrict__ z, T *__rest
 // FP64 start: state from z.r, f.f and the initial r.r (warm start) or f.f
 __global__ void __launch_bounds__(256) pcg_init_scalar(PcgState *st, const double *part_zr, int nz,
                                                        const double *part_ff, int nf, const double *part_rr0,
-                                                       int nr, double tol, int maxit, int iter0) {
+                                                       int nr, double tol, const double *tol_dev, int maxit, int iter0) {
+  if (tol_dev) tol = *tol_dev;
   __shared__ double sbuf[32];
   const double zr = sum_partials(part_zr, nz, sbuf);
   const double ff = sum_partials(part_ff, nf, sbuf);
@@ -465,7 +651,8 @@ __global__ void keep_best(int64_t n4, const double *__restrict__ u, double *__re
 
 // mixed path start: lenf = |f| (with the reference's normaliser)
 __global__ void __launch_bounds__(256) mixed_init_scalar(PcgState *st, const double *part_ff, int nf, double tol,
-                                                         int maxit) {
+                                                         const double *tol_dev, int maxit) {
+  if (tol_dev) tol = *tol_dev;
   __shared__ double sbuf[32];
   const double ff = sum_partials(part_ff, nf, sbuf);
   if (threadIdx.x == 0) {
@@ -481,15 +668,15 @@ __global__ void __launch_bounds__(256) mixed_init_scalar(PcgState *st, const dou
 }
 
 // Jacobi / block-Jacobi inverse per node from the diagonal block; 3 padded rows
-template <typename T>
-__global__ void build_dinv(int64_t nnode, const int32_t *__restrict__ diag, const double *__restrict__ K,
+template <typename T, typename KT>
+__global__ void build_dinv(int64_t nnode, const int32_t *__restrict__ diag, const KT *__restrict__ K,
                            T *__restrict__ dinv, int block) {
   const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (n >= nnode) return;
   T *D = dinv + 12 * n;
   const int32_t d = diag[n];
   double a[9];
-  for (int k = 0; k < 9; k++) a[k] = (d >= 0) ? K[(int64_t)d * 9 + k] : (k % 4 == 0 ? 1.0 : 0.0);
+  for (int k = 0; k < 9; k++) a[k] = (d >= 0) ? (double)K[(int64_t)d * 9 + k] : (k % 4 == 0 ? 1.0 : 0.0);
   double inv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   if (!block) {
     inv[0] = 1.0 / a[0];
@@ -608,8 +795,60 @@ static void spmv64_go(const Ctx &c, int G, int64_t nn, const double *Ks, const d
     default: spmv_f64<MODE, 16><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, Ks, x, b, y, part, skip);
   }
 }
+// tiles of the bulk-staged SpMV: up to kBulkRows consecutive block-rows, cut
+// earlier when their values would pass kBulkTileBytes; built once per pattern
+constexpr int kBulkRows = 16;
+constexpr int64_t kBulkTileBytes = 48 * 1024;
+
+cudaError_t ensure_bulk_tiles(Ctx &c) {
+  if (c.d_tile_row) return cudaSuccess;
+  std::vector<int32_t> tr(1, 0);
+  int64_t vmax = 0;
+  const int64_t n = c.nnode;
+  for (int64_t r = 0; r < n;) {
+    int64_t e = std::min<int64_t>(r + kBulkRows, n);
+    while (e > r + 1 && 36 * (int64_t)(c.h_srow[e] - c.h_srow[r]) > kBulkTileBytes) e--;
+    vmax = std::max<int64_t>(vmax, 36 * (int64_t)(c.h_srow[e] - c.h_srow[r]));
+    tr.push_back((int32_t)e);
+    r = e;
+  }
+  c.bulk_vbytes = (int)((vmax + 127) / 128 * 128);
+  c.bulk_cbytes = (int)((vmax / 9 + 127) / 128 * 128);
+  c.bulk_ntiles = (int)tr.size() - 1;
+  cudaError_t e = cudaMalloc((void **)&c.d_tile_row, sizeof(int32_t) * tr.size());
+  if (e != cudaSuccess) return e;
+  e = cudaMemcpy(c.d_tile_row, tr.data(), sizeof(int32_t) * tr.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return e;
+  const int smem = 2 * (c.bulk_vbytes + c.bulk_cbytes);
+  int per_sm = 0;
+  for (auto kern : {spmv_f32_bulk<8>, spmv_f32_bulk<16>}) {
+    if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+    int a = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, kern, kBulkThreads, smem)) != cudaSuccess) return e;
+    per_sm = per_sm ? std::min(per_sm, a) : a;
+  }
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  c.bulk_grid = (int)std::min<int64_t>((int64_t)per_sm * c.sm_count, c.bulk_ntiles);
+  return cudaSuccess;
+}
+
+// CTAs (= p.w partials) of the FP32 SpMV in use
+static int spmv32_parts(const Ctx &c) { return c.spmv32_bulk ? c.bulk_grid : spmv_grid(c); }
+
 static void spmv32_go(const Ctx &c, int G, int64_t nn, const float *Ks, const float *x, float *y, double *part,
                       const int32_t *skip) {
+  if (c.spmv32_bulk) {
+    const int smem = 2 * (c.bulk_vbytes + c.bulk_cbytes);
+    if (c.lpr32 >= 16)
+      spmv_f32_bulk<16><<<c.bulk_grid, kBulkThreads, smem, c.stream>>>(c.bulk_ntiles, c.d_tile_row, c.d_srow, c.d_scol, Ks,
+                                                                        x, y, part, skip, c.d_status, c.bulk_vbytes,
+                                                                        c.bulk_cbytes);
+    else
+      spmv_f32_bulk<8><<<c.bulk_grid, kBulkThreads, smem, c.stream>>>(c.bulk_ntiles, c.d_tile_row, c.d_srow, c.d_scol, Ks,
+                                                                       x, y, part, skip, c.d_status, c.bulk_vbytes,
+                                                                       c.bulk_cbytes);
+    return;
+  }
   switch (c.lpr32) {
     case 4: spmv_f32<0, 4><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, Ks, x, nullptr, y, part, skip); break;
     case 16: spmv_f32<0, 16><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, Ks, x, nullptr, y, part, skip); break;
@@ -619,7 +858,62 @@ static void spmv32_go(const Ctx &c, int G, int64_t nn, const float *Ks, const fl
 }
 
 cudaError_t launch_to_soa(Ctx &c, const double *K, double *Ks, float *Ks32) {
-  aos_to_soa<<<spmv_grid(c), 256, 0, c.stream>>>(c.nnode, c.d_rowptr, c.d_srow, K, Ks, Ks32);
+  aos_to_soa<double><<<spmv_grid(c), 256, 0, c.stream>>>(c.nnode, c.d_rowptr, c.d_srow, K, Ks, Ks32);
+  c.launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_to_soa32(Ctx &c, const float *K32, float *Ks32) {
+  aos_to_soa<float><<<spmv_grid(c), 256, 0, c.stream>>>(c.nnode, c.d_rowptr, c.d_srow, K32, nullptr, Ks32);
+  c.launches++;
+  return cudaGetLastError();
+}
+
+// r = f - g on the padded node vectors (g = K u from the element kernels),
+// r.r per block; nothing while *skip is non-zero
+__global__ void __launch_bounds__(kSpmvThreads)
+sub_residual(int64_t n4, const double *__restrict__ f, const double *__restrict__ g, double *__restrict__ r,
+             double *__restrict__ part, const int32_t *__restrict__ skip) {
+  if (skip && *skip) return;
+  __shared__ double sbuf[32];
+  double rr = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)kSpmvThreads + threadIdx.x; i < n4; i += (int64_t)gridDim.x * kSpmvThreads) {
+    const double v = f[i] - g[i];
+    r[i] = v;
+    rr += v * v;
+  }
+  const double t = block_sum<kSpmvThreads>(rr, sbuf);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+__global__ void copy_unless(int64_t n, const double *__restrict__ a, double *__restrict__ b,
+                            const int32_t *__restrict__ skip) {
+  if (skip && *skip) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = a[i];
+}
+
+cudaError_t launch_matfree_residual(Ctx &c, const double *f, const double *u, double *r, double *part,
+                                    const int32_t *skip) {
+  const int64_t n4 = 4 * c.nnode;
+  cudaError_t e;
+  const double *uu = u;
+  if (c.has_ties()) {
+    // the full displacement field, slaves from their masters, in the FP64
+    // second search-direction buffer (unused by the mixed iteration)
+    copy_unless<<<kRedBlocks, 256, 0, c.stream>>>(n4, u, c.d_p2, skip);
+    c.launches++;
+    if ((e = launch_tie_prolong(c, c.d_p2)) != cudaSuccess) return e;
+    uu = c.d_p2;
+  }
+  if ((e = cudaMemsetAsync(c.d_gint, 0, sizeof(double) * n4, c.stream)) != cudaSuccess) return e;
+  if ((e = launch_tl_at(c, nullptr, c.d_gint, false, true, uu, skip)) != cudaSuccess) return e;
+  if (c.has_ties()) {
+    if ((e = launch_tied_matvec(c, uu, c.d_gint, skip)) != cudaSuccess) return e;
+    if ((e = launch_tie_restrict(c, c.d_gint)) != cudaSuccess) return e;
+    if ((e = launch_tie_zero(c, c.d_gint)) != cudaSuccess) return e;
+  }
+  sub_residual<<<spmv_grid(c), kSpmvThreads, 0, c.stream>>>(n4, f, c.d_gint, r, part, skip);
   c.launches++;
   return cudaGetLastError();
 }
@@ -638,8 +932,13 @@ cudaError_t launch_spmv32(Ctx &c, const float *Ks, const float *x, float *y) {
 
 cudaError_t launch_residual(Ctx &c, const double *Ks, const double *f, const double *u, double *r, double *rr_out) {
   double *part = P_E(c);
-  spmv64_go<1>(c, spmv_grid(c), c.nnode, Ks, u, f, r, part, nullptr);
-  c.launches++;
+  if (Ks) {
+    spmv64_go<1>(c, spmv_grid(c), c.nnode, Ks, u, f, r, part, nullptr);
+    c.launches++;
+  } else {
+    cudaError_t e = launch_matfree_residual(c, f, u, r, part, nullptr);
+    if (e != cudaSuccess) return e;
+  }
   finish_sum<<<1, 256, 0, c.stream>>>(part, spmv_grid(c), rr_out);
   c.launches++;
   return cudaGetLastError();
@@ -674,9 +973,20 @@ cudaError_t launch_node_to_eq(Ctx &c, const double *nodev, double *eqv) {
 cudaError_t launch_build_precond(Ctx &c, const double *K, int precond) {
   const int bs = 256;
   const unsigned g = (unsigned)((c.nnode + bs - 1) / bs);
-  build_dinv<double><<<g, bs, 0, c.stream>>>(c.nnode, c.d_diag, K, c.d_dinv, precond);
+  build_dinv<double, double><<<g, bs, 0, c.stream>>>(c.nnode, c.d_diag, K, c.d_dinv, precond);
   c.launches++;
-  build_dinv<float><<<g, bs, 0, c.stream>>>(c.nnode, c.d_diag, K, c.s_dinv, precond);
+  build_dinv<float, double><<<g, bs, 0, c.stream>>>(c.nnode, c.d_diag, K, c.s_dinv, precond);
+  c.launches++;
+  c.precond_built = precond;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_build_precond32(Ctx &c, const float *K32, int precond) {
+  const int bs = 256;
+  const unsigned g = (unsigned)((c.nnode + bs - 1) / bs);
+  build_dinv<double, float><<<g, bs, 0, c.stream>>>(c.nnode, c.d_diag, K32, c.d_dinv, precond);
+  c.launches++;
+  build_dinv<float, float><<<g, bs, 0, c.stream>>>(c.nnode, c.d_diag, K32, c.s_dinv, precond);
   c.launches++;
   c.precond_built = precond;
   return cudaGetLastError();
@@ -693,8 +1003,8 @@ cudaError_t launch_build_precond(Ctx &c, const double *K, int precond) {
 // same fixed order, so the scalars agree in every block without a broadcast
 // and a solve stays bit-reproducible.  Data written by other blocks during
 // the launch (p and the partials) is read through L2 (ld.global.cg).  The
-// scalars and the exit codes are exactly those of pcg_alpha/pcg_update/
-// pcg_beta/pcg_pupdate; block 0 writes them back to the PcgState at the end.
+// scalars and the exit codes are exactly those of pcg_update_fused /
+// pcg_direction_fused; block 0 writes them back to the PcgState at the end.
 constexpr int kPersistThreads = 512;
 constexpr uint64_t kBarrierWaitNs = 2000000000ull;  // one barrier wait; then the launch gives up
 
@@ -1235,11 +1545,13 @@ static cudaError_t drive(Ctx &c, int maxit, int chunk, cudaGraphExec_t *graph, i
   return cudaStreamSynchronize(c.stream);
 }
 
-cudaError_t pcg_fp64(Ctx &c, bool warm, double tol, int maxit, int chunk, int iter0) {
+// ---- the two PCG paths in pieces: initialisation and one chunk of
+// iterations, stream-ordered on c.stream (kernel-per-step form)
+
+static void fp64_init(Ctx &c, bool warm, double tol, const double *tol_dev, int maxit, int iter0) {
   const int64_t nn = c.nnode;
   const int G = spmv_grid(c), R = kRedBlocks;
   PcgState *st = c.d_state;
-  cudaError_t e;
   if (warm) {
     spmv64_go<1>(c, G, nn, c.d_Ks, c.d_u, c.d_f, c.d_r, P_E(c), nullptr);
     c.launches++;
@@ -1248,9 +1560,77 @@ cudaError_t pcg_fp64(Ctx &c, bool warm, double tol, int maxit, int chunk, int it
     cudaMemcpyAsync(c.d_r, c.d_f, sizeof(double) * 4 * nn, cudaMemcpyDeviceToDevice, c.stream);
   }
   pcg_precond<double><<<R, kVecThreads, 0, c.stream>>>(nn, c.d_r, c.d_z, c.d_p, c.d_dinv, c.d_f, P_C(c), P_D(c));
-  c.launches++;
-  pcg_init_scalar<<<1, 256, 0, c.stream>>>(st, P_C(c), R, P_D(c), R, warm ? P_E(c) : nullptr, G, tol, maxit, iter0);
-  c.launches++;
+  pcg_init_scalar<<<1, 256, 0, c.stream>>>(st, P_C(c), R, P_D(c), R, warm ? P_E(c) : nullptr, G, tol, tol_dev, maxit,
+                                           iter0);
+  c.launches += 2;
+}
+
+static void fp64_chunk(Ctx &c, int k) {
+  const int64_t nn = c.nnode;
+  const int G = spmv_grid(c), R = kRedBlocks;
+  PcgState *st = c.d_state;
+  for (int i = 0; i < k; i++) {
+    c.begin_span(0);
+    spmv64_go<0>(c, G, nn, c.d_Ks, c.d_p, nullptr, c.d_w, P_A(c), &st->done);
+    c.end_span();
+    pcg_update_fused<double><<<R, kVecThreads, 0, c.stream>>>(nn, c.d_u, c.d_r, c.d_z, c.d_p, c.d_w, c.d_dinv, st,
+                                                               P_A(c), G, P_B(c), P_C(c));
+    pcg_direction_fused<double><<<R, kVecThreads, 0, c.stream>>>(nn, c.d_p, c.d_z, st, P_B(c), P_C(c), R);
+    c.launches += 3;
+  }
+}
+
+static void mixed_init(Ctx &c, bool warm, double tol, const double *tol_dev, int maxit) {
+  const int64_t nn = c.nnode;
+  const int R = kRedBlocks;
+  if (!warm) cudaMemsetAsync(c.d_u, 0, sizeof(double) * 4 * nn, c.stream);
+  cudaMemsetAsync(c.s_x, 0, sizeof(float) * 4 * nn, c.stream);
+  sumsq_kernel<<<R, 256, 0, c.stream>>>(4 * nn, c.d_f, P_D(c));
+  mixed_init_scalar<<<1, 256, 0, c.stream>>>(c.d_state, P_D(c), R, tol, tol_dev, maxit);
+  c.launches += 2;
+}
+
+// mixed path: flush the FP32 correction into the FP64 solution, recompute
+// r = f - K u in FP64 (from the FP64 matrix, or element by element when the
+// stiffness is the tensor-core FP32 one) and restart the FP32 recurrence from it
+static void mixed_reliable(Ctx &c) {
+  const int64_t nn = c.nnode;
+  const int G = spmv_grid(c), R = kRedBlocks;
+  PcgState *st = c.d_state;
+  flush_correction<<<R, 256, 0, c.stream>>>(4 * nn, c.d_u, c.s_x, st);
+  if (c.K32_current) {
+    launch_matfree_residual(c, c.d_f, c.d_u, c.d_r, P_E(c), &st->final);  // counts its own launches
+  } else {
+    c.begin_span(0);
+    spmv64_go<1>(c, G, nn, c.d_Ks, c.d_u, c.d_f, c.d_r, P_E(c), &st->final);
+    c.end_span();
+    c.launches++;
+  }
+  replace_residual<<<R, kVecThreads, 0, c.stream>>>(nn, c.d_r, c.s_r, c.s_z, c.s_p, c.s_dinv, st, P_C(c));
+  reliable_scalar<<<1, 256, 0, c.stream>>>(st, P_E(c), G, P_C(c), R);
+  keep_best<<<R, 256, 0, c.stream>>>(4 * nn, c.d_u, c.d_ubest, st);
+  c.launches += 4;
+}
+
+static void mixed_chunk(Ctx &c, int k) {
+  const int64_t nn = c.nnode;
+  const int G = spmv_grid(c), R = kRedBlocks;
+  PcgState *st = c.d_state;
+  for (int i = 0; i < k; i++) {
+    c.begin_span(1);
+    spmv32_go(c, G, nn, c.d_Ks32, c.s_p, c.s_w, P_A(c), &st->done);
+    c.end_span();
+    pcg_update_fused<float><<<R, kVecThreads, 0, c.stream>>>(nn, c.s_x, c.s_r, c.s_z, c.s_p, c.s_w, c.s_dinv, st,
+                                                              P_A(c), spmv32_parts(c), P_B(c), P_C(c));
+    pcg_direction_fused<float><<<R, kVecThreads, 0, c.stream>>>(nn, c.s_p, c.s_z, st, P_B(c), P_C(c), R);
+    c.launches += 3;
+  }
+  mixed_reliable(c);
+}
+
+cudaError_t pcg_fp64(Ctx &c, bool warm, double tol, int maxit, int chunk, int iter0) {
+  cudaError_t e;
+  fp64_init(c, warm, tol, nullptr, maxit, iter0);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (use_persistent(c)) {
     const int pchunk = chunk < 64 ? 64 : chunk;  // each chunk is one launch: read the state back less often
@@ -1259,68 +1639,83 @@ cudaError_t pcg_fp64(Ctx &c, bool warm, double tol, int maxit, int chunk, int it
     });
   }
   return drive(c, maxit, chunk, &c.graph_fp64, &c.graph_fp64_chunk, &c.graph_fp64_kernels, [&](int k) -> cudaError_t {
-    for (int i = 0; i < k; i++) {
-      c.begin_span(0);
-      spmv64_go<0>(c, G, nn, c.d_Ks, c.d_p, nullptr, c.d_w, P_A(c), &st->done);
-      c.end_span();
-      pcg_alpha<<<1, 256, 0, c.stream>>>(st, P_A(c), G);
-      pcg_update<double><<<R, kVecThreads, 0, c.stream>>>(nn, c.d_u, c.d_r, c.d_z, c.d_p, c.d_w, c.d_dinv, st,
-                                                           P_B(c), P_C(c));
-      pcg_beta<<<1, 256, 0, c.stream>>>(st, P_B(c), P_C(c), R);
-      pcg_pupdate<double><<<R, kVecThreads, 0, c.stream>>>(nn, c.d_p, c.d_z, st);
-      c.launches += 5;
-    }
+    fp64_chunk(c, k);
     return cudaGetLastError();
   });
 }
 
 // FP32 PCG with FP64 reliable updates every `chunk` iterations.
 cudaError_t pcg_mixed(Ctx &c, bool warm, double tol, int maxit, int chunk) {
-  const int64_t nn = c.nnode;
-  const int G = spmv_grid(c), R = kRedBlocks;
-  PcgState *st = c.d_state;
   cudaError_t e;
-  if (!warm) cudaMemsetAsync(c.d_u, 0, sizeof(double) * 4 * nn, c.stream);
-  cudaMemsetAsync(c.s_x, 0, sizeof(float) * 4 * nn, c.stream);
-  sumsq_kernel<<<R, 256, 0, c.stream>>>(4 * nn, c.d_f, P_D(c));
-  mixed_init_scalar<<<1, 256, 0, c.stream>>>(st, P_D(c), R, tol, maxit);
-  c.launches += 2;
-  auto reliable = [&]() {
-    flush_correction<<<R, 256, 0, c.stream>>>(4 * nn, c.d_u, c.s_x, st);
-    c.begin_span(0);
-    spmv64_go<1>(c, G, nn, c.d_Ks, c.d_u, c.d_f, c.d_r, P_E(c), &st->final);
-    c.end_span();
-    replace_residual<<<R, kVecThreads, 0, c.stream>>>(nn, c.d_r, c.s_r, c.s_z, c.s_p, c.s_dinv, st, P_C(c));
-    reliable_scalar<<<1, 256, 0, c.stream>>>(st, P_E(c), G, P_C(c), R);
-    keep_best<<<R, 256, 0, c.stream>>>(4 * nn, c.d_u, c.d_ubest, st);
-    c.launches += 5;
-  };
-  reliable();
+  mixed_init(c, warm, tol, nullptr, maxit);
+  mixed_reliable(c);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (use_persistent(c)) {
     return drive(c, maxit, chunk, nullptr, nullptr, nullptr, [&](int k) -> cudaError_t {
       cudaError_t el = launch_persistent<float>(c, c.d_Ks32, c.s_x, c.s_r, c.s_z, c.s_p, c.s_p2, c.s_w, c.s_dinv, k);
       if (el != cudaSuccess) return el;
-      reliable();
+      mixed_reliable(c);
       return cudaGetLastError();
     });
   }
   return drive(c, maxit, chunk, &c.graph_mixed, &c.graph_mixed_chunk, &c.graph_mixed_kernels,
                [&](int k) -> cudaError_t {
-    for (int i = 0; i < k; i++) {
-      c.begin_span(1);
-      spmv32_go(c, G, nn, c.d_Ks32, c.s_p, c.s_w, P_A(c), &st->done);
-      c.end_span();
-      pcg_alpha<<<1, 256, 0, c.stream>>>(st, P_A(c), G);
-      pcg_update<float><<<R, kVecThreads, 0, c.stream>>>(nn, c.s_x, c.s_r, c.s_z, c.s_p, c.s_w, c.s_dinv, st,
-                                                          P_B(c), P_C(c));
-      pcg_beta<<<1, 256, 0, c.stream>>>(st, P_B(c), P_C(c), R);
-      pcg_pupdate<float><<<R, kVecThreads, 0, c.stream>>>(nn, c.s_p, c.s_z, st);
-      c.launches += 5;
-    }
-    reliable();
+    mixed_chunk(c, k);
     return cudaGetLastError();
   });
+}
+
+// ---- a whole solve inside a CUDA graph
+// keeps the WHILE node looping while the iteration runs (done == 0)
+__global__ void pcg_loop_cond(cudaGraphConditionalHandle h, const PcgState *__restrict__ st) {
+  cudaGraphSetConditional(h, st->done == 0 ? 1u : 0u);
+}
+
+cudaError_t record_pcg(Ctx &c, bool mixed, bool warm, double tol, const double *tol_dev, int maxit, int chunk) {
+  cudaError_t e;
+  if (mixed) {
+    mixed_init(c, warm, tol, tol_dev, maxit);
+    mixed_reliable(c);
+  } else {
+    fp64_init(c, warm, tol, tol_dev, maxit, 0);
+  }
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  // the WHILE node, appended to the graph being captured on c.stream
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t ndeps = 0;
+  if ((e = cudaStreamGetCaptureInfo(c.stream, &cs, nullptr, &g, &deps, &ndeps)) != cudaSuccess) return e;
+  if (cs != cudaStreamCaptureStatusActive || !g) return cudaErrorStreamCaptureUnmatched;
+  cudaGraphConditionalHandle h;
+  if ((e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault)) != cudaSuccess) return e;
+  cudaGraphNodeParams np{};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  if ((e = cudaGraphAddNode(&node, g, deps, ndeps, &np)) != cudaSuccess) return e;
+  if ((e = cudaStreamUpdateCaptureDependencies(c.stream, &node, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess)
+    return e;
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  // the loop body: one chunk and the condition, captured on the side stream
+  if (!c.side_stream && (e = cudaStreamCreateWithFlags(&c.side_stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return e;
+  cudaStream_t main = c.stream;
+  c.stream = c.side_stream;
+  e = cudaStreamBeginCaptureToGraph(c.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    if (mixed) mixed_chunk(c, chunk);
+    else fp64_chunk(c, chunk);
+    pcg_loop_cond<<<1, 1, 0, c.stream>>>(h, c.d_state);
+    c.launches++;
+    cudaError_t el = cudaGetLastError();
+    e = cudaStreamEndCapture(c.stream, &body);
+    if (e == cudaSuccess) e = el;
+  }
+  c.stream = main;
+  return e;
 }
 
 }  // namespace fastgpu

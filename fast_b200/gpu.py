@@ -30,7 +30,7 @@ FAST_GPU_OK = 0
 ERRORS = {-1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ESTATE", -5: "ENONCONV", -6: "EDETJ", -7: "ENOTSUP",
           -8: "ENOTFOUND", -9: "ETOOBIG"}
 ELEM = {"hex8": 1, "hex20": 2, "bsp": 3}
-ASM_K, ASM_M, ASM_G = 1, 2, 3
+ASM_K, ASM_M, ASM_G, ASM_K_TF32 = 1, 2, 3, 4
 FORM_SMALL, FORM_TL = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 PRECOND_JACOBI, PRECOND_BLOCK_JACOBI = 0, 1
@@ -39,7 +39,7 @@ PRECOND_JACOBI, PRECOND_BLOCK_JACOBI = 0, 1
 EXPORTS = [
     "fast_gpu_create", "fast_gpu_destroy", "fast_gpu_last_error", "fast_gpu_version", "fast_gpu_set_stream",
     "fast_gpu_synchronize", "fast_gpu_upload_mesh", "fast_gpu_pattern_info", "fast_gpu_update_coords",
-    "fast_gpu_update_material", "fast_gpu_zero", "fast_gpu_assemble", "fast_gpu_add", "fast_gpu_get",
+    "fast_gpu_update_material", "fast_gpu_zero", "fast_gpu_assemble", "fast_gpu_add", "fast_gpu_add_mat", "fast_gpu_get",
     "fast_gpu_mult_vect", "fast_gpu_solve", "fast_gpu_solve_device", "fast_gpu_face_load_vector",
     "fast_gpu_get_lower_csr", "fast_gpu_element_matrices", "fast_gpu_launch_count", "fast_gpu_kernel_timing", "fast_gpu_kernel_stats",
     "fast_gpu_inspect_pattern", "fast_gpu_pcg_solve_noalloc", "fast_gpu_set_displacement",
@@ -51,9 +51,11 @@ EXPORTS = [
     "fast_gpu_mlp_loss_grad", "fast_gpu_mlp_gemm", "fast_gpu_ws_configure", "fast_gpu_ws_last_input",
     "fast_gpu_set_option", "fast_gpu_set_problems", "fast_gpu_solve_batch", "fast_gpu_newmark",
 ]
-OPT_PERSISTENT_MAX_NODES, OPT_SPMV_LANES_FP32, OPT_SPMV_LANES_FP64 = 1, 2, 3
+OPT_PERSISTENT_MAX_NODES, OPT_SPMV_LANES_FP32, OPT_SPMV_LANES_FP64, OPT_GRAPH_STEPS = 1, 2, 3, 4
+OPT_SPMV_BULK_FP32 = 5
 KERNEL_SPMV_FP64, KERNEL_SPMV_FP32, KERNEL_ASSEMBLE = 0, 1, 2
 KERNEL_PREDICT_NET, KERNEL_PREDICT_GALERKIN, KERNEL_INTERNAL_FORCE, KERNEL_LINEAR_SOLVE = 3, 4, 5, 6
+KERNEL_ASSEMBLE_TF32 = 7
 
 
 class FastGpuError(RuntimeError):
@@ -180,11 +182,13 @@ class NewmarkReport(ctypes.Structure):
 class TuneReport(ctypes.Structure):
     _fields_ = [("lanes_fp32", ctypes.c_int32), ("lanes_fp64", ctypes.c_int32), ("ms_fp32", ctypes.c_double * 4),
                 ("ms_fp64", ctypes.c_double * 4), ("persistent_max_nodes", ctypes.c_int64),
-                ("us_iter_persistent", ctypes.c_double), ("us_iter_kernels", ctypes.c_double)]
+                ("us_iter_persistent", ctypes.c_double), ("us_iter_kernels", ctypes.c_double),
+                ("ms_fp32_bulk", ctypes.c_double * 2), ("bulk_fp32", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
     def as_dict(self):
         return {"lanes_fp32": self.lanes_fp32, "lanes_fp64": self.lanes_fp64,
                 "ms_fp32_lanes_4_8_16_32": list(self.ms_fp32), "ms_fp64_lanes_4_8_16_32": list(self.ms_fp64),
+                "ms_fp32_bulk_lanes_8_16": list(self.ms_fp32_bulk), "bulk_fp32": bool(self.bulk_fp32),
                 "persistent_max_nodes": self.persistent_max_nodes, "us_iter_persistent": self.us_iter_persistent,
                 "us_iter_kernels": self.us_iter_kernels}
 
@@ -252,6 +256,7 @@ def load_library(path: str = LIB_PATH):
     L.fast_gpu_zero.argtypes = [vp, ctypes.c_int32]
     L.fast_gpu_assemble.argtypes = [vp, ctypes.c_int32]
     L.fast_gpu_add.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_double]
+    L.fast_gpu_add_mat.argtypes = [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_int32]
     L.fast_gpu_get.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _dp]
     L.fast_gpu_mult_vect.argtypes = [vp, ctypes.c_int32, _dp, _dp]
     L.fast_gpu_solve.argtypes = [vp, _dp, _dp, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveReport)]
@@ -661,6 +666,10 @@ class GpuSystem:
 
     def add(self, i, j, v, what=ASM_K):
         self._ck(self.L.fast_gpu_add(self.ctx, what, int(i), int(j), float(v)), "add")
+
+    def add_mat(self, a, dst=ASM_K, src=ASM_M):
+        """cSysMatrix::AddMat(a, M): K += a M on the device."""
+        self._ck(self.L.fast_gpu_add_mat(self.ctx, dst, float(a), src), "add_mat")
 
     def get(self, i, j, what=ASM_K):
         v = ctypes.c_double()

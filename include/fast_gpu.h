@@ -3,8 +3,8 @@
  *
  * The library sits under FAST's own C++ interfaces.  Each entry point below
  * names the reference interface it replaces (file:line inside the FAST
- * tree).  INTEGRATION.md shows the C++ shim a FAST maintainer adds: a
- * cSysMatrix subclass whose virtuals forward here, and a batched
+ * tree).  Above it sits a C++ shim in FAST's own terms: a cSysMatrix
+ * subclass whose virtuals forward here, and a batched
  * cControl::StiffnessMatrix that uploads the mesh once and assembles on the
  * device.
  *
@@ -66,6 +66,16 @@ extern "C" {
                                    displacements */
 #define FAST_ASM_MASS       2   /* cControl::MassMatrix      (ctrl/ctrl.cpp:979-1027) */
 #define FAST_ASM_INTERNAL_FORCE 3  /* element internal forces (fast_gpu_element_matrices only) */
+#define FAST_ASM_STIFFNESS_TF32 4  /* the stiffness for the mixed-precision solve: element
+                                      products B^T C B on the tensor cores (tcgen05, 3xTF32 split,
+                                      FP32 accumulation), blocks stored in FP32.  Small-strain
+                                      hex8 / hex20 buckets and B-spline solids of degree (2,2,2),
+                                      (3,3,3) or (3,3,2); elements touching a tied node keep FP64
+                                      element matrices, scattered into the FP32 blocks.  The FP64 stiffness slot is
+                                      then stale: fast_gpu_solve takes FAST_PREC_MIXED only and forms
+                                      its FP64 residuals r = f - K u element by element in FP64
+                                      (the small-strain internal force at u); the next
+                                      FAST_ASM_STIFFNESS assembly restores the FP64 path. */
 
 /* ---- solver precision ------------------------------------------------- */
 #define FAST_PREC_FP64      0   /* FP64 Jacobi PCG, as PCGSolver (mlib/sysmat.cpp:1061-1125) */
@@ -177,6 +187,13 @@ int         fast_gpu_synchronize(fast_gpu_ctx *ctx);
                                             0 = always one kernel per step of the iteration */
 #define FAST_OPT_SPMV_LANES_FP32      2  /* lanes per block-row of the FP32 SpMV: 4, 8 (default), 16, 32 */
 #define FAST_OPT_SPMV_LANES_FP64      3  /* lanes per block-row of the FP64 SpMV: 4, 8, 16 (default), 32 */
+#define FAST_OPT_SPMV_BULK_FP32       5  /* 1: the FP32 SpMV streams the matrix through shared memory by
+                                            bulk copies (tiles of block-rows, two stages); 0 (default
+                                            until fast_gpu_autotune measures it): register loads */
+#define FAST_OPT_GRAPH_STEPS          4  /* 1 (default): fast_gpu_newmark replays every step after the first
+                                            as one CUDA graph, and fast_gpu_nr_solve every Newton
+                                            iteration after a step's first (the PCG loop inside as a
+                                            conditional WHILE node); 0: launch kernel by kernel */
 int         fast_gpu_set_option(fast_gpu_ctx *ctx, int32_t option, int64_t value);
 
 /* Autotuner (no reference counterpart): times the SpMV of the assembled
@@ -190,6 +207,9 @@ typedef struct {
   double  ms_fp32[4], ms_fp64[4];       /* per launch for 4, 8, 16, 32 lanes              */
   int64_t persistent_max_nodes;         /* chosen limit for the persistent PCG kernel     */
   double  us_iter_persistent, us_iter_kernels;  /* FP64 PCG per iteration, or 0 if not timed */
+  double  ms_fp32_bulk[2];              /* bulk-staged FP32 SpMV per launch, 8 and 16 lanes per row */
+  int32_t bulk_fp32;                    /* 1: the bulk-staged FP32 SpMV was kept                  */
+  int32_t reserved;
 } fast_gpu_tune_report;
 int         fast_gpu_autotune(fast_gpu_ctx *ctx, fast_gpu_tune_report *rep);
 
@@ -495,6 +515,13 @@ int fast_gpu_assemble(fast_gpu_ctx *ctx, int32_t what);
 /* cSysMatrix::Add(i, j, v): adds v to K(i,j) and K(j,i) when i != j, like the
  * reference's symmetric matrices; (i, j) must lie in the pattern. */
 int fast_gpu_add(fast_gpu_ctx *ctx, int32_t what, int32_t i, int32_t j, double v);
+/* cSysMatrix::AddMat(a, M) (mlib/sysmat.h:98, used by cCtrlNewmark for
+ * K_eff = K + a0 M, ctrl/ctrlnewmark.cpp:141,160): K += a M over the shared
+ * block pattern, on the device.  dst must be FAST_ASM_STIFFNESS and src
+ * FAST_ASM_MASS, both assembled (FAST_GPU_ESTATE otherwise).  Fixed DOFs keep
+ * the stiffness slot's unit diagonal (the mass slot holds 0 there).  The
+ * stiffness slot then holds K + a M: the next stiffness assembly rebuilds K. */
+int fast_gpu_add_mat(fast_gpu_ctx *ctx, int32_t dst, double a, int32_t src);
 /* cSysMatrix::Get(i, j) */
 int fast_gpu_get(fast_gpu_ctx *ctx, int32_t what, int32_t i, int32_t j, double *v);
 /* cSysMatrix::MultVect(in, out): out = K in, equation space, host buffers. */
@@ -571,13 +598,15 @@ int fast_gpu_nodal_stress(fast_gpu_ctx *ctx, int32_t bucket, double *elem_nodal,
 int fast_gpu_inspect_pattern(const fast_gpu_mesh *mesh, int64_t *nnz_blocks, int64_t *nnz_lower_eq,
                              int32_t *num_colors, int32_t *rowptr, int32_t *col, int32_t *color);
 /* Equation-space lower triangle of the assembled matrix as CSR (what the
- * reference's symmetric matrices store).  Call with col == NULL to get nnz. */
+ * reference's symmetric matrices store).  Call with col == NULL to get nnz.
+ * what = FAST_ASM_STIFFNESS_TF32 reads the tensor-core FP32 stiffness. */
 int fast_gpu_get_lower_csr(fast_gpu_ctx *ctx, int32_t what, int64_t *nnz,
                            int64_t *rowptr, int32_t *col, double *val);
 /* Element matrices of elements [first, first+count) of a bucket, computed by
  * the same device kernels as the assembly: [count][3nn][3nn] row-major in
  * FAST's element DOF order (cElement::GetElmDofs); with
- * FAST_ASM_INTERNAL_FORCE the element internal forces, [count][3nn]. */
+ * FAST_ASM_INTERNAL_FORCE the element internal forces, [count][3nn]; with
+ * FAST_ASM_STIFFNESS_TF32 the tensor-core (3xTF32) element stiffness. */
 int fast_gpu_element_matrices(fast_gpu_ctx *ctx, int32_t what, int32_t bucket, int64_t first,
                               int64_t count, double *Ke);
 
@@ -589,6 +618,7 @@ int fast_gpu_element_matrices(fast_gpu_ctx *ctx, int32_t what, int32_t bucket, i
 #define FAST_KERNEL_PREDICT_GALERKIN  4  /* learned predictor: reduced Newton corrections  */
 #define FAST_KERNEL_INTERNAL_FORCE    5  /* one internal-force evaluation                  */
 #define FAST_KERNEL_LINEAR_SOLVE      6  /* one fast_gpu_solve_device call                 */
+#define FAST_KERNEL_ASSEMBLE_TF32     7  /* one tensor-core stiffness assembly (FP32 blocks)   */
 /* Kernels this context has launched so far (every entry point counts). */
 int fast_gpu_launch_count(fast_gpu_ctx *ctx, int64_t *count);
 /* Live timing: while enabled, every SpMV launched by a solve, every
@@ -611,15 +641,29 @@ int fast_gpu_kernel_stats(fast_gpu_ctx *ctx, int32_t which, int64_t *launches, d
  * equation-space CSR matrix (full symmetric storage: d_rowptr [num_eq+1],
  * d_col / d_val [nnz]), load d_f and solution d_u [num_eq], all device
  * memory.  Needs no context.  Work vectors live in a static device array of
- * the library (20 MB on each device that loads it, held until exit), so
+ * the library (20 MB on each device that has loaded it, held until exit), so
  * num_eq is limited to 500000; a larger system is rejected with
- * FAST_GPU_ETOOBIG before any CUDA call.  The first call on a device looks up
- * that array's device address with the device current; make that first call
- * before any stream capture.  Calls share the array and it keeps the last
- * call's contents (each call re-initialises what it uses): calls that overlap
- * on the GPU race.  Runs on cuda_stream (a cudaStream_t, NULL = legacy
- * default stream) and synchronises it every 32 iterations; rep may be NULL
- * (its true_rel_residual is not computed here and is set to -1). */
+ * FAST_GPU_ETOOBIG before any CUDA call.
+ *   First call on a device: with CUDA's lazy module loading (the default
+ *   unless CUDA_MODULE_LOADING=EAGER) the array is loaded onto the device,
+ *   and so takes its 20 MB of device memory, during the first call made
+ *   there; that call may also synchronise the device, and fails with
+ *   FAST_GPU_ECUDA if no device memory is left.  num_eq = 0 (pointers may be
+ *   NULL) does only this set-up and returns FAST_GPU_OK: make it before the
+ *   caller's pool takes the device and before any stream capture.  Later
+ *   calls allocate nothing.
+ *   Every call looks up the array's device address with the caller's device
+ *   current.  Calls share the array and it keeps the last call's contents
+ *   (each call re-initialises what it uses): calls that overlap on the GPU
+ *   race.
+ *   tol <= 0 gives 1e-5 and maxit <= 0 gives num_eq, cSysMatrix's defaults
+ *   (mlib/sysmat.h:76-77).  Runs on cuda_stream (a cudaStream_t, NULL =
+ *   legacy default stream) and synchronises it every 32 iterations; rep may
+ *   be NULL (its true_rel_residual is not computed here and is set to -1).
+ *   Returns FAST_GPU_EINVAL for a row whose diagonal is not stored, zero or
+ *   not finite (Jacobi is undefined), and FAST_GPU_ENONCONV when maxit is
+ *   reached or on a breakdown (p.Kp not positive or a non-finite value: K is
+ *   not positive definite), the latter with rep->iterations below maxit. */
 int fast_gpu_pcg_solve_noalloc(int32_t num_eq, const int64_t *d_rowptr, const int32_t *d_col, const double *d_val,
                                const double *d_f, double *d_u, double tol, int32_t maxit, void *cuda_stream,
                                fast_gpu_solve_report *rep);

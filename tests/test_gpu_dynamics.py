@@ -47,3 +47,23 @@ def test_newmark_warm_start_saves_iterations():
     assert r1["linear_iterations"] < r0["linear_iterations"]
     np.testing.assert_allclose(h1, h0, rtol=1e-8, atol=1e-14)
     s.close()
+
+
+@pytest.mark.parametrize("precision", [gpu.PREC_FP64, gpu.PREC_MIXED])
+def test_newmark_graph_replay_equals_direct_launches(precision):
+    """Every step after the first replays one captured CUDA graph (the PCG
+    loop as a conditional WHILE node); launching kernel by kernel gives the
+    same steps."""
+    d, g = gio.load("nm_hex20_box")
+    s = gpu.GpuSystem(0)
+    s.upload(d)
+    args = (g["ref_f"], int(g["steps"]), float(g["time_step"]))
+    probes = np.arange(s.neq)
+    (u1, _, _), h1, r1 = s.newmark(*args, precision=precision, tol=1e-12, probes=probes)
+    s.set_option(gpu.OPT_GRAPH_STEPS, 0)
+    (u0, _, _), h0, r0 = s.newmark(*args, precision=precision, tol=1e-12, probes=probes)
+    assert r1["steps_done"] == r0["steps_done"] == int(g["steps"])
+    if precision == gpu.PREC_FP64:
+        assert r1["linear_iterations"] == r0["linear_iterations"]
+    assert gio.rel(h1, h0) < 1e-10 and gio.rel(u1, u0) < 1e-10
+    s.close()

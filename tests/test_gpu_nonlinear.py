@@ -122,3 +122,28 @@ def test_arclength_reports_failure():
     with pytest.raises(gpu.FastGpuError) as ei:
         s.arclength_solve(q, "clinal", 2, 0.5, tol=1e-30, max_iter=3)
     assert ei.value.rc == -5
+
+
+@pytest.mark.parametrize("precision", [gpu.PREC_FP64, gpu.PREC_MIXED])
+def test_newton_graph_replay_equals_direct_launches(precision):
+    """Newton iterations after the first replay one captured CUDA graph
+    (tangent, preconditioner, the PCG as a conditional WHILE node, update,
+    internal force, norms); kernel-by-kernel launches give the same steps."""
+    d = decks.plate_tl_hex8(8, 8, 2, L=4.0, t=0.4, pressure=10.0, steps=6, tol=1e-8)
+    q = gpu.face_load_vector(d)
+    s = system(d)
+    kw = dict(tol=1e-8, predictor=gpu.PREDICT_SECANT, precision=precision, lin_tol=1e-10,
+              lin_tol_rel=1e-3 if precision == gpu.PREC_MIXED else 0.0)
+    h1, it1, r1 = s.nr_solve(q, 6, 1 / 6, **kw)
+    s.set_option(gpu.OPT_GRAPH_STEPS, 0)
+    h0, it0, r0 = s.nr_solve(q, 6, 1 / 6, **kw)
+    assert r1["converged_steps"] == r0["converged_steps"] == 6
+    if precision == gpu.PREC_FP64:
+        # the same iteration, so the same Newton iterations
+        assert (it1 == it0).all(), (it1, it0)
+        assert gio.rel(h1, h0) < 1e-10
+    else:
+        # the FP64 residual replacements fall on other iterations (the replayed
+        # loop refreshes every 16): both meet the Newton tolerance
+        assert gio.rel(h1, h0) < 1e-7
+    s.close()

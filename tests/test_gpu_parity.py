@@ -133,6 +133,28 @@ def test_mass_matrices_match_reference():
     assert abs(Ml - R).max() / abs(R).max() < TOL_K
 
 
+def test_add_mat_forms_newmark_effective_stiffness():
+    """cSysMatrix::AddMat(a0, M) as cCtrlNewmark uses it: K + a0 M on the device."""
+    d, g = gio.load("cfg_hex8_mass")
+    s = system(d)
+    s.assemble_mass()
+    s.assemble()
+    Kl = s.lower_csr()
+    Ml = s.lower_csr(gpu.ASM_M)
+    a0 = 4.0 / (1e-2 ** 2)
+    s.add_mat(a0)
+    Keff = s.lower_csr()
+    R = (Kl + a0 * Ml).tocsr()
+    assert abs(Keff - R).max() / abs(R).max() < 1e-15
+    # the solve uses K + a0 M, and the next stiffness assembly restores K
+    f = np.ones(s.neq)
+    u, rep = s.solve(f, tol=1e-12, precision=gpu.PREC_FP64)
+    Kf = R + sp.tril(R, -1).T
+    assert rep["converged"] and np.linalg.norm(Kf @ u - f) / np.linalg.norm(f) < 1e-10
+    s.assemble()
+    assert abs(s.lower_csr() - Kl).max() == 0.0
+
+
 @PATHS
 @pytest.mark.parametrize("precond", [gpu.PRECOND_JACOBI, gpu.PRECOND_BLOCK_JACOBI])
 def test_medium_hex20_against_oracle(precond, persistent):
