@@ -44,7 +44,10 @@ struct BspSmem {
 // of NT node pairs (they write disjoint blocks of K); the geometry is
 // recomputed by each.  Fills the GPU when a colour holds few elements (a
 // degree-3 patch needs 64 colours).
-template <int PR, int PS, int PT, int NG1, int NT>
+// MASS: the consistent mass instead (cElmParam::MassMat, elc/elmparam.cpp:
+// 672-739, on the same Gauss points as the stiffness): block (a, b) =
+// rho sum_g c_g N_a N_b I3 with the (rational) basis values N.
+template <int PR, int PS, int PT, int NG1, int NT, bool MASS>
 __global__ void __launch_bounds__(NT, 1) bsp_elem_kernel(ElemArgs A, int split) {
   using S = BspSmem<PR, PS, PT, NG1>;
   constexpr int QR = S::QR, QS = S::QS, QT = S::QT, NN = S::NN, NG = S::NG, NP = S::NP, ND = 3 * NN;
@@ -99,6 +102,7 @@ __global__ void __launch_bounds__(NT, 1) bsp_elem_kernel(ElemArgs A, int split) 
         D[NN + a] = fr[0] * fs[1] * ft[0] * w;
         D[2 * NN + a] = fr[0] * fs[0] * ft[1] * w;
       } else {
+        if (MASS) sB[g * NN + a] = fr[0] * fs[0] * ft[0];
         D[a] = fr[1] * fs[0] * ft[0];
         D[NN + a] = fr[0] * fs[1] * ft[0];
         D[2 * NN + a] = fr[0] * fs[0] * ft[1];
@@ -211,9 +215,18 @@ __global__ void __launch_bounds__(NT, 1) bsp_elem_kernel(ElemArgs A, int split) 
     }
     __syncthreads();
 
+    if (MASS && rat) {
+      // the rational basis values N_a = B_a w_a / W
+      for (int t = tid; t < NG * NN; t += NT) {
+        const int g = t / NN;
+        sB[t] = sB[t] / sWg[4 * g];
+      }
+      __syncthreads();
+    }
     const double E = A.E[e], nu = A.nu[e];
     const double dd = (1.0 + nu) * (1.0 - 2.0 * nu);
     const double C00 = E * (1.0 - nu) / dd, C01 = E * nu / dd, G = 0.5 * E / (1.0 + nu);
+    const double rho = (MASS && A.rho) ? A.rho[e] : 0.0;
     for (int q = tid + part * NT; q < NP; q += NT * split) {
       const int pa = spair[2 * q], pb = spair[2 * q + 1];
       // the pair's two K blocks are loaded before its Gauss-point sum, so the
@@ -230,26 +243,34 @@ __global__ void __launch_bounds__(NT, 1) bsp_elem_kernel(ElemArgs A, int split) 
           for (int k = 0; k < 9; k++) oba[k] = Kba[k];
         }
       }
-      double M[9];
-#pragma unroll
-      for (int k = 0; k < 9; k++) M[k] = 0.0;
-      for (int g = 0; g < NG; g++) {
-        const double *D = sD + g * ND;
-        const double cg = sc[g];
-        const double a0 = cg * D[pa], a1 = cg * D[NN + pa], a2 = cg * D[2 * NN + pa];
-        const double b0 = D[pb], b1 = D[NN + pb], b2 = D[2 * NN + pb];
-        M[0] = fma(a0, b0, M[0]); M[1] = fma(a0, b1, M[1]); M[2] = fma(a0, b2, M[2]);
-        M[3] = fma(a1, b0, M[3]); M[4] = fma(a1, b1, M[4]); M[5] = fma(a1, b2, M[5]);
-        M[6] = fma(a2, b0, M[6]); M[7] = fma(a2, b1, M[7]); M[8] = fma(a2, b2, M[8]);
-      }
-      // isotropic block (cSolid::QMatrix elc/anmodel.cpp:1286-1298, BMatrix :1418-1447)
       double v[9];
-      const double tr = M[0] + M[4] + M[8];
+      if (MASS) {
+        double sm_ab = 0.0;
+        for (int g = 0; g < NG; g++) sm_ab += sc[g] * sB[g * NN + pa] * sB[g * NN + pb];
+        sm_ab *= rho;
 #pragma unroll
-      for (int i = 0; i < 3; i++)
+        for (int k = 0; k < 9; k++) v[k] = (k % 4 == 0) ? sm_ab : 0.0;
+      } else {
+        double M[9];
 #pragma unroll
-        for (int j = 0; j < 3; j++)
-          v[3 * i + j] = (i == j) ? C00 * M[4 * i] + G * (tr - M[4 * i]) : C01 * M[3 * i + j] + G * M[3 * j + i];
+        for (int k = 0; k < 9; k++) M[k] = 0.0;
+        for (int g = 0; g < NG; g++) {
+          const double *D = sD + g * ND;
+          const double cg = sc[g];
+          const double a0 = cg * D[pa], a1 = cg * D[NN + pa], a2 = cg * D[2 * NN + pa];
+          const double b0 = D[pb], b1 = D[NN + pb], b2 = D[2 * NN + pb];
+          M[0] = fma(a0, b0, M[0]); M[1] = fma(a0, b1, M[1]); M[2] = fma(a0, b2, M[2]);
+          M[3] = fma(a1, b0, M[3]); M[4] = fma(a1, b1, M[4]); M[5] = fma(a1, b2, M[5]);
+          M[6] = fma(a2, b0, M[6]); M[7] = fma(a2, b1, M[7]); M[8] = fma(a2, b2, M[8]);
+        }
+        // isotropic block (cSolid::QMatrix elc/anmodel.cpp:1286-1298, BMatrix :1418-1447)
+        const double tr = M[0] + M[4] + M[8];
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+          for (int j = 0; j < 3; j++)
+            v[3 * i + j] = (i == j) ? C00 * M[4 * i] + G * (tr - M[4 * i]) : C01 * M[3 * i + j] + G * M[3 * j + i];
+      }
       if (A.Ke_out) {
         double *Ko = A.Ke_out + it * ND * ND;
 #pragma unroll
@@ -275,11 +296,11 @@ __global__ void __launch_bounds__(NT, 1) bsp_elem_kernel(ElemArgs A, int split) 
   }
 }
 
-template <int PR, int PS, int PT, int NG1, int NT>
+template <int PR, int PS, int PT, int NG1, int NT, bool MASS = false>
 static cudaError_t run_bsp(Ctx &c, ElemArgs a, int64_t count) {
   if (count <= 0) return cudaSuccess;
   using S = BspSmem<PR, PS, PT, NG1>;
-  auto kern = bsp_elem_kernel<PR, PS, PT, NG1, NT>;
+  auto kern = bsp_elem_kernel<PR, PS, PT, NG1, NT, MASS>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -570,13 +591,20 @@ bool bsp_supported(const int pd[3], int ngp) {
   return false;
 }
 
-cudaError_t launch_bsp_elements(Ctx &c, const Bucket &B, ElemArgs a, int64_t count) {
+cudaError_t launch_bsp_elements(Ctx &c, const Bucket &B, ElemArgs a, int64_t count, bool mass) {
   a.span = B.d_span;
   for (int d = 0; d < 3; d++) a.bas[d] = B.d_bas + B.bas_off[d];
   a.wt = B.d_wt;
   a.rational = B.rational;
   const int ng = B.ngp[0];
   const int *p = B.pd;
+  if (mass) {
+    if (p[0] == 2 && p[1] == 2 && p[2] == 2 && ng == 3) return run_bsp<2, 2, 2, 3, 384, true>(c, a, count);
+    if (p[0] == 2 && p[1] == 2 && p[2] == 2 && ng == 4) return run_bsp<2, 2, 2, 4, 384, true>(c, a, count);
+    if (p[0] == 3 && p[1] == 3 && p[2] == 3 && ng == 4) return run_bsp<3, 3, 3, 4, 384, true>(c, a, count);
+    if (p[0] == 3 && p[1] == 3 && p[2] == 2 && ng == 4) return run_bsp<3, 3, 2, 4, 384, true>(c, a, count);
+    return cudaErrorNotSupported;
+  }
   if (p[0] == 2 && p[1] == 2 && p[2] == 2 && ng == 3) return run_bsp<2, 2, 2, 3, 384>(c, a, count);
   if (p[0] == 2 && p[1] == 2 && p[2] == 2 && ng == 4) return run_bsp<2, 2, 2, 4, 384>(c, a, count);
   if (p[0] == 3 && p[1] == 3 && p[2] == 3 && ng == 4) return run_bsp<3, 3, 3, 4, 384>(c, a, count);

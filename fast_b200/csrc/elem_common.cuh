@@ -34,8 +34,9 @@ struct ElemArgs {
 
 struct Ctx;
 struct Bucket;
-// B-spline solid buckets (bsp_kernels.cu): stiffness scatter or element matrices
-cudaError_t launch_bsp_elements(Ctx &c, const Bucket &B, ElemArgs a, int64_t count);
+// B-spline solid buckets (bsp_kernels.cu): stiffness (or, with mass, the
+// consistent mass; degrees up to 3) scatter or element matrices
+cudaError_t launch_bsp_elements(Ctx &c, const Bucket &B, ElemArgs a, int64_t count, bool mass = false);
 // B-spline solid buckets (bsp_tl.cu): total-Lagrangian tangent and / or
 // internal force (mode 0 both, 1 tangent, 2 force), small-strain internal force
 cudaError_t launch_bsp_tl(Ctx &c, const Bucket &B, ElemArgs a, int64_t count, int mode);

@@ -285,7 +285,7 @@ static cudaError_t run(Ctx &c, ElemArgs a, int64_t count) {
 template <bool MASS>
 static cudaError_t dispatch(Ctx &c, const Bucket &B, ElemArgs a, int64_t count) {
   const int ng = B.ng;
-  if (B.type == FAST_ELEM_BSP_SOLID) return MASS ? cudaErrorNotSupported : launch_bsp_elements(c, B, a, count);
+  if (B.type == FAST_ELEM_BSP_SOLID) return launch_bsp_elements(c, B, a, count, MASS);
   if (B.type == FAST_ELEM_HEX8) {
     switch (ng) {
       case 1: return run<8, 1, 64, MASS>(c, a, count);

@@ -318,8 +318,8 @@ int fast_gpu_upload_mesh(fast_gpu_ctx *c, const fast_gpu_mesh *m) {
     B.tl = bk.formulation == FAST_FORM_TOTAL_LAGRANGIAN;
     if (B.type == FAST_ELEM_BSP_SOLID) {
       const fast_gpu_patch &P = *bk.patch;
-      if (B.has_rho) {
-        c->err = "upload_mesh: B-spline solids have no mass matrix here (no density)";
+      if (B.has_rho && !bsp_tc_supported(B.pd, B.ngp[0])) {
+        c->err = "upload_mesh: B-spline solids take a density (mass matrix) for degrees (2,2,2), (3,3,3), (3,3,2)";
         return FAST_GPU_ENOTSUP;
       }
       if (!P.span) { c->err = "upload_mesh: B-spline solid bucket without element spans"; return FAST_GPU_EINVAL; }
@@ -870,10 +870,10 @@ int fast_gpu_element_matrices(fast_gpu_ctx *c, int32_t what, int32_t b, int64_t 
              "(3,3,3), (3,3,2) buckets only";
     return FAST_GPU_ENOTSUP;
   }
-  if (B.type == FAST_ELEM_BSP_SOLID && (what == FAST_ASM_MASS || (what == FAST_ASM_INTERNAL_FORCE &&
-                                                                 !bsp_tl_supported(B.pd, B.ngp[0])))) {
-    c->err = "element_matrices: B-spline solids provide the stiffness matrix (and, for the tangent kernels' "
-             "degrees, the internal force) only";
+  if (B.type == FAST_ELEM_BSP_SOLID && ((what == FAST_ASM_MASS && !bsp_tc_supported(B.pd, B.ngp[0])) ||
+                                        (what == FAST_ASM_INTERNAL_FORCE && !bsp_tl_supported(B.pd, B.ngp[0])))) {
+    c->err = "element_matrices: B-spline solids provide the mass matrix for degrees up to 3 and the internal "
+             "force for the tangent kernels' degrees";
     return FAST_GPU_ENOTSUP;
   }
   const int nd = 3 * B.nn;

@@ -309,6 +309,8 @@ cudaError_t launch_tl_at(Ctx &c, double *K, double *G, bool want_k, bool want_g,
 
 // elem_tc.cu: stiffness on the tensor cores (3xTF32, FP32 blocks), small-strain hex buckets
 bool tc_supported(const Bucket &B);
+// B-spline degrees / rules of the tensor-core kernel (and of the mass kernel)
+bool bsp_tc_supported(const int pd[3], int ngp);
 cudaError_t launch_assemble_tc(Ctx &c, float *K32);
 cudaError_t launch_element_matrices_tc(Ctx &c, int bucket, int64_t count, double *d_out_and_index);
 cudaError_t launch_tl_element(Ctx &c, int what, int bucket, int64_t count, double *d_out_and_index);

@@ -1,12 +1,12 @@
 // newmark.cu - linear Newmark time integration on the device
 // (fast_gpu_newmark), the loop of cCtrlNewmark::Solver
-// (ctrl/ctrlnewmark.cpp:79-254) without damping:
+// (ctrl/ctrlnewmark.cpp:79-254), with Rayleigh damping when asked:
 //
 //   a0 = 1/(beta dt^2), a2 = 1/(beta dt), a3 = 1/(2 beta) - 1,
 //   a6 = (1 - gamma) dt, a7 = gamma dt
 //   f = ExtLoadVector (a step load: the same f at every time), M a = f
-//   K_eff = K + a0 M
-//   each step: f_eff = f + M (a0 u + a2 v + a3 a);  K_eff u_new = f_eff
+//   K_eff = K + a0 M [+ a1 C],  C = alpha M + beta K (Rayleigh)
+//   each step: f_eff = f + M (a0 u + a2 v + a3 a) [+ C (a1 u + a4 v + a5 a)];  K_eff u_new = f_eff
 //              du = u_new - u;  a <- -a3 a + a0 du - a2 v;  v <- v + a6 a_old + a7 a
 //
 // The reference factors K_eff once (skyline Crout); here every step is a PCG
@@ -49,6 +49,27 @@ __global__ void nm_rhs(int64_t n, const double *__restrict__ q, const double *__
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     f[i] = q[i] + z[i];
     x[i] = u[i];
+  }
+}
+
+// f_eff = (q + z) + z2 (inertia, then damping terms); the solver's first iterate = u
+__global__ void nm_rhs2(int64_t n, const double *__restrict__ q, const double *__restrict__ z,
+                        const double *__restrict__ z2, const double *__restrict__ u, double *__restrict__ f,
+                        double *__restrict__ x) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    f[i] = q[i] + z[i] + z2[i];
+    x[i] = u[i];
+  }
+}
+
+// C = alpha M + beta K (cCtrlNewmark::DampingMatrix: C = 0, += alpha M, += beta K)
+__global__ void nm_rayleigh(int64_t n, double alpha, const double *__restrict__ M, double beta,
+                            const double *__restrict__ K, double *__restrict__ C) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double v = 0.0;
+    v += alpha * M[i];
+    v += beta * K[i];
+    C[i] = v;
   }
 }
 
@@ -130,12 +151,41 @@ __global__ void nm_probe_step(int nprobe, const int32_t *__restrict__ probe, con
     }                                                                         \
   } while (0)
 
+// Rayleigh damping of cCtrlNewmark (ctrl/ctrlnewmark.cpp:56-59, 150-161,
+// 262-278): C = alpha M + beta K with the reference's alpha, beta from
+// (omega1, omega2, xi1, xi2); its SoA copy, and the work vectors of C w
+struct NmDamp {
+  bool on = false;
+  double a1 = 0, a4 = 0, a5 = 0;
+  double *C = nullptr, *Cs = nullptr, *w2 = nullptr, *z2 = nullptr;
+};
+
+// f_eff = q + M (a0 u + a2 v + a3 a) [+ C (a1 u + a4 v + a5 a)], the solver's
+// first iterate = u (cCtrlNewmark::Solver, ctrl/ctrlnewmark.cpp:190-207)
+static cudaError_t step_rhs(Ctx &c, int64_t n4, double a0, double a2, double a3, const double *d_q, const double *d_u,
+                            const double *d_v, const double *d_a, double *d_w, double *d_z, const NmDamp &dm) {
+  nm_inertia<<<kNmBlocks, 256, 0, c.stream>>>(n4, a0, a2, a3, d_u, d_v, d_a, d_w);
+  c.launches++;
+  cudaError_t e = launch_spmv(c, c.d_Ms, d_w, d_z);  // z = M w
+  if (e != cudaSuccess) return e;
+  if (dm.on) {
+    nm_inertia<<<kNmBlocks, 256, 0, c.stream>>>(n4, dm.a1, dm.a4, dm.a5, d_u, d_v, d_a, dm.w2);
+    c.launches++;
+    if ((e = launch_spmv(c, dm.Cs, dm.w2, dm.z2)) != cudaSuccess) return e;  // z2 = C w2
+    nm_rhs2<<<kNmBlocks, 256, 0, c.stream>>>(n4, d_q, d_z, dm.z2, d_u, c.d_f, c.d_u);
+  } else {
+    nm_rhs<<<kNmBlocks, 256, 0, c.stream>>>(n4, d_q, d_z, d_u, c.d_f, c.d_u);
+  }
+  c.launches++;
+  return cudaGetLastError();
+}
+
 // Steps first .. steps-1 as replays of one captured step graph (the first
 // step has run directly: the preconditioner and solve copies of K_eff exist).
 static int graph_steps(fast_gpu_ctx *c, const fast_gpu_newmark_opts *o, int first, int64_t n4, double a0, double a2,
                        double a3, double a6, double a7, const double *d_q, double *d_u, double *d_v, double *d_a,
                        double *d_w, double *d_z, unsigned long long *d_max, int32_t nprobe, const int32_t *d_probe,
-                       double *d_hist, const fast_gpu_solve_report &last, fast_gpu_newmark_report &R) {
+                       double *d_hist, const NmDamp &dm, fast_gpu_newmark_report &R) {
   int rc = FAST_GPU_OK;
   int32_t *d_stats = nullptr;
   int32_t h_stats[4] = {first, R.linear_iterations, R.max_step_iterations, 0};
@@ -148,16 +198,13 @@ static int graph_steps(fast_gpu_ctx *c, const fast_gpu_newmark_opts *o, int firs
   const int chunk = lo.check_every > 0 ? lo.check_every : 16;
   const int64_t before = c->launches;
   int64_t per_step = 0;
-  (void)last;
   NMCK(cudaMalloc((void **)&d_stats, sizeof(h_stats)));
   NMCK(cudaMemcpyAsync(d_stats, h_stats, sizeof(h_stats), cudaMemcpyHostToDevice, c->stream));
   NMCK(cudaStreamSynchronize(c->stream));
   NMCK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
   {
-    nm_inertia<<<kNmBlocks, 256, 0, c->stream>>>(n4, a0, a2, a3, d_u, d_v, d_a, d_w);
-    launch_spmv(*c, c->d_Ms, d_w, d_z);  // z = M w
-    nm_rhs<<<kNmBlocks, 256, 0, c->stream>>>(n4, d_q, d_z, d_u, c->d_f, c->d_u);
-    cudaError_t e = record_pcg(*c, mixed, lo.warm_start != 0, tol, nullptr, maxit, chunk);
+    cudaError_t e = step_rhs(*c, n4, a0, a2, a3, d_q, d_u, d_v, d_a, d_w, d_z, dm);
+    if (e == cudaSuccess) e = record_pcg(*c, mixed, lo.warm_start != 0, tol, nullptr, maxit, chunk);
     nm_step_end<<<1, 1, 0, c->stream>>>(c->d_state, d_stats);
     nm_update<<<kNmBlocks, 256, 0, c->stream>>>(n4, a0, a2, a3, a6, a7, c->d_u, d_u, d_v, d_a, d_max);
     if (nprobe > 0)
@@ -167,7 +214,7 @@ static int graph_steps(fast_gpu_ctx *c, const fast_gpu_newmark_opts *o, int firs
     NMCK(e);
     NMCK(ec);
   }
-  per_step = c->launches - before + 4 + (nprobe > 0 ? 1 : 0);
+  per_step = c->launches - before + 2 + (nprobe > 0 ? 1 : 0);
   c->launches = before;
   NMCK(cudaGraphInstantiate(&ge, g, 0));
   for (int s = first; s < o->steps; s++) {
@@ -214,6 +261,11 @@ extern "C" int fast_gpu_newmark(fast_gpu_ctx *c, const double *q, const fast_gpu
   unsigned long long h_max[3] = {0, 0, 0};
   fast_gpu_solve_report lr{};
   std::vector<double> tmp;
+  NmDamp dm;
+  dm.on = o->damping != 0;
+  dm.a1 = gamma / (beta * dt);
+  dm.a4 = gamma / beta - 1.0;
+  dm.a5 = (0.5 * gamma / beta - 1.0) * dt;
   {
     cudaError_t e = cudaSuccess;
     for (double **b : {&d_q, &d_u, &d_v, &d_a, &d_w, &d_z})
@@ -246,11 +298,29 @@ extern "C" int fast_gpu_newmark(fast_gpu_ctx *c, const double *q, const fast_gpu
   nm_amax0<<<kNmBlocks, 256, 0, c->stream>>>(n4, d_a, d_max);
   c->launches++;
 
-  // K_eff = K + a0 M
+  // K_eff = K + a0 M (+ a1 C)
   rc = fast_gpu_assemble(c, FAST_ASM_STIFFNESS);
   if (rc != FAST_GPU_OK) goto done;
+  if (dm.on) {
+    const double w1 = o->omega1, w2 = o->omega2, x1 = o->xi1, x2 = o->xi2;
+    const double alphar = 2 * w1 * w2 * (x1 * w2 - x2 * w1) / (w2 * w2 - w1 * w1);
+    const double betar = 2 * (x2 * w2 - x1 * w1) / (w2 * w2 - w1 * w1);
+    const size_t nv = (size_t)9 * c->nnzb_pad;
+    NMCK(cudaMalloc((void **)&dm.C, sizeof(double) * 9 * c->nnzb));
+    NMCK(cudaMalloc((void **)&dm.Cs, sizeof(double) * nv));
+    NMCK(cudaMemsetAsync(dm.Cs, 0, sizeof(double) * nv, c->stream));  // padding stays zero
+    NMCK(cudaMalloc((void **)&dm.w2, sizeof(double) * n4));
+    NMCK(cudaMalloc((void **)&dm.z2, sizeof(double) * n4));
+    nm_rayleigh<<<kNmBlocks, 256, 0, c->stream>>>(9 * c->nnzb, alphar, c->d_M, betar, c->d_K, dm.C);
+    c->launches++;
+    NMCK(launch_to_soa(*c, dm.C, dm.Cs, nullptr));
+  }
   nm_axpy<<<kNmBlocks, 256, 0, c->stream>>>(9 * c->nnzb, a0, c->d_M, c->d_K);
   c->launches++;
+  if (dm.on) {
+    nm_axpy<<<kNmBlocks, 256, 0, c->stream>>>(9 * c->nnzb, dm.a1, dm.C, c->d_K);
+    c->launches++;
+  }
   matrix_changed(*c, FAST_ASM_STIFFNESS);
   NMCK(solve_layout(*c, FAST_ASM_MASS, false));
 
@@ -259,15 +329,11 @@ extern "C" int fast_gpu_newmark(fast_gpu_ctx *c, const double *q, const fast_gpu
       // every later step replays one captured graph: right-hand side, the
       // whole PCG (a WHILE node over chunks of iterations), update, probes
       rc = graph_steps(c, o, s, n4, a0, a2, a3, a6, a7, d_q, d_u, d_v, d_a, d_w, d_z, d_max, nprobe, d_probe, d_hist,
-                       lr, R);
+                       dm, R);
       if (rc != FAST_GPU_OK) goto done;
       break;
     }
-    nm_inertia<<<kNmBlocks, 256, 0, c->stream>>>(n4, a0, a2, a3, d_u, d_v, d_a, d_w);
-    c->launches++;
-    NMCK(launch_spmv(*c, c->d_Ms, d_w, d_z));  // z = M w
-    nm_rhs<<<kNmBlocks, 256, 0, c->stream>>>(n4, d_q, d_z, d_u, c->d_f, c->d_u);
-    c->launches++;
+    NMCK(step_rhs(*c, n4, a0, a2, a3, d_q, d_u, d_v, d_a, d_w, d_z, dm));
     rc = solve_nodes(*c, &o->lin, o->lin.warm_start != 0, &lr);
     R.linear_iterations += lr.iterations;
     if (lr.iterations > R.max_step_iterations) R.max_step_iterations = lr.iterations;
@@ -311,6 +377,8 @@ done:
     if (b) cudaFree(b);
   if (d_probe) cudaFree(d_probe);
   if (d_max) cudaFree(d_max);
+  for (double *b : {dm.C, dm.Cs, dm.w2, dm.z2})
+    if (b) cudaFree(b);
   // the K slot now holds K_eff (or M): the next stiffness assembly rebuilds K
   return rc;
 }

@@ -105,6 +105,7 @@ class Deck:
     arc_load_coeff: Optional[float] = None    # arc-length: %HEADER.ANALYSIS.ARC-LENGTH (load coefficient)
     target_iter: Optional[int] = None         # %HEADER.ANALYSIS.TARGET.ITERATIONS (reference default 1)
     newmark: tuple = (0.5, 0.25)              # Newmark: (gamma, beta), cCtrlNewmark defaults
+    rayleigh: Optional[tuple] = None          # Newmark: (omega1, omega2, xi1, xi2), %HEADER.ANALYSIS.RAYLEIGH.DAMPING
     print_step: int = 1                       # %HEADER.ANALYSIS.PRINT.STEPS
     node_labels: Optional[np.ndarray] = None  # [nnode] labels used in a .dat
     title: str = "deck"
@@ -702,6 +703,8 @@ def write_dat(deck: Deck, base: str) -> str:
     if deck.algorithm.lower() == "newmark":
         lines += ["%HEADER.ANALYSIS.TIME.STEP", _fmt(deck.time_step), ""]
         lines += ["%HEADER.ANALYSIS.NEWMARK.PARAMETERS", f"{_fmt(deck.newmark[0])} {_fmt(deck.newmark[1])}", ""]
+        if deck.rayleigh is not None:
+            lines += ["%HEADER.ANALYSIS.RAYLEIGH.DAMPING", " ".join(_fmt(v) for v in deck.rayleigh), ""]
         lines += ["%HEADER.ANALYSIS.PRINT.STEPS", str(int(deck.print_step)), ""]
     lines += ["%HEADER.OUTPUT.PRECISION", "15", ""]
     lines += ["%NODE", str(deck.num_nodes), "", "%NODE.COORD", str(deck.num_nodes)]
@@ -838,7 +841,7 @@ def read_dat(path: str) -> Deck:
         row = [int(v) for v in t[1 + 7 * k: 8 + 7 * k]]
         ords[row[0]] = tuple(row[1:4])
     if "ELEMENT.BSPLINE.SOLID" in blk or "ELEMENT.BSPLINE.SOLIDTL" in blk:
-        return _read_bsp(blk, coords, labels, l2i, fixed, mats, secs, ords, path)
+        return _read_bsp(blk, coords, labels, l2i, fixed, mats, secs, ords, path, dens)
     kind, tl, key = None, False, None
     for k, (kd, t_) in {"ELEMENT.BRICK8": ("hex8", False), "ELEMENT.BRICK20": ("hex20", False),
                         "ELEMENT.BRICK8TL": ("hex8", True), "ELEMENT.BRICK20TL": ("hex20", True)}.items():
@@ -891,7 +894,7 @@ def _analysis_header(blk) -> dict:
                 step_factor=s1("HEADER.ANALYSIS.STEP.FACTOR", 1.0, float))
 
 
-def _read_bsp(blk, coords, labels, l2i, fixed, mats, secs, ords, path) -> Deck:
+def _read_bsp(blk, coords, labels, l2i, fixed, mats, secs, ords, path, dens=None) -> Deck:
     """%PATCH (one 'bspsol' patch, 'General' knot vectors), %CONTROL.POINT.WEIGHT
     and %ELEMENT.BSPLINE.SOLID (cBspPat::Read geom/patch.cpp:1459-1484,
     cKnotVector::ReadKnot/ReadMult geom/knotvec.cpp:91-170, cShapeBsp::ReadIGA
@@ -948,11 +951,12 @@ def _read_bsp(blk, coords, labels, l2i, fixed, mats, secs, ords, path) -> Deck:
                     loc += 1
     E = np.array([mats[secs[int(s_)]][0] for s_ in a[:, 1]])
     nu = np.array([mats[secs[int(s_)]][1] for s_ in a[:, 1]])
+    rho = np.array([dens.get(secs[int(s_)], 0.0) for s_ in a[:, 1]]) if dens else None
     ordset = {ords[int(o)] for o in a[:, 2]}
     if len(ordset) != 1:
         raise ValueError("one integration order per deck is read here")
     patch = Patch(tuple(degs), knots, span, tuple(nbas), cps, weights, rational)
-    return Deck("bsp", coords, conn, E, nu, ordset.pop(), fixed, patch=patch, total_lagrangian=tl,
+    return Deck("bsp", coords, conn, E, nu, ordset.pop(), fixed, rho=rho, patch=patch, total_lagrangian=tl,
                 node_labels=labels, title=os.path.basename(path), solver_rank=_solver_rank(blk, len(coords)),
                 **_analysis_header(blk))
 

@@ -165,8 +165,10 @@ PREDICT_NONE, PREDICT_SECANT, PREDICT_CALLBACK = 0, 1, 2
 
 
 class NewmarkOpts(ctypes.Structure):
-    _fields_ = [("steps", ctypes.c_int32), ("reserved", ctypes.c_int32), ("dt", ctypes.c_double),
-                ("gamma", ctypes.c_double), ("beta", ctypes.c_double), ("lin", SolveOpts), ("mass", SolveOpts)]
+    _fields_ = [("steps", ctypes.c_int32), ("damping", ctypes.c_int32), ("dt", ctypes.c_double),
+                ("gamma", ctypes.c_double), ("beta", ctypes.c_double), ("lin", SolveOpts), ("mass", SolveOpts),
+                ("omega1", ctypes.c_double), ("omega2", ctypes.c_double), ("xi1", ctypes.c_double),
+                ("xi2", ctypes.c_double)]
 
 
 class NewmarkReport(ctypes.Structure):
@@ -416,14 +418,16 @@ class GpuSystem:
             pass
 
     def newmark(self, q, steps, dt, gamma=0.5, beta=0.25, precision=PREC_FP64, precond=PRECOND_JACOBI, tol=1e-10,
-                warm=True, mass_tol=1e-12, probes=None, check_every=0):
-        """Linear Newmark (cCtrlNewmark::Solver) under the step load q.
+                warm=True, mass_tol=1e-12, probes=None, check_every=0, rayleigh=None):
+        """Linear Newmark (cCtrlNewmark::Solver) under the step load q, with
+        Rayleigh damping when rayleigh = (omega1, omega2, xi1, xi2).
         Returns (u, v, a) at the last step, u at the probe equations per step
         ([steps][len(probes)], or None) and the report."""
         q = np.ascontiguousarray(q, dtype=np.float64)
         lin = SolveOpts(precision, precond, 0, int(bool(warm)), float(tol), 0.0, 0, int(check_every))
         mass = SolveOpts(PREC_FP64, PRECOND_JACOBI, 0, 0, float(mass_tol), 0.0, 0, 0)
-        o = NewmarkOpts(int(steps), 0, float(dt), float(gamma), float(beta), lin, mass)
+        ray = tuple(float(v) for v in rayleigh) if rayleigh is not None else (0.0, 1.0, 0.0, 0.0)
+        o = NewmarkOpts(int(steps), int(rayleigh is not None), float(dt), float(gamma), float(beta), lin, mass, *ray)
         u, v, a = np.zeros(self.neq), np.zeros(self.neq), np.zeros(self.neq)
         pr = np.ascontiguousarray(probes if probes is not None else [], dtype=np.int32)
         hist = np.zeros((steps, len(pr))) if len(pr) else None

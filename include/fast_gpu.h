@@ -53,7 +53,9 @@ extern "C" {
                                    (2,2,2) with 3 or 4 Gauss points per direction, (3,3,3) and
                                    (3,3,2) with 4, (4,2,4) and (4,2,2) with 5, (5,2,5) with 6;
                                    FAST_FORM_TOTAL_LAGRANGIAN (%ELEMENT.BSPLINE.SOLIDTL) for
-                                   (2,2,2), (3,3,3), (3,3,2) and (4,2,2); no mass; needs a patch */
+                                   (2,2,2), (3,3,3), (3,3,2) and (4,2,2); the consistent mass
+                                   (a density per element) for (2,2,2), (3,3,3), (3,3,2);
+                                   needs a patch */
 
 /* ---- element formulation --------------------------------------------- */
 #define FAST_FORM_SMALL_STRAIN       0  /* cElmParam   (%ELEMENT.BRICK8 / BRICK20)     */
@@ -464,11 +466,14 @@ int fast_gpu_mlp_gemm(fast_gpu_ctx *ctx, int32_t M, int32_t N, int32_t K, const 
  * slot (the next fast_gpu_assemble rebuilds K). */
 typedef struct {
   int32_t steps;              /* MAXIMUM.STEPS                                        */
-  int32_t reserved;
+  int32_t damping;            /* 1: RAYLEIGH.DAMPING with omega1, omega2, xi1, xi2     */
   double  dt;                 /* TIME.STEP                                            */
   double  gamma, beta;        /* NEWMARK.PARAMETERS (0.5, 0.25: average acceleration) */
   fast_gpu_solve_opts lin;    /* the step solves                                      */
   fast_gpu_solve_opts mass;   /* M a(0) = q                                           */
+  double  omega1, omega2, xi1, xi2;  /* %HEADER.ANALYSIS.RAYLEIGH.DAMPING: C = alpha M + beta K with
+                                        cCtrlNewmark::DampingMatrix's alpha, beta
+                                        (ctrl/ctrlnewmark.cpp:262-278)                */
 } fast_gpu_newmark_opts;
 
 typedef struct {

@@ -10,6 +10,9 @@ Run where the reference tree is present, with FAST_REF set to it:
     python tests/golden/make_golden.py pos      (.pos files next to the numbers they print)
     python tests/golden/make_golden.py modal    (natural frequencies and mode shapes)
     python tests/golden/make_golden.py buckling (buckling factors, modes, geometric stiffness)
+    python tests/golden/make_golden.py damped   (Newmark with Rayleigh damping)
+    python tests/golden/make_golden.py bspmass  (consistent mass of B-spline solids)
+    python tests/golden/make_golden.py variants (cCtrlNR on the learned predictor's training variants)
 
 It builds ``oracle/_ref/fastref`` (the reference's own sources compiled by
 ``oracle/Makefile``, plus a dump harness), writes each deck with
@@ -149,6 +152,43 @@ def iga_cases(tmp):
                            ("iga_thincyl_deg5", "ThinCylinderDeg5.dat", np.array([0, 40, 79]))):
         iga_reference_deck(tmp, nm, deck, keep)
     iga_tl_cases(tmp)
+
+
+def plate_variant_cases(tmp, variants=2, steps=4):
+    """The learned predictor's training data come from seeded pressure /
+    stiffness variants of one plate (fast_b200.learned.trajectories): the
+    reference's own cCtrlNR (unmodified `fast` binary) on the same variants,
+    every printed step, to check those trajectories against."""
+    base_deck = dict(nx=8, ny=8, nz=2, L=4.0, t=0.4, pressure=8.0, steps=steps, tol=1e-10, maxit=30)
+    d0 = decks.plate_tl_hex8(**base_deck)
+    out = deck_arrays(d0)
+    base0 = os.path.join(tmp, "plate_variant_base")
+    decks.write_dat(d0, base0)
+    ref = refdump.run_dump(base0, base0 + ".bin", "--no-solve", "--no-triplets")
+    out.update(ref_neq=ref["neq"], ref_node_eq=ref["node_eq"], ref_f=ref["f"])
+    us = []
+    for v in range(variants):
+        ps, E = decks.plate_variant_params(v, d0.num_elems, float(np.median(d0.E)))
+        d = decks.plate_tl_hex8(**{**base_deck, "pressure": base_deck["pressure"] * ps})
+        d.E = E
+        base = os.path.join(tmp, "plate_variant_%d" % v)
+        decks.write_dat(d, base)
+        subprocess.run([refdump.FAST, base, "-silent"], check=True, stdout=subprocess.DEVNULL)
+        us.append(decks.read_pos_displacements(base + ".pos"))
+    out.update(ref_u_steps=np.stack(us), variants=np.array(variants), steps=np.array(steps),
+               tol=np.array(base_deck["tol"]), maxit=np.array(base_deck["maxit"]))
+    np.savez_compressed(os.path.join(HERE, "nr_plate_variants.npz"), **out)
+    print("nr_plate_variants:", out["ref_u_steps"].shape)
+
+
+def bspline_mass_cases(tmp):
+    """Consistent mass of B-spline solids (cElmParam::MassMat on the
+    cShapeBspSolid basis): jittered degree-2 and degree-3 blocks with density."""
+    for name, p, n, L, seed in (("iga_p2_mass", 2, (3, 2, 2), (3.0, 2.0, 1.0), 4),
+                                ("iga_p3_mass", 3, (2, 2, 1), (2.0, 2.0, 0.5), 5)):
+        d = decks.bspline_box(p, n, L=L, jitter=0.05, seed=seed)
+        d.rho = np.full(d.num_elems, 1.3e-3)   # one material: one density
+        run_case(name, d, tmp, mass=True, triplets=False, keep_elems=np.arange(6 if p == 2 else 2))
 
 
 def iga_tl_cases(tmp):
@@ -438,9 +478,56 @@ def buckling_cases(tmp):
         print(name, lam)
 
 
+def newmark_case(tmp, name, rayleigh=None):
+    """The reference's own linear Newmark (cCtrlNewmark, unmodified `fast`
+    binary, skyline): displacements, velocities and accelerations of every
+    step of a hex20 box with density under a step load, optionally with
+    Rayleigh damping (omega1, omega2, xi1, xi2)."""
+    d = decks.box_hex20_lognormal(4, 4, 2, seed=7)
+    d.rho = np.full(d.num_elems, 1e-3)
+    d.algorithm = "newmark"
+    d.time_step = 2e-4
+    d.maxstep = 20
+    d.rayleigh = rayleigh
+    base = os.path.join(tmp, name)
+    decks.write_dat(d, base)
+    subprocess.run([refdump.FAST, base, "-silent"], check=True, stdout=subprocess.DEVNULL)
+    # read the printed steps before the harness reuses the deck's output file
+    blocks = {k: decks.read_pos_block(base + ".pos", k) for k in ("NODAL.DISPLACEMENT", "VELOCITY", "ACCELERATION")}
+    ref = refdump.run_dump(base, base + ".bin", "--no-solve", "--no-triplets")
+    out = deck_arrays(d)
+    out.update(ref_neq=ref["neq"], ref_node_eq=ref["node_eq"], ref_f=ref["f"],
+               ref_u_steps=blocks["NODAL.DISPLACEMENT"], ref_v_steps=blocks["VELOCITY"],
+               ref_a_steps=blocks["ACCELERATION"],
+               steps=np.array(d.maxstep), time_step=np.array(d.time_step),
+               gamma=np.array(d.newmark[0]), beta=np.array(d.newmark[1]))
+    if rayleigh is not None:
+        out["rayleigh"] = np.array(rayleigh, dtype=np.float64)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name + ":", out["ref_u_steps"].shape)
+
+
 def main():
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"FAST_REF={FAST_REF}", "ref"], check=True)
     tmp = tempfile.mkdtemp(prefix="golden_")
+    if len(sys.argv) > 1 and sys.argv[1] == "variants":
+        try:
+            plate_variant_cases(tmp)
+        finally:
+            shutil.rmtree(tmp, ignore_errors=True)
+        return
+    if len(sys.argv) > 1 and sys.argv[1] == "bspmass":
+        try:
+            bspline_mass_cases(tmp)
+        finally:
+            shutil.rmtree(tmp, ignore_errors=True)
+        return
+    if len(sys.argv) > 1 and sys.argv[1] == "damped":
+        try:
+            newmark_case(tmp, "nm_hex20_box_damped", rayleigh=(10.0, 200.0, 0.02, 0.05))
+        finally:
+            shutil.rmtree(tmp, ignore_errors=True)
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "buckling":
         try:
             buckling_cases(tmp)
@@ -535,28 +622,8 @@ def main():
         np.savez_compressed(os.path.join(HERE, "nr_plate_tl.npz"), **out)
         print("nr_plate_tl:", us.shape, "max |w|", np.abs(us[..., 2]).max())
 
-        # the reference's own linear Newmark (cCtrlNewmark, unmodified `fast`
-        # binary, skyline): displacements, velocities and accelerations of every
-        # step of a hex20 box with density under a step load
-        d = decks.box_hex20_lognormal(4, 4, 2, seed=7)
-        d.rho = np.full(d.num_elems, 1e-3)
-        d.algorithm = "newmark"
-        d.time_step = 2e-4
-        d.maxstep = 20
-        base = os.path.join(tmp, "nm_hex20_box")
-        decks.write_dat(d, base)
-        subprocess.run([refdump.FAST, base, "-silent"], check=True, stdout=subprocess.DEVNULL)
-        # read the printed steps before the harness reuses the deck's output file
-        blocks = {k: decks.read_pos_block(base + ".pos", k) for k in ("NODAL.DISPLACEMENT", "VELOCITY", "ACCELERATION")}
-        ref = refdump.run_dump(base, base + ".bin", "--no-solve", "--no-triplets")
-        out = deck_arrays(d)
-        out.update(ref_neq=ref["neq"], ref_node_eq=ref["node_eq"], ref_f=ref["f"],
-                   ref_u_steps=blocks["NODAL.DISPLACEMENT"], ref_v_steps=blocks["VELOCITY"],
-                   ref_a_steps=blocks["ACCELERATION"],
-                   steps=np.array(d.maxstep), time_step=np.array(d.time_step),
-                   gamma=np.array(d.newmark[0]), beta=np.array(d.newmark[1]))
-        np.savez_compressed(os.path.join(HERE, "nm_hex20_box.npz"), **out)
-        print("nm_hex20_box:", out["ref_u_steps"].shape)
+        newmark_case(tmp, "nm_hex20_box")
+        newmark_case(tmp, "nm_hex20_box_damped", rayleigh=(10.0, 200.0, 0.02, 0.05))
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
 

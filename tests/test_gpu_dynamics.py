@@ -67,3 +67,24 @@ def test_newmark_graph_replay_equals_direct_launches(precision):
         assert r1["linear_iterations"] == r0["linear_iterations"]
     assert gio.rel(h1, h0) < 1e-10 and gio.rel(u1, u0) < 1e-10
     s.close()
+
+
+@pytest.mark.parametrize("precision,tol,bound", [(gpu.PREC_FP64, 1e-13, 1e-9), (gpu.PREC_MIXED, 1e-12, 1e-8)])
+def test_damped_newmark_matches_reference(precision, tol, bound):
+    """Rayleigh damping (%HEADER.ANALYSIS.RAYLEIGH.DAMPING): C = alpha M +
+    beta K, K_eff = K + a0 M + a1 C, f_eff += C (a1 u + a4 v + a5 a), against
+    the reference binary's damped run of the same box."""
+    d, g = gio.load("nm_hex20_box_damped")
+    s = gpu.GpuSystem(0)
+    s.upload(d)
+    eq = g["ref_node_eq"].reshape(-1, 3)
+    steps = int(g["steps"])
+    (u, v, a), hist, rep = s.newmark(g["ref_f"], steps, float(g["time_step"]), float(g["gamma"]), float(g["beta"]),
+                                     precision=precision, tol=tol, probes=np.arange(s.neq),
+                                     rayleigh=tuple(g["rayleigh"]))
+    assert rep["steps_done"] == steps and rep["failed_step"] == 0
+    for k in range(steps):
+        assert gio.rel(node_field(eq, hist[k]), g["ref_u_steps"][k]) < bound, k
+    assert gio.rel(node_field(eq, v), g["ref_v_steps"][-1]) < 10 * bound
+    assert gio.rel(node_field(eq, a), g["ref_a_steps"][-1]) < 100 * bound
+    s.close()

@@ -168,3 +168,22 @@ def test_total_lagrangian_bspline_curved_beam():
                   (0.95, (-22.0535, 13.1954, 51.6480))):
         assert np.abs(tip[lf] - np.array(v)).max() <= 5e-6 * np.abs(v).max(), (lf, tip[lf])
     s.close()
+
+
+@pytest.mark.parametrize("name", ["iga_p2_mass", "iga_p3_mass"])
+def test_bspline_mass_matrices_match_reference(name):
+    """Consistent mass of B-spline solids (cElmParam::MassMat on the
+    cShapeBspSolid basis, same Gauss points as the stiffness) against the
+    reference's dumps; the assembled mass is the scatter of the same blocks."""
+    d, g = gio.load(name)
+    s = gpu.GpuSystem(0)
+    s.upload(d)
+    for k, e in enumerate(g["ref_elems"]):
+        Me = s.element_matrices(int(e), 1, what=gpu.ASM_M)[0]
+        assert gio.rel(Me, g["ref_elm_M"][k]) < TOL_K, (name, e)
+    s.assemble_mass()
+    Ml = s.lower_csr(gpu.ASM_M)
+    Ma = s.element_matrices(0, d.num_elems, what=gpu.ASM_M)
+    R = sp.tril(fo.assemble(d, Ma)).tocsr()
+    assert abs(Ml - R).max() / abs(R).max() < TOL_K
+    s.close()

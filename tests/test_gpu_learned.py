@@ -7,6 +7,7 @@ import pytest
 
 from fast_b200 import decks, gpu, learned
 from oracle import mlp_oracle as mo
+from tests import golden_io as gio
 
 pytestmark = pytest.mark.gpu
 
@@ -220,3 +221,27 @@ def test_predictor_spans_are_timed(system, small_plate, predictor):
     assert st[gpu.KERNEL_LINEAR_SOLVE][0] == r["iterations"]
     assert st[gpu.KERNEL_INTERNAL_FORCE][0] >= r["iterations"] + 15
     assert all(v[1] > 0 for v in st.values())
+
+
+def test_training_trajectories_are_the_reference_cctrlnr_paths():
+    """The predictor trains on load-step trajectories of seeded pressure /
+    stiffness variants (fast_b200.learned.trajectories, the device Newton
+    driver).  On two such variants of a small plate those trajectories are the
+    ones the reference's own cCtrlNR computes (the `fast` binary run on the
+    same variant decks, every step)."""
+    from fast_b200 import learned
+    d, g = gio.load("nr_plate_variants")
+    q = gpu.face_load_vector(d)
+    s = gpu.GpuSystem(0)
+    s.upload(d)
+    eq = d.node_eq()
+    m = eq > 0
+    got = list(learned.trajectories(s, d, q, int(g["variants"]), seed=0, steps=int(g["steps"]), tol=float(g["tol"]),
+                                    max_iter=int(g["maxit"]), precision=gpu.PREC_FP64))
+    assert len(got) == int(g["variants"])
+    for v, (lam, h, rep) in enumerate(got):
+        for k in range(h.shape[0]):
+            un = np.zeros((d.num_nodes, 3))
+            un[m] = h[k][eq[m] - 1]
+            assert gio.rel(un, g["ref_u_steps"][v][k]) < 1e-8, (v, k)
+    s.close()
