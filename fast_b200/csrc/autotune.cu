@@ -2,6 +2,13 @@
 // (fast_gpu_autotune; no reference counterpart).
 //
 // What is tuned, and why it is worth measuring:
+//   * the launch shape of the element kernels, bucket by bucket: resident
+//     CTAs per SM (fewer CTAs leave each more L1 and shared-memory bandwidth,
+//     more hide the latency of the gathers and the scatter) and, for B-spline
+//     buckets, how many CTAs share one element's node pairs (more CTAs per
+//     element fill the GPU on short colours but repeat the element's
+//     geometry work); the best point depends on the element type, its Gauss
+//     rule and the colour sizes of the mesh, so each is timed on the mesh;
 //   * lanes per block-row of the FP32 and FP64 SpMV: the best split of a row's
 //     blocks over lanes depends on the row length (27 blocks for hex8 meshes,
 //     ~57 for hex20, ~125 for degree-3 B-spline patches) and on how many rows a
@@ -58,10 +65,79 @@ cudaError_t median_ms(Ctx &c, const std::function<cudaError_t()> &launch, int re
     }                                                                                 \
   } while (0)
 
+namespace {
+
+// Times one bucket's assembly under every launch shape the kernels admit and
+// keeps the fastest (a shape replaces the default only when it is at least
+// 2 % faster).  `tc`: the tensor-core kernels (resident CTAs per SM only).
+cudaError_t tune_bucket(Ctx &c, size_t b, bool tc, double &ms_default, double &ms_best) {
+  Bucket &B = c.buckets[b];
+  auto launch = [&] {
+    return tc ? launch_assemble_tc_bucket(c, b, c.d_K32) : launch_assemble_bucket(c, b, c.d_K);
+  };
+  constexpr int kReps = 3;
+  int &ctas = tc ? B.tune_tc_ctas : B.tune_ctas;
+  ctas = 0;
+  if (!tc) B.tune_split = 0;
+  c.elem_occ = c.elem_split_max = 0;
+  cudaError_t e = median_ms(c, launch, kReps, ms_default);
+  if (e != cudaSuccess) return e;
+  const int occ = std::min(c.elem_occ, 16);
+  const int smax = (tc || B.type != FAST_ELEM_BSP_SOLID) ? 0 : std::min(c.elem_split_max, 16);
+  int best_c = 0, best_s = 0;
+  ms_best = ms_default;
+  for (int k = 1; k <= occ; k++)
+    for (int sp = 0; sp <= smax; sp++) {
+      if (k == occ && sp == 0) continue;  // the default
+      ctas = k;
+      if (!tc) B.tune_split = sp;
+      double ms = 0.0;
+      e = median_ms(c, launch, kReps, ms);
+      if (e != cudaSuccess) return e;
+      if (ms < 0.98 * ms_best) { ms_best = ms; best_c = k; best_s = sp; }
+    }
+  ctas = best_c;
+  if (!tc) B.tune_split = best_s;
+  return cudaSuccess;
+}
+
+}  // namespace
+
 extern "C" int fast_gpu_autotune(fast_gpu_ctx *c, fast_gpu_tune_report *rep) {
   if (!c || !rep) return FAST_GPU_EINVAL;
   if (!c->K_ok) { c->err = "autotune: matrix not assembled"; return FAST_GPU_ESTATE; }
   fast_gpu_tune_report R{};
+
+  // element launch shapes (the timed assemblies add into K; it is rebuilt below)
+  bool all_tc = !c->buckets.empty();
+  for (const Bucket &B : c->buckets) all_tc = all_tc && tc_supported(B);
+  if (all_tc && !c->d_K32) {
+    ATK(cudaMalloc((void **)&c->d_K32, sizeof(float) * 9 * (size_t)c->nnzb));
+    ATK(cudaMemsetAsync(c->d_K32, 0, sizeof(float) * 9 * (size_t)c->nnzb, c->stream));
+  }
+  R.elem_tc = all_tc ? 1 : 0;
+  for (size_t b = 0; b < c->buckets.size(); b++) {
+    if (c->buckets[b].tl) continue;  // tangent kernels: not tuned
+    double d64 = 0.0, t64 = 0.0, dtc = 0.0, ttc = 0.0;
+    ATK(tune_bucket(*c, b, false, d64, t64));
+    if (all_tc) ATK(tune_bucket(*c, b, true, dtc, ttc));
+    if (b < 8) {
+      const Bucket &B = c->buckets[b];
+      R.elem_buckets = (int32_t)b + 1;
+      R.elem_ctas[b] = B.tune_ctas;
+      R.elem_split[b] = B.tune_split;
+      R.elem_tc_ctas[b] = B.tune_tc_ctas;
+      R.elem_ms_default[b] = d64;
+      R.elem_ms_tuned[b] = t64;
+      R.elem_tc_ms_default[b] = dtc;
+      R.elem_tc_ms_tuned[b] = ttc;
+    }
+  }
+  ATK(cudaStreamSynchronize(c->stream));
+  {
+    const int rc = fast_gpu_assemble(c, FAST_ASM_STIFFNESS);
+    if (rc != FAST_GPU_OK) return rc;
+  }
   ATK(solve_layout(*c, FAST_ASM_STIFFNESS, true));
   const size_t n4 = 4 * (size_t)c->nnode;
   ATK(cudaMemsetAsync(c->d_p, 0x3F, sizeof(double) * n4, c->stream));  // any finite vector

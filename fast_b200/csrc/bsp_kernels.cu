@@ -307,10 +307,15 @@ static cudaError_t run_bsp(Ctx &c, ElemArgs a, int64_t count) {
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, S::bytes);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  per_sm = elem_per_sm(c, per_sm, a.ctas_per_sm);
   // as many CTAs per element as fit in one wave (a second, partial wave would
-  // double the launch time), at most one per block of NT node pairs
+  // double the launch time), at most one per block of NT node pairs; a tuned
+  // shape fixes the count instead
   const int64_t slots = (int64_t)per_sm * c.sm_count;
-  int split = (int)std::min<int64_t>((S::NP + NT - 1) / NT, std::max<int64_t>(1, slots / count));
+  const int smax = (S::NP + NT - 1) / NT;
+  if (smax > c.elem_split_max) c.elem_split_max = smax;
+  int split = (int)std::min<int64_t>(smax, std::max<int64_t>(1, slots / count));
+  if (a.split > 0) split = std::min(a.split, smax);
   int64_t grid = std::min<int64_t>(slots, count * split);
   a.ne = count;
   kern<<<(unsigned)grid, NT, S::bytes, c.stream>>>(a, split);
@@ -573,6 +578,7 @@ static cudaError_t run_bsp_big(Ctx &c, ElemArgs a, int64_t count) {
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, S::bytes);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  per_sm = elem_per_sm(c, per_sm, a.ctas_per_sm);
   const int split = (S::NP + NT * PPT - 1) / (NT * PPT);
   const int64_t slots = (int64_t)per_sm * c.sm_count;
   const int64_t grid = std::min<int64_t>(slots, count * split);

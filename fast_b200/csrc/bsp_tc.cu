@@ -390,6 +390,7 @@ cudaError_t run_bsp_tc(Ctx &c, ElemArgs a, int64_t count, float *K32) {
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   if (per_sm * S::TCOLS > 512) per_sm = 512 / S::TCOLS;
+  per_sm = elem_per_sm(c, per_sm, a.ctas_per_sm);
   int64_t grid = (int64_t)per_sm * c.sm_count;
   if (grid > count) grid = count;
   a.ne = count;

@@ -30,6 +30,9 @@ struct ElemArgs {
   const double *bas[3];       // per direction [nspan][ngp][p+1][2] {N, dN/dt}
   const double *wt;           // [nnode] control-point weights (rational patches)
   int rational;
+  // launch shape (0: default)
+  int ctas_per_sm;            // resident CTAs per SM at most
+  int split;                  // B-spline kernels: CTAs sharing one element at most
 };
 
 struct Ctx;

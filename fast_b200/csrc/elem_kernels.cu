@@ -273,7 +273,7 @@ static cudaError_t run(Ctx &c, ElemArgs a, int64_t count) {
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, S::bytes);
   if (e != cudaSuccess) return e;
-  if (per_sm < 1) per_sm = 1;
+  per_sm = elem_per_sm(c, per_sm, a.ctas_per_sm);
   int64_t grid = (int64_t)per_sm * c.sm_count;
   if (grid > count) grid = count;
   a.ne = count;
@@ -318,6 +318,8 @@ static ElemArgs base_args(Ctx &c, const Bucket &B, double *K) {
   a.w = B.d_w;
   a.K = K;
   a.status = c.d_status;
+  a.ctas_per_sm = B.tune_ctas;
+  a.split = B.tune_split;
   return a;
 }
 
@@ -376,6 +378,18 @@ cudaError_t launch_assemble(Ctx &c, int what, double *target) {
     }
   }
   if (what == FAST_ASM_STIFFNESS) return launch_tied_assemble(c, target);
+  return cudaSuccess;
+}
+
+cudaError_t launch_assemble_bucket(Ctx &c, size_t b, double *target) {
+  const Bucket &B = c.buckets[b];
+  if (B.tl) return cudaErrorNotSupported;
+  for (size_t k = 0; k + 1 < B.color_off.size(); k++) {
+    ElemArgs a = base_args(c, B, target);
+    a.offset = B.color_off[k];
+    cudaError_t e = dispatch<false>(c, B, a, B.color_off[k + 1] - B.color_off[k]);
+    if (e != cudaSuccess) return e;
+  }
   return cudaSuccess;
 }
 

@@ -337,6 +337,7 @@ cudaError_t run_tc(Ctx &c, ElemArgs a, int64_t count, float *K32) {
   if (per_sm < 1) per_sm = 1;
   // tensor-memory columns of the CTAs resident on one SM stay within its 512
   if (per_sm * S::TCOLS > 512) per_sm = 512 / S::TCOLS;
+  per_sm = elem_per_sm(c, per_sm, a.ctas_per_sm);
   int64_t grid = (int64_t)per_sm * c.sm_count;
   if (grid > count) grid = count;
   a.ne = count;
@@ -375,6 +376,7 @@ ElemArgs tc_args(Ctx &c, const Bucket &B) {
   a.dN = B.d_dN;
   a.w = B.d_w;
   a.status = c.d_status;
+  a.ctas_per_sm = B.tune_tc_ctas;
   return a;
 }
 
@@ -425,6 +427,19 @@ cudaError_t launch_assemble_tc(Ctx &c, float *K32) {
   }
   // elements with a tied node: FP64 element matrices, scattered as T^T K_e T
   return launch_tied_assemble32(c, K32);
+}
+
+cudaError_t launch_assemble_tc_bucket(Ctx &c, size_t b, float *K32) {
+  const Bucket &B = c.buckets[b];
+  if (!tc_supported(B)) return cudaErrorNotSupported;
+  for (size_t k = 0; k + 1 < B.color_off.size(); k++) {
+    ElemArgs a = tc_args(c, B);
+    a.offset = B.color_off[k];
+    const int64_t cnt = B.color_off[k + 1] - B.color_off[k];
+    cudaError_t e = B.type == FAST_ELEM_BSP_SOLID ? launch_bsp_tc(c, B, a, cnt, K32) : dispatch_tc(c, B, a, cnt, K32);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 // Element matrices of the tensor-core path, dense FP64 [count][3nn][3nn], for

@@ -62,6 +62,10 @@ struct Bucket {
   double *d_N = nullptr;           // [ng][nn] shape functions
   double *d_w = nullptr;           // [ng] Gauss weights
   int64_t ne_regular = 0;          // colour-scheduled elements; the tied ones follow in perm order
+  // launch shape chosen by fast_gpu_autotune (0: the occupancy-derived default)
+  int tune_ctas = 0;               // FP64 element kernels: resident CTAs per SM at most
+  int tune_split = 0;              // B-spline FP64 kernels: CTAs sharing one element at most
+  int tune_tc_ctas = 0;            // tensor-core element kernels: resident CTAs per SM at most
   // B-spline solids (FAST_ELEM_BSP_SOLID)
   int pd[3] = {0, 0, 0};           // degree per direction
   int rational = 0;
@@ -216,6 +220,9 @@ struct Ctx {
   // FP32 SpMV with the matrix streamed through shared memory by bulk copies
   // (spmv_f32_bulk): its row tiles, their largest value / column bytes and grid
   bool spmv32_bulk = false;
+  // widest launch shape the element kernels could take since last reset
+  // (read by the autotuner to bound its candidates)
+  int elem_occ = 0, elem_split_max = 0;
   int32_t *d_tile_row = nullptr;
   int bulk_ntiles = 0, bulk_vbytes = 0, bulk_cbytes = 0, bulk_grid = 0;
   int persist_grid = 0;           // blocks of that kernel (0: not yet sized)
@@ -251,6 +258,15 @@ struct Ctx {
   bool set_error(const std::string &m) { err = m; return false; }
 };
 
+// Resident CTAs per SM of one element-kernel launch: the occupancy `occ`,
+// capped by a tuned shape `cap` (0 = none); the widest occupancy seen is kept
+// for the autotuner.
+inline int elem_per_sm(Ctx &c, int occ, int cap) {
+  if (occ < 1) occ = 1;
+  if (occ > c.elem_occ) c.elem_occ = occ;
+  return (cap > 0 && cap < occ) ? cap : occ;
+}
+
 // pattern.cpp
 bool build_pattern(Ctx &c, const fast_gpu_mesh &m);
 
@@ -277,6 +293,8 @@ cudaError_t launch_zero_matrix(Ctx &c, double *K, bool identity_on_fixed);
 // 1 on the diagonal of every fixed DOF (the stiffness slot's convention)
 cudaError_t launch_fixed_identity(Ctx &c, double *K);
 cudaError_t launch_assemble(Ctx &c, int what, double *target);
+// the small-strain stiffness of one bucket, every colour (no tied elements)
+cudaError_t launch_assemble_bucket(Ctx &c, size_t b, double *target);
 // device face loads (face_loads.cu)
 void free_face_loads(Ctx &c);
 // tied interfaces (ties.cu)
@@ -312,6 +330,8 @@ bool tc_supported(const Bucket &B);
 // B-spline degrees / rules of the tensor-core kernel (and of the mass kernel)
 bool bsp_tc_supported(const int pd[3], int ngp);
 cudaError_t launch_assemble_tc(Ctx &c, float *K32);
+// one bucket of it, every colour (no zeroing, no tied elements)
+cudaError_t launch_assemble_tc_bucket(Ctx &c, size_t b, float *K32);
 cudaError_t launch_element_matrices_tc(Ctx &c, int bucket, int64_t count, double *d_out_and_index);
 cudaError_t launch_tl_element(Ctx &c, int what, int bucket, int64_t count, double *d_out_and_index);
 

@@ -185,8 +185,9 @@ static cudaError_t step_rhs(Ctx &c, int64_t n4, double a0, double a2, double a3,
 static int graph_steps(fast_gpu_ctx *c, const fast_gpu_newmark_opts *o, int first, int64_t n4, double a0, double a2,
                        double a3, double a6, double a7, const double *d_q, double *d_u, double *d_v, double *d_a,
                        double *d_w, double *d_z, unsigned long long *d_max, int32_t nprobe, const int32_t *d_probe,
-                       double *d_hist, const NmDamp &dm, fast_gpu_newmark_report &R) {
+                       double *d_hist, const NmDamp &dm, fast_gpu_newmark_report &R, bool *captured) {
   int rc = FAST_GPU_OK;
+  *captured = false;
   int32_t *d_stats = nullptr;
   int32_t h_stats[4] = {first, R.linear_iterations, R.max_step_iterations, 0};
   cudaGraph_t g = nullptr;
@@ -211,12 +212,19 @@ static int graph_steps(fast_gpu_ctx *c, const fast_gpu_newmark_opts *o, int firs
       nm_probe_step<<<(nprobe + 127) / 128, 128, 0, c->stream>>>(nprobe, d_probe, c->d_dof_of_eq, d_u, d_hist, d_stats);
     if (e == cudaSuccess) e = cudaGetLastError();
     cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
-    NMCK(e);
-    NMCK(ec);
+    if (e == cudaSuccess) e = ec;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&ge, g, 0);
+    if (e != cudaSuccess) {
+      // capture refused (nothing of it ran): the caller goes on kernel by kernel
+      (void)cudaGetLastError();
+      ge = nullptr;
+      c->launches = before;
+      goto done;
+    }
   }
+  *captured = true;
   per_step = c->launches - before + 2 + (nprobe > 0 ? 1 : 0);
   c->launches = before;
-  NMCK(cudaGraphInstantiate(&ge, g, 0));
   for (int s = first; s < o->steps; s++) {
     NMCK(cudaGraphLaunch(ge, c->stream));
     c->launches += per_step;   // the kernels of the chunks the loop ran are not counted
@@ -328,10 +336,11 @@ extern "C" int fast_gpu_newmark(fast_gpu_ctx *c, const double *q, const fast_gpu
     if (s == 1 && c->graph_steps) {
       // every later step replays one captured graph: right-hand side, the
       // whole PCG (a WHILE node over chunks of iterations), update, probes
+      bool captured = false;
       rc = graph_steps(c, o, s, n4, a0, a2, a3, a6, a7, d_q, d_u, d_v, d_a, d_w, d_z, d_max, nprobe, d_probe, d_hist,
-                       dm, R);
+                       dm, R, &captured);
       if (rc != FAST_GPU_OK) goto done;
-      break;
+      if (captured) break;
     }
     NMCK(step_rhs(*c, n4, a0, a2, a3, d_q, d_u, d_v, d_a, d_w, d_z, dm));
     rc = solve_nodes(*c, &o->lin, o->lin.warm_start != 0, &lr);

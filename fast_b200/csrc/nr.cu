@@ -244,6 +244,7 @@ extern "C" int fast_gpu_nr_solve(fast_gpu_ctx *c, const double *q_host, const fa
   fast_gpu_nr_report R{};
   double lam = 0.0, flen2 = 0.0, rlen2 = 0.0, glen2 = 0.0, best = 0.0;
   int64_t graph_kernels = 0;
+  bool graph_refused = false;
   std::vector<double> hq;
   const double tol = o->tol > 0 ? o->tol : 1e-5;
   if (n <= 0) return FAST_GPU_EINVAL;
@@ -379,8 +380,13 @@ extern "C" int fast_gpu_nr_solve(fast_gpu_ctx *c, const double *q_host, const fa
       NRCK(norms2(*c, w, w.r, w.f, &rlen2, &flen2));
       // every later iteration replays this one as a captured graph (the
       // solve copies and work buffers exist now)
-      if (c->graph_steps && !c->timing && !w.graph)
-        NRCK(capture_iteration(*c, w, o, o->lin.precision == FAST_PREC_MIXED, &graph_kernels));
+      if (c->graph_steps && !c->timing && !w.graph && !graph_refused &&
+          capture_iteration(*c, w, o, o->lin.precision == FAST_PREC_MIXED, &graph_kernels) != cudaSuccess) {
+        // capture refused (nothing of it ran): go on kernel by kernel
+        (void)cudaGetLastError();
+        w.graph = nullptr;
+        graph_refused = true;
+      }
       }
       R.iterations++;
       const double flen = std::sqrt(flen2), rlen = std::sqrt(rlen2);

@@ -53,6 +53,14 @@ EXPORTS = [
 ]
 OPT_PERSISTENT_MAX_NODES, OPT_SPMV_LANES_FP32, OPT_SPMV_LANES_FP64, OPT_GRAPH_STEPS = 1, 2, 3, 4
 OPT_SPMV_BULK_FP32 = 5
+OPT_ELEM_SHAPE = 6
+
+
+def elem_shape(bucket: int, ctas: int = 0, split: int = 0, tc_ctas: int = 0) -> int:
+    """The value of OPT_ELEM_SHAPE for one bucket (each field 0..255, 0 = default)."""
+    for v in (ctas, split, tc_ctas):
+        assert 0 <= v <= 255
+    return (int(bucket) << 24) | (tc_ctas << 16) | (split << 8) | ctas
 KERNEL_SPMV_FP64, KERNEL_SPMV_FP32, KERNEL_ASSEMBLE = 0, 1, 2
 KERNEL_PREDICT_NET, KERNEL_PREDICT_GALERKIN, KERNEL_INTERNAL_FORCE, KERNEL_LINEAR_SOLVE = 3, 4, 5, 6
 KERNEL_ASSEMBLE_TF32 = 7
@@ -185,14 +193,23 @@ class TuneReport(ctypes.Structure):
     _fields_ = [("lanes_fp32", ctypes.c_int32), ("lanes_fp64", ctypes.c_int32), ("ms_fp32", ctypes.c_double * 4),
                 ("ms_fp64", ctypes.c_double * 4), ("persistent_max_nodes", ctypes.c_int64),
                 ("us_iter_persistent", ctypes.c_double), ("us_iter_kernels", ctypes.c_double),
-                ("ms_fp32_bulk", ctypes.c_double * 2), ("bulk_fp32", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("ms_fp32_bulk", ctypes.c_double * 2), ("bulk_fp32", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("elem_buckets", ctypes.c_int32), ("elem_tc", ctypes.c_int32), ("elem_ctas", ctypes.c_int32 * 8),
+                ("elem_split", ctypes.c_int32 * 8), ("elem_tc_ctas", ctypes.c_int32 * 8),
+                ("elem_ms_default", ctypes.c_double * 8), ("elem_ms_tuned", ctypes.c_double * 8),
+                ("elem_tc_ms_default", ctypes.c_double * 8), ("elem_tc_ms_tuned", ctypes.c_double * 8)]
 
     def as_dict(self):
         return {"lanes_fp32": self.lanes_fp32, "lanes_fp64": self.lanes_fp64,
                 "ms_fp32_lanes_4_8_16_32": list(self.ms_fp32), "ms_fp64_lanes_4_8_16_32": list(self.ms_fp64),
                 "ms_fp32_bulk_lanes_8_16": list(self.ms_fp32_bulk), "bulk_fp32": bool(self.bulk_fp32),
                 "persistent_max_nodes": self.persistent_max_nodes, "us_iter_persistent": self.us_iter_persistent,
-                "us_iter_kernels": self.us_iter_kernels}
+                "us_iter_kernels": self.us_iter_kernels,
+                "elements": [{"ctas_per_sm": self.elem_ctas[b], "split": self.elem_split[b],
+                              "ms_default": self.elem_ms_default[b], "ms_tuned": self.elem_ms_tuned[b],
+                              "tc_ctas_per_sm": self.elem_tc_ctas[b], "tc_ms_default": self.elem_tc_ms_default[b],
+                              "tc_ms_tuned": self.elem_tc_ms_tuned[b]} for b in range(self.elem_buckets)],
+                "elements_tensor_core_timed": bool(self.elem_tc)}
 
 
 class ProblemReport(ctypes.Structure):
@@ -516,8 +533,10 @@ class GpuSystem:
         return en, avg
 
     def autotune(self) -> dict:
-        """Measure the SpMV lanes-per-row choices and the PCG iteration path on
-        this (assembled) system and keep the fastest (fast_gpu_autotune)."""
+        """Measure the element kernels' launch shapes (bucket by bucket), the
+        SpMV lanes-per-row choices and the PCG iteration path on this
+        (assembled) system and keep the fastest (fast_gpu_autotune); K is
+        re-assembled with the chosen shapes."""
         r = TuneReport()
         self._ck(self.L.fast_gpu_autotune(self.ctx, ctypes.byref(r)), "autotune")
         return r.as_dict()
@@ -551,6 +570,7 @@ class GpuSystem:
         self.deck = deck
         m, keep = _mesh_struct(deck)
         self.neq = int(m.num_eq)
+        self.nbuckets = int(m.num_buckets)
         self._ck(self.L.fast_gpu_upload_mesh(self.ctx, ctypes.byref(m)), "upload_mesh")
         self.node_eq = keep[1]
         return self

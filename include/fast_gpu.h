@@ -196,14 +196,25 @@ int         fast_gpu_synchronize(fast_gpu_ctx *ctx);
                                             as one CUDA graph, and fast_gpu_nr_solve every Newton
                                             iteration after a step's first (the PCG loop inside as a
                                             conditional WHILE node); 0: launch kernel by kernel */
+#define FAST_OPT_ELEM_SHAPE           6  /* launch shape of one bucket's element kernels, value =
+                                            bucket << 24 | tc_ctas << 16 | split << 8 | ctas (each field
+                                            0..255, 0 = the default): resident CTAs per SM of the FP64
+                                            kernels (ctas) and of the tensor-core kernels (tc_ctas), CTAs
+                                            sharing one B-spline element (split); what fast_gpu_autotune
+                                            chooses, for callers that cache its choices */
 int         fast_gpu_set_option(fast_gpu_ctx *ctx, int32_t option, int64_t value);
 
-/* Autotuner (no reference counterpart): times the SpMV of the assembled
- * stiffness for every lanes-per-row choice in both precisions (CUDA events,
- * median of 9 launches each) and, for systems small enough for the persistent
- * PCG kernel, one 64-iteration FP64 PCG chunk on each iteration path; keeps
- * the fastest choices as the context's options.  Needs an assembled K; uses
- * the solver's work vectors (call it before a solve, not during one). */
+/* Autotuner (no reference counterpart): times, per bucket of small-strain
+ * elements, the stiffness assembly for every launch shape of its element
+ * kernels (resident CTAs per SM; for B-spline buckets also the CTAs that
+ * share one element) on the FP64 path and, where every bucket has one, on the
+ * tensor-core path (CUDA events, median of 3 assemblies each), then
+ * re-assembles K with the chosen shapes; times the SpMV of the assembled
+ * stiffness for every lanes-per-row choice in both precisions (median of 9
+ * launches each) and, for systems small enough for the persistent PCG kernel,
+ * one 64-iteration FP64 PCG chunk on each iteration path; keeps the fastest
+ * choices as the context's options.  Needs an assembled K; uses the solver's
+ * work vectors (call it before a solve, not during one). */
 typedef struct {
   int32_t lanes_fp32, lanes_fp64;       /* chosen lanes per block-row                      */
   double  ms_fp32[4], ms_fp64[4];       /* per launch for 4, 8, 16, 32 lanes              */
@@ -212,6 +223,11 @@ typedef struct {
   double  ms_fp32_bulk[2];              /* bulk-staged FP32 SpMV per launch, 8 and 16 lanes per row */
   int32_t bulk_fp32;                    /* 1: the bulk-staged FP32 SpMV was kept                  */
   int32_t reserved;
+  int32_t elem_buckets;                 /* buckets reported below (the first 8; TL buckets untimed)  */
+  int32_t elem_tc;                      /* 1: the tensor-core kernels were timed too                 */
+  int32_t elem_ctas[8], elem_split[8], elem_tc_ctas[8];  /* chosen shapes (0 = default)             */
+  double  elem_ms_default[8], elem_ms_tuned[8];          /* FP64 stiffness of the bucket, per assembly */
+  double  elem_tc_ms_default[8], elem_tc_ms_tuned[8];    /* tensor-core stiffness of the bucket      */
 } fast_gpu_tune_report;
 int         fast_gpu_autotune(fast_gpu_ctx *ctx, fast_gpu_tune_report *rep);
 

@@ -16,11 +16,19 @@ def test_autotune_choices_and_solution():
     s = gpu.GpuSystem(0)
     s.upload(d)
     s.assemble()
+    K0 = s.lower_csr()
     u0, r0 = s.solve(f, tol=1e-12, precision=gpu.PREC_FP64)
     t = s.autotune()
     assert t["lanes_fp32"] in (4, 8, 16, 32) and t["lanes_fp64"] in (4, 8, 16, 32)
     assert all(v > 0 for v in t["ms_fp32_lanes_4_8_16_32"] + t["ms_fp64_lanes_4_8_16_32"])
     assert t["us_iter_persistent"] > 0 and t["us_iter_kernels"] > 0
+    # element launch shapes: one bucket (hex20), timed on both paths
+    assert len(t["elements"]) == 1 and t["elements_tensor_core_timed"]
+    el = t["elements"][0]
+    assert el["ms_default"] > 0 and 0 < el["ms_tuned"] <= el["ms_default"]
+    assert el["tc_ms_default"] > 0 and 0 < el["tc_ms_tuned"] <= el["tc_ms_default"]
+    # K is rebuilt after the timed assemblies: the same matrix, bit for bit
+    assert (s.lower_csr() != K0).nnz == 0
     for prec in (gpu.PREC_FP64, gpu.PREC_MIXED):
         u, r = s.solve(f, tol=1e-12, precision=prec)
         assert r["converged"] and gio.rel(u, u0) < 1e-9
@@ -48,4 +56,44 @@ def test_lane_option_rejects_bad_values():
     s = gpu.GpuSystem(0)
     with pytest.raises(gpu.FastGpuError):
         s.set_option(gpu.OPT_SPMV_LANES_FP32, 12)
+    s.close()
+
+
+def test_every_element_launch_shape_gives_the_same_stiffness():
+    """The tied column has hex8, hex20 and B-spline p=2 / p=3 buckets; every
+    resident-CTA cap, every B-spline split and every tensor-core cap leaves K
+    (FP64 and FP32) bit-identical, and the autotuner's choices keep it too."""
+    d = decks.tied_column()
+    s = gpu.GpuSystem(0)
+    s.upload(d)
+    s.assemble()
+    K0 = s.lower_csr()
+    s.assemble(gpu.ASM_K_TF32)
+    K0_32 = s.lower_csr(gpu.ASM_K_TF32)
+    nb = s.nbuckets
+    assert nb == 4
+    for b in range(nb):
+        for ctas, split, tc in ((1, 0, 1), (2, 1, 2), (1, 2, 1), (3, 4, 0)):
+            s.set_option(gpu.OPT_ELEM_SHAPE, gpu.elem_shape(b, ctas, split, tc))
+            s.assemble()
+            assert (s.lower_csr() != K0).nnz == 0, (b, ctas, split)
+            s.assemble(gpu.ASM_K_TF32)
+            assert (s.lower_csr(gpu.ASM_K_TF32) != K0_32).nnz == 0, (b, tc)
+        s.set_option(gpu.OPT_ELEM_SHAPE, gpu.elem_shape(b))
+    s.assemble()
+    t = s.autotune()
+    assert len(t["elements"]) == nb
+    assert (s.lower_csr() != K0).nnz == 0
+    s.assemble(gpu.ASM_K_TF32)
+    assert (s.lower_csr(gpu.ASM_K_TF32) != K0_32).nnz == 0
+    print(t["elements"])
+    s.close()
+
+
+def test_element_shape_option_rejects_a_missing_bucket():
+    d = decks.box_hex20_lognormal(2, 2, 1, seed=1)
+    s = gpu.GpuSystem(0)
+    s.upload(d)
+    with pytest.raises(gpu.FastGpuError):
+        s.set_option(gpu.OPT_ELEM_SHAPE, gpu.elem_shape(5, 1))
     s.close()
