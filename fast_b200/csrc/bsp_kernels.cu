@@ -231,14 +231,20 @@ __global__ void __launch_bounds__(NT, 1) bsp_elem_kernel(ElemArgs A, int split) 
       const int pa = spair[2 * q], pb = spair[2 * q + 1];
       // the pair's two K blocks are loaded before its Gauss-point sum, so the
       // read latency overlaps the arithmetic
+      // (blocks this element writes first, by the first-touch flags, are not read)
       double *Kab = nullptr, *Kba = nullptr;
       double oab[9], oba[9];
+      bool fab = false, fba = false;
       if (A.K) {
         Kab = A.K + (int64_t)A.slot[(e * NN + pa) * NN + pb] * 9;
         Kba = pa != pb ? A.K + (int64_t)A.slot[(e * NN + pb) * NN + pa] * 9 : nullptr;
+        fab = first_touch(A, e, pa * NN + pb);
+        fba = Kba && first_touch(A, e, pb * NN + pa);
+        if (!fab) {
 #pragma unroll
-        for (int k = 0; k < 9; k++) oab[k] = Kab[k];
-        if (Kba) {
+          for (int k = 0; k < 9; k++) oab[k] = Kab[k];
+        }
+        if (Kba && !fba) {
 #pragma unroll
           for (int k = 0; k < 9; k++) oba[k] = Kba[k];
         }
@@ -286,11 +292,14 @@ __global__ void __launch_bounds__(NT, 1) bsp_elem_kernel(ElemArgs A, int split) 
 #pragma unroll
         for (int i = 0; i < 3; i++)
 #pragma unroll
-          for (int j = 0; j < 3; j++)
-            if (!((fa >> i) & 1) && !((fb >> j) & 1)) {
-              Kab[3 * i + j] = oab[3 * i + j] + v[3 * i + j];
-              if (Kba) Kba[3 * j + i] = oba[3 * j + i] + v[3 * i + j];
-            }
+          for (int j = 0; j < 3; j++) {
+            const bool fixed = ((fa >> i) & 1) || ((fb >> j) & 1);
+            double out;
+            if (entry_value(fab, fixed, pa == pb && i == j, fab ? 0.0 : oab[3 * i + j], v[3 * i + j], out))
+              Kab[3 * i + j] = out;
+            if (Kba && entry_value(fba, fixed, false, fba ? 0.0 : oba[3 * j + i], v[3 * i + j], out))
+              Kba[3 * j + i] = out;
+          }
       }
     }
   }
@@ -553,15 +562,21 @@ __global__ void __launch_bounds__(NT, 1) bsp_big_kernel(ElemArgs A, int split) {
       if (A.K) {
         double *Kab = A.K + (int64_t)A.slot[(e * NN + a) * NN + b] * 9;
         double *Kba = a != b ? A.K + (int64_t)A.slot[(e * NN + b) * NN + a] * 9 : nullptr;
+        const bool fab = first_touch(A, e, a * NN + b), fba = Kba && first_touch(A, e, b * NN + a);
         const uint8_t fa = sfix[a], fb = sfix[b];
 #pragma unroll
         for (int i = 0; i < 3; i++)
 #pragma unroll
-          for (int j = 0; j < 3; j++)
-            if (!((fa >> i) & 1) && !((fb >> j) & 1)) {
-              Kab[3 * i + j] += v[3 * i + j];
-              if (Kba) Kba[3 * j + i] += v[3 * i + j];
+          for (int j = 0; j < 3; j++) {
+            // add where both DOFs have equations; a first write stores instead
+            const bool fixed = ((fa >> i) & 1) || ((fb >> j) & 1);
+            if (fab) Kab[3 * i + j] = fixed ? ((a == b && i == j) ? 1.0 : 0.0) : v[3 * i + j];
+            else if (!fixed) Kab[3 * i + j] += v[3 * i + j];
+            if (Kba) {
+              if (fba) Kba[3 * j + i] = fixed ? 0.0 : v[3 * i + j];
+              else if (!fixed) Kba[3 * j + i] += v[3 * i + j];
             }
+          }
       }
     }
   }

@@ -348,17 +348,28 @@ __global__ void __launch_bounds__(kBtThreads, 1) bsp_tc_kernel(ElemArgs A, float
               Ko[(3 * b + j) * ND + 3 * a + i] = v[j];
             }
           }
-          if (K32 && !((fa >> i) & 1)) {
+          if (K32) {
+            // add where both DOFs have equations; a first write (first-touch
+            // flags) stores the entry instead, 1 / 0 where a DOF is fixed
             const uint8_t fb = sfix[b];
+            const bool fai = (fa >> i) & 1;
+            const bool f1 = first_touch(A, e, a * NN + b);
             float *Kab = K32 + (int64_t)A.slot[(e * NN + a) * NN + b] * 9;
 #pragma unroll
-            for (int j = 0; j < 3; j++)
-              if (!((fb >> j) & 1)) Kab[3 * i + j] += (float)v[j];
+            for (int j = 0; j < 3; j++) {
+              const bool fixed = fai || ((fb >> j) & 1);
+              if (f1) Kab[3 * i + j] = fixed ? ((a == b && i == j) ? 1.f : 0.f) : (float)v[j];
+              else if (!fixed) Kab[3 * i + j] += (float)v[j];
+            }
             if (b != a) {
+              const bool f2 = first_touch(A, e, b * NN + a);
               float *Kba = K32 + (int64_t)A.slot[(e * NN + b) * NN + a] * 9;
 #pragma unroll
-              for (int j = 0; j < 3; j++)
-                if (!((fb >> j) & 1)) Kba[3 * j + i] += (float)v[j];
+              for (int j = 0; j < 3; j++) {
+                const bool fixed = fai || ((fb >> j) & 1);
+                if (f2) Kba[3 * j + i] = fixed ? 0.f : (float)v[j];
+                else if (!fixed) Kba[3 * j + i] += (float)v[j];
+              }
             }
           }
         }

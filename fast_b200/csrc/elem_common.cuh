@@ -33,7 +33,32 @@ struct ElemArgs {
   // launch shape (0: default)
   int ctas_per_sm;            // resident CTAs per SM at most
   int split;                  // B-spline kernels: CTAs sharing one element at most
+  // first-touch flags (stiffness assembly without a zero fill) or null:
+  // [*][fw] words, bit a*NN+b set when this element writes block (a, b) first
+  const uint32_t *first;
+  int fw;
 };
+
+// Whether colour-sorted element e writes the block of its node pair q =
+// a*NN+b first (then it stores the block outright instead of adding to it)
+__device__ __forceinline__ bool first_touch(const ElemArgs &A, int64_t e, int q) {
+  return A.first && ((__ldg(A.first + e * A.fw + (q >> 5)) >> (q & 31)) & 1u);
+}
+
+// The value a block entry (i, j) of node pair (a, b) takes: old + add where
+// both DOFs have equations; where one is fixed the entry is left alone,
+// unless this is the block's first write, which stores 1 on the diagonal of a
+// fixed DOF and 0 elsewhere.  Returns false when the entry is left alone.
+template <typename T>
+__device__ __forceinline__ bool entry_value(bool first, bool fixed, bool diag, T old, double add, T &out) {
+  if (fixed) {
+    if (!first) return false;
+    out = diag ? T(1) : T(0);
+    return true;
+  }
+  out = first ? T(add) : T(old + T(add));
+  return true;
+}
 
 struct Ctx;
 struct Bucket;

@@ -110,23 +110,30 @@ __global__ void __launch_bounds__(NT, (NT >= 128 ? 3 : 8)) elem_kernel(ElemArgs 
     for (int i = tid; i < NN; i += NT) sfix[i] = A.fix[en[i]];
 
     // early scatter loads: slots, then the current block values
+    // (a block this element writes first is not read: sSlot holds ~slot for it)
     double *Kab = nullptr, *Kba = nullptr;
     double oab[9], oba[9];
+    bool fab = false, fba = false;
     if (S::STAGE && A.K) {
       const int32_t *es = A.slot + e * NN * NN;
       for (int t = tid; t < NN * NN * 9; t += NT) {
         const int q = t / 9, k = t - 9 * q;
         const int32_t sl = es[q];
-        if (k == 0) sSlot[q] = sl;
-        cp_async8(sKo + t, A.K + (int64_t)sl * 9 + k);
+        const bool fst = first_touch(A, e, q);
+        if (k == 0) sSlot[q] = fst ? ~sl : sl;
+        if (!fst) cp_async8(sKo + t, A.K + (int64_t)sl * 9 + k);
       }
       cp_async_commit();
     } else if (A.K && tid < NP) {
       Kab = A.K + (int64_t)A.slot[(e * NN + pa) * NN + pb] * 9;
       if (pa != pb) Kba = A.K + (int64_t)A.slot[(e * NN + pb) * NN + pa] * 9;
+      fab = first_touch(A, e, pa * NN + pb);
+      fba = Kba && first_touch(A, e, pb * NN + pa);
+      if (!fab) {
 #pragma unroll
-      for (int k = 0; k < 9; k++) oab[k] = Kab[k];
-      if (Kba) {
+        for (int k = 0; k < 9; k++) oab[k] = Kab[k];
+      }
+      if (Kba && !fba) {
 #pragma unroll
         for (int k = 0; k < 9; k++) oba[k] = Kba[k];
       }
@@ -240,24 +247,32 @@ __global__ void __launch_bounds__(NT, (NT >= 128 ? 3 : 8)) elem_kernel(ElemArgs 
 #pragma unroll
         for (int i = 0; i < 3; i++)
 #pragma unroll
-          for (int j = 0; j < 3; j++)
-            if (!((fa >> i) & 1) && !((fb >> j) & 1)) {
-              Kab[3 * i + j] = oab[3 * i + j] + v[3 * i + j];
-              if (Kba) Kba[3 * j + i] = oba[3 * j + i] + v[3 * i + j];
-            }
+          for (int j = 0; j < 3; j++) {
+            const bool fixed = ((fa >> i) & 1) || ((fb >> j) & 1);
+            double out;
+            if (entry_value(fab, fixed, pa == pb && i == j, fab ? 0.0 : oab[3 * i + j], v[3 * i + j], out))
+              Kab[3 * i + j] = out;
+            if (Kba && entry_value(fba, fixed, false, fba ? 0.0 : oba[3 * j + i], v[3 * i + j], out))
+              Kba[3 * j + i] = out;
+          }
       }
     }
     if (S::STAGE && A.K) {
       cp_async_wait_all();
       __syncthreads();
-      // old + new for every entry whose two DOFs have equations
+      // old + new for every entry whose two DOFs have equations (first
+      // writes: new, and the fixed entries too)
       for (int t = tid; t < NN * NN * 9; t += NT) {
         const int q = t / 9, k = t - 9 * q;
         const int a = q / NN, b = q - NN * a, i = k / 3, j = k - 3 * i;
-        if (((sfix[a] >> i) & 1) || ((sfix[b] >> j) & 1)) continue;
+        const int32_t s0 = sSlot[q];
+        const bool fst = s0 < 0;
+        const bool fixed = ((sfix[a] >> i) & 1) || ((sfix[b] >> j) & 1);
         const double add = (a <= b) ? sV[9 * (a * NN - a * (a - 1) / 2 + (b - a)) + k]
                                     : sV[9 * (b * NN - b * (b - 1) / 2 + (a - b)) + 3 * j + i];
-        A.K[(int64_t)sSlot[q] * 9 + k] = sKo[t] + add;
+        double out;
+        if (entry_value(fst, fixed, a == b && i == j, fst ? 0.0 : sKo[t], add, out))
+          A.K[(int64_t)(fst ? ~s0 : s0) * 9 + k] = out;
       }
     }
   }
@@ -372,6 +387,10 @@ cudaError_t launch_assemble(Ctx &c, int what, double *target) {
     for (size_t k = 0; k + 1 < B.color_off.size(); k++) {
       ElemArgs a = base_args(c, B, target);
       a.offset = B.color_off[k];
+      if (what == FAST_ASM_STIFFNESS && c.use_first_touch()) {
+        a.first = B.d_first;
+        a.fw = first_words(B.nn);
+      }
       const int64_t cnt = B.color_off[k + 1] - B.color_off[k];
       cudaError_t e = (what == FAST_ASM_MASS) ? dispatch<true>(c, B, a, cnt) : dispatch<false>(c, B, a, cnt);
       if (e != cudaSuccess) return e;
@@ -387,6 +406,10 @@ cudaError_t launch_assemble_bucket(Ctx &c, size_t b, double *target) {
   for (size_t k = 0; k + 1 < B.color_off.size(); k++) {
     ElemArgs a = base_args(c, B, target);
     a.offset = B.color_off[k];
+    if (c.use_first_touch()) {
+      a.first = B.d_first;
+      a.fw = first_words(B.nn);
+    }
     cudaError_t e = dispatch<false>(c, B, a, B.color_off[k + 1] - B.color_off[k]);
     if (e != cudaSuccess) return e;
   }

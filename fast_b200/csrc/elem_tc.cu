@@ -84,9 +84,12 @@ struct TcHex {
   static constexpr int oc = oJ + al(NG * 9 * 8);              // double [NG]
   static constexpr int oSlot = oc + al(NG * 8);               // int32 [NN][NN] (bulk-copy target)
   static constexpr int oConn = oSlot + al(NN * NN * 4);       // int32 [NN] (bulk-copy target)
-  static constexpr int oFix = oConn + al(NN * 4);             // uint8 [NN]
+  static constexpr int FW = (NN * NN + 127) / 128 * 4;        // first-touch flag words (first_words)
+  static constexpr int oFirst = oConn + al(NN * 4);           // uint32 [FW] (bulk-copy target)
+  static constexpr int oFix = oFirst + FW * 4;                // uint8 [NN]
   static constexpr int oBar = oFix + al(NN);                  // 2 mbarriers
-  static_assert(odN % 16 == 0 && oSlot % 16 == 0 && oConn % 16 == 0 && oBar % 16 == 0 && OPB % 16 == 0,
+  static_assert(odN % 16 == 0 && oSlot % 16 == 0 && oConn % 16 == 0 && oFirst % 16 == 0 && oBar % 16 == 0 &&
+                    OPB % 16 == 0 && (FW * 4) % 16 == 0,
                 "bulk-copy targets and barriers on 16-byte boundaries");
   static constexpr int bytes = oBar + 16 + 1024;                        // + alignment slack
 };
@@ -112,6 +115,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) elem_tc_kernel(ElemArgs A, floa
   double *sc = reinterpret_cast<double *>(sm + S::oc);
   int32_t *sSlot = reinterpret_cast<int32_t *>(sm + S::oSlot);
   int32_t *sConn = reinterpret_cast<int32_t *>(sm + S::oConn);
+  uint32_t *sFirst = reinterpret_cast<uint32_t *>(sm + S::oFirst);
   uint8_t *sfix = sm + S::oFix;
   uint64_t *bars = reinterpret_cast<uint64_t *>(sm + S::oBar);  // [0] bulk copies, [1] MMAs
   __shared__ uint32_t tmem_base_sh;
@@ -159,9 +163,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) elem_tc_kernel(ElemArgs A, floa
     if (fail_sh) break;
     const int64_t e = A.index ? (int64_t)A.index[it] : A.offset + it;
     if (tid == 0) {
-      tc::mbar_arrive_tx(&bars[0], NN * NN * 4 + NN * 4);
+      tc::mbar_arrive_tx(&bars[0], NN * NN * 4 + NN * 4 + (A.first ? S::FW * 4 : 0));
       tc::bulk_g2s(sSlot, A.slot + e * NN * NN, NN * NN * 4, &bars[0]);
       tc::bulk_g2s(sConn, A.conn + e * NN, NN * 4, &bars[0]);
+      if (A.first) tc::bulk_g2s(sFirst, A.first + e * S::FW, S::FW * 4, &bars[0]);
     }
     if (!tc::mbar_wait(&bars[0], ph_tma, kTcWaitNs)) atomicExch(&fail_sh, 1);
     ph_tma ^= 1;
@@ -172,7 +177,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) elem_tc_kernel(ElemArgs A, floa
     if (K32) {
       for (int t = tid; t < NN * NN * 9; t += kTcThreads) {
         const int q = t / 9;
-        cp_async4(sKo + t, K32 + (int64_t)sSlot[q] * 9 + (t - 9 * q));
+        // a block this element writes first is not read
+        if (!(A.first && ((sFirst[q >> 5] >> (q & 31)) & 1u))) cp_async4(sKo + t, K32 + (int64_t)sSlot[q] * 9 + (t - 9 * q));
       }
       asm volatile("cp.async.commit_group;\n" ::);
     }
@@ -299,14 +305,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) elem_tc_kernel(ElemArgs A, floa
       asm volatile("cp.async.wait_all;\n" ::: "memory");
       __syncthreads();
       // old + new for every entry whose two DOFs have equations (block (b, a)
-      // is the transpose of (a, b))
+      // is the transpose of (a, b)); first writes store new, fixed entries too
       for (int t = tid; t < NN * NN * 9; t += kTcThreads) {
         const int q = t / 9, k = t - 9 * q;
         const int a = q / NN, b = q - NN * a, i = k / 3, j = k - 3 * i;
-        if (((sfix[a] >> i) & 1) || ((sfix[b] >> j) & 1)) continue;
+        const bool fst = A.first && ((sFirst[q >> 5] >> (q & 31)) & 1u);
+        const bool fixed = ((sfix[a] >> i) & 1) || ((sfix[b] >> j) & 1);
         const float add = (a <= b) ? sV[9 * (a * NN - a * (a - 1) / 2 + (b - a)) + k]
                                    : sV[9 * (b * NN - b * (b - 1) / 2 + (a - b)) + 3 * j + i];
-        K32[(int64_t)sSlot[q] * 9 + k] = sKo[t] + add;
+        float out;
+        if (entry_value(fst, fixed, a == b && i == j, fst ? 0.f : sKo[t], add, out)) K32[(int64_t)sSlot[q] * 9 + k] = out;
       }
     }
   }
@@ -410,16 +418,23 @@ bool tc_supported(const Bucket &B) {
 // scratch buffer the element-by-element residual reuses) and are scattered
 // into K32 by the tied-interface kernel.
 cudaError_t launch_assemble_tc(Ctx &c, float *K32) {
-  cudaError_t e = cudaMemsetAsync(K32, 0, sizeof(float) * 9 * (size_t)c.nnzb, c.stream);
-  if (e != cudaSuccess) return e;
-  zero_fixed_identity32<<<(unsigned)((c.nnode + 255) / 256), 256, 0, c.stream>>>(c.nnode, c.d_fix, c.d_diag, K32);
-  c.launches++;
+  cudaError_t e = cudaSuccess;
+  if (!c.use_first_touch()) {  // (with first-touch flags every block is stored by its first writer)
+    e = cudaMemsetAsync(K32, 0, sizeof(float) * 9 * (size_t)c.nnzb, c.stream);
+    if (e != cudaSuccess) return e;
+    zero_fixed_identity32<<<(unsigned)((c.nnode + 255) / 256), 256, 0, c.stream>>>(c.nnode, c.d_fix, c.d_diag, K32);
+    c.launches++;
+  }
   for (size_t b = 0; b < c.buckets.size(); b++) {
     const Bucket &B = c.buckets[b];
     if (!tc_supported(B)) return cudaErrorNotSupported;
     for (size_t k = 0; k + 1 < B.color_off.size(); k++) {
       ElemArgs a = tc_args(c, B);
       a.offset = B.color_off[k];
+      if (c.use_first_touch()) {
+        a.first = B.d_first;
+        a.fw = first_words(B.nn);
+      }
       const int64_t cnt = B.color_off[k + 1] - B.color_off[k];
       e = B.type == FAST_ELEM_BSP_SOLID ? launch_bsp_tc(c, B, a, cnt, K32) : dispatch_tc(c, B, a, cnt, K32);
       if (e != cudaSuccess) return e;
@@ -435,6 +450,10 @@ cudaError_t launch_assemble_tc_bucket(Ctx &c, size_t b, float *K32) {
   for (size_t k = 0; k + 1 < B.color_off.size(); k++) {
     ElemArgs a = tc_args(c, B);
     a.offset = B.color_off[k];
+    if (c.use_first_touch()) {
+      a.first = B.d_first;
+      a.fw = first_words(B.nn);
+    }
     const int64_t cnt = B.color_off[k + 1] - B.color_off[k];
     cudaError_t e = B.type == FAST_ELEM_BSP_SOLID ? launch_bsp_tc(c, B, a, cnt, K32) : dispatch_tc(c, B, a, cnt, K32);
     if (e != cudaSuccess) return e;

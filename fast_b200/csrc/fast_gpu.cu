@@ -40,7 +40,7 @@ void dfree(T *&p) {
 void free_mesh(Ctx &c) {
   c.drop_graphs();
   for (Bucket &B : c.buckets) {
-    dfree(B.d_conn); dfree(B.d_E); dfree(B.d_nu); dfree(B.d_rho); dfree(B.d_slot);
+    dfree(B.d_conn); dfree(B.d_E); dfree(B.d_nu); dfree(B.d_rho); dfree(B.d_slot); dfree(B.d_first);
     dfree(B.d_dN); dfree(B.d_N); dfree(B.d_w);
     dfree(B.d_span); dfree(B.d_bas); dfree(B.d_wt);
     dfree(B.d_tr); dfree(B.d_nptr); dfree(B.d_nent);
@@ -220,6 +220,11 @@ int fast_gpu_set_option(fast_gpu_ctx *c, int32_t option, int64_t value) {
     c->graph_steps = value != 0;
     return FAST_GPU_OK;
   }
+  if (option == FAST_OPT_ZERO_FILL) {
+    if (value != 0 && value != 1) return FAST_GPU_EINVAL;
+    c->zero_fill = value != 0;
+    return FAST_GPU_OK;
+  }
   if (option == FAST_OPT_ELEM_SHAPE) {
     const int64_t b = value >> 24;
     if (value < 0 || b >= (int64_t)c->buckets.size()) return FAST_GPU_EINVAL;
@@ -392,6 +397,11 @@ int fast_gpu_upload_mesh(fast_gpu_ctx *c, const fast_gpu_mesh *m) {
     CK(dalloc(&B.d_slot, ne * B.nn * B.nn));
     CK(cudaMemcpy(B.d_slot, B.h_slot.data(), sizeof(int32_t) * ne * B.nn * B.nn, cudaMemcpyHostToDevice));
     std::vector<int32_t>().swap(B.h_slot);
+    if (!B.h_first.empty()) {
+      CK(dalloc(&B.d_first, B.h_first.size()));
+      CK(cudaMemcpy(B.d_first, B.h_first.data(), sizeof(uint32_t) * B.h_first.size(), cudaMemcpyHostToDevice));
+      std::vector<uint32_t>().swap(B.h_first);
+    }
     CK(dalloc(&B.d_E, ne));
     CK(cudaMemcpy(B.d_E, E.data(), sizeof(double) * ne, cudaMemcpyHostToDevice));
     CK(dalloc(&B.d_nu, ne));
@@ -610,7 +620,8 @@ int fast_gpu_assemble(fast_gpu_ctx *c, int32_t what) {
   double *T = target_of(*c, what);
   CK(cudaMemsetAsync(c->d_status, 0, sizeof(int32_t), c->stream));
   if (what == FAST_ASM_STIFFNESS) c->begin_span(2);
-  CK(launch_zero_matrix(*c, T, what == FAST_ASM_STIFFNESS));
+  // (with first-touch flags every block is stored by its first writer)
+  if (!(what == FAST_ASM_STIFFNESS && c->use_first_touch())) CK(launch_zero_matrix(*c, T, what == FAST_ASM_STIFFNESS));
   CK(launch_assemble(*c, what, T));
   if (what == FAST_ASM_STIFFNESS) CK(launch_tl(*c, T, nullptr, true, false));
   if (what == FAST_ASM_STIFFNESS) c->end_span();

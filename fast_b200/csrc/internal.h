@@ -42,6 +42,10 @@ struct PcgState {
   uint32_t arrive_dir;      // blocks finished in the fused direction kernel
 };
 
+// 32-bit words of one element's first-touch flags: nn*nn bits, rows padded
+// to 16 bytes (bulk-copy size)
+inline int first_words(int nn) { return (nn * nn + 127) / 128 * 4; }
+
 struct Bucket {
   int type = 0;            // FAST_ELEM_*
   int nn = 0;              // nodes per element
@@ -62,6 +66,11 @@ struct Bucket {
   double *d_N = nullptr;           // [ng][nn] shape functions
   double *d_w = nullptr;           // [ng] Gauss weights
   int64_t ne_regular = 0;          // colour-scheduled elements; the tied ones follow in perm order
+  // first-touch flags (when Ctx::first_touch): per colour-sorted element
+  // first_words(nn) words, bit a*nn+b set when the element is the first of the
+  // stiffness assembly to write the block of its node pair (a, b)
+  std::vector<uint32_t> h_first;
+  uint32_t *d_first = nullptr;
   // launch shape chosen by fast_gpu_autotune (0: the occupancy-derived default)
   int tune_ctas = 0;               // FP64 element kernels: resident CTAs per SM at most
   int tune_split = 0;              // B-spline FP64 kernels: CTAs sharing one element at most
@@ -223,6 +232,11 @@ struct Ctx {
   // widest launch shape the element kernels could take since last reset
   // (read by the autotuner to bound its candidates)
   int elem_occ = 0, elem_split_max = 0;
+  // the stiffness assembly initialises every block by its first writer (no
+  // zero fill; set by the pattern build where that covers every block)
+  bool first_touch = false;
+  bool zero_fill = false;  // option: zero-fill K all the same
+  bool use_first_touch() const { return first_touch && !zero_fill; }
   int32_t *d_tile_row = nullptr;
   int bulk_ntiles = 0, bulk_vbytes = 0, bulk_cbytes = 0, bulk_grid = 0;
   int persist_grid = 0;           // blocks of that kernel (0: not yet sized)

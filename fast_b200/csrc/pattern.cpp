@@ -380,6 +380,42 @@ bool build_pattern(Ctx &c, const fast_gpu_mesh &m) {
       }
     }
   }
+  // 4. first-touch flags: the stiffness assembly visits buckets, then
+  // colours, in order; the first element to reach a block writes it outright
+  // (no read; fixed entries zero, 1 on the diagonal of a fixed DOF), so K
+  // needs no zero fill.  Only where every block is reached that way: no tied
+  // interfaces (their blocks come from the tied scatter), no total-Lagrangian
+  // buckets (their tangent is added by other kernels), no block left over.
+  c.first_touch = false;
+  bool eligible = c.tied.n == 0;
+  for (const Bucket &B : c.buckets) eligible = eligible && !B.tl && B.ne_regular == B.ne;
+  if (eligible) {
+    const int64_t nnzb = c.h_rowptr[nnode];
+    std::vector<uint8_t> touched((size_t)nnzb, 0);
+    for (Bucket &B : c.buckets) {
+      const int nn = B.nn;
+      const int fw = first_words(nn);
+      B.h_first.assign((size_t)B.ne * fw, 0u);
+      for (size_t k = 0; k + 1 < B.color_off.size(); k++) {
+        // elements of one colour share no node, hence no block
+#pragma omp parallel for schedule(static)
+        for (int64_t s = B.color_off[k]; s < B.color_off[k + 1]; s++) {
+          const int32_t *sl = &B.h_slot[(size_t)s * nn * nn];
+          uint32_t *f = &B.h_first[(size_t)s * fw];
+          for (int q = 0; q < nn * nn; q++)
+            if (!touched[sl[q]]) {
+              touched[sl[q]] = 1;
+              f[q >> 5] |= 1u << (q & 31);
+            }
+        }
+      }
+    }
+    bool all = true;
+    for (int64_t q = 0; q < nnzb && all; q++) all = touched[q] != 0;
+    c.first_touch = all;
+    if (!all)
+      for (Bucket &B : c.buckets) std::vector<uint32_t>().swap(B.h_first);
+  }
   c.pattern_seconds = now_s() - t0;
   return true;
 }

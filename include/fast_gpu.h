@@ -196,6 +196,10 @@ int         fast_gpu_synchronize(fast_gpu_ctx *ctx);
                                             as one CUDA graph, and fast_gpu_nr_solve every Newton
                                             iteration after a step's first (the PCG loop inside as a
                                             conditional WHILE node); 0: launch kernel by kernel */
+#define FAST_OPT_ZERO_FILL            7  /* 0 (default): where every block of the pattern is reached by an
+                                            element (no tied interfaces, no total-Lagrangian buckets), the
+                                            stiffness assembly stores each block at its first write instead
+                                            of zero-filling K and adding to it; 1: zero-fill all the same */
 #define FAST_OPT_ELEM_SHAPE           6  /* launch shape of one bucket's element kernels, value =
                                             bucket << 24 | tc_ctas << 16 | split << 8 | ctas (each field
                                             0..255, 0 = the default): resident CTAs per SM of the FP64

@@ -312,3 +312,29 @@ def test_batch_rejects_coupled_problems():
     with pytest.raises(gpu.FastGpuError) as ei:
         s.set_problems(bad)
     assert ei.value.rc == -1
+
+
+@pytest.mark.parametrize("name", ["cfg_hex8_cantilever", "cfg_hex20_lognormal_8x8x4", "iga_p2_box", "iga_p3_box"])
+def test_first_touch_assembly_equals_the_zero_filled_one(name):
+    """Without tied interfaces or total-Lagrangian buckets every block's first
+    writer stores it (no zero fill, no read of zeros); K, FP64 and the
+    tensor-core FP32 one, equals the zero-filled assembly's entry for entry."""
+    d, g = gio.load(name)
+    s = system(d)
+    n0 = s.launch_count()
+    s.assemble()
+    first_launches = s.launch_count() - n0
+    K1 = s.lower_csr()
+    s.assemble(gpu.ASM_K_TF32)
+    K1_32 = s.lower_csr(gpu.ASM_K_TF32)
+    s.set_option(gpu.OPT_ZERO_FILL, 1)
+    n0 = s.launch_count()
+    s.assemble()
+    # the zero-filled assembly adds the kernel that puts 1 on fixed diagonals
+    assert s.launch_count() - n0 == first_launches + 1
+    K0 = s.lower_csr()
+    s.assemble(gpu.ASM_K_TF32)
+    K0_32 = s.lower_csr(gpu.ASM_K_TF32)
+    assert K1.nnz == K0.nnz and abs(K1 - K0).max() == 0
+    assert abs(K1_32 - K0_32).max() == 0
+    s.close()
