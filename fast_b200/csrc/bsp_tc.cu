@@ -1,5 +1,6 @@
 // bsp_tc.cu - B-spline / NURBS solid stiffness on the tensor cores
-// (tcgen05.mma.kind::tf32, 3xTF32, FP32 accumulators in tensor memory).
+// (tcgen05.mma.kind::tf32, TF32 operands split in three, FP32 accumulators
+// in tensor memory).
 //
 // The element is that of bsp_kernels.cu (cElmParam::StiffMat,
 // elc/elmparam.cpp:539-597, on the basis of cShapeBspSolid,
@@ -10,8 +11,10 @@
 // elc/anmodel.cpp:1286-1298).  c_g keeps its sign (a left-handed patch has
 // detJ < 0, as in the reference), so the two factors differ: A rows
 // (a, i) hold c_g dN_a/dx_i, B rows (b, j) hold dN_b/dx_j, and H = A B^T is
-// formed as A_hi B_hi + A_hi B_lo + A_lo B_hi from TF32 halves (3xTF32, FP32
-// accumulation), for the mixed-precision path whose stiffness is FP32.
+// formed from TF32 parts A = A_hi + A_lo + A_mid, B likewise, as the six
+// partial products down to 2^-22 of the product, smallest first (FP32
+// accumulation: FP32-accurate entries, as the mixed-precision path whose
+// stiffness is FP32 needs; see elem_tc.cu).
 //
 // Layout.  A rows are node-major in quads, row 4a + i (i < 3; row 4a + 3 is
 // zero), so the three rows of a node sit in one warp's tensor-memory lanes;
@@ -56,7 +59,7 @@ struct BspTc {
   static constexpr int TCOLS = MT == 1 ? (NB <= 32 ? 32 : NB <= 64 ? 64 : NB <= 128 ? 128 : 256) : 512;
   static constexpr int NBUF = NCH > 1 ? 2 : 1;
   static constexpr int OA = RA * KC * 4, OB = NB * KC * 4;
-  static constexpr int OBUF = 2 * OA + 2 * OB;          // A_hi, A_lo, B_hi, B_lo
+  static constexpr int OBUF = 3 * OA + 3 * OB;          // A_hi, A_lo, A_mid, B_hi, B_lo, B_mid
   static_assert(NG1 % LPC == 0, "whole chunks");
   static_assert(MT <= 2 && NB <= 256, "at most two M tiles, N <= 256");
   static constexpr int al(int x) { return (x + 15) / 16 * 16; }
@@ -72,6 +75,7 @@ struct BspTc {
   static constexpr int oBar = oFix + al(NN);                     // NBUF mbarriers
   static constexpr int bytes = oBar + 16 + 1024;
   static_assert(OA % 16 == 0 && OB % 16 == 0, "operand sections on 16-byte boundaries");
+  static_assert(bytes <= 232448, "shared memory of one CTA");
 };
 
 template <int PR, int PS, int PT, int NG1, int LPC>
@@ -248,7 +252,8 @@ __global__ void __launch_bounds__(kBtThreads, 1) bsp_tc_kernel(ElemArgs A, float
       __syncthreads();
       if (fail_sh) break;
       uint8_t *op = sm + S::oOp + buf * S::OBUF;
-      uint8_t *aHi = op, *aLo = op + S::OA, *bHi = op + 2 * S::OA, *bLo = op + 2 * S::OA + S::OB;
+      uint8_t *aPart[3] = {op, op + S::OA, op + 2 * S::OA};
+      uint8_t *bPart[3] = {op + 3 * S::OA, op + 3 * S::OA + S::OB, op + 3 * S::OA + 2 * S::OB};
       // dN/dx, split into the TF32 operands: A row 4a+i = c_g dN_a/dx_i, B row 3b+j = dN_b/dx_j
       for (int t = tid; t < GCH * NN; t += kBtThreads) {
         const int gl = t / NN, a = t - NN * gl;
@@ -259,36 +264,36 @@ __global__ void __launch_bounds__(kBtThreads, 1) bsp_tc_kernel(ElemArgs A, float
                              J[6] * d0 + J[7] * d1 + J[8] * d2};
 #pragma unroll
         for (int i = 0; i < 3; i++) {
-          uint32_t hi, lo;
-          tc::split_tf32(cg * x[i], hi, lo);
+          uint32_t pt[3];
+          tc::split3_tf32(cg * x[i], pt[0], pt[1], pt[2]);
           const uint32_t oa = tc::kmajor_off4(4 * a + i, gl, KC);
-          *reinterpret_cast<uint32_t *>(aHi + oa) = hi;
-          *reinterpret_cast<uint32_t *>(aLo + oa) = lo;
-          tc::split_tf32(x[i], hi, lo);
+#pragma unroll
+          for (int k = 0; k < 3; k++) *reinterpret_cast<uint32_t *>(aPart[k] + oa) = pt[k];
+          tc::split3_tf32(x[i], pt[0], pt[1], pt[2]);
           const uint32_t ob = tc::kmajor_off4(3 * a + i, gl, KC);
-          *reinterpret_cast<uint32_t *>(bHi + ob) = hi;
-          *reinterpret_cast<uint32_t *>(bLo + ob) = lo;
+#pragma unroll
+          for (int k = 0; k < 3; k++) *reinterpret_cast<uint32_t *>(bPart[k] + ob) = pt[k];
         }
       }
       tc::fence_async_smem();
       __syncthreads();
       if (tid == 0) {
         tc::fence_after();
-        const uint32_t uaHi = tc::smem_u32(aHi), uaLo = tc::smem_u32(aLo);
-        const uint32_t ubHi = tc::smem_u32(bHi), ubLo = tc::smem_u32(bLo);
+        const uint32_t ua[3] = {tc::smem_u32(aPart[0]), tc::smem_u32(aPart[1]), tc::smem_u32(aPart[2])};
+        const uint32_t ub[3] = {tc::smem_u32(bPart[0]), tc::smem_u32(bPart[1]), tc::smem_u32(bPart[2])};
 #pragma unroll
         for (int t = 0; t < MT; t++) {
           const uint32_t d = tmem + t * S::TSTRIDE;
           const uint32_t toff = t * 16 * kSBO;   // 128 rows = 16 row groups
 #pragma unroll
-          for (int kk = 0; kk < KC / 8; kk++) {
-            const uint64_t dAh = tc::smem_desc(uaHi + toff + kk * 256, kLBO, kSBO);
-            const uint64_t dAl = tc::smem_desc(uaLo + toff + kk * 256, kLBO, kSBO);
-            const uint64_t dBh = tc::smem_desc(ubHi + kk * 256, kLBO, kSBO);
-            const uint64_t dBl = tc::smem_desc(ubLo + kk * 256, kLBO, kSBO);
-            tc::mma_tf32(d, dAh, dBh, kId, (ch > 0 || kk > 0) ? 1u : 0u);
-            tc::mma_tf32(d, dAh, dBl, kId, 1u);
-            tc::mma_tf32(d, dAl, dBh, kId, 1u);
+          for (int tm = 0; tm < tc::kSplitTerms; tm++) {
+            int pa_, pb_;
+            tc::split_term(tm, pa_, pb_);
+#pragma unroll
+            for (int kk = 0; kk < KC / 8; kk++)
+              tc::mma_tf32(d, tc::smem_desc(ua[pa_] + toff + kk * 256, kLBO, kSBO),
+                           tc::smem_desc(ub[pb_] + kk * 256, kLBO, kSBO), kId,
+                           (ch > 0 || tm > 0 || kk > 0) ? 1u : 0u);
           }
         }
         tc::commit(&bars[buf]);

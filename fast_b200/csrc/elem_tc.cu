@@ -12,13 +12,18 @@
 // from H and the isotropic C (cSolid::QMatrix, elc/anmodel.cpp:1286-1298):
 //     i == j : C00 H_ii + G (tr - H_ii),   i != j : C01 H_ij + G H_ji .
 //
-// This kernel serves the mixed-precision path, whose stiffness only has to be
-// as accurate as its FP32 storage: H is formed on the tensor cores from TF32
-// operands split in two, D = D_hi + D_lo, as D_hi D_hi^T + D_hi D_lo^T +
-// D_lo D_hi^T accumulated in FP32 (the "3xTF32" product; the dropped D_lo D_lo^T
-// and the split remainder are about 2^-21 of each product), and the blocks
-// are added into an FP32 block matrix.  Geometry (Jacobian, determinant,
-// inverse, dN/dx) stays in FP64.
+// This kernel serves the mixed-precision path, whose stiffness has to be as
+// accurate as its FP32 storage: the iteration's FP32 operator and the FP64
+// residual it is corrected by may differ by little more than FP32 rounding,
+// or the corrections stall on ill-conditioned systems.  H is formed on the
+// tensor cores from TF32 operands split in three, D = D_hi + D_lo + D_mid,
+// as the six partial products down to 2^-22 of the product (D_lo D_lo^T,
+// D_hi D_mid^T, D_mid D_hi^T, D_hi D_lo^T, D_lo D_hi^T, D_hi D_hi^T, smallest
+// first) accumulated in FP32; the dropped terms are below 2^-32 of it.  (The
+// two-part "3xTF32" product leaves about 2^-21, some 8x the FP32 rounding of
+// the entries, which stalled the corrections on slender and large models.)
+// The blocks are added into an FP32 block matrix.  Geometry (Jacobian,
+// determinant, inverse, dN/dx) stays in FP64.
 //
 // Per element (one CTA processes the elements of one colour in turn):
 //   1. one thread starts bulk copies (cp.async.bulk, completion on an
@@ -26,11 +31,11 @@
 //      the natural-derivative table was brought in the same way once per CTA;
 //   2. coordinates are gathered, the element's current FP32 K blocks are
 //      requested with cp.async (they arrive while the element is computed);
-//   3. Jacobians, inverses and D in FP64; D is split and written as two
+//   3. Jacobians, inverses and D in FP64; D is split and written as three
 //      K-major TF32 operands (rows (i, a), K = Gauss points padded to 8);
-//   4. one elected thread issues 3 x KP/8 tcgen05.mma (M = 128 rows, N = the
-//      rows rounded up to 16; A and B are the same operand in shared memory)
-//      and commits them to an mbarrier;
+//   4. one elected thread issues 6 x KP/8 tcgen05.mma (M = 128 rows, N = the
+//      rows rounded up to 16; A and B are operands in shared memory) and
+//      commits them to an mbarrier;
 //   5. the accumulator is read back with tcgen05.ld (one thread per row),
 //      staged as H in shared memory, turned into 3x3 blocks by one thread per
 //      node pair and added to the old blocks; the write-back is coalesced and
@@ -65,7 +70,7 @@ struct TcHex {
   static constexpr int N = (R + 15) / 16 * 16;     // accumulator columns (M = 128 needs N % 16 == 0)
   static constexpr int RP = 128;                   // operand rows held (one M tile)
   static constexpr int NP = NN * (NN + 1) / 2;
-  static constexpr int OPB = RP * KP * 4;          // bytes of one operand (hi or lo)
+  static constexpr int OPB = RP * KP * 4;          // bytes of one operand part (hi, lo or mid)
   static constexpr int TCOLS = pow2_cols(N);
   static_assert(R <= 128, "one M tile");
   static_assert(NP <= kTcThreads, "one thread per node pair");
@@ -73,8 +78,8 @@ struct TcHex {
                 "bulk-copy sizes are multiples of 16 bytes");
   // shared memory carve-up (bytes, every piece starts on a 16-byte boundary)
   static constexpr int al(int x) { return (x + 15) / 16 * 16; }
-  static constexpr int oHi = 0, oLo = oHi + OPB;
-  static constexpr int oH = oLo + OPB;                        // float [R][R]
+  static constexpr int oHi = 0, oLo = oHi + OPB, oMid = oLo + OPB;
+  static constexpr int oH = oMid + OPB;                       // float [R][R]
   static constexpr int oKo = oH + al(R * R * 4);              // float [NN*NN][9] old blocks
   static constexpr int oV = oKo + al(NN * NN * 9 * 4);        // float [NP][9] new blocks
   static constexpr int odN = oV + al(NP * 9 * 4);             // double [NG][NN][3] (bulk-copy target)
@@ -92,6 +97,7 @@ struct TcHex {
                     OPB % 16 == 0 && (FW * 4) % 16 == 0,
                 "bulk-copy targets and barriers on 16-byte boundaries");
   static constexpr int bytes = oBar + 16 + 1024;                        // + alignment slack
+  static_assert(bytes <= 232448, "shared memory of one CTA");
 };
 
 __device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
@@ -104,7 +110,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) elem_tc_kernel(ElemArgs A, floa
   constexpr int R = S::R, KP = S::KP, N = S::N;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *sm = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint8_t *opHi = sm + S::oHi, *opLo = sm + S::oLo;
+  uint8_t *opHi = sm + S::oHi, *opLo = sm + S::oLo, *opMid = sm + S::oMid;
   float *sH = reinterpret_cast<float *>(sm + S::oH);
   float *sKo = reinterpret_cast<float *>(sm + S::oKo);
   float *sV = reinterpret_cast<float *>(sm + S::oV);
@@ -131,7 +137,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) elem_tc_kernel(ElemArgs A, floa
   }
   // operands start as zeros: the K padding (Gauss points NG..KP-1) and rows
   // R..127 stay zero for every element
-  for (int i = tid; i < 2 * S::OPB / 16; i += kTcThreads) reinterpret_cast<uint4 *>(opHi)[i] = make_uint4(0, 0, 0, 0);
+  for (int i = tid; i < 3 * S::OPB / 16; i += kTcThreads) reinterpret_cast<uint4 *>(opHi)[i] = make_uint4(0, 0, 0, 0);
   if (tid == 0) {
     tc::mbar_init(&bars[0], 1);
     tc::mbar_init(&bars[1], 1);
@@ -213,7 +219,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) elem_tc_kernel(ElemArgs A, floa
       sc[g] = sqrt(fmax(sw[g] * det, 0.0));
     }
     __syncthreads();
-    // D[(i,a)][g] = sqrt(c_g) dN_a/dx_i, split into two TF32 operands
+    // D[(i,a)][g] = sqrt(c_g) dN_a/dx_i, split into three TF32 operands
     for (int t = tid; t < NG * NN; t += kTcThreads) {
       const int g = t / NN, a = t - NN * g;
       const double *J = sJ + 9 * g;
@@ -223,27 +229,27 @@ __global__ void __launch_bounds__(kTcThreads, 1) elem_tc_kernel(ElemArgs A, floa
                            sq * (J[6] * d0 + J[7] * d1 + J[8] * d2)};
 #pragma unroll
       for (int i = 0; i < 3; i++) {
-        uint32_t hi, lo;
-        tc::split_tf32(x[i], hi, lo);
+        uint32_t hi, lo, mid;
+        tc::split3_tf32(x[i], hi, lo, mid);
         const uint32_t off = tc::kmajor_off4(i * NN + a, g, KP);
         *reinterpret_cast<uint32_t *>(opHi + off) = hi;
         *reinterpret_cast<uint32_t *>(opLo + off) = lo;
+        *reinterpret_cast<uint32_t *>(opMid + off) = mid;
       }
     }
     tc::fence_async_smem();
     __syncthreads();
     if (tid == 0) {
       tc::fence_after();
-      const uint32_t aHi = tc::smem_u32(opHi), aLo = tc::smem_u32(opLo);
-      uint32_t acc = 0;
+      const uint32_t part[3] = {tc::smem_u32(opHi), tc::smem_u32(opLo), tc::smem_u32(opMid)};
 #pragma unroll
-      for (int kk = 0; kk < KP / 8; kk++) {
-        const uint64_t dHi = tc::smem_desc(aHi + kk * 256, kLBO, kSBO);
-        const uint64_t dLo = tc::smem_desc(aLo + kk * 256, kLBO, kSBO);
-        tc::mma_tf32(tmem, dHi, dHi, kId, acc);
-        acc = 1;
-        tc::mma_tf32(tmem, dHi, dLo, kId, 1);
-        tc::mma_tf32(tmem, dLo, dHi, kId, 1);
+      for (int tm = 0; tm < tc::kSplitTerms; tm++) {
+        int pa_, pb_;
+        tc::split_term(tm, pa_, pb_);
+#pragma unroll
+        for (int kk = 0; kk < KP / 8; kk++)
+          tc::mma_tf32(tmem, tc::smem_desc(part[pa_] + kk * 256, kLBO, kSBO),
+                       tc::smem_desc(part[pb_] + kk * 256, kLBO, kSBO), kId, (tm > 0 || kk > 0) ? 1u : 0u);
       }
       tc::commit(&bars[1]);
     }

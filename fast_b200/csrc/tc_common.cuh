@@ -126,6 +126,30 @@ __device__ __forceinline__ void split_tf32(double x, uint32_t &hi, uint32_t &lo)
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(rem));
 }
 
+// x (FP64) -> three TF32 parts, x ~ hi + lo + mid to about 2^-33 relative
+// (each part the round-to-nearest TF32 conversion of what the earlier parts
+// leave).  Of the nine partial products of x y the six down to 2^-22 |x y|
+// (hi hi, hi lo, lo hi, lo lo, hi mid, mid hi) bring the product to FP32
+// accuracy; the three dropped ones are below 2^-32 |x y|.
+__device__ __forceinline__ void split3_tf32(double x, uint32_t &hi, uint32_t &lo, uint32_t &mid) {
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"((float)x));
+  const double r1 = x - (double)__uint_as_float(hi);
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"((float)r1));
+  const double r2 = r1 - (double)__uint_as_float(lo);
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(mid) : "f"((float)r2));
+}
+
+// The six partial products of the three-part split as (A part, B part)
+// indices (0 hi, 1 lo, 2 mid), smallest first, so the accumulator takes the
+// small terms before the large ones
+constexpr int kSplitTerms = 6;
+__device__ __forceinline__ void split_term(int t, int &pa, int &pb) {
+  // (lo,lo) (hi,mid) (mid,hi) (hi,lo) (lo,hi) (hi,hi)
+  constexpr int A[6] = {1, 0, 2, 0, 1, 0}, B[6] = {1, 2, 0, 1, 0, 0};
+  pa = A[t];
+  pb = B[t];
+}
+
 // byte offset of element (row r, k) of a 4-byte K-major operand with kp
 // columns in the canonical layout above
 __device__ __forceinline__ uint32_t kmajor_off4(int r, int k, int kp) {

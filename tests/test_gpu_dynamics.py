@@ -53,19 +53,29 @@ def test_newmark_warm_start_saves_iterations():
 def test_newmark_graph_replay_equals_direct_launches(precision):
     """Every step after the first replays one captured CUDA graph (the PCG
     loop as a conditional WHILE node); launching kernel by kernel gives the
-    same steps."""
+    same steps.  With the same kernels on both sides (the kernel-per-step PCG
+    iteration, the same check interval) the steps are the same bits; the
+    persistent cooperative PCG kernel, which the launched steps take for small
+    systems by default, sums in another order, so that run agrees to the
+    solver tolerance instead."""
     d, g = gio.load("nm_hex20_box")
     s = gpu.GpuSystem(0)
     s.upload(d)
     args = (g["ref_f"], int(g["steps"]), float(g["time_step"]))
     probes = np.arange(s.neq)
-    (u1, _, _), h1, r1 = s.newmark(*args, precision=precision, tol=1e-12, probes=probes)
+    kw = dict(precision=precision, tol=1e-12, probes=probes, check_every=16)
+    (u_p, _, _), h_p, r_p = s.newmark(*args, **kw)            # graphs (the default)
+    s.set_option(gpu.OPT_PERSISTENT_MAX_NODES, 0)
+    (u1, _, _), h1, r1 = s.newmark(*args, **kw)
     s.set_option(gpu.OPT_GRAPH_STEPS, 0)
-    (u0, _, _), h0, r0 = s.newmark(*args, precision=precision, tol=1e-12, probes=probes)
-    assert r1["steps_done"] == r0["steps_done"] == int(g["steps"])
-    if precision == gpu.PREC_FP64:
-        assert r1["linear_iterations"] == r0["linear_iterations"]
-    assert gio.rel(h1, h0) < 1e-10 and gio.rel(u1, u0) < 1e-10
+    (u0, _, _), h0, r0 = s.newmark(*args, **kw)
+    assert r1["steps_done"] == r0["steps_done"] == r_p["steps_done"] == int(g["steps"])
+    assert r1["linear_iterations"] == r0["linear_iterations"]
+    assert np.array_equal(h1, h0) and np.array_equal(u1, u0)
+    s.set_option(gpu.OPT_PERSISTENT_MAX_NODES, 1 << 20)
+    (u2, _, _), h2, r2 = s.newmark(*args, **kw)                # launched, persistent PCG
+    assert abs(r2["linear_iterations"] - r1["linear_iterations"]) <= 2 * int(g["steps"])
+    assert gio.rel(h2, h1) < 1e-9 and gio.rel(u2, u1) < 1e-9
     s.close()
 
 
