@@ -45,6 +45,7 @@ void free_mesh(Ctx &c) {
     dfree(B.d_span); dfree(B.d_bas); dfree(B.d_wt);
     dfree(B.d_tr); dfree(B.d_nptr); dfree(B.d_nent);
   }
+  free_persist_plan(c);
   c.buckets.clear();
   free_ties(c);
   free_face_loads(c);
@@ -218,6 +219,11 @@ int fast_gpu_set_option(fast_gpu_ctx *c, int32_t option, int64_t value) {
   if (option == FAST_OPT_GRAPH_STEPS) {
     if (value != 0 && value != 1) return FAST_GPU_EINVAL;
     c->graph_steps = value != 0;
+    return FAST_GPU_OK;
+  }
+  if (option == FAST_OPT_PERSISTENT_ASSEMBLY) {
+    if (value != 0 && value != 1) return FAST_GPU_EINVAL;
+    c->persist_asm = value != 0;
     return FAST_GPU_OK;
   }
   if (option == FAST_OPT_ZERO_FILL) {

@@ -131,6 +131,8 @@ struct TieMaps {
   double *d_mw = nullptr;
 };
 
+struct PersistPlanHost;  // elem_persist.cu
+
 struct Ctx {
   int device = 0;
   cudaStream_t own_stream = nullptr;
@@ -236,6 +238,10 @@ struct Ctx {
   // zero fill; set by the pattern build where that covers every block)
   bool first_touch = false;
   bool zero_fill = false;  // option: zero-fill K all the same
+  // the tensor-core stiffness of all buckets in one persistent launch (option)
+  bool persist_asm = false;
+  PersistPlanHost *persist = nullptr;   // its work list, built on first use
+  bool persist_first = false;           // first-touch flags in the work list's arguments
   bool use_first_touch() const { return first_touch && !zero_fill; }
   int32_t *d_tile_row = nullptr;
   int bulk_ntiles = 0, bulk_vbytes = 0, bulk_cbytes = 0, bulk_grid = 0;
@@ -346,6 +352,11 @@ bool bsp_tc_supported(const int pd[3], int ngp);
 cudaError_t launch_assemble_tc(Ctx &c, float *K32);
 // one bucket of it, every colour (no zeroing, no tied elements)
 cudaError_t launch_assemble_tc_bucket(Ctx &c, size_t b, float *K32);
+// elem_persist.cu: the regular elements of every bucket into K32 in one
+// cooperative launch, and whether the mesh's buckets allow it
+cudaError_t launch_persist_elements(Ctx &c, float *K32);
+bool persist_supported(const Ctx &c);
+void free_persist_plan(Ctx &c);
 cudaError_t launch_element_matrices_tc(Ctx &c, int bucket, int64_t count, double *d_out_and_index);
 cudaError_t launch_tl_element(Ctx &c, int what, int bucket, int64_t count, double *d_out_and_index);
 

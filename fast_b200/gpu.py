@@ -55,6 +55,7 @@ OPT_PERSISTENT_MAX_NODES, OPT_SPMV_LANES_FP32, OPT_SPMV_LANES_FP64, OPT_GRAPH_ST
 OPT_SPMV_BULK_FP32 = 5
 OPT_ELEM_SHAPE = 6
 OPT_ZERO_FILL = 7
+OPT_PERSISTENT_ASSEMBLY = 8
 
 
 def elem_shape(bucket: int, ctas: int = 0, split: int = 0, tc_ctas: int = 0) -> int:

@@ -200,6 +200,11 @@ int         fast_gpu_synchronize(fast_gpu_ctx *ctx);
                                             element (no tied interfaces, no total-Lagrangian buckets), the
                                             stiffness assembly stores each block at its first write instead
                                             of zero-filling K and adding to it; 1: zero-fill all the same */
+#define FAST_OPT_PERSISTENT_ASSEMBLY  8  /* 1: FAST_ASM_STIFFNESS_TF32 integrates the elements of every
+                                            bucket in one persistent cooperative launch (colour k of
+                                            every bucket is phase k, grid barriers between phases, CTAs
+                                            take elements from a counter, heaviest kinds first); 0
+                                            (default): one launch per bucket and colour */
 #define FAST_OPT_ELEM_SHAPE           6  /* launch shape of one bucket's element kernels, value =
                                             bucket << 24 | tc_ctas << 16 | split << 8 | ctas (each field
                                             0..255, 0 = the default): resident CTAs per SM of the FP64

@@ -176,3 +176,54 @@ def test_tensor_core_path_with_tied_interfaces():
     assert rep["converged"] and rep["true_rel_residual"] < 1e-11, rep
     assert gio.rel(u, u_o) < TOL_U
     s.close()
+
+
+@pytest.mark.parametrize("which", ["tied_column", "hex20_box", "iga_p3_box", "mixed_hex"])
+def test_persistent_multi_bucket_assembly_equals_per_colour_launches(which):
+    """FAST_OPT_PERSISTENT_ASSEMBLY: the regular elements of every bucket
+    (hex8, hex20, B-spline p=2 / p=3) in one cooperative launch, colour k of
+    every bucket as phase k.  K32 is the same bits as the per-colour launches'
+    (with first-touch stores and with the zero fill), in far fewer launches,
+    and the mixed solve on it converges as before."""
+    if which == "tied_column":
+        d = decks.tied_column(hex8=(4, 4, 2), hex20=(3, 3, 2), p2=(3, 3, 2), p3=(2, 2, 2), jitter=0.05, seed=3)
+        f = decks.nodal_load_vector(d)
+    elif which == "hex20_box":
+        d = decks.box_hex20_lognormal(8, 8, 4, seed=4)
+        f = gpu.face_load_vector(d)
+    elif which == "iga_p3_box":
+        d, g = gio.load("iga_p3_box")
+        f = decks.nodal_load_vector(d)
+    else:
+        # two buckets sharing the nodes of their interface (one box, its
+        # halves on the 3x3x3 and 2x2x2 rules): their phases run one after
+        # the other
+        import dataclasses
+        d0 = decks.box_hex20_lognormal(6, 6, 4, seed=6)
+        f = gpu.face_load_vector(d0)
+        h = d0.num_elems // 2
+        nofaces = dict(face_elem=None, face_corners=None, face_q=None, face_local=None, blocks=[])
+        blk = dataclasses.replace(d0, conn=d0.conn[h:], E=d0.E[h:], nu=d0.nu[h:], ngp=(2, 2, 2), **nofaces)
+        d = dataclasses.replace(d0, conn=d0.conn[:h], E=d0.E[:h], nu=d0.nu[:h], **nofaces)
+        d.blocks = [blk]
+    s = system(d)
+    for zero_fill in (0, 1):
+        s.set_option(gpu.OPT_ZERO_FILL, zero_fill)
+        s.set_option(gpu.OPT_PERSISTENT_ASSEMBLY, 0)
+        n0 = s.launch_count()
+        s.assemble(gpu.ASM_K_TF32)
+        n_col = s.launch_count() - n0
+        K_col = s.lower_csr(gpu.ASM_K_TF32)
+        s.set_option(gpu.OPT_PERSISTENT_ASSEMBLY, 1)
+        n0 = s.launch_count()
+        s.assemble(gpu.ASM_K_TF32)
+        n_per = s.launch_count() - n0
+        K_per = s.lower_csr(gpu.ASM_K_TF32)
+        assert K_per.nnz == K_col.nnz and abs(K_per - K_col).max() == 0, (which, zero_fill)
+        assert n_per < n_col or n_col <= 3, (n_per, n_col)
+        print(which, "zero fill" if zero_fill else "first touch", "launches per colour %d, persistent %d"
+              % (n_col, n_per))
+    s.set_option(gpu.OPT_ZERO_FILL, 0)
+    u, rep = s.solve(f, tol=1e-10, precision=gpu.PREC_MIXED)
+    assert rep["converged"], rep
+    s.close()
