@@ -529,6 +529,25 @@ def tied_blocks(local, args):
                 best = (dt, u, rep)
         runs["mixed_tf32"] = best
         tc = {"assembly_ms": tms, "assembly_GB_per_s": tbytes / (tms / 1e3) / 1e9}
+        # every bucket in one persistent cooperative launch (colour phases)
+        S.set_option(gpu.OPT_PERSISTENT_ASSEMBLY, 1)
+        S.assemble(gpu.ASM_K_TF32)
+        S.synchronize()
+        n0 = S.launch_count()
+        S.kernel_timing(True)
+        for _ in range(3):
+            S.assemble(gpu.ASM_K_TF32)
+        S.synchronize()
+        pn, pms, _ = S.kernel_stats(gpu.KERNEL_ASSEMBLE_TF32)
+        S.kernel_timing(False)
+        pl = (S.launch_count() - n0) // 3
+        S.set_option(gpu.OPT_PERSISTENT_ASSEMBLY, 0)
+        n0 = S.launch_count()
+        S.assemble(gpu.ASM_K_TF32)
+        S.synchronize()
+        tc.update({"launches_per_colour": S.launch_count() - n0, "persistent_launches": pl,
+                   "persistent_assembly_ms": pms / max(1, pn),
+                   "persistent_speedup": tms / (pms / max(1, pn))})
     except Exception as ex:  # reported, not fatal
         tc = {"error": str(ex)[:300]}
     clk = clocks.stop()

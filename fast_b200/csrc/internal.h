@@ -40,6 +40,10 @@ struct PcgState {
   int32_t best;     // the last FP64 residual was the smallest so far (mixed path)
   uint32_t arrive_update;   // blocks finished in the fused update kernel (the last one commits)
   uint32_t arrive_dir;      // blocks finished in the fused direction kernel
+  int32_t restarts_left;    // mixed path: fresh starts of the recurrence still allowed after a stall
+  int32_t fresh;            // the last FP64 residual restarts the recurrence (p = z)
+  int32_t restarts;         // fresh starts taken
+  int32_t pad_;
 };
 
 // 32-bit words of one element's first-touch flags: nn*nn bits, rows padded

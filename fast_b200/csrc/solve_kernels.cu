@@ -621,24 +621,41 @@ __global__ void __launch_bounds__(256) reliable_scalar(PcgState *st, const doubl
     st->err = st->err_true;
     st->updates += 1;
     st->best = 0;
+    st->fresh = 0;
     if (!isfinite(st->err_true)) { st->done = 3; return; }
     if (st->err_true < st->tol) { st->done = 1; st->final = 1; st->best = 1; return; }
     // The FP64 residual must halve within 10 replacements (10 chunks of FP32
     // iterations) and must not grow 100x above its best; otherwise FP32
-    // iterates cannot resolve this system (cond(K) * eps_fp32 near 1).
-    if (st->updates > 1 && st->err_true > 100.0 * st->best_err) { st->done = 4; return; }
+    // iterates cannot resolve this system (cond(K) * eps_fp32 near 1).  Where
+    // the FP32 operator is not the rounded FP64 one (the tensor-core
+    // stiffness against the element-by-element FP64 residual) the search
+    // directions stop fitting the replaced residuals first: the recurrence
+    // then starts afresh from the FP64 residual (restarted iterative
+    // refinement, a fixed number of times) before stagnation is declared.
+    const bool grew = st->updates > 1 && st->err_true > 100.0 * st->best_err;
     if (st->updates == 1 || st->err_true < st->best_err) st->best = 1;
-    if (st->updates == 1 || st->err_true < 0.5 * st->best_err) {
+    if (!grew && (st->updates == 1 || st->err_true < 0.5 * st->best_err)) {
       st->best_err = st->err_true;
       st->stall = 0;
-    } else if (++st->stall >= 10) {
-      st->done = 4;
-      return;
+    } else if (grew || ++st->stall >= 10) {
+      if (st->restarts_left <= 0) { st->done = 4; return; }
+      st->restarts_left--;
+      st->restarts++;
+      st->fresh = 1;
+      st->stall = 0;
     }
     if (st->best) st->best_err = fmin(st->best_err, st->err_true);
     st->done = 0;
     st->dot0 = zr;
   }
+}
+
+// mixed path: a fresh start of the recurrence from the replaced residual
+__global__ void restart_direction(int64_t n4, const float *__restrict__ z, float *__restrict__ p,
+                                  const PcgState *__restrict__ st) {
+  if (!st->fresh) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = z[i];
 }
 
 // mixed path: remember the FP64 iterate with the smallest true residual
@@ -651,7 +668,7 @@ __global__ void keep_best(int64_t n4, const double *__restrict__ u, double *__re
 
 // mixed path start: lenf = |f| (with the reference's normaliser)
 __global__ void __launch_bounds__(256) mixed_init_scalar(PcgState *st, const double *part_ff, int nf, double tol,
-                                                         const double *tol_dev, int maxit) {
+                                                         const double *tol_dev, int maxit, int restarts) {
   if (tol_dev) tol = *tol_dev;
   __shared__ double sbuf[32];
   const double ff = sum_partials(part_ff, nf, sbuf);
@@ -660,6 +677,7 @@ __global__ void __launch_bounds__(256) mixed_init_scalar(PcgState *st, const dou
     double lenf = sqrt(ff);
     s.tol = tol;
     s.maxit = maxit;
+    s.restarts_left = restarts;
     if (lenf < tol) { s.done = 1; s.null_rhs = 1; }   // PCGSolver returns at once for a null load
     if (lenf > 10e+10) lenf = 1.0;
     s.lenf = lenf > 0.0 ? lenf : 1.0;
@@ -1586,7 +1604,8 @@ static void mixed_init(Ctx &c, bool warm, double tol, const double *tol_dev, int
   if (!warm) cudaMemsetAsync(c.d_u, 0, sizeof(double) * 4 * nn, c.stream);
   cudaMemsetAsync(c.s_x, 0, sizeof(float) * 4 * nn, c.stream);
   sumsq_kernel<<<R, 256, 0, c.stream>>>(4 * nn, c.d_f, P_D(c));
-  mixed_init_scalar<<<1, 256, 0, c.stream>>>(c.d_state, P_D(c), R, tol, tol_dev, maxit);
+  // the tensor-core stiffness may restart its recurrence (see reliable_scalar)
+  mixed_init_scalar<<<1, 256, 0, c.stream>>>(c.d_state, P_D(c), R, tol, tol_dev, maxit, c.K32_current ? 40 : 0);
   c.launches += 2;
 }
 
@@ -1610,6 +1629,10 @@ static void mixed_reliable(Ctx &c) {
   reliable_scalar<<<1, 256, 0, c.stream>>>(st, P_E(c), G, P_C(c), R);
   keep_best<<<R, 256, 0, c.stream>>>(4 * nn, c.d_u, c.d_ubest, st);
   c.launches += 4;
+  if (c.K32_current) {
+    restart_direction<<<R, 256, 0, c.stream>>>(4 * nn, c.s_z, c.s_p, st);
+    c.launches++;
+  }
 }
 
 static void mixed_chunk(Ctx &c, int k) {
