@@ -1464,19 +1464,29 @@ cudaError_t launch_pcg_batch(Ctx &c, int nprob, const int32_t *d_order, const in
 
 // k iterations of the persistent kernel; false when the system is too large
 // for it (the caller then uses the per-kernel iteration)
+// (reset_barrier false: inside a graph's loop body, where the barrier words
+// were reset before the loop and every completed launch leaves them reset)
 template <typename T>
 static cudaError_t launch_persistent(Ctx &c, const T *val, T *u, T *r, T *z, T *p, T *p2, T *w, const T *dinv,
-                                     int k) {
-  cudaError_t e = cudaMemsetAsync(c.d_bar, 0, sizeof(GridBarrier), c.stream);
+                                     int k, bool reset_barrier = true) {
+  cudaError_t e = reset_barrier ? cudaMemsetAsync(c.d_bar, 0, sizeof(GridBarrier), c.stream) : cudaSuccess;
   if (e != cudaSuccess) return e;
   int64_t nn = c.nnode;
   const int32_t *srow = c.d_srow, *scol = c.d_scol;
   PcgState *st = c.d_state;
   double *pa = c.d_partials, *pb = c.d_partials + 2048, *pc = c.d_partials + 4096;
   GridBarrier *bar = static_cast<GridBarrier *>(c.d_bar);
-  void *args[] = {&nn, &srow, &scol, &val, &u, &r, &z, &p, &p2, &w, &dinv, &st, &pa, &pb, &pc, &bar, &k};
-  e = cudaLaunchCooperativeKernel((const void *)pcg_persistent<T>, dim3(c.persist_grid), dim3(kPersistThreads), args,
-                                  0, c.stream);
+  // a cooperative launch (all blocks resident), also as a node of a captured graph
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(c.persist_grid);
+  cfg.blockDim = dim3(kPersistThreads);
+  cfg.stream = c.stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  e = cudaLaunchKernelEx(&cfg, pcg_persistent<T>, nn, srow, scol, val, u, r, z, p, p2, w, dinv, st, pa, pb, pc, bar, k);
   c.launches++;
   return e;
 }
@@ -1703,6 +1713,10 @@ cudaError_t record_pcg(Ctx &c, bool mixed, bool warm, double tol, const double *
     fp64_init(c, warm, tol, tol_dev, maxit, 0);
   }
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  // small systems iterate in the persistent cooperative kernel (as the
+  // launched solves do), a chunk per loop pass; its barrier words reset once
+  const bool persist = use_persistent(c);
+  if (persist && (e = cudaMemsetAsync(c.d_bar, 0, sizeof(GridBarrier), c.stream)) != cudaSuccess) return e;
   // the WHILE node, appended to the graph being captured on c.stream
   cudaStreamCaptureStatus cs;
   cudaGraph_t g = nullptr;
@@ -1729,11 +1743,22 @@ cudaError_t record_pcg(Ctx &c, bool mixed, bool warm, double tol, const double *
   c.stream = c.side_stream;
   e = cudaStreamBeginCaptureToGraph(c.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    if (mixed) mixed_chunk(c, chunk);
-    else fp64_chunk(c, chunk);
+    cudaError_t el = cudaSuccess;
+    if (persist && mixed) {
+      el = launch_persistent<float>(c, c.d_Ks32, c.s_x, c.s_r, c.s_z, c.s_p, c.s_p2, c.s_w, c.s_dinv, chunk, false);
+      mixed_reliable(c);
+    } else if (persist) {
+      el = launch_persistent<double>(c, c.d_Ks, c.d_u, c.d_r, c.d_z, c.d_p, c.d_p2, c.d_w, c.d_dinv,
+                                     chunk < 64 ? 64 : chunk, false);
+    } else if (mixed) {
+      mixed_chunk(c, chunk);
+    } else {
+      fp64_chunk(c, chunk);
+    }
+    if (el != cudaSuccess) (void)cudaGetLastError();
     pcg_loop_cond<<<1, 1, 0, c.stream>>>(h, c.d_state);
     c.launches++;
-    cudaError_t el = cudaGetLastError();
+    if (el == cudaSuccess) el = cudaGetLastError();
     e = cudaStreamEndCapture(c.stream, &body);
     if (e == cudaSuccess) e = el;
   }
