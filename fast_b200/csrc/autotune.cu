@@ -9,7 +9,8 @@
 //     element fill the GPU on short colours but repeat the element's
 //     geometry work); the best point depends on the element type, its Gauss
 //     rule and the colour sizes of the mesh, so each is timed on the mesh;
-//   * lanes per block-row of the FP32 and FP64 SpMV: the best split of a row's
+//   * lanes per block-row of the FP32 and FP64 SpMV (and for FP32 the
+//     bulk-staged and the cache-streaming forms): the best split of a row's
 //     blocks over lanes depends on the row length (27 blocks for hex8 meshes,
 //     ~57 for hex20, ~125 for degree-3 B-spline patches) and on how many rows a
 //     warp then covers;
@@ -143,6 +144,7 @@ extern "C" int fast_gpu_autotune(fast_gpu_ctx *c, fast_gpu_tune_report *rep) {
   ATK(cudaMemsetAsync(c->d_p, 0x3F, sizeof(double) * n4, c->stream));  // any finite vector
   ATK(cudaMemsetAsync(c->s_p, 0x3F, sizeof(float) * n4, c->stream));
   const int lanes[4] = {4, 8, 16, 32};
+  c->spmv32_bulk = c->spmv32_stream = false;   // the plain kernels first
   int best32 = c->lpr32, best64 = c->lpr64;
   double b32 = 1e300, b64 = 1e300;
   for (int i = 0; i < 4; i++) {
@@ -162,8 +164,19 @@ extern "C" int fast_gpu_autotune(fast_gpu_ctx *c, fast_gpu_tune_report *rep) {
     ATK(median_ms(*c, [&] { return launch_spmv32(*c, c->d_Ks32, c->s_p, c->s_w); }, 9, R.ms_fp32_bulk[i]));
     if (R.ms_fp32_bulk[i] < b32) { b32 = R.ms_fp32_bulk[i]; best32 = c->lpr32; bulk = true; }
   }
+  c->spmv32_bulk = false;
+  // cache-streaming matrix loads, 8 and 16 lanes
+  bool stream = false;
+  c->spmv32_stream = true;
+  for (int i = 0; i < 2; i++) {
+    c->lpr32 = i == 0 ? 8 : 16;
+    ATK(median_ms(*c, [&] { return launch_spmv32(*c, c->d_Ks32, c->s_p, c->s_w); }, 9, R.ms_fp32_stream[i]));
+    if (R.ms_fp32_stream[i] < b32) { b32 = R.ms_fp32_stream[i]; best32 = c->lpr32; stream = true; bulk = false; }
+  }
+  c->spmv32_stream = stream;
   c->spmv32_bulk = bulk;
   R.bulk_fp32 = bulk ? 1 : 0;
+  R.stream_fp32 = stream ? 1 : 0;
   c->lpr32 = best32;
   c->lpr64 = best64;
   c->drop_graphs();

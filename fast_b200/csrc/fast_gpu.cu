@@ -214,11 +214,20 @@ int fast_gpu_set_option(fast_gpu_ctx *c, int32_t option, int64_t value) {
     if (value) CK(ensure_bulk_tiles(*c));
     c->drop_graphs();
     c->spmv32_bulk = value != 0;
+    if (value) c->spmv32_stream = false;
     return FAST_GPU_OK;
   }
   if (option == FAST_OPT_GRAPH_STEPS) {
     if (value != 0 && value != 1) return FAST_GPU_EINVAL;
     c->graph_steps = value != 0;
+    return FAST_GPU_OK;
+  }
+  if (option == FAST_OPT_SPMV_STREAM_FP32) {
+    if (value != 0 && value != 1) return FAST_GPU_EINVAL;
+    CK(cudaStreamSynchronize(c->stream));
+    c->drop_graphs();
+    c->spmv32_stream = value != 0;
+    if (value) c->spmv32_bulk = false;
     return FAST_GPU_OK;
   }
   if (option == FAST_OPT_PERSISTENT_ASSEMBLY) {

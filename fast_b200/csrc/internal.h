@@ -235,6 +235,7 @@ struct Ctx {
   // FP32 SpMV with the matrix streamed through shared memory by bulk copies
   // (spmv_f32_bulk): its row tiles, their largest value / column bytes and grid
   bool spmv32_bulk = false;
+  bool spmv32_stream = false;   // FP32 SpMV with cache-streaming matrix loads (8 or 16 lanes)
   // widest launch shape the element kernels could take since last reset
   // (read by the autotuner to bound its candidates)
   int elem_occ = 0, elem_split_max = 0;

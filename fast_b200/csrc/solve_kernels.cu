@@ -141,10 +141,19 @@ __device__ __forceinline__ void spmv_row_out(int64_t row, XT a0, XT a1, XT a2, c
   }
 }
 
+// matrix loads of the FP32 SpMV: plain, or cache-streaming (evict-first:
+// the values and columns are read once per product, so the lines they take
+// are the first to go and x, gathered many times, keeps its place in L1/L2)
+template <bool CS, typename T>
+__device__ __forceinline__ T ldm(const T *p) {
+  if (CS) return __ldcs(p);
+  return *p;
+}
+
 // FP32 SpMV: LPR lanes per block-row; a lane takes 4 blocks per trip (one
 // int4 of columns, nine float4 of values, four float4 gathers of x): 14
-// independent 16-byte loads in flight per lane.
-template <int MODE, int LPR>
+// independent 16-byte loads in flight per lane.  CS: matrix loads streamed.
+template <int MODE, int LPR, bool CS = false>
 __global__ void __launch_bounds__(kSpmvThreads, 4)
 spmv_f32(int64_t nrows, const int32_t *__restrict__ srow, const int32_t *__restrict__ scol,
          const float *__restrict__ val, const float *__restrict__ x, const float *__restrict__ b,
@@ -168,10 +177,10 @@ spmv_f32(int64_t nrows, const int32_t *__restrict__ srow, const int32_t *__restr
     const float *__restrict__ vr = val + 9 * (int64_t)s0;
     float a0 = 0.f, a1 = 0.f, a2 = 0.f;
     for (int j = 4 * q; j < nbp; j += 4 * LPR) {
-      const int4 c = *reinterpret_cast<const int4 *>(scol + s0 + j);
+      const int4 c = ldm<CS>(reinterpret_cast<const int4 *>(scol + s0 + j));
       float4 v[9];
 #pragma unroll
-      for (int k = 0; k < 9; k++) v[k] = *reinterpret_cast<const float4 *>(vr + k * nbp + j);
+      for (int k = 0; k < 9; k++) v[k] = ldm<CS>(reinterpret_cast<const float4 *>(vr + k * nbp + j));
       const float4 xa = x4[c.x], xb = x4[c.y], xc = x4[c.z], xd = x4[c.w];
       a0 += v[0].x * xa.x + v[1].x * xa.y + v[2].x * xa.z + v[0].y * xb.x + v[1].y * xb.y + v[2].y * xb.z +
             v[0].z * xc.x + v[1].z * xc.y + v[2].z * xc.z + v[0].w * xd.x + v[1].w * xd.y + v[2].w * xd.z;
@@ -865,6 +874,13 @@ static void spmv32_go(const Ctx &c, int G, int64_t nn, const float *Ks, const fl
       spmv_f32_bulk<8><<<c.bulk_grid, kBulkThreads, smem, c.stream>>>(c.bulk_ntiles, c.d_tile_row, c.d_srow, c.d_scol, Ks,
                                                                        x, y, part, skip, c.d_status, c.bulk_vbytes,
                                                                        c.bulk_cbytes);
+    return;
+  }
+  if (c.spmv32_stream) {
+    if (c.lpr32 >= 16)
+      spmv_f32<0, 16, true><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, Ks, x, nullptr, y, part, skip);
+    else
+      spmv_f32<0, 8, true><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol, Ks, x, nullptr, y, part, skip);
     return;
   }
   switch (c.lpr32) {

@@ -56,6 +56,7 @@ OPT_SPMV_BULK_FP32 = 5
 OPT_ELEM_SHAPE = 6
 OPT_ZERO_FILL = 7
 OPT_PERSISTENT_ASSEMBLY = 8
+OPT_SPMV_STREAM_FP32 = 9
 
 
 def elem_shape(bucket: int, ctas: int = 0, split: int = 0, tc_ctas: int = 0) -> int:
@@ -199,7 +200,8 @@ class TuneReport(ctypes.Structure):
                 ("elem_buckets", ctypes.c_int32), ("elem_tc", ctypes.c_int32), ("elem_ctas", ctypes.c_int32 * 8),
                 ("elem_split", ctypes.c_int32 * 8), ("elem_tc_ctas", ctypes.c_int32 * 8),
                 ("elem_ms_default", ctypes.c_double * 8), ("elem_ms_tuned", ctypes.c_double * 8),
-                ("elem_tc_ms_default", ctypes.c_double * 8), ("elem_tc_ms_tuned", ctypes.c_double * 8)]
+                ("elem_tc_ms_default", ctypes.c_double * 8), ("elem_tc_ms_tuned", ctypes.c_double * 8),
+                ("ms_fp32_stream", ctypes.c_double * 2), ("stream_fp32", ctypes.c_int32), ("reserved2", ctypes.c_int32)]
 
     def as_dict(self):
         return {"lanes_fp32": self.lanes_fp32, "lanes_fp64": self.lanes_fp64,
@@ -211,7 +213,8 @@ class TuneReport(ctypes.Structure):
                               "ms_default": self.elem_ms_default[b], "ms_tuned": self.elem_ms_tuned[b],
                               "tc_ctas_per_sm": self.elem_tc_ctas[b], "tc_ms_default": self.elem_tc_ms_default[b],
                               "tc_ms_tuned": self.elem_tc_ms_tuned[b]} for b in range(self.elem_buckets)],
-                "elements_tensor_core_timed": bool(self.elem_tc)}
+                "elements_tensor_core_timed": bool(self.elem_tc),
+                "ms_fp32_stream_lanes_8_16": list(self.ms_fp32_stream), "stream_fp32": bool(self.stream_fp32)}
 
 
 class ProblemReport(ctypes.Structure):

@@ -200,6 +200,9 @@ int         fast_gpu_synchronize(fast_gpu_ctx *ctx);
                                             element (no tied interfaces, no total-Lagrangian buckets), the
                                             stiffness assembly stores each block at its first write instead
                                             of zero-filling K and adding to it; 1: zero-fill all the same */
+#define FAST_OPT_SPMV_STREAM_FP32     9  /* 1: the FP32 SpMV loads the matrix with cache-streaming (evict-
+                                            first) loads, 8 or 16 lanes per row; 0 (default until
+                                            fast_gpu_autotune measures it): plain loads */
 #define FAST_OPT_PERSISTENT_ASSEMBLY  8  /* 1: FAST_ASM_STIFFNESS_TF32 integrates the elements of every
                                             bucket in one persistent cooperative launch (colour k of
                                             every bucket is phase k, grid barriers between phases, CTAs
@@ -237,6 +240,9 @@ typedef struct {
   int32_t elem_ctas[8], elem_split[8], elem_tc_ctas[8];  /* chosen shapes (0 = default)             */
   double  elem_ms_default[8], elem_ms_tuned[8];          /* FP64 stiffness of the bucket, per assembly */
   double  elem_tc_ms_default[8], elem_tc_ms_tuned[8];    /* tensor-core stiffness of the bucket      */
+  double  ms_fp32_stream[2];            /* FP32 SpMV with cache-streaming matrix loads, 8 and 16 lanes   */
+  int32_t stream_fp32;                  /* 1: the cache-streaming FP32 SpMV was kept                      */
+  int32_t reserved2;
 } fast_gpu_tune_report;
 int         fast_gpu_autotune(fast_gpu_ctx *ctx, fast_gpu_tune_report *rep);
 

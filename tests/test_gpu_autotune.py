@@ -97,3 +97,23 @@ def test_element_shape_option_rejects_a_missing_bucket():
     with pytest.raises(gpu.FastGpuError):
         s.set_option(gpu.OPT_ELEM_SHAPE, gpu.elem_shape(5, 1))
     s.close()
+
+
+@pytest.mark.parametrize("lanes", [8, 16])
+def test_streaming_spmv_gives_the_same_bits(lanes):
+    """FAST_OPT_SPMV_STREAM_FP32: the FP32 SpMV with cache-streaming matrix
+    loads does the same arithmetic in the same order as the plain one, so the
+    mixed solve returns the same bits."""
+    d = decks.box_hex20_lognormal(10, 10, 5, seed=8)
+    f = gpu.face_load_vector(d)
+    s = gpu.GpuSystem(0)
+    s.set_option(gpu.OPT_PERSISTENT_MAX_NODES, 0)   # the kernels the option applies to
+    s.set_option(gpu.OPT_SPMV_LANES_FP32, lanes)
+    s.upload(d)
+    s.assemble()
+    u0, r0 = s.solve(f, tol=1e-10, precision=gpu.PREC_MIXED)
+    s.set_option(gpu.OPT_SPMV_STREAM_FP32, 1)
+    u1, r1 = s.solve(f, tol=1e-10, precision=gpu.PREC_MIXED)
+    assert r0["converged"] and r1["iterations"] == r0["iterations"]
+    assert np.array_equal(u0, u1)
+    s.close()
