@@ -749,11 +749,33 @@ int solve_node_space(fast_gpu_ctx *c, const fast_gpu_solve_opts *o, bool warm, f
   if (mixed) {
     CK(pcg_mixed(*c, warm, tol, maxit, chunk));
     R.outer = c->h_state->updates;
-    const int done = c->h_state->done, it = c->h_state->iter;
-    if ((done == 3 || done == 4) && it < maxit && !k32) {
+    int done = c->h_state->done, it = c->h_state->iter;
+    if ((done == 3 || done == 4) && it < maxit && k32) {
+      // The tensor-core FP32 stiffness (entries to about 1e-6 of the largest
+      // on degree-3 B-splines) could not take this system to the tolerance
+      // against its element-by-element FP64 residual, restarts included:
+      // assemble the FP64 stiffness and go on with the mixed iteration on it
+      // from the best FP64 iterate seen (its FP32 copy is the rounded FP64 K).
+      R.escalated = 2;
+      CK(cudaMemcpyAsync(c->d_u, c->d_ubest, sizeof(double) * 4 * c->nnode, cudaMemcpyDeviceToDevice, c->stream));
+      if (!c->use_first_touch()) CK(launch_zero_matrix(*c, c->d_K, true));
+      CK(launch_assemble(*c, FAST_ASM_STIFFNESS, c->d_K));
+      c->K_ok = true;
+      c->K32_current = false;
+      invalidate(*c, FAST_ASM_STIFFNESS);
+      CK(launch_build_precond(*c, c->d_K, precond));
+      c->precond_built = precond;
+      CK(ensure_soa(*c, FAST_ASM_STIFFNESS, true));
+      CK(pcg_mixed(*c, true, tol, maxit - it, chunk));
+      R.outer += c->h_state->updates;
+      c->h_state->iter += it;
+      done = c->h_state->done;
+      it = c->h_state->iter;
+    }
+    if ((done == 3 || done == 4) && it < maxit && !c->K32_current) {
       // FP32 iterates stopped making progress (ill-conditioned system): go on
       // with the FP64 iteration from the best FP64 iterate seen
-      R.escalated = 1;
+      R.escalated |= 1;
       CK(cudaMemcpyAsync(c->d_u, c->d_ubest, sizeof(double) * 4 * c->nnode, cudaMemcpyDeviceToDevice, c->stream));
       CK(pcg_fp64(*c, true, tol, maxit, chunk, it));
     }
@@ -764,13 +786,13 @@ int solve_node_space(fast_gpu_ctx *c, const fast_gpu_solve_opts *o, bool warm, f
   c->harvest();
   const PcgState &st = *c->h_state;
   R.iterations = st.iter;
-  R.rel_residual = (mixed && !R.escalated) ? st.err_true : st.err;
+  R.rel_residual = (mixed && !(R.escalated & 1)) ? st.err_true : st.err;
   R.converged = (st.done == 1);
-  // true FP64 residual |f - K u| / |f|
+  // true FP64 residual |f - K u| / |f| (element by element on the tensor-core stiffness)
   {
     double *d_rr = c->d_partials + 12290;
     double *d_ff = c->d_partials + 12291;
-    CK(launch_residual(*c, k32 ? nullptr : c->d_Ks, c->d_f, c->d_u, c->d_r, d_rr));  // null: element by element
+    CK(launch_residual(*c, c->K32_current ? nullptr : c->d_Ks, c->d_f, c->d_u, c->d_r, d_rr));  // null: element by element
     CK(launch_norm2(*c, c->d_f, 4 * c->nnode, d_ff));
     double h[2] = {0, 0};
     CK(cudaMemcpyAsync(h, d_rr, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));

@@ -169,7 +169,9 @@ typedef struct {
   int32_t converged;
   int32_t iterations;      /* PCG iterations (FP32 + FP64 iterations when mixed)  */
   int32_t outer;           /* FP64 residual replacements (mixed), 1 for FP64        */
-  int32_t escalated;       /* mixed: FP32 iterates stalled, finished in FP64       */
+  int32_t escalated;       /* mixed: bit 0 FP32 iterates stalled, finished in FP64; bit 1 the tensor-core
+                              stiffness stalled, the FP64 stiffness was assembled and the mixed
+                              iteration went on with it */
   double  rel_residual;    /* |r|/|f| of the final FP64 residual (mixed) or recurrence (FP64) */
   double  true_rel_residual; /* |f - K u| / |f| recomputed in FP64 at exit           */
 } fast_gpu_solve_report;
