@@ -290,6 +290,15 @@ def newton_plate(local, args):
         S.nr_solve(q, 40, 1.0 / 40, tol=1e-8, max_iter=30, **runs["secant_mixed"])
         t_nog.append(time.perf_counter() - t)
     S.set_option(gpu.OPT_GRAPH_STEPS, 1)
+    # the predictor's two phases per load step (live spans, one learned run)
+    S.kernel_timing(True)
+    S.nr_solve(q, 40, 1.0 / 40, tol=1e-8, max_iter=30, **runs["learned_mixed"])
+    S.synchronize()
+    pn_n, pn_ms, _ = S.kernel_stats(gpu.KERNEL_PREDICT_NET)
+    pg_n, pg_ms, _ = S.kernel_stats(gpu.KERNEL_PREDICT_GALERKIN)
+    S.kernel_timing(False)
+    pred_ms = {"network_ms_per_step": pn_ms / max(1, pn_n), "galerkin_ms_per_step": pg_ms / max(1, pg_n),
+               "steps": int(pn_n)}
     u_ref = out["plain_fp64"][0]
     zplate = load_fixture("full_plate_tl_40x40x4")
     eqn = d.node_eq()
@@ -325,6 +334,7 @@ def newton_plate(local, args):
         "speedup_secant_vs_plain": res["plain_fp64"]["ms"] / res["secant_mixed"]["ms"],
         "speedup_learned_vs_secant": res["secant_mixed"]["ms"] / res["learned_mixed"]["ms"],
         "secant_mixed_without_graphs_ms": min(t_nog) * 1e3,
+        "predictor": pred_ms,
         "training": {"seconds": train_s, "variants": info["converged_variants"], "samples": rep["samples"],
                      "modes": rep["modes"], "params": rep["params"], "captured_energy": rep["captured_energy"],
                      "first_loss": rep["first_loss"], "last_loss": rep["last_loss"],
@@ -507,7 +517,7 @@ def tied_blocks(local, args):
         runs[name] = best
     S.set_option(gpu.OPT_PERSISTENT_MAX_NODES, tuned)
     # the mixed path on the tensor-core stiffness (B-spline and hex buckets on
-    # tcgen05 in 3xTF32, tied elements' FP64 matrices, FP64 residuals element
+    # tcgen05 (TF32 operands split in three), tied elements' FP64 matrices, FP64 residuals element
     # by element)
     tc = None
     try:
@@ -766,7 +776,7 @@ def run_ours(args):
     rel_u = float(np.abs(u_main - u64).max() / np.abs(u64).max())
 
     # ---- the mixed path on the tensor-core stiffness: element products in
-    # 3xTF32 on tcgen05 (FP32 blocks), FP32 PCG, FP64 residuals element by
+    # three-part TF32 products on tcgen05 (FP32 blocks), FP32 PCG, FP64 residuals element by
     # element; timed like the value path, after two untimed steps
     def step_tc():
         S.assemble(gpu.ASM_K_TF32)

@@ -11,8 +11,10 @@ namespace fastgpu {
 
 namespace {
 
+// two CTAs per SM where their shared memory fits (registers held to 128)
 template <int PR, int PS, int PT, int NG1, int LPC>
-__global__ void __launch_bounds__(tcb::kThreads, 1) bsp_tc_kernel(ElemArgs A, float *__restrict__ K32) {
+__global__ void __launch_bounds__(tcb::kThreads, tcb::BspTc<PR, PS, PT, NG1, LPC>::bytes <= 116 * 1024 ? 2 : 1)
+    bsp_tc_kernel(ElemArgs A, float *__restrict__ K32) {
   using S = tcb::BspTc<PR, PS, PT, NG1, LPC>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *sm = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));

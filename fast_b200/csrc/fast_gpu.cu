@@ -1017,22 +1017,19 @@ int fast_gpu_kernel_stats(fast_gpu_ctx *c, int32_t which, int64_t *launches, dou
     // (the padding blocks of the solve layout are not counted: they are overhead)
     if (which == FAST_KERNEL_SPMV_FP64) algo = (double)c->nnzb * (9 * 8 + 4) + 4.0 * (c->nnode + 1) + 2.0 * 8 * n4;
     if (which == FAST_KERNEL_SPMV_FP32) algo = (double)c->nnzb * (9 * 4 + 4) + 4.0 * (c->nnode + 1) + 2.0 * 4 * n4;
-    if (which == FAST_KERNEL_ASSEMBLE) {
+    if (which == FAST_KERNEL_ASSEMBLE || which == FAST_KERNEL_ASSEMBLE_TF32) {
       // scatter model per element: incidence + coordinates + fixity + E, nu + slot map + 3x3 block
-      // read-modify-write, plus the zero fill of the block values
+      // read-modify-write (72-byte FP64 or 36-byte FP32 blocks), plus the zero fill of the block
+      // values; with first-touch stores the zero fill is gone, each block's first write reads
+      // nothing, and the flag words are read instead
+      const double blk = which == FAST_KERNEL_ASSEMBLE ? 72.0 : 36.0;
+      const bool ft = c->use_first_touch();
       for (const Bucket &B : c->buckets) {
         const double nn = B.nn;
-        algo += (double)B.ne * (nn * (4 + 24 + 1) + 16 + nn * nn * (4 + 2 * 72));
+        algo += (double)B.ne * (nn * (4 + 24 + 1) + 16 + nn * nn * (4 + 2 * blk));
+        if (ft) algo += (double)B.ne * 4.0 * first_words(B.nn);
       }
-      algo += 72.0 * c->nnzb;
-    }
-    if (which == FAST_KERNEL_ASSEMBLE_TF32) {
-      // the same model with FP32 blocks (36 bytes)
-      for (const Bucket &B : c->buckets) {
-        const double nn = B.nn;
-        algo += (double)B.ne * (nn * (4 + 24 + 1) + 16 + nn * nn * (4 + 2 * 36));
-      }
-      algo += 36.0 * c->nnzb;
+      algo += ft ? -blk * c->nnzb : blk * c->nnzb;
     }
     *bytes = algo;
   }

@@ -331,11 +331,14 @@ cudaError_t launch_tied_assemble(Ctx &c, double *K);
 // matrices (the scratch buffer) scattered as T_e^T K_e T_e in FP32
 cudaError_t launch_tied_assemble32(Ctx &c, float *K32);
 // G += K_e u_e of every tied element (node space, u with its slave values,
-// from the scratch buffer of the last assembly); DOFs without an equation take
-// nothing; nothing is done while *skip is non-zero
+// from the scratch buffer of the last assembly), every DOF of the element
+// (slave DOFs feed the restriction; fixed ones are zeroed by the caller);
+// nothing is done while *skip is non-zero
 cudaError_t launch_tied_matvec(Ctx &c, const double *u, double *G, const int32_t *skip);
 cudaError_t launch_tie_restrict(Ctx &c, double *f);  // f <- T^T f (padded node layout)
 cudaError_t launch_tie_zero(Ctx &c, double *v);      // v[slave DOFs] = 0
+// v[DOFs without an equation] = 0 (supports and slaves); nothing while *skip
+cudaError_t launch_zero_fixed(Ctx &c, double *v, const int32_t *skip);
 cudaError_t launch_tie_prolong(Ctx &c, double *u);   // u[slave] = sum w u[master]
 cudaError_t launch_element_matrices(Ctx &c, int what, int bucket, int64_t first_sorted, int64_t count,
                                     double *d_out);
@@ -350,7 +353,7 @@ cudaError_t launch_tl(Ctx &c, double *K, double *G, bool want_k, bool want_g);
 // nothing while *skip (a device flag, may be null) is non-zero
 cudaError_t launch_tl_at(Ctx &c, double *K, double *G, bool want_k, bool want_g, const double *U, const int32_t *skip);
 
-// elem_tc.cu: stiffness on the tensor cores (3xTF32, FP32 blocks), small-strain hex buckets
+// elem_tc.cu: stiffness on the tensor cores (TF32 operands split in three, FP32 blocks), small-strain hex buckets
 bool tc_supported(const Bucket &B);
 // B-spline degrees / rules of the tensor-core kernel (and of the mass kernel)
 bool bsp_tc_supported(const int pd[3], int ngp);

@@ -945,7 +945,7 @@ cudaError_t launch_matfree_residual(Ctx &c, const double *f, const double *u, do
   if (c.has_ties()) {
     if ((e = launch_tied_matvec(c, uu, c.d_gint, skip)) != cudaSuccess) return e;
     if ((e = launch_tie_restrict(c, c.d_gint)) != cudaSuccess) return e;
-    if ((e = launch_tie_zero(c, c.d_gint)) != cudaSuccess) return e;
+    if ((e = launch_zero_fixed(c, c.d_gint, skip)) != cudaSuccess) return e;
   }
   sub_residual<<<spmv_grid(c), kSpmvThreads, 0, c.stream>>>(n4, f, c.d_gint, r, part, skip);
   c.launches++;

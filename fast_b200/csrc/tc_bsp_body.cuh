@@ -313,15 +313,45 @@ __device__ bool tc_bsp_element(const ElemArgs &A, float *__restrict__ K32, uint8
       tc::ld_32x32b_x8(taddr + grp * 24, h);
       tc::ld_32x32b_x8(taddr + grp * 24 + 8, h + 8);
       tc::ld_32x32b_x8(taddr + grp * 24 + 16, h + 16);
+      // the current values of the group's blocks (row i of (a, b), column i
+      // of (b, a)), every load issued before any store, so their latencies
+      // overlap; a block this element writes first is not read
+      // (four blocks at a time: the registers of eight cost the SM a CTA)
 #pragma unroll
-      for (int bl = 0; bl < 8; bl++) {
-        const int b = grp * 8 + bl;
+      for (int half = 0; half < 2; half++) {
+      float oab[4][3], oba[4][3];
+      float *pab[4], *pba[4];
+      bool f1[4], f2[4];
+#pragma unroll
+      for (int bl = 0; bl < 4; bl++) {
+        const int b = grp * 8 + half * 4 + bl;
+        pab[bl] = pba[bl] = nullptr;
+        f1[bl] = f2[bl] = false;
+        if (!K32 || !own || b >= NN || b < a) continue;
+        pab[bl] = K32 + (int64_t)A.slot[(e * NN + a) * NN + b] * 9 + 3 * i;
+        f1[bl] = first_touch(A, e, a * NN + b);
+        if (!f1[bl]) {
+#pragma unroll
+          for (int j = 0; j < 3; j++) oab[bl][j] = pab[bl][j];
+        }
+        if (b != a) {
+          pba[bl] = K32 + (int64_t)A.slot[(e * NN + b) * NN + a] * 9 + i;
+          f2[bl] = first_touch(A, e, b * NN + a);
+          if (!f2[bl]) {
+#pragma unroll
+            for (int j = 0; j < 3; j++) oba[bl][j] = pba[bl][3 * j];
+          }
+        }
+      }
+#pragma unroll
+      for (int bl = 0; bl < 4; bl++) {
+        const int b = grp * 8 + half * 4 + bl;
         // the 3x3 block M[s][j] = H[(a,s),(b,j)] from the quad of node a
         double M[9];
 #pragma unroll
         for (int s2 = 0; s2 < 3; s2++)
 #pragma unroll
-          for (int j = 0; j < 3; j++) M[3 * s2 + j] = (double)__shfl_sync(0xffffffffu, h[3 * bl + j], qbase + s2);
+          for (int j = 0; j < 3; j++) M[3 * s2 + j] = (double)__shfl_sync(0xffffffffu, h[3 * (half * 4 + bl) + j], qbase + s2);
         if (!own || b >= NN || b < a) continue;
         const double tr = M[0] + M[4] + M[8];
         double v[3];
@@ -336,30 +366,27 @@ __device__ bool tc_bsp_element(const ElemArgs &A, float *__restrict__ K32, uint8
             Ko[(3 * b + j) * ND + 3 * a + i] = v[j];
           }
         }
-        if (K32) {
+        if (pab[bl]) {
           // add where both DOFs have equations; a first write (first-touch
           // flags) stores the entry instead, 1 / 0 where a DOF is fixed
           const uint8_t fb = sfix[b];
           const bool fai = (fa >> i) & 1;
-          const bool f1 = first_touch(A, e, a * NN + b);
-          float *Kab = K32 + (int64_t)A.slot[(e * NN + a) * NN + b] * 9;
 #pragma unroll
           for (int j = 0; j < 3; j++) {
             const bool fixed = fai || ((fb >> j) & 1);
-            if (f1) Kab[3 * i + j] = fixed ? ((a == b && i == j) ? 1.f : 0.f) : (float)v[j];
-            else if (!fixed) Kab[3 * i + j] += (float)v[j];
+            if (f1[bl]) pab[bl][j] = fixed ? ((a == b && i == j) ? 1.f : 0.f) : (float)v[j];
+            else if (!fixed) pab[bl][j] = oab[bl][j] + (float)v[j];
           }
-          if (b != a) {
-            const bool f2 = first_touch(A, e, b * NN + a);
-            float *Kba = K32 + (int64_t)A.slot[(e * NN + b) * NN + a] * 9;
+          if (pba[bl]) {
 #pragma unroll
             for (int j = 0; j < 3; j++) {
               const bool fixed = fai || ((fb >> j) & 1);
-              if (f2) Kba[3 * j + i] = fixed ? 0.f : (float)v[j];
-              else if (!fixed) Kba[3 * j + i] += (float)v[j];
+              if (f2[bl]) pba[bl][3 * j] = fixed ? 0.f : (float)v[j];
+              else if (!fixed) pba[bl][3 * j] = oba[bl][j] + (float)v[j];
             }
           }
         }
+      }
       }
     }
   }

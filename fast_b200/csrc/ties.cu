@@ -275,8 +275,7 @@ __global__ void __launch_bounds__(256) tied_matvec(int64_t first, int64_t count,
                                                    const int32_t *__restrict__ econn,
                                                    const int64_t *__restrict__ keoff, const int32_t *__restrict__ nn_of,
                                                    const double *__restrict__ ke, const double *__restrict__ u,
-                                                   const uint8_t *__restrict__ fix, double *__restrict__ G,
-                                                   const int32_t *__restrict__ skip) {
+                                                   double *__restrict__ G, const int32_t *__restrict__ skip) {
   if (skip && *skip) return;
   __shared__ double su[3 * 64];
   for (int64_t it = blockIdx.x; it < count; it += gridDim.x) {
@@ -287,9 +286,10 @@ __global__ void __launch_bounds__(256) tied_matvec(int64_t first, int64_t count,
     __syncthreads();
     for (int i = threadIdx.x; i < nd; i += blockDim.x) su[i] = u[4 * (int64_t)en[i / 3] + (i % 3)];
     __syncthreads();
+    // every row, slave DOFs included (they carry the element's force to the
+    // masters in the restriction that follows; the caller zeroes fixed DOFs)
     for (int r = threadIdx.x; r < nd; r += blockDim.x) {
       const int a = r / 3, i = r - 3 * a;
-      if ((fix[en[a]] >> i) & 1) continue;
       const double *row = Ke + (int64_t)r * nd;
       double g = 0.0;
       for (int k = 0; k < nd; k++) g = fma(row[k], su[k], g);
@@ -304,13 +304,30 @@ cudaError_t launch_tied_matvec(Ctx &c, const double *u, double *G, const int32_t
     const int64_t first = T.color_off[k], cnt = T.color_off[k + 1] - first;
     if (cnt <= 0) continue;
     const unsigned grid = (unsigned)std::min<int64_t>(cnt, 4LL * c.sm_count);
-    tied_matvec<<<grid, 256, 0, c.stream>>>(first, cnt, T.d_eptr, T.d_econn, T.d_keoff, T.d_nn, T.d_ke, u, c.d_fix,
-                                            G, skip);
+    tied_matvec<<<grid, 256, 0, c.stream>>>(first, cnt, T.d_eptr, T.d_econn, T.d_keoff, T.d_nn, T.d_ke, u, G, skip);
     c.launches++;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+// v[DOF] = 0 for every DOF without an equation (supports and tied slaves)
+__global__ void zero_fixed_dofs(int64_t nnode, const uint8_t *__restrict__ fix, double *__restrict__ v,
+                                const int32_t *__restrict__ skip) {
+  if (skip && *skip) return;
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= nnode) return;
+  const uint8_t f = fix[n];
+  if (!f) return;
+  for (int i = 0; i < 3; i++)
+    if ((f >> i) & 1) v[4 * n + i] = 0.0;
+}
+
+cudaError_t launch_zero_fixed(Ctx &c, double *v, const int32_t *skip) {
+  zero_fixed_dofs<<<(unsigned)((c.nnode + 255) / 256), 256, 0, c.stream>>>(c.nnode, c.d_fix, v, skip);
+  c.launches++;
+  return cudaGetLastError();
 }
 
 cudaError_t launch_tie_restrict(Ctx &c, double *f) {

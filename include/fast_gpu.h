@@ -69,7 +69,7 @@ extern "C" {
 #define FAST_ASM_MASS       2   /* cControl::MassMatrix      (ctrl/ctrl.cpp:979-1027) */
 #define FAST_ASM_INTERNAL_FORCE 3  /* element internal forces (fast_gpu_element_matrices only) */
 #define FAST_ASM_STIFFNESS_TF32 4  /* the stiffness for the mixed-precision solve: element
-                                      products B^T C B on the tensor cores (tcgen05, 3xTF32 split,
+                                      products B^T C B on the tensor cores (tcgen05, TF32 operands split in three,
                                       FP32 accumulation), blocks stored in FP32.  Small-strain
                                       hex8 / hex20 buckets and B-spline solids of degree (2,2,2),
                                       (3,3,3) or (3,3,2); elements touching a tied node keep FP64
@@ -644,14 +644,14 @@ int fast_gpu_get_lower_csr(fast_gpu_ctx *ctx, int32_t what, int64_t *nnz,
  * the same device kernels as the assembly: [count][3nn][3nn] row-major in
  * FAST's element DOF order (cElement::GetElmDofs); with
  * FAST_ASM_INTERNAL_FORCE the element internal forces, [count][3nn]; with
- * FAST_ASM_STIFFNESS_TF32 the tensor-core (3xTF32) element stiffness. */
+ * FAST_ASM_STIFFNESS_TF32 the tensor-core (three-part TF32) element stiffness. */
 int fast_gpu_element_matrices(fast_gpu_ctx *ctx, int32_t what, int32_t bucket, int64_t first,
                               int64_t count, double *Ke);
 
 /* ---- measurement ------------------------------------------------------ */
 #define FAST_KERNEL_SPMV_FP64  0   /* K.p with FP64 values (FP64 PCG, FP64 residuals)       */
 #define FAST_KERNEL_SPMV_FP32  1   /* K.p with FP32 values (mixed path)                     */
-#define FAST_KERNEL_ASSEMBLE   2   /* one stiffness assembly (zero fill + all colours)      */
+#define FAST_KERNEL_ASSEMBLE   2   /* one stiffness assembly (zero fill unless first-touch, all colours) */
 #define FAST_KERNEL_PREDICT_NET       3  /* learned predictor: projections, network, start */
 #define FAST_KERNEL_PREDICT_GALERKIN  4  /* learned predictor: reduced Newton corrections  */
 #define FAST_KERNEL_INTERNAL_FORCE    5  /* one internal-force evaluation                  */
