@@ -119,6 +119,14 @@ __device__ bool tc_bsp_element(const ElemArgs &A, float *__restrict__ K32, uint8
     sfix[i] = A.fix[en[i]];
     sW[i] = (rat && A.wt) ? A.wt[en[i]] : 1.0;
   }
+  // the element's slot row and its current K blocks, prefetched into L2 while
+  // the geometry is computed: the epilogue's read-modify-writes then wait on
+  // L2, not on DRAM
+  if (K32) {
+    const int32_t *es = A.slot + e * NN * NN;
+#pragma unroll 4
+    for (int q = tid; q < NN * NN; q += kThreads) tc::prefetch_l2(K32 + (int64_t)es[q] * 9);
+  }
   const int sr = A.span[4 * e], ss = A.span[4 * e + 1], st = A.span[4 * e + 2];
   const double *br = A.bas[0] + (size_t)sr * NG1 * QR * 2;
   const double *bs = A.bas[1] + (size_t)ss * NG1 * QS * 2;

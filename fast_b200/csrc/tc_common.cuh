@@ -150,6 +150,11 @@ __device__ __forceinline__ void split_term(int t, int &pa, int &pb) {
   pb = B[t];
 }
 
+// bring the line holding p into L2 (no register result, nothing waits on it)
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 // byte offset of element (row r, k) of a 4-byte K-major operand with kp
 // columns in the canonical layout above
 __device__ __forceinline__ uint32_t kmajor_off4(int r, int k, int kp) {

@@ -201,7 +201,8 @@ class TuneReport(ctypes.Structure):
                 ("elem_split", ctypes.c_int32 * 8), ("elem_tc_ctas", ctypes.c_int32 * 8),
                 ("elem_ms_default", ctypes.c_double * 8), ("elem_ms_tuned", ctypes.c_double * 8),
                 ("elem_tc_ms_default", ctypes.c_double * 8), ("elem_tc_ms_tuned", ctypes.c_double * 8),
-                ("ms_fp32_stream", ctypes.c_double * 2), ("stream_fp32", ctypes.c_int32), ("reserved2", ctypes.c_int32)]
+                ("ms_fp32_stream", ctypes.c_double * 2), ("stream_fp32", ctypes.c_int32), ("reserved2", ctypes.c_int32),
+                ("us_iter_mixed", ctypes.c_double * 6)]
 
     def as_dict(self):
         return {"lanes_fp32": self.lanes_fp32, "lanes_fp64": self.lanes_fp64,
@@ -214,7 +215,8 @@ class TuneReport(ctypes.Structure):
                               "tc_ctas_per_sm": self.elem_tc_ctas[b], "tc_ms_default": self.elem_tc_ms_default[b],
                               "tc_ms_tuned": self.elem_tc_ms_tuned[b]} for b in range(self.elem_buckets)],
                 "elements_tensor_core_timed": bool(self.elem_tc),
-                "ms_fp32_stream_lanes_8_16": list(self.ms_fp32_stream), "stream_fp32": bool(self.stream_fp32)}
+                "ms_fp32_stream_lanes_8_16": list(self.ms_fp32_stream), "stream_fp32": bool(self.stream_fp32),
+                "us_per_mixed_iteration_plain_8_16_stream_8_16_bulk_8_16": list(self.us_iter_mixed)}
 
 
 class ProblemReport(ctypes.Structure):

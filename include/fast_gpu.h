@@ -225,7 +225,8 @@ int         fast_gpu_set_option(fast_gpu_ctx *ctx, int32_t option, int64_t value
  * tensor-core path (CUDA events, median of 3 assemblies each), then
  * re-assembles K with the chosen shapes; times the SpMV of the assembled
  * stiffness for every lanes-per-row choice in both precisions (median of 9
- * launches each) and, for systems small enough for the persistent PCG kernel,
+ * launches each), chooses the FP32 SpMV form by 64 mixed PCG iterations with
+ * each (median of 3) and, for systems small enough for the persistent PCG kernel,
  * one 64-iteration FP64 PCG chunk on each iteration path; keeps the fastest
  * choices as the context's options.  Needs an assembled K; uses the solver's
  * work vectors (call it before a solve, not during one). */
@@ -245,6 +246,8 @@ typedef struct {
   double  ms_fp32_stream[2];            /* FP32 SpMV with cache-streaming matrix loads, 8 and 16 lanes   */
   int32_t stream_fp32;                  /* 1: the cache-streaming FP32 SpMV was kept                      */
   int32_t reserved2;
+  double  us_iter_mixed[6];             /* mixed PCG per iteration with each FP32 form (the choice):
+                                           8 / 16 lanes plain, cache-streaming, bulk-staged (0: not run) */
 } fast_gpu_tune_report;
 int         fast_gpu_autotune(fast_gpu_ctx *ctx, fast_gpu_tune_report *rep);
 
