@@ -80,25 +80,47 @@ cudaError_t tune_bucket(Ctx &c, size_t b, bool tc, double &ms_default, double &m
   int &ctas = tc ? B.tune_tc_ctas : B.tune_ctas;
   ctas = 0;
   if (!tc) B.tune_split = 0;
+  if (!tc) B.tune_kernel = 0;
   c.elem_occ = c.elem_split_max = 0;
   cudaError_t e = median_ms(c, launch, kReps, ms_default);
   if (e != cudaSuccess) return e;
-  const int occ = std::min(c.elem_occ, 16);
-  const int smax = (tc || B.type != FAST_ELEM_BSP_SOLID) ? 0 : std::min(c.elem_split_max, 16);
-  int best_c = 0, best_s = 0;
+  int best_c = 0, best_s = 0, best_k = 0;
   ms_best = ms_default;
-  for (int k = 1; k <= occ; k++)
-    for (int sp = 0; sp <= smax; sp++) {
-      if (k == occ && sp == 0) continue;  // the default
-      ctas = k;
-      if (!tc) B.tune_split = sp;
+  // FP64 hex buckets: both kernels (CTA per element, warp per element)
+  const int kernels = (!tc && warp_supported(B)) ? 2 : 1;
+  for (int kern = 0; kern < kernels; kern++) {
+    if (!tc) B.tune_kernel = kern;
+    int occ = 0;
+    if (kern == 0) {
+      occ = c.elem_occ;
+    } else {
+      // the warp kernel's own occupancy from a run at its default shape
+      ctas = 0;
+      c.elem_occ = 0;
       double ms = 0.0;
       e = median_ms(c, launch, kReps, ms);
       if (e != cudaSuccess) return e;
-      if (ms < 0.98 * ms_best) { ms_best = ms; best_c = k; best_s = sp; }
+      if (ms < 0.98 * ms_best) { ms_best = ms; best_c = 0; best_s = 0; best_k = kern; }
+      occ = c.elem_occ;
     }
+    occ = std::min(occ, 16);
+    const int smax = (tc || B.type != FAST_ELEM_BSP_SOLID) ? 0 : std::min(c.elem_split_max, 16);
+    for (int k = 1; k <= occ; k++)
+      for (int sp = 0; sp <= smax; sp++) {
+        if (k == occ && sp == 0) continue;  // the kernel's default
+        ctas = k;
+        if (!tc) B.tune_split = sp;
+        double ms = 0.0;
+        e = median_ms(c, launch, kReps, ms);
+        if (e != cudaSuccess) return e;
+        if (ms < 0.98 * ms_best) { ms_best = ms; best_c = k; best_s = sp; best_k = kern; }
+      }
+  }
   ctas = best_c;
-  if (!tc) B.tune_split = best_s;
+  if (!tc) {
+    B.tune_split = best_s;
+    B.tune_kernel = best_k;
+  }
   return cudaSuccess;
 }
 
@@ -128,6 +150,7 @@ extern "C" int fast_gpu_autotune(fast_gpu_ctx *c, fast_gpu_tune_report *rep) {
       R.elem_ctas[b] = B.tune_ctas;
       R.elem_split[b] = B.tune_split;
       R.elem_tc_ctas[b] = B.tune_tc_ctas;
+      R.elem_kernel[b] = B.tune_kernel;
       R.elem_ms_default[b] = d64;
       R.elem_ms_tuned[b] = t64;
       R.elem_tc_ms_default[b] = dtc;

@@ -301,6 +301,8 @@ template <bool MASS>
 static cudaError_t dispatch(Ctx &c, const Bucket &B, ElemArgs a, int64_t count) {
   const int ng = B.ng;
   if (B.type == FAST_ELEM_BSP_SOLID) return launch_bsp_elements(c, B, a, count, MASS);
+  // the warp-per-element kernel, where the autotuner chose it (stiffness into K only)
+  if (!MASS && B.tune_kernel == 1 && a.K && !a.Ke_out && warp_supported(B)) return launch_warp_elements(c, B, a, count);
   if (B.type == FAST_ELEM_HEX8) {
     switch (ng) {
       case 1: return run<8, 1, 64, MASS>(c, a, count);

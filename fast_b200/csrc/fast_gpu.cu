@@ -241,14 +241,16 @@ int fast_gpu_set_option(fast_gpu_ctx *c, int32_t option, int64_t value) {
     return FAST_GPU_OK;
   }
   if (option == FAST_OPT_ELEM_SHAPE) {
-    const int64_t b = value >> 24;
-    if (value < 0 || b >= (int64_t)c->buckets.size()) return FAST_GPU_EINVAL;
+    const int64_t b = (value >> 24) & 0xFF, kern = value >> 32;
+    if (value < 0 || b >= (int64_t)c->buckets.size() || kern < 0 || kern > 1) return FAST_GPU_EINVAL;
+    if (kern == 1 && !warp_supported(c->buckets[(size_t)b])) return FAST_GPU_EINVAL;
     CK(cudaStreamSynchronize(c->stream));
     c->drop_graphs();
     Bucket &B = c->buckets[(size_t)b];
     B.tune_ctas = (int)(value & 0xFF);
     B.tune_split = (int)((value >> 8) & 0xFF);
     B.tune_tc_ctas = (int)((value >> 16) & 0xFF);
+    B.tune_kernel = (int)kern;
     return FAST_GPU_OK;
   }
   return FAST_GPU_EINVAL;

@@ -79,6 +79,7 @@ struct Bucket {
   int tune_ctas = 0;               // FP64 element kernels: resident CTAs per SM at most
   int tune_split = 0;              // B-spline FP64 kernels: CTAs sharing one element at most
   int tune_tc_ctas = 0;            // tensor-core element kernels: resident CTAs per SM at most
+  int tune_kernel = 0;             // FP64 hex stiffness: 0 CTA per element, 1 warp per element (elem_warp.cu)
   // B-spline solids (FAST_ELEM_BSP_SOLID)
   int pd[3] = {0, 0, 0};           // degree per direction
   int rational = 0;
@@ -318,6 +319,10 @@ cudaError_t launch_zero_matrix(Ctx &c, double *K, bool identity_on_fixed);
 // 1 on the diagonal of every fixed DOF (the stiffness slot's convention)
 cudaError_t launch_fixed_identity(Ctx &c, double *K);
 cudaError_t launch_assemble(Ctx &c, int what, double *target);
+// elem_warp.cu: FP64 hex stiffness with one warp per element (one colour)
+struct ElemArgs;
+bool warp_supported(const Bucket &B);
+cudaError_t launch_warp_elements(Ctx &c, const Bucket &B, ElemArgs a, int64_t count);
 // the small-strain stiffness of one bucket, every colour (no tied elements)
 cudaError_t launch_assemble_bucket(Ctx &c, size_t b, double *target);
 // device face loads (face_loads.cu)

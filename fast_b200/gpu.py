@@ -59,11 +59,13 @@ OPT_PERSISTENT_ASSEMBLY = 8
 OPT_SPMV_STREAM_FP32 = 9
 
 
-def elem_shape(bucket: int, ctas: int = 0, split: int = 0, tc_ctas: int = 0) -> int:
-    """The value of OPT_ELEM_SHAPE for one bucket (each field 0..255, 0 = default)."""
+def elem_shape(bucket: int, ctas: int = 0, split: int = 0, tc_ctas: int = 0, kernel: int = 0) -> int:
+    """The value of OPT_ELEM_SHAPE for one bucket (each field 0..255, 0 = default;
+    kernel 1: the FP64 hex stiffness with one warp per element)."""
     for v in (ctas, split, tc_ctas):
         assert 0 <= v <= 255
-    return (int(bucket) << 24) | (tc_ctas << 16) | (split << 8) | ctas
+    assert kernel in (0, 1)
+    return (int(kernel) << 32) | (int(bucket) << 24) | (tc_ctas << 16) | (split << 8) | ctas
 KERNEL_SPMV_FP64, KERNEL_SPMV_FP32, KERNEL_ASSEMBLE = 0, 1, 2
 KERNEL_PREDICT_NET, KERNEL_PREDICT_GALERKIN, KERNEL_INTERNAL_FORCE, KERNEL_LINEAR_SOLVE = 3, 4, 5, 6
 KERNEL_ASSEMBLE_TF32 = 7
@@ -202,7 +204,7 @@ class TuneReport(ctypes.Structure):
                 ("elem_ms_default", ctypes.c_double * 8), ("elem_ms_tuned", ctypes.c_double * 8),
                 ("elem_tc_ms_default", ctypes.c_double * 8), ("elem_tc_ms_tuned", ctypes.c_double * 8),
                 ("ms_fp32_stream", ctypes.c_double * 2), ("stream_fp32", ctypes.c_int32), ("reserved2", ctypes.c_int32),
-                ("us_iter_mixed", ctypes.c_double * 6)]
+                ("us_iter_mixed", ctypes.c_double * 6), ("elem_kernel", ctypes.c_int32 * 8)]
 
     def as_dict(self):
         return {"lanes_fp32": self.lanes_fp32, "lanes_fp64": self.lanes_fp64,
@@ -210,7 +212,8 @@ class TuneReport(ctypes.Structure):
                 "ms_fp32_bulk_lanes_8_16": list(self.ms_fp32_bulk), "bulk_fp32": bool(self.bulk_fp32),
                 "persistent_max_nodes": self.persistent_max_nodes, "us_iter_persistent": self.us_iter_persistent,
                 "us_iter_kernels": self.us_iter_kernels,
-                "elements": [{"ctas_per_sm": self.elem_ctas[b], "split": self.elem_split[b],
+                "elements": [{"kernel": "warp" if self.elem_kernel[b] == 1 else "cta",
+                              "ctas_per_sm": self.elem_ctas[b], "split": self.elem_split[b],
                               "ms_default": self.elem_ms_default[b], "ms_tuned": self.elem_ms_tuned[b],
                               "tc_ctas_per_sm": self.elem_tc_ctas[b], "tc_ms_default": self.elem_tc_ms_default[b],
                               "tc_ms_tuned": self.elem_tc_ms_tuned[b]} for b in range(self.elem_buckets)],

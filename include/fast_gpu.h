@@ -211,11 +211,13 @@ int         fast_gpu_synchronize(fast_gpu_ctx *ctx);
                                             take elements from a counter, heaviest kinds first); 0
                                             (default): one launch per bucket and colour */
 #define FAST_OPT_ELEM_SHAPE           6  /* launch shape of one bucket's element kernels, value =
-                                            bucket << 24 | tc_ctas << 16 | split << 8 | ctas (each field
-                                            0..255, 0 = the default): resident CTAs per SM of the FP64
-                                            kernels (ctas) and of the tensor-core kernels (tc_ctas), CTAs
-                                            sharing one B-spline element (split); what fast_gpu_autotune
-                                            chooses, for callers that cache its choices */
+                                            kernel << 32 | bucket << 24 | tc_ctas << 16 | split << 8 | ctas
+                                            (each field 0..255, 0 = the default): resident CTAs per SM of
+                                            the FP64 kernels (ctas) and of the tensor-core kernels
+                                            (tc_ctas), CTAs sharing one B-spline element (split), the FP64
+                                            hex stiffness kernel (0 one CTA per element, 1 one warp per
+                                            element); what fast_gpu_autotune chooses, for callers that
+                                            cache its choices */
 int         fast_gpu_set_option(fast_gpu_ctx *ctx, int32_t option, int64_t value);
 
 /* Autotuner (no reference counterpart): times, per bucket of small-strain
@@ -248,6 +250,8 @@ typedef struct {
   int32_t reserved2;
   double  us_iter_mixed[6];             /* mixed PCG per iteration with each FP32 form (the choice):
                                            8 / 16 lanes plain, cache-streaming, bulk-staged (0: not run) */
+  int32_t elem_kernel[8];               /* FP64 hex stiffness kernel chosen per bucket: 0 one CTA per
+                                           element, 1 one warp per element                            */
 } fast_gpu_tune_report;
 int         fast_gpu_autotune(fast_gpu_ctx *ctx, fast_gpu_tune_report *rep);
 

@@ -72,11 +72,15 @@ def test_every_element_launch_shape_gives_the_same_stiffness():
     K0_32 = s.lower_csr(gpu.ASM_K_TF32)
     nb = s.nbuckets
     assert nb == 4
+    kinds = [bk.kind for bk in d.buckets()]
     for b in range(nb):
-        for ctas, split, tc in ((1, 0, 1), (2, 1, 2), (1, 2, 1), (3, 4, 0)):
-            s.set_option(gpu.OPT_ELEM_SHAPE, gpu.elem_shape(b, ctas, split, tc))
+        shapes = [(1, 0, 1, 0), (2, 1, 2, 0), (1, 2, 1, 0), (3, 4, 0, 0)]
+        if kinds[b] in ("hex8", "hex20"):
+            shapes += [(0, 0, 0, 1), (1, 0, 0, 1), (2, 0, 0, 1)]   # one warp per element
+        for ctas, split, tc, kern in shapes:
+            s.set_option(gpu.OPT_ELEM_SHAPE, gpu.elem_shape(b, ctas, split, tc, kern))
             s.assemble()
-            assert (s.lower_csr() != K0).nnz == 0, (b, ctas, split)
+            assert (s.lower_csr() != K0).nnz == 0, (b, ctas, split, kern)
             s.assemble(gpu.ASM_K_TF32)
             assert (s.lower_csr(gpu.ASM_K_TF32) != K0_32).nnz == 0, (b, tc)
         s.set_option(gpu.OPT_ELEM_SHAPE, gpu.elem_shape(b))
@@ -117,3 +121,31 @@ def test_streaming_spmv_gives_the_same_bits(lanes):
     assert r0["converged"] and r1["iterations"] == r0["iterations"]
     assert np.array_equal(u0, u1)
     s.close()
+
+
+@pytest.mark.parametrize("ng", [(2, 2, 2), (3, 3, 3)])
+def test_warp_per_element_stiffness_matches_reference(ng):
+    """The FP64 hex stiffness with one warp per element gives the same K, bit
+    for bit, as the CTA-per-element kernel (same arithmetic in the same
+    order), and so the reference's K (hex20 lognormal box, first-touch
+    stores)."""
+    d = decks.box_hex20_lognormal(6, 6, 3, seed=12)
+    d.ngp = ng
+    s = gpu.GpuSystem(0)
+    s.upload(d)
+    s.assemble()
+    K0 = s.lower_csr()
+    s.set_option(gpu.OPT_ELEM_SHAPE, gpu.elem_shape(0, kernel=1))
+    n0 = s.launch_count()
+    s.assemble()
+    K1 = s.lower_csr()
+    assert K1.nnz == K0.nnz and abs(K1 - K0).max() == 0
+    K = fo.assemble(d)
+    R = fo_lower(K)
+    assert abs(K1 - R).max() / abs(R).max() < 1e-12
+    s.close()
+
+
+def fo_lower(K):
+    import scipy.sparse as sp
+    return sp.tril(K).tocsr()
