@@ -109,7 +109,11 @@ typedef struct {
 } fast_gpu_patch;
 
 /* One bucket = one element type with one Gauss rule (a FAST element reader
- * block with one %INTEGRATION.ORDER). */
+ * block with one %INTEGRATION.ORDER).  Material: isotropic linear elastic per
+ * element (E, nu: cMatElastIso), the constitutive matrix of cSolid::QMatrix;
+ * the element kernels fold it into the Gauss-point contraction, so a general
+ * 6x6 tangent (cConstModel::TangMat of other material models) has no device
+ * path. */
 typedef struct {
   int32_t        elem_type;     /* FAST_ELEM_*                                 */
   int32_t        ngp[3];        /* Gauss points per direction (r, s, t)        */
