@@ -25,25 +25,38 @@ namespace {
 
 using tcb::kThreads;
 
+// elements sharing one 128-row operand tile per pass: five hex8 or two hex20
+template <int NN> constexpr int kEpt = 128 / (3 * NN);
+
 template <int NN, int NG>
 __global__ void __launch_bounds__(kThreads, 1) elem_tc_kernel(ElemArgs A, float *__restrict__ K32) {
-  using S = tcb::TcHex<NN, NG>;
+  constexpr int EPT = kEpt<NN>;
+  using S = tcb::TcHex<NN, NG, EPT>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *sm = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   __shared__ __align__(8) uint64_t bars[2];   // [0] bulk copies, [1] MMAs
   __shared__ uint32_t tmem_sh;
   __shared__ int fail_sh;
   tcb::Cta c = tcb::cta_begin(S::TCOLS, bars, &tmem_sh, &fail_sh);
-  bool ok = tcb::tc_hex_setup<NN, NG>(A, sm, c);
-  for (int64_t it = blockIdx.x; ok && it < A.ne; it += gridDim.x)
-    ok = tcb::tc_hex_element<NN, NG>(A, K32, sm, c, it, A.index ? (int64_t)A.index[it] : A.offset + it);
+  bool ok = tcb::tc_hex_setup<NN, NG, EPT>(A, sm, c);
+  // pass k of this CTA takes items (blockIdx.x + k gridDim.x) EPT .. + EPT-1
+  for (int64_t it0 = (int64_t)blockIdx.x * EPT; ok && it0 < A.ne; it0 += (int64_t)gridDim.x * EPT) {
+    const int nv = (int)(A.ne - it0 < EPT ? A.ne - it0 : EPT);
+    int64_t its[EPT], es[EPT];
+#pragma unroll
+    for (int j = 0; j < EPT; j++) {
+      its[j] = it0 + (j < nv ? j : 0);
+      es[j] = A.index ? (int64_t)A.index[its[j]] : A.offset + its[j];
+    }
+    ok = tcb::tc_hex_elements<NN, NG, EPT>(A, K32, sm, c, its, es, nv);
+  }
   tcb::cta_end(c, S::TCOLS, A.status);
 }
 
 template <int NN, int NG>
 cudaError_t run_tc(Ctx &c, ElemArgs a, int64_t count, float *K32) {
   if (count <= 0) return cudaSuccess;
-  using S = tcb::TcHex<NN, NG>;
+  using S = tcb::TcHex<NN, NG, kEpt<NN>>;
   auto kern = elem_tc_kernel<NN, NG>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, S::bytes);
   if (e != cudaSuccess) return e;
@@ -55,7 +68,8 @@ cudaError_t run_tc(Ctx &c, ElemArgs a, int64_t count, float *K32) {
   if (per_sm * S::TCOLS > 512) per_sm = 512 / S::TCOLS;
   per_sm = elem_per_sm(c, per_sm, a.ctas_per_sm);
   int64_t grid = (int64_t)per_sm * c.sm_count;
-  if (grid > count) grid = count;
+  const int64_t passes = (count + kEpt<NN> - 1) / kEpt<NN>;
+  if (grid > passes) grid = passes;
   a.ne = count;
   kern<<<(unsigned)grid, kThreads, S::bytes, c.stream>>>(a, K32);
   c.launches++;

@@ -133,50 +133,57 @@ __device__ __forceinline__ bool wait_bar_drain(Cta &c, int b) {
   return false;
 }
 
-template <int NN, int NG>
+// EPT elements share one 128-row operand tile: rows j*R .. j*R+R-1 hold
+// element j (hex8: five elements, hex20: two), and the MMA forms all their
+// products at once (the off-diagonal blocks between elements are not read),
+// so every phase of a pass works on EPT elements between the same barriers.
+template <int NN, int NG, int EPT = 1>
 struct TcHex {
-  static constexpr int R = 3 * NN;                 // operand rows (i, a), i-major
+  static constexpr int R = 3 * NN;                 // operand rows (i, a) of one element, i-major
   static constexpr int KP = (NG + 7) / 8 * 8;      // Gauss points padded to the MMA K
-  static constexpr int N = (R + 15) / 16 * 16;     // accumulator columns (M = 128 needs N % 16 == 0)
+  static constexpr int N = (EPT * R + 15) / 16 * 16;  // accumulator columns (M = 128 needs N % 16 == 0)
   static constexpr int RP = 128;                   // operand rows held (one M tile)
   static constexpr int NP = NN * (NN + 1) / 2;
   static constexpr int OPB = RP * KP * 4;          // bytes of one operand part (hi, lo or mid)
   static constexpr int TCOLS = pow2_cols(N);
-  static_assert(R <= 128, "one M tile");
+  static_assert(EPT * R <= 128, "the elements of a pass share one M tile");
   static_assert(NP <= kThreads, "one thread per node pair");
   static_assert((NN * NN * 4) % 16 == 0 && (NN * 4) % 16 == 0 && (NG * NN * 3 * 8) % 16 == 0,
                 "bulk-copy sizes are multiples of 16 bytes");
   // shared memory carve-up (bytes from a 1024-aligned base, every piece on a
-  // 16-byte boundary)
+  // 16-byte boundary); per-element pieces repeat EPT times at stride s*
   static constexpr int al(int x) { return (x + 15) / 16 * 16; }
-  static constexpr int oHi = 0, oLo = oHi + OPB, oMid = oLo + OPB;
-  static constexpr int oH = oMid + OPB;                       // float [R][R]
-  static constexpr int oKo = oH + al(R * R * 4);              // float [NN*NN][9] old blocks
-  static constexpr int oV = oKo + al(NN * NN * 9 * 4);        // float [NP][9] new blocks
-  static constexpr int odN = oV + al(NP * 9 * 4);             // double [NG][NN][3] (bulk-copy target)
-  static constexpr int ow = odN + al(NG * NN * 3 * 8);        // double [NG]
-  static constexpr int oX = ow + al(NG * 8);                  // double [NN][3]
-  static constexpr int oJ = oX + al(NN * 3 * 8);              // double [NG][9]
-  static constexpr int oc = oJ + al(NG * 9 * 8);              // double [NG]
-  static constexpr int oSlot = oc + al(NG * 8);               // int32 [NN][NN] (bulk-copy target)
-  static constexpr int oConn = oSlot + al(NN * NN * 4);       // int32 [NN] (bulk-copy target)
+  static constexpr int sH = al(R * R * 4), sKo = al(NN * NN * 9 * 4), sV = al(NP * 9 * 4);
+  static constexpr int sX = al(NN * 3 * 8), sJ = al(NG * 9 * 8), sC = al(NG * 8);
   static constexpr int FW = (NN * NN + 127) / 128 * 4;        // first-touch flag words (first_words)
-  static constexpr int oFirst = oConn + al(NN * 4);           // uint32 [FW] (bulk-copy target)
-  static constexpr int oFix = oFirst + FW * 4;                // uint8 [NN]
-  static constexpr int used = oFix + al(NN);
+  static constexpr int sSlot = al(NN * NN * 4), sConn = al(NN * 4), sFirst = FW * 4, sFix = al(NN);
+  static constexpr int oHi = 0, oLo = oHi + OPB, oMid = oLo + OPB;
+  static constexpr int oH = oMid + OPB;                       // float [EPT][R][R]
+  static constexpr int oKo = oH + EPT * sH;                   // float [EPT][NN*NN][9] old blocks
+  static constexpr int oV = oKo + EPT * sKo;                  // float [EPT][NP][9] new blocks
+  static constexpr int odN = oV + EPT * sV;                   // double [NG][NN][3] (bulk-copy target)
+  static constexpr int ow = odN + al(NG * NN * 3 * 8);        // double [NG]
+  static constexpr int oX = ow + al(NG * 8);                  // double [EPT][NN][3]
+  static constexpr int oJ = oX + EPT * sX;                    // double [EPT][NG][9]
+  static constexpr int oc = oJ + EPT * sJ;                    // double [EPT][NG]
+  static constexpr int oSlot = oc + EPT * sC;                 // int32 [EPT][NN][NN] (bulk-copy targets)
+  static constexpr int oConn = oSlot + EPT * sSlot;           // int32 [EPT][NN] (bulk-copy targets)
+  static constexpr int oFirst = oConn + EPT * sConn;          // uint32 [EPT][FW] (bulk-copy targets)
+  static constexpr int oFix = oFirst + EPT * sFirst;          // uint8 [EPT][NN]
+  static constexpr int used = oFix + EPT * sFix;
   static_assert(odN % 16 == 0 && oSlot % 16 == 0 && oConn % 16 == 0 && oFirst % 16 == 0 && OPB % 16 == 0 &&
-                    (FW * 4) % 16 == 0,
+                    sFirst % 16 == 0 && sSlot % 16 == 0 && sConn % 16 == 0,
                 "bulk-copy targets on 16-byte boundaries");
   static constexpr int bytes = used + 1024;                   // + alignment slack of the base
   static_assert(bytes <= 232448, "shared memory of one CTA");
 };
 
 // A hex bucket's set-up in a CTA: operands zeroed (the K padding, Gauss
-// points NG..KP-1, and rows R..127 stay zero for every element), the Gauss
+// points NG..KP-1, and rows past the last element stay zero), the Gauss
 // tables in shared memory (bulk copy on barrier 0).  False on a failed wait.
-template <int NN, int NG>
+template <int NN, int NG, int EPT = 1>
 __device__ bool tc_hex_setup(const ElemArgs &A, uint8_t *sm, Cta &c) {
-  using S = TcHex<NN, NG>;
+  using S = TcHex<NN, NG, EPT>;
   const int tid = threadIdx.x;
   for (int i = tid; i < 3 * S::OPB / 16; i += kThreads) reinterpret_cast<uint4 *>(sm + S::oHi)[i] = make_uint4(0, 0, 0, 0);
   double *sdN = reinterpret_cast<double *>(sm + S::odN);
@@ -192,67 +199,79 @@ __device__ bool tc_hex_setup(const ElemArgs &A, uint8_t *sm, Cta &c) {
   return *c.fail == 0;
 }
 
-// Element `it` of the launch (colour-sorted position e): its blocks into K32
-// (null: only the dense FP64 element matrix into A.Ke_out).  False on a
-// failed wait, after its work in flight has finished (bounded).
-template <int NN, int NG>
-__device__ bool tc_hex_element(const ElemArgs &A, float *__restrict__ K32, uint8_t *sm, Cta &c, int64_t it,
-                               int64_t e) {
-  using S = TcHex<NN, NG>;
-  constexpr int R = S::R, KP = S::KP, N = S::N;
+// One pass over nv <= EPT elements: element j is launch item its[j] at
+// colour-sorted position es[j] (the same values in every thread).  Their
+// blocks go into K32 (null: only the dense FP64 element matrices into
+// A.Ke_out, at the items' positions).  False on a failed wait, after the
+// work in flight has finished (bounded).
+template <int NN, int NG, int EPT>
+__device__ bool tc_hex_elements(const ElemArgs &A, float *__restrict__ K32, uint8_t *sm, Cta &c,
+                                const int64_t (&its)[EPT], const int64_t (&es)[EPT], int nv) {
+  using S = TcHex<NN, NG, EPT>;
+  constexpr int R = S::R, KP = S::KP, N = S::N, NP = S::NP;
   uint8_t *opHi = sm + S::oHi, *opLo = sm + S::oLo, *opMid = sm + S::oMid;
-  float *sH = reinterpret_cast<float *>(sm + S::oH);
-  float *sKo = reinterpret_cast<float *>(sm + S::oKo);
-  float *sV = reinterpret_cast<float *>(sm + S::oV);
   double *sdN = reinterpret_cast<double *>(sm + S::odN);
   double *sw = reinterpret_cast<double *>(sm + S::ow);
-  double *sX = reinterpret_cast<double *>(sm + S::oX);
-  double *sJ = reinterpret_cast<double *>(sm + S::oJ);
-  double *sc = reinterpret_cast<double *>(sm + S::oc);
-  int32_t *sSlot = reinterpret_cast<int32_t *>(sm + S::oSlot);
-  int32_t *sConn = reinterpret_cast<int32_t *>(sm + S::oConn);
-  uint32_t *sFirst = reinterpret_cast<uint32_t *>(sm + S::oFirst);
-  uint8_t *sfix = sm + S::oFix;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   constexpr uint32_t kLBO = 128, kSBO = (KP / 4) * 128;
   constexpr uint32_t kId = tc::idesc(128, N, tc::kTypeTF32);
-  int32_t pa = 0, pb = 0;
-  if (tid < S::NP) pair_of(tid, NN, pa, pb);
+  auto H = [&](int j) { return reinterpret_cast<float *>(sm + S::oH + j * S::sH); };
+  auto Ko = [&](int j) { return reinterpret_cast<float *>(sm + S::oKo + j * S::sKo); };
+  auto V = [&](int j) { return reinterpret_cast<float *>(sm + S::oV + j * S::sV); };
+  auto X = [&](int j) { return reinterpret_cast<double *>(sm + S::oX + j * S::sX); };
+  auto Jm = [&](int j) { return reinterpret_cast<double *>(sm + S::oJ + j * S::sJ); };
+  auto Cg = [&](int j) { return reinterpret_cast<double *>(sm + S::oc + j * S::sC); };
+  auto Slot = [&](int j) { return reinterpret_cast<int32_t *>(sm + S::oSlot + j * S::sSlot); };
+  auto Conn = [&](int j) { return reinterpret_cast<int32_t *>(sm + S::oConn + j * S::sConn); };
+  auto First = [&](int j) { return reinterpret_cast<uint32_t *>(sm + S::oFirst + j * S::sFirst); };
+  auto Fix = [&](int j) { return sm + S::oFix + j * S::sFix; };
 
   __syncthreads();
   if (tid == 0) {
-    tc::mbar_arrive_tx(&c.bars[0], NN * NN * 4 + NN * 4 + (A.first ? S::FW * 4 : 0));
-    tc::bulk_g2s(sSlot, A.slot + e * NN * NN, NN * NN * 4, &c.bars[0]);
-    tc::bulk_g2s(sConn, A.conn + e * NN, NN * 4, &c.bars[0]);
-    if (A.first) tc::bulk_g2s(sFirst, A.first + e * S::FW, S::FW * 4, &c.bars[0]);
+    tc::mbar_arrive_tx(&c.bars[0], nv * (NN * NN * 4 + NN * 4 + (A.first ? S::FW * 4 : 0)));
+    for (int j = 0; j < nv; j++) {
+      tc::bulk_g2s(Slot(j), A.slot + es[j] * NN * NN, NN * NN * 4, &c.bars[0]);
+      tc::bulk_g2s(Conn(j), A.conn + es[j] * NN, NN * 4, &c.bars[0]);
+      if (A.first) tc::bulk_g2s(First(j), A.first + es[j] * S::FW, S::FW * 4, &c.bars[0]);
+    }
   }
   wait_bar_drain(c, 0);
   __syncthreads();
   if (*c.fail) return false;
-  for (int i = tid; i < NN * 3; i += kThreads) sX[i] = A.X[3 * (int64_t)sConn[i / 3] + (i % 3)];
-  for (int i = tid; i < NN; i += kThreads) sfix[i] = A.fix[sConn[i]];
+  for (int t = tid; t < nv * NN * 3; t += kThreads) {
+    const int j = t / (NN * 3), i = t - j * NN * 3;
+    X(j)[i] = A.X[3 * (int64_t)Conn(j)[i / 3] + (i % 3)];
+  }
+  for (int t = tid; t < nv * NN; t += kThreads) {
+    const int j = t / NN, i = t - j * NN;
+    Fix(j)[i] = A.fix[Conn(j)[i]];
+  }
   if (K32) {
-    for (int t = tid; t < NN * NN * 9; t += kThreads) {
-      const int q = t / 9;
+    for (int t = tid; t < nv * NN * NN * 9; t += kThreads) {
+      const int j = t / (NN * NN * 9), tt = t - j * NN * NN * 9, q = tt / 9;
       // a block this element writes first is not read
-      if (!(A.first && ((sFirst[q >> 5] >> (q & 31)) & 1u))) cp_async4(sKo + t, K32 + (int64_t)sSlot[q] * 9 + (t - 9 * q));
+      if (!(A.first && ((First(j)[q >> 5] >> (q & 31)) & 1u)))
+        cp_async4(Ko(j) + tt, K32 + (int64_t)Slot(j)[q] * 9 + (tt - 9 * q));
     }
     asm volatile("cp.async.commit_group;\n" ::);
   }
   __syncthreads();
   // Jacobians J[g][p][q] = sum_a dN_a/dxi_p X_a,q (cShapeSolid::DrvShpXYZ, shp/shpsolid.cpp:58-126)
-  for (int t = tid; t < NG * 9; t += kThreads) {
-    const int g = t / 9, pq = t - 9 * g, p = pq / 3, q = pq - 3 * p;
+  for (int t = tid; t < nv * NG * 9; t += kThreads) {
+    const int j = t / (NG * 9), tt = t - j * NG * 9;
+    const int g = tt / 9, pq = tt - 9 * g, p = pq / 3, q = pq - 3 * p;
     const double *d = sdN + g * NN * 3 + p;
+    const double *x = X(j);
     double s = 0.0;
 #pragma unroll 4
-    for (int a = 0; a < NN; a++) s += d[3 * a] * sX[3 * a + q];
-    sJ[t] = s;
+    for (int a = 0; a < NN; a++) s += d[3 * a] * x[3 * a + q];
+    Jm(j)[tt] = s;
   }
   __syncthreads();
   // determinant and inverse by cofactors (cShape::ShpMatInv, shp/shape.cpp:360-393)
-  for (int g = tid; g < NG; g += kThreads) {
-    double *J = sJ + 9 * g;
+  for (int t = tid; t < nv * NG; t += kThreads) {
+    const int j = t / NG, g = t - j * NG;
+    double *J = Jm(j) + 9 * g;
     const double j00 = J[0], j01 = J[1], j02 = J[2], j10 = J[3], j11 = J[4], j12 = J[5], j20 = J[6],
                  j21 = J[7], j22 = J[8];
     const double det = j00 * (j11 * j22 - j12 * j21) - j01 * (j10 * j22 - j12 * j20) + j02 * (j10 * j21 - j11 * j20);
@@ -267,22 +286,24 @@ __device__ bool tc_hex_element(const ElemArgs &A, float *__restrict__ K32, uint8
     J[6] = (j10 * j21 - j11 * j20) * id;
     J[7] = -(j00 * j21 - j01 * j20) * id;
     J[8] = (j00 * j11 - j01 * j10) * id;
-    sc[g] = sqrt(fmax(sw[g] * det, 0.0));
+    Cg(j)[g] = sqrt(fmax(sw[g] * det, 0.0));
   }
   __syncthreads();
-  // D[(i,a)][g] = sqrt(c_g) dN_a/dx_i, split into three TF32 operands
-  for (int t = tid; t < NG * NN; t += kThreads) {
-    const int g = t / NN, a = t - NN * g;
-    const double *J = sJ + 9 * g;
+  // D[(i,a)][g] = sqrt(c_g) dN_a/dx_i, split into three TF32 operands; element
+  // j on rows j*R .. j*R+R-1
+  for (int t = tid; t < nv * NG * NN; t += kThreads) {
+    const int j = t / (NG * NN), tt = t - j * NG * NN;
+    const int g = tt / NN, a = tt - NN * g;
+    const double *J = Jm(j) + 9 * g;
     const double *dn = sdN + (g * NN + a) * 3;
-    const double d0 = dn[0], d1 = dn[1], d2 = dn[2], sq = sc[g];
+    const double d0 = dn[0], d1 = dn[1], d2 = dn[2], sq = Cg(j)[g];
     const double x[3] = {sq * (J[0] * d0 + J[1] * d1 + J[2] * d2), sq * (J[3] * d0 + J[4] * d1 + J[5] * d2),
                          sq * (J[6] * d0 + J[7] * d1 + J[8] * d2)};
 #pragma unroll
     for (int i = 0; i < 3; i++) {
       uint32_t hi, lo, mid;
       tc::split3_tf32(x[i], hi, lo, mid);
-      const uint32_t off = tc::kmajor_off4(i * NN + a, g, KP);
+      const uint32_t off = tc::kmajor_off4(j * R + i * NN + a, g, KP);
       *reinterpret_cast<uint32_t *>(opHi + off) = hi;
       *reinterpret_cast<uint32_t *>(opLo + off) = lo;
       *reinterpret_cast<uint32_t *>(opMid + off) = mid;
@@ -311,30 +332,37 @@ __device__ bool tc_hex_element(const ElemArgs &A, float *__restrict__ K32, uint8
     return false;
   }
   tc::fence_after();
-  // accumulator -> H (lane = row (i, a), column = (j, b))
-  if (warp < 4 && warp * 32 < R) {
+  // accumulator -> H_j (lane = row j*R + (i, a), columns j*R + (j', b) of its own element)
+  if (warp < 4 && warp * 32 < nv * R) {
     const int r = warp * 32 + lane;
+    const int j = r / R, rr = r - j * R;
     const uint32_t tb = c.tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll 1
     for (int c0 = 0; c0 < N; c0 += 8) {
       float v[8];
       tc::ld_32x32b_x8(tb + c0, v);
-      if (r < R) {
+      if (r < nv * R) {
 #pragma unroll
-        for (int j = 0; j < 8; j++)
-          if (c0 + j < R) sH[r * R + c0 + j] = v[j];
+        for (int k = 0; k < 8; k++) {
+          const int col = c0 + k - j * R;
+          if (col >= 0 && col < R) H(j)[rr * R + col] = v[k];
+        }
       }
     }
   }
   tc::fence_before();
   __syncthreads();
-  if (tid < S::NP) {
+  for (int t = tid; t < nv * NP; t += kThreads) {
+    const int j = t / NP, pp = t - j * NP;
+    int pa, pb;
+    pair_of(pp, NN, pa, pb);
+    const float *Hj = H(j);
     double M[9];
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
-      for (int j = 0; j < 3; j++) M[3 * i + j] = (double)sH[(i * NN + pa) * R + j * NN + pb];
-    const double E = A.E[e], nu = A.nu[e];
+      for (int jj = 0; jj < 3; jj++) M[3 * i + jj] = (double)Hj[(i * NN + pa) * R + jj * NN + pb];
+    const double E = A.E[es[j]], nu = A.nu[es[j]];
     const double dd = (1.0 + nu) * (1.0 - 2.0 * nu);
     const double C00 = E * (1.0 - nu) / dd, C01 = E * nu / dd, G = 0.5 * E / (1.0 + nu);
     const double tr = M[0] + M[4] + M[8];
@@ -342,39 +370,52 @@ __device__ bool tc_hex_element(const ElemArgs &A, float *__restrict__ K32, uint8
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
-      for (int j = 0; j < 3; j++)
-        v[3 * i + j] = (i == j) ? C00 * M[4 * i] + G * (tr - M[4 * i]) : C01 * M[3 * i + j] + G * M[3 * j + i];
+      for (int jj = 0; jj < 3; jj++)
+        v[3 * i + jj] = (i == jj) ? C00 * M[4 * i] + G * (tr - M[4 * i]) : C01 * M[3 * i + jj] + G * M[3 * jj + i];
     if (A.Ke_out) {
       constexpr int ND = 3 * NN;
-      double *Ko = A.Ke_out + it * ND * ND;
+      double *Kout = A.Ke_out + its[j] * ND * ND;
 #pragma unroll
       for (int i = 0; i < 3; i++)
 #pragma unroll
-        for (int j = 0; j < 3; j++) {
-          Ko[(3 * pa + i) * ND + 3 * pb + j] = v[3 * i + j];
-          Ko[(3 * pb + j) * ND + 3 * pa + i] = v[3 * i + j];
+        for (int jj = 0; jj < 3; jj++) {
+          Kout[(3 * pa + i) * ND + 3 * pb + jj] = v[3 * i + jj];
+          Kout[(3 * pb + jj) * ND + 3 * pa + i] = v[3 * i + jj];
         }
     }
+    float *Vj = V(j);
 #pragma unroll
-    for (int k = 0; k < 9; k++) sV[9 * tid + k] = (float)v[k];
+    for (int k = 0; k < 9; k++) Vj[9 * pp + k] = (float)v[k];
   }
   if (K32) {
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
     // old + new for every entry whose two DOFs have equations (block (b, a)
     // is the transpose of (a, b)); first writes store new, fixed entries too
-    for (int t = tid; t < NN * NN * 9; t += kThreads) {
-      const int q = t / 9, k = t - 9 * q;
-      const int a = q / NN, b = q - NN * a, i = k / 3, j = k - 3 * i;
-      const bool fst = A.first && ((sFirst[q >> 5] >> (q & 31)) & 1u);
-      const bool fixed = ((sfix[a] >> i) & 1) || ((sfix[b] >> j) & 1);
-      const float add = (a <= b) ? sV[9 * (a * NN - a * (a - 1) / 2 + (b - a)) + k]
-                                 : sV[9 * (b * NN - b * (b - 1) / 2 + (a - b)) + 3 * j + i];
+    for (int t = tid; t < nv * NN * NN * 9; t += kThreads) {
+      const int j = t / (NN * NN * 9), tt = t - j * NN * NN * 9;
+      const int q = tt / 9, k = tt - 9 * q;
+      const int a = q / NN, b = q - NN * a, i = k / 3, jj = k - 3 * i;
+      const bool fst = A.first && ((First(j)[q >> 5] >> (q & 31)) & 1u);
+      const uint8_t *fx = Fix(j);
+      const bool fixed = ((fx[a] >> i) & 1) || ((fx[b] >> jj) & 1);
+      const float *Vj = V(j);
+      const float add = (a <= b) ? Vj[9 * (a * NN - a * (a - 1) / 2 + (b - a)) + k]
+                                 : Vj[9 * (b * NN - b * (b - 1) / 2 + (a - b)) + 3 * jj + i];
       float out;
-      if (entry_value(fst, fixed, a == b && i == j, fst ? 0.f : sKo[t], add, out)) K32[(int64_t)sSlot[q] * 9 + k] = out;
+      if (entry_value(fst, fixed, a == b && i == jj, fst ? 0.f : Ko(j)[tt], add, out))
+        K32[(int64_t)Slot(j)[q] * 9 + k] = out;
     }
   }
   return true;
+}
+
+// One element (the persistent kernel's unit of work)
+template <int NN, int NG>
+__device__ bool tc_hex_element(const ElemArgs &A, float *__restrict__ K32, uint8_t *sm, Cta &c, int64_t it,
+                               int64_t e) {
+  const int64_t its[1] = {it}, es[1] = {e};
+  return tc_hex_elements<NN, NG, 1>(A, K32, sm, c, its, es, 1);
 }
 
 }  // namespace tcb
