@@ -24,8 +24,13 @@ __global__ void __launch_bounds__(tcb::kThreads, tcb::BspTc<PR, PS, PT, NG1, LPC
   tcb::Cta c = tcb::cta_begin(S::TCOLS, bars, &tmem_sh, &fail_sh);
   tcb::tc_bsp_setup<PR, PS, PT, NG1, LPC>(sm);
   bool ok = true;
-  for (int64_t it = blockIdx.x; ok && it < A.ne; it += gridDim.x)
-    ok = tcb::tc_bsp_element<PR, PS, PT, NG1, LPC>(A, K32, sm, c, it, A.index ? (int64_t)A.index[it] : A.offset + it);
+  // A.split (1, or S::MT: the element's two tiles on two CTAs) parts per element
+  const int np = A.split > 1 ? S::MT : 1;
+  for (int64_t w = blockIdx.x; ok && w < A.ne * np; w += gridDim.x) {
+    const int64_t it = w / np;
+    ok = tcb::tc_bsp_element<PR, PS, PT, NG1, LPC>(A, K32, sm, c, it, A.index ? (int64_t)A.index[it] : A.offset + it,
+                                                  (int)(w - it * np), np);
+  }
   tcb::cta_end(c, S::TCOLS, A.status);
 }
 
@@ -42,8 +47,11 @@ cudaError_t run_bsp_tc(Ctx &c, ElemArgs a, int64_t count, float *K32) {
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   if (per_sm * S::TCOLS > 512) per_sm = 512 / S::TCOLS;
   per_sm = elem_per_sm(c, per_sm, a.ctas_per_sm);
-  int64_t grid = (int64_t)per_sm * c.sm_count;
-  if (grid > count) grid = count;
+  const int64_t slots = (int64_t)per_sm * c.sm_count;
+  // two-tile elements go to two CTAs each when a colour does not fill the GPU
+  a.split = (S::MT > 1 && count < slots) ? S::MT : 1;
+  int64_t grid = slots;
+  if (grid > count * a.split) grid = count * a.split;
   a.ne = count;
   kern<<<(unsigned)grid, tcb::kThreads, S::bytes, c.stream>>>(a, K32);
   c.launches++;

@@ -90,11 +90,14 @@ __device__ void tc_bsp_setup(uint8_t *sm) {
 
 // Element `it` of the launch (colour-sorted position e): its blocks into K32
 // (null: only the dense FP64 element matrix into A.Ke_out).  The chunks' MMAs
-// complete on barriers 0 and 1 (one per operand buffer).  False on a failed
-// wait, after the MMAs in flight have finished (bounded).
+// complete on barriers 0 and 1 (one per operand buffer).  With nparts = MT
+// (two 128-row tiles) the element is shared by two CTAs: part p forms and
+// scatters tile p only (the node pairs whose first node is in it), both
+// compute the element's geometry.  False on a failed wait, after the MMAs in
+// flight have finished (bounded).
 template <int PR, int PS, int PT, int NG1, int LPC>
 __device__ bool tc_bsp_element(const ElemArgs &A, float *__restrict__ K32, uint8_t *sm, Cta &c, int64_t it,
-                               int64_t e) {
+                               int64_t e, int part = 0, int nparts = 1) {
   using S = BspTc<PR, PS, PT, NG1, LPC>;
   constexpr int QR = S::QR, QS = S::QS, NN = S::NN, GCH = S::GCH, KC = S::KC, MT = S::MT, NB = S::NB;
   constexpr int ND = 3 * NN;
@@ -254,13 +257,16 @@ __device__ bool tc_bsp_element(const ElemArgs &A, float *__restrict__ K32, uint8
       const double d0 = D[a], d1 = D[NN + a], d2 = D[2 * NN + a], cg = sc[gl];
       const double x[3] = {J[0] * d0 + J[1] * d1 + J[2] * d2, J[3] * d0 + J[4] * d1 + J[5] * d2,
                            J[6] * d0 + J[7] * d1 + J[8] * d2};
+      const bool mine = nparts == 1 || ((4 * a) >> 7) == part;   // this part's A tile
 #pragma unroll
       for (int i = 0; i < 3; i++) {
         uint32_t pt[3];
-        tc::split3_tf32(cg * x[i], pt[0], pt[1], pt[2]);
-        const uint32_t oa = tc::kmajor_off4(4 * a + i, gl, KC);
+        if (mine) {
+          tc::split3_tf32(cg * x[i], pt[0], pt[1], pt[2]);
+          const uint32_t oa = tc::kmajor_off4(4 * a + i, gl, KC);
 #pragma unroll
-        for (int k = 0; k < 3; k++) *reinterpret_cast<uint32_t *>(aPart[k] + oa) = pt[k];
+          for (int k = 0; k < 3; k++) *reinterpret_cast<uint32_t *>(aPart[k] + oa) = pt[k];
+        }
         tc::split3_tf32(x[i], pt[0], pt[1], pt[2]);
         const uint32_t ob = tc::kmajor_off4(3 * a + i, gl, KC);
 #pragma unroll
@@ -275,6 +281,7 @@ __device__ bool tc_bsp_element(const ElemArgs &A, float *__restrict__ K32, uint8
       const uint32_t ub[3] = {tc::smem_u32(bPart[0]), tc::smem_u32(bPart[1]), tc::smem_u32(bPart[2])};
 #pragma unroll
       for (int t = 0; t < MT; t++) {
+        if (nparts > 1 && t != part) continue;
         const uint32_t d = c.tmem + t * S::TSTRIDE;
         const uint32_t toff = t * 16 * kSBO;   // 128 rows = 16 row groups
 #pragma unroll
@@ -304,7 +311,9 @@ __device__ bool tc_bsp_element(const ElemArgs &A, float *__restrict__ K32, uint8
   tc::fence_after();
 
   // epilogue: warp w reads tile w / 4, lanes 32 (w % 4) ..; row 4a + i
-  const int tile = warp >> 2, sub = warp & 3;
+  // (split: both warp quartets read the part's tile, even / odd column groups)
+  const int tile = nparts > 1 ? part : (warp >> 2), sub = warp & 3;
+  const int grp0 = nparts > 1 ? (warp >> 2) : 0, gstep = nparts > 1 ? 2 : 1;
   if (tile < MT) {
     const int row = tile * 128 + sub * 32 + lane;
     const int a = row >> 2, i = row & 3;
@@ -316,7 +325,7 @@ __device__ bool tc_bsp_element(const ElemArgs &A, float *__restrict__ K32, uint8
     const double C00 = E * (1.0 - nu) / dd, C01 = E * nu / dd, G = 0.5 * E / (1.0 + nu);
     const uint8_t fa = own ? sfix[a] : 0;
 #pragma unroll 1
-    for (int grp = 0; grp < S::NGRP; grp++) {
+    for (int grp = grp0; grp < S::NGRP; grp += gstep) {
       float h[24];
       tc::ld_32x32b_x8(taddr + grp * 24, h);
       tc::ld_32x32b_x8(taddr + grp * 24 + 8, h + 8);
