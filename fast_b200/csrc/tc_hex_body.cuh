@@ -30,9 +30,8 @@
 //
 // Per element (one CTA, 256 threads):
 //   1. one thread starts bulk copies (cp.async.bulk, completion on mbarrier
-//      0) of the element's incidence row, its NN x NN slot row and its
-//      first-touch flags; the natural-derivative table was brought in the
-//      same way by the bucket's set-up;
+//      0) of the elements' incidence rows, NN x NN slot rows and first-touch
+//      flags; the natural-derivative table is read through L1;
 //   2. coordinates are gathered, the element's current FP32 K blocks are
 //      requested with cp.async (they arrive while the element is computed);
 //   3. Jacobians, inverses and D in FP64; D is split and written as three
@@ -158,11 +157,13 @@ struct TcHex {
   static constexpr int FW = (NN * NN + 127) / 128 * 4;        // first-touch flag words (first_words)
   static constexpr int sSlot = al(NN * NN * 4), sConn = al(NN * 4), sFirst = FW * 4, sFix = al(NN);
   static constexpr int oHi = 0, oLo = oHi + OPB, oMid = oLo + OPB;
-  static constexpr int oH = oMid + OPB;                       // float [EPT][R][R]
-  static constexpr int oKo = oH + EPT * sH;                   // float [EPT][NN*NN][9] old blocks
+  // H is staged over the operands (dead once the MMAs completed); the next
+  // pass rewrites the operand rows it uses and zeroes their K padding
+  static constexpr int oH = 0;                                // float [EPT][R][R]
+  static constexpr int sOpH = 3 * OPB > EPT * sH ? 3 * OPB : EPT * sH;
+  static constexpr int oKo = sOpH;                            // float [EPT][NN*NN][9] old blocks
   static constexpr int oV = oKo + EPT * sKo;                  // float [EPT][NP][9] new blocks
-  static constexpr int odN = oV + EPT * sV;                   // double [NG][NN][3] (bulk-copy target)
-  static constexpr int ow = odN + al(NG * NN * 3 * 8);        // double [NG]
+  static constexpr int ow = oV + EPT * sV;                    // double [NG] (the natural derivatives stay in global memory, read through L1)
   static constexpr int oX = ow + al(NG * 8);                  // double [EPT][NN][3]
   static constexpr int oJ = oX + EPT * sX;                    // double [EPT][NG][9]
   static constexpr int oc = oJ + EPT * sJ;                    // double [EPT][NG]
@@ -171,30 +172,22 @@ struct TcHex {
   static constexpr int oFirst = oConn + EPT * sConn;          // uint32 [EPT][FW] (bulk-copy targets)
   static constexpr int oFix = oFirst + EPT * sFirst;          // uint8 [EPT][NN]
   static constexpr int used = oFix + EPT * sFix;
-  static_assert(odN % 16 == 0 && oSlot % 16 == 0 && oConn % 16 == 0 && oFirst % 16 == 0 && OPB % 16 == 0 &&
+  static_assert(oSlot % 16 == 0 && oConn % 16 == 0 && oFirst % 16 == 0 && OPB % 16 == 0 &&
                     sFirst % 16 == 0 && sSlot % 16 == 0 && sConn % 16 == 0,
                 "bulk-copy targets on 16-byte boundaries");
   static constexpr int bytes = used + 1024;                   // + alignment slack of the base
   static_assert(bytes <= 232448, "shared memory of one CTA");
 };
 
-// A hex bucket's set-up in a CTA: operands zeroed (the K padding, Gauss
-// points NG..KP-1, and rows past the last element stay zero), the Gauss
-// tables in shared memory (bulk copy on barrier 0).  False on a failed wait.
+// A hex bucket's set-up in a CTA: operands zeroed, the Gauss weights in
+// shared memory.  False on a failed wait.
 template <int NN, int NG, int EPT = 1>
 __device__ bool tc_hex_setup(const ElemArgs &A, uint8_t *sm, Cta &c) {
   using S = TcHex<NN, NG, EPT>;
   const int tid = threadIdx.x;
   for (int i = tid; i < 3 * S::OPB / 16; i += kThreads) reinterpret_cast<uint4 *>(sm + S::oHi)[i] = make_uint4(0, 0, 0, 0);
-  double *sdN = reinterpret_cast<double *>(sm + S::odN);
   double *sw = reinterpret_cast<double *>(sm + S::ow);
-  __syncthreads();
-  if (tid == 0) {
-    tc::mbar_arrive_tx(&c.bars[0], NG * NN * 3 * 8);
-    tc::bulk_g2s(sdN, A.dN, NG * NN * 3 * 8, &c.bars[0]);
-  }
-  for (int g = tid; g < NG; g += kThreads) sw[g] = A.w[g];  // 8 * NG bytes: not a bulk-copy size
-  wait_bar_drain(c, 0);
+  for (int g = tid; g < NG; g += kThreads) sw[g] = A.w[g];
   __syncthreads();
   return *c.fail == 0;
 }
@@ -210,7 +203,7 @@ __device__ bool tc_hex_elements(const ElemArgs &A, float *__restrict__ K32, uint
   using S = TcHex<NN, NG, EPT>;
   constexpr int R = S::R, KP = S::KP, N = S::N, NP = S::NP;
   uint8_t *opHi = sm + S::oHi, *opLo = sm + S::oLo, *opMid = sm + S::oMid;
-  double *sdN = reinterpret_cast<double *>(sm + S::odN);
+  const double *__restrict__ sdN = A.dN;   // [NG][NN][3], read through L1
   double *sw = reinterpret_cast<double *>(sm + S::ow);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   constexpr uint32_t kLBO = 128, kSBO = (KP / 4) * 128;
@@ -289,6 +282,16 @@ __device__ bool tc_hex_elements(const ElemArgs &A, float *__restrict__ K32, uint
     Cg(j)[g] = sqrt(fmax(sw[g] * det, 0.0));
   }
   __syncthreads();
+  // the K padding (Gauss points NG..KP-1) of the rows in use: zero (the last
+  // pass staged H over it)
+  if (KP > NG)
+    for (int t = tid; t < nv * R * (KP - NG); t += kThreads) {
+      const int r = t / (KP - NG), g = NG + (t - r * (KP - NG));
+      const uint32_t off = tc::kmajor_off4(r, g, KP);
+      *reinterpret_cast<uint32_t *>(opHi + off) = 0u;
+      *reinterpret_cast<uint32_t *>(opLo + off) = 0u;
+      *reinterpret_cast<uint32_t *>(opMid + off) = 0u;
+    }
   // D[(i,a)][g] = sqrt(c_g) dN_a/dx_i, split into three TF32 operands; element
   // j on rows j*R .. j*R+R-1
   for (int t = tid; t < nv * NG * NN; t += kThreads) {
