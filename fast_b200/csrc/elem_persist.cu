@@ -16,7 +16,8 @@
 //   * within a phase the CTAs take elements one at a time from an atomic
 //     counter, the segments of the heaviest element kinds first, so a CTA
 //     that drew a degree-3 B-spline element does not hold up the phase while
-//     others idle;
+//     others idle; an element of two 128-row tiles (degree 3) is two work
+//     items, one per tile;
 //   * a CTA keeps its tensor memory (the widest kind's columns), its two
 //     mbarriers and its shared memory across elements; when the next element
 //     is of another bucket it sets that bucket up (operands zeroed, Gauss
@@ -105,7 +106,12 @@ __device__ bool kind_setup(int k, const ElemArgs &A, uint8_t *sm, tcb::Cta &c) {
   }
 }
 
-__device__ bool kind_element(int k, const ElemArgs &A, float *K32, uint8_t *sm, tcb::Cta &c, int64_t e) {
+// CTAs that share one element of a kind: the two-tile B-spline kinds are
+// split by tile (each part forms and scatters one 128-row tile)
+__host__ __device__ constexpr int kind_parts(int k) { return (k == 8 || k == 9) ? 2 : 1; }
+static_assert(kind_parts(kBsp333G4) == 2 && kind_parts(kBsp332G4) == 2 && kind_parts(kBsp222G4) == 1, "parts");
+
+__device__ bool kind_element(int k, const ElemArgs &A, float *K32, uint8_t *sm, tcb::Cta &c, int64_t e, int part) {
   switch (k) {
     case kHex8G1: return tcb::tc_hex_element<8, 1>(A, K32, sm, c, 0, e);
     case kHex8G8: return tcb::tc_hex_element<8, 8>(A, K32, sm, c, 0, e);
@@ -115,8 +121,8 @@ __device__ bool kind_element(int k, const ElemArgs &A, float *K32, uint8_t *sm, 
     case kHex20G64: return tcb::tc_hex_element<20, 64>(A, K32, sm, c, 0, e);
     case kBsp222G3: return tcb::tc_bsp_element<2, 2, 2, 3, 3>(A, K32, sm, c, 0, e);
     case kBsp222G4: return tcb::tc_bsp_element<2, 2, 2, 4, 2>(A, K32, sm, c, 0, e);
-    case kBsp333G4: return tcb::tc_bsp_element<3, 3, 3, 4, 1>(A, K32, sm, c, 0, e);
-    case kBsp332G4: return tcb::tc_bsp_element<3, 3, 2, 4, 1>(A, K32, sm, c, 0, e);
+    case kBsp333G4: return tcb::tc_bsp_element<3, 3, 3, 4, 1>(A, K32, sm, c, 0, e, part, 2);
+    case kBsp332G4: return tcb::tc_bsp_element<3, 3, 2, 4, 1>(A, K32, sm, c, 0, e, part, 2);
     default: return false;
   }
 }
@@ -124,6 +130,7 @@ __device__ bool kind_element(int k, const ElemArgs &A, float *K32, uint8_t *sm, 
 struct PersistBucket {
   ElemArgs a;   // the bucket's arguments (first-touch flags, B-spline tables)
   int kind;
+  int parts;    // CTAs per element (kind_parts)
 };
 
 struct Barrier {
@@ -177,7 +184,7 @@ struct Plan {
   const int32_t *phase_seg;        // [nphase + 1] segment ranges of the phases
   const int32_t *seg_bucket;       // [nseg]
   const int64_t *seg_first;        // [nseg] first colour-sorted element
-  const int64_t *seg_count;        // [nseg]
+  const int64_t *seg_count;        // [nseg] work items: elements x parts
   const PersistBucket *buckets;    // [nbucket]
   unsigned int *counters;          // [nphase] elements handed out (zero at launch)
   Barrier *bar;                    // (zero at launch)
@@ -193,7 +200,7 @@ __global__ void __launch_bounds__(kThreads, 1) elem_persist_kernel(Plan P, uint3
   __shared__ int fail_sh, ok_sh;
   __shared__ long long item_sh;
   __shared__ ElemArgs args_sh;
-  __shared__ int kind_sh;
+  __shared__ int kind_sh, parts_sh;
   tcb::Cta c = tcb::cta_begin(cols, bars, &tmem_sh, &fail_sh);
   const int tid = threadIdx.x;
   int cur = -1;   // bucket set up in shared memory
@@ -215,12 +222,17 @@ __global__ void __launch_bounds__(kThreads, 1) elem_persist_kernel(Plan P, uint3
         if (tid == 0) {
           args_sh = P.buckets[b].a;
           kind_sh = P.buckets[b].kind;
+          parts_sh = P.buckets[b].parts;
         }
         __syncthreads();
         cur = b;
         if (!kind_setup(kind_sh, args_sh, sm, c)) { ok = false; break; }
       }
-      if (!kind_element(kind_sh, args_sh, P.K32, sm, c, P.seg_first[s] + item)) { ok = false; break; }
+      const int64_t el = item / parts_sh;
+      if (!kind_element(kind_sh, args_sh, P.K32, sm, c, P.seg_first[s] + el, (int)(item - el * parts_sh))) {
+        ok = false;
+        break;
+      }
     }
     if (!ok) {
       if (tid == 0) atomicExch(&P.bar->err, 1);
@@ -297,7 +309,7 @@ cudaError_t build_plan(Ctx &c, PersistPlanHost &H) {
       if (cnt <= 0) continue;
       seg_bucket.push_back(b);
       seg_first.push_back(B.color_off[k]);
-      seg_count.push_back(cnt);
+      seg_count.push_back(cnt * kind_parts(kind[b]));
     }
     phase_seg[p + 1] = (int32_t)seg_bucket.size();
   }
@@ -320,6 +332,7 @@ cudaError_t build_plan(Ctx &c, PersistPlanHost &H) {
     a.rational = B.rational;
     pb[b].a = a;   // first-touch flags are set per launch
     pb[b].kind = kind[b];
+    pb[b].parts = kind_parts(kind[b]);
   }
   // one allocation: buckets, counters + barrier, then the index arrays
   const size_t nseg = seg_bucket.size();
