@@ -167,7 +167,7 @@ extern "C" int fast_gpu_autotune(fast_gpu_ctx *c, fast_gpu_tune_report *rep) {
   ATK(cudaMemsetAsync(c->d_p, 0x3F, sizeof(double) * n4, c->stream));  // any finite vector
   ATK(cudaMemsetAsync(c->s_p, 0x3F, sizeof(float) * n4, c->stream));
   const int lanes[4] = {4, 8, 16, 32};
-  c->spmv32_bulk = c->spmv32_stream = false;   // the plain kernels first
+  c->spmv32_bulk = c->spmv32_stream = c->spmv32_c16 = false;   // the plain kernels first
   int best32 = c->lpr32, best64 = c->lpr64;
   double b32 = 1e300, b64 = 1e300;
   for (int i = 0; i < 4; i++) {
@@ -208,27 +208,33 @@ extern "C" int fast_gpu_autotune(fast_gpu_ctx *c, fast_gpu_tune_report *rep) {
     ATK(cudaMemsetAsync(c->d_f, 0x3F, sizeof(double) * n4, c->stream));
     const int64_t saved_p = c->persist_max_nodes;
     c->persist_max_nodes = 0;
-    struct Form { int lanes; bool stream, bulk; };
-    const Form forms[6] = {{8, false, false}, {16, false, false}, {8, true, false},
-                           {16, true, false}, {8, false, true}, {16, false, true}};
+    struct Form { int lanes; bool stream, bulk, c16; };
+    const Form forms[8] = {{8, false, false, false}, {16, false, false, false}, {8, true, false, false},
+                           {16, true, false, false}, {8, false, true, false},  {16, false, true, false},
+                           {8, false, false, true},  {16, false, false, true}};
+    const bool c16 = ensure_col16(*c) == cudaSuccess;   // rows spanning 65,536 nodes or more: not offered
+    (void)cudaGetLastError();
     constexpr int kIt = 64;
     double best = 1e300;
-    Form pick{best32, false, bulk};
-    for (int f = 0; f < 6; f++) {
-      if (forms[f].bulk && !tiles) continue;
+    Form pick{best32, false, bulk, false};
+    for (int f = 0; f < 8; f++) {
+      if ((forms[f].bulk && !tiles) || (forms[f].c16 && !c16)) continue;
       c->lpr32 = forms[f].lanes;
       c->spmv32_stream = forms[f].stream;
       c->spmv32_bulk = forms[f].bulk;
+      c->spmv32_c16 = forms[f].c16;
       c->drop_graphs();
       double ms = 0.0;
       ATK(median_ms(*c, [&] { return pcg_mixed(*c, false, 0.0, kIt, kIt); }, 3, ms));
-      R.us_iter_mixed[f] = ms * 1e3 / kIt;
+      (f < 6 ? R.us_iter_mixed[f] : R.us_iter_mixed_col16[f - 6]) = ms * 1e3 / kIt;
       if (ms < best) { best = ms; pick = forms[f]; }
     }
     c->persist_max_nodes = saved_p;
     best32 = pick.lanes;
     stream = pick.stream;
     bulk = pick.bulk;
+    c->spmv32_c16 = pick.c16;
+    R.col16_fp32 = pick.c16 ? 1 : 0;
   }
   c->spmv32_stream = stream;
   c->spmv32_bulk = bulk;

@@ -49,7 +49,8 @@ void free_mesh(Ctx &c) {
   c.buckets.clear();
   free_ties(c);
   free_face_loads(c);
-  dfree(c.d_X); dfree(c.d_fix); dfree(c.d_dof_of_eq);
+  dfree(c.d_X); dfree(c.d_fix); dfree(c.d_dof_of_eq); dfree(c.d_scol16); dfree(c.d_rowbase);
+  c.spmv32_c16 = false;
   dfree(c.d_rowptr); dfree(c.d_col); dfree(c.d_diag); dfree(c.d_srow); dfree(c.d_scol);
   dfree(c.d_tile_row);
   c.bulk_ntiles = 0;
@@ -214,7 +215,7 @@ int fast_gpu_set_option(fast_gpu_ctx *c, int32_t option, int64_t value) {
     if (value) CK(ensure_bulk_tiles(*c));
     c->drop_graphs();
     c->spmv32_bulk = value != 0;
-    if (value) c->spmv32_stream = false;
+    if (value) c->spmv32_stream = c->spmv32_c16 = false;
     return FAST_GPU_OK;
   }
   if (option == FAST_OPT_GRAPH_STEPS) {
@@ -227,7 +228,21 @@ int fast_gpu_set_option(fast_gpu_ctx *c, int32_t option, int64_t value) {
     CK(cudaStreamSynchronize(c->stream));
     c->drop_graphs();
     c->spmv32_stream = value != 0;
-    if (value) c->spmv32_bulk = false;
+    if (value) c->spmv32_bulk = c->spmv32_c16 = false;
+    return FAST_GPU_OK;
+  }
+  if (option == FAST_OPT_SPMV_COL16_FP32) {
+    if (value != 0 && value != 1) return FAST_GPU_EINVAL;
+    CK(cudaStreamSynchronize(c->stream));
+    if (value) {
+      if (!c->d_K) return FAST_GPU_ESTATE;
+      const cudaError_t e = ensure_col16(*c);
+      if (e == cudaErrorNotSupported) { c->err = "set_option: a block-row spans 65,536 nodes or more"; return FAST_GPU_ENOTSUP; }
+      CK(e);
+    }
+    c->drop_graphs();
+    c->spmv32_c16 = value != 0;
+    if (value) c->spmv32_bulk = c->spmv32_stream = false;
     return FAST_GPU_OK;
   }
   if (option == FAST_OPT_PERSISTENT_ASSEMBLY) {

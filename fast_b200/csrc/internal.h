@@ -237,6 +237,9 @@ struct Ctx {
   // (spmv_f32_bulk): its row tiles, their largest value / column bytes and grid
   bool spmv32_bulk = false;
   bool spmv32_stream = false;   // FP32 SpMV with cache-streaming matrix loads (8 or 16 lanes)
+  bool spmv32_c16 = false;      // FP32 SpMV with 16-bit column offsets (8 or 16 lanes)
+  uint16_t *d_scol16 = nullptr; // [nnzb_pad] column offsets from the row's smallest column
+  int32_t *d_rowbase = nullptr; // [nnode] that column
   // widest launch shape the element kernels could take since last reset
   // (read by the autotuner to bound its candidates)
   int elem_occ = 0, elem_split_max = 0;
@@ -379,6 +382,9 @@ cudaError_t launch_build_precond(Ctx &c, const double *K, int precond);
 cudaError_t launch_build_precond32(Ctx &c, const float *K32, int precond);
 // row tiles of the bulk-staged FP32 SpMV (once per pattern)
 cudaError_t ensure_bulk_tiles(Ctx &c);
+// 16-bit column offsets of the FP32 SpMV (once per pattern; not supported when
+// a block-row spans 65,536 nodes or more)
+cudaError_t ensure_col16(Ctx &c);
 // FP32 blocks -> the FP32 row-local SoA copy
 cudaError_t launch_to_soa32(Ctx &c, const float *K32, float *Ks32);
 // r = f - K u in FP64 without the assembled matrix: the small-strain internal

@@ -203,6 +203,61 @@ spmv_f32(int64_t nrows, const int32_t *__restrict__ srow, const int32_t *__restr
   }
 }
 
+// FP32 SpMV with 16-bit column indices: each block-row stores its columns as
+// offsets from the row's smallest column (every row of the mesh must span
+// fewer than 65,536 nodes), 38 instead of 40 bytes per block for the matrix
+// stream; otherwise spmv_f32<MODE, LPR> (the same sums in the same order).
+template <int LPR>
+__global__ void __launch_bounds__(kSpmvThreads, 4)
+spmv_f32_c16(int64_t nrows, const int32_t *__restrict__ srow, const uint16_t *__restrict__ scol16,
+             const int32_t *__restrict__ rowbase, const float *__restrict__ val, const float *__restrict__ x,
+             float *__restrict__ y, double *__restrict__ part, const int32_t *__restrict__ skip) {
+  if (skip && *skip) return;
+  __shared__ double sbuf[32];
+  constexpr int RPW = 32 / LPR;
+  const int lane = threadIdx.x & 31, q = lane % LPR;
+  const int64_t warp = (blockIdx.x * (int64_t)kSpmvThreads + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * kSpmvThreads) >> 5;
+  const float4 *__restrict__ x4 = reinterpret_cast<const float4 *>(x);
+  double pacc = 0.0;
+  for (int64_t row0 = warp * RPW; row0 < nrows; row0 += nwarps * RPW) {
+    const int64_t row = row0 + lane / LPR;
+    const bool live = row < nrows;
+    int32_t s0 = 0, nbp = 0, base = 0;
+    if (live) {
+      s0 = srow[row];
+      nbp = srow[row + 1] - s0;
+      base = rowbase[row];
+    }
+    const float *__restrict__ vr = val + 9 * (int64_t)s0;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+    for (int j = 4 * q; j < nbp; j += 4 * LPR) {
+      const ushort4 d = *reinterpret_cast<const ushort4 *>(scol16 + s0 + j);
+      float4 v[9];
+#pragma unroll
+      for (int k = 0; k < 9; k++) v[k] = *reinterpret_cast<const float4 *>(vr + k * nbp + j);
+      const float4 xa = x4[base + d.x], xb = x4[base + d.y], xc = x4[base + d.z], xd = x4[base + d.w];
+      a0 += v[0].x * xa.x + v[1].x * xa.y + v[2].x * xa.z + v[0].y * xb.x + v[1].y * xb.y + v[2].y * xb.z +
+            v[0].z * xc.x + v[1].z * xc.y + v[2].z * xc.z + v[0].w * xd.x + v[1].w * xd.y + v[2].w * xd.z;
+      a1 += v[3].x * xa.x + v[4].x * xa.y + v[5].x * xa.z + v[3].y * xb.x + v[4].y * xb.y + v[5].y * xb.z +
+            v[3].z * xc.x + v[4].z * xc.y + v[5].z * xc.z + v[3].w * xd.x + v[4].w * xd.y + v[5].w * xd.z;
+      a2 += v[6].x * xa.x + v[7].x * xa.y + v[8].x * xa.z + v[6].y * xb.x + v[7].y * xb.y + v[8].y * xb.z +
+            v[6].z * xc.x + v[7].z * xc.y + v[8].z * xc.z + v[6].w * xd.x + v[7].w * xd.y + v[8].w * xd.z;
+    }
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) {
+      a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+      a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+      a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+    }
+    if (live && q == 0) spmv_row_out<float, 0>(row, a0, a1, a2, x, nullptr, y, part != nullptr, pacc);
+  }
+  if (part) {
+    const double t = block_sum<kSpmvThreads>(pacc, sbuf);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+  }
+}
+
 // FP32 SpMV with the matrix streamed through shared memory.  In the
 // row-local SoA layout the values of consecutive block-rows are one
 // contiguous range (and so are their column indices), so a tile of rows
@@ -859,6 +914,31 @@ cudaError_t ensure_bulk_tiles(Ctx &c) {
   return cudaSuccess;
 }
 
+// 16-bit column offsets of the solve layout (once per pattern); not offered
+// when a block-row spans 65,536 nodes or more
+cudaError_t ensure_col16(Ctx &c) {
+  if (c.d_scol16) return cudaSuccess;
+  const int64_t n = c.nnode;
+  std::vector<int32_t> base((size_t)n);
+  std::vector<uint16_t> d16((size_t)c.nnzb_pad);
+  for (int64_t i = 0; i < n; i++) {
+    const int32_t s0 = c.h_srow[i], s1 = c.h_srow[i + 1];
+    int32_t lo = c.h_scol[s0];
+    for (int32_t k = s0; k < s1; k++) lo = std::min(lo, c.h_scol[k]);
+    base[(size_t)i] = lo;
+    for (int32_t k = s0; k < s1; k++) {
+      const int64_t d = (int64_t)c.h_scol[k] - lo;
+      if (d > 65535) return cudaErrorNotSupported;
+      d16[(size_t)k] = (uint16_t)d;
+    }
+  }
+  cudaError_t e = cudaMalloc((void **)&c.d_rowbase, sizeof(int32_t) * std::max<int64_t>(1, n));
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c.d_scol16, sizeof(uint16_t) * std::max<int64_t>(4, c.nnzb_pad));
+  if (e == cudaSuccess) e = cudaMemcpy(c.d_rowbase, base.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(c.d_scol16, d16.data(), sizeof(uint16_t) * c.nnzb_pad, cudaMemcpyHostToDevice);
+  return e;
+}
+
 // CTAs (= p.w partials) of the FP32 SpMV in use
 static int spmv32_parts(const Ctx &c) { return c.spmv32_bulk ? c.bulk_grid : spmv_grid(c); }
 
@@ -874,6 +954,13 @@ static void spmv32_go(const Ctx &c, int G, int64_t nn, const float *Ks, const fl
       spmv_f32_bulk<8><<<c.bulk_grid, kBulkThreads, smem, c.stream>>>(c.bulk_ntiles, c.d_tile_row, c.d_srow, c.d_scol, Ks,
                                                                        x, y, part, skip, c.d_status, c.bulk_vbytes,
                                                                        c.bulk_cbytes);
+    return;
+  }
+  if (c.spmv32_c16) {
+    if (c.lpr32 >= 16)
+      spmv_f32_c16<16><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol16, c.d_rowbase, Ks, x, y, part, skip);
+    else
+      spmv_f32_c16<8><<<G, kSpmvThreads, 0, c.stream>>>(nn, c.d_srow, c.d_scol16, c.d_rowbase, Ks, x, y, part, skip);
     return;
   }
   if (c.spmv32_stream) {

@@ -57,6 +57,7 @@ OPT_ELEM_SHAPE = 6
 OPT_ZERO_FILL = 7
 OPT_PERSISTENT_ASSEMBLY = 8
 OPT_SPMV_STREAM_FP32 = 9
+OPT_SPMV_COL16_FP32 = 10
 
 
 def elem_shape(bucket: int, ctas: int = 0, split: int = 0, tc_ctas: int = 0, kernel: int = 0) -> int:
@@ -204,7 +205,8 @@ class TuneReport(ctypes.Structure):
                 ("elem_ms_default", ctypes.c_double * 8), ("elem_ms_tuned", ctypes.c_double * 8),
                 ("elem_tc_ms_default", ctypes.c_double * 8), ("elem_tc_ms_tuned", ctypes.c_double * 8),
                 ("ms_fp32_stream", ctypes.c_double * 2), ("stream_fp32", ctypes.c_int32), ("reserved2", ctypes.c_int32),
-                ("us_iter_mixed", ctypes.c_double * 6), ("elem_kernel", ctypes.c_int32 * 8)]
+                ("us_iter_mixed", ctypes.c_double * 6), ("us_iter_mixed_col16", ctypes.c_double * 2),
+                ("col16_fp32", ctypes.c_int32), ("reserved3", ctypes.c_int32), ("elem_kernel", ctypes.c_int32 * 8)]
 
     def as_dict(self):
         return {"lanes_fp32": self.lanes_fp32, "lanes_fp64": self.lanes_fp64,
@@ -219,7 +221,9 @@ class TuneReport(ctypes.Structure):
                               "tc_ms_tuned": self.elem_tc_ms_tuned[b]} for b in range(self.elem_buckets)],
                 "elements_tensor_core_timed": bool(self.elem_tc),
                 "ms_fp32_stream_lanes_8_16": list(self.ms_fp32_stream), "stream_fp32": bool(self.stream_fp32),
-                "us_per_mixed_iteration_plain_8_16_stream_8_16_bulk_8_16": list(self.us_iter_mixed)}
+                "us_per_mixed_iteration_plain_8_16_stream_8_16_bulk_8_16": list(self.us_iter_mixed),
+                "us_per_mixed_iteration_col16_8_16": list(self.us_iter_mixed_col16),
+                "col16_fp32": bool(self.col16_fp32)}
 
 
 class ProblemReport(ctypes.Structure):

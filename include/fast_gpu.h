@@ -209,6 +209,10 @@ int         fast_gpu_synchronize(fast_gpu_ctx *ctx);
 #define FAST_OPT_SPMV_STREAM_FP32     9  /* 1: the FP32 SpMV loads the matrix with cache-streaming (evict-
                                             first) loads, 8 or 16 lanes per row; 0 (default until
                                             fast_gpu_autotune measures it): plain loads */
+#define FAST_OPT_SPMV_COL16_FP32     10  /* 1: the FP32 SpMV reads 16-bit column offsets from each row's
+                                            smallest column (38 instead of 40 bytes per block; every row
+                                            must span fewer than 65,536 nodes, else FAST_GPU_ENOTSUP);
+                                            0 (default until fast_gpu_autotune measures it): 32-bit */
 #define FAST_OPT_PERSISTENT_ASSEMBLY  8  /* 1: FAST_ASM_STIFFNESS_TF32 integrates the elements of every
                                             bucket in one persistent cooperative launch (colour k of
                                             every bucket is phase k, grid barriers between phases, CTAs
@@ -254,6 +258,9 @@ typedef struct {
   int32_t reserved2;
   double  us_iter_mixed[6];             /* mixed PCG per iteration with each FP32 form (the choice):
                                            8 / 16 lanes plain, cache-streaming, bulk-staged (0: not run) */
+  double  us_iter_mixed_col16[2];       /* the same with 16-bit column offsets, 8 / 16 lanes (0: not run) */
+  int32_t col16_fp32;                   /* 1: the 16-bit column offsets were kept                        */
+  int32_t reserved3;
   int32_t elem_kernel[8];               /* FP64 hex stiffness kernel chosen per bucket: 0 one CTA per
                                            element, 1 one warp per element                            */
 } fast_gpu_tune_report;

@@ -149,3 +149,23 @@ def test_warp_per_element_stiffness_matches_reference(ng):
 def fo_lower(K):
     import scipy.sparse as sp
     return sp.tril(K).tocsr()
+
+
+@pytest.mark.parametrize("lanes", [8, 16])
+def test_col16_spmv_gives_the_same_bits(lanes):
+    """FAST_OPT_SPMV_COL16_FP32: 16-bit column offsets from each row's smallest
+    column (rows of this box span far fewer than 65,536 nodes) give the same
+    gathers, so the mixed solve returns the same bits."""
+    d = decks.box_hex20_lognormal(10, 10, 5, seed=8)
+    f = gpu.face_load_vector(d)
+    s = gpu.GpuSystem(0)
+    s.set_option(gpu.OPT_PERSISTENT_MAX_NODES, 0)   # the kernels the option applies to
+    s.set_option(gpu.OPT_SPMV_LANES_FP32, lanes)
+    s.upload(d)
+    s.assemble()
+    u0, r0 = s.solve(f, tol=1e-10, precision=gpu.PREC_MIXED)
+    s.set_option(gpu.OPT_SPMV_COL16_FP32, 1)
+    u1, r1 = s.solve(f, tol=1e-10, precision=gpu.PREC_MIXED)
+    assert r0["converged"] and r1["iterations"] == r0["iterations"]
+    assert np.array_equal(u0, u1)
+    s.close()
