@@ -33,6 +33,8 @@ cudaError_t gemm_bf16(cudaStream_t s, int M, int N, int K, const float *A, int l
                       int ldaux, int32_t *status, float *ws = nullptr);
 int gemm_splits(int M, int N, int K, int epi);
 
+struct MlpRow;  // mlp_row.cuh
+
 // Fully connected tanh network: dims[0] -> dims[1] -> ... -> dims[L] with
 // tanh on the hidden layers and a linear output.  Parameters are FP32
 // (layer l: W_l [dims[l+1]][dims[l]] row-major, then b_l [dims[l+1]]).
@@ -58,6 +60,12 @@ struct Mlp {
   void release();
   // h[0] must hold the input rows; output in h[L]
   cudaError_t forward(cudaStream_t s, int batch);
+  // one row (batch 1) through the network on the CUDA cores by one CTA
+  // (mlp_row.cuh): h[0] row 0 -> h[L] row 0, one launch
+  cudaError_t forward_row(cudaStream_t s);
+  // the layer sizes and offsets the single-row forward reads; false when the
+  // network is deeper or wider than it takes
+  bool row_layout(MlpRow &r) const;
   // after forward: loss vs d_target (mean squared error), gradients in d_grads
   cudaError_t backward(cudaStream_t s, int batch);
   cudaError_t adam(cudaStream_t s, float lr, float beta1, float beta2, float eps);

@@ -24,6 +24,7 @@
 
 #include "internal.h"
 #include "learned.h"
+#include "mlp_row.cuh"
 
 namespace fastgpu {
 
@@ -362,6 +363,15 @@ uint64_t splitmix(uint64_t &x) {
   return z ^ (z >> 31);
 }
 
+// one input row (FP32, global) through the network by one CTA
+__global__ void __launch_bounds__(512) mlp_row_kernel(MlpRow m, const float *__restrict__ P,
+                                                      const float *__restrict__ x, float *__restrict__ y) {
+  __shared__ float in[kMlpRowMaxDim], tmp[kMlpRowMaxDim];
+  for (int t = threadIdx.x; t < m.dims[0]; t += blockDim.x) in[t] = bf16_round(x[t]);
+  __syncthreads();
+  mlp_row_forward(m, P, in, tmp, y);
+}
+
 }  // namespace
 
 int gemm_splits(int M, int N, int K, int epi) {
@@ -475,6 +485,29 @@ cudaError_t Mlp::forward(cudaStream_t s, int batch) {
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+bool Mlp::row_layout(MlpRow &r) const {
+  const int L = layers();
+  if (L < 1 || L > kMlpRowMaxLayers) return false;
+  r.L = L;
+  for (int l = 0; l <= L; l++) {
+    if (dims[l] > kMlpRowMaxDim) return false;
+    r.dims[l] = dims[l];
+  }
+  for (int l = 0; l < L; l++) {
+    r.w_off[l] = w_off[l];
+    r.b_off[l] = b_off[l];
+  }
+  return true;
+}
+
+cudaError_t Mlp::forward_row(cudaStream_t s) {
+  MlpRow r;
+  if (!row_layout(r)) return cudaErrorInvalidValue;
+  mlp_row_kernel<<<1, 512, 0, s>>>(r, d_params, d_h[0], d_h[layers()]);
+  launches++;
+  return cudaGetLastError();
 }
 
 cudaError_t Mlp::backward(cudaStream_t s, int batch) {

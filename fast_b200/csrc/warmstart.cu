@@ -25,6 +25,7 @@
 
 #include "internal.h"
 #include "learned.h"
+#include "mlp_row.cuh"
 
 using namespace fastgpu;
 
@@ -66,24 +67,6 @@ __global__ void ws_block_spmm(int64_t nnode, int k, const int32_t *__restrict__ 
   Y[(4 * i + 3) * k + m] = 0.0;
 }
 
-// u += Phi da
-__global__ void ws_add_phi(int32_t n, int k, const double *__restrict__ phi, const double *__restrict__ da,
-                           double *__restrict__ u) {
-  __shared__ double s[64];
-  if (threadIdx.x < k) s[threadIdx.x] = da[threadIdx.x];
-  __syncthreads();
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    double t = 0.0;
-    for (int m = 0; m < k; m++) t += phi[i * k + m] * s[m];
-    u[i] += t;
-  }
-}
-
-__global__ void ws_sub(int32_t n, const double *__restrict__ a, const double *__restrict__ b, double *__restrict__ out) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    out[i] = a[i] - b[i];
-}
-
 // network input from the coefficient ring: slot[j] holds a_{s-j} (-1: zero)
 struct FeatArgs {
   int k, kk, H;
@@ -91,29 +74,92 @@ struct FeatArgs {
   int slot[18];
 };
 
-__global__ void ws_features(FeatArgs a, const double *__restrict__ ring, const double *__restrict__ sigma,
-                            const double *__restrict__ delta, float *__restrict__ x) {
-  const int nin = 1 + a.H * a.kk;
-  for (int t = threadIdx.x; t < nin; t += blockDim.x) {
-    float v = 0.f;
-    if (t == 0) {
-      v = (float)a.lambda;
-    } else {
-      const int h = (t - 1) / a.kk, j = (t - 1) % a.kk;
-      if (j < a.k) {
-        // block 0: a_{s-1} / sigma;  block h >= 1: (a_{s-h} - a_{s-h-1}) / delta
-        const int sp = a.slot[h == 0 ? 1 : h], sq = a.slot[h + 1];
-        const double p = sp < 0 ? 0.0 : ring[sp * 64 + j];
-        if (h == 0) {
-          v = (float)(p / sigma[j]);
-        } else {
-          const double q = sq < 0 ? 0.0 : ring[sq * 64 + j];
-          v = (float)((p - q) / delta[j]);
-        }
-      }
-    }
-    x[t] = v;
+// input t of the network; the ring slot cur_slot is read from cur (shared
+// memory: the coefficients this block has just formed)
+__device__ float ws_feature(const FeatArgs &a, int t, const double *ring, int cur_slot, const double *cur,
+                            const double *__restrict__ sigma, const double *__restrict__ delta) {
+  if (t == 0) return (float)a.lambda;
+  const int h = (t - 1) / a.kk, j = (t - 1) % a.kk;
+  if (j >= a.k) return 0.f;
+  auto coef = [&](int sl) -> double {
+    if (sl < 0) return 0.0;
+    return sl == cur_slot ? cur[j] : __ldcg(ring + sl * 64 + j);
+  };
+  // block 0: a_{s-1} / sigma;  block h >= 1: (a_{s-h} - a_{s-h-1}) / delta
+  const double p = coef(a.slot[h == 0 ? 1 : h]);
+  if (h == 0) return (float)(p / sigma[j]);
+  return (float)((p - coef(a.slot[h + 1])) / delta[j]);
+}
+
+// what the last block of ws_project needs for the network step
+struct NetArgs {
+  FeatArgs f;
+  MlpRow m;
+  int cur_slot;
+  const float *params;
+  const double *ring, *sigma, *delta;
+  float *x;  // network input (kept for fast_gpu_ws_last_input)
+  float *y;  // network output
+};
+
+constexpr int kProjBlocks = 148, kProjThreads = 256;
+
+// out[m] = sum_i (a[i] - b[i]) Phi[i][m] for m < k (b may be null), Phi
+// [n][k] row-major.  A warp takes one row at a time (lane = mode), each block
+// a fixed set of rows; the last block to finish adds the block partials in
+// block order, so the sums do not depend on which block that is.  With
+// with_net that block goes on to build the network input from out and the
+// coefficient ring and runs the network (mlp_row.cuh).  The ticket is back
+// at 0 when the kernel ends.
+__global__ void __launch_bounds__(kProjThreads) ws_project(int32_t n, int k, const double *__restrict__ a,
+                                                           const double *__restrict__ b, const double *__restrict__ phi,
+                                                           double *part, unsigned int *ticket, double *out,
+                                                           int with_net, NetArgs na) {
+  constexpr int NW = kProjThreads / 32;
+  __shared__ double red[NW][64];
+  __shared__ double cur[64];
+  __shared__ float xin[kMlpRowMaxDim], tmp[kMlpRowMaxDim];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double s0 = 0.0, s1 = 0.0;
+#pragma unroll 4
+  for (int64_t r = (int64_t)blockIdx.x * NW + warp; r < n; r += (int64_t)gridDim.x * NW) {
+    const double v = b ? a[r] - b[r] : a[r];
+    const double *pr = phi + r * k;
+    if (lane < k) s0 = fma(v, pr[lane], s0);
+    if (lane + 32 < k) s1 = fma(v, pr[lane + 32], s1);
   }
+  red[warp][lane] = s0;
+  red[warp][lane + 32] = s1;
+  __syncthreads();
+  if (threadIdx.x < k) {
+    double t = 0.0;
+    for (int w = 0; w < NW; w++) t += red[w][threadIdx.x];
+    part[blockIdx.x * 64 + threadIdx.x] = t;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x < k) {
+    double t = 0.0;
+    for (unsigned g = 0; g < gridDim.x; g++) t += __ldcg(part + g * 64 + threadIdx.x);
+    cur[threadIdx.x] = t;
+    out[threadIdx.x] = t;
+  }
+  if (threadIdx.x == 0) *ticket = 0u;
+  if (!with_net) return;
+  __syncthreads();
+  const int nin = 1 + na.f.H * na.f.kk;
+  for (int t = threadIdx.x; t < nin; t += blockDim.x) {
+    const float v = ws_feature(na.f, t, na.ring, na.cur_slot, cur, na.sigma, na.delta);
+    na.x[t] = v;
+    xin[t] = bf16_round(v);
+  }
+  __syncthreads();
+  mlp_row_forward(na.m, na.params, xin, tmp, na.y);
 }
 
 // start = u_last + rho (u_last - u_prev) + Phi (tau * y)   (y: network output, or none)
@@ -184,25 +230,36 @@ __global__ void ws_chol(int k, const double *__restrict__ E, double *__restrict_
   if (threadIdx.x == 0) *ok = bad ? 0 : 1;
 }
 
-// da = Ainv t (Ainv from ws_chol), or 0 when the factor failed or |t| <= tol |tf|;
-// one warp, thread i forms row i
-__global__ void ws_reduced_solve(int k, const double *__restrict__ Ainv, const int32_t *__restrict__ ok,
-                                 const double *__restrict__ t, const double *__restrict__ tf, double tol,
-                                 double *__restrict__ da) {
-  const int lane = threadIdx.x;
-  double tn = 0.0, fn = 0.0;
-  for (int j = lane; j < k; j += 32) { tn += t[j] * t[j]; fn += tf[j] * tf[j]; }
+// da = Ainv t (Ainv from ws_chol), or 0 when the factor failed or |t| <= tol
+// |tf|, then u += Phi da.  Every block forms da itself (its first warp, lane i
+// row i: k <= 64 rows of k products); block 0 also stores it.
+__global__ void ws_reduced_add(int32_t n, int k, const double *__restrict__ Ainv, const int32_t *__restrict__ ok,
+                               const double *__restrict__ t, const double *__restrict__ tf, double tol,
+                               const double *__restrict__ phi, double *__restrict__ u, double *__restrict__ da_out) {
+  __shared__ double da[64];
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    double tn = 0.0, fn = 0.0;
+    for (int j = lane; j < k; j += 32) { tn += t[j] * t[j]; fn += tf[j] * tf[j]; }
 #pragma unroll
-  for (int m = 16; m > 0; m >>= 1) {
-    tn += __shfl_xor_sync(0xffffffffu, tn, m);
-    fn += __shfl_xor_sync(0xffffffffu, fn, m);
+    for (int m = 16; m > 0; m >>= 1) {
+      tn += __shfl_xor_sync(0xffffffffu, tn, m);
+      fn += __shfl_xor_sync(0xffffffffu, fn, m);
+    }
+    const bool skip = !*ok || !(sqrt(tn) > tol * sqrt(fn));
+    for (int i = lane; i < k; i += 32) {
+      double v = 0.0;
+      if (!skip)
+        for (int j = 0; j < k; j++) v += Ainv[i * k + j] * t[j];
+      da[i] = v;
+    }
   }
-  const bool skip = !*ok || !(sqrt(tn) > tol * sqrt(fn));
-  for (int i = lane; i < k; i += 32) {
+  __syncthreads();
+  if (blockIdx.x == 0 && threadIdx.x < k) da_out[threadIdx.x] = da[threadIdx.x];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double v = 0.0;
-    if (!skip)
-      for (int j = 0; j < k; j++) v += Ainv[i * k + j] * t[j];
-    da[i] = v;
+    for (int m = 0; m < k; m++) v += phi[i * k + m] * da[m];
+    u[i] += v;
   }
 }
 
@@ -261,7 +318,8 @@ struct fast_gpu_ws {
   double *d_Er = nullptr;        // [64*64] Phi^T K Phi
   double *d_L = nullptr;         // [64*64] its inverse (from the Cholesky factor)
   int32_t *d_ok = nullptr;
-  double *d_g = nullptr, *d_r = nullptr;  // [n]
+  double *d_g = nullptr;         // [n] internal force of the refined start
+  unsigned int *d_ticket = nullptr;       // finishing-block counter of ws_project
   double *d_skinny = nullptr;    // [kSkinnyBlocks][kSkinnyMaxOut] partials of the skinny products
   int64_t n_pred = 0, n_gal = 0;
   double pred_ms = 0.0;
@@ -286,6 +344,14 @@ struct fast_gpu_ws {
     if (e != cudaSuccess) return e;
     launches += dgemm_splits(M, N, K) > 1 ? 2 : 1;
     return dgemm(c->stream, M, N, K, A, lda, ta, B, ldb, tb, C, ldc, d_ws);
+  }
+  // out = Phi^T (a - b) (b may be null), one launch; with na the network
+  // step follows in the same launch
+  cudaError_t project(const double *a, const double *b, double *out, const NetArgs *na) {
+    launches++;
+    ws_project<<<kProjBlocks, kProjThreads, 0, c->stream>>>(n, k, a, b, d_phi, d_skinny, d_ticket, out,
+                                                            na ? 1 : 0, na ? *na : NetArgs{});
+    return cudaGetLastError();
   }
   cudaError_t atb(int64_t rows, int p, int q, const double *A, int lda, const double *B, int ldb, double *C,
                   int ldc) {
@@ -361,8 +427,9 @@ extern "C" int fast_gpu_ws_create(fast_gpu_ctx *ctx, const fast_gpu_ws_opts *opt
   if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_L, sizeof(double) * 64 * 64);
   if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_ok, sizeof(int32_t));
   if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_g, sizeof(double) * (size_t)w->n);
-  if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_r, sizeof(double) * (size_t)w->n);
   if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_skinny, sizeof(double) * kSkinnyBlocks * kSkinnyMaxOut);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&w->d_ticket, sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMemset(w->d_ticket, 0, sizeof(unsigned int));
   for (int i = 0; i < fast_gpu_ws::kRing; i++) w->ring_step[i] = -1;
   if (e != cudaSuccess) {
     ctx->err = std::string("ws_create: ") + cudaGetErrorString(e);
@@ -378,9 +445,10 @@ extern "C" void fast_gpu_ws_destroy(fast_gpu_ws *w) {
   if (w->c) cudaStreamSynchronize(w->c->stream);
   for (double *p : w->traj) cudaFree(p);
   for (double *p : {w->d_phi, w->d_ws, w->d_coef, w->d_delta, w->d_ring, w->d_scales, w->d_phin, w->d_Y, w->d_Er,
-                    w->d_L, w->d_g, w->d_r, w->d_skinny})
+                    w->d_L, w->d_g, w->d_skinny})
     if (p) cudaFree(p);
   if (w->d_ok) cudaFree(w->d_ok);
+  if (w->d_ticket) cudaFree(w->d_ticket);
   w->net.release();
   delete w;
 }
@@ -667,34 +735,39 @@ extern "C" int fast_gpu_ws_predict(void *user, int32_t step, double lambda, cons
   const float *y = nullptr;
   const int64_t span_net = c.begin_span(FAST_KERNEL_PREDICT_NET);
   if (w->use_network) {
-    // a_{s-1} = Phi^T u_last, a_{s-2} = Phi^T u_prev into the ring
+    Mlp &net = w->net;
+    WCK(net.reserve(1));
     const int s1 = (step - 1) % R, s2 = (step - 2) % R;
-    WCK(w->atb(n, 1, k, d_u_last, 1, w->d_phi, k, w->d_ring + s1 * 64, k));
-    w->ring_step[s1] = step - 1;
-    if (step - 2 >= 1) {
-      WCK(w->atb(n, 1, k, d_u_prev, 1, w->d_phi, k, w->d_ring + s2 * 64, k));
+    // a_{s-2} = Phi^T u_prev unless the ring has it from the last prediction
+    // (then it was that step's u_last)
+    if (step - 2 >= 1 && w->ring_step[s2] != step - 2) {
+      WCK(w->project(d_u_prev, nullptr, w->d_ring + s2 * 64, nullptr));
       w->ring_step[s2] = step - 2;
     }
-    FeatArgs fa{};
-    fa.k = k;
-    fa.kk = kk;
-    fa.H = H;
-    fa.lambda = lambda;
-    for (int j = 0; j < 18; j++) fa.slot[j] = -1;
+    NetArgs na{};
+    na.f.k = k;
+    na.f.kk = kk;
+    na.f.H = H;
+    na.f.lambda = lambda;
+    for (int j = 0; j < 18; j++) na.f.slot[j] = -1;
+    w->ring_step[s1] = step - 1;
     for (int j = 1; j <= H + 1 && j < 18; j++) {
       // a_{s-j}: zero before the first step; a step missing from the ring
       // repeats the closest earlier one that is there
       for (int st = step - j; st >= 1; st--)
-        if (w->ring_step[st % R] == st) { fa.slot[j] = st % R; break; }
+        if (w->ring_step[st % R] == st) { na.f.slot[j] = st % R; break; }
     }
-    Mlp &net = w->net;
-    WCK(net.reserve(1));
-    ws_features<<<1, 256, 0, c.stream>>>(fa, w->d_ring, w->d_scales, w->d_scales + 64, net.d_h[0]);
-    w->launches++;
-    const int64_t l0 = net.launches;
-    WCK(net.forward(c.stream, 1));
-    w->launches += net.launches - l0;
-    y = net.d_h[net.layers()];
+    if (!net.row_layout(na.m)) { c.err = "ws_predict: network too large for the single-row forward"; return FAST_GPU_EINVAL; }
+    na.cur_slot = s1;
+    na.params = net.d_params;
+    na.ring = w->d_ring;
+    na.sigma = w->d_scales;
+    na.delta = w->d_scales + 64;
+    na.x = net.d_h[0];
+    na.y = net.d_h[net.layers()];
+    // a_{s-1} = Phi^T u_last into the ring, then the network, in one launch
+    WCK(w->project(d_u_last, nullptr, w->d_ring + s1 * 64, &na));
+    y = na.y;
   }
   ws_start<<<148, 256, 0, c.stream>>>(n, k, rho, d_u_last, d_u_prev, w->d_phi, tau, y, d_u_pred);
   w->launches++;
@@ -713,19 +786,16 @@ extern "C" int fast_gpu_ws_predict(void *user, int32_t step, double lambda, cons
     WCK(w->atb(nrow, k, k, w->d_phin, k, w->d_Y, k, w->d_Er, k));
     ws_chol<<<1, 64, 0, c.stream>>>(k, w->d_Er, w->d_L, w->d_ok);
     w->launches++;
-    WCK(w->atb(n, 1, k, d_f, 1, w->d_phi, k, w->d_coef + 64, k));
+    WCK(w->project(d_f, nullptr, w->d_coef + 64, nullptr));  // Phi^T f
     fast_gpu_ctx *fc = static_cast<fast_gpu_ctx *>(w->c);
     for (int it = 0; it < w->gal_iters; it++) {
       int rc = fast_gpu_set_displacement_device(fc, d_u_pred);
       if (rc == FAST_GPU_OK) rc = fast_gpu_internal_force_device(fc, w->d_g);
       if (rc != FAST_GPU_OK) return rc;
-      ws_sub<<<148, 256, 0, c.stream>>>(n, d_f, w->d_g, w->d_r);
+      WCK(w->project(d_f, w->d_g, w->d_coef, nullptr));  // Phi^T (f - g)
+      ws_reduced_add<<<148, 256, 0, c.stream>>>(n, k, w->d_L, w->d_ok, w->d_coef, w->d_coef + 64, w->gal_tol,
+                                                w->d_phi, d_u_pred, w->d_delta);
       w->launches++;
-      WCK(w->atb(n, 1, k, w->d_r, 1, w->d_phi, k, w->d_coef, k));  // Phi^T r
-      ws_reduced_solve<<<1, 32, 0, c.stream>>>(k, w->d_L, w->d_ok, w->d_coef, w->d_coef + 64, w->gal_tol,
-                                                w->d_delta);
-      ws_add_phi<<<148, 256, 0, c.stream>>>(n, k, w->d_phi, w->d_delta, d_u_pred);
-      w->launches += 2;
       w->n_gal++;
     }
     WCK(cudaGetLastError());
@@ -810,7 +880,9 @@ extern "C" int fast_gpu_mlp_forward(fast_gpu_ws *w, int32_t batch, const float *
   WCK(cudaMemcpyAsync(net.d_h[0], x, sizeof(float) * (size_t)batch * net.dims[0], cudaMemcpyHostToDevice, c.stream));
   WCK(cudaMemsetAsync(net.d_status, 0, sizeof(int32_t), c.stream));
   const int64_t l0 = net.launches;
-  WCK(net.forward(c.stream, batch));
+  // a single row takes the CUDA-core form the predictor uses
+  if (batch == 1) WCK(net.forward_row(c.stream));
+  else WCK(net.forward(c.stream, batch));
   int32_t status = 0;
   WCK(cudaMemcpyAsync(y, net.d_h[net.layers()], sizeof(float) * (size_t)batch * net.dims.back(),
                       cudaMemcpyDeviceToHost, c.stream));

@@ -493,7 +493,10 @@ int fast_gpu_ws_get_samples(fast_gpu_ws *ws, float *x, float *t);
 int fast_gpu_ws_last_input(fast_gpu_ws *ws, float *x);
 
 /* The network alone (gradient checks against a CPU oracle).  Parameters are
- * FP32, per layer W [out][in] row-major then b [out]. */
+ * FP32, per layer W [out][in] row-major then b [out].  A batch of one row
+ * runs the single-CTA CUDA-core forward fast_gpu_ws_predict uses (the same
+ * BF16 operands and FP32 sums in another order); larger batches run the
+ * tcgen05 GEMMs of training. */
 int fast_gpu_mlp_params(fast_gpu_ws *ws, float *get, const float *set, int64_t *count);
 int fast_gpu_mlp_forward(fast_gpu_ws *ws, int32_t batch, const float *x, float *y);
 /* Mean squared error against t and its gradient with respect to every parameter. */

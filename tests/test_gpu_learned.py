@@ -92,6 +92,34 @@ def test_mlp_forward_and_gradients_match_oracle(system, small_plate, batch):
         p.close()
 
 
+@pytest.mark.parametrize("dims_key", ["129-256-256-32", "65-64-64-16"])
+def test_single_row_forward_matches_batched_forward(system, small_plate, dims_key):
+    """The single-row CUDA-core forward the predictor runs (batch 1) against
+    the tcgen05 batched forward of the same rows and the BF16-emulating
+    oracle; the same bits on every call."""
+    dims = [int(v) for v in dims_key.split("-")]
+    p = gpu.LearnedPredictor(system, modes=dims[-1], history=(dims[0] - 1) // dims[-1], width=dims[1],
+                             hidden=len(dims) - 2, seed=5)
+    try:
+        assert p.dims() == dims
+        net = mo.Mlp(dims)
+        rng = np.random.default_rng(9)
+        params = (rng.standard_normal(p.params().size) * 0.08).astype(np.float32)
+        p.params(set_to=params)
+        x = rng.standard_normal((6, dims[0])).astype(np.float32)
+        yb = p.forward(x)
+        ye = net.forward(params, x, emulate=True)[-1]
+        for i in range(x.shape[0]):
+            y1 = p.forward(x[i:i + 1])
+            # a BF16 rounding of a hidden activation may flip between the two
+            # summation orders, as it does against the oracle
+            assert rel(y1[0], yb[i]) < 1e-4, i
+            assert rel(y1[0], ye[i]) < 1e-4, i
+            assert np.array_equal(y1, p.forward(x[i:i + 1]))
+    finally:
+        p.close()
+
+
 def test_pod_basis_matches_dense_svd(system, small_plate, predictor):
     d, q = small_plate
     p, info = predictor
