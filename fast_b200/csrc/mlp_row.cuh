@@ -20,6 +20,7 @@ namespace fastgpu {
 
 constexpr int kMlpRowMaxLayers = 9;
 constexpr int kMlpRowMaxDim = 1025;  // 1 + history 16 x 64 modes; hidden width <= 1024
+constexpr int kMlpRowUnroll = 8;     // inputs per lane per trip
 
 // layer sizes and parameter offsets (layer l: W_l [dims[l+1]][dims[l]]
 // row-major at w_off[l], b_l at b_off[l])
@@ -44,16 +45,26 @@ __device__ inline void mlp_row_forward(const MlpRow &m, const float *__restrict_
     const float *W = P + m.w_off[l];
     const float *bias = P + m.b_off[l];
     for (int j0 = 4 * warp; j0 < fo; j0 += 4 * nw) {
-      // four outputs per warp at a time: four independent loads per input
+      // four outputs per warp at a time, eight inputs per lane per trip: all
+      // 32 weight loads of a trip are in flight together (L2 latency, not
+      // bandwidth, bounds one CTA); the sums run over k in increasing order
       const float *w0 = W + (int64_t)j0 * fi;
       float acc[4] = {0.f, 0.f, 0.f, 0.f};
       const int nr = min(4, fo - j0);
-#pragma unroll 2
-      for (int k = lane; k < fi; k += 32) {
-        const float x = a[k];
+      for (int k0 = 0; k0 < fi; k0 += 32 * kMlpRowUnroll) {
+        float wv[4][kMlpRowUnroll], xv[kMlpRowUnroll];
 #pragma unroll
-        for (int r = 0; r < 4; r++)
-          if (r < nr) acc[r] = fmaf(bf16_round(__ldg(w0 + (int64_t)r * fi + k)), x, acc[r]);
+        for (int u = 0; u < kMlpRowUnroll; u++) {
+          const int k = k0 + 32 * u + lane;
+          const bool in = k < fi;
+          xv[u] = in ? a[k] : 0.f;
+#pragma unroll
+          for (int r = 0; r < 4; r++) wv[r][u] = (in && r < nr) ? __ldg(w0 + (int64_t)r * fi + k) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < kMlpRowUnroll; u++)
+#pragma unroll
+          for (int r = 0; r < 4; r++) acc[r] = fmaf(bf16_round(wv[r][u]), xv[u], acc[r]);
       }
 #pragma unroll
       for (int r = 0; r < 4; r++)
