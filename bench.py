@@ -252,7 +252,8 @@ def newton_plate(local, args):
       secant:  secant start, mixed-precision PCG, inexact Newton;
       learned: the learned start (POD + MLP trained on 64 seeded
                pressure/stiffness variants, one POD-Galerkin correction),
-               mixed-precision PCG, inexact Newton.
+               mixed-precision PCG, inexact Newton;
+      learned, network only: the same without the Galerkin correction.
     Each solve is timed 3 times (minimum reported); training is timed once."""
     from fast_b200 import decks, gpu, learned
     d = decks.plate_tl_hex8(40, 40, 4, L=10.0, t=1.0, pressure=40.0, steps=40, tol=1e-8)
@@ -268,7 +269,11 @@ def newton_plate(local, args):
         "secant_mixed": dict(predictor=gpu.PREDICT_SECANT, precision=gpu.PREC_MIXED, lin_tol=1e-10,
                              lin_tol_rel=1e-3),
         "learned_mixed": dict(learned=pred, precision=gpu.PREC_MIXED, lin_tol=1e-10, lin_tol_rel=1e-3),
+        "learned_mixed_network_only": dict(learned=pred, precision=gpu.PREC_MIXED, lin_tol=1e-10,
+                                           lin_tol_rel=1e-3),
     }
+    # Galerkin corrections of the learned start per run (the network-only run has none)
+    galerkin = {"learned_mixed": 1, "learned_mixed_network_only": 0}
     times = {k: [] for k in runs}
     out = {}
     clocks = ClockSampler(local)
@@ -276,6 +281,8 @@ def newton_plate(local, args):
     n0 = S.launch_count()
     for rep in range(3):
         for k, kw in runs.items():
+            if k in galerkin:
+                pred.configure(use_network=True, galerkin_iters=galerkin[k], galerkin_tol=1e-3)
             t = time.perf_counter()
             h, it, r = S.nr_solve(q, 40, 1.0 / 40, tol=1e-8, max_iter=30, **kw)
             times[k].append(time.perf_counter() - t)
@@ -291,6 +298,7 @@ def newton_plate(local, args):
         t_nog.append(time.perf_counter() - t)
     S.set_option(gpu.OPT_GRAPH_STEPS, 1)
     # the predictor's two phases per load step (live spans, one learned run)
+    pred.configure(use_network=True, galerkin_iters=1, galerkin_tol=1e-3)
     S.kernel_timing(True)
     S.nr_solve(q, 40, 1.0 / 40, tol=1e-8, max_iter=30, **runs["learned_mixed"])
     S.synchronize()
@@ -333,6 +341,7 @@ def newton_plate(local, args):
         "speedup_learned_vs_plain": res["plain_fp64"]["ms"] / res["learned_mixed"]["ms"],
         "speedup_secant_vs_plain": res["plain_fp64"]["ms"] / res["secant_mixed"]["ms"],
         "speedup_learned_vs_secant": res["secant_mixed"]["ms"] / res["learned_mixed"]["ms"],
+        "speedup_learned_network_only_vs_secant": res["secant_mixed"]["ms"] / res["learned_mixed_network_only"]["ms"],
         "secant_mixed_without_graphs_ms": min(t_nog) * 1e3,
         "predictor": pred_ms,
         "training": {"seconds": train_s, "variants": info["converged_variants"], "samples": rep["samples"],
@@ -674,6 +683,31 @@ def run_reference(args):
     return 0
 
 
+def spmv_kernel_name(tune, which):
+    """The SpMV form the autotuner left in place for the timed solve."""
+    if which != gpu_const("KERNEL_SPMV_FP32"):
+        return "spmv_f64<0, %d> (FP64 PCG K.p)" % tune["lanes_fp64"]
+    if tune.get("col16_fp32"):
+        return "spmv_f32_c16<%d> (FP32 PCG K.p, 16-bit column offsets)" % tune["lanes_fp32"]
+    if tune.get("bulk_fp32"):
+        return "spmv_f32_bulk<%d> (FP32 PCG K.p, bulk-staged)" % tune["lanes_fp32"]
+    if tune.get("stream_fp32"):
+        return "spmv_f32<0, %d, 1> (FP32 PCG K.p, streamed matrix loads)" % tune["lanes_fp32"]
+    return "spmv_f32<0, %d> (FP32 PCG K.p)" % tune["lanes_fp32"]
+
+
+def spmv_profile_file(tune, which):
+    """The ncu summary under profiles/ that holds the DRAM traffic of that form."""
+    if which != gpu_const("KERNEL_SPMV_FP32"):
+        return "spmv_soa_fp64_hex20_64x64x32.txt"
+    return "spmv_c16_fp32_hex20_64x64x32.txt" if tune.get("col16_fp32") else "spmv_soa_fp32_hex20_64x64x32.txt"
+
+
+def gpu_const(name):
+    from fast_b200 import gpu
+    return getattr(gpu, name)
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -829,8 +863,7 @@ def run_ours(args):
     achieved = k_bytes / (k_ms / 1e3) / 1e9 if k_ms > 0 else 0.0
     a_gbs = a_bytes / (a_ms / 1e3) / 1e9 if a_ms > 0 else 0.0
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "spmv_soa_fp32_hex20_64x64x32.txt" if spmv_which == gpu.KERNEL_SPMV_FP32
-                      else "spmv_soa_fp64_hex20_64x64x32.txt")
+    tp = os.path.join(ROOT, "profiles", spmv_profile_file(tune, spmv_which))
     if os.path.exists(tp):
         for ln in open(tp):
             if ln.startswith("dram_bytes_per_launch:"):
@@ -906,8 +939,7 @@ def run_ours(args):
             "config": workload_config(args, neq),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic,
-                         "kernel": "spmv_soa<float,float> (FP32 PCG K.p)" if spmv_which == gpu.KERNEL_SPMV_FP32
-                         else "spmv_soa<double,double> (FP64 PCG K.p)",
+                         "kernel": spmv_kernel_name(tune, spmv_which),
                          "bytes_per_launch": k_bytes, "ms_per_launch": k_ms, "launches_timed": k_n,
                          "spans_timed": k_span,
                          "peak_kind": hbm_kind},

@@ -69,6 +69,45 @@ cudaError_t launch_bsp_elements(Ctx &c, const Bucket &B, ElemArgs a, int64_t cou
 // internal force (mode 0 both, 1 tangent, 2 force), small-strain internal force
 cudaError_t launch_bsp_tl(Ctx &c, const Bucket &B, ElemArgs a, int64_t count, int mode);
 
+// The entries (element j, block q = a NN + b of its NN x NN node-pair grid,
+// entry k of the 3x3 block) of a CTA's elements, walked with k fixed per
+// thread: thread t < 9 QS takes entry k = t % 9 of the blocks t / 9,
+// t / 9 + QS, ... (q counted over all elements, element-major).  Consecutive
+// threads take consecutive entries, as a plain t, t + NT, ... walk over 9 q +
+// k would, but the block, element and node indices advance by additions
+// instead of divisions per entry.
+template <int NN, int NT>
+struct BlockWalk {
+  static constexpr int QS = NT / 9;  // blocks per trip
+  static_assert(QS / NN + 1 <= NN, "one carry per step");
+  int k, q, j, a, b;
+  __device__ __forceinline__ explicit BlockWalk(int t) {
+    k = t % 9;
+    q = t / 9;
+    j = q / (NN * NN);
+    const int qq = q - j * NN * NN;
+    a = qq / NN;
+    b = qq - NN * a;
+  }
+  __device__ __forceinline__ static bool takes(int t) { return t < 9 * QS; }
+  __device__ __forceinline__ int qq() const { return a * NN + b; }
+  __device__ __forceinline__ void next() {
+    q += QS;
+    b += QS % NN;
+    a += QS / NN;
+    if (b >= NN) { b -= NN; a++; }
+    if (a >= NN) { a -= NN; j++; }
+  }
+};
+
+// 9 x the index of the upper-triangle pair (min(a,b), max(a,b)) plus the
+// entry k (a <= b) or its transpose kt (a > b): where a node-pair block of
+// the element sits among the blocks stored for a <= b
+template <int NN>
+__device__ __forceinline__ int upper_entry(int a, int b, int k, int kt) {
+  return a <= b ? 9 * (a * NN - a * (a - 1) / 2 + (b - a)) + k : 9 * (b * NN - b * (b - 1) / 2 + (a - b)) + kt;
+}
+
 // (a, b) pair index -> a <= b, row-major over the upper triangle
 __device__ __forceinline__ void pair_of(int p, int n, int &a, int &b) {
   int r = 0;

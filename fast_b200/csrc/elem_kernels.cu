@@ -116,13 +116,13 @@ __global__ void __launch_bounds__(NT, (NT >= 128 ? 3 : 8)) elem_kernel(ElemArgs 
     bool fab = false, fba = false;
     if (S::STAGE && A.K) {
       const int32_t *es = A.slot + e * NN * NN;
-      for (int t = tid; t < NN * NN * 9; t += NT) {
-        const int q = t / 9, k = t - 9 * q;
-        const int32_t sl = es[q];
-        const bool fst = first_touch(A, e, q);
-        if (k == 0) sSlot[q] = fst ? ~sl : sl;
-        if (!fst) cp_async8(sKo + t, A.K + (int64_t)sl * 9 + k);
-      }
+      if (BlockWalk<NN, NT>::takes(tid))
+        for (BlockWalk<NN, NT> w(tid); w.q < NN * NN; w.next()) {
+          const int32_t sl = es[w.q];
+          const bool fst = first_touch(A, e, w.q);
+          if (w.k == 0) sSlot[w.q] = fst ? ~sl : sl;
+          if (!fst) cp_async8(sKo + 9 * w.q + w.k, A.K + (int64_t)sl * 9 + w.k);
+        }
       cp_async_commit();
     } else if (A.K && tid < NP) {
       Kab = A.K + (int64_t)A.slot[(e * NN + pa) * NN + pb] * 9;
@@ -262,17 +262,18 @@ __global__ void __launch_bounds__(NT, (NT >= 128 ? 3 : 8)) elem_kernel(ElemArgs 
       __syncthreads();
       // old + new for every entry whose two DOFs have equations (first
       // writes: new, and the fixed entries too)
-      for (int t = tid; t < NN * NN * 9; t += NT) {
-        const int q = t / 9, k = t - 9 * q;
-        const int a = q / NN, b = q - NN * a, i = k / 3, j = k - 3 * i;
-        const int32_t s0 = sSlot[q];
-        const bool fst = s0 < 0;
-        const bool fixed = ((sfix[a] >> i) & 1) || ((sfix[b] >> j) & 1);
-        const double add = (a <= b) ? sV[9 * (a * NN - a * (a - 1) / 2 + (b - a)) + k]
-                                    : sV[9 * (b * NN - b * (b - 1) / 2 + (a - b)) + 3 * j + i];
-        double out;
-        if (entry_value(fst, fixed, a == b && i == j, fst ? 0.0 : sKo[t], add, out))
-          A.K[(int64_t)(fst ? ~s0 : s0) * 9 + k] = out;
+      if (BlockWalk<NN, NT>::takes(tid)) {
+        BlockWalk<NN, NT> w(tid);
+        const int k = w.k, i = k / 3, j = k - 3 * i, kt = 3 * j + i;
+        for (; w.q < NN * NN; w.next()) {
+          const int32_t s0 = sSlot[w.q];
+          const bool fst = s0 < 0;
+          const bool fixed = ((sfix[w.a] >> i) & 1) || ((sfix[w.b] >> j) & 1);
+          const double add = sV[upper_entry<NN>(w.a, w.b, k, kt)];
+          double out;
+          if (entry_value(fst, fixed, w.a == w.b && i == j, fst ? 0.0 : sKo[9 * w.q + k], add, out))
+            A.K[(int64_t)(fst ? ~s0 : s0) * 9 + k] = out;
+        }
       }
     }
   }

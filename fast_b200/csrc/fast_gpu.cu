@@ -1033,7 +1033,10 @@ int fast_gpu_kernel_stats(fast_gpu_ctx *c, int32_t which, int64_t *launches, dou
     // SpMV: block values + column indices + row pointers + x read once + y written once
     // (the padding blocks of the solve layout are not counted: they are overhead)
     if (which == FAST_KERNEL_SPMV_FP64) algo = (double)c->nnzb * (9 * 8 + 4) + 4.0 * (c->nnode + 1) + 2.0 * 8 * n4;
-    if (which == FAST_KERNEL_SPMV_FP32) algo = (double)c->nnzb * (9 * 4 + 4) + 4.0 * (c->nnode + 1) + 2.0 * 4 * n4;
+    // (16-bit column offsets: 2 bytes per block plus a 4-byte base per row)
+    if (which == FAST_KERNEL_SPMV_FP32)
+      algo = c->spmv32_c16 ? (double)c->nnzb * (9 * 4 + 2) + 4.0 * (c->nnode + 1) + 4.0 * c->nnode + 2.0 * 4 * n4
+                           : (double)c->nnzb * (9 * 4 + 4) + 4.0 * (c->nnode + 1) + 2.0 * 4 * n4;
     if (which == FAST_KERNEL_ASSEMBLE || which == FAST_KERNEL_ASSEMBLE_TF32) {
       // scatter model per element: incidence + coordinates + fixity + E, nu + slot map + 3x3 block
       // read-modify-write (72-byte FP64 or 36-byte FP32 blocks), plus the zero fill of the block

@@ -125,7 +125,7 @@ __global__ void nr_collect(const double *__restrict__ sums, const PcgState *__re
 
 struct NrWork {
   double *q = nullptr, *f = nullptr, *g = nullptr, *r = nullptr, *u = nullptr, *du = nullptr, *up = nullptr,
-         *ucand = nullptr, *part = nullptr, *sums = nullptr, *hsums = nullptr;
+         *ucand = nullptr, *gsave = nullptr, *part = nullptr, *sums = nullptr, *hsums = nullptr;
   double *par = nullptr;                 // [3] linear tolerance, 1/|r|, |r|
   NrIterOut *d_out = nullptr, *h_out = nullptr;
   cudaGraphExec_t graph = nullptr;       // one Newton iteration, captured
@@ -250,7 +250,7 @@ extern "C" int fast_gpu_nr_solve(fast_gpu_ctx *c, const double *q_host, const fa
   if (n <= 0) return FAST_GPU_EINVAL;
   {
     cudaError_t e = cudaSuccess;
-    double **bufs[] = {&w.q, &w.f, &w.g, &w.r, &w.u, &w.du, &w.up, &w.ucand};
+    double **bufs[] = {&w.q, &w.f, &w.g, &w.r, &w.u, &w.du, &w.up, &w.ucand, &w.gsave};
     for (double **b : bufs)
       if (e == cudaSuccess) e = cudaMalloc((void **)b, nb);
     if (e == cudaSuccess) e = cudaMalloc((void **)&w.part, sizeof(double) * 2 * kNrBlocks);
@@ -275,37 +275,56 @@ extern "C" int fast_gpu_nr_solve(fast_gpu_ctx *c, const double *q_host, const fa
     // start of the step: the last converged u (the reference), the secant
     // extrapolation 2 u_k - u_{k-1} (equal load steps), or the caller's
     // prediction when its residual is smaller than the secant start's
+    // Each candidate start is evaluated once: the chosen one's displacement
+    // (set on the device), g, r = f - g and norms (w.sums: |r|^2, |f|^2) are
+    // kept for the first iteration instead of being formed again.
     NRCK(cudaMemcpyAsync(w.ucand, w.u, nb, cudaMemcpyDeviceToDevice, c->stream));
+    bool have_r = false;
     if (step >= 2 && o->predictor != FAST_NR_PREDICT_NONE) {
       NRCK(axpby(*c, 2.0, w.u, -1.0, w.up, w.ucand));
       NRRC(fast_gpu_set_displacement_device(c, w.ucand));
       NRRC(fast_gpu_internal_force_device(c, w.g));
       NRCK(axpby(*c, 1.0, w.f, -1.0, w.g, w.r));
-      NRCK(norms2(*c, w, w.r, nullptr, &best, nullptr));
+      NRCK(norms2(*c, w, w.r, w.f, &best, &flen2));
+      rlen2 = best;
+      have_r = true;
       R.secant_starts++;
       if (o->predictor == FAST_NR_PREDICT_CALLBACK && predictor) {
         // the caller writes its prediction of u at this load level into du
+        NRCK(cudaMemcpyAsync(w.gsave, w.g, nb, cudaMemcpyDeviceToDevice, c->stream));
         const int prc = predictor(predictor_user, step, lam, w.u, w.up, w.f, w.du);
         if (prc == 0) {
           NRRC(fast_gpu_set_displacement_device(c, w.du));
           NRRC(fast_gpu_internal_force_device(c, w.g));
           NRCK(axpby(*c, 1.0, w.f, -1.0, w.g, w.r));
           double rl = 0.0;
-          NRCK(norms2(*c, w, w.r, nullptr, &rl, nullptr));
+          NRCK(norms2(*c, w, w.r, w.f, &rl, &flen2));
           R.predictions++;
           if (rl < best) {
             R.predictions_accepted++;
+            rlen2 = rl;
             NRCK(cudaMemcpyAsync(w.ucand, w.du, nb, cudaMemcpyDeviceToDevice, c->stream));
+          } else {
+            // back to the secant start's state
+            NRCK(cudaMemcpyAsync(w.g, w.gsave, nb, cudaMemcpyDeviceToDevice, c->stream));
+            NRCK(axpby(*c, 1.0, w.f, -1.0, w.g, w.r));
+            NRRC(fast_gpu_set_displacement_device(c, w.ucand));
+            NRCK(norms2(*c, w, w.r, w.f, &rlen2, &flen2));
           }
+        } else {
+          // the predictor's own evaluations may have moved the displacement
+          NRRC(fast_gpu_set_displacement_device(c, w.ucand));
         }
       }
     }
     NRCK(cudaMemcpyAsync(w.up, w.u, nb, cudaMemcpyDeviceToDevice, c->stream));  // last converged
     NRCK(cudaMemcpyAsync(w.u, w.ucand, nb, cudaMemcpyDeviceToDevice, c->stream));
-    NRRC(fast_gpu_set_displacement_device(c, w.u));
-    NRRC(fast_gpu_internal_force_device(c, w.g));
-    NRCK(axpby(*c, 1.0, w.f, -1.0, w.g, w.r));  // r = f - g
-    NRCK(norms2(*c, w, w.r, w.f, &rlen2, &flen2));
+    if (!have_r) {
+      NRRC(fast_gpu_set_displacement_device(c, w.u));
+      NRRC(fast_gpu_internal_force_device(c, w.g));
+      NRCK(axpby(*c, 1.0, w.f, -1.0, w.g, w.r));  // r = f - g
+      NRCK(norms2(*c, w, w.r, w.f, &rlen2, &flen2));
+    }
 
     int conv = 0, it = 0;
     bool start_ok = false;
@@ -422,7 +441,7 @@ done:
   if (w.h_out) cudaFreeHost(w.h_out);
   if (w.par) cudaFree(w.par);
   if (w.d_out) cudaFree(w.d_out);
-  for (double *p : {w.q, w.f, w.g, w.r, w.u, w.du, w.up, w.ucand, w.part, w.sums})
+  for (double *p : {w.q, w.f, w.g, w.r, w.u, w.du, w.up, w.ucand, w.gsave, w.part, w.sums})
     if (p) cudaFree(p);
   return rc;
 }

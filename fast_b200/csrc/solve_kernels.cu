@@ -153,8 +153,10 @@ __device__ __forceinline__ T ldm(const T *p) {
 // FP32 SpMV: LPR lanes per block-row; a lane takes 4 blocks per trip (one
 // int4 of columns, nine float4 of values, four float4 gathers of x): 14
 // independent 16-byte loads in flight per lane.  CS: matrix loads streamed.
+// Three CTAs per SM: at four the 52 registers of one trip's loads spill
+// (measured 10 % slower in the PCG loop).
 template <int MODE, int LPR, bool CS = false>
-__global__ void __launch_bounds__(kSpmvThreads, 4)
+__global__ void __launch_bounds__(kSpmvThreads, 3)
 spmv_f32(int64_t nrows, const int32_t *__restrict__ srow, const int32_t *__restrict__ scol,
          const float *__restrict__ val, const float *__restrict__ x, const float *__restrict__ b,
          float *__restrict__ y, double *__restrict__ part, const int32_t *__restrict__ skip) {
@@ -208,7 +210,7 @@ spmv_f32(int64_t nrows, const int32_t *__restrict__ srow, const int32_t *__restr
 // fewer than 65,536 nodes), 38 instead of 40 bytes per block for the matrix
 // stream; otherwise spmv_f32<MODE, LPR> (the same sums in the same order).
 template <int LPR>
-__global__ void __launch_bounds__(kSpmvThreads, 4)
+__global__ void __launch_bounds__(kSpmvThreads, 3)
 spmv_f32_c16(int64_t nrows, const int32_t *__restrict__ srow, const uint16_t *__restrict__ scol16,
              const int32_t *__restrict__ rowbase, const float *__restrict__ val, const float *__restrict__ x,
              float *__restrict__ y, double *__restrict__ part, const int32_t *__restrict__ skip) {

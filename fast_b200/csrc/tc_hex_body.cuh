@@ -240,12 +240,13 @@ __device__ bool tc_hex_elements(const ElemArgs &A, float *__restrict__ K32, uint
     Fix(j)[i] = A.fix[Conn(j)[i]];
   }
   if (K32) {
-    for (int t = tid; t < nv * NN * NN * 9; t += kThreads) {
-      const int j = t / (NN * NN * 9), tt = t - j * NN * NN * 9, q = tt / 9;
-      // a block this element writes first is not read
-      if (!(A.first && ((First(j)[q >> 5] >> (q & 31)) & 1u)))
-        cp_async4(Ko(j) + tt, K32 + (int64_t)Slot(j)[q] * 9 + (tt - 9 * q));
-    }
+    if (BlockWalk<NN, kThreads>::takes(tid))
+      for (BlockWalk<NN, kThreads> w(tid); w.j < nv; w.next()) {
+        const int q = w.qq();
+        // a block this element writes first is not read
+        if (!(A.first && ((First(w.j)[q >> 5] >> (q & 31)) & 1u)))
+          cp_async4(Ko(w.j) + 9 * q + w.k, K32 + (int64_t)Slot(w.j)[q] * 9 + w.k);
+      }
     asm volatile("cp.async.commit_group;\n" ::);
   }
   __syncthreads();
@@ -395,19 +396,19 @@ __device__ bool tc_hex_elements(const ElemArgs &A, float *__restrict__ K32, uint
     __syncthreads();
     // old + new for every entry whose two DOFs have equations (block (b, a)
     // is the transpose of (a, b)); first writes store new, fixed entries too
-    for (int t = tid; t < nv * NN * NN * 9; t += kThreads) {
-      const int j = t / (NN * NN * 9), tt = t - j * NN * NN * 9;
-      const int q = tt / 9, k = tt - 9 * q;
-      const int a = q / NN, b = q - NN * a, i = k / 3, jj = k - 3 * i;
-      const bool fst = A.first && ((First(j)[q >> 5] >> (q & 31)) & 1u);
-      const uint8_t *fx = Fix(j);
-      const bool fixed = ((fx[a] >> i) & 1) || ((fx[b] >> jj) & 1);
-      const float *Vj = V(j);
-      const float add = (a <= b) ? Vj[9 * (a * NN - a * (a - 1) / 2 + (b - a)) + k]
-                                 : Vj[9 * (b * NN - b * (b - 1) / 2 + (a - b)) + 3 * jj + i];
-      float out;
-      if (entry_value(fst, fixed, a == b && i == jj, fst ? 0.f : Ko(j)[tt], add, out))
-        K32[(int64_t)Slot(j)[q] * 9 + k] = out;
+    if (BlockWalk<NN, kThreads>::takes(tid)) {
+      BlockWalk<NN, kThreads> w(tid);
+      const int k = w.k, i = k / 3, jj = k - 3 * i, kt = 3 * jj + i;
+      for (; w.j < nv; w.next()) {
+        const int j = w.j, a = w.a, b = w.b, q = w.qq();
+        const bool fst = A.first && ((First(j)[q >> 5] >> (q & 31)) & 1u);
+        const uint8_t *fx = Fix(j);
+        const bool fixed = ((fx[a] >> i) & 1) || ((fx[b] >> jj) & 1);
+        const float add = V(j)[upper_entry<NN>(a, b, k, kt)];
+        float out;
+        if (entry_value(fst, fixed, a == b && i == jj, fst ? 0.f : Ko(j)[9 * q + k], add, out))
+          K32[(int64_t)Slot(j)[q] * 9 + k] = out;
+      }
     }
   }
   return true;
