@@ -122,6 +122,52 @@ __global__ void __launch_bounds__(NT) skinny_atb_part(int64_t n, int p, int q, c
   }
 }
 
+// The same partial sums for many outputs (p q > NT, p, q <= 64): each block
+// takes a contiguous range of rows in tiles of TR rows staged in shared
+// memory (coalesced row loads), and each thread keeps up to kMaxOut / NT
+// outputs in registers, summing its tile rows in order.
+constexpr int kTiledMaxCols = 64;
+template <int NT, int TR>
+__global__ void __launch_bounds__(NT) skinny_atb_tiled(int64_t n, int p, int q, const double *__restrict__ A, int lda,
+                                                       const double *__restrict__ B, int ldb,
+                                                       double *__restrict__ part) {
+  constexpr int MO = kSkinnyMaxOut / NT;
+  __shared__ double As[TR][kTiledMaxCols], Bs[TR][kTiledMaxCols];
+  const int pq = p * q, tid = threadIdx.x;
+  double acc[MO];
+#pragma unroll
+  for (int m = 0; m < MO; m++) acc[m] = 0.0;
+  const int64_t r0 = n * blockIdx.x / gridDim.x, r1 = n * (blockIdx.x + 1) / gridDim.x;
+  for (int64_t t0 = r0; t0 < r1; t0 += TR) {
+    const int nr = (int)(r1 - t0 < TR ? r1 - t0 : TR);
+    for (int e = tid; e < nr * p; e += NT) {
+      const int r = e / p, c = e - r * p;
+      As[r][c] = A[(t0 + r) * lda + c];
+    }
+    for (int e = tid; e < nr * q; e += NT) {
+      const int r = e / q, c = e - r * q;
+      Bs[r][c] = B[(t0 + r) * ldb + c];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < MO; m++) {
+      const int o = tid + m * NT;
+      if (o < pq) {
+        const int a = o / q, b = o - a * q;
+        double t = acc[m];
+        for (int r = 0; r < nr; r++) t = fma(As[r][a], Bs[r][b], t);
+        acc[m] = t;
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int m = 0; m < MO; m++) {
+    const int o = tid + m * NT;
+    if (o < pq) part[(int64_t)blockIdx.x * pq + o] = acc[m];
+  }
+}
+
 // one warp per output entry: lane l sums the partials l, l+32, ... in order,
 // then a fixed butterfly combines the lanes (deterministic)
 __global__ void skinny_finish(int nblk, int p, int q, const double *__restrict__ part, double *__restrict__ C,
@@ -140,7 +186,10 @@ __global__ void skinny_finish(int nblk, int p, int q, const double *__restrict__
 cudaError_t skinny_atb(cudaStream_t s, int64_t n, int p, int q, const double *A, int lda, const double *B, int ldb,
                        double *C, int ldc, double *ws) {
   if (n <= 0 || p <= 0 || q <= 0 || p * q > kSkinnyMaxOut || !ws) return cudaErrorInvalidValue;
-  skinny_atb_part<256><<<kSkinnyBlocks, 256, 0, s>>>(n, p, q, A, lda, B, ldb, ws);
+  if (p * q > 256 && p <= kTiledMaxCols && q <= kTiledMaxCols)
+    skinny_atb_tiled<256, 32><<<kSkinnyBlocks, 256, 0, s>>>(n, p, q, A, lda, B, ldb, ws);
+  else
+    skinny_atb_part<256><<<kSkinnyBlocks, 256, 0, s>>>(n, p, q, A, lda, B, ldb, ws);
   skinny_finish<<<(p * q + 7) / 8, 256, 0, s>>>(kSkinnyBlocks, p, q, ws, C, ldc);
   return cudaGetLastError();
 }

@@ -941,8 +941,13 @@ cudaError_t ensure_col16(Ctx &c) {
   return e;
 }
 
+// grid of the FP32 SpMV kernels: two full waves of their three resident CTAs
+// per SM (the row groups are interleaved over the CTAs, so every CTA has the
+// same work and a partial last wave would idle a third of the SMs' slots)
+static int spmv32_grid(const Ctx &c) { return c.sm_count * 6; }
+
 // CTAs (= p.w partials) of the FP32 SpMV in use
-static int spmv32_parts(const Ctx &c) { return c.spmv32_bulk ? c.bulk_grid : spmv_grid(c); }
+static int spmv32_parts(const Ctx &c) { return c.spmv32_bulk ? c.bulk_grid : spmv32_grid(c); }
 
 static void spmv32_go(const Ctx &c, int G, int64_t nn, const float *Ks, const float *x, float *y, double *part,
                       const int32_t *skip) {
@@ -1048,7 +1053,7 @@ cudaError_t launch_spmv(Ctx &c, const double *Ks, const double *x, double *y) {
 }
 
 cudaError_t launch_spmv32(Ctx &c, const float *Ks, const float *x, float *y) {
-  spmv32_go(c, spmv_grid(c), c.nnode, Ks, x, y, nullptr, nullptr);
+  spmv32_go(c, spmv32_grid(c), c.nnode, Ks, x, y, nullptr, nullptr);
   c.launches++;
   return cudaGetLastError();
 }
@@ -1752,7 +1757,7 @@ static void mixed_reliable(Ctx &c) {
 
 static void mixed_chunk(Ctx &c, int k) {
   const int64_t nn = c.nnode;
-  const int G = spmv_grid(c), R = kRedBlocks;
+  const int G = spmv32_grid(c), R = kRedBlocks;
   PcgState *st = c.d_state;
   for (int i = 0; i < k; i++) {
     c.begin_span(1);

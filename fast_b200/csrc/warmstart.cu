@@ -177,7 +177,7 @@ __global__ void ws_start(int32_t n, int k, double rho, const double *__restrict_
   }
 }
 
-// Cholesky factor of the (symmetrised) reduced tangent, one block; ok = 0
+// Cholesky factor L of the (symmetrised) reduced tangent, one block; ok = 0
 // when a pivot is not positive
 __global__ void ws_chol(int k, const double *__restrict__ E, double *__restrict__ L, int32_t *__restrict__ ok) {
   __shared__ double A[64][65];
@@ -211,32 +211,23 @@ __global__ void ws_chol(int k, const double *__restrict__ E, double *__restrict_
     __syncthreads();
   }
   __syncthreads();
-  // explicit inverse (L L^T)^-1, one column per thread, so that every reduced
-  // solve of the step is a k x k product
-  for (int c = threadIdx.x; c < k; c += blockDim.x) {
-    double y[64];
-    for (int i = 0; i < k; i++) {
-      double v = (i == c) ? 1.0 : 0.0;
-      for (int p = 0; p < i; p++) v -= A[i][p] * y[p];
-      y[i] = v / A[i][i];
-    }
-    for (int i = k - 1; i >= 0; i--) {
-      double v = y[i];
-      for (int p = i + 1; p < k; p++) v -= A[p][i] * y[p];
-      y[i] = v / A[i][i];
-    }
-    for (int i = 0; i < k; i++) L[i * k + c] = y[i];
+  // the factor L (lower triangle, row-major); the reduced solves run two
+  // triangular solves on it
+  for (int t = threadIdx.x; t < k * k; t += blockDim.x) {
+    const int i = t / k, j = t % k;
+    L[t] = j <= i ? A[i][j] : 0.0;
   }
   if (threadIdx.x == 0) *ok = bad ? 0 : 1;
 }
 
-// da = Ainv t (Ainv from ws_chol), or 0 when the factor failed or |t| <= tol
-// |tf|, then u += Phi da.  Every block forms da itself (its first warp, lane i
-// row i: k <= 64 rows of k products); block 0 also stores it.
-__global__ void ws_reduced_add(int32_t n, int k, const double *__restrict__ Ainv, const int32_t *__restrict__ ok,
+// da = (L L^T)^-1 t (L from ws_chol), or 0 when the factor failed or |t| <=
+// tol |tf|, then u += Phi da.  Every block forms da itself (its first warp:
+// a forward and a backward substitution, each row's sum split over the lanes
+// and combined by a fixed butterfly); block 0 also stores it.
+__global__ void ws_reduced_add(int32_t n, int k, const double *__restrict__ L, const int32_t *__restrict__ ok,
                                const double *__restrict__ t, const double *__restrict__ tf, double tol,
                                const double *__restrict__ phi, double *__restrict__ u, double *__restrict__ da_out) {
-  __shared__ double da[64];
+  __shared__ double da[64], y[64];
   if (threadIdx.x < 32) {
     const int lane = threadIdx.x;
     double tn = 0.0, fn = 0.0;
@@ -247,11 +238,27 @@ __global__ void ws_reduced_add(int32_t n, int k, const double *__restrict__ Ainv
       fn += __shfl_xor_sync(0xffffffffu, fn, m);
     }
     const bool skip = !*ok || !(sqrt(tn) > tol * sqrt(fn));
-    for (int i = lane; i < k; i += 32) {
-      double v = 0.0;
-      if (!skip)
-        for (int j = 0; j < k; j++) v += Ainv[i * k + j] * t[j];
-      da[i] = v;
+    if (skip) {
+      for (int i = lane; i < k; i += 32) da[i] = 0.0;
+    } else {
+      // L y = t
+      for (int i = 0; i < k; i++) {
+        double s = 0.0;
+        for (int p = lane; p < i; p += 32) s += L[i * k + p] * y[p];
+#pragma unroll
+        for (int m = 16; m > 0; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
+        if (lane == 0) y[i] = (t[i] - s) / L[i * k + i];
+        __syncwarp();
+      }
+      // L^T da = y
+      for (int i = k - 1; i >= 0; i--) {
+        double s = 0.0;
+        for (int p = i + 1 + lane; p < k; p += 32) s += L[p * k + i] * da[p];
+#pragma unroll
+        for (int m = 16; m > 0; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
+        if (lane == 0) da[i] = (y[i] - s) / L[i * k + i];
+        __syncwarp();
+      }
     }
   }
   __syncthreads();
@@ -316,7 +323,7 @@ struct fast_gpu_ws {
   double *d_phin = nullptr;      // [nnode*4][k] basis in the node-padded layout
   double *d_Y = nullptr;         // [nnode*4][k] K Phi
   double *d_Er = nullptr;        // [64*64] Phi^T K Phi
-  double *d_L = nullptr;         // [64*64] its inverse (from the Cholesky factor)
+  double *d_L = nullptr;         // [64*64] its Cholesky factor (lower, row-major)
   int32_t *d_ok = nullptr;
   double *d_g = nullptr;         // [n] internal force of the refined start
   unsigned int *d_ticket = nullptr;       // finishing-block counter of ws_project
