@@ -53,7 +53,9 @@ __global__ void ws_block_spmm(int64_t nnode, int k, const int32_t *__restrict__ 
   const int64_t i = t / k;
   const int m = (int)(t % k);
   double y0 = 0.0, y1 = 0.0, y2 = 0.0;
-  for (int32_t b = rowptr[i]; b < rowptr[i + 1]; b++) {
+  const int32_t b0 = rowptr[i], b1 = rowptr[i + 1];
+#pragma unroll 4
+  for (int32_t b = b0; b < b1; b++) {
     const double *v = K + 9 * (int64_t)b;
     const int64_t j = col[b];
     const double x0 = phin[(4 * j + 0) * k + m], x1 = phin[(4 * j + 1) * k + m], x2 = phin[(4 * j + 2) * k + m];
@@ -227,7 +229,12 @@ __global__ void ws_chol(int k, const double *__restrict__ E, double *__restrict_
 __global__ void ws_reduced_add(int32_t n, int k, const double *__restrict__ L, const int32_t *__restrict__ ok,
                                const double *__restrict__ t, const double *__restrict__ tf, double tol,
                                const double *__restrict__ phi, double *__restrict__ u, double *__restrict__ da_out) {
-  __shared__ double da[64], y[64];
+  __shared__ double da[64], y[64], ts[64], Ls[64 * 64];
+  // the factor and t into shared memory first (all threads, coalesced): the
+  // two substitutions below are chains of k dependent steps each
+  for (int e = threadIdx.x; e < k * k; e += blockDim.x) Ls[e] = L[e];
+  if (threadIdx.x < k) ts[threadIdx.x] = t[threadIdx.x];
+  __syncthreads();
   if (threadIdx.x < 32) {
     const int lane = threadIdx.x;
     double tn = 0.0, fn = 0.0;
@@ -244,19 +251,19 @@ __global__ void ws_reduced_add(int32_t n, int k, const double *__restrict__ L, c
       // L y = t
       for (int i = 0; i < k; i++) {
         double s = 0.0;
-        for (int p = lane; p < i; p += 32) s += L[i * k + p] * y[p];
+        for (int p = lane; p < i; p += 32) s += Ls[i * k + p] * y[p];
 #pragma unroll
         for (int m = 16; m > 0; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
-        if (lane == 0) y[i] = (t[i] - s) / L[i * k + i];
+        if (lane == 0) y[i] = (ts[i] - s) / Ls[i * k + i];
         __syncwarp();
       }
       // L^T da = y
       for (int i = k - 1; i >= 0; i--) {
         double s = 0.0;
-        for (int p = i + 1 + lane; p < k; p += 32) s += L[p * k + i] * da[p];
+        for (int p = i + 1 + lane; p < k; p += 32) s += Ls[p * k + i] * da[p];
 #pragma unroll
         for (int m = 16; m > 0; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
-        if (lane == 0) da[i] = (y[i] - s) / L[i * k + i];
+        if (lane == 0) da[i] = (y[i] - s) / Ls[i * k + i];
         __syncwarp();
       }
     }
