@@ -50,6 +50,9 @@ void free_mesh(Ctx &c) {
   free_ties(c);
   free_face_loads(c);
   dfree(c.d_X); dfree(c.d_fix); dfree(c.d_dof_of_eq); dfree(c.d_scol16); dfree(c.d_rowbase);
+  dfree(c.d_elem_g); dfree(c.d_gptr); dfree(c.d_ginc);
+  c.force_gather = false;
+  c.elem_g_off.clear();
   c.spmv32_c16 = false;
   dfree(c.d_rowptr); dfree(c.d_col); dfree(c.d_diag); dfree(c.d_srow); dfree(c.d_scol);
   dfree(c.d_tile_row);
@@ -243,6 +246,13 @@ int fast_gpu_set_option(fast_gpu_ctx *c, int32_t option, int64_t value) {
     c->drop_graphs();
     c->spmv32_c16 = value != 0;
     if (value) c->spmv32_bulk = c->spmv32_stream = false;
+    return FAST_GPU_OK;
+  }
+  if (option == FAST_OPT_FORCE_GATHER) {
+    if (value != 0 && value != 1) return FAST_GPU_EINVAL;
+    CK(cudaStreamSynchronize(c->stream));
+    c->drop_graphs();
+    c->use_force_gather = value != 0;
     return FAST_GPU_OK;
   }
   if (option == FAST_OPT_PERSISTENT_ASSEMBLY) {
@@ -487,6 +497,39 @@ int fast_gpu_upload_mesh(fast_gpu_ctx *c, const fast_gpu_mesh *m) {
     CK(cudaMemcpy(B.d_w, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice));
   }
   CK(upload_ties(*c));
+  {
+    // the per-node gather of the element-wise internal force (hex buckets
+    // only): each node's element entries in bucket, then colour-sorted order
+    bool all_hex = !c->buckets.empty();
+    for (const Bucket &B : c->buckets)
+      all_hex = all_hex && ((B.type == FAST_ELEM_HEX8 && (B.ng == 1 || B.ng == 8 || B.ng == 27)) ||
+                            (B.type == FAST_ELEM_HEX20 && (B.ng == 8 || B.ng == 27 || B.ng == 64)));
+    if (all_hex) {
+      std::vector<int64_t> ptr(nnode + 1, 0);
+      c->elem_g_off.assign(c->buckets.size(), 0);
+      int64_t off = 0;
+      for (size_t b = 0; b < c->buckets.size(); b++) {
+        const Bucket &B = c->buckets[b];
+        const int64_t nreg = B.color_off.empty() ? 0 : B.color_off.back();
+        c->elem_g_off[b] = off;
+        for (int64_t e = 0; e < nreg * B.nn; e++) ptr[B.h_conn[e] + 1]++;
+        off += nreg * B.nn * 3;
+      }
+      for (int64_t n = 0; n < nnode; n++) ptr[n + 1] += ptr[n];
+      std::vector<int64_t> inc(ptr[nnode]), pos(ptr.begin(), ptr.end() - 1);
+      for (size_t b = 0; b < c->buckets.size(); b++) {
+        const Bucket &B = c->buckets[b];
+        const int64_t nreg = B.color_off.empty() ? 0 : B.color_off.back();
+        for (int64_t e = 0; e < nreg * B.nn; e++) inc[pos[B.h_conn[e]]++] = c->elem_g_off[b] + 3 * e;
+      }
+      CK(dalloc(&c->d_elem_g, off));
+      CK(dalloc(&c->d_gptr, nnode + 1));
+      CK(cudaMemcpy(c->d_gptr, ptr.data(), sizeof(int64_t) * (nnode + 1), cudaMemcpyHostToDevice));
+      CK(dalloc(&c->d_ginc, inc.size()));
+      if (!inc.empty()) CK(cudaMemcpy(c->d_ginc, inc.data(), sizeof(int64_t) * inc.size(), cudaMemcpyHostToDevice));
+      c->force_gather = true;
+    }
+  }
   const int64_t n4 = 4 * nnode;
   CK(dalloc(&c->d_K, 9 * c->nnzb));
   CK(dalloc(&c->d_u, n4)); CK(dalloc(&c->d_r, n4)); CK(dalloc(&c->d_z, n4)); CK(dalloc(&c->d_p, n4));

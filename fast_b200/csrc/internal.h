@@ -240,6 +240,17 @@ struct Ctx {
   bool spmv32_c16 = false;      // FP32 SpMV with 16-bit column offsets (8 or 16 lanes)
   uint16_t *d_scol16 = nullptr; // [nnzb_pad] column offsets from the row's smallest column
   int32_t *d_rowbase = nullptr; // [nnode] that column
+  // internal force element by element, then gathered per node (every bucket a
+  // hex bucket): element forces [bucket][colour-sorted element][nn][3] at
+  // elem_g_off[bucket], and per node the offsets of its elements' entries in
+  // bucket, then colour order (the order the colour-by-colour scatter adds
+  // them in, so both give the same bits)
+  bool force_gather = false;      // available for this mesh
+  bool use_force_gather = true;   // FAST_OPT_FORCE_GATHER
+  double *d_elem_g = nullptr;
+  int64_t *d_gptr = nullptr;      // [nnode + 1]
+  int64_t *d_ginc = nullptr;      // [sum of elements x nn]
+  std::vector<int64_t> elem_g_off;
   // widest launch shape the element kernels could take since last reset
   // (read by the autotuner to bound its candidates)
   int elem_occ = 0, elem_split_max = 0;

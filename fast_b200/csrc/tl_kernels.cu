@@ -357,7 +357,50 @@ cudaError_t launch_tl(Ctx &c, double *K, double *G, bool want_k, bool want_g) {
   return launch_tl_at(c, K, G, want_k, want_g, c.d_disp, nullptr);
 }
 
+// G[n][i] += sum of the node's element entries, in the order of d_ginc, on
+// the DOFs without a fixity (the colour scatter's additions, one node per
+// thread); nothing when *skip
+__global__ void gather_elem_force(int64_t nnode, const int64_t *__restrict__ ptr, const int64_t *__restrict__ inc,
+                                  const double *__restrict__ Fe, const uint8_t *__restrict__ fix,
+                                  double *__restrict__ G, const int32_t *__restrict__ skip) {
+  if (skip && *skip) return;
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= nnode) return;
+  double *Gn = G + 4 * n;
+  double g0 = Gn[0], g1 = Gn[1], g2 = Gn[2];
+  for (int64_t p = ptr[n]; p < ptr[n + 1]; p++) {
+    const double *f = Fe + inc[p];
+    g0 += f[0];
+    g1 += f[1];
+    g2 += f[2];
+  }
+  const uint8_t fx = fix[n];
+  if (!(fx & 1)) Gn[0] = g0;
+  if (!(fx & 2)) Gn[1] = g1;
+  if (!(fx & 4)) Gn[2] = g2;
+}
+
 cudaError_t launch_tl_at(Ctx &c, double *K, double *G, bool want_k, bool want_g, const double *U, const int32_t *skip) {
+  if (!want_k && want_g && G && c.force_gather && c.use_force_gather) {
+    // every element of a bucket in one launch, its force into its own slot,
+    // then one gather over the nodes
+    for (size_t b = 0; b < c.buckets.size(); b++) {
+      const Bucket &B = c.buckets[b];
+      const int64_t cnt = B.color_off.empty() ? 0 : B.color_off.back();
+      if (cnt == 0) continue;
+      ElemArgs a = tl_args(c, B, nullptr, nullptr);
+      a.U = U;
+      a.skip = skip;
+      a.offset = 0;
+      a.Ke_out = c.d_elem_g + c.elem_g_off[b];
+      cudaError_t e = B.tl ? dispatch_tl<true>(c, B, a, cnt, 2) : dispatch_tl<false>(c, B, a, cnt, 2);
+      if (e != cudaSuccess) return e;
+    }
+    gather_elem_force<<<(unsigned)((c.nnode + 255) / 256), 256, 0, c.stream>>>(c.nnode, c.d_gptr, c.d_ginc,
+                                                                              c.d_elem_g, c.d_fix, G, skip);
+    c.launches++;
+    return cudaGetLastError();
+  }
   for (size_t b = 0; b < c.buckets.size(); b++) {
     const Bucket &B = c.buckets[b];
     int mode;

@@ -58,6 +58,7 @@ OPT_ZERO_FILL = 7
 OPT_PERSISTENT_ASSEMBLY = 8
 OPT_SPMV_STREAM_FP32 = 9
 OPT_SPMV_COL16_FP32 = 10
+OPT_FORCE_GATHER = 11
 
 
 def elem_shape(bucket: int, ctas: int = 0, split: int = 0, tc_ctas: int = 0, kernel: int = 0) -> int:

@@ -213,6 +213,10 @@ int         fast_gpu_synchronize(fast_gpu_ctx *ctx);
                                             smallest column (38 instead of 40 bytes per block; every row
                                             must span fewer than 65,536 nodes, else FAST_GPU_ENOTSUP);
                                             0 (default until fast_gpu_autotune measures it): 32-bit */
+#define FAST_OPT_FORCE_GATHER        11  /* 1 (default): where every bucket is a hex bucket, the internal
+                                            force is formed element by element in one launch per bucket
+                                            and gathered per node in the order the colour-by-colour
+                                            scatter adds it (the same bits); 0: one launch per colour */
 #define FAST_OPT_PERSISTENT_ASSEMBLY  8  /* 1: FAST_ASM_STIFFNESS_TF32 integrates the elements of every
                                             bucket in one persistent cooperative launch (colour k of
                                             every bucket is phase k, grid barriers between phases, CTAs

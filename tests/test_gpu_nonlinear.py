@@ -147,3 +147,46 @@ def test_newton_graph_replay_equals_direct_launches(precision):
         # loop refreshes every 16): both meet the Newton tolerance
         assert gio.rel(h1, h0) < 1e-7
     s.close()
+
+
+@pytest.mark.parametrize("which", ["tl_plate", "hex20_box", "two_buckets"])
+def test_gathered_internal_force_equals_colour_scatter(which):
+    """FAST_OPT_FORCE_GATHER: the internal force formed element by element in
+    one launch per bucket and gathered per node (in bucket, then colour order)
+    is the same bits as the colour-by-colour scatter, in fewer launches; so
+    are the Newton steps built on it."""
+    import dataclasses
+    if which == "tl_plate":
+        d = decks.plate_tl_hex8(8, 8, 2, L=4.0, t=0.4, pressure=10.0, steps=6, tol=1e-8)
+    elif which == "hex20_box":
+        d = decks.box_hex20_lognormal(6, 6, 3, seed=9)
+    else:
+        # two hex20 buckets sharing their interface nodes (3x3x3 and 2x2x2 rules)
+        d0 = decks.box_hex20_lognormal(6, 6, 4, seed=6)
+        h = d0.num_elems // 2
+        nofaces = dict(face_elem=None, face_corners=None, face_q=None, face_local=None, blocks=[])
+        blk = dataclasses.replace(d0, conn=d0.conn[h:], E=d0.E[h:], nu=d0.nu[h:], ngp=(2, 2, 2), **nofaces)
+        d = dataclasses.replace(d0, conn=d0.conn[:h], E=d0.E[:h], nu=d0.nu[:h], **nofaces)
+        d.blocks = [blk]
+    s = system(d)
+    u = np.random.default_rng(5).standard_normal(d.num_eq()) * 1e-2
+    s.set_displacement(u)
+    g = {}
+    launches = {}
+    for opt in (1, 0):
+        s.set_option(gpu.OPT_FORCE_GATHER, opt)
+        n0 = s.launch_count()
+        g[opt] = s.internal_force()
+        launches[opt] = s.launch_count() - n0
+    assert np.array_equal(g[1], g[0]) and np.abs(g[0]).max() > 0
+    assert launches[1] <= launches[0], launches
+    if which == "tl_plate":
+        q = gpu.face_load_vector(d)
+        kw = dict(tol=1e-8, predictor=gpu.PREDICT_SECANT, precision=gpu.PREC_FP64, lin_tol=1e-10)
+        h = {}
+        for opt in (1, 0):
+            s.set_option(gpu.OPT_FORCE_GATHER, opt)
+            h[opt], _, r = s.nr_solve(q, 6, 1 / 6, **kw)
+            assert r["converged_steps"] == 6
+        assert np.array_equal(h[1], h[0])
+    s.close()
