@@ -307,9 +307,15 @@ def newton_plate(local, args):
     S.synchronize()
     pn_n, pn_ms, _ = S.kernel_stats(gpu.KERNEL_PREDICT_NET)
     pg_n, pg_ms, _ = S.kernel_stats(gpu.KERNEL_PREDICT_GALERKIN)
+    # where the device time of that (kernel-by-kernel) learned run goes
+    brk = {}
+    for name, kind in (("linear_solves", gpu.KERNEL_LINEAR_SOLVE), ("internal_forces", gpu.KERNEL_INTERNAL_FORCE),
+                       ("tangent_assemblies", gpu.KERNEL_ASSEMBLE)):
+        kn, kms, _ = S.kernel_stats(kind)
+        brk[name] = {"count": int(kn), "ms": kms}
     S.kernel_timing(False)
     pred_ms = {"network_ms_per_step": pn_ms / max(1, pn_n), "galerkin_ms_per_step": pg_ms / max(1, pg_n),
-               "steps": int(pn_n)}
+               "steps": int(pn_n), "device_time_of_a_learned_run_without_graphs": brk}
     u_ref = out["plain_fp64"][0]
     zplate = load_fixture("full_plate_tl_40x40x4")
     eqn = d.node_eq()
