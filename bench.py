@@ -274,9 +274,14 @@ def newton_plate(local, args):
                                            lin_tol_rel=1e-3),
         "learned_mixed_two_corrections": dict(learned=pred, precision=gpu.PREC_MIXED, lin_tol=1e-10,
                                               lin_tol_rel=1e-3),
+        # the same starts with FP64 inner solves (inexact Newton alike)
+        "secant_fp64_inexact": dict(predictor=gpu.PREDICT_SECANT, precision=gpu.PREC_FP64, lin_tol=1e-10,
+                                    lin_tol_rel=1e-3),
+        "learned_fp64_inexact": dict(learned=pred, precision=gpu.PREC_FP64, lin_tol=1e-10, lin_tol_rel=1e-3),
     }
     # Galerkin corrections of the learned start per run (the network-only run has none)
-    galerkin = {"learned_mixed": 1, "learned_mixed_network_only": 0, "learned_mixed_two_corrections": 2}
+    galerkin = {"learned_mixed": 1, "learned_mixed_network_only": 0, "learned_mixed_two_corrections": 2,
+                "learned_fp64_inexact": 1}
     times = {k: [] for k in runs}
     out = {}
     clocks = ClockSampler(local)
