@@ -1136,14 +1136,10 @@ cudaError_t launch_build_precond32(Ctx &c, const float *K32, int precond) {
 constexpr int kPersistThreads = 512;
 constexpr uint64_t kBarrierWaitNs = 2000000000ull;  // one barrier wait; then the launch gives up
 
-// Sense-reversal barrier over all blocks of a cooperative launch: thread 0 of
-// each block arrives on a counter; the last one resets it and advances the
-// generation word the others wait on.  (A flag barrier, each block posting
-// its own word and block 0 releasing, measured slower here: 17 vs 13.5 us per
-// iteration.)  Every wait is bounded: when one runs out the error word is set
-// and every block leaves at its next barrier.
-struct GridBarrier {
-  unsigned int count;
+// Barrier over all blocks of a cooperative launch (grid_barrier below); the
+// words are zeroed before a solve's first launch.
+struct alignas(8) GridBarrier {
+  unsigned int count;  // with gen: one 64-bit arrival counter (8-byte aligned)
   unsigned int gen;
   int32_t err;
   int32_t pad;
@@ -1156,27 +1152,34 @@ __device__ __forceinline__ uint64_t now_ns() {
   return t;
 }
 
+// One 64-bit arrival counter (the count and gen words read as one), never
+// reset within a solve: thread 0 of each block adds 1 with release semantics
+// and polls with acquire loads until the counter reaches the next multiple of
+// the grid.  (Measured against a sense-reversal barrier whose last arriver
+// resets the count and advances a generation word behind full fences: 11.4
+// against 13.6 us per FP32 PCG iteration on a 22,815-equation tangent; a flag
+// barrier, each block posting its own word and block 0 releasing, was slower
+// still.)  Every wait is bounded: when one runs out the error word is set and
+// every block leaves at its next barrier.
 __device__ bool grid_barrier(GridBarrier *b, int *ok_sh) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned int *vgen = &b->gen;
     volatile int32_t *verr = &b->err;
     int ok = *verr == 0;
     if (ok) {
-      const unsigned int g = *vgen;
-      __threadfence();
-      if (atomicAdd(&b->count, 1u) == gridDim.x - 1) {
-        atomicExch(&b->count, 0u);
-        __threadfence();
-        atomicAdd(&b->gen, 1u);
-      } else {
+      unsigned long long *ctr = reinterpret_cast<unsigned long long *>(&b->count);
+      unsigned long long old, cur;
+      asm volatile("atom.add.release.gpu.u64 %0, [%1], 1;" : "=l"(old) : "l"(ctr) : "memory");
+      const unsigned long long target = (old / gridDim.x + 1) * gridDim.x;
+      asm volatile("ld.acquire.gpu.u64 %0, [%1];" : "=l"(cur) : "l"(ctr) : "memory");
+      if (cur < target) {
         const uint64_t t0 = now_ns();
-        while (*vgen == g) {
+        do {
           if (*verr != 0) { ok = 0; break; }
           if (now_ns() - t0 > kBarrierWaitNs) { atomicExch(&b->err, 1); ok = 0; break; }
-        }
+          asm volatile("ld.acquire.gpu.u64 %0, [%1];" : "=l"(cur) : "l"(ctr) : "memory");
+        } while (cur < target);
       }
-      __threadfence();
     }
     *ok_sh = ok;
   }
