@@ -618,12 +618,13 @@ class GpuSystem:
     # -- load-control Newton-Raphson (cCtrlNR::Solver)
     def nr_solve(self, q, steps, step_factor, tol=1e-8, max_iter=30, predictor=PREDICT_NONE, callback=None,
                  precision=PREC_FP64, precond=PRECOND_JACOBI, lin_tol=1e-12, lin_tol_rel=0.0, lin_tol_min=1e-12,
-                 lin_tol_max=1e-2, keep_history=True, raise_on_fail=True, learned=None):
+                 lin_tol_max=1e-2, keep_history=True, raise_on_fail=True, learned=None, lin_check_every=0):
         """Load-control Newton-Raphson.  ``learned``: a trained
         :class:`LearnedPredictor` used as the caller predictor (implies
-        ``predictor=PREDICT_CALLBACK``)."""
+        ``predictor=PREDICT_CALLBACK``).  ``lin_check_every``: PCG iterations
+        per chunk of the inner solves (0: the library's default)."""
         q = np.ascontiguousarray(q, dtype=np.float64)
-        lin = SolveOpts(precision, precond, 0, 0, float(lin_tol), 0.0, 0, 0)
+        lin = SolveOpts(precision, precond, 0, 0, float(lin_tol), 0.0, 0, int(lin_check_every))
         o = NrOpts(int(steps), int(max_iter), float(step_factor), float(tol), int(predictor), 0, lin,
                    float(lin_tol_rel), float(lin_tol_min), float(lin_tol_max))
         hist = np.zeros((steps, self.neq)) if keep_history else None
