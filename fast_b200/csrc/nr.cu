@@ -141,11 +141,12 @@ static cudaError_t capture_iteration(Ctx &c, NrWork &w, const fast_gpu_nr_opts *
   const fast_gpu_solve_opts &lo = o->lin;
   const int32_t n = c.neq;
   const int maxit = lo.maxit > 0 ? lo.maxit : std::max(20 * c.neq, 100);
-  // the chunk of the direct solves (fast_gpu_solve): a mixed solve's FP64
-  // residual every 50 FP32 iterations (measured on the TL plate's Newton run:
-  // 16 -> 133.7, 32 -> 127.2, 50 -> 124.5, 64 -> 122.6 ms; 128 stalls the
-  // refinement and doubles the PCG iterations)
-  const int chunk = lo.check_every > 0 ? lo.check_every : (mixed ? 50 : 32);
+  // a mixed solve's FP64 residual every 50 FP32 iterations, the direct
+  // solves' chunk (measured on the TL plate's Newton run: 16 -> 133.7, 32 ->
+  // 127.2, 50 -> 124.5, 64 -> 122.6 ms; 128 stalls the refinement and doubles
+  // the PCG iterations), every 16 for linear tolerances below 1e-10, which
+  // need the more frequent corrections
+  const int chunk = lo.check_every > 0 ? lo.check_every : (mixed ? (lo.tol > 0 && lo.tol < 1e-10 ? 16 : 50) : 32);
   const double tol = o->tol > 0 ? o->tol : 1e-5;
   cudaGraph_t g = nullptr;
   cudaError_t e = cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal);
