@@ -57,7 +57,9 @@ __global__ void modal_ratio(int64_t nnode, const int32_t *__restrict__ diag, con
 // rows of this block (A, B: q vectors of n rows each, vector-major)
 __global__ void __launch_bounds__(256) modal_gram(int q, int64_t n, const double *__restrict__ A,
                                                   const double *__restrict__ B, double *__restrict__ part) {
-  __shared__ double sA[kMaxSub][kGramRows], sB[kMaxSub][kGramRows];
+  // rows padded by one: the threads of a warp read different vectors at the
+  // same row, which an unpadded 32-double row would put in one bank
+  __shared__ double sA[kMaxSub][kGramRows + 1], sB[kMaxSub][kGramRows + 1];
   const int qq = q * q;
   double acc[kMaxSub * kMaxSub / 256] = {0, 0, 0, 0};
   for (int64_t r0 = (int64_t)blockIdx.x * kGramRows; r0 < n; r0 += (int64_t)gridDim.x * kGramRows) {
