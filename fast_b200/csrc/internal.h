@@ -315,7 +315,7 @@ bool gauss_rule(int n, double *r, double *w);
 void gauss_point_tables(int type, const int ngp[3], std::vector<double> &N, std::vector<double> &dN,
                         std::vector<double> &w);
 // stress extrapolation TR [nn][ng] of a hex type and Gauss rule
-bool extrapolation_matrix(int type, const int ngp[3], std::vector<double> &TR);
+bool extrapolation_matrix(int type, const int ngp[3], std::vector<double> &TR, const int *pd = nullptr);
 int nodes_of(int type);
 // B-spline solid kernels exist for these (degree per direction, Gauss order)
 bool bsp_supported(const int pd[3], int ngp);

@@ -255,8 +255,13 @@ bool bspline_gauss_tables(int p, int nknots, const double *U, int ng, int &nspan
 // node: TR[a][g] = c_a^T A^-1 u_g with A = sum_g u_g u_g^T, u = (1, r, s, t),
 // c_a the node's (1, r, s, t).  A is symmetric, so each row is one 4x4 solve
 // A y = c_a followed by y . u_g.  A one-point first order gives the average.
-bool extrapolation_matrix(int type, const int ngp[3], std::vector<double> &TR) {
-  const int nn = nodes_of(type);
+bool extrapolation_matrix(int type, const int ngp[3], std::vector<double> &TR, const int *pd) {
+  // B-spline solids: the control points' natural coordinates are the uniform
+  // grid of (p+1) points per direction over [-1, 1], r fastest
+  // (cShapeBspSolid::NodeNatCoord, shp/shpbsp.cpp:906-923)
+  const bool bsp = type == FAST_ELEM_BSP_SOLID;
+  if (bsp && (!pd || pd[0] < 1 || pd[1] < 1 || pd[2] < 1)) return false;
+  const int nn = bsp ? (pd[0] + 1) * (pd[1] + 1) * (pd[2] + 1) : nodes_of(type);
   const int ng = ngp[0] * ngp[1] * ngp[2];
   if (nn <= 0 || ng <= 0) return false;
   TR.assign((size_t)nn * ng, 0.0);
@@ -279,11 +284,20 @@ bool extrapolation_matrix(int type, const int ngp[3], std::vector<double> &TR) {
     for (int p = 0; p < 4; p++)
       for (int q = 0; q < 4; q++) A0[p][q] += u[4 * g + p] * u[4 * g + q];
   for (int a = 0; a < nn; a++) {
-    const int *nat = type == FAST_ELEM_HEX8 ? kHex8Nat[a] : kHex20Nat[a];
+    double nat[3];
+    if (bsp) {
+      const int k = a % (pd[0] + 1), j = (a / (pd[0] + 1)) % (pd[1] + 1), i = a / ((pd[0] + 1) * (pd[1] + 1));
+      nat[0] = -1.0 + (2.0 / pd[0]) * k;
+      nat[1] = -1.0 + (2.0 / pd[1]) * j;
+      nat[2] = -1.0 + (2.0 / pd[2]) * i;
+    } else {
+      const int *h = type == FAST_ELEM_HEX8 ? kHex8Nat[a] : kHex20Nat[a];
+      for (int d = 0; d < 3; d++) nat[d] = (double)h[d];
+    }
     double A[8][8] = {};
     for (int p = 0; p < 4; p++)
       for (int q = 0; q < 4; q++) A[p][q] = A0[p][q];
-    double y[8] = {1.0, (double)nat[0], (double)nat[1], (double)nat[2]};
+    double y[8] = {1.0, nat[0], nat[1], nat[2]};
     if (!small_solve(4, A, y)) return false;
     for (int g = 0; g < ng; g++)
       TR[(size_t)a * ng + g] = y[0] * u[4 * g] + y[1] * u[4 * g + 1] + y[2] * u[4 * g + 2] + y[3] * u[4 * g + 3];

@@ -254,6 +254,43 @@ __global__ void average_at_nodes(int64_t nnode, const int64_t *__restrict__ ptr,
   for (int c = 0; c < 6; c++) out[n * 6 + c] = p1 > p0 ? acc[c] / cnt : 0.0;
 }
 
+// the same for any node and point count (B-spline buckets)
+__global__ void extrapolate_to_nodes_n(int64_t ne, int nn, int ng, const double *__restrict__ TR,
+                                       const double *__restrict__ Sg, double *__restrict__ Sn) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= ne * nn) return;
+  const int64_t k = t / nn;
+  const int a = (int)(t - k * nn);
+  const double *sg = Sg + k * ng * 6;
+  const double *tr = TR + (int64_t)a * ng;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int g = 0; g < ng; g++) {
+    const double w = tr[g];
+#pragma unroll
+    for (int c = 0; c < 6; c++) acc[c] = fma(w, sg[6 * g + c], acc[c]);
+  }
+#pragma unroll
+  for (int c = 0; c < 6; c++) Sn[t * 6 + c] = acc[c];
+}
+
+// B-spline bucket: Gauss-point stresses (strains into scratch), extrapolated
+// to the control points, averaged
+template <int PR, int PS, int PT, int NG1>
+cudaError_t run_nodal_bsp(Ctx &c, const Bucket &B, const int32_t *idx, double *Se, double *Sg, double *Sn,
+                          double *avg) {
+  constexpr int NG = NG1 * NG1 * NG1;
+  const int64_t ne = B.ne;
+  cudaError_t e = run_bsp<PR, PS, PT, NG1>(c, B, ne, idx, Se, Sg);
+  if (e != cudaSuccess) return e;
+  extrapolate_to_nodes_n<<<(unsigned)((ne * B.nn + 127) / 128), 128, 0, c.stream>>>(ne, B.nn, NG, B.d_tr, Sg, Sn);
+  c.launches++;
+  if (avg) {
+    average_at_nodes<<<(unsigned)((c.nnode + 127) / 128), 128, 0, c.stream>>>(c.nnode, B.d_nptr, B.d_nent, Sn, avg);
+    c.launches++;
+  }
+  return cudaGetLastError();
+}
+
 template <int NN, int NG>
 cudaError_t run_nodal(Ctx &c, const Bucket &B, const int32_t *idx, double *Sg, double *Sn, double *avg) {
   const int64_t ne = B.ne;
@@ -333,7 +370,7 @@ extern "C" int fast_gpu_gauss_stress(fast_gpu_ctx *c, int32_t b, int64_t first, 
 static int nodal_tables(Ctx &c, Bucket &B) {
   if (B.d_tr) return FAST_GPU_OK;
   std::vector<double> TR;
-  if (!extrapolation_matrix(B.type, B.ngp, TR)) {
+  if (!extrapolation_matrix(B.type, B.ngp, TR, B.pd)) {
     c.err = "nodal_stress: no extrapolation for this element and rule";
     return FAST_GPU_ENOTSUP;
   }
@@ -366,8 +403,13 @@ static int nodal_tables(Ctx &c, Bucket &B) {
 extern "C" int fast_gpu_nodal_stress(fast_gpu_ctx *c, int32_t b, double *elem_nodal, double *nodal) {
   if (!c || b < 0 || b >= (int)c->buckets.size() || (!elem_nodal && !nodal)) return FAST_GPU_EINVAL;
   Bucket &B = c->buckets[b];
-  if (B.tl || B.type == FAST_ELEM_BSP_SOLID) {
-    c->err = "nodal_stress: small-strain hex buckets only";
+  if (B.tl) {
+    c->err = "nodal_stress: small-strain buckets only";
+    return FAST_GPU_ENOTSUP;
+  }
+  const bool bsp = B.type == FAST_ELEM_BSP_SOLID;
+  if (bsp && !(B.ngp[0] == B.ngp[1] && B.ngp[1] == B.ngp[2])) {
+    c->err = "nodal_stress: B-spline buckets with the same Gauss rule in every direction only";
     return FAST_GPU_ENOTSUP;
   }
   if (!c->d_disp) {
@@ -379,9 +421,11 @@ extern "C" int fast_gpu_nodal_stress(fast_gpu_ctx *c, int32_t b, double *elem_no
   const int64_t ne = B.ne, nn = B.nn, ng = B.ng;
   const size_t nsg = (size_t)ne * ng * 6, nsn = (size_t)ne * nn * 6, nav = (size_t)c->nnode * 6;
   double *buf = nullptr;
-  SCK(cudaMalloc((void **)&buf, sizeof(double) * (nsg + nsn + nav) + sizeof(int32_t) * ne + 16));
-  double *Sg = buf, *Sn = buf + nsg, *avg = nodal ? buf + nsg + nsn : nullptr;
-  int32_t *d_idx = reinterpret_cast<int32_t *>(buf + nsg + nsn + nav);
+  // (B-spline buckets: their Gauss-point strains go to a scratch block too)
+  const size_t nse = bsp ? nsg : 0;
+  SCK(cudaMalloc((void **)&buf, sizeof(double) * (nsg + nsn + nav + nse) + sizeof(int32_t) * ne + 16));
+  double *Sg = buf, *Sn = buf + nsg, *avg = nodal ? buf + nsg + nsn : nullptr, *Se = buf + nsg + nsn + nav;
+  int32_t *d_idx = reinterpret_cast<int32_t *>(buf + nsg + nsn + nav + nse);
   SCK(cudaMemcpyAsync(d_idx, B.inv.data(), sizeof(int32_t) * ne, cudaMemcpyHostToDevice, c->stream));
   SCK(cudaMemsetAsync(c->d_status, 0, sizeof(int32_t), c->stream));
   cudaError_t e = cudaErrorInvalidValue;
@@ -391,6 +435,16 @@ extern "C" int fast_gpu_nodal_stress(fast_gpu_ctx *c, int32_t b, double *elem_no
   else if (B.type == FAST_ELEM_HEX20 && ng == 27) e = run_nodal<20, 27>(*c, B, d_idx, Sg, Sn, avg);
   else if (B.type == FAST_ELEM_HEX20 && ng == 8) e = run_nodal<20, 8>(*c, B, d_idx, Sg, Sn, avg);
   else if (B.type == FAST_ELEM_HEX20 && ng == 64) e = run_nodal<20, 64>(*c, B, d_idx, Sg, Sn, avg);
+  else if (bsp) {
+    const int *p = B.pd, g1 = B.ngp[0];
+    if (p[0] == 2 && p[1] == 2 && p[2] == 2 && g1 == 3) e = run_nodal_bsp<2, 2, 2, 3>(*c, B, d_idx, Se, Sg, Sn, avg);
+    else if (p[0] == 2 && p[1] == 2 && p[2] == 2 && g1 == 4) e = run_nodal_bsp<2, 2, 2, 4>(*c, B, d_idx, Se, Sg, Sn, avg);
+    else if (p[0] == 3 && p[1] == 3 && p[2] == 3 && g1 == 4) e = run_nodal_bsp<3, 3, 3, 4>(*c, B, d_idx, Se, Sg, Sn, avg);
+    else if (p[0] == 3 && p[1] == 3 && p[2] == 2 && g1 == 4) e = run_nodal_bsp<3, 3, 2, 4>(*c, B, d_idx, Se, Sg, Sn, avg);
+    else if (p[0] == 4 && p[1] == 2 && p[2] == 4 && g1 == 5) e = run_nodal_bsp<4, 2, 4, 5>(*c, B, d_idx, Se, Sg, Sn, avg);
+    else if (p[0] == 4 && p[1] == 2 && p[2] == 2 && g1 == 5) e = run_nodal_bsp<4, 2, 2, 5>(*c, B, d_idx, Se, Sg, Sn, avg);
+    else if (p[0] == 5 && p[1] == 2 && p[2] == 5 && g1 == 6) e = run_nodal_bsp<5, 2, 5, 6>(*c, B, d_idx, Se, Sg, Sn, avg);
+  }
   SCK(e);
   if (elem_nodal) SCK(cudaMemcpyAsync(elem_nodal, Sn, sizeof(double) * nsn, cudaMemcpyDeviceToHost, c->stream));
   if (nodal) SCK(cudaMemcpyAsync(nodal, avg, sizeof(double) * nav, cudaMemcpyDeviceToHost, c->stream));

@@ -643,10 +643,14 @@ int fast_gpu_support_reactions(fast_gpu_ctx *ctx, const uint8_t *supported, int3
 int fast_gpu_gauss_stress(fast_gpu_ctx *ctx, int32_t bucket, int64_t first, int64_t count, double *strain,
                           double *stress);
 /* The printing step's nodal stresses at the current displacements, for a
- * whole small-strain hex bucket: elem_nodal [num_elems][nn][6] (caller's
- * element order) = TR x the Gauss-point stresses, TR the extrapolation of
+ * whole small-strain hex or B-spline bucket (B-spline: the same Gauss rule in
+ * every direction): elem_nodal [num_elems][nn][6] (caller's element order) =
+ * TR x the Gauss-point stresses, TR the extrapolation of
  * cElmParam::CompTRMatrix (elc/elmparam.cpp:1444-1535: least-squares linear
- * field in r, s, t evaluated at the nodes; the average for a one-point rule),
+ * field in r, s, t evaluated at the nodes' natural coordinates, for a
+ * B-spline element the uniform grid of its control points over [-1, 1]^3,
+ * cShapeBspSolid::NodeNatCoord shp/shpbsp.cpp:906-923; the average for a
+ * one-point rule),
  * as cElmParam::NodalStress returns them (:1304-1312); nodal [num_nodes][6]
  * their average at each node over the bucket's elements, summed in element
  * order as cControl::PrintAvrNodalStress does (ctrl/ctrl.cpp:2397-2440),

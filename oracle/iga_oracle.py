@@ -191,3 +191,25 @@ def elem_tl(deck, e, ue):
 def elems_stiff(deck, elems=None):
     elems = range(deck.num_elems) if elems is None else elems
     return np.array([elem_stiff(deck, int(e)) for e in elems])
+
+
+def extrapolation_matrix(degree, ngp):
+    """TR [nn][ng] of cElmParam::CompTRMatrix (elc/elmparam.cpp:1444-1535)
+    for a B-spline solid element: the least-squares linear field in (r, s, t)
+    through the Gauss points (rule order, r fastest) evaluated at the control
+    points' natural coordinates, the uniform grid of p+1 points per
+    direction over [-1, 1] (cShapeBspSolid::NodeNatCoord,
+    shp/shpbsp.cpp:906-923, r fastest); the point average for a one-point
+    rule."""
+    nb = [int(p) + 1 for p in degree]
+    gp = [(r, s, t) for t in _GR.get(ngp[2], [0.0]) for s in _GR.get(ngp[1], [0.0]) for r in _GR.get(ngp[0], [0.0])]
+    ng = len(gp)
+    nn = nb[0] * nb[1] * nb[2]
+    if ngp[0] == 1:
+        return np.full((nn, ng), 1.0 / ng)
+    U = np.array([[1.0, r, s, t] for r, s, t in gp])
+    A = U.T @ U
+    Q = np.linalg.solve(A, U.T)                     # [4][ng]: A^-1 u_g for every point
+    CN = np.array([[1.0, -1.0 + 2.0 * k / degree[0], -1.0 + 2.0 * j / degree[1], -1.0 + 2.0 * i / degree[2]]
+                   for i in range(nb[2]) for j in range(nb[1]) for k in range(nb[0])])
+    return CN @ Q

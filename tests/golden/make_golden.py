@@ -128,7 +128,7 @@ def iga_cases(tmp):
     d = decks.bspline_box(2, (3, 2, 2), L=(3.0, 2.0, 1.0), jitter=0.05, seed=1)
     d.tol = 1e-13
     d.maxit = 100000
-    run_case("iga_p2_box", d, tmp, extra=("--stress",))
+    run_case("iga_p2_box", d, tmp, extra=("--stress", "--nodal"))
     d = decks.bspline_box(3, (2, 2, 1), L=(2.0, 2.0, 0.5), jitter=0.05, seed=2)
     d.tol = 1e-13
     d.maxit = 100000

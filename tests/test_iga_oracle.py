@@ -126,3 +126,15 @@ def test_bspline_gauss_point_stresses():
         st, ss = io.elem_stress(d, int(e), un[d.conn[e]].ravel())
         assert np.abs(st - g["ref_elm_strain"][k]).max() <= 1e-12 * np.abs(g["ref_elm_strain"]).max()
         assert np.abs(ss - g["ref_elm_stress"][k]).max() <= 1e-12 * np.abs(g["ref_elm_stress"]).max()
+
+
+def test_bspline_extrapolation_matches_reference_nodal_stress():
+    """The restated CompTRMatrix for a B-spline element (least squares through
+    the Gauss points, evaluated on the control points' uniform natural grid)
+    times the reference's Gauss-point stresses gives the element-nodal
+    stresses the reference's cElmParam::NodalStress returned."""
+    d, g = gio.load("iga_p2_box")
+    TR = io.extrapolation_matrix(d.patch.degree, d.ngp)
+    est = np.einsum("ag,egk->eak", TR, g["ref_elm_stress"])
+    ref = g["ref_elm_nodal_stress"]
+    assert np.abs(est - ref).max() <= 1e-12 * np.abs(ref).max()
